@@ -1,0 +1,274 @@
+/*
+ * pgk_gpu.h -- C ABI of libpgkgpu.so, the B200 (sm_100a) force-and-integration
+ * engine for the peachgk_md molecular-dynamics driver.
+ *
+ * The reference program keeps all state in Fortran module globals
+ * (md_global.inc) and calls subroutines with explicit interfaces
+ * (interface_interact.F90, interface_mdtech.F90, interface_mddriver.F90).
+ * This header exposes the same operations as plain C functions taking plain
+ * pointers and sizes.  Every array follows the reference layout:
+ *   - coordinates / velocities / forces: (3,natom) Fortran column-major, i.e.
+ *     x,y,z interleaved per atom, FP64, reduced units (calbase.F90:21-40);
+ *   - atom indices: 1-based, exactly as stored in the Fortran arrays;
+ *   - CSR lists: 1-based start indices with the reference's 0 sentinel for an
+ *     empty row (mkexcl.F90, mklist_cell.F90:297-329).
+ * The library owns device mirrors of the state.  Between downloads the device
+ * copy is authoritative.  Every entry point returns a pgk_status (0 = OK); the
+ * reference STOPs on the same conditions.
+ *
+ * One context is driven from one host thread; it uses one CUDA stream.
+ */
+#ifndef PGK_GPU_H
+#define PGK_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque engine context: device mirrors of the md_global state. */
+typedef struct pgk_ctx pgk_ctx;
+
+/* ---- status codes (each replaces a STOP of the reference) ---------------- */
+typedef int32_t pgk_status;
+#define PGK_OK                 0
+#define PGK_E_LIST_OVERFLOW    1  /* mklist_cell.F90:342-346 "nlistnball exceed" */
+#define PGK_E_CELL_OVERFLOW    2  /* mklist_cell.F90:121-145,170-176 */
+#define PGK_E_RATTLE_NOCONV    3  /* rattle.F90 "RATTLE(C) failed to converge" */
+#define PGK_E_BOX_TOO_SMALL    4  /* calvol.F90 / calbox.F90 "rcut is over half cell" */
+#define PGK_E_DEVICE_TIMEOUT   5  /* a bounded device wait gave up */
+#define PGK_E_CUDA             6  /* a CUDA runtime call failed */
+#define PGK_E_INVALID          7  /* bad argument (null pointer, size, unsupported option) */
+#define PGK_E_NOMEM            8  /* device allocation failed */
+#define PGK_E_UNSUPPORTED      9  /* option of the reference that this engine does not build */
+#define PGK_E_RATTLEV_NOCONV  10  /* rattle_mtk.F90 "RATTLE(V) failed to converge" */
+
+/* ---- option values ------------------------------------------------------- */
+#define PGK_PREC_FP64   0   /* all-FP64 device path (parity path) */
+#define PGK_PREC_MIXED  1   /* FP32 pair/SPME/bonded arithmetic, int64 fixed-point sums */
+
+#define PGK_MTS_LONG    1   /* md_global.inc:130 MTS_LONG */
+#define PGK_MTS_SHORT   3   /* md_global.inc:132 MTS_SHORT */
+#define PGK_MTS_NONE    0   /* term switched off (commented-out mts_* keyword) */
+
+#define PGK_PCONT_ISO    0  /* pcont_axis 'iso'   (nhcpisoint.F90)            */
+#define PGK_PCONT_ANISO  1  /* pcont_axis 'aniso' (nhcpanisoint.F90, dir 0)   */
+#define PGK_PCONT_X      2  /* pcont_axis 'x'     (nhcpanisoint.F90, dir 1)   */
+#define PGK_PCONT_Y      3
+#define PGK_PCONT_Z      4
+
+#define PGK_LIST_AUTO    0  /* ifcellindex with the rdscript.F90:1595-1610 fallback */
+#define PGK_LIST_CELL    1  /* force mklist_cell order */
+#define PGK_LIST_ALLPAIR 2  /* force mklist2a order   */
+
+/* ---- system description (topology + parameters), read once at pgk_init --
+ * Per-term parameters are already expanded from the reference's type tables
+ * (e.g. para_cbond(indexbondtyp(k)) -> para_cbond[k-1]).  Angles/phases are
+ * in radians (prepmd.F90:230-237 converts degrees); charges are already
+ * multiplied by 1/sqrt(4 pi eps0) (prepmd.F90:239-241). */
+typedef struct pgk_system {
+    int32_t natom;
+    const double*  atmmass;       /* [natom]                                  */
+    const double*  atmchrg;       /* [natom]                                  */
+    const int32_t* atmindex;      /* [natom] 1-based LJ type                  */
+    int32_t        ntyp;
+    const double*  vdw_radij;     /* [ntyp*ntyp] column-major (i,j): R_min,ij  */
+    const double*  vdw_welij;     /* [ntyp*ntyp] well depth E_ij              */
+    const int32_t* inter_inttyp;  /* [ntyp*ntyp] 1 = INTTYPE_VDW, else no LJ; NULL = all LJ */
+
+    int32_t        nmole;         /* molecules (transcor.F90, calpress.F90)    */
+    const int32_t* molept_index;  /* [nmole+1], 1-based                        */
+    const int32_t* molept_list;   /* [molept_index[nmole]-1], 1-based atoms    */
+
+    const int32_t* index_excl;    /* [natom+1] mkexcl.F90 output (j>i, 0 sentinel) */
+    const int32_t* list_excl;
+
+    int32_t nbond;                /* calbond.F90 */
+    const int32_t *ibond, *jbond;
+    const double  *para_cbond, *para_eqbond;
+
+    int32_t nangl;                /* calangl.F90 */
+    const int32_t *iangl, *jangl, *kangl;
+    const double  *para_cangl, *para_eqangl;
+
+    int32_t ntors;                /* caltors.F90 + 1-4 flags of calnon14.F90 */
+    const int32_t *itors, *jtors, *ktors, *ltors;
+    const int32_t *para_divfac;
+    const double  *para_barhig, *para_phsang, *para_period;
+    const int32_t *ifcalnonb14;   /* may be NULL: no 1-4 from periodic torsions */
+    const double  *para_divfac_vdw, *para_divfac_elc, *ring14;
+
+    int32_t ntorsrb;              /* caltorsrb.F90 */
+    const int32_t *itorsrb, *jtorsrb, *ktorsrb, *ltorsrb;
+    const double  *para_barhigrb; /* [6*ntorsrb], C0..C5 per term             */
+    const int32_t *ifcalnonb14_rb;
+    const double  *para_divfac_vdwrb, *para_divfac_elcrb, *ring14_rb;
+
+    int32_t nconst;               /* constraint groups (rattle.F90 DOconstr)   */
+    const int32_t* index_mconst;  /* [nconst+1], 1-based                        */
+    const int32_t* list_mconst;   /* 1-based constraint ids                     */
+    int32_t nconstraint;
+    const int32_t *iconst, *jconst;
+    const double  *dconst;
+
+    int32_t degfree_all;          /* prepmd.F90:250-330                          */
+} pgk_system;
+
+/* ---- run-time parameters (peachgk.ini keywords after calbase) ----------- */
+typedef struct pgk_params {
+    double  xcel, ycel, zcel;     /* initial box                               */
+    double  alpha;                /* Ewald alpha [1/length]                    */
+    double  rrcut;                /* Ewald real-space cutoff                   */
+    double  rcut;                 /* LJ cutoff                                 */
+    double  rcut_book;            /* bookkeeping radius                        */
+    int32_t nstep_book;           /* list renewal interval                     */
+    int32_t list_mode;            /* PGK_LIST_*                                */
+    int32_t ifspme;               /* 1: SPME reciprocal space                  */
+    int32_t nfft1, nfft2, nfft3, pme_order;
+    int32_t nspltbl;              /* erfc spline table points (spline_interp.F90) */
+    int32_t precision;            /* PGK_PREC_*                                */
+    int32_t mts_bond, mts_angl, mts_tors, mts_torsrb;
+    int32_t mts_vdw;              /* gates ewaldr (LJ + real-space Ewald)      */
+    int32_t mts_ewk;              /* gates fft_pme                             */
+    int32_t mts_vdw14, mts_elc14; /* calnon14 runs when both equal the flag    */
+    int32_t ifnetqcorrp;          /* net-charge correction for pressure        */
+    int32_t max_nbr;              /* per-atom capacity of the device pair list (0 = auto) */
+} pgk_params;
+
+/* ---- integrator parameters (moldyn_*.F90 arguments) ---------------------- */
+typedef struct pgk_mdparams {
+    double  dt_long_cal;          /* reduced time step                         */
+    int32_t nstep_short;          /* XO-RESPA inner steps                      */
+    int32_t mchain;               /* NHC length (<= 8)                         */
+    double  text;                 /* reduced target temperature                */
+    double  qmass[8];             /* prepmd.F90:515-518                        */
+    double  vmass;                /* prepmd.F90:521-525                        */
+    int32_t next, nyosh;          /* Trotter sub-steps, Yoshida-Suzuki order   */
+    double  yscoeff[8];           /* prepmd.F90:535-547                        */
+    double  pext;                 /* reduced external pressure                 */
+    int32_t pcont_axis;           /* PGK_PCONT_*                               */
+    int32_t ifrattle;
+    double  eps_rattle;
+    int32_t pressinterval;        /* calpress cadence in NVT (MTK: every step) */
+    int32_t outinterval;          /* energies are evaluated on these steps     */
+} pgk_mdparams;
+
+/* ---- energies (calforce.F90 OUTPUT names) ------------------------------- */
+typedef struct pgk_energies {
+    double pot_tot, pot_nonbon;
+    double pot_vdw, pot_elc, pot_ewk, pot_ewc, pot_ewnq;
+    double pot_vdw14, pot_elc14;
+    double pot_bond, pot_angl, pot_tors, pot_torsrb;
+} pgk_energies;
+
+/* ---- virials (ewaldrp / fft_pmep / cal*p OUTPUT names), tensors (3,3)
+ *      column-major: t[a + 3*b] = sum f_a * r_b. ---------------------------- */
+typedef struct pgk_virials {
+    double pot_viri_coul, pot_viri_lj;
+    double pot_virit_coul[9], pot_virit_lj[9];
+    double atm_viri_bond, atm_viri_angl, atm_viri_tors, atm_viri_14;
+    double atm_virit_bond[9], atm_virit_angl[9], atm_virit_tors[9], atm_virit_14[9];
+} pgk_virials;
+
+/* ---- thermostat / barostat state (md_global.inc xlogs, vlogs, ...) ------- */
+typedef struct pgk_chain {
+    double xlogs[8], vlogs[8];
+    double xlogv, vlogv;
+    double xboxh[3], vboxg[3];
+    double pint, pintt[9];
+} pgk_chain;
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* Library version string. */
+const char* pgk_version(void);
+/* Human-readable text of a status code (the reference's STOP message). */
+const char* pgk_status_string(pgk_status s);
+
+/* Build a context: copies the topology and parameters to the device, builds
+ * the erfc spline tables (spline_interp_init, spline_interp.F90:14-136), the
+ * B-spline moduli and self energy (fft_pme_init, fft_pme_init.F90:14-180) and
+ * the Ewald k-cutoff (erf_corr_cutoff.F90:28-62).  Replaces the L3
+ * pre-processing calls main_md.F90:1101-1185 for the device side. */
+pgk_status pgk_init(const pgk_system* sys, const pgk_params* prm, pgk_ctx** out);
+pgk_status pgk_free(pgk_ctx* ctx);
+/* Last error message recorded on this context (empty if none). */
+const char* pgk_last_error(const pgk_ctx* ctx);
+
+/* ---- state transfer (host module arrays <-> device mirrors) -------------- */
+/* atmcor/atmvel: (3,natom); box: xcel,ycel,zcel.  atmvel may be NULL. */
+pgk_status pgk_upload_state(pgk_ctx* ctx, const double* atmcor, const double* atmvel,
+                            const double* box);
+pgk_status pgk_download_state(pgk_ctx* ctx, double* atmcor, double* atmvel, double* box);
+pgk_status pgk_set_chain(pgk_ctx* ctx, const pgk_chain* ch);
+pgk_status pgk_get_chain(pgk_ctx* ctx, pgk_chain* ch);
+
+/* ---- fine-grained operations with the reference's names ----------------- */
+/* transcor.F90: wrap each molecule by its first atom into [0,L). */
+pgk_status pgk_transcor(pgk_ctx* ctx);
+
+/* mklist_cell.F90:8-352 / mklist2a (mklist.F90:8-234) with the
+ * rdscript.F90:1595-1610 fallback: builds the bookkeeping pair list on the
+ * device.  *nlistnball receives the reference's nlistnball (entries incl.
+ * the 0 sentinels of empty rows). */
+pgk_status pgk_mklist_cell(pgk_ctx* ctx, int64_t* nlistnball);
+
+/* Copy the last list out in the reference CSR layout: nb_indexall[natom]
+ * (1-based start of row i; the entry after the last row holds
+ * nlistnball+1) and nb_listall[nlistnball] (1-based j, 0 sentinel),
+ * rows in the reference order (cell scan order for mklist_cell, ascending j
+ * for mklist2a).  cap = capacity of nb_listall. */
+pgk_status pgk_get_nblist(pgk_ctx* ctx, int32_t* nb_indexall, int32_t* nb_listall,
+                          int64_t cap, int64_t* nlistnball);
+
+/* calforce.F90:8-1073 for one MTS group (PGK_MTS_LONG / PGK_MTS_SHORT):
+ * force (3,natom) is OVERWRITTEN with the group's force (not acceleration);
+ * ene / vir may be NULL.  want_virial selects the *p (virial) variants. */
+pgk_status pgk_calforce(pgk_ctx* ctx, int32_t mts_flag, double* force,
+                        pgk_energies* ene, pgk_virials* vir);
+
+/* Single-kernel entries used by the parity tests (force += into `force`): */
+/* ewaldrp (ewaldr.F90:404-838) incl. the excluded-pair erf correction. */
+pgk_status pgk_ewaldr(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
+/* fft_pmep (fft_pme.F90:144-270): SPME reciprocal force, pot_ewk, tensor. */
+pgk_status pgk_fft_pme(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
+/* calbondp/calanglp/caltorsp/caltorsrbp/calnon14p (all terms, no MTS gate). */
+pgk_status pgk_calbonded(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
+
+/* rattle_c (rattle.F90:6-272) on the device state, given atmcor_old (3,natom)
+ * on the host (copied in).  dt_short = time step used for the correction. */
+pgk_status pgk_rattle_c(pgk_ctx* ctx, const double* atmcor_old, double eps_rattle,
+                        double dt_short_cal);
+/* rattlep_v (rattle_mtk.F90:278-542) on the device velocities. */
+pgk_status pgk_rattlep_v(pgk_ctx* ctx, double eps_rattle);
+
+/* ---- stage drivers: the whole XO-RESPA loop stays on the device ---------- */
+/* moldyn.F90 NVE (no thermostat), moldyn_nhc.F90 NVT-NHC and moldyn_mtk.F90
+ * NPT-MTK, steps inistep..endstep inclusive (step 0 = initial force only).
+ * `ene` receives the energies of the last step whose index is a multiple of
+ * md->outinterval (or of endstep when outinterval <= 0); may be NULL. */
+pgk_status pgk_moldyn_nve(pgk_ctx* ctx, int64_t inistep, int64_t endstep,
+                          const pgk_mdparams* md, pgk_energies* ene);
+pgk_status pgk_moldyn_nhc(pgk_ctx* ctx, int64_t inistep, int64_t endstep,
+                          const pgk_mdparams* md, pgk_energies* ene);
+pgk_status pgk_moldyn_mtk(pgk_ctx* ctx, int64_t inistep, int64_t endstep,
+                          const pgk_mdparams* md, pgk_energies* ene);
+
+/* Kinetic energy sum(m v^2) and atomic pressure tensor (calpress.F90, atomic
+ * branch) of the current device state; press9 may be NULL. */
+pgk_status pgk_calpress(pgk_ctx* ctx, double* kint, double* pressatm_tot, double* press9);
+
+/* Wait for the context's stream; returns the first sticky device error. */
+pgk_status pgk_sync(pgk_ctx* ctx);
+
+/* Number of kernels this context has launched so far (for launch accounting). */
+int64_t pgk_kernel_launches(const pgk_ctx* ctx);
+
+/* CUDA stream of the context (cudaStream_t as void*), for callers that time
+ * the context's kernels with their own events. */
+void* pgk_stream(const pgk_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PGK_GPU_H */

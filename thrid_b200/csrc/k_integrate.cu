@@ -1,0 +1,531 @@
+// k_integrate.cu -- FP64 integrator pieces of moldyn.F90 / moldyn_nhc.F90 /
+// moldyn_mtk.F90, RATTLE (rattle.F90, rattle_mtk.F90), the NHC / MTK chain
+// updates (nhcint.F90, nhcpisoint.F90, nhcpanisoint.F90), calvol/calbox and
+// the atomic pressure of calpress.F90.  Everything here is FP64 in both
+// precision modes (positions, velocities, constraints, chain variables).
+//
+// Per-atom kernels are HBM-bound (one read + one write of x/v, one read of the
+// force accumulator); the chain and box kernels run on one thread and read
+// the kinetic-energy / virial sums from the fixed-point accumulators, so a
+// whole MD step needs no host round trip and can be captured in a CUDA graph.
+#include <cmath>
+
+#include "pgk_ctx.cuh"
+
+template <bool MIXED>
+__global__ void k_kick_long(double* __restrict__ vel, const void* __restrict__ fl, const double* __restrict__ mass,
+                            int n, const DynState* __restrict__ dyn) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    int d = k % 3;
+    double a = force_get<MIXED>(fl, k) / mass[k / 3];
+    vel[k] = vel[k] * dyn->kl_s[d] + a * dyn->kl_b[d];
+}
+
+template <bool MIXED>
+__global__ void k_kick_short(double* __restrict__ vel, const void* __restrict__ fs, const double* __restrict__ mass,
+                             int n, const DynState* __restrict__ dyn) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    double a = force_get<MIXED>(fs, k) / mass[k / 3];
+    vel[k] = vel[k] + dyn->ks_b * a;
+}
+
+__global__ void k_drift(double* __restrict__ pos, double* __restrict__ old, const double* __restrict__ vel, int n,
+                        const DynState* __restrict__ dyn, int save) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    int d = k % 3;
+    double x = pos[k];
+    if (save) old[k] = x;
+    pos[k] = x * dyn->dr_a[d] + vel[k] * dyn->dr_b[d];
+}
+
+// rattle_c / rattle_cmtk: one thread per constraint group, Gauss-Seidel sweeps
+// in the reference order, at most 300 sweeps (bounded; failure -> status bit).
+__global__ void k_rattle_pos(double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ old,
+                             const double* __restrict__ mass, const int* __restrict__ gidx,
+                             const int* __restrict__ glist, const int2* __restrict__ cij, const double* __restrict__ cd,
+                             int ngroup, double eps, double dt, int use_rv, const DynState* __restrict__ dyn,
+                             unsigned* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroup) return;
+    int i1 = gidx[g], i2 = gidx[g + 1];
+    double rvi[3] = {1.0, 1.0, 1.0};
+    if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+    bool finished = false;
+    for (int it = 0; it < 300 && !finished; ++it) {
+        finished = true;
+        for (int ii = i1; ii < i2; ++ii) {
+            int nc = glist[ii];
+            int ib = cij[nc].x, jb = cij[nc].y;
+            double dij = cd[nc];
+            double R0 = pos[3 * ib] - pos[3 * jb], R1 = pos[3 * ib + 1] - pos[3 * jb + 1],
+                   R2 = pos[3 * ib + 2] - pos[3 * jb + 2];
+            double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
+            double d2 = dij * dij;
+            double delta = fabs(Rsq - d2) / d2;
+            if (delta < eps) continue;
+            finished = false;
+            double O0 = old[3 * ib] - old[3 * jb], O1 = old[3 * ib + 1] - old[3 * jb + 1],
+                   O2 = old[3 * ib + 2] - old[3 * jb + 2];
+            double RR = R0 * O0 + R1 * O1 + R2 * O2;
+            double mi = 1.0 / mass[ib], mj = 1.0 / mass[jb];
+            double gij = (Rsq - d2) / (2.0 * RR * (mi + mj) * dt);
+            double G[3] = {gij * O0, gij * O1, gij * O2};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pos[3 * ib + d] = pos[3 * ib + d] - mi * G[d] * dt;
+                pos[3 * jb + d] = pos[3 * jb + d] + mj * G[d] * dt;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double Gv = G[d] * rvi[d];
+                vel[3 * ib + d] = vel[3 * ib + d] - mi * Gv;
+                vel[3 * jb + d] = vel[3 * jb + d] + mj * Gv;
+            }
+        }
+    }
+    if (!finished) atomicOr(status, ST_RATTLE_NOCONV);
+}
+
+// rattlep_v (rattle_mtk.F90:278-542)
+__global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ mass,
+                             const int* __restrict__ gidx, const int* __restrict__ glist, const int2* __restrict__ cij,
+                             const double* __restrict__ cd, int ngroup, double eps, unsigned* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroup) return;
+    int i1 = gidx[g], i2 = gidx[g + 1];
+    double eps2 = eps * eps;
+    bool finished = false;
+    for (int it = 0; it < 300 && !finished; ++it) {
+        finished = true;
+        for (int ii = i1; ii < i2; ++ii) {
+            int nc = glist[ii];
+            int ib = cij[nc].x, jb = cij[nc].y;
+            double dij = cd[nc];
+            double R[3], V[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                R[d] = pos[3 * ib + d] - pos[3 * jb + d];
+                V[d] = vel[3 * ib + d] - vel[3 * jb + d];
+            }
+            double RV = R[0] * V[0] + R[1] * V[1] + R[2] * V[2];
+            double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+            double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+            double phi = RV * RV / R2 * V2;   // precedence as in the reference
+            if (phi < eps2) continue;
+            finished = false;
+            double mi = 1.0 / mass[ib], mj = 1.0 / mass[jb];
+            double kij = RV / (dij * dij * (mi + mj));
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double KR = kij * R[d];
+                vel[3 * ib + d] = vel[3 * ib + d] - mi * KR;
+                vel[3 * jb + d] = vel[3 * jb + d] + mj * KR;
+            }
+        }
+    }
+    if (!finished) atomicOr(status, ST_RATTLEV_NOCONV);
+}
+
+// sum m v^2 and sum m v_a v_b (nhcint kint, calpress kinetic terms)
+__global__ void k_kinetic(const double* __restrict__ vel, const double* __restrict__ mass, int n, long long* acc) {
+    double v[10] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m = mass[i], x = vel[3 * i], y = vel[3 * i + 1], z = vel[3 * i + 2];
+        v[0] += m * (x * x + y * y + z * z);
+        const double w[3] = {x, y, z};
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) v[1 + a + 3 * b] += m * w[a] * w[b];
+    }
+    const int idx[10] = {A_KE, A_KET + 0, A_KET + 1, A_KET + 2, A_KET + 3, A_KET + 4, A_KET + 5, A_KET + 6,
+                         A_KET + 7, A_KET + 8};
+    block_acc<10>(v, acc, idx);
+}
+
+__device__ __forceinline__ double fixv(const long long* acc, int k) { return (double)acc[k] * PGK_FORCE_ISCALE; }
+
+// ---- chain updates (single thread) -------------------------------------------
+struct ChainArgs {
+    pgk_mdparams md;
+    int degfree;
+    int kind;          // 1 nhcint, 2 nhcpisoint, 3 nhcpanisoint
+};
+
+__device__ void chain_tail(ChainDev& c, const pgk_mdparams& md, double* glogs, double w4, double w8, double gkt,
+                           bool down) {
+    int M = md.mchain;
+    const double* q = md.qmass;
+    if (down) {
+        glogs[M - 1] = (q[M - 2] * c.vlogs[M - 2] * c.vlogs[M - 2] - gkt) / q[M - 1];
+        c.vlogs[M - 1] = c.vlogs[M - 1] + glogs[M - 1] * w4;
+        for (int i = M - 2; i >= 1; --i) {
+            glogs[i] = (q[i - 1] * c.vlogs[i - 1] * c.vlogs[i - 1] - gkt) / q[i];
+            double e8 = exp(-1.0 * w8 * c.vlogs[i + 1]);
+            c.vlogs[i] = c.vlogs[i] * e8 * e8 + w4 * glogs[i] * e8;
+        }
+    } else {
+        for (int i = 1; i <= M - 2; ++i) {
+            glogs[i] = (q[i - 1] * c.vlogs[i - 1] * c.vlogs[i - 1] - gkt) / q[i];
+            double e8 = exp(-1.0 * w8 * c.vlogs[i + 1]);
+            c.vlogs[i] = c.vlogs[i] * e8 * e8 + w4 * glogs[i] * e8;
+        }
+        glogs[M - 1] = (q[M - 2] * c.vlogs[M - 2] * c.vlogs[M - 2] - gkt) / q[M - 1];
+        c.vlogs[M - 1] = c.vlogs[M - 1] + glogs[M - 1] * w4;
+    }
+}
+
+__global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ChainDev c = *chain;
+    const pgk_mdparams& md = a.md;
+    int M = md.mchain;
+    double dt = md.dt_long_cal;
+    double kint = fixv(acc, A_KE);
+    double glogs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double gkt = md.text;
+    if (a.kind == 1) {   // nhcint.F90:8-140
+        double gnkt = md.text * (double)a.degfree;
+        glogs[0] = (kint - gnkt) / md.qmass[0];
+        for (int inc = 0; inc < md.next; ++inc)
+            for (int iy = 0; iy < md.nyosh; ++iy) {
+                double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
+                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                double e8 = exp(-1.0 * w8 * c.vlogs[1]);
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                chain_tail(c, md, glogs, w4, w8, gkt, false);
+            }
+    } else if (a.kind == 2) {   // nhcpisoint.F90:6-162
+        double gn1kt = md.text * (double)(a.degfree + 1);
+        double dnf = 3.0 / (double)a.degfree;
+        double vol = exp(3.0 * c.xlogv);
+        glogs[0] = (kint + md.vmass * c.vlogv * c.vlogv - gn1kt) / md.qmass[0];
+        double glogv = (dnf * kint + 3.0 * vol * (c.pint - md.pext)) / md.vmass;
+        for (int inc = 0; inc < md.next; ++inc)
+            for (int iy = 0; iy < md.nyosh; ++iy) {
+                double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
+                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                double e8 = exp(-1.0 * w8 * c.vlogs[1]);
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                e8 = exp(-1.0 * w8 * c.vlogs[0]);
+                c.vlogv = c.vlogv * e8 * e8 + w4 * glogv * e8;
+                for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
+                c.vlogv = c.vlogv * e8 * e8 + w4 * glogv * e8;
+                glogs[0] = (kint + md.vmass * c.vlogv * c.vlogv - gn1kt) / md.qmass[0];
+                e8 = exp(-1.0 * w8 * c.vlogs[1]);
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                chain_tail(c, md, glogs, w4, w8, gkt, false);
+            }
+    } else {   // nhcpanisoint.F90:8-189
+        int dir = md.pcont_axis == PGK_PCONT_ANISO ? 0 : md.pcont_axis - 1;
+        double gndfkt = md.text * (double)(a.degfree + (dir == 0 ? 3 : 1));
+        double dnf = 1.0 / (double)a.degfree;
+        double vol = c.xboxh[0] * c.xboxh[1] * c.xboxh[2];
+        double pv[3] = {c.pintt[0], c.pintt[4], c.pintt[8]};
+        double vb2 = c.vboxg[0] * c.vboxg[0] + c.vboxg[1] * c.vboxg[1] + c.vboxg[2] * c.vboxg[2];
+        glogs[0] = (kint + md.vmass * vb2 - gndfkt) / md.qmass[0];
+        double gb[3];
+        for (int d = 0; d < 3; ++d) gb[d] = (dnf * kint + vol * (pv[d] - md.pext)) / md.vmass;
+        for (int inc = 0; inc < md.next; ++inc)
+            for (int iy = 0; iy < md.nyosh; ++iy) {
+                double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
+                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                double e8 = exp(-1.0 * w8 * c.vlogs[1]);
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                e8 = exp(-1.0 * w8 * c.vlogs[0]);
+                for (int d = 0; d < 3; ++d)
+                    if (dir == 0 || d == dir - 1) c.vboxg[d] = c.vboxg[d] * e8 * e8 + w4 * gb[d] * e8;
+                for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
+                for (int d = 0; d < 3; ++d)
+                    if (dir == 0 || d == dir - 1) c.vboxg[d] = c.vboxg[d] * e8 * e8 + w4 * gb[d] * e8;
+                vb2 = c.vboxg[0] * c.vboxg[0] + c.vboxg[1] * c.vboxg[1] + c.vboxg[2] * c.vboxg[2];
+                glogs[0] = (kint + md.vmass * vb2 - gndfkt) / md.qmass[0];
+                e8 = exp(-1.0 * w8 * c.vlogs[1]);
+                c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+                chain_tail(c, md, glogs, w4, w8, gkt, false);
+            }
+    }
+    *chain = c;
+}
+
+// kick / drift coefficients of the step (moldyn_*.F90 at istep_short == 1)
+// kind: 0 NVE, 1 NHC, 2 MTK
+struct CoefArgs { pgk_mdparams md; int degfree; int kind; };
+
+__global__ void k_coeffs(DynState* __restrict__ dyn, const ChainDev* __restrict__ chain, CoefArgs a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const pgk_mdparams& md = a.md;
+    const double dtl = md.dt_long_cal, dts = md.dt_long_cal / (double)md.nstep_short;
+    const double e2 = 1.0 / 6.0, e4 = e2 / 20.0, e6 = e4 / 42.0, e8 = e6 / 72.0;
+    const ChainDev& c = *chain;
+    dyn->ks_b = 0.5 * dts;
+    for (int d = 0; d < 3; ++d) { dyn->dr_a[d] = 1.0; dyn->dr_b[d] = dts; dyn->rvinv[d] = 1.0; }
+    if (a.kind == 0) {
+        for (int d = 0; d < 3; ++d) { dyn->kl_s[d] = 1.0; dyn->kl_b[d] = 0.5 * dtl; }
+        return;
+    }
+    bool aniso = a.kind == 2 && md.pcont_axis != PGK_PCONT_ISO;
+    if (!aniso) {
+        double vext = c.vlogs[0];
+        if (a.kind == 2) vext = c.vlogs[0] + (1.0 + 3.0 / (double)a.degfree) * c.vlogv;
+        double ec4 = exp(-0.25 * dtl * vext);
+        double a2 = (0.25 * dtl * vext) * (0.25 * dtl * vext);
+        double poly = 1.0 + a2 * (e2 + a2 * (e4 + a2 * (e6 + a2 * e8)));
+        double cf = ec4 * poly;
+        for (int d = 0; d < 3; ++d) { dyn->kl_s[d] = ec4 * ec4; dyn->kl_b[d] = cf * 0.5 * dtl; }
+    } else {
+        int dir = md.pcont_axis == PGK_PCONT_ANISO ? 0 : md.pcont_axis - 1;
+        double vx[3] = {c.vlogs[0], c.vlogs[0], c.vlogs[0]};
+        if (dir == 0) {
+            double tr = c.vboxg[0] + c.vboxg[1] + c.vboxg[2];
+            for (int d = 0; d < 3; ++d) vx[d] = c.vlogs[0] + c.vboxg[d] + 1.0 / (double)a.degfree * tr;
+        } else {
+            vx[dir - 1] = vx[dir - 1] + c.vboxg[dir - 1] + 1.0 / (double)a.degfree * c.vboxg[dir - 1];
+        }
+        for (int d = 0; d < 3; ++d) {
+            double ec4 = exp(-0.25 * dtl * vx[d]);
+            double a2 = (0.25 * dtl * vx[d]) * (0.25 * dtl * vx[d]);
+            double poly = 1.0 + a2 * (e2 + a2 * (e4 + a2 * (e6 + a2 * e8)));
+            dyn->kl_s[d] = ec4 * ec4;
+            dyn->kl_b[d] = ec4 * poly * 0.5 * dtl;
+        }
+    }
+    if (a.kind == 2) {
+        if (!aniso) {
+            double aa = exp(0.5 * dts * c.vlogv), aa2 = aa * aa;
+            double a2 = (0.5 * dts * c.vlogv) * (0.5 * dts * c.vlogv);
+            double poly = 1.0 + a2 * (e2 + a2 * (e4 + a2 * (e6 + a2 * e8)));
+            for (int d = 0; d < 3; ++d) {
+                dyn->dr_a[d] = aa2;
+                dyn->dr_b[d] = aa * poly * dts;
+                dyn->rvinv[d] = 1.0 / (aa * poly);
+            }
+        } else {
+            for (int d = 0; d < 3; ++d) {
+                double aa = exp(0.5 * dts * c.vboxg[d]);
+                double a2 = (0.5 * dts * c.vboxg[d]) * (0.5 * dts * c.vboxg[d]);
+                double poly = 1.0 + a2 * (e2 + a2 * (e4 + a2 * (e6 + a2 * e8)));
+                dyn->dr_a[d] = aa * aa;
+                dyn->dr_b[d] = aa * poly * dts;
+                dyn->rvinv[d] = 1.0 / (aa * poly);
+            }
+        }
+    }
+}
+
+// erf_corr_cutoff.F90:28-62 (the reference's min-ish rule kept)
+__device__ double rkcut_of(const double* box, int n1, int n2, int n3) {
+    double m1 = 0.5 * (n1 / box[0]);
+    double rk = m1;
+    double m2 = 0.5 * (n2 / box[1]);
+    if (m2 < m1) rk = m2;
+    double m3 = 0.5 * (n3 / box[2]);
+    if (m3 < m2) rk = m3;
+    return 0.9 * rk;
+}
+
+// volume / box update of one short step (calvol.F90, calbox.F90)
+struct BoxArgs { double dts, rcut, rcut_book; int aniso, nfft1, nfft2, nfft3, update_rk; };
+
+__global__ void k_box(DynState* __restrict__ dyn, ChainDev* __restrict__ chain, BoxArgs a, unsigned* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    ChainDev& c = *chain;
+    double b[3];
+    if (!a.aniso) {
+        c.xlogv = c.xlogv + c.vlogv * a.dts;
+        double vol = exp(3.0 * c.xlogv);
+        b[0] = pow(vol / dyn->yratio / dyn->zratio, 1.0 / 3.0);
+        b[1] = dyn->yratio * b[0];
+        b[2] = dyn->zratio * b[0];
+    } else {
+        for (int d = 0; d < 3; ++d) c.xboxh[d] = c.xboxh[d] * exp(c.vboxg[d] * a.dts);
+        for (int d = 0; d < 3; ++d) b[d] = c.xboxh[d];
+        dyn->yratio = b[1] / b[0];
+        dyn->zratio = b[2] / b[0];
+    }
+    for (int d = 0; d < 3; ++d) { dyn->box[d] = b[d]; dyn->boxinv[d] = 1.0 / b[d]; }
+    double h = fmin(b[0] * 0.5, fmin(b[1] * 0.5, b[2] * 0.5));
+    if (a.rcut > h || a.rcut_book > h) atomicOr(status, ST_BOX_TOO_SMALL);
+    if (a.update_rk) dyn->rkcut = rkcut_of(b, a.nfft1, a.nfft2, a.nfft3);
+}
+
+__global__ void k_rkcut(DynState* __restrict__ dyn, int n1, int n2, int n3) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) dyn->rkcut = rkcut_of(dyn->box, n1, n2, n3);
+}
+
+// calpress, atomic branch: pint / pintt of the current state from the kinetic
+// sums and both groups' virials (+ self and net-charge terms)
+struct PressArgs { double pot_ewc, netchrgsq, alpha; int ifspme, ifnetqcorrp; };
+
+__global__ void k_press(const long long* __restrict__ acc, const DynState* __restrict__ dyn, ChainDev* chain,
+                        PressArgs a) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const long long* A = acc;              // kinetic sums live in group 0
+    double K = fixv(A, A_KE);
+    double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    double pi = 3.14159265358979323846;
+    double a1 = -pi / (a.alpha * a.alpha * vol);
+    double ewnq = a.ifspme ? 0.5 * a1 * a.netchrgsq : 0.0;
+    double ewc = a.ifspme ? a.pot_ewc : 0.0;
+    double W = ewc + ewnq, Wt[9];
+    for (int k = 0; k < 9; ++k) Wt[k] = 0.0;
+    for (int g = 0; g < 2; ++g) {
+        const long long* G = acc + (size_t)g * NACC;
+        W += fixv(G, A_VC) + fixv(G, A_VLJ) + fixv(G, A_VB) + fixv(G, A_VA) + fixv(G, A_VT) + fixv(G, A_V14);
+        for (int k = 0; k < 9; ++k) {
+            // coulomb / LJ tensors are stored as their lower triangle
+            int r = k % 3, cl = k / 3;
+            int ks = r >= cl ? k : cl + 3 * r;
+            Wt[k] += fixv(G, A_VTC + ks) + fixv(G, A_VTLJ + ks) + fixv(G, A_VTB + k) + fixv(G, A_VTA + k) +
+                     fixv(G, A_VTT + k) + fixv(G, A_VT14 + k);
+        }
+    }
+    if (a.ifspme && !a.ifnetqcorrp) {      // calforce.F90:1018-1050 (long group)
+        W += a1 * a.netchrgsq;
+        for (int d = 0; d < 3; ++d) Wt[4 * d] += 0.5 * a1 * a.netchrgsq;
+    } else if (a.ifspme) {
+        W -= 0.5 * a1 * a.netchrgsq;
+    }
+    double b3 = (1.0 / dyn->box[0]) * (1.0 / dyn->box[1]) * (1.0 / dyn->box[2]);
+    chain->pint = 1.0 / 3.0 * b3 * (K + W);
+    for (int k = 0; k < 9; ++k) chain->pintt[k] = 1.0 * b3 * (fixv(A, A_KET + k) + Wt[k]);
+}
+
+template <bool MIXED>
+__global__ void k_copy_force(const void* __restrict__ f, double* __restrict__ out, int n3) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n3) out[k] = force_get<MIXED>(f, k);
+}
+
+// ---- launchers ----------------------------------------------------------------
+pgk_status launch_zero_group(pgk_ctx* c, int g) {
+    PGK_CUDA(c, cudaMemsetAsync(c->facc[g], 0, (size_t)24 * c->natom, c->st));
+    PGK_CUDA(c, cudaMemsetAsync(c->acc + (size_t)g * NACC, 0, sizeof(long long) * NACC, c->st));
+    return PGK_OK;
+}
+
+pgk_status launch_kick_long(pgk_ctx* c) {
+    int n3 = 3 * c->natom;
+    if (c->mixed()) k_kick_long<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[0], c->mass, c->natom, c->dyn);
+    else k_kick_long<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[0], c->mass, c->natom, c->dyn);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_kick_short(pgk_ctx* c) {
+    int n3 = 3 * c->natom;
+    if (c->mixed()) k_kick_short<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
+    else k_kick_short<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_drift(pgk_ctx* c, bool save_old) {
+    int n3 = 3 * c->natom;
+    k_drift<<<(n3 + 255) / 256, 256, 0, c->st>>>(c->pos, c->pos_old, c->vel, c->natom, c->dyn, save_old ? 1 : 0);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
+    if (c->ncgroup == 0) return PGK_OK;
+    k_rattle_pos<<<(c->ncgroup + 127) / 128, 128, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->mass, c->cg_idx,
+                                                               c->cg_list, c->c_ij, c->c_d, c->ncgroup, eps, dt,
+                                                               use_rv ? 1 : 0, c->dyn, c->status);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
+    if (c->ncgroup == 0) return PGK_OK;
+    k_rattle_vel<<<(c->ncgroup + 127) / 128, 128, 0, c->st>>>(c->pos, c->vel, c->mass, c->cg_idx, c->cg_list, c->c_ij,
+                                                               c->c_d, c->ncgroup, eps, c->status);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_kinetic(pgk_ctx* c, int group) {
+    long long* acc = c->acc + (size_t)group * NACC;
+    PGK_CUDA(c, cudaMemsetAsync(acc + A_KE, 0, sizeof(long long) * 10, c->st));
+    int blocks = std::min(c->nsm * 2, (c->natom + 255) / 256);
+    if (blocks < 1) blocks = 1;
+    k_kinetic<<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, acc);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md) {
+    ChainArgs a;
+    a.md = md;
+    a.degfree = c->degfree;
+    a.kind = kind;
+    k_chain<<<1, 32, 0, c->st>>>(c->chain, c->acc, a);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int) {
+    CoefArgs a;
+    a.md = md;
+    a.degfree = c->degfree;
+    a.kind = kind;
+    k_coeffs<<<1, 32, 0, c->st>>>(c->dyn, c->chain, a);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md) {
+    BoxArgs a;
+    a.dts = md.dt_long_cal / (double)md.nstep_short;
+    a.rcut = c->prm.rcut;
+    a.rcut_book = c->prm.rcut_book;
+    a.aniso = (kind == 2 && md.pcont_axis != PGK_PCONT_ISO) ? 1 : 0;
+    a.nfft1 = c->prm.nfft1; a.nfft2 = c->prm.nfft2; a.nfft3 = c->prm.nfft3;
+    a.update_rk = c->prm.mts_ewk == PGK_MTS_SHORT ? 1 : 0;
+    k_box<<<1, 32, 0, c->st>>>(c->dyn, c->chain, a, c->status);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_rkcut(pgk_ctx* c) {
+    k_rkcut<<<1, 32, 0, c->st>>>(c->dyn, c->prm.nfft1, c->prm.nfft2, c->prm.nfft3);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_press(pgk_ctx* c) {
+    PressArgs a;
+    a.pot_ewc = c->pot_ewc;
+    a.netchrgsq = c->netchrgsq;
+    a.alpha = c->prm.alpha;
+    a.ifspme = c->prm.ifspme;
+    a.ifnetqcorrp = c->prm.ifnetqcorrp;
+    k_press<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, a);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_copy_force(pgk_ctx* c, int group, double* dst) {
+    int n3 = 3 * c->natom;
+    if (c->mixed()) k_copy_force<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->facc[group], dst, n3);
+    else k_copy_force<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->facc[group], dst, n3);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}

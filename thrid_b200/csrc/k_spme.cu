@@ -1,0 +1,533 @@
+// k_spme.cu -- smooth particle-mesh Ewald reciprocal space (fft_pmep,
+// fft_pme.F90:144-937; fft_pme_init.F90:14-289; erf_corr_cutoff.F90).
+//
+//  k_spread   get_scaled_fractionals + get_bspline_coeffs + fill_charge_grid:
+//             one thread per atom, p^3 atomic adds into the accumulation grid
+//             (int64 fixed point 2^40 in mixed precision -> order-independent,
+//             deterministic; double in FP64 precision).
+//  k_fft      hand-written shared-memory pencil FFT (Stockham autosort,
+//             radix 4/2/3/5), one launch per axis and direction; the first
+//             forward pass reads the accumulation grid directly.  Replaces the
+//             FFTPACK cfftf/cfftb passes of pubz3d (fft_pme.F90:809-869).
+//  k_scalar   scalar_sum: influence function, energy, virial tensor, Q *= eterm.
+//  k_gather   grad_sum: force from the convolved grid, p^3 loads per atom.
+// Complex grid: float2 (mixed) or double2 (FP64), x fastest, K1*K2*K3.
+#include <cmath>
+#include <vector>
+
+#include "pgk_ctx.cuh"
+
+// ---- B-spline weights: fill_bspline (fft_pme_init.F90:216-260) ---------------
+template <typename T, int P>
+__device__ __forceinline__ void fill_bspline_d(T w, T* arr, T* darr) {
+    arr[P - 1] = 0;
+    arr[1] = w;
+    arr[0] = T(1) - w;
+#pragma unroll
+    for (int k = 3; k <= P - 1; ++k) {
+        T div = T(1) / T(k - 1);
+        arr[k - 1] = div * w * arr[k - 2];
+#pragma unroll
+        for (int j = 1; j <= k - 2; ++j)
+            arr[k - j - 1] = div * ((w + T(j)) * arr[k - j - 2] + (T(k - j) - w) * arr[k - j - 1]);
+        arr[0] = div * (T(1) - w) * arr[0];
+    }
+    darr[0] = -arr[0];
+#pragma unroll
+    for (int j = 2; j <= P; ++j) darr[j - 1] = arr[j - 2] - arr[j - 1];
+    T div = T(1) / T(P - 1);
+    arr[P - 1] = div * w * arr[P - 2];
+#pragma unroll
+    for (int j = 1; j <= P - 2; ++j)
+        arr[P - j - 1] = div * ((w + T(j)) * arr[P - j - 2] + (T(P - j) - w) * arr[P - j - 1]);
+    arr[0] = div * (T(1) - w) * arr[0];
+}
+
+// scaled fractional coordinate (get_scaled_fractionals) -> base index, w
+__device__ __forceinline__ void frac_coord(double x, double recip, int K, int& base, double& w) {
+    double f = x * recip;
+    f = f - floor(f);
+    double fr = (double)K * f;
+    base = (int)fr;
+    w = fr - trunc(fr);
+}
+
+template <bool MIXED, int P>
+__global__ void k_spread(const double* __restrict__ pos, const double* __restrict__ chrg, int n,
+                         const DynState* __restrict__ dyn, int K1, int K2, int K3, void* __restrict__ qacc) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    double th[3][P], dth[3][P];
+    int base[3];
+    const int Kd[3] = {K1, K2, K3};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w;
+        frac_coord(pos[3 * a + d], dyn->boxinv[d], Kd[d], base[d], w);
+        fill_bspline_d<double, P>(w, th[d], dth[d]);
+    }
+    double q = chrg[a];
+#pragma unroll
+    for (int i3 = 0; i3 < P; ++i3) {
+        int k = base[2] - P + 1 + i3;
+        k = k < 0 ? k + K3 : k;
+        double p1 = th[2][i3] * q;
+#pragma unroll
+        for (int i2 = 0; i2 < P; ++i2) {
+            int j = base[1] - P + 1 + i2;
+            j = j < 0 ? j + K2 : j;
+            double p2 = th[1][i2] * p1;
+            size_t row = (size_t)K1 * (j + (size_t)K2 * k);
+#pragma unroll
+            for (int i1 = 0; i1 < P; ++i1) {
+                int i = base[0] - P + 1 + i1;
+                i = i < 0 ? i + K1 : i;
+                double v = th[0][i1] * p2;
+                if (MIXED) atomicAdd((unsigned long long*)qacc + row + i,
+                                     (unsigned long long)__double2ll_rn(v * PGK_GRID_SCALE));
+                else atomicAdd((double*)qacc + row + i, v);
+            }
+        }
+    }
+}
+
+// ---- FFT --------------------------------------------------------------------
+template <typename T> struct C2;
+template <> struct C2<float> { typedef float2 t; };
+template <> struct C2<double> { typedef double2 t; };
+
+template <typename T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) { a.x += b.x; a.y += b.y; return a; }
+template <typename T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename T2, typename T> __device__ __forceinline__ T2 cscale(T2 a, T s) { a.x *= s; a.y *= s; return a; }
+template <typename T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+    T2 r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename T2, typename T> __device__ __forceinline__ T2 mul_i(T2 a, T s) {   // (s*i) * a
+    T2 r; r.x = -s * a.y; r.y = s * a.x; return r;
+}
+
+struct FftDev {
+    int n, nstage;
+    int radix[PGK_MAX_RADIX_STAGES];
+    const void* tw;
+};
+
+template <typename T, typename T2>
+__device__ __forceinline__ void dft_r(T2* v, int R, T sg) {
+    if (R == 2) {
+        T2 a = v[0], b = v[1];
+        v[0] = cadd(a, b); v[1] = csub(a, b);
+    } else if (R == 4) {
+        T2 a0 = v[0], a1 = v[1], a2 = v[2], a3 = v[3];
+        T2 s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3), d13 = csub(a1, a3);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        T2 t = mul_i<T2, T>(d13, sg);
+        v[1] = cadd(d02, t);
+        v[3] = csub(d02, t);
+    } else if (R == 3) {
+        const T s60 = T(0.86602540378443864676);
+        T2 a0 = v[0], a1 = v[1], a2 = v[2];
+        T2 t1 = cadd(a1, a2);
+        T2 t2 = csub(a0, cscale<T2, T>(t1, T(0.5)));
+        T2 t3 = mul_i<T2, T>(csub(a1, a2), sg * s60);
+        v[0] = cadd(a0, t1);
+        v[1] = cadd(t2, t3);
+        v[2] = csub(t2, t3);
+    } else if (R == 5) {
+        const T c72 = T(0.30901699437494742410), s72 = T(0.95105651629515357212);
+        const T c144 = T(-0.80901699437494742410), s144 = T(0.58778525229247312917);
+        T2 a0 = v[0];
+        T2 b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+        T2 c1 = csub(v[1], v[4]), c2 = csub(v[2], v[3]);
+        T2 t1 = cadd(a0, cadd(cscale<T2, T>(b1, c72), cscale<T2, T>(b2, c144)));
+        T2 t2 = cadd(a0, cadd(cscale<T2, T>(b1, c144), cscale<T2, T>(b2, c72)));
+        T2 u1 = cadd(cscale<T2, T>(c1, s72), cscale<T2, T>(c2, s144));
+        T2 u2 = csub(cscale<T2, T>(c1, s144), cscale<T2, T>(c2, s72));
+        T2 iu1 = mul_i<T2, T>(u1, sg), iu2 = mul_i<T2, T>(u2, sg);
+        v[0] = cadd(a0, cadd(b1, b2));
+        v[1] = cadd(t1, iu1);
+        v[4] = csub(t1, iu1);
+        v[2] = cadd(t2, iu2);
+        v[3] = csub(t2, iu2);
+    }
+}
+
+// AXIS 0: pencils along x (contiguous); 1: along y; 2: along z.
+// SRC: 0 = complex grid in place, 1 = int64 fixed-point accumulation grid,
+//      2 = double accumulation grid (both real, first forward pass).
+template <typename T, int AXIS, int SRC>
+__global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ data, const void* __restrict__ acc,
+                                             int K1, int K2, int K3, FftDev plan, int P, T sg) {
+    typedef typename C2<T>::t T2;
+    extern __shared__ unsigned char smraw[];
+    T2* bufA = (T2*)smraw;
+    T2* bufB = bufA + P * plan.n;
+    const int n = plan.n;
+    size_t base;
+    size_t stride;
+    if (AXIS == 0) {
+        base = (size_t)blockIdx.x * P * K1;
+        stride = 1;
+    } else if (AXIS == 1) {
+        int nxb = (K1 + P - 1) / P;
+        int z = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * P;
+        base = (size_t)x0 + (size_t)K1 * K2 * z;
+        stride = K1;
+    } else {
+        int nxb = (K1 + P - 1) / P;
+        int y = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * P;
+        base = (size_t)x0 + (size_t)K1 * y;
+        stride = (size_t)K1 * K2;
+    }
+    const int tot = P * n;
+    const int npen_total = AXIS == 0 ? K2 * K3 : K1;
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        int p, m;
+        if (AXIS == 0) { p = idx / n; m = idx % n; } else { m = idx / P; p = idx % P; }
+        int pg = AXIS == 0 ? blockIdx.x * P + p : (int)(base % K1) + p;
+        T2 v;
+        v.x = 0; v.y = 0;
+        bool ok = AXIS == 0 ? pg < npen_total : pg < K1;
+        if (ok) {
+            size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
+            if (SRC == 0) v = data[off];
+            else if (SRC == 1) v.x = (T)((double)((const long long*)acc)[off] * PGK_GRID_ISCALE);
+            else v.x = (T)((const double*)acc)[off];
+        }
+        bufA[p * n + m] = v;
+    }
+    __syncthreads();
+    const T2* tw = (const T2*)plan.tw;
+    T2* src = bufA;
+    T2* dst = bufB;
+    int Ns = 1;
+    for (int s = 0; s < plan.nstage; ++s) {
+        const int R = plan.radix[s];
+        const int nr = n / R;
+        const int twstep = n / (Ns * R);
+        for (int w = threadIdx.x; w < P * nr; w += blockDim.x) {
+            int p = w / nr, j = w % nr;
+            int k = j % Ns;
+            T2 v[5];
+            const T2* sp = src + p * n;
+#pragma unroll
+            for (int r = 0; r < 5; ++r)
+                if (r < R) {
+                    T2 x = sp[j + r * nr];
+                    if (r > 0 && k > 0) {
+                        T2 t = tw[r * k * twstep];
+                        if (sg > 0) t.y = -t.y;
+                        x = cmul(x, t);
+                    }
+                    v[r] = x;
+                }
+            dft_r<T, T2>(v, R, sg);
+            int o = (j / Ns) * Ns * R + k;
+            T2* dp = dst + p * n;
+#pragma unroll
+            for (int r = 0; r < 5; ++r)
+                if (r < R) dp[o + r * Ns] = v[r];
+        }
+        __syncthreads();
+        T2* t = src; src = dst; dst = t;
+        Ns *= R;
+    }
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        int p, m;
+        if (AXIS == 0) { p = idx / n; m = idx % n; } else { m = idx / P; p = idx % P; }
+        int pg = AXIS == 0 ? blockIdx.x * P + p : (int)(base % K1) + p;
+        bool ok = AXIS == 0 ? pg < npen_total : pg < K1;
+        if (ok) {
+            size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
+            data[off] = src[p * n + m];
+        }
+    }
+}
+
+// ---- scalar_sum (fft_pme.F90:544-690) ----------------------------------------
+template <typename T>
+__global__ void k_scalar(typename C2<T>::t* __restrict__ q, int K1, int K2, int K3, const double* __restrict__ bsp,
+                         const DynState* __restrict__ dyn, double alpha, double netchrgsq, int corr,
+                         long long* __restrict__ acc, int want) {
+    typedef typename C2<T>::t T2;
+    size_t KK = (size_t)K1 * K2 * K3;
+    const double pi = 3.14159265358979323846;
+    const double fac = pi * pi / (alpha * alpha);
+    const double r0 = dyn->boxinv[0], r1 = dyn->boxinv[1], r2 = dyn->boxinv[2];
+    const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    const double rk2 = dyn->rkcut * dyn->rkcut;
+    int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
+    int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
+    int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
+    double en = 0, vs = 0, vt[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x; ind < KK;
+         ind += (size_t)gridDim.x * blockDim.x) {
+        if (ind == 0) continue;     // m = 0 is skipped by scalar_sum's loop bounds
+        int k3 = (int)(ind / ((size_t)K1 * K2));
+        size_t jnd = ind - (size_t)k3 * K1 * K2;
+        int k2 = (int)(jnd / K1), k1 = (int)(jnd - (size_t)k2 * K1);
+        int m1 = k1 < nf1 ? k1 : k1 - K1;
+        int m2 = k2 < nf2 ? k2 : k2 - K2;
+        int m3 = k3 < nf3 ? k3 : k3 - K3;
+        double h1 = r0 * m1, h2 = r1 * m2, h3 = r2 * m3;
+        double msq = h1 * h1 + h2 * h2 + h3 * h3;
+        T2 v = q[ind];
+        double eterm = 0.0;
+        if (msq <= rk2) {
+            double denom = pi * vol * bsp[k1] * bsp[K1 + k2] * bsp[K1 + K2 + k3] * msq;
+            double ex = exp(-fac * msq);
+            eterm = ex / denom;
+            if (want) {
+                double vterm = 2.0 * (fac * msq + 1.0) / msq;
+                double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+                double es = eterm * s2;
+                en += es;
+                if (corr) {
+                    double e2 = ex * netchrgsq / (pi * vol * msq);
+                    vs += e2 * (-1.0 + 2.0 * fac * msq);
+                    es -= e2;
+                }
+                vt[0] += es * (vterm * h1 * h1 - 1.0);
+                vt[1] += es * (vterm * h1 * h2);
+                vt[2] += es * (vterm * h1 * h3);
+                vt[3] += es * (vterm * h2 * h2 - 1.0);
+                vt[4] += es * (vterm * h2 * h3);
+                vt[5] += es * (vterm * h3 * h3 - 1.0);
+            }
+        }
+        v.x = (T)((double)v.x * eterm);
+        v.y = (T)((double)v.y * eterm);
+        q[ind] = v;
+    }
+    if (want) {
+        // pot_ewk = en/2; pot_viri_coul += pot_ewk + vir_sca; virit -= vt/2
+        double out[9] = {0.5 * en, 0.5 * en + 0.5 * vs, 0.5 * vs,
+                         -0.5 * vt[0], -0.5 * vt[1], -0.5 * vt[2], -0.5 * vt[3], -0.5 * vt[4], -0.5 * vt[5]};
+        const int idx[9] = {A_EWK, A_VC, A_VSCA, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
+        block_acc<9>(out, acc, idx);
+    }
+}
+
+// ---- grad_sum (fft_pme.F90:872-937) ------------------------------------------
+template <bool MIXED, int P>
+__global__ void k_gather(const double* __restrict__ pos, const double* __restrict__ chrg, int n,
+                         const DynState* __restrict__ dyn, int K1, int K2, int K3, const void* __restrict__ qc,
+                         void* facc) {
+    typedef typename std::conditional<MIXED, float, double>::type T;
+    typedef typename C2<T>::t T2;
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    T th[3][P], dth[3][P];
+    int base[3];
+    const int Kd[3] = {K1, K2, K3};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w;
+        frac_coord(pos[3 * a + d], dyn->boxinv[d], Kd[d], base[d], w);
+        fill_bspline_d<T, P>((T)w, th[d], dth[d]);
+    }
+    const T2* Q = (const T2*)qc;
+    T f0 = 0, f1 = 0, f2 = 0;
+    const T q = (T)chrg[a];
+#pragma unroll
+    for (int i3 = 0; i3 < P; ++i3) {
+        int k = base[2] - P + 1 + i3;
+        k = k < 0 ? k + K3 : k;
+#pragma unroll
+        for (int i2 = 0; i2 < P; ++i2) {
+            int j = base[1] - P + 1 + i2;
+            j = j < 0 ? j + K2 : j;
+            size_t row = (size_t)K1 * (j + (size_t)K2 * k);
+#pragma unroll
+            for (int i1 = 0; i1 < P; ++i1) {
+                int i = base[0] - P + 1 + i1;
+                i = i < 0 ? i + K1 : i;
+                T term = q * Q[row + i].x;
+                f0 = f0 - (T)K1 * term * dth[0][i1] * th[1][i2] * th[2][i3];
+                f1 = f1 - (T)K2 * term * th[0][i1] * dth[1][i2] * th[2][i3];
+                f2 = f2 - (T)K3 * term * th[0][i1] * th[1][i2] * dth[2][i3];
+            }
+        }
+    }
+    force_add<MIXED>(facc, a, dyn->boxinv[0] * (double)f0, dyn->boxinv[1] * (double)f1,
+                     dyn->boxinv[2] * (double)f2);
+}
+
+// ---- host side ------------------------------------------------------------------
+static void fill_bspline_h(double w, int order, double* arr, double* darr) {
+    arr[order - 1] = 0.0; arr[1] = w; arr[0] = 1.0 - w;
+    for (int k = 3; k <= order - 1; ++k) {
+        double div = 1.0 / (double)(k - 1);
+        arr[k - 1] = div * w * arr[k - 2];
+        for (int j = 1; j <= k - 2; ++j) arr[k - j - 1] = div * ((w + j) * arr[k - j - 2] + (k - j - w) * arr[k - j - 1]);
+        arr[0] = div * (1 - w) * arr[0];
+    }
+    darr[0] = -arr[0];
+    for (int j = 2; j <= order; ++j) darr[j - 1] = arr[j - 2] - arr[j - 1];
+    double div = 1.0 / (double)(order - 1);
+    arr[order - 1] = div * w * arr[order - 2];
+    for (int j = 1; j <= order - 2; ++j)
+        arr[order - j - 1] = div * ((w + j) * arr[order - j - 2] + (order - j - w) * arr[order - j - 1]);
+    arr[0] = div * (1 - w) * arr[0];
+}
+
+static bool factor(int n, FftPlan& pl) {
+    pl.n = n; pl.nstage = 0;
+    int m = n;
+    while (m > 1) {
+        int r = 0;
+        for (int c : {4, 2, 3, 5}) if (m % c == 0) { r = c; break; }
+        if (r == 0 || pl.nstage >= PGK_MAX_RADIX_STAGES) return false;
+        pl.radix[pl.nstage++] = r;
+        m /= r;
+    }
+    return true;
+}
+
+pgk_status spme_setup(pgk_ctx* c) {
+    c->K[0] = c->prm.nfft1; c->K[1] = c->prm.nfft2; c->K[2] = c->prm.nfft3;
+    c->order = c->prm.pme_order;
+    if (c->order < 3 || c->order > 8) return pgk_fail(c, PGK_E_UNSUPPORTED, "pme_order must be 3..8");
+    size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
+    PGK_CUDA(c, cudaMalloc(&c->qacc, KK * 8));
+    PGK_CUDA(c, cudaMalloc(&c->qc, KK * (c->mixed() ? sizeof(float2) : sizeof(double2))));
+    // B-spline moduli (DFTMOD, fft_pme_init.F90:263-289)
+    double arr[16], darr[16];
+    fill_bspline_h(0.0, c->order, arr, darr);
+    std::vector<double> bsp;
+    for (int d = 0; d < 3; ++d) {
+        int n = c->K[d];
+        std::vector<double> a((size_t)n, 0.0), mod((size_t)n, 0.0);
+        for (int i = 2; i <= c->order + 1 && i - 1 < n; ++i) a[i - 1] = arr[i - 2];
+        const double twopi = 2.0 * 3.14159265358979323846;
+        for (int k = 0; k < n; ++k) {
+            double s1 = 0, s2 = 0;
+            for (int j = 0; j < n; ++j) {
+                double arg = twopi * (double)k * (double)j / (double)n;
+                s1 += a[j] * std::cos(arg);
+                s2 += a[j] * std::sin(arg);
+            }
+            mod[k] = s1 * s1 + s2 * s2;
+        }
+        for (int k = 1; k < n - 1; ++k) if (mod[k] < 1.0e-7) mod[k] = 0.5 * (mod[k - 1] + mod[k + 1]);
+        bsp.insert(bsp.end(), mod.begin(), mod.end());
+    }
+    PGK_CUDA(c, cudaMalloc(&c->bsp, bsp.size() * sizeof(double)));
+    PGK_CUDA(c, cudaMemcpy(c->bsp, bsp.data(), bsp.size() * sizeof(double), cudaMemcpyHostToDevice));
+    for (int d = 0; d < 3; ++d) {
+        if (!factor(c->K[d], c->plan[d]))
+            return pgk_fail(c, PGK_E_UNSUPPORTED, "SPME grid sizes must factor into 2, 3, 5");
+        int n = c->K[d];
+        if (c->mixed()) {
+            std::vector<float2> tw(n);
+            for (int m = 0; m < n; ++m) {
+                double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
+                tw[m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+            }
+            PGK_CUDA(c, cudaMalloc(&c->plan[d].tw, n * sizeof(float2)));
+            PGK_CUDA(c, cudaMemcpy(c->plan[d].tw, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
+        } else {
+            std::vector<double2> tw(n);
+            for (int m = 0; m < n; ++m) {
+                double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
+                tw[m] = make_double2(std::cos(ang), std::sin(ang));
+            }
+            PGK_CUDA(c, cudaMalloc(&c->plan[d].tw, n * sizeof(double2)));
+            PGK_CUDA(c, cudaMemcpy(c->plan[d].tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+        }
+    }
+    return PGK_OK;
+}
+
+template <typename T, int AXIS, int SRC>
+static pgk_status fft_pass(pgk_ctx* c, int sign) {
+    typedef typename C2<T>::t T2;
+    const FftPlan& pl = c->plan[AXIS];
+    FftDev fd;
+    fd.n = pl.n; fd.nstage = pl.nstage;
+    for (int s = 0; s < PGK_MAX_RADIX_STAGES; ++s) fd.radix[s] = pl.radix[s];
+    fd.tw = pl.tw;
+    int K1 = c->K[0], K2 = c->K[1], K3 = c->K[2];
+    int P = sizeof(T) == 4 ? 16 : 8;
+    if (AXIS == 0) P = std::max(1, (sizeof(T) == 4 ? 2048 : 1024) / K1);
+    int grid;
+    if (AXIS == 0) grid = (K2 * K3 + P - 1) / P;
+    else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3;
+    else grid = ((K1 + P - 1) / P) * K2;
+    size_t sm = (size_t)2 * P * pl.n * sizeof(T2);
+    cudaFuncSetAttribute(k_fft<T, AXIS, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_fft<T, AXIS, SRC><<<grid, 256, sm, c->st>>>((T2*)c->qc, c->qacc, K1, K2, K3, fd, P, (T)sign);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+template <typename T>
+static pgk_status fft3(pgk_ctx* c, int sign, bool first) {
+    pgk_status s;
+    if (first) {
+        if (sizeof(T) == 4) s = fft_pass<T, 0, 1>(c, sign);
+        else s = fft_pass<T, 0, 2>(c, sign);
+    } else {
+        s = fft_pass<T, 0, 0>(c, sign);
+    }
+    if (s) return s;
+    if ((s = fft_pass<T, 1, 0>(c, sign))) return s;
+    return fft_pass<T, 2, 0>(c, sign);
+}
+
+template <bool MIXED, int P>
+static void spread_gather(pgk_ctx* c, bool gather, int group) {
+    int n = c->natom;
+    if (!gather)
+        k_spread<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
+                                                               c->K[2], c->qacc);
+    else
+        k_gather<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
+                                                               c->K[2], c->qc, c->facc[group]);
+    PGK_LAUNCHED(c);
+}
+
+template <bool MIXED>
+static pgk_status dispatch_sg(pgk_ctx* c, bool gather, int group) {
+    switch (c->order) {
+        case 3: spread_gather<MIXED, 3>(c, gather, group); break;
+        case 4: spread_gather<MIXED, 4>(c, gather, group); break;
+        case 5: spread_gather<MIXED, 5>(c, gather, group); break;
+        case 6: spread_gather<MIXED, 6>(c, gather, group); break;
+        case 7: spread_gather<MIXED, 7>(c, gather, group); break;
+        case 8: spread_gather<MIXED, 8>(c, gather, group); break;
+        default: return pgk_fail(c, PGK_E_UNSUPPORTED, "pme_order");
+    }
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir) {
+    size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
+    PGK_CUDA(c, cudaMemsetAsync(c->qacc, 0, KK * 8, c->st));
+    pgk_status s;
+    long long* acc = c->acc + (size_t)group * NACC;
+    int want = (ene || vir) ? 1 : 0;
+    int blocks = c->nsm * 4;
+    if (c->mixed()) {
+        if ((s = dispatch_sg<true>(c, false, group))) return s;
+        if ((s = fft3<float>(c, -1, true))) return s;
+        k_scalar<float><<<blocks, 256, 0, c->st>>>((float2*)c->qc, c->K[0], c->K[1], c->K[2], c->bsp, c->dyn,
+                                                   c->prm.alpha, c->netchrgsq, c->prm.ifnetqcorrp, acc, want);
+        PGK_LAUNCHED(c);
+        if ((s = fft3<float>(c, +1, false))) return s;
+        if ((s = dispatch_sg<true>(c, true, group))) return s;
+    } else {
+        if ((s = dispatch_sg<false>(c, false, group))) return s;
+        if ((s = fft3<double>(c, -1, true))) return s;
+        k_scalar<double><<<blocks, 256, 0, c->st>>>((double2*)c->qc, c->K[0], c->K[1], c->K[2], c->bsp, c->dyn,
+                                                    c->prm.alpha, c->netchrgsq, c->prm.ifnetqcorrp, acc, want);
+        PGK_LAUNCHED(c);
+        if ((s = fft3<double>(c, +1, false))) return s;
+        if ((s = dispatch_sg<false>(c, true, group))) return s;
+    }
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}

@@ -1,0 +1,664 @@
+// pgk_api.cu -- C ABI of libpgkgpu.so (include/pgk_gpu.h): context set-up,
+// state transfer, the fine-grained reference-named operations and the stage
+// drivers that keep the whole XO-RESPA loop on the device.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pgk_ctx.cuh"
+
+pgk_status launch_rkcut(pgk_ctx* c);
+
+pgk_status pgk_fail(pgk_ctx* c, pgk_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+namespace {
+
+// natural cubic spline of spline_interp.F90:139-190 (cal_spl_coeff)
+void spl_coeff(int n, double h, const std::vector<double>& x, const std::vector<double>& t, std::vector<double>& b,
+               std::vector<double>& cc, std::vector<double>& d) {
+    std::vector<double> al(n, 0.0), l(n, 0.0), mu(n, 0.0), z(n, 0.0);
+    b.assign(n, 0.0); cc.assign(n, 0.0); d.assign(n, 0.0);
+    for (int i = 1; i < n - 1; ++i) al[i] = 3.0 / h * ((t[i + 1] - t[i]) - (t[i] - t[i - 1]));
+    l[0] = 1.0;
+    for (int i = 1; i < n - 1; ++i) {
+        l[i] = 2.0 * (x[i + 1] - x[i - 1]) - h * mu[i - 1];
+        mu[i] = h / l[i];
+        z[i] = (al[i] - h * z[i - 1]) / l[i];
+    }
+    for (int i = n - 2; i >= 0; --i) {
+        cc[i] = z[i] - mu[i] * cc[i + 1];
+        b[i] = (t[i + 1] - t[i]) / h - h * (cc[i + 1] + 2.0 * cc[i]) / 3.0;
+        d[i] = (cc[i + 1] - cc[i]) / (3.0 * h);
+    }
+}
+
+double rkcut_host(const double* box, int n1, int n2, int n3) {   // erf_corr_cutoff.F90
+    double m1 = 0.5 * (n1 / box[0]);
+    double rk = m1;
+    double m2 = 0.5 * (n2 / box[1]);
+    if (m2 < m1) rk = m2;
+    double m3 = 0.5 * (n3 / box[2]);
+    if (m3 < m2) rk = m3;
+    return 0.9 * rk;
+}
+
+template <typename T>
+pgk_status upload(pgk_ctx* c, T** dst, const std::vector<T>& v) {
+    if (v.empty()) { *dst = nullptr; return PGK_OK; }
+    PGK_CUDA(c, cudaMalloc(dst, v.size() * sizeof(T)));
+    PGK_CUDA(c, cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PGK_OK;
+}
+
+pgk_status read_status(pgk_ctx* c) {
+    unsigned st = 0;
+    PGK_CUDA(c, cudaMemcpyAsync(&st, c->status, sizeof(st), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    if (!st) return PGK_OK;
+    unsigned z = 0;
+    PGK_CUDA(c, cudaMemcpy(c->status, &z, sizeof(z), cudaMemcpyHostToDevice));
+    if (st & ST_RATTLE_NOCONV) return pgk_fail(c, PGK_E_RATTLE_NOCONV, "ERROR: RATTLE(C) failed to converge within MAXITER = 300");
+    if (st & ST_RATTLEV_NOCONV) return pgk_fail(c, PGK_E_RATTLEV_NOCONV, "ERROR: RATTLE(V) failed to converge within MAXITER = 300");
+    if (st & ST_BOX_TOO_SMALL) return pgk_fail(c, PGK_E_BOX_TOO_SMALL, "Error: rcut is over half cell length");
+    if (st & ST_LIST_OVERFLOW) return pgk_fail(c, PGK_E_LIST_OVERFLOW, "Error: nlistnball exceed number of nonbonded list");
+    if (st & ST_CELL_OVERFLOW) return pgk_fail(c, PGK_E_CELL_OVERFLOW, "Error: number of atoms in cell exceeds max");
+    if (st & ST_UNSUPPORTED) return pgk_fail(c, PGK_E_UNSUPPORTED, "Periodicity not supported");
+    return pgk_fail(c, PGK_E_CUDA, "unknown device status");
+}
+
+// one MTS group of calforce (calforce.F90:8-1073)
+pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir) {
+    int g = flag == PGK_MTS_LONG ? 0 : 1;
+    pgk_status s;
+    if ((s = launch_zero_group(c, g))) return s;
+    if (c->prm.mts_vdw == flag) {
+        if (!c->list_valid && (s = launch_mklist(c))) return s;
+        if ((s = launch_pack(c))) return s;
+        if ((s = launch_pair(c, g, ene, vir))) return s;
+        if ((s = launch_excl(c, g, ene, vir))) return s;
+    }
+    if (c->prm.ifspme && c->prm.mts_ewk == flag)
+        if ((s = launch_spme(c, g, ene, vir))) return s;
+    return launch_bonded(c, g, ene, vir, false);
+}
+
+double fixv(long long v) { return (double)v * PGK_FORCE_ISCALE; }
+
+// energies / virials of the accumulators of the given groups
+pgk_status read_acc(pgk_ctx* c, int gmask, pgk_energies* e, pgk_virials* v, bool add_ewald_consts) {
+    std::vector<long long> a(2 * NACC);
+    PGK_CUDA(c, cudaMemcpyAsync(a.data(), c->acc, sizeof(long long) * 2 * NACC, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    double S[NACC];
+    for (int k = 0; k < NACC; ++k) {
+        S[k] = 0;
+        for (int g = 0; g < 2; ++g) if (gmask & (1 << g)) S[k] += fixv(a[(size_t)g * NACC + k]);
+    }
+    for (int base : {A_VTC, A_VTLJ}) { S[base + 3] = S[base + 1]; S[base + 6] = S[base + 2]; S[base + 7] = S[base + 5]; }
+    double pi = std::acos(-1.0);
+    const double* b = c->hdyn.box;
+    double a1 = -pi / (c->prm.alpha * c->prm.alpha * b[0] * b[1] * b[2]);
+    if (add_ewald_consts && c->prm.ifspme) {
+        if (!c->prm.ifnetqcorrp) {
+            S[A_VC] += a1 * c->netchrgsq;
+            for (int d = 0; d < 3; ++d) S[A_VTC + 4 * d] += 0.5 * a1 * c->netchrgsq;
+        } else {
+            S[A_VC] -= 0.5 * a1 * c->netchrgsq;
+        }
+    }
+    if (e) {
+        memset(e, 0, sizeof(*e));
+        e->pot_vdw = S[A_VDW]; e->pot_elc = S[A_ELC]; e->pot_ewk = S[A_EWK];
+        e->pot_vdw14 = S[A_VDW14]; e->pot_elc14 = S[A_ELC14];
+        e->pot_bond = S[A_BOND]; e->pot_angl = S[A_ANGL]; e->pot_tors = S[A_TORS]; e->pot_torsrb = S[A_TORSRB];
+        if (add_ewald_consts && c->prm.ifspme) { e->pot_ewc = c->pot_ewc; e->pot_ewnq = 0.5 * a1 * c->netchrgsq; }
+        e->pot_nonbon = e->pot_vdw + e->pot_elc + e->pot_ewk + e->pot_ewc + e->pot_ewnq + e->pot_vdw14 + e->pot_elc14;
+        e->pot_tot = e->pot_bond + e->pot_angl + e->pot_tors + e->pot_torsrb + e->pot_nonbon;
+    }
+    if (v) {
+        memset(v, 0, sizeof(*v));
+        v->pot_viri_coul = S[A_VC]; v->pot_viri_lj = S[A_VLJ];
+        v->atm_viri_bond = S[A_VB]; v->atm_viri_angl = S[A_VA]; v->atm_viri_tors = S[A_VT]; v->atm_viri_14 = S[A_V14];
+        for (int k = 0; k < 9; ++k) {
+            v->pot_virit_coul[k] = S[A_VTC + k]; v->pot_virit_lj[k] = S[A_VTLJ + k];
+            v->atm_virit_bond[k] = S[A_VTB + k]; v->atm_virit_angl[k] = S[A_VTA + k];
+            v->atm_virit_tors[k] = S[A_VTT + k]; v->atm_virit_14[k] = S[A_VT14 + k];
+        }
+    }
+    return PGK_OK;
+}
+
+pgk_status force_to_host(pgk_ctx* c, int g, double* force, bool add) {
+    int n3 = 3 * c->natom;
+    if (!c->fout) PGK_CUDA(c, cudaMalloc(&c->fout, sizeof(double) * n3));
+    pgk_status s = launch_copy_force(c, g, c->fout);
+    if (s) return s;
+    c->hbuf.resize(n3);
+    PGK_CUDA(c, cudaMemcpyAsync(c->hbuf.data(), c->fout, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    for (int k = 0; k < n3; ++k) force[k] = add ? force[k] + c->hbuf[k] : c->hbuf[k];
+    return PGK_OK;
+}
+
+pgk_status set_dyn_box(pgk_ctx* c, const double* box) {
+    PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    for (int d = 0; d < 3; ++d) { c->hdyn.box[d] = box[d]; c->hdyn.boxinv[d] = 1.0 / box[d]; }
+    c->hdyn.rkcut = rkcut_host(box, c->prm.nfft1, c->prm.nfft2, c->prm.nfft3);
+    PGK_CUDA(c, cudaMemcpyAsync(c->dyn, &c->hdyn, sizeof(DynState), cudaMemcpyHostToDevice, c->st));
+    return PGK_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char* pgk_version(void) { return "pgk-b200 1.0 (sm_100a)"; }
+
+const char* pgk_status_string(pgk_status s) {
+    switch (s) {
+        case PGK_OK: return "ok";
+        case PGK_E_LIST_OVERFLOW: return "Error: nlistnball(local) exceed number of nonbonded list";
+        case PGK_E_CELL_OVERFLOW: return "Error: number of atoms in cell exceeds max (vdw and elc)";
+        case PGK_E_RATTLE_NOCONV: return "ERROR: RATTLE(C) failed to converge within MAXITER";
+        case PGK_E_BOX_TOO_SMALL: return "Error: rcut is over half cell length";
+        case PGK_E_DEVICE_TIMEOUT: return "device wait timed out";
+        case PGK_E_CUDA: return "CUDA error";
+        case PGK_E_INVALID: return "invalid argument";
+        case PGK_E_NOMEM: return "device memory exhausted";
+        case PGK_E_UNSUPPORTED: return "unsupported option";
+        case PGK_E_RATTLEV_NOCONV: return "ERROR: RATTLE(V) failed to converge within MAXITER";
+        default: return "unknown status";
+    }
+}
+
+const char* pgk_last_error(const pgk_ctx* c) { return c ? c->err.c_str() : ""; }
+
+}  // extern "C"
+
+extern "C" {
+
+pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
+    if (!s || !p || !out) return PGK_E_INVALID;
+    *out = nullptr;
+    int n = s->natom;
+    if (n < 2 || !s->atmmass || !s->atmchrg || !s->atmindex || !s->index_excl || !s->list_excl)
+        return PGK_E_INVALID;
+    if (p->precision != PGK_PREC_FP64 && p->precision != PGK_PREC_MIXED) return PGK_E_INVALID;
+    if (p->rcut_book <= 0 || p->rcut <= 0 || p->rrcut <= 0) return PGK_E_INVALID;
+    if (p->mts_vdw != p->mts_vdw) return PGK_E_INVALID;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return PGK_E_CUDA;
+    pgk_ctx* c = new pgk_ctx();
+    c->natom = n;
+    c->prec = p->precision;
+    c->prm = *p;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return PGK_E_CUDA; }
+    c->degfree = s->degfree_all;
+    pgk_status st;
+#define TRY(x) do { if ((st = (x)) != PGK_OK) { pgk_free(c); return st; } } while (0)
+    // ---- atoms ----
+    std::vector<double> mass(s->atmmass, s->atmmass + n), chrg(s->atmchrg, s->atmchrg + n);
+    std::vector<int> typ(n);
+    for (int i = 0; i < n; ++i) {
+        typ[i] = s->atmindex[i] - 1;
+        if (typ[i] < 0 || typ[i] >= s->ntyp) { pgk_free(c); return PGK_E_INVALID; }
+    }
+    TRY(upload(c, &c->mass, mass));
+    TRY(upload(c, &c->chrg, chrg));
+    TRY(upload(c, &c->typ, typ));
+    double q = 0, q2 = 0;
+    for (int i = 0; i < n; ++i) { q += chrg[i]; q2 += chrg[i] * chrg[i]; }
+    c->netchrgsq = q * q;
+    c->pot_ewc = -1.0 / std::sqrt(std::acos(-1.0)) * p->alpha * q2;   // fft_pme_init.F90:147-156
+    size_t n3 = (size_t)3 * n;
+    if (cudaMalloc(&c->pos, n3 * 8) || cudaMalloc(&c->vel, n3 * 8) || cudaMalloc(&c->pos_old, n3 * 8) ||
+        cudaMalloc(&c->facc[0], n3 * 8) || cudaMalloc(&c->facc[1], n3 * 8) ||
+        cudaMalloc(&c->acc, sizeof(long long) * 2 * NACC) || cudaMalloc(&c->dyn, sizeof(DynState)) ||
+        cudaMalloc(&c->chain, sizeof(ChainDev)) || cudaMalloc(&c->status, sizeof(unsigned))) {
+        pgk_free(c);
+        return PGK_E_NOMEM;
+    }
+    cudaMemset(c->vel, 0, n3 * 8);
+    cudaMemset(c->pos, 0, n3 * 8);
+    cudaMemset(c->status, 0, sizeof(unsigned));
+    cudaMemset(c->acc, 0, sizeof(long long) * 2 * NACC);
+    // ---- LJ tables ----
+    c->ntyp = s->ntyp;
+    std::vector<double2> lj64(s->ntyp * s->ntyp);
+    std::vector<float2> lj32(s->ntyp * s->ntyp);
+    for (int i = 0; i < s->ntyp; ++i)
+        for (int j = 0; j < s->ntyp; ++j) {
+            double R = s->vdw_radij[i + s->ntyp * j], E = s->vdw_welij[i + s->ntyp * j];
+            if (s->inter_inttyp && s->inter_inttyp[i + s->ntyp * j] != 1) E = 0.0;
+            lj64[i * s->ntyp + j] = make_double2(R * R, E);
+            lj32[i * s->ntyp + j] = make_float2((float)(R * R), (float)E);
+        }
+    TRY(upload(c, &c->lj64, lj64));
+    TRY(upload(c, &c->lj32, lj32));
+    // ---- spline tables (spline_interp.F90:14-136) ----
+    {
+        int ns = p->nspltbl > 0 ? p->nspltbl : 1100;
+        double h = (p->rrcut + 2.0) / (double)ns;
+        c->nspl = ns; c->hspl = h;
+        double rootpi = std::sqrt(std::acos(-1.0)), piE = 2.0 / rootpi * p->alpha;
+        std::vector<double> x(ns), t[4];
+        for (int i = 0; i < ns; ++i) x[i] = (double)i * h;
+        for (int k = 0; k < 4; ++k) { t[k].assign(ns, 0.0); t[k][0] = 1.0; }
+        for (int i = 1; i < ns; ++i) {
+            double r = x[i], inv = 1.0 / r, arg = p->alpha * r;
+            double ec = std::erfc(arg), ex = std::exp(-arg * arg);
+            t[0][i] = inv * (piE * ex * inv + ec * inv * inv);
+            t[1][i] = ec * inv;
+            t[2][i] = inv * (-piE * ex * inv + (1.0 - ec) * inv * inv);
+            t[3][i] = (1.0 - ec) * inv;
+        }
+        std::vector<double4> s64(4 * (size_t)ns);
+        std::vector<float4> s32(4 * (size_t)ns);
+        for (int k = 0; k < 4; ++k) {
+            std::vector<double> b, cc, d;
+            spl_coeff(ns, h, x, t[k], b, cc, d);
+            for (int i = 0; i < ns; ++i) {
+                s64[(size_t)k * ns + i] = make_double4(t[k][i], b[i], cc[i], d[i]);
+                s32[(size_t)k * ns + i] = make_float4((float)t[k][i], (float)b[i], (float)cc[i], (float)d[i]);
+            }
+        }
+        TRY(upload(c, &c->spl64, s64));
+        TRY(upload(c, &c->spl32, s32));
+    }
+    // ---- exclusions ----
+    {
+        std::vector<std::vector<int>> part(n);
+        std::vector<int2> pairs;
+        for (int i = 0; i < n; ++i) {
+            int b = s->index_excl[i] - 1, e = s->index_excl[i + 1] - 1;
+            for (int k = b; k < e; ++k) {
+                int v = s->list_excl[k];
+                if (v <= 0) continue;
+                int j = v - 1;
+                if (j <= i || j >= n) continue;
+                part[i].push_back(j);
+                part[j].push_back(i);
+                if (i < n - 1) pairs.push_back(make_int2(i, j));
+            }
+        }
+        std::vector<int> idx(n + 1, 0), lst;
+        for (int i = 0; i < n; ++i) {
+            std::sort(part[i].begin(), part[i].end());
+            part[i].erase(std::unique(part[i].begin(), part[i].end()), part[i].end());
+            idx[i] = (int)lst.size();
+            lst.insert(lst.end(), part[i].begin(), part[i].end());
+            c->max_excl = std::max(c->max_excl, (int)part[i].size());
+        }
+        idx[n] = (int)lst.size();
+        if (lst.empty()) lst.push_back(-1);
+        TRY(upload(c, &c->exs_idx, idx));
+        TRY(upload(c, &c->exs_list, lst));
+        c->nexpair = (int)pairs.size();
+        TRY(upload(c, &c->expair, pairs));
+    }
+    // ---- molecules ----
+    {
+        c->nmole = s->nmole;
+        if (s->nmole > 0 && s->molept_index && s->molept_list) {
+            std::vector<int> mi(s->nmole + 1), ml;
+            for (int m = 0; m <= s->nmole; ++m) mi[m] = s->molept_index[m] - 1;
+            for (int k = 0; k < mi[s->nmole]; ++k) ml.push_back(s->molept_list[k] - 1);
+            TRY(upload(c, &c->mol_idx, mi));
+            TRY(upload(c, &c->mol_list, ml));
+        } else {
+            c->nmole = 0;
+        }
+    }
+    // ---- bonded ----
+    {
+        std::vector<int2> bij; std::vector<double2> bp;
+        for (int k = 0; k < s->nbond; ++k) {
+            bij.push_back(make_int2(s->ibond[k] - 1, s->jbond[k] - 1));
+            bp.push_back(make_double2(s->para_cbond[k], s->para_eqbond[k]));
+        }
+        c->nbond = s->nbond;
+        TRY(upload(c, &c->bond_ij, bij)); TRY(upload(c, &c->bond_p, bp));
+        std::vector<int4> aijk; std::vector<double2> ap;
+        for (int k = 0; k < s->nangl; ++k) {
+            aijk.push_back(make_int4(s->iangl[k] - 1, s->jangl[k] - 1, s->kangl[k] - 1, 0));
+            ap.push_back(make_double2(s->para_cangl[k], s->para_eqangl[k]));
+        }
+        c->nangl = s->nangl;
+        TRY(upload(c, &c->angl_ijk, aijk)); TRY(upload(c, &c->angl_p, ap));
+        std::vector<int4> tij; std::vector<double4> tp;
+        std::vector<int2> p14; std::vector<double2> f14;
+        for (int k = 0; k < s->ntors; ++k) {
+            tij.push_back(make_int4(s->itors[k] - 1, s->jtors[k] - 1, s->ktors[k] - 1, s->ltors[k] - 1));
+            tp.push_back(make_double4(s->para_barhig[k] / (double)s->para_divfac[k], s->para_phsang[k],
+                                      std::fabs(s->para_period[k]), std::cos(s->para_phsang[k])));
+            // caltors divides inside the force term as barhig*period/divfac; same value
+        }
+        c->ntors = s->ntors;
+        TRY(upload(c, &c->tors_ijkl, tij)); TRY(upload(c, &c->tors_p, tp));
+        std::vector<int4> rij; std::vector<double> rc;
+        for (int k = 0; k < s->ntorsrb; ++k) {
+            rij.push_back(make_int4(s->itorsrb[k] - 1, s->jtorsrb[k] - 1, s->ktorsrb[k] - 1, s->ltorsrb[k] - 1));
+            for (int qq = 0; qq < 6; ++qq) rc.push_back(s->para_barhigrb[6 * k + qq]);
+        }
+        c->ntorsrb = s->ntorsrb;
+        TRY(upload(c, &c->rb_ijkl, rij)); TRY(upload(c, &c->rb_c, rc));
+        // 1-4 pairs in calnon14p order: periodic torsions, then RB torsions
+        if (s->ifcalnonb14)
+            for (int k = 0; k < s->ntors; ++k) {
+                if (!s->ifcalnonb14[k]) continue;
+                int i = s->itors[k] - 1, j = s->ltors[k] - 1;
+                if (i == j) continue;
+                p14.push_back(make_int2(i, j));
+                f14.push_back(make_double2(1.0 / s->para_divfac_elc[k] * s->ring14[k],
+                                           1.0 / s->para_divfac_vdw[k] * s->ring14[k]));
+            }
+        if (s->ifcalnonb14_rb)
+            for (int k = 0; k < s->ntorsrb; ++k) {
+                if (!s->ifcalnonb14_rb[k]) continue;
+                int i = s->itorsrb[k] - 1, j = s->ltorsrb[k] - 1;
+                if (i == j) continue;
+                p14.push_back(make_int2(i, j));
+                f14.push_back(make_double2(1.0 / s->para_divfac_elcrb[k] * s->ring14_rb[k],
+                                           1.0 / s->para_divfac_vdwrb[k] * s->ring14_rb[k]));
+            }
+        c->n14 = (int)p14.size();
+        TRY(upload(c, &c->p14_ij, p14)); TRY(upload(c, &c->p14_f, f14));
+    }
+    // ---- constraints ----
+    {
+        c->ncgroup = s->nconst;
+        c->nconstraint = s->nconstraint;
+        if (s->nconst > 0) {
+            std::vector<int> gi(s->nconst + 1), gl;
+            for (int g = 0; g <= s->nconst; ++g) gi[g] = s->index_mconst[g] - 1;
+            for (int k = 0; k < gi[s->nconst]; ++k) gl.push_back(s->list_mconst[k] - 1);
+            std::vector<int2> cij; std::vector<double> cd;
+            for (int k = 0; k < s->nconstraint; ++k) {
+                cij.push_back(make_int2(s->iconst[k] - 1, s->jconst[k] - 1));
+                cd.push_back(s->dconst[k]);
+            }
+            TRY(upload(c, &c->cg_idx, gi)); TRY(upload(c, &c->cg_list, gl));
+            TRY(upload(c, &c->c_ij, cij)); TRY(upload(c, &c->c_d, cd));
+        }
+    }
+    // ---- pair list buffers ----
+    {
+        double vol = p->xcel * p->ycel * p->zcel;
+        double rb = p->rcut_book;
+        double expect = (double)n / vol * 4.0 / 3.0 * std::acos(-1.0) * rb * rb * rb;
+        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(1.25 * expect + 96);
+        cap = std::min(cap, ((n + 31) / 32) * 32);
+        cap = ((cap + 31) / 32) * 32;
+        c->cap = std::max(cap, 32);
+        if (cudaMalloc(&c->nbr, (size_t)n * c->cap * sizeof(int)) || cudaMalloc(&c->ncnt, n * sizeof(int)) ||
+            cudaMalloc(&c->perm, n * sizeof(int)) || cudaMalloc(&c->iperm, n * sizeof(int)) ||
+            cudaMalloc(&c->cell_of, n * sizeof(int)) || cudaMalloc(&c->pos_s, n3 * 8) ||
+            cudaMalloc(&c->typ_s, n * sizeof(int)) || cudaMalloc(&c->counters, 4 * sizeof(unsigned long long))) {
+            pgk_free(c);
+            return PGK_E_NOMEM;
+        }
+        if (c->mixed()) { if (cudaMalloc(&c->xq, n * sizeof(int4))) { pgk_free(c); return PGK_E_NOMEM; } }
+        else { if (cudaMalloc(&c->xq64, n * sizeof(double4))) { pgk_free(c); return PGK_E_NOMEM; } }
+    }
+    // ---- SPME ----
+    if (p->ifspme) TRY(spme_setup(c));
+    // ---- dynamic state ----
+    {
+        DynState& h = c->hdyn;
+        memset(&h, 0, sizeof(h));
+        double box[3] = {p->xcel, p->ycel, p->zcel};
+        for (int d = 0; d < 3; ++d) { h.box[d] = box[d]; h.boxinv[d] = 1.0 / box[d]; }
+        h.rkcut = rkcut_host(box, p->nfft1, p->nfft2, p->nfft3);
+        h.yratio = p->ycel / p->xcel;
+        h.zratio = p->zcel / p->xcel;
+        for (int d = 0; d < 3; ++d) { h.kl_s[d] = 1.0; h.dr_a[d] = 1.0; h.rvinv[d] = 1.0; }
+        if (cudaMemcpy(c->dyn, &h, sizeof(h), cudaMemcpyHostToDevice)) { pgk_free(c); return PGK_E_CUDA; }
+        ChainDev ch;
+        memset(&ch, 0, sizeof(ch));
+        ch.xlogv = std::log(p->xcel * p->ycel * p->zcel) / 3.0;   // prepmd.F90:527
+        ch.xboxh[0] = p->xcel; ch.xboxh[1] = p->ycel; ch.xboxh[2] = p->zcel;
+        if (cudaMemcpy(c->chain, &ch, sizeof(ch), cudaMemcpyHostToDevice)) { pgk_free(c); return PGK_E_CUDA; }
+    }
+#undef TRY
+    if (cudaDeviceSynchronize() != cudaSuccess) { pgk_free(c); return PGK_E_CUDA; }
+    *out = c;
+    return PGK_OK;
+}
+
+pgk_status pgk_free(pgk_ctx* c) {
+    if (!c) return PGK_OK;
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
+                    c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list,
+                    c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
+                    c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
+                    c->cell_of, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->nbr,
+                    c->ncnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
+                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout};
+    for (void* b : bufs) if (b) cudaFree(b);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return PGK_OK;
+}
+
+pgk_status pgk_upload_state(pgk_ctx* c, const double* cor, const double* vel, const double* box) {
+    if (!c || !cor) return PGK_E_INVALID;
+    size_t b = (size_t)24 * c->natom;
+    PGK_CUDA(c, cudaMemcpyAsync(c->pos, cor, b, cudaMemcpyHostToDevice, c->st));
+    if (vel) PGK_CUDA(c, cudaMemcpyAsync(c->vel, vel, b, cudaMemcpyHostToDevice, c->st));
+    if (box) {
+        pgk_status s = set_dyn_box(c, box);
+        if (s) return s;
+    }
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return PGK_OK;
+}
+
+pgk_status pgk_download_state(pgk_ctx* c, double* cor, double* vel, double* box) {
+    if (!c) return PGK_E_INVALID;
+    size_t b = (size_t)24 * c->natom;
+    if (cor) PGK_CUDA(c, cudaMemcpyAsync(cor, c->pos, b, cudaMemcpyDeviceToHost, c->st));
+    if (vel) PGK_CUDA(c, cudaMemcpyAsync(vel, c->vel, b, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    if (box) for (int d = 0; d < 3; ++d) box[d] = c->hdyn.box[d];
+    return PGK_OK;
+}
+
+pgk_status pgk_set_chain(pgk_ctx* c, const pgk_chain* ch) {
+    if (!c || !ch) return PGK_E_INVALID;
+    ChainDev d;
+    static_assert(sizeof(ChainDev) == sizeof(pgk_chain), "chain layout");
+    memcpy(&d, ch, sizeof(d));
+    PGK_CUDA(c, cudaMemcpyAsync(c->chain, &d, sizeof(d), cudaMemcpyHostToDevice, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return PGK_OK;
+}
+
+pgk_status pgk_get_chain(pgk_ctx* c, pgk_chain* ch) {
+    if (!c || !ch) return PGK_E_INVALID;
+    PGK_CUDA(c, cudaMemcpyAsync(ch, c->chain, sizeof(ChainDev), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return PGK_OK;
+}
+
+pgk_status pgk_transcor(pgk_ctx* c) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s = launch_transcor(c);
+    if (s) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_mklist_cell(pgk_ctx* c, int64_t* nl) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s = launch_mklist(c);
+    if (s) return s;
+    if (nl) *nl = c->hdyn.nlistnball;
+    return PGK_OK;
+}
+
+pgk_status pgk_get_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_t cap, int64_t* nl) {
+    if (!c || !nl) return PGK_E_INVALID;
+    return export_nblist(c, nb_index, nb_list, cap, nl);
+}
+
+pgk_status pgk_calforce(pgk_ctx* c, int32_t flag, double* force, pgk_energies* e, pgk_virials* v) {
+    if (!c || (flag != PGK_MTS_LONG && flag != PGK_MTS_SHORT)) return PGK_E_INVALID;
+    bool want = e || v;
+    pgk_status s = force_group(c, flag, want, want);
+    if (s) return s;
+    int g = flag == PGK_MTS_LONG ? 0 : 1;
+    if (force && (s = force_to_host(c, g, force, false))) return s;
+    if (want && (s = read_acc(c, 1 << g, e, v, flag == PGK_MTS_LONG))) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_ewaldr(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s;
+    bool want = e || v;
+    if ((s = launch_zero_group(c, 0))) return s;
+    if (!c->list_valid && (s = launch_mklist(c))) return s;
+    if ((s = launch_pack(c)) || (s = launch_pair(c, 0, want, want)) || (s = launch_excl(c, 0, want, want))) return s;
+    if (force && (s = force_to_host(c, 0, force, true))) return s;
+    if (want && (s = read_acc(c, 1, e, v, false))) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_fft_pme(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
+    if (!c) return PGK_E_INVALID;
+    if (!c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
+    pgk_status s;
+    bool want = e || v;
+    if ((s = launch_zero_group(c, 0)) || (s = launch_spme(c, 0, want, want))) return s;
+    if (force && (s = force_to_host(c, 0, force, true))) return s;
+    if (want && (s = read_acc(c, 1, e, v, false))) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_calbonded(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s;
+    bool want = e || v;
+    if ((s = launch_zero_group(c, 0)) || (s = launch_bonded(c, 0, want, want, true))) return s;
+    if (force && (s = force_to_host(c, 0, force, true))) return s;
+    if (want && (s = read_acc(c, 1, e, v, false))) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_rattle_c(pgk_ctx* c, const double* old, double eps, double dts) {
+    if (!c || !old) return PGK_E_INVALID;
+    PGK_CUDA(c, cudaMemcpyAsync(c->pos_old, old, (size_t)24 * c->natom, cudaMemcpyHostToDevice, c->st));
+    pgk_status s = launch_rattle_pos(c, eps, dts, false);
+    if (s) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_rattlep_v(pgk_ctx* c, double eps) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s = launch_rattle_vel(c, eps);
+    if (s) return s;
+    return read_status(c);
+}
+
+pgk_status pgk_calpress(pgk_ctx* c, double* kint, double* ptot, double* p9) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s;
+    if ((s = launch_kinetic(c, 0)) || (s = launch_press(c))) return s;
+    pgk_chain ch;
+    if ((s = pgk_get_chain(c, &ch))) return s;
+    if (kint) {
+        long long k;
+        PGK_CUDA(c, cudaMemcpy(&k, c->acc + A_KE, sizeof(k), cudaMemcpyDeviceToHost));
+        *kint = fixv(k);
+    }
+    if (ptot) *ptot = ch.pint;
+    if (p9) for (int k = 0; k < 9; ++k) p9[k] = ch.pintt[k];
+    return PGK_OK;
+}
+
+pgk_status pgk_sync(pgk_ctx* c) {
+    if (!c) return PGK_E_INVALID;
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return read_status(c);
+}
+
+int64_t pgk_kernel_launches(const pgk_ctx* c) { return c ? c->launches : 0; }
+void* pgk_stream(const pgk_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+}  // extern "C"
+
+// ---- stage drivers ---------------------------------------------------------------
+static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* eo) {
+    if (!c || !md || md->nstep_short < 1 || md->dt_long_cal <= 0) return PGK_E_INVALID;
+    if (kind >= 1 && (md->mchain < 2 || md->mchain > 8 || md->nyosh < 1 || md->nyosh > 8 || md->next < 1))
+        return pgk_fail(c, PGK_E_INVALID, "chain parameters");
+    const int nb = c->prm.nstep_book > 0 ? c->prm.nstep_book : 1;
+    const double dts = md->dt_long_cal / (double)md->nstep_short;
+    const bool rattle = md->ifrattle && c->ncgroup > 0;
+    const bool mtk = kind == 2;
+    const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);
+    pgk_status s;
+#define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
+    for (int64_t step = ini; step <= end; ++step) {
+        bool out = md->outinterval > 0 ? (step % md->outinterval == 0) : (step == end);
+        bool ene = out && eo;
+        bool vir = mtk;
+        if (step % nb == 1 || nb == 1 || step == 0) RUN(launch_transcor(c));
+        if (step % nb == 0 || nb == 1) RUN(launch_mklist(c));
+        if (step == 0) {
+            RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir));
+            RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir));
+            if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
+        } else {
+            if (kind >= 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
+            RUN(launch_coeffs(c, kind, *md, 0));
+            for (int is = 1; is <= md->nstep_short; ++is) {
+                bool last = is == md->nstep_short;
+                if (is == 1) RUN(launch_kick_long(c));
+                RUN(launch_kick_short(c));
+                RUN(launch_drift(c, rattle));
+                if (mtk) RUN(launch_box_update(c, kind, *md));
+                if (rattle) RUN(launch_rattle_pos(c, md->eps_rattle, dts, mtk));
+                RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir));
+                if (last) {
+                    if (mtk && c->prm.mts_ewk == PGK_MTS_LONG) RUN(launch_rkcut(c));
+                    RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir));
+                }
+                RUN(launch_kick_short(c));
+                if (last) RUN(launch_kick_long(c));
+                if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
+            }
+            if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
+            if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); RUN(launch_chain(c, chain_kind, *md)); }
+        }
+        if (ene) RUN(read_acc(c, 3, eo, nullptr, true));
+    }
+#undef RUN
+    return read_status(c);
+}
+
+extern "C" {
+pgk_status pgk_moldyn_nve(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e) {
+    return run_md(c, 0, ini, end, md, e);
+}
+pgk_status pgk_moldyn_nhc(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e) {
+    return run_md(c, 1, ini, end, md, e);
+}
+pgk_status pgk_moldyn_mtk(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e) {
+    return run_md(c, 2, ini, end, md, e);
+}
+}

@@ -1,0 +1,214 @@
+"""Host-side mirror of the reference's operator interface over libpgkgpu.so.
+
+The Fortran driver calls subroutines such as ``mklist_cell``, ``calforce``,
+``ewaldr``, ``fft_pme``, ``rattle_c``, ``moldyn_nhc`` on module globals; this
+class exposes the same operations on one device context through the C ABI of
+include/pgk_gpu.h (names, argument meaning, STOP conditions turned into
+:class:`PgkError`).  There is no CPU fallback: constructing an engine without
+the built library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpgkgpu.so")
+HEADER = os.path.join(HERE, "..", "include", "pgk_gpu.h")
+
+_lib = None
+
+
+class PgkError(RuntimeError):
+    def __init__(self, status, msg=""):
+        super().__init__(f"pgk status {status}: {msg}")
+        self.status = status
+
+
+def header_symbols():
+    """Entry points declared in include/pgk_gpu.h."""
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(pgk_[a-z0-9_]+)\s*\(", txt)))
+
+
+def lib():
+    """Load libpgkgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PgkError(abi.PGK_E_CUDA, f"{LIB_PATH} is not built (run thrid_b200/build.py)")
+    L = C.CDLL(LIB_PATH)
+    vp, pd, pi = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    E, V = C.POINTER(abi.EnergiesStruct), C.POINTER(abi.VirialsStruct)
+    L.pgk_version.restype = C.c_char_p
+    L.pgk_status_string.restype = C.c_char_p
+    L.pgk_status_string.argtypes = [C.c_int32]
+    L.pgk_last_error.restype = C.c_char_p
+    L.pgk_last_error.argtypes = [vp]
+    L.pgk_init.argtypes = [C.POINTER(abi.SystemStruct), C.POINTER(abi.ParamsStruct), C.POINTER(vp)]
+    L.pgk_free.argtypes = [vp]
+    L.pgk_upload_state.argtypes = [vp, pd, pd, pd]
+    L.pgk_download_state.argtypes = [vp, pd, pd, pd]
+    L.pgk_set_chain.argtypes = [vp, C.POINTER(abi.ChainStruct)]
+    L.pgk_get_chain.argtypes = [vp, C.POINTER(abi.ChainStruct)]
+    L.pgk_transcor.argtypes = [vp]
+    L.pgk_mklist_cell.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.pgk_get_nblist.argtypes = [vp, pi, pi, C.c_int64, C.POINTER(C.c_int64)]
+    L.pgk_calforce.argtypes = [vp, C.c_int32, pd, E, V]
+    for f in ("pgk_ewaldr", "pgk_fft_pme", "pgk_calbonded"):
+        getattr(L, f).argtypes = [vp, pd, E, V]
+    L.pgk_rattle_c.argtypes = [vp, pd, C.c_double, C.c_double]
+    L.pgk_rattlep_v.argtypes = [vp, C.c_double]
+    for f in ("pgk_moldyn_nve", "pgk_moldyn_nhc", "pgk_moldyn_mtk"):
+        getattr(L, f).argtypes = [vp, C.c_int64, C.c_int64, C.POINTER(abi.MdParamsStruct), E]
+    L.pgk_calpress.argtypes = [vp, pd, pd, pd]
+    L.pgk_sync.argtypes = [vp]
+    L.pgk_kernel_launches.restype = C.c_int64
+    L.pgk_kernel_launches.argtypes = [vp]
+    L.pgk_stream.restype = vp
+    L.pgk_stream.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class PgkEngine:
+    """One device context (the md_global state of one system)."""
+
+    def __init__(self, system, params=None, upload=True):
+        self.L = lib()
+        self.sys = system
+        self.csys = abi.CSystem(system)
+        self.params = dict(params or system.params)
+        self.prm = abi.params_struct(self.params)
+        h = C.c_void_p()
+        st = self.L.pgk_init(C.byref(self.csys.struct), C.byref(self.prm), C.byref(h))
+        if st != abi.PGK_OK:
+            raise PgkError(st, "pgk_init failed: " + self.L.pgk_status_string(st).decode())
+        self.h = h
+        if upload:
+            self.upload_state(system.atmcor, system.atmvel, system.box)
+
+    # -- lifetime ---------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pgk_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != abi.PGK_OK:
+            msg = self.L.pgk_last_error(self.h)
+            raise PgkError(st, (msg or b"").decode() or self.L.pgk_status_string(st).decode())
+
+    # -- state --------------------------------------------------------------------
+    def upload_state(self, atmcor, atmvel=None, box=None):
+        cor = np.ascontiguousarray(atmcor, dtype=np.float64)
+        vel = None if atmvel is None else np.ascontiguousarray(atmvel, dtype=np.float64)
+        bx = None if box is None else np.ascontiguousarray(box, dtype=np.float64)
+        self._check(self.L.pgk_upload_state(self.h, _p(cor), _p(vel) if vel is not None else None,
+                                            _p(bx) if bx is not None else None))
+
+    def download_state(self):
+        n = self.sys.natom
+        cor = np.zeros((n, 3)); vel = np.zeros((n, 3)); box = np.zeros(3)
+        self._check(self.L.pgk_download_state(self.h, _p(cor), _p(vel), _p(box)))
+        return cor, vel, box
+
+    def set_chain(self, ch):
+        self._check(self.L.pgk_set_chain(self.h, C.byref(ch)))
+
+    def get_chain(self):
+        ch = abi.ChainStruct()
+        self._check(self.L.pgk_get_chain(self.h, C.byref(ch)))
+        return ch
+
+    # -- reference-named operations ----------------------------------------------
+    def transcor(self):
+        self._check(self.L.pgk_transcor(self.h))
+
+    def mklist_cell(self):
+        nl = C.c_int64(0)
+        self._check(self.L.pgk_mklist_cell(self.h, C.byref(nl)))
+        return nl.value
+
+    def get_nblist(self):
+        n = self.sys.natom
+        idx = np.zeros(n, np.int32)
+        nl = C.c_int64(0)
+        self._check(self.L.pgk_get_nblist(self.h, idx.ctypes.data_as(C.POINTER(C.c_int32)), None, 0, C.byref(nl)))
+        lst = np.zeros(max(nl.value, 1), np.int32)
+        self._check(self.L.pgk_get_nblist(self.h, idx.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          lst.ctypes.data_as(C.POINTER(C.c_int32)), nl.value, C.byref(nl)))
+        return idx, lst[:nl.value]
+
+    def _fev(self, fn, *pre):
+        f = np.zeros((self.sys.natom, 3))
+        e = abi.EnergiesStruct()
+        v = abi.VirialsStruct()
+        self._check(fn(self.h, *pre, _p(f), C.byref(e), C.byref(v)))
+        return f, e.as_dict(), v.as_dict()
+
+    def calforce(self, mts_flag=abi.MTS_LONG):
+        return self._fev(self.L.pgk_calforce, mts_flag)
+
+    def ewaldr(self):
+        return self._fev(self.L.pgk_ewaldr)
+
+    def fft_pme(self):
+        return self._fev(self.L.pgk_fft_pme)
+
+    def calbonded(self):
+        return self._fev(self.L.pgk_calbonded)
+
+    def rattle_c(self, atmcor_old, eps_rattle, dt_short_cal):
+        old = np.ascontiguousarray(atmcor_old, dtype=np.float64)
+        self._check(self.L.pgk_rattle_c(self.h, _p(old), eps_rattle, dt_short_cal))
+
+    def rattlep_v(self, eps_rattle):
+        self._check(self.L.pgk_rattlep_v(self.h, eps_rattle))
+
+    def calpress(self):
+        k = C.c_double(); p = C.c_double(); t = np.zeros(9)
+        self._check(self.L.pgk_calpress(self.h, C.byref(k), C.byref(p), _p(t)))
+        return k.value, p.value, t.reshape(3, 3, order="F")
+
+    def _md(self, fn, ini, end, md):
+        e = abi.EnergiesStruct()
+        self._check(fn(self.h, int(ini), int(end), C.byref(md), C.byref(e)))
+        return e.as_dict()
+
+    def moldyn_nve(self, ini, end, md):
+        return self._md(self.L.pgk_moldyn_nve, ini, end, md)
+
+    def moldyn_nhc(self, ini, end, md):
+        return self._md(self.L.pgk_moldyn_nhc, ini, end, md)
+
+    def moldyn_mtk(self, ini, end, md):
+        return self._md(self.L.pgk_moldyn_mtk, ini, end, md)
+
+    def sync(self):
+        self._check(self.L.pgk_sync(self.h))
+
+    @property
+    def kernel_launches(self):
+        return int(self.L.pgk_kernel_launches(self.h))
+
+    @property
+    def stream(self):
+        return self.L.pgk_stream(self.h)
