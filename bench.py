@@ -1,0 +1,324 @@
+"""Throughput of the B200 force-and-integration engine on the 200k-atom butane
+NPT workload (flexible butane, 14,286 molecules = 200,004 atoms, 130 A box,
+anisotropic MTK barostat at 1 atm + NHC thermostat at 250 K, rc 12 A, SPME
+128^3 order 5, dt 1 fs, mixed precision, RATTLE on the X-H bonds).
+
+A step is one outer MD step (dt_long) of moldyn_mtk, pair-list rebuilds
+included at their natural interval (nstep_book = 50).  Synthetic, seeded
+inputs of that shape (no dataset).  The working set (pair list ~0.6 GB) is
+larger than L2, so no explicit flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, no collective on the data
+path: the reference path does not shard); value = all ranks' atom-steps / max
+rank time.  --impl reference times the CPU restatement of the reference
+algorithm (the Fortran reference cannot be compiled in this image) on the
+host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-steps/s (200k-atom butane NPT, mixed precision)"
+UNIT = "atom-steps/s"
+WORKLOAD = "butane_200004_npt_mtk_aniso_nhc_spme128_o5_rc12_dt1fs"
+NSTEP_BOOK = 50
+
+
+def make_system(precision):
+    from thrid_b200 import systems as S
+    s = S.butane_box(precision=precision)
+    s.params["nstep_book"] = NSTEP_BOOK
+    return s
+
+
+def md_params(s, nstep_short=1):
+    from thrid_b200 import abi
+    from thrid_b200 import systems as S
+    T = S.kelvin_to_reduced(250.0)
+    return abi.md_struct(S.fs_to_reduced(1.0), nstep_short=nstep_short, mchain=3, text=T,
+                         tfreq=1.0e13 * S.TIMEREF, vfreq=0.2e12 * S.TIMEREF, pext=S.pa_to_reduced(1.01325e5),
+                         pcont_axis=abi.PCONT_ANISO, degfree=s.degfree_all, ifrattle=1, eps_rattle=1e-7,
+                         outinterval=0)
+
+
+def ns_per_day(steps_per_s, dt_fs=1.0):
+    return steps_per_s * dt_fs * 86400.0 * 1e-6
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def profiled_traffic():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_pair_mixed_butane200k.md")
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from thrid_b200 import abi
+    from thrid_b200.pgk import PgkEngine
+
+    torch.cuda.set_device(local_rank)
+    s = make_system(abi.PREC_MIXED)
+    md = md_params(s)
+    eng = PgkEngine(s)
+    stream = torch.cuda.ExternalStream(eng.stream)
+    eng.set_chain(abi.chain_init(s.box))
+    # ---- warm-up: step 0 (initial forces) + W steps ----
+    eng.moldyn_mtk(0, args.warmup, md)
+    eng.sync()
+    dist_barrier(world)
+    step0 = args.warmup + 1
+    launches0 = eng.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        e0.record(stream)
+        ene = eng.moldyn_mtk(step0, step0 + args.steps - 1, md)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist_barrier(world)
+    ms = e0.elapsed_time(e1)
+    launches = eng.kernel_launches - launches0
+    ms_max = dist_max(ms, world)
+    # ---- end to end through the public API with host buffers ----
+    e2e = e2e_leg(eng, s, md, step0 + args.steps, max(3, args.steps // 4), world)
+    # ---- dominant kernel roofline (pair kernel), measured live ----
+    roof = roofline(eng)
+    eng.close()
+    natom = s.natom
+    value = world * natom * args.steps / (ms_max / 1e3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int64 (pair/SPME/bonded), fp64 (x, v, RATTLE, MTK)",
+        "data": "synthetic (seeded butane lattice, OPLS-like parameters)",
+        "config": {"workload": WORKLOAD, "natom": natom, "replicas": world, "global_batch": world * natom,
+                   "parallelism": f"replicas{world}", "nstep_book": NSTEP_BOOK,
+                   "l2": "working set > L2 (pair list ~0.6 GB), no flush"},
+        "ns_per_day": ns_per_day(args.steps / (ms_max / 1e3)),
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+        "energies_last": {k: ene[k] for k in ("pot_tot", "pot_vdw", "pot_elc", "pot_ewk")} if ene else None,
+    }
+    out["clocks"] = clk.summary()
+    if rank == 0:
+        out["cpu_baseline"] = cpu_baseline(args)
+    return out
+
+
+def e2e_leg(eng, s, md, start, nsteps, world):
+    """Host-driver ownership of the state (like the Fortran module arrays):
+    every step uploads x, v from pinned host memory, runs one outer step and
+    reads back x, v and the energies."""
+    import torch
+    n = s.natom
+    cor = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    vel = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    c, v, _ = eng.download_state()
+    cor.numpy()[:] = c
+    vel.numpy()[:] = v
+    cn, vn = cor.numpy(), vel.numpy()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    t0 = time.perf_counter()
+    for k in range(nsteps):
+        eng.upload_state(cn, vn)
+        eng.moldyn_mtk(start + k, start + k, md)
+        c, v, _ = eng.download_state()
+        cn[:] = c
+        vn[:] = v
+    torch.cuda.synchronize()
+    dt = dist_max(time.perf_counter() - t0, world)
+    return {"value": world * n * nsteps / dt, "unit": UNIT, "steps": nsteps,
+            "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 2 * 24 * n + 13 * 8}
+
+
+def roofline(eng):
+    import ctypes as C
+    ms = C.c_double(); units = C.c_double(); entries = C.c_double()
+    st = eng.L.pgk_bench_kernel(eng.h, 0, 20, C.byref(ms), C.byref(units), C.byref(entries))
+    if st != 0:
+        return {"error": f"pgk_bench_kernel status {st}"}
+    flop = 61.0 * units.value                       # algorithmic flop per interacting pair
+    achieved = flop / (ms.value * 1e-3) / 1e12       # TFLOP/s
+    peaks = measured_peaks()
+    clk = peaks.get("sm_max_mhz", 1965.0)
+    peak = 148 * 128 * 2 * clk * 1e6 / 1e12           # FP32 CUDA-core FMA peak at the max SM clock
+    traffic = profiled_traffic()
+    return {"kernel": "k_pair_mixed<ENE,VIR>", "bound": "fp32", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "peak_source": f"nominal FP32 FMA peak 148 SM x 128 lanes x 2 x {clk:.0f} MHz "
+                           "(MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
+            "ms_per_launch": ms.value, "pairs_per_launch": units.value, "list_entries": entries.value,
+            "hbm_gbs_index_stream": entries.value * 4 / (ms.value * 1e-3) / 1e9,
+            "hbm_peak_gbs": peaks.get("hbm_gbs")}
+
+
+def cpu_baseline(args, nsteps=None, threads=None):
+    """The oracle (C++ FP64 restatement of the reference loops) on the host
+    cores, on a bounded sample of the same workload."""
+    from oracle import oracle as orc
+    from thrid_b200 import abi
+    threads = threads or os.cpu_count() or 1
+    s = make_system(abi.PREC_FP64)
+    md = md_params(s)
+    o = orc.Oracle(s, threads=threads)
+    o.set_chain(abi.chain_init(s.box))
+    t0 = time.perf_counter()
+    st, _ = o.moldyn(2, 0, 0, md)              # list build + initial forces (not timed)
+    t_init = time.perf_counter() - t0
+    nsteps = nsteps or 3
+    t0 = time.perf_counter()
+    st2, _ = o.moldyn(2, 1, nsteps, md)
+    dt = time.perf_counter() - t0
+    return {"value": s.natom * nsteps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nsteps} outer MTK steps of the 200,004-atom butane system after step 0 "
+                      f"(step-0 list build + forces took {t_init:.1f} s, untimed)",
+            "status": int(st2)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    cb = cpu_baseline(args, nsteps=max(1, min(args.steps, 3)))
+    return {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * 200004 / cb["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded butane lattice)",
+            "config": {"workload": WORKLOAD, "natom": 200004, "parallelism": "host threads"},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Fortran cannot be compiled here (no gfortran); its C++ restatement runs instead"}
+
+
+# ---- torch.distributed plumbing (replicas; barrier + max over ranks only) ----
+_pg = None
+
+
+def dist_init():
+    global _pg
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        _pg = dist
+    return rank, world, local
+
+
+def dist_barrier(world):
+    if world > 1 and _pg is not None:
+        _pg.barrier()
+
+
+def dist_max(x, world):
+    if world > 1 and _pg is not None:
+        import torch
+        t = torch.tensor([float(x)], device="cuda")
+        _pg.all_reduce(t, op=_pg.ReduceOp.MAX)
+        return float(t.item())
+    return float(x)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_init()
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+    else:
+        out = run_ours(args, rank, world, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out))
+    if world > 1 and _pg is not None:
+        _pg.barrier()
+        _pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -268,6 +268,17 @@ int64_t pgk_kernel_launches(const pgk_ctx* ctx);
  * the context's kernels with their own events. */
 void* pgk_stream(const pgk_ctx* ctx);
 
+/* Instrumentation (no reference counterpart): launch one kernel of the force
+ * path `iters` times back to back on the context's stream, bracketed by CUDA
+ * events, and return the mean device time per launch in *ms.  which:
+ *   0 = real-space pair kernel (ewaldrp) with virials, 1 = SPME spread,
+ *   2 = SPME gather, 3 = one forward 3-D FFT (three axis passes).
+ * *units receives the algorithmic work of one launch: unique pairs inside
+ * the cutoff (0), atoms (1, 2) or grid points (3); *entries the number of
+ * full-list entries the pair kernel reads. */
+pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
+                            double* entries);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,298 @@
+"""Parity of the sm_100a engine (through the C ABI) with the FP64 oracle.
+
+Bars (written here, per result):
+  pair list          bit-exact: identical nb_indexall / nb_listall / nlistnball
+  FP64 device path   force RMS relative error <= 1e-12, energies <= 1e-10 relative
+  mixed precision    force RMS relative error <= 1e-5
+  MD trajectories    FP64 positions within 1e-9 A of the oracle after the steps run
+"""
+import numpy as np
+import pytest
+
+from tests.conftest import rel_rms
+from thrid_b200 import abi
+from thrid_b200 import systems as S
+from thrid_b200.pgk import PgkEngine, PgkError
+
+pytestmark = pytest.mark.gpu
+
+FP64_FORCE = 1e-12
+FP64_ENERGY = 1e-10
+MIXED_FORCE = 1e-5
+MIXED_ENERGY = 1e-5
+
+_cache = {}
+
+
+def case(name):
+    if name not in _cache:
+        _cache[name] = {
+            "water": lambda: S.water_box(),                                   # mklist2a fallback, 2^3 cells
+            "propanol_small": lambda: S.small_box("propanol", nside=4, spacing=5.6),
+            "propanol_cells": lambda: S.propanol_box(nside=11, box=57.2),    # mklist_cell, 4^3 cells
+            "butane_small": lambda: S.small_box("butane", nside=5, spacing=5.4, nfft=24, order=5),
+            "nacl": lambda: _jittered(S.nacl_lattice()),
+        }[name]()
+    return _cache[name]
+
+
+def _jittered(s, amp=0.05, seed=11):
+    """Perfect lattices have ~0 net force; displace ions so forces are O(1)."""
+    s.atmcor = s.atmcor + np.random.default_rng(seed).normal(0.0, amp, s.atmcor.shape)
+    return s
+
+
+def engine(s, prec, **over):
+    p = dict(s.params)
+    p["precision"] = prec
+    p.update(over)
+    return PgkEngine(s, p)
+
+
+def oracle_for(oracle_mod, s, **over):
+    p = dict(s.params)
+    p.update(over)
+    return oracle_mod.Oracle(s, p)
+
+
+def erel(a, b):
+    return abs(a - b) / max(1.0, abs(b))
+
+
+# ---------------------------------------------------------------- pair list ---
+@pytest.mark.parametrize("name", ["water", "propanol_small", "propanol_cells", "nacl"])
+def test_pair_list_is_bit_exact(oracle_mod, name):
+    s = case(name)
+    o = oracle_for(oracle_mod, s)
+    mode, oidx, olst = o.mklist()
+    e = engine(s, abi.PREC_FP64)
+    nl = e.mklist_cell()
+    idx, lst = e.get_nblist()
+    assert nl == len(olst)
+    assert np.array_equal(idx, oidx)
+    assert np.array_equal(lst, olst)
+
+
+def test_pair_list_regrows_rows_on_overflow(oracle_mod):
+    s = case("propanol_small")
+    o = oracle_for(oracle_mod, s)
+    _, oidx, olst = o.mklist()
+    e = engine(s, abi.PREC_MIXED, max_nbr=32)     # far too small: the engine regrows and rebuilds
+    e.mklist_cell()
+    idx, lst = e.get_nblist()
+    assert np.array_equal(idx, oidx) and np.array_equal(lst, olst)
+
+
+def test_cell_mode_order_matches_mklist_cell(oracle_mod):
+    s = case("propanol_cells")
+    o = oracle_for(oracle_mod, s, list_mode=abi.LIST_CELL)
+    mode, oidx, olst = o.mklist()
+    assert mode == abi.LIST_CELL
+    e = engine(s, abi.PREC_FP64, list_mode=abi.LIST_CELL)
+    e.mklist_cell()
+    idx, lst = e.get_nblist()
+    assert np.array_equal(idx, oidx) and np.array_equal(lst, olst)
+
+
+def test_transcor_matches(oracle_mod):
+    s = case("propanol_small")
+    x = s.atmcor + np.array([30.0, -25.0, 0.5])      # push molecules out of the box
+    o = oracle_for(oracle_mod, s)
+    o.set_state(x)
+    o.transcor()
+    ox, _, _ = o.get_state()
+    e = engine(s, abi.PREC_FP64)
+    e.upload_state(x)
+    e.transcor()
+    gx, _, _ = e.download_state()
+    assert np.array_equal(gx, ox)
+
+
+# ------------------------------------------------------------------- forces ---
+def _ref_terms(oracle_mod, s):
+    o = oracle_for(oracle_mod, s)
+    o.mklist()
+    return o, o.ewaldrp(), o.fft_pmep(), o.bonded()
+
+
+@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl"])
+def test_fp64_forces_energies_virials(oracle_mod, name):
+    s = case(name)
+    o, (rf, re, rv), (kf, ke, kv), (bf, be, bv) = _ref_terms(oracle_mod, s)
+    e = engine(s, abi.PREC_FP64)
+    e.mklist_cell()
+    f, en, vi = e.ewaldr()
+    assert rel_rms(f, rf) < FP64_FORCE
+    assert erel(en["pot_vdw"], re["pot_vdw"]) < FP64_ENERGY
+    assert erel(en["pot_elc"], re["pot_elc"]) < FP64_ENERGY
+    assert erel(vi["pot_viri_lj"], rv["pot_viri_lj"]) < FP64_ENERGY
+    assert np.abs(vi["pot_virit_coul"] - rv["pot_virit_coul"]).max() < 1e-9 * max(1, np.abs(rv["pot_virit_coul"]).max())
+    assert np.abs(vi["pot_virit_lj"] - rv["pot_virit_lj"]).max() < 1e-9 * max(1, np.abs(rv["pot_virit_lj"]).max())
+    f, en, vi = e.fft_pme()
+    assert rel_rms(f, kf) < FP64_FORCE
+    assert erel(en["pot_ewk"], ke["pot_ewk"]) < FP64_ENERGY
+    assert np.abs(vi["pot_virit_coul"] - kv["pot_virit_coul"]).max() < 1e-9 * max(1, np.abs(kv["pot_virit_coul"]).max())
+    if np.abs(bf).max() > 0:
+        f, en, vi = e.calbonded()
+        assert rel_rms(f, bf) < FP64_FORCE
+        for k in ("pot_bond", "pot_angl", "pot_tors", "pot_torsrb", "pot_elc14", "pot_vdw14"):
+            assert erel(en[k], be[k]) < FP64_ENERGY, k
+        for k in ("atm_viri_angl", "atm_viri_tors", "atm_viri_14"):
+            assert erel(vi[k], bv[k]) < 1e-9, k
+
+
+@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl"])
+def test_mixed_forces_within_1e5(oracle_mod, name):
+    s = case(name)
+    o, (rf, re, rv), (kf, ke, kv), (bf, be, bv) = _ref_terms(oracle_mod, s)
+    e = engine(s, abi.PREC_MIXED)
+    e.mklist_cell()
+    f1, en, _ = e.ewaldr()
+    assert rel_rms(f1, rf) < MIXED_FORCE
+    assert erel(en["pot_elc"], re["pot_elc"]) < MIXED_ENERGY * max(1, abs(re["pot_elc"]))
+    f2, en, _ = e.fft_pme()
+    assert rel_rms(f2, kf) < MIXED_FORCE
+    f3, en, _ = e.calbonded()
+    if np.abs(bf).max() > 0:
+        assert rel_rms(f3, bf) < MIXED_FORCE
+    assert rel_rms(f1 + f2 + f3, rf + kf + bf) < MIXED_FORCE
+
+
+def test_calforce_mts_groups(oracle_mod):
+    s = case("propanol_small")
+    over = dict(mts_bond=abi.MTS_SHORT, mts_angl=abi.MTS_SHORT, mts_tors=abi.MTS_SHORT,
+                mts_torsrb=abi.MTS_SHORT)
+    o = oracle_for(oracle_mod, s, **over)
+    o.mklist()
+    e = engine(s, abi.PREC_FP64, **over)
+    e.mklist_cell()
+    for flag in (abi.MTS_SHORT, abi.MTS_LONG):
+        rf, re, rv = o.calforce(flag)
+        f, en, vi = e.calforce(flag)
+        assert rel_rms(f, rf) < FP64_FORCE
+        for k in ("pot_tot", "pot_nonbon", "pot_ewc", "pot_ewnq"):
+            assert erel(en[k], re[k]) < FP64_ENERGY, (flag, k)
+        assert erel(vi["pot_viri_coul"], rv["pot_viri_coul"]) < 1e-9
+
+
+def test_mixed_is_deterministic():
+    s = case("propanol_small")
+    e = engine(s, abi.PREC_MIXED)
+    e.mklist_cell()
+    a, ea, _ = e.calforce(abi.MTS_LONG)
+    b, eb, _ = e.calforce(abi.MTS_LONG)
+    assert np.array_equal(a, b)
+    assert ea == eb
+
+
+# ------------------------------------------------------------------ RATTLE ---
+def test_rattle_matches_oracle(oracle_mod):
+    s = case("water")
+    dt = S.fs_to_reduced(1.0)
+    old = s.atmcor.copy()
+    new = old + dt * s.atmvel
+    o = oracle_for(oracle_mod, s)
+    o.set_state(new, s.atmvel)
+    assert o.rattle_c(old, 1e-7, dt) == 0
+    assert o.rattlep_v(1e-7) == 0
+    ox, ov, _ = o.get_state()
+    e = engine(s, abi.PREC_FP64)
+    e.upload_state(new, s.atmvel)
+    e.rattle_c(old, 1e-7, dt)
+    e.rattlep_v(1e-7)
+    gx, gv, _ = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-12
+    assert np.abs(gv - ov).max() < 1e-10
+
+
+def test_rattle_nonconvergence_is_a_status_not_a_fault():
+    s = case("water")
+    dt = S.fs_to_reduced(1.0)
+    old = s.atmcor.copy()
+    e = engine(s, abi.PREC_FP64)
+    e.upload_state(old + dt * s.atmvel, s.atmvel)
+    with pytest.raises(PgkError) as ex:
+        e.rattle_c(old, 0.0, dt)       # tolerance 0 cannot be met: bounded loop gives up
+    assert ex.value.status == abi.PGK_E_RATTLE_NOCONV
+    e.rattle_c(old, 1e-7, dt)          # context still usable afterwards
+
+
+# -------------------------------------------------------------- MD drivers ---
+def _md(s, dt_fs=1.0, kind="nve", nstep_short=1, T=300.0, pext_pa=0.0, axis=abi.PCONT_ISO, outinterval=0):
+    Tr = S.kelvin_to_reduced(T)
+    return abi.md_struct(S.fs_to_reduced(dt_fs), nstep_short=nstep_short, mchain=3, text=Tr,
+                         tfreq=1.0e13 * S.TIMEREF, vfreq=0.2e12 * S.TIMEREF, pext=S.pa_to_reduced(pext_pa),
+                         pcont_axis=axis, degfree=s.degfree_all, ifrattle=1, eps_rattle=1e-7,
+                         outinterval=outinterval)
+
+
+def _run_pair(oracle_mod, s, kind, md, steps, prec=abi.PREC_FP64, **over):
+    o = oracle_for(oracle_mod, s, **over)
+    o.set_chain(abi.chain_init(s.box))
+    st, oe = o.moldyn({"nve": 0, "nhc": 1, "mtk": 2}[kind], 0, steps, md)
+    assert st == 0
+    e = engine(s, prec, **over)
+    e.set_chain(abi.chain_init(s.box))
+    ge = getattr(e, "moldyn_" + kind)(0, steps, md)
+    return o, e, oe, ge
+
+
+@pytest.mark.parametrize("kind,name", [("nve", "water"), ("nhc", "propanol_small"), ("mtk", "propanol_small")])
+def test_fp64_md_matches_oracle(oracle_mod, kind, name):
+    s = case(name)
+    md = _md(s, kind=kind, pext_pa=1.0e5)
+    o, e, oe, ge = _run_pair(oracle_mod, s, kind, md, 8)
+    ox, ov, ob = o.get_state()
+    gx, gv, gb = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-9
+    assert np.abs(gv - ov).max() < 1e-8
+    assert np.abs(gb - ob).max() < 1e-12
+    assert erel(ge["pot_tot"], oe["pot_tot"]) < 1e-8
+    if kind != "nve":
+        oc, gc = o.get_chain(), e.get_chain()
+        assert np.abs(np.array(gc.vlogs[:3]) - np.array(oc.vlogs[:3])).max() < 1e-9
+    if kind == "mtk":
+        assert abs(gc.vlogv - oc.vlogv) < 1e-9 * max(1.0, abs(oc.vlogv))
+        assert abs(gc.pint - oc.pint) < 1e-8 * max(1.0, abs(oc.pint))
+
+
+def test_fp64_mtk_aniso_matches_oracle(oracle_mod):
+    s = case("propanol_small")
+    md = _md(s, kind="mtk", pext_pa=1.0e5, axis=abi.PCONT_ANISO)
+    o, e, oe, ge = _run_pair(oracle_mod, s, "mtk", md, 6)
+    ox, _, ob = o.get_state()
+    gx, _, gb = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-9
+    assert np.abs(gb - ob).max() < 1e-12
+    oc, gc = o.get_chain(), e.get_chain()
+    assert np.abs(np.array(gc.vboxg[:]) - np.array(oc.vboxg[:])).max() < 1e-9
+
+
+def test_fp64_respa_matches_oracle(oracle_mod):
+    s = case("propanol_small")
+    over = dict(mts_bond=abi.MTS_SHORT, mts_angl=abi.MTS_SHORT, mts_tors=abi.MTS_SHORT, mts_torsrb=abi.MTS_SHORT)
+    md = _md(s, dt_fs=2.0, kind="nhc", nstep_short=4)
+    o, e, oe, ge = _run_pair(oracle_mod, s, "nhc", md, 5, **over)
+    ox, _, _ = o.get_state()
+    gx, _, _ = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-9
+
+
+def test_mixed_md_tracks_fp64(oracle_mod):
+    s = case("propanol_small")
+    md = _md(s, kind="nhc")
+    o, e, oe, ge = _run_pair(oracle_mod, s, "nhc", md, 10, prec=abi.PREC_MIXED)
+    ox, _, _ = o.get_state()
+    gx, _, _ = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-4
+    assert erel(ge["pot_tot"], oe["pot_tot"]) < 1e-4 * max(1.0, abs(oe["pot_tot"]))
+
+
+def test_list_rebuild_inside_md_run(oracle_mod):
+    s = case("water")
+    md = _md(s, kind="nve")
+    over = dict(nstep_book=3)
+    o, e, oe, ge = _run_pair(oracle_mod, s, "nve", md, 7, **over)
+    ox, _, _ = o.get_state()
+    gx, _, _ = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-9

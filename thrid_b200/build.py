@@ -1,6 +1,7 @@
 """Build libpgkgpu.so in-tree with nvcc for sm_100a (B200)."""
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -11,7 +12,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpgkgpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+OBJDIR = os.path.join(HERE, "_build")
 
 
 def sources():
@@ -31,12 +33,27 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compile each .cu to an object in parallel, then link the shared library."""
     if not force and not needs_build():
         return LIB
-    cmd = [NVCC, *ARCH, *FLAGS, *extra, "-o", LIB, *sources(), "-lcudart"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.check_call(cmd)
+    os.makedirs(OBJDIR, exist_ok=True)
+
+    def one(src):
+        obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", "-o", obj, src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0 or verbose:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}")
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        objs = list(ex.map(one, sources()))
+    link = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+    subprocess.check_call(link)
     return LIB
 
 

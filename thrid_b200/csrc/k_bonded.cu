@@ -76,7 +76,7 @@ __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ 
     if (want) {
         const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
                              A_VTB + 6, A_VTB + 7, A_VTB + 8};
-        block_acc<11>(v, acc, idx);
+        block_acc<11>(v, acc, idx, !MIXED);
     }
 }
 
@@ -124,7 +124,7 @@ __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ 
     if (want) {
         const int idx[11] = {A_ANGL, A_VA, A_VTA + 0, A_VTA + 1, A_VTA + 2, A_VTA + 3, A_VTA + 4, A_VTA + 5,
                              A_VTA + 6, A_VTA + 7, A_VTA + 8};
-        block_acc<11>(v, acc, idx);
+        block_acc<11>(v, acc, idx, !MIXED);
     }
 }
 
@@ -218,7 +218,7 @@ __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ 
     if (want) {
         const int idx[11] = {RB ? A_TORSRB : A_TORS, A_VT, A_VTT + 0, A_VTT + 1, A_VTT + 2, A_VTT + 3, A_VTT + 4,
                              A_VTT + 5, A_VTT + 6, A_VTT + 7, A_VTT + 8};
-        block_acc<11>(v, acc, idx);
+        block_acc<11>(v, acc, idx, !MIXED);
     }
 }
 
@@ -258,7 +258,7 @@ __global__ void k_non14(const double* __restrict__ pos, const double* __restrict
     if (want) {
         const int idx[12] = {A_ELC14, A_VDW14, A_V14, A_VT14 + 0, A_VT14 + 1, A_VT14 + 2, A_VT14 + 3, A_VT14 + 4,
                              A_VT14 + 5, A_VT14 + 6, A_VT14 + 7, A_VT14 + 8};
-        block_acc<12>(v, acc, idx);
+        block_acc<12>(v, acc, idx, !MIXED);
     }
 }
 

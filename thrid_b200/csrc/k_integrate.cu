@@ -130,7 +130,8 @@ __global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict_
 }
 
 // sum m v^2 and sum m v_a v_b (nhcint kint, calpress kinetic terms)
-__global__ void k_kinetic(const double* __restrict__ vel, const double* __restrict__ mass, int n, long long* acc) {
+__global__ void k_kinetic(const double* __restrict__ vel, const double* __restrict__ mass, int n, long long* acc,
+                          int dbl) {
     double v[10] = {0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double m = mass[i], x = vel[3 * i], y = vel[3 * i + 1], z = vel[3 * i + 2];
@@ -143,15 +144,15 @@ __global__ void k_kinetic(const double* __restrict__ vel, const double* __restri
     }
     const int idx[10] = {A_KE, A_KET + 0, A_KET + 1, A_KET + 2, A_KET + 3, A_KET + 4, A_KET + 5, A_KET + 6,
                          A_KET + 7, A_KET + 8};
-    block_acc<10>(v, acc, idx);
+    block_acc<10>(v, acc, idx, dbl != 0);
 }
 
-__device__ __forceinline__ double fixv(const long long* acc, int k) { return (double)acc[k] * PGK_FORCE_ISCALE; }
 
 // ---- chain updates (single thread) -------------------------------------------
 struct ChainArgs {
     pgk_mdparams md;
     int degfree;
+    int dbl;
     int kind;          // 1 nhcint, 2 nhcpisoint, 3 nhcpanisoint
 };
 
@@ -184,7 +185,7 @@ __global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restric
     const pgk_mdparams& md = a.md;
     int M = md.mchain;
     double dt = md.dt_long_cal;
-    double kint = fixv(acc, A_KE);
+    double kint = acc_get(acc, A_KE, a.dbl != 0);
     double glogs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     double gkt = md.text;
     if (a.kind == 1) {   // nhcint.F90:8-140
@@ -360,13 +361,14 @@ __global__ void k_rkcut(DynState* __restrict__ dyn, int n1, int n2, int n3) {
 
 // calpress, atomic branch: pint / pintt of the current state from the kinetic
 // sums and both groups' virials (+ self and net-charge terms)
-struct PressArgs { double pot_ewc, netchrgsq, alpha; int ifspme, ifnetqcorrp; };
+struct PressArgs { double pot_ewc, netchrgsq, alpha; int ifspme, ifnetqcorrp, dbl; };
 
 __global__ void k_press(const long long* __restrict__ acc, const DynState* __restrict__ dyn, ChainDev* chain,
                         PressArgs a) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const long long* A = acc;              // kinetic sums live in group 0
-    double K = fixv(A, A_KE);
+    const bool dbl = a.dbl != 0;
+    double K = acc_get(A, A_KE, dbl);
     double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
     double pi = 3.14159265358979323846;
     double a1 = -pi / (a.alpha * a.alpha * vol);
@@ -376,13 +378,13 @@ __global__ void k_press(const long long* __restrict__ acc, const DynState* __res
     for (int k = 0; k < 9; ++k) Wt[k] = 0.0;
     for (int g = 0; g < 2; ++g) {
         const long long* G = acc + (size_t)g * NACC;
-        W += fixv(G, A_VC) + fixv(G, A_VLJ) + fixv(G, A_VB) + fixv(G, A_VA) + fixv(G, A_VT) + fixv(G, A_V14);
+        W += acc_get(G, A_VC, dbl) + acc_get(G, A_VLJ, dbl) + acc_get(G, A_VB, dbl) + acc_get(G, A_VA, dbl) + acc_get(G, A_VT, dbl) + acc_get(G, A_V14, dbl);
         for (int k = 0; k < 9; ++k) {
             // coulomb / LJ tensors are stored as their lower triangle
             int r = k % 3, cl = k / 3;
             int ks = r >= cl ? k : cl + 3 * r;
-            Wt[k] += fixv(G, A_VTC + ks) + fixv(G, A_VTLJ + ks) + fixv(G, A_VTB + k) + fixv(G, A_VTA + k) +
-                     fixv(G, A_VTT + k) + fixv(G, A_VT14 + k);
+            Wt[k] += acc_get(G, A_VTC + ks, dbl) + acc_get(G, A_VTLJ + ks, dbl) + acc_get(G, A_VTB + k, dbl) + acc_get(G, A_VTA + k, dbl) +
+                     acc_get(G, A_VTT + k, dbl) + acc_get(G, A_VT14 + k, dbl);
         }
     }
     if (a.ifspme && !a.ifnetqcorrp) {      // calforce.F90:1018-1050 (long group)
@@ -393,7 +395,7 @@ __global__ void k_press(const long long* __restrict__ acc, const DynState* __res
     }
     double b3 = (1.0 / dyn->box[0]) * (1.0 / dyn->box[1]) * (1.0 / dyn->box[2]);
     chain->pint = 1.0 / 3.0 * b3 * (K + W);
-    for (int k = 0; k < 9; ++k) chain->pintt[k] = 1.0 * b3 * (fixv(A, A_KET + k) + Wt[k]);
+    for (int k = 0; k < 9; ++k) chain->pintt[k] = 1.0 * b3 * (acc_get(A, A_KET + k, dbl) + Wt[k]);
 }
 
 template <bool MIXED>
@@ -459,7 +461,7 @@ pgk_status launch_kinetic(pgk_ctx* c, int group) {
     PGK_CUDA(c, cudaMemsetAsync(acc + A_KE, 0, sizeof(long long) * 10, c->st));
     int blocks = std::min(c->nsm * 2, (c->natom + 255) / 256);
     if (blocks < 1) blocks = 1;
-    k_kinetic<<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, acc);
+    k_kinetic<<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, acc, c->mixed() ? 0 : 1);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -469,6 +471,7 @@ pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md) {
     ChainArgs a;
     a.md = md;
     a.degfree = c->degfree;
+    a.dbl = c->mixed() ? 0 : 1;
     a.kind = kind;
     k_chain<<<1, 32, 0, c->st>>>(c->chain, c->acc, a);
     PGK_LAUNCHED(c);
@@ -515,6 +518,7 @@ pgk_status launch_press(pgk_ctx* c) {
     a.alpha = c->prm.alpha;
     a.ifspme = c->prm.ifspme;
     a.ifnetqcorrp = c->prm.ifnetqcorrp;
+    a.dbl = c->mixed() ? 0 : 1;
     k_press<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, a);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());

@@ -18,6 +18,8 @@
 //
 // Roofline: FP32 pipe (61 algorithmic flop per interacting pair) plus one
 // 4-byte index and one 16-byte (32-byte FP64) gather per list entry.
+#include <vector>
+
 #include "pgk_ctx.cuh"
 
 // ---- pack: sorted positions for the pair kernel -------------------------------
@@ -157,11 +159,11 @@ __global__ void __launch_bounds__(256, 2) k_pair_mixed(const int4* __restrict__ 
         if (VIR) {
             const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
                                  A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
-            block_acc<16>(v, a.acc, idx);
+            block_acc<16>(v, a.acc, idx, false);
         } else {
             double v2[2] = {v[0], v[1]};
             const int idx[2] = {A_VDW, A_ELC};
-            block_acc<2>(v2, a.acc, idx);
+            block_acc<2>(v2, a.acc, idx, false);
         }
     }
 }
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
                         0.5 * (vl[0] + vl[3] + vl[5])};
         const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
                              A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
-        block_acc<16>(v, a.acc, idx);
+        block_acc<16>(v, a.acc, idx, true);
     }
 }
 
@@ -341,7 +343,7 @@ __global__ void k_excl(const double* __restrict__ pos, const double* __restrict_
     if (want) {
         double v[8] = {-e, -e, t[0], t[1], t[2], t[3], t[4], t[5]};
         const int idx[8] = {A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
-        block_acc<8>(v, acc, idx);
+        block_acc<8>(v, acc, idx, !MIXED);
     }
 }
 
@@ -357,5 +359,44 @@ pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir) {
                                              c->hspl, c->dyn, c->facc[group], acc, ene || vir);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+// ---- diagnostic: number of unique pairs inside the interaction cutoff --------
+// (the algorithmic work unit of the pair kernel; run outside any timed region)
+__global__ void k_count_pairs(const double* __restrict__ pos_s, const int* __restrict__ nbr,
+                              const int* __restrict__ ncnt, int cap, int n, double rmax2,
+                              const DynState* __restrict__ dyn, unsigned long long* out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    unsigned long long c = 0;
+    const double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
+    for (int k = 0; k < ncnt[s]; ++k) {
+        int t = nbr[(size_t)s * cap + k];
+        if (t <= s) continue;
+        double dx = pos_s[3 * s] - pos_s[3 * t]; dx -= L0 * round(dx / L0);
+        double dy = pos_s[3 * s + 1] - pos_s[3 * t + 1]; dy -= L1 * round(dy / L1);
+        double dz = pos_s[3 * s + 2] - pos_s[3 * t + 2]; dz -= L2 * round(dz / L2);
+        if (dx * dx + dy * dy + dz * dz <= rmax2) ++c;
+    }
+    atomicAdd(out, c);
+}
+
+pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries) {
+    unsigned long long* d = c->counters + 2;
+    PGK_CUDA(c, cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->st));
+    double rr2 = c->prm.rrcut * c->prm.rrcut, rl2 = c->prm.rcut * c->prm.rcut;
+    k_count_pairs<<<(c->natom + 255) / 256, 256, 0, c->st>>>(c->pos_s, c->nbr, c->ncnt, c->cap, c->natom,
+                                                              rr2 > rl2 ? rr2 : rl2, c->dyn, d);
+    PGK_CUDA(c, cudaGetLastError());
+    unsigned long long h = 0;
+    PGK_CUDA(c, cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    std::vector<int> cnt(c->natom);
+    PGK_CUDA(c, cudaMemcpyAsync(cnt.data(), c->ncnt, sizeof(int) * c->natom, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    long long e = 0;
+    for (int v : cnt) e += v;
+    *npair = (long long)h;
+    *nentries = e;
     return PGK_OK;
 }

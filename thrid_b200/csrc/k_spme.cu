@@ -305,7 +305,7 @@ __global__ void k_scalar(typename C2<T>::t* __restrict__ q, int K1, int K2, int 
         double out[9] = {0.5 * en, 0.5 * en + 0.5 * vs, 0.5 * vs,
                          -0.5 * vt[0], -0.5 * vt[1], -0.5 * vt[2], -0.5 * vt[3], -0.5 * vt[4], -0.5 * vt[5]};
         const int idx[9] = {A_EWK, A_VC, A_VSCA, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
-        block_acc<9>(out, acc, idx);
+        block_acc<9>(out, acc, idx, sizeof(T) == 8);
     }
 }
 
@@ -530,4 +530,11 @@ pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir) {
     }
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
+}
+
+// single stages of launch_spme for pgk_bench_kernel (1 spread, 2 gather, 3 forward FFT)
+pgk_status spme_bench(pgk_ctx* c, int which) {
+    if (which == 1) return c->mixed() ? dispatch_sg<true>(c, false, 0) : dispatch_sg<false>(c, false, 0);
+    if (which == 2) return c->mixed() ? dispatch_sg<true>(c, true, 0) : dispatch_sg<false>(c, true, 0);
+    return c->mixed() ? fft3<float>(c, -1, false) : fft3<double>(c, -1, false);
 }

@@ -11,6 +11,7 @@
 #include "pgk_ctx.cuh"
 
 pgk_status launch_rkcut(pgk_ctx* c);
+pgk_status spme_bench(pgk_ctx* c, int which);
 
 pgk_status pgk_fail(pgk_ctx* c, pgk_status s, const std::string& msg) {
     if (c) c->err = msg;
@@ -88,7 +89,12 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir) {
     return launch_bonded(c, g, ene, vir, false);
 }
 
-double fixv(long long v) { return (double)v * PGK_FORCE_ISCALE; }
+double accv(const pgk_ctx* c, long long v) {
+    if (c->mixed()) return (double)v * PGK_FORCE_ISCALE;
+    double d;
+    memcpy(&d, &v, sizeof(d));
+    return d;
+}
 
 // energies / virials of the accumulators of the given groups
 pgk_status read_acc(pgk_ctx* c, int gmask, pgk_energies* e, pgk_virials* v, bool add_ewald_consts) {
@@ -99,7 +105,7 @@ pgk_status read_acc(pgk_ctx* c, int gmask, pgk_energies* e, pgk_virials* v, bool
     double S[NACC];
     for (int k = 0; k < NACC; ++k) {
         S[k] = 0;
-        for (int g = 0; g < 2; ++g) if (gmask & (1 << g)) S[k] += fixv(a[(size_t)g * NACC + k]);
+        for (int g = 0; g < 2; ++g) if (gmask & (1 << g)) S[k] += accv(c, a[(size_t)g * NACC + k]);
     }
     for (int base : {A_VTC, A_VTLJ}) { S[base + 3] = S[base + 1]; S[base + 6] = S[base + 2]; S[base + 7] = S[base + 5]; }
     double pi = std::acos(-1.0);
@@ -583,7 +589,7 @@ pgk_status pgk_calpress(pgk_ctx* c, double* kint, double* ptot, double* p9) {
     if (kint) {
         long long k;
         PGK_CUDA(c, cudaMemcpy(&k, c->acc + A_KE, sizeof(k), cudaMemcpyDeviceToHost));
-        *kint = fixv(k);
+        *kint = accv(c, k);
     }
     if (ptot) *ptot = ch.pint;
     if (p9) for (int k = 0; k < 9; ++k) p9[k] = ch.pintt[k];
@@ -597,6 +603,46 @@ pgk_status pgk_sync(pgk_ctx* c) {
 }
 
 int64_t pgk_kernel_launches(const pgk_ctx* c) { return c ? c->launches : 0; }
+
+pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms, double* units, double* entries) {
+    if (!c || iters < 1 || !ms) return PGK_E_INVALID;
+    pgk_status s;
+    if (!c->list_valid && (s = launch_mklist(c))) return s;
+    if ((s = launch_pack(c))) return s;
+    if (which == 0) {
+        long long np = 0, ne = 0;
+        if ((s = count_pairs(c, &np, &ne))) return s;
+        if (units) *units = (double)np;
+        if (entries) *entries = (double)ne;
+    } else if (units) {
+        *units = which == 3 ? (double)c->K[0] * c->K[1] * c->K[2] : (double)c->natom;
+    }
+    if (which >= 1 && !c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
+    cudaEvent_t e0, e1;
+    PGK_CUDA(c, cudaEventCreate(&e0));
+    PGK_CUDA(c, cudaEventCreate(&e1));
+    auto one = [&]() -> pgk_status {
+        switch (which) {
+            case 0: return launch_pair(c, 0, true, true);
+            case 1: return spme_bench(c, 1);
+            case 2: return spme_bench(c, 2);
+            case 3: return spme_bench(c, 3);
+            default: return pgk_fail(c, PGK_E_INVALID, "unknown kernel id");
+        }
+    };
+    if ((s = launch_zero_group(c, 0)) || (s = one())) return s;    // warm-up launch
+    PGK_CUDA(c, cudaEventRecord(e0, c->st));
+    for (int k = 0; k < iters; ++k)
+        if ((s = one())) return s;
+    PGK_CUDA(c, cudaEventRecord(e1, c->st));
+    PGK_CUDA(c, cudaEventSynchronize(e1));
+    float t = 0;
+    PGK_CUDA(c, cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = (double)t / iters;
+    return launch_zero_group(c, 0);
+}
 void* pgk_stream(const pgk_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 }  // extern "C"

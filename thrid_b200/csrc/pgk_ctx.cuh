@@ -123,6 +123,7 @@ pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_
 pgk_status launch_pack(pgk_ctx* c);
 pgk_status launch_pair(pgk_ctx* c, int group, bool ene, bool vir);
 pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir);
+pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries);
 
 // ---- launchers (k_spme.cu) ----
 pgk_status spme_setup(pgk_ctx* c);

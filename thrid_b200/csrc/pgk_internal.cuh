@@ -88,10 +88,21 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
+// Energy / virial / kinetic accumulators: int64 fixed point (2^32) in mixed
+// precision (order-independent, deterministic), IEEE double in FP64 precision
+// (the slot's 8 bytes hold a double).
+__device__ __forceinline__ void acc_add(long long* p, double x, bool dbl) {
+    if (dbl) atomicAdd((double*)p, x);
+    else acc_fix(p, x);
+}
+__device__ __forceinline__ double acc_get(const long long* acc, int k, bool dbl) {
+    return dbl ? __longlong_as_double(acc[k]) : (double)acc[k] * PGK_FORCE_ISCALE;
+}
+
 // Block reduction of NV doubles; thread 0 adds the block total into
-// acc[idx[k]] as fixed point.  blockDim.x must be a multiple of 32 (<=1024).
+// acc[idx[k]].  blockDim.x must be a multiple of 32 (<=1024).
 template <int NV>
-__device__ __forceinline__ void block_acc(double (&v)[NV], long long* acc, const int (&idx)[NV]) {
+__device__ __forceinline__ void block_acc(double (&v)[NV], long long* acc, const int (&idx)[NV], bool dbl) {
     __shared__ double red[32][NV];
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
@@ -106,7 +117,7 @@ __device__ __forceinline__ void block_acc(double (&v)[NV], long long* acc, const
         for (int k = 0; k < NV; ++k) {
             double x = lane < nw ? red[lane][k] : 0.0;
             x = warp_sum(x);
-            if (lane == 0 && x != 0.0) acc_fix(&acc[idx[k]], x);
+            if (lane == 0 && x != 0.0) acc_add(&acc[idx[k]], x, dbl);
         }
     }
 }

@@ -74,6 +74,7 @@ def lib():
     L.pgk_kernel_launches.argtypes = [vp]
     L.pgk_stream.restype = vp
     L.pgk_stream.argtypes = [vp]
+    L.pgk_bench_kernel.argtypes = [vp, C.c_int32, C.c_int32, pd, pd, pd]
     _lib = L
     return L
 

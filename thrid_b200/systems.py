@@ -68,6 +68,8 @@ LJ_TYPES = {
     "HC": (1.008, 2.50, 0.030),
     "OH": (15.999, 3.12, 0.170),
     "HO": (1.008, None, 0.0),
+    "IP": (22.99, None, 0.0),        # bare ions of the Madelung known-answer lattice
+    "IM": (35.45, None, 0.0),
 }
 
 
@@ -573,3 +575,31 @@ def small_box(kind="propanol", nside=3, spacing=5.2, seed=7, precision=PREC_FP64
     p = default_params((box, box, box), rcut=rc, rrcut=rc, alpha=3.2 / rc, nfft=(nfft, nfft, nfft),
                        pme_order=order, precision=precision)
     return build_system(f"{kind}_small", [(mol, nside ** 3)], (box, box, box), fn, seed + 2, 300.0, p)
+
+
+def ion_template(sign):
+    q = np.array([1.0 if sign > 0 else -1.0])
+    return Molecule("ion+" if sign > 0 else "ion-", ["IP" if sign > 0 else "IM"], q, np.zeros((1, 3)),
+                    [], [], [], [], [], (0, 0))
+
+
+def nacl_lattice(nside=8, a=2.82, alpha=None, nfft=32, order=6, rcut=None, precision=PREC_FP64):
+    """Rock-salt lattice of +-1 point charges (nearest-neighbour distance a);
+    the Ewald energy per ion pair is -M q^2/a with the Madelung constant
+    M = 1.747564594633 (known answer for the Ewald + SPME path)."""
+    L = nside * a
+    rc = L / 2.0 - 0.01 if rcut is None else rcut
+    al = 3.6 / rc if alpha is None else alpha
+    g = np.arange(nside)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    plus = pts[(pts.sum(axis=1) % 2) == 0] * a
+    minus = pts[(pts.sum(axis=1) % 2) == 1] * a
+    p = default_params((L, L, L), rcut=rc, rrcut=rc, alpha=al, nfft=(nfft, nfft, nfft), pme_order=order,
+                       rcut_book=rc + 0.005, precision=precision)
+    p["list_mode"] = 2
+    sysobj = build_system("nacl", [(ion_template(+1), len(plus)), (ion_template(-1), len(minus))], (L, L, L),
+                          lambda mol, m: (plus if mol.name == "ion+" else minus)[m][None, :] + 0.0,
+                          1, 0.0, p)
+    sysobj.atmvel[:] = 0.0
+    return sysobj
