@@ -159,7 +159,7 @@ def run_ours(args, rank, world, local_rank):
     launches = eng.kernel_launches - launches0
     ms_max = dist_max(ms, world)
     # ---- end to end through the public API with host buffers ----
-    e2e = e2e_leg(eng, s, md, step0 + args.steps, max(3, args.steps // 4), world)
+    e2e = None if args.no_e2e else e2e_leg(eng, s, md, step0 + args.steps, max(3, args.steps // 4), world)
     # ---- dominant kernel roofline (pair kernel), measured live ----
     roof = roofline(eng)
     eng.close()
@@ -178,7 +178,7 @@ def run_ours(args, rank, world, local_rank):
         "energies_last": {k: ene[k] for k in ("pot_tot", "pot_vdw", "pot_elc", "pot_ewk")} if ene else None,
     }
     out["clocks"] = clk.summary()
-    if rank == 0:
+    if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
 
@@ -306,6 +306,8 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_init()

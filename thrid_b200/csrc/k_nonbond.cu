@@ -68,7 +68,60 @@ struct PairArgs {
 };
 
 template <bool ENE, bool VIR>
-__global__ void __launch_bounds__(256, 2) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
+__device__ __forceinline__ void pair_term(const int4 pi, const float qi, const int ti, const int4 pj, const int tj,
+                                          const float sx, const float sy, const float sz, const float rmax2,
+                                          const float rr2, const float rl2, const float inv_h, const float h,
+                                          const float4* __restrict__ sf, const float4* __restrict__ sp,
+                                          const float2* __restrict__ slj, float& fx, float& fy, float& fz,
+                                          float& ev, float& ee, float* wc, float* wl) {
+    const float dx = (float)(pi.x - pj.x) * sx;
+    const float dy = (float)(pi.y - pj.y) * sy;
+    const float dz = (float)(pi.z - pj.z) * sz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (r2 > rmax2) return;
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    float fc = 0.f, fl = 0.f;
+    if (r2 <= rr2) {
+        const float r = r2 * rinv;
+        const float qq = qi * __int_as_float(pj.w);
+        const int idx = (int)(r * inv_h);
+        const float d = fmaf(-(float)idx, h, r);
+        const float4 c = sf[idx];
+        fc = qq * fmaf(d, fmaf(d, fmaf(d, c.w, c.z), c.y), c.x);
+        if (ENE || VIR) {
+            const float4 p = sp[idx];
+            ee = fmaf(qq, fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x), ee);
+        }
+    }
+    if (r2 <= rl2) {
+        const float2 lp = slj[ti + tj];
+        const float t2 = rinv2 * lp.x;
+        const float t6 = t2 * t2 * t2;
+        const float t12 = t6 * t6;
+        fl = 12.f * lp.y * (t12 - t6) * rinv2;
+        if (ENE || VIR) ev = fmaf(lp.y, t12 - 2.f * t6, ev);
+    }
+    const float fs = fc + fl;
+    fx = fmaf(fs, dx, fx);
+    fy = fmaf(fs, dy, fy);
+    fz = fmaf(fs, dz, fz);
+    if (VIR) {
+        const float cx = fc * dx, cy = fc * dy, cz = fc * dz;
+        wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
+        wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
+        const float lx = fl * dx, ly = fl * dy, lz = fl * dz;
+        wl[0] = fmaf(lx, dx, wl[0]); wl[1] = fmaf(lx, dy, wl[1]); wl[2] = fmaf(lx, dz, wl[2]);
+        wl[3] = fmaf(ly, dy, wl[3]); wl[4] = fmaf(ly, dz, wl[4]); wl[5] = fmaf(lz, dz, wl[5]);
+    }
+}
+
+// Each lane walks entries lane, lane+32, ... of the row; the next entry's
+// index, position and type are loaded before the current pair is evaluated
+// (two gathers in flight per lane).  Per-lane energy/virial sums stay in
+// FP32 registers across all atoms of the warp and are reduced once per block.
+template <bool ENE, bool VIR>
+__global__ void __launch_bounds__(256, 4) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
                                                        const float2* __restrict__ lj_g,
                                                        const float4* __restrict__ spl_g,
                                                        const DynState* __restrict__ dyn) {
@@ -90,72 +143,39 @@ __global__ void __launch_bounds__(256, 2) k_pair_mixed(const int4* __restrict__ 
     const float inv_h = (float)a.inv_h, h = (float)a.h;
     const int lane = threadIdx.x & 31;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    double e_vdw = 0, e_elc = 0, vc[6] = {0, 0, 0, 0, 0, 0}, vl[6] = {0, 0, 0, 0, 0, 0};
+    const int* __restrict__ typ_s = a.typ_s;
+    float ev = 0.f, ee = 0.f;
+    float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
     for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.n; s += nwarps) {
-        const int4 pi = xq[s];
+        const int4 pi = __ldg(xq + s);
         const float qi = __int_as_float(pi.w);
-        const int ti = a.typ_s[s] * a.ntyp;
-        const int cnt = a.ncnt[s];
-        const int* row = a.nbr + (size_t)s * a.cap;
+        const int ti = __ldg(typ_s + s) * a.ntyp;
+        const int cnt = __ldg(a.ncnt + s);
+        const int* __restrict__ row = a.nbr + (size_t)s * a.cap;
         float fx = 0.f, fy = 0.f, fz = 0.f;
-        float ev = 0.f, ee = 0.f;
-        float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
-        for (int k = lane; k < cnt; k += 32) {
-            const int j = __ldg(row + k);
-            const int4 pj = __ldg(xq + j);
-            const float dx = (float)(pi.x - pj.x) * sx;
-            const float dy = (float)(pi.y - pj.y) * sy;
-            const float dz = (float)(pi.z - pj.z) * sz;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > rmax2) continue;
-            const float rinv2 = __frcp_rn(r2);
-            float fc = 0.f, fl = 0.f;
-            if (r2 <= rr2) {
-                const float r = sqrtf(r2);
-                const float qq = qi * __int_as_float(pj.w);
-                const int idx = (int)(r * inv_h);
-                const float d = fmaf(-(float)idx, h, r);
-                const float4 c = sf[idx];
-                fc = qq * fmaf(d, fmaf(d, fmaf(d, c.w, c.z), c.y), c.x);
-                if (ENE || VIR) {
-                    const float4 p = sp[idx];
-                    ee += qq * fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x);
-                }
-            }
-            if (r2 <= rl2) {
-                const float2 lp = slj[ti + a.typ_s[j]];
-                const float t2 = rinv2 * lp.x;
-                const float t6 = t2 * t2 * t2;
-                const float t12 = t6 * t6;
-                fl = 12.f * lp.y * (t12 - t6) * rinv2;
-                if (ENE || VIR) ev += lp.y * (t12 - 2.f * t6);
-            }
-            const float fs = fc + fl;
-            fx = fmaf(fs, dx, fx);
-            fy = fmaf(fs, dy, fy);
-            fz = fmaf(fs, dz, fz);
-            if (VIR) {
-                wc[0] += fc * dx * dx; wc[1] += fc * dx * dy; wc[2] += fc * dx * dz;
-                wc[3] += fc * dy * dy; wc[4] += fc * dy * dz; wc[5] += fc * dz * dz;
-                wl[0] += fl * dx * dx; wl[1] += fl * dx * dy; wl[2] += fl * dx * dz;
-                wl[3] += fl * dy * dy; wl[4] += fl * dy * dz; wl[5] += fl * dz * dz;
-            }
+        int k = lane;
+        int j = k < cnt ? __ldg(row + k) : s;
+        int4 pj = __ldg(xq + j);
+        int tj = __ldg(typ_s + j);
+        while (k < cnt) {
+            const int kn = k + 32;
+            const int jn = kn < cnt ? __ldg(row + kn) : s;
+            const int4 pjn = __ldg(xq + jn);
+            const int tjn = __ldg(typ_s + jn);
+            pair_term<ENE, VIR>(pi, qi, ti, pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h, sf, sp, slj,
+                                fx, fy, fz, ev, ee, wc, wl);
+            k = kn; pj = pjn; tj = tjn;
         }
         fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
         if (lane == 0) force_add<true>(a.facc, a.perm[s], (double)fx, (double)fy, (double)fz);
-        if (ENE || VIR) { e_vdw += (double)ev; e_elc += (double)ee; }
-        if (VIR) {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) { vc[q] += (double)wc[q]; vl[q] += (double)wl[q]; }
-        }
     }
     if (ENE || VIR) {
         // pairs were counted from both sides: factor 1/2.  Tensor (a,b) -> 3*b + a.
-        double v[16] = {0.5 * e_vdw, 0.5 * e_elc, 0.5 * e_elc,
-                        0.5 * vc[0], 0.5 * vc[1], 0.5 * vc[2], 0.5 * vc[3], 0.5 * vc[4], 0.5 * vc[5],
-                        0.5 * vl[0], 0.5 * vl[1], 0.5 * vl[2], 0.5 * vl[3], 0.5 * vl[4], 0.5 * vl[5],
-                        0.5 * (vl[0] + vl[3] + vl[5])};
+        double v[16] = {0.5 * ev, 0.5 * ee, 0.5 * ee,
+                        0.5 * wc[0], 0.5 * wc[1], 0.5 * wc[2], 0.5 * wc[3], 0.5 * wc[4], 0.5 * wc[5],
+                        0.5 * wl[0], 0.5 * wl[1], 0.5 * wl[2], 0.5 * wl[3], 0.5 * wl[4], 0.5 * wl[5],
+                        0.5 * ((double)wl[0] + (double)wl[3] + (double)wl[5])};
         if (VIR) {
             const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
                                  A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
