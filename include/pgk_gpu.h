@@ -43,6 +43,7 @@ typedef int32_t pgk_status;
 #define PGK_E_NOMEM            8  /* device allocation failed */
 #define PGK_E_UNSUPPORTED      9  /* option of the reference that this engine does not build */
 #define PGK_E_RATTLEV_NOCONV  10  /* rattle_mtk.F90 "RATTLE(V) failed to converge" */
+#define PGK_E_SCRATCH_LIMIT   11  /* size beyond the static scratch of pgk_fft_pme_noalloc */
 
 /* ---- option values ------------------------------------------------------- */
 #define PGK_PREC_FP64   0   /* all-FP64 device path (parity path) */
@@ -278,6 +279,29 @@ void* pgk_stream(const pgk_ctx* ctx);
  * full-list entries the pair kernel reads. */
 pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
                             double* entries);
+
+/* Allocation-free SPME reciprocal force.  No counterpart in the reference.
+ * For callers that must not allocate device memory during a run -- a host
+ * driver or a replica server that reserves all of HBM up front, where
+ * cudaMalloc/cudaFree would synchronise the device and could fail -- this
+ * entry point computes fft_pmep's force on caller-owned device buffers and
+ * allocates nothing: its temporaries live in one fixed static device array
+ * (about 6.3 MB, held by every GPU that loads the library until exit).
+ *   d_atmcor  (3,natom) device positions, d_atmchrg (natom) device charges
+ *             (scaled as in prepmd.F90), box = host xcel,ycel,zcel;
+ *   d_force   (3,natom) device forces, the reciprocal force is ADDED;
+ *   pot_ewk   host pointer for the reciprocal energy (NULL = not needed;
+ *             when given, the call waits for its stream);
+ *   stream    cudaStream_t as void* (NULL = default stream).
+ * Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256 and a product of 2, 3
+ * and 5, 3 <= pme_order <= 8; larger sizes return PGK_E_SCRATCH_LIMIT.
+ * The first call on a device looks up the array's address on that device;
+ * make it before any stream capture.  All calls share the array and keep its
+ * last contents: calls that overlap on the GPU race, so serialise them. */
+pgk_status pgk_fft_pme_noalloc(const double* d_atmcor, const double* d_atmchrg, int32_t natom,
+                               const double* box, double alpha, int32_t nfft1, int32_t nfft2,
+                               int32_t nfft3, int32_t pme_order, double* d_force, double* pot_ewk,
+                               void* stream);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@ PGK_E_INVALID = 7
 PGK_E_NOMEM = 8
 PGK_E_UNSUPPORTED = 9
 PGK_E_RATTLEV_NOCONV = 10
+PGK_E_SCRATCH_LIMIT = 11
 
 PREC_FP64, PREC_MIXED = 0, 1
 MTS_LONG, MTS_SHORT, MTS_NONE = 1, 3, 0

@@ -538,3 +538,195 @@ pgk_status spme_bench(pgk_ctx* c, int which) {
     if (which == 2) return c->mixed() ? dispatch_sg<true>(c, true, 0) : dispatch_sg<false>(c, true, 0);
     return c->mixed() ? fft3<float>(c, -1, false) : fft3<double>(c, -1, false);
 }
+
+// ============================================================================
+// Allocation-free SPME reciprocal force: pgk_fft_pme_noalloc.
+//
+// For callers that cannot call cudaMalloc during a run: a host driver or a
+// serving process that reserves all device memory up front (cudaMalloc and
+// cudaFree synchronise the whole device and can fail once a pool owns the
+// HBM), so per-call allocation would stall other streams or break the
+// memory budget.  The caller passes device buffers for the inputs and the
+// output; every temporary of the computation lives in the file-scope array
+// below, of fixed size, which every GPU that loads this library holds until
+// the process exits.
+//
+// Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256 and a product of 2, 3
+// and 5, 3 <= pme_order <= 8.  Larger sizes return PGK_E_SCRATCH_LIMIT.
+// The first call on a device looks up the array's device address there
+// (cudaGetSymbolAddress); make that first call before any stream capture.
+// All calls share the one array: calls that overlap on the GPU (two streams,
+// two host threads) race on it and must be serialised by the caller.
+// FP64 arithmetic (the device parity path); forces are ADDED to d_force.
+// ============================================================================
+#define NOALLOC_MAX_GRID (64 * 64 * 64)
+#define NOALLOC_MAX_N 256
+#define NOALLOC_OFF_DYN 0
+#define NOALLOC_OFF_ACC 1024
+#define NOALLOC_OFF_BSP (NOALLOC_OFF_ACC + 2048)
+#define NOALLOC_OFF_TW (NOALLOC_OFF_BSP + 3 * NOALLOC_MAX_N * 8)
+#define NOALLOC_OFF_QACC (NOALLOC_OFF_TW + 3 * NOALLOC_MAX_N * 16)
+#define NOALLOC_OFF_QC (NOALLOC_OFF_QACC + NOALLOC_MAX_GRID * 8)
+#define NOALLOC_BYTES (NOALLOC_OFF_QC + NOALLOC_MAX_GRID * 16)
+static_assert(sizeof(DynState) <= NOALLOC_OFF_ACC, "DynState slot");
+static_assert(NACC * 8 <= NOALLOC_OFF_BSP - NOALLOC_OFF_ACC, "accumulator slot");
+static_assert(NOALLOC_OFF_QACC % 256 == 0 && NOALLOC_OFF_QC % 256 == 0, "alignment");
+
+static __device__ __align__(256) unsigned char g_spme_scratch[NOALLOC_BYTES];
+
+#define NOALLOC_MAX_DEVICES 64
+static unsigned char* g_scratch_ptr[NOALLOC_MAX_DEVICES];   // device address of g_spme_scratch, per device
+static int g_scratch_key[NOALLOC_MAX_DEVICES][4];           // (K1, K2, K3, order) of the tables in place
+
+// twiddles exp(-2 pi i m / n) per axis and the B-spline moduli (DFTMOD,
+// fft_pme_init.F90:263-289), written into the scratch array
+__global__ void k_noalloc_tables(unsigned char* base, int K1, int K2, int K3, int order) {
+    double* bsp = (double*)(base + NOALLOC_OFF_BSP);
+    double2* tw = (double2*)(base + NOALLOC_OFF_TW);
+    const int Kd[3] = {K1, K2, K3};
+    double arr[8], darr[8];
+    switch (order) {
+        case 3: fill_bspline_d<double, 3>(0.0, arr, darr); break;
+        case 4: fill_bspline_d<double, 4>(0.0, arr, darr); break;
+        case 5: fill_bspline_d<double, 5>(0.0, arr, darr); break;
+        case 6: fill_bspline_d<double, 6>(0.0, arr, darr); break;
+        case 7: fill_bspline_d<double, 7>(0.0, arr, darr); break;
+        default: fill_bspline_d<double, 8>(0.0, arr, darr); break;
+    }
+    int off = 0;
+    for (int d = 0; d < 3; ++d) {
+        int n = Kd[d];
+        for (int m = threadIdx.x; m < n; m += blockDim.x) {
+            double s, c;
+            sincospi(-2.0 * (double)m / (double)n, &s, &c);
+            tw[d * NOALLOC_MAX_N + m] = make_double2(c, s);
+            double s1 = 0.0, s2 = 0.0;
+            for (int j = 1; j <= order && j < n; ++j) {   // bsp_arr(j+1) = array(j)
+                double sn, cs;
+                sincospi(2.0 * (double)(((long long)m * j) % n) / (double)n, &sn, &cs);
+                s1 += arr[j - 1] * cs;
+                s2 += arr[j - 1] * sn;
+            }
+            bsp[off + m] = s1 * s1 + s2 * s2;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 1; k < n - 1; ++k)
+                if (bsp[off + k] < 1.0e-7) bsp[off + k] = 0.5 * (bsp[off + k - 1] + bsp[off + k + 1]);
+        __syncthreads();
+        off += n;
+    }
+}
+
+__global__ void k_noalloc_dyn(DynState* d, double b0, double b1, double b2, double rk) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        d->box[0] = b0; d->box[1] = b1; d->box[2] = b2;
+        d->boxinv[0] = 1.0 / b0; d->boxinv[1] = 1.0 / b1; d->boxinv[2] = 1.0 / b2;
+        d->rkcut = rk;
+    }
+}
+
+template <int AXIS, int SRC>
+static cudaError_t noalloc_fft_pass(unsigned char* base, const FftPlan& pl, int K1, int K2, int K3, int sign,
+                                    cudaStream_t st) {
+    FftDev fd;
+    fd.n = pl.n; fd.nstage = pl.nstage;
+    for (int s = 0; s < PGK_MAX_RADIX_STAGES; ++s) fd.radix[s] = pl.radix[s];
+    fd.tw = base + NOALLOC_OFF_TW + (size_t)AXIS * NOALLOC_MAX_N * 16;
+    int P = 8;
+    if (AXIS == 0) P = std::max(1, 1024 / K1);
+    int grid = AXIS == 0 ? (K2 * K3 + P - 1) / P : ((K1 + P - 1) / P) * (AXIS == 1 ? K3 : K2);
+    size_t sm = (size_t)2 * P * pl.n * sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(k_fft<double, AXIS, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_fft<double, AXIS, SRC><<<grid, 256, sm, st>>>((double2*)(base + NOALLOC_OFF_QC), base + NOALLOC_OFF_QACC,
+                                                    K1, K2, K3, fd, P, (double)sign);
+    return cudaGetLastError();
+}
+
+template <int P>
+static void noalloc_sg(unsigned char* base, const double* pos, const double* chrg, int n, int K1, int K2, int K3,
+                       double* force, bool gather, cudaStream_t st) {
+    const DynState* dyn = (const DynState*)(base + NOALLOC_OFF_DYN);
+    if (!gather)
+        k_spread<false, P><<<(n + 127) / 128, 128, 0, st>>>(pos, chrg, n, dyn, K1, K2, K3, base + NOALLOC_OFF_QACC);
+    else
+        k_gather<false, P><<<(n + 127) / 128, 128, 0, st>>>(pos, chrg, n, dyn, K1, K2, K3, base + NOALLOC_OFF_QC,
+                                                            force);
+}
+
+static void noalloc_sg_order(int order, unsigned char* base, const double* pos, const double* chrg, int n, int K1,
+                             int K2, int K3, double* force, bool gather, cudaStream_t st) {
+    switch (order) {
+        case 3: noalloc_sg<3>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+        case 4: noalloc_sg<4>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+        case 5: noalloc_sg<5>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+        case 6: noalloc_sg<6>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+        case 7: noalloc_sg<7>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+        default: noalloc_sg<8>(base, pos, chrg, n, K1, K2, K3, force, gather, st); break;
+    }
+}
+
+extern "C" pgk_status pgk_fft_pme_noalloc(const double* d_atmcor, const double* d_atmchrg, int32_t natom,
+                                          const double* box, double alpha, int32_t nfft1, int32_t nfft2,
+                                          int32_t nfft3, int32_t pme_order, double* d_force, double* pot_ewk,
+                                          void* stream) {
+    if (!d_atmcor || !d_atmchrg || !d_force || !box || natom < 1 || alpha <= 0.0) return PGK_E_INVALID;
+    if (nfft1 < 2 || nfft2 < 2 || nfft3 < 2 || nfft1 > NOALLOC_MAX_N || nfft2 > NOALLOC_MAX_N ||
+        nfft3 > NOALLOC_MAX_N || (long long)nfft1 * nfft2 * nfft3 > NOALLOC_MAX_GRID || pme_order < 3 ||
+        pme_order > 8)
+        return PGK_E_SCRATCH_LIMIT;
+    FftPlan pl[3];
+    const int Kd[3] = {nfft1, nfft2, nfft3};
+    for (int d = 0; d < 3; ++d)
+        if (!factor(Kd[d], pl[d])) return PGK_E_SCRATCH_LIMIT;
+    cudaStream_t st = (cudaStream_t)stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PGK_E_CUDA;
+    if (!g_scratch_ptr[dev]) {   // once per device, with that device current
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_spme_scratch) != cudaSuccess || !p) return PGK_E_CUDA;
+        g_scratch_ptr[dev] = (unsigned char*)p;
+        g_scratch_key[dev][0] = 0;
+    }
+    unsigned char* base = g_scratch_ptr[dev];
+    int* key = g_scratch_key[dev];
+    if (key[0] != nfft1 || key[1] != nfft2 || key[2] != nfft3 || key[3] != pme_order) {
+        k_noalloc_tables<<<1, 256, 0, st>>>(base, nfft1, nfft2, nfft3, pme_order);
+        if (cudaGetLastError() != cudaSuccess) return PGK_E_CUDA;
+        key[0] = nfft1; key[1] = nfft2; key[2] = nfft3; key[3] = pme_order;
+    }
+    // erf_corr_cutoff.F90:28-62 (min-ish rule of the reference)
+    double m1 = 0.5 * (nfft1 / box[0]), rk = m1, m2 = 0.5 * (nfft2 / box[1]), m3 = 0.5 * (nfft3 / box[2]);
+    if (m2 < m1) rk = m2;
+    if (m3 < m2) rk = m3;
+    k_noalloc_dyn<<<1, 32, 0, st>>>((DynState*)(base + NOALLOC_OFF_DYN), box[0], box[1], box[2], 0.9 * rk);
+    // the grid accumulates and the energy slots sum: both start at zero
+    size_t KK = (size_t)nfft1 * nfft2 * nfft3;
+    if (cudaMemsetAsync(base + NOALLOC_OFF_QACC, 0, KK * 8, st) != cudaSuccess) return PGK_E_CUDA;
+    if (cudaMemsetAsync(base + NOALLOC_OFF_ACC, 0, NACC * 8, st) != cudaSuccess) return PGK_E_CUDA;
+    noalloc_sg_order(pme_order, base, d_atmcor, d_atmchrg, natom, nfft1, nfft2, nfft3, d_force, false, st);
+    if (noalloc_fft_pass<0, 2>(base, pl[0], nfft1, nfft2, nfft3, -1, st) != cudaSuccess ||
+        noalloc_fft_pass<1, 0>(base, pl[1], nfft1, nfft2, nfft3, -1, st) != cudaSuccess ||
+        noalloc_fft_pass<2, 0>(base, pl[2], nfft1, nfft2, nfft3, -1, st) != cudaSuccess)
+        return PGK_E_CUDA;
+    k_scalar<double><<<148 * 2, 256, 0, st>>>((double2*)(base + NOALLOC_OFF_QC), nfft1, nfft2, nfft3,
+                                              (const double*)(base + NOALLOC_OFF_BSP),
+                                              (const DynState*)(base + NOALLOC_OFF_DYN), alpha, 0.0, 0,
+                                              (long long*)(base + NOALLOC_OFF_ACC), 1);
+    if (noalloc_fft_pass<0, 0>(base, pl[0], nfft1, nfft2, nfft3, +1, st) != cudaSuccess ||
+        noalloc_fft_pass<1, 0>(base, pl[1], nfft1, nfft2, nfft3, +1, st) != cudaSuccess ||
+        noalloc_fft_pass<2, 0>(base, pl[2], nfft1, nfft2, nfft3, +1, st) != cudaSuccess)
+        return PGK_E_CUDA;
+    noalloc_sg_order(pme_order, base, d_atmcor, d_atmchrg, natom, nfft1, nfft2, nfft3, d_force, true, st);
+    if (cudaGetLastError() != cudaSuccess) return PGK_E_CUDA;
+    if (pot_ewk) {
+        double e_ewk = 0.0;
+        if (cudaMemcpyAsync(&e_ewk, base + NOALLOC_OFF_ACC + A_EWK * 8, sizeof(double), cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return PGK_E_CUDA;
+        *pot_ewk = e_ewk;
+    }
+    return PGK_OK;
+}

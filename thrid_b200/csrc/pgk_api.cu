@@ -182,6 +182,7 @@ const char* pgk_status_string(pgk_status s) {
         case PGK_E_NOMEM: return "device memory exhausted";
         case PGK_E_UNSUPPORTED: return "unsupported option";
         case PGK_E_RATTLEV_NOCONV: return "ERROR: RATTLE(V) failed to converge within MAXITER";
+        case PGK_E_SCRATCH_LIMIT: return "size exceeds the static scratch maximum of pgk_fft_pme_noalloc";
         default: return "unknown status";
     }
 }
