@@ -180,6 +180,55 @@ typedef struct pgk_chain {
     double pint, pintt[9];
 } pgk_chain;
 
+/* ---- heat flux and region Langevin thermostat ----------------------------
+ * moldyn_hf.F90 (NVE-RESPA driver of the -DHF build), calforce_hf.F90,
+ * ewaldr_hf.F90, cal{bond,angl,tors,torsrb,non14}_hf.F90, calvirihf.F90,
+ * calheatf.F90, calcom.F90, langevin_regist.F90, langevin_region.F90.
+ * Built: the local volume-based Irving-Kirkpatrick flux (ifhfvol), z
+ * direction only (the default build: no _HF_ALL_DIR / _HF_BULK), bare 1/r
+ * Coulomb in the pair virial (the default of ewaldr_hf.F90:336), atom- or
+ * molecule-based positions per atom (hftyp_atm), streaming velocity zero. */
+#define PGK_HF_MAX_REGIONS  32
+#define PGK_LT_MAX_REGIONS   8
+#define PGK_HFTYP_ATOM       1   /* md_global.F90:112 HFTYP_ATOM */
+#define PGK_HFTYP_MOLE       2   /* md_global.F90:113 HFTYP_MOLE */
+#define PGK_HF_NCOL         18   /* values per region in a heat-flux record */
+/* Per-atom categories of calheatf (pot_*_atm / viri*_atm arrays). */
+#define PGK_HF_BO    0   /* bonds            pot_bo_atm,   viribot_atm   */
+#define PGK_HF_AN    1   /* angles           pot_an_atm,   viriant_atm   */
+#define PGK_HF_TO    2   /* torsions (+ RB)  pot_to_atm,   viritot_atm   */
+#define PGK_HF_14    3   /* 1-4 pairs        pot_14_atm,   viri14t_atm   */
+#define PGK_HF_ELIN  4   /* intramolecular Coulomb  pot_elin_atm, virielint_atm */
+#define PGK_HF_LJIN  5   /* intramolecular LJ       pot_ljin_atm, viriljint_atm */
+#define PGK_HF_ELC   6   /* intermolecular Coulomb  pot_elc_atm,  virielct_atm  */
+#define PGK_HF_VDW   7   /* intermolecular LJ       pot_vdw_atm,  viriljt_atm   */
+/* A heat-flux record holds, for each region r, PGK_HF_NCOL z components in
+ * the order of calheatf.F90's output arrays, each divided by the region
+ * volume (calheatf.F90:1330-1460):
+ *   [r*18 + 0]      hfkin_atm(3,r)
+ *   [r*18 + 1..8]   hfpot{bo,an,to,14,elin,ljin,elc,lj}_atm(3,r)
+ *   [r*18 + 9..16]  hfviri{bo,an,to,14,elin,ljin,elc,lj}_atm(3,r)
+ *   [r*18 + 17]     hftot_atm(3,r) */
+typedef struct pgk_hfparams {
+    int32_t nhfregion;            /* heat-flux z slabs (<= PGK_HF_MAX_REGIONS)  */
+    int32_t ifhfvol;              /* must be 1: local volume-based method       */
+    int32_t heatfinterval;        /* flux on steps with mod(step, n) == 1, or n == 1 */
+    int32_t nlangeregion;         /* Langevin regions (<= 8); 0 = no thermostat */
+    double  hfzpos1[PGK_HF_MAX_REGIONS], hfzpos2[PGK_HF_MAX_REGIONS];
+    const int32_t* hftyp_atm;     /* [natom] PGK_HFTYP_*; NULL = all atom-based */
+    const int32_t* lt_mole_based; /* [nmole] 1: register the molecule by its centre of
+                                     mass (water, and poly without iftcratom); 0: per
+                                     atom (langevin_regist.F90:86-360); NULL = all 0 */
+    double  ltxpos1[PGK_LT_MAX_REGIONS], ltxpos2[PGK_LT_MAX_REGIONS];
+    double  ltypos1[PGK_LT_MAX_REGIONS], ltypos2[PGK_LT_MAX_REGIONS];
+    double  ltzpos1[PGK_LT_MAX_REGIONS], ltzpos2[PGK_LT_MAX_REGIONS];
+    double  r_ltemp[PGK_LT_MAX_REGIONS];   /* reduced temperature (T / tempref)     */
+    double  r_ltdamp[PGK_LT_MAX_REGIONS];  /* reduced damping rate (gamma * timeref) */
+    uint64_t seed;                /* key of the counter-based random stream     */
+    int32_t ifoutthc;             /* tally det_ene_kin per Langevin region      */
+    int32_t _pad;
+} pgk_hfparams;
+
 /* ---- lifetime ------------------------------------------------------------ */
 /* Library version string. */
 const char* pgk_version(void);
@@ -254,6 +303,37 @@ pgk_status pgk_moldyn_nhc(pgk_ctx* ctx, int64_t inistep, int64_t endstep,
                           const pgk_mdparams* md, pgk_energies* ene);
 pgk_status pgk_moldyn_mtk(pgk_ctx* ctx, int64_t inistep, int64_t endstep,
                           const pgk_mdparams* md, pgk_energies* ene);
+
+/* Heat-flux regions, their atom/molecule typing and the region Langevin
+ * thermostat (preheatf.F90, rdlangevin.F90 settings); replaces any earlier
+ * setting.  Atom registration for the thermostat happens here once
+ * (langevin_regist at current_step 0 of moldyn_hf.F90:1425-1440). */
+pgk_status pgk_set_hf(pgk_ctx* ctx, const pgk_hfparams* hf);
+
+/* moldyn_hf.F90:1405-2480: NVE XO-RESPA with the region Langevin half steps
+ * (langevin_region former half before the RESPA loop, re-registration and
+ * latter half after it) and, on heat-flux steps (mod(step, heatfinterval) == 1
+ * or heatfinterval == 1, step > 0), calforce_hf + calheatf.  Each heat-flux
+ * step appends one record of nhfregion * PGK_HF_NCOL doubles to hf_out (at
+ * most cap_records; *nrecords returns the count, which may exceed the
+ * capacity).  hf_out may be NULL. */
+pgk_status pgk_moldyn_hf(pgk_ctx* ctx, int64_t inistep, int64_t endstep, const pgk_mdparams* md,
+                         pgk_energies* ene, double* hf_out, int64_t cap_records, int64_t* nrecords);
+
+/* calcom + the per-atom heat-flux quantities of calforce_hf (ewaldrp_hf and
+ * the *_hf bonded routines, calvirihf) at the current positions, then
+ * calheatf with the current velocities: one record of nhfregion * 18. */
+pgk_status pgk_calheatf(pgk_ctx* ctx, double* hf);
+
+/* Per-atom arrays of the last heat-flux evaluation: pot_atm[c*natom + i]
+ * (category c = PGK_HF_*, both MTS groups summed) and the z column of the
+ * per-atom virial, viri_atm[((c*nhfregion + r)*3 + a)*natom + i] =
+ * viri*_atm(a,3,i,r).  Either pointer may be NULL. */
+pgk_status pgk_get_hf_atm(pgk_ctx* ctx, double* pot_atm, double* viri_atm);
+
+/* det_ene_kin of langevin_region.F90 (kinetic energy put in (+) or taken out
+ * (-) per Langevin region) summed since the last call, then reset. */
+pgk_status pgk_langevin_dekin(pgk_ctx* ctx, double* det_ene_kin);
 
 /* Kinetic energy sum(m v^2) and atomic pressure tensor (calpress.F90, atomic
  * branch) of the current device state; press9 may be NULL. */

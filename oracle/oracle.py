@@ -65,6 +65,14 @@ def lib():
         L.orc_fft1d.argtypes = [pd, C.c_int, C.c_int]
         L.orc_moldyn.argtypes = [vp, C.c_int, C.c_longlong, C.c_longlong, C.POINTER(abi.MdParamsStruct),
                                  C.POINTER(abi.EnergiesStruct)]
+        L.orc_set_hf.argtypes = [vp, C.POINTER(abi.HfParamsStruct)]
+        L.orc_calheatf.argtypes = [vp, pd]
+        L.orc_get_hf_atm.argtypes = [vp, pd, pd]
+        L.orc_moldyn_hf.argtypes = [vp, C.c_longlong, C.c_longlong, C.POINTER(abi.MdParamsStruct),
+                                    C.POINTER(abi.EnergiesStruct), pd, C.c_longlong, i64p]
+        L.orc_langevin_dekin.argtypes = [vp, pd]
+        L.orc_lt_regions.argtypes = [vp, pi]
+        L.orc_philox.argtypes = [C.c_uint64, C.c_longlong, C.c_int, pd]
         _lib = L
     return _lib
 
@@ -163,6 +171,43 @@ class Oracle:
         st = self.L.orc_moldyn(self.h, kind, ini, end, C.byref(md), C.byref(e))
         return st, e.as_dict()
 
+    # ---- heat flux + region Langevin ----
+    def set_hf(self, hfd):
+        self._hf = abi.CHfParams(hfd)
+        st = self.L.orc_set_hf(self.h, C.byref(self._hf.struct))
+        if st:
+            raise RuntimeError(f"orc_set_hf status {st}")
+
+    def calheatf(self):
+        out = np.zeros((self._hf.nreg, abi.HF_NCOL))
+        st = self.L.orc_calheatf(self.h, _p(out))
+        if st:
+            raise RuntimeError(f"orc_calheatf status {st}")
+        return out
+
+    def hf_atm(self):
+        n = self.sys.natom
+        pot = np.zeros((8, n)); W = np.zeros((8, self._hf.nreg, 3, n))
+        self.L.orc_get_hf_atm(self.h, _p(pot), _p(W))
+        return pot, W
+
+    def moldyn_hf(self, ini, end, md, cap=100000):
+        e = abi.EnergiesStruct()
+        rec = np.zeros((max(cap, 1), max(self._hf.nreg, 1), abi.HF_NCOL))
+        nr = C.c_longlong(0)
+        st = self.L.orc_moldyn_hf(self.h, ini, end, C.byref(md), C.byref(e), _p(rec), cap, C.byref(nr))
+        return st, e.as_dict(), rec[:min(nr.value, cap)]
+
+    def langevin_dekin(self):
+        out = np.zeros(abi.LT_MAX_REGIONS)
+        self.L.orc_langevin_dekin(self.h, _p(out))
+        return out[:self._hf.nlt]
+
+    def lt_regions(self):
+        out = np.zeros(self.sys.natom, np.int32)
+        self.L.orc_lt_regions(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)))
+        return out
+
     def spline(self, k, x):
         return self.L.orc_spline(self.h, k, x)
 
@@ -187,6 +232,12 @@ def fill_bspline(w, order):
     a = np.zeros(order); d = np.zeros(order)
     lib().orc_fill_bspline(w, order, _p(a), _p(d))
     return a, d
+
+
+def philox_uniforms(seed, step, atom):
+    u = np.zeros(4)
+    lib().orc_philox(seed, step, atom, _p(u))
+    return u
 
 
 def fft1d(x, sign):

@@ -136,6 +136,21 @@ struct Oracle {
     double yratio = 1, zratio = 1;
     int status = 0;
     Forces F;
+    // heat flux + region Langevin (moldyn_hf.F90 state)
+    struct HF {
+        bool set = false;
+        int nreg = 0, heatfinterval = 1, nlt = 0, ifoutthc = 0;
+        double z1[PGK_HF_MAX_REGIONS], z2[PGK_HF_MAX_REGIONS];
+        std::vector<int> hftyp, molof, ltmole;
+        std::vector<double> molecom, molevel;
+        std::vector<double> pot;   // [8][natom]
+        std::vector<double> W;     // [8][nreg][3][natom]: viri*_atm(a,3,i,r)
+        double lx1[8], lx2[8], ly1[8], ly2[8], lz1[8], lz2[8], ltemp[8], ldamp[8];
+        uint64_t seed = 0;
+        std::vector<int> ltreg;    // Langevin region of each atom (-1: none)
+        std::vector<double> frand; // 3N accelerations of the former half
+        double dekin[8];
+    } hf;
 };
 
 // ---- spline_interp.F90:139-190 cal_spl_coeff ----
@@ -1240,6 +1255,544 @@ int moldyn(Oracle& o, int kind, long long ini, long long end, const pgk_mdparams
     return PGK_OK;
 }
 
+
+// ============================================================================
+// Heat flux of the -DHF build (volume-based IK, z direction) and the region
+// Langevin thermostat.  The force routines above are unchanged; on a heat-
+// flux step these restatements add the per-atom quantities that
+// ewaldrp_hf / cal*p_hf compute next to the same forces.
+// ============================================================================
+enum { HF_BO = 0, HF_AN, HF_TO, HF_14, HF_ELIN, HF_LJIN, HF_ELC, HF_VDW };
+
+inline double wrap1(double x, double L) {   // the single-shift P.B.C. of calcom / calvirihf / calheatf
+    if (x < 0.0) return x + L;
+    if (x >= L) return x - L;
+    return x;
+}
+inline size_t widx(const Oracle& o, int cat, int r, int a, int i) {
+    return (((size_t)cat * o.hf.nreg + r) * 3 + a) * o.natom + i;
+}
+
+// calcom.F90: molecule centres of mass from atmcor (monatomic molecules take
+// the atom position), then wrapped once per axis
+void calcom(Oracle& o, const std::vector<double>& x, std::vector<double>& out) {
+    int nm = (int)o.molidx.size() - 1;
+    out.assign((size_t)3 * nm, 0.0);
+    for (int m = 0; m < nm; ++m) {
+        int b = o.molidx[m], e = o.molidx[m + 1];
+        if (e - b == 1) {
+            int i = o.mollist[b];
+            for (int d = 0; d < 3; ++d) out[3 * m + d] = x[3 * i + d];
+        } else {
+            double mass = 0.0, c[3] = {0, 0, 0};
+            for (int q = b; q < e; ++q) {
+                int i = o.mollist[q];
+                mass = mass + o.atmmass[i];
+                for (int d = 0; d < 3; ++d) c[d] = c[d] + o.atmmass[i] * x[3 * i + d];
+            }
+            double inv = 1.0 / mass;
+            for (int d = 0; d < 3; ++d) out[3 * m + d] = c[d] * inv;
+        }
+        for (int d = 0; d < 3; ++d) out[3 * m + d] = wrap1(out[3 * m + d], o.box[d]);
+    }
+}
+
+// calvirihf.F90:8-405, local volume-based branch without _HF_ALL_DIR/_HF_BULK:
+// viri(:,3,i,r) += fi * f, viri(:,3,j,r) += -fj * f, f = +-(z length of the
+// i-j segment inside slab r) * nbodycoeff
+void calvirihf(Oracle& o, int i, int j, const double* fi, const double* fj, double nbc, int cat) {
+    Oracle::HF& h = o.hf;
+    int atomflag = 0;
+    double zi, zj;
+    if (h.hftyp[i] == PGK_HFTYP_MOLE) zi = h.molecom[3 * h.molof[i] + 2];
+    else { ++atomflag; zi = wrap1(o.atmcor[3 * i + 2], o.box[2]); }
+    if (h.hftyp[j] == PGK_HFTYP_MOLE) zj = h.molecom[3 * h.molof[j] + 2];
+    else { ++atomflag; zj = wrap1(o.atmcor[3 * j + 2], o.box[2]); }
+    if (atomflag == 0 && h.molof[i] == h.molof[j]) return;
+    double rz = zi - zj;
+    double az = std::fabs(rz);
+    if (az * (1.0 / o.box[2]) >= 0.5) return;
+    for (int r = 0; r < h.nreg; ++r) {
+        double p1i = zi - h.z1[r], p1j = zj - h.z1[r];
+        double p2i = zi - h.z2[r], p2j = zj - h.z2[r];
+        int np = 0;
+        bool c1 = false;
+        if (p1i * p1j < 0.0) { c1 = true; ++np; }
+        if (p2i * p2j < 0.0) ++np;
+        double frag;
+        if (np == 0) {
+            if (p1i * p2i > 0.0) continue;
+            frag = az;
+        } else if (np == 1) {
+            if (c1) frag = p1i > 0.0 ? p1i : p1j;
+            else frag = p2i < 0.0 ? -p2i : -p2j;
+        } else {
+            frag = h.z2[r] - h.z1[r];
+        }
+        double fact = rz >= 0.0 ? frag * nbc : -frag * nbc;
+        for (int a = 0; a < 3; ++a) {
+            h.W[widx(o, cat, r, a, i)] += fi[a] * fact;
+            h.W[widx(o, cat, r, a, j)] += (-fj[a]) * fact;
+        }
+    }
+}
+
+// ewaldr_hf.F90:213-520 heat-flux part (default: bare 1/r Coulomb)
+void ewaldrp_hf(Oracle& o) {
+    int n = o.natom;
+    double sqcut = o.prm.rrcut * o.prm.rrcut, sqcut2 = o.prm.rcut * o.prm.rcut;
+    if (sqcut2 > sqcut) sqcut = sqcut2;
+    double binv[3] = {1.0 / o.box[0], 1.0 / o.box[1], 1.0 / o.box[2]};
+    Oracle::HF& h = o.hf;
+    for (int i = 0; i < n - 1; ++i) {
+        int j1 = o.nb_index[i] - 1, j2 = o.nb_index[i + 1] - 2;
+        int it = o.atmindex[i], im = h.molof[i];
+        if (o.nb_list[j1] == 0) continue;
+        for (int jx = j1; jx <= j2; ++jx) {
+            int jj = o.nb_list[jx] - 1, jm = h.molof[jj];
+            double rij[3];
+            for (int d = 0; d < 3; ++d) {
+                double r = o.atmcor[3 * i + d] - o.atmcor[3 * jj + d];
+                rij[d] = r - o.box[d] * dnint(r * binv[d]);
+            }
+            double r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+            if (r2 > sqcut) continue;
+            double rinv2 = 1.0 / r2;
+            double r = std::sqrt(r2), rinv1 = 1.0 / r;
+            if (r <= o.prm.rrcut) {
+                double potij = o.atmchrg[i] * o.atmchrg[jj] * rinv1;
+                double ftmp = potij * rinv2;
+                double fij[3] = {ftmp * rij[0], ftmp * rij[1], ftmp * rij[2]};
+                double fji[3] = {-fij[0], -fij[1], -fij[2]};
+                int cat = im == jm ? HF_ELIN : HF_ELC;
+                h.pot[(size_t)cat * n + i] += 0.5 * potij;
+                h.pot[(size_t)cat * n + jj] += 0.5 * potij;
+                calvirihf(o, i, jj, fij, fji, 0.5, cat);
+            }
+            if (r2 <= sqcut2) {
+                int jt = o.atmindex[jj];
+                if (!o.inttyp.empty() && o.inttyp[it + o.ntyp * jt] != 1) continue;
+                double R = o.radij[it + o.ntyp * jt];
+                double t2 = rinv2 * (R * R), t6 = t2 * t2 * t2, t12 = t6 * t6;
+                double E = o.welij[it + o.ntyp * jt];
+                double potij = E * (t12 - 2.0 * t6);
+                double ftmp = 12.0 * E * (t12 - t6) * rinv2;
+                double fij[3] = {ftmp * rij[0], ftmp * rij[1], ftmp * rij[2]};
+                double fji[3] = {-fij[0], -fij[1], -fij[2]};
+                int cat = im == jm ? HF_LJIN : HF_VDW;
+                h.pot[(size_t)cat * n + i] += 0.5 * potij;
+                h.pot[(size_t)cat * n + jj] += 0.5 * potij;
+                calvirihf(o, i, jj, fij, fji, 0.5, cat);
+            }
+        }
+    }
+}
+
+// calbond_hf.F90:95-160 (nbodycoeff 1/2)
+void calbondp_hf(Oracle& o) {
+    int n = o.natom;
+    for (size_t k = 0; k < o.bi.size(); ++k) {
+        if (std::fabs(o.bk[k]) < 1.0e-16) continue;
+        int i = o.bi[k], j = o.bj[k];
+        double rij[3]; mi(o, i, j, rij);
+        double r = std::sqrt(rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2]);
+        double dp = o.bk[k] * (r - o.br0[k]) * (r - o.br0[k]);
+        o.hf.pot[(size_t)HF_BO * n + i] += 0.5 * dp;
+        o.hf.pot[(size_t)HF_BO * n + j] += 0.5 * dp;
+        double fa = -2.0 * o.bk[k] * (r - o.br0[k]);
+        double f[3] = {fa * rij[0] / r, fa * rij[1] / r, fa * rij[2] / r};
+        double fji[3] = {-f[0], -f[1], -f[2]};
+        calvirihf(o, i, j, f, fji, 0.5, HF_BO);
+    }
+}
+
+// calangl_hf.F90:140-230 (nbodycoeff 1/3; pairs (i,j), (j,k), (k,i))
+void calanglp_hf(Oracle& o) {
+    int n = o.natom;
+    const double c3 = 1.0 / 3.0;
+    for (size_t q = 0; q < o.ai.size(); ++q) {
+        if (std::fabs(o.akk[q]) < 1.0e-32) continue;
+        int i = o.ai[q], j = o.aj[q], k = o.ak[q];
+        double rij[3], rkj[3];
+        mi(o, j, i, rij); mi(o, j, k, rkj);
+        double ra = std::sqrt(rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2]);
+        double rb = std::sqrt(rkj[0] * rkj[0] + rkj[1] * rkj[1] + rkj[2] * rkj[2]);
+        double c = (rij[0] * rkj[0] + rij[1] * rkj[1] + rij[2] * rkj[2]) / (ra * rb);
+        if (c > 1.0) c = 1.0; else if (c < -1.0) c = -1.0;
+        double th = std::acos(c), sn = std::sin(th);
+        double dp = o.akk[q] * (th - o.at0[q]) * (th - o.at0[q]);
+        o.hf.pot[(size_t)HF_AN * n + i] += c3 * dp;
+        o.hf.pot[(size_t)HF_AN * n + j] += c3 * dp;
+        o.hf.pot[(size_t)HF_AN * n + k] += c3 * dp;
+        double fi[3] = {0, 0, 0}, fj[3] = {0, 0, 0}, fk[3] = {0, 0, 0};
+        if (std::fabs(sn) > 1.0e-14) {
+            double ft = -2.0 * o.akk[q] * (th - o.at0[q]) / sn;
+            for (int d = 0; d < 3; ++d) {
+                fi[d] = ft * ((rkj[d] / rb - rij[d] * c / ra) / ra);
+                fk[d] = ft * ((rij[d] / ra - rkj[d] * c / rb) / rb);
+                fj[d] = -fi[d] - fk[d];
+            }
+        }
+        calvirihf(o, i, j, fi, fj, c3, HF_AN);
+        calvirihf(o, j, k, fj, fk, c3, HF_AN);
+        calvirihf(o, k, i, fk, fi, c3, HF_AN);
+    }
+}
+
+// caltors_hf.F90 / caltorsrb_hf.F90:130-200 (nbodycoeff 1/4, six pairs)
+void tors_hf_add(Oracle& o, int i, int j, int k, int l, double dp, const double* fi, const double* fj,
+                 const double* fk, const double* fl) {
+    int n = o.natom;
+    const int at[4] = {i, j, k, l};
+    for (int q = 0; q < 4; ++q) o.hf.pot[(size_t)HF_TO * n + at[q]] += 0.25 * dp;
+    calvirihf(o, i, j, fi, fj, 0.25, HF_TO);
+    calvirihf(o, i, k, fi, fk, 0.25, HF_TO);
+    calvirihf(o, i, l, fi, fl, 0.25, HF_TO);
+    calvirihf(o, j, k, fj, fk, 0.25, HF_TO);
+    calvirihf(o, j, l, fj, fl, 0.25, HF_TO);
+    calvirihf(o, k, l, fk, fl, 0.25, HF_TO);
+}
+void caltorsp_hf(Oracle& o) {
+    for (size_t q = 0; q < o.ti.size(); ++q) {
+        int i = o.ti[q], j = o.tj[q], k = o.tk[q], l = o.tl[q];
+        double rij[3], rkj[3], rkl[3], rik[3], rjl[3];
+        tors_vecs(o, i, j, k, l, rij, rkj, rkl, rik, rjl);
+        TorsGeo g; tors_geo(rij, rkj, rkl, g);
+        double period = std::fabs(o.tper[q]);
+        double bar = o.tbar[q], ph = o.tph[q], div = (double)o.tdiv[q];
+        double dp = bar / div * (1.0 + std::cos(period * g.phi - ph));
+        int np = (int)std::lround(period);
+        double c = g.cphi, fa;
+        if (np == 1) fa = 1.0;
+        else if (np == 2) fa = 2.0 * c;
+        else if (np == 3) fa = -4.0 * g.sphi * g.sphi + 3.0;
+        else if (np == 4) fa = 4.0 * c * (2.0 * c * c - 1.0);
+        else if (np == 5) { fa = 4.0 * c * c; fa = fa * (fa - 3.0) + 1.0; }
+        else if (np == 6) { fa = 4.0 * c * c; fa = 2.0 * c * (fa - 3.0) * (fa - 1.0); }
+        else fa = 0.0;
+        fa = -fa * std::cos(ph) * bar * period / div;
+        double fi[3], fj[3], fk[3], fl[3];
+        tors_forces(fa, g, rij, rkj, rkl, rik, rjl, fi, fj, fk, fl);
+        tors_hf_add(o, i, j, k, l, dp, fi, fj, fk, fl);
+    }
+}
+void caltorsrbp_hf(Oracle& o) {
+    for (size_t q = 0; q < o.rbi.size(); ++q) {
+        int i = o.rbi[q], j = o.rbj[q], k = o.rbk[q], l = o.rbl[q];
+        double rij[3], rkj[3], rkl[3], rik[3], rjl[3];
+        tors_vecs(o, i, j, k, l, rij, rkj, rkl, rik, rjl);
+        TorsGeo g; tors_geo(rij, rkj, rkl, g);
+        const double* C = &o.rbc[6 * q];
+        double bt[6] = {C[0], -C[1], C[2], -C[3], C[4], -C[5]};
+        double dp = bt[5], fa = 0.0;
+        for (int m = 4; m >= 0; --m) { fa = fa * g.cphi + dp; dp = dp * g.cphi + bt[m]; }
+        fa = -fa;
+        double fi[3], fj[3], fk[3], fl[3];
+        tors_forces(fa, g, rij, rkj, rkl, rik, rjl, fi, fj, fk, fl);
+        tors_hf_add(o, i, j, k, l, dp, fi, fj, fk, fl);
+    }
+}
+
+// calnon14_hf.F90:160-250 (nbodycoeff 1/2; Coulomb and LJ parts)
+void calnon14p_hf(Oracle& o) {
+    int n = o.natom;
+    for (size_t q = 0; q < o.p14i.size(); ++q) {
+        int i = o.p14i[q], j = o.p14j[q];
+        int it = o.atmindex[i], jt = o.atmindex[j];
+        double rij[3]; mi(o, i, j, rij);
+        double r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+        double ri2 = 1.0 / r2, ri1 = std::sqrt(ri2);
+        double de = o.atmchrg[i] * o.atmchrg[j] * ri1;
+        de = de * o.p14e[q];
+        double fe[3] = {de * ri2 * rij[0], de * ri2 * rij[1], de * ri2 * rij[2]};
+        double fe41[3] = {-fe[0], -fe[1], -fe[2]};
+        o.hf.pot[(size_t)HF_14 * n + i] += 0.5 * de;
+        o.hf.pot[(size_t)HF_14 * n + j] += 0.5 * de;
+        calvirihf(o, i, j, fe, fe41, 0.5, HF_14);
+        double R = o.radij[it + o.ntyp * jt];
+        double t2 = ri2 * (R * R), t6 = t2 * t2 * t2, t12 = t6 * t6;
+        double E = o.welij[it + o.ntyp * jt] * o.p14v[q];
+        double dv = E * (t12 - 2.0 * t6);
+        double ft = 12.0 * E * (t12 - t6) * ri2;
+        double fv[3] = {ft * rij[0], ft * rij[1], ft * rij[2]};
+        double fv41[3] = {-fv[0], -fv[1], -fv[2]};
+        o.hf.pot[(size_t)HF_14 * n + i] += 0.5 * dv;
+        o.hf.pot[(size_t)HF_14 * n + j] += 0.5 * dv;
+        calvirihf(o, i, j, fv, fv41, 0.5, HF_14);
+    }
+}
+
+// calforce_hf.F90:430-460 (zeroing) + the heat-flux parts of every term;
+// molecom from calcom at the current positions
+void calforce_hf_atm(Oracle& o) {
+    Oracle::HF& h = o.hf;
+    calcom(o, o.atmcor, h.molecom);
+    h.pot.assign((size_t)8 * o.natom, 0.0);
+    h.W.assign((size_t)8 * h.nreg * 3 * o.natom, 0.0);
+    auto on = [](int mts) { return mts == PGK_MTS_LONG || mts == PGK_MTS_SHORT; };   // term not switched off
+    if (on(o.prm.mts_vdw)) ewaldrp_hf(o);
+    if (on(o.prm.mts_bond)) calbondp_hf(o);
+    if (on(o.prm.mts_angl)) calanglp_hf(o);
+    if (on(o.prm.mts_tors)) caltorsp_hf(o);
+    if (on(o.prm.mts_torsrb)) caltorsrbp_hf(o);
+    if (on(o.prm.mts_vdw14) && o.prm.mts_vdw14 == o.prm.mts_elc14) calnon14p_hf(o);
+}
+
+// calheatf.F90:365-1466, volume-based, z components; streaming velocity 0
+void calheatf(Oracle& o, double* out) {
+    Oracle::HF& h = o.hf;
+    int n = o.natom, nm = (int)o.molidx.size() - 1;
+    h.molevel.assign((size_t)3 * nm, 0.0);
+    for (int m = 0; m < nm; ++m) {   // :556-607 (monatomic: the atom velocity)
+        int b = o.molidx[m], e = o.molidx[m + 1];
+        if (e - b == 1) {
+            for (int d = 0; d < 3; ++d) h.molevel[3 * m + d] = o.atmvel[3 * o.mollist[b] + d];
+            continue;
+        }
+        double mass = 0.0, v[3] = {0, 0, 0};
+        for (int q = b; q < e; ++q) {
+            int i = o.mollist[q];
+            mass = mass + o.atmmass[i];
+            for (int d = 0; d < 3; ++d) v[d] = v[d] + o.atmmass[i] * o.atmvel[3 * i + d];
+        }
+        double inv = 1.0 / mass;
+        for (int d = 0; d < 3; ++d) h.molevel[3 * m + d] = v[d] * inv;
+    }
+    std::fill(out, out + (size_t)h.nreg * PGK_HF_NCOL, 0.0);
+    for (int i = 0; i < n; ++i) {   // :614-760 kinetic + potential (transport) part
+        double pz, vz;
+        if (h.hftyp[i] == PGK_HFTYP_MOLE) {
+            pz = h.molecom[3 * h.molof[i] + 2];
+            vz = h.molevel[3 * h.molof[i] + 2];
+        } else {
+            pz = o.atmcor[3 * i + 2];
+            vz = o.atmvel[3 * i + 2];
+        }
+        pz = wrap1(pz, o.box[2]);
+        for (int r = 0; r < h.nreg; ++r) {
+            if (!(h.z1[r] <= pz && pz <= h.z2[r])) continue;
+            const double* v = &o.atmvel[3 * i];
+            double kin = 0.5 * o.atmmass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            double* rec = out + (size_t)r * PGK_HF_NCOL;
+            rec[0] += kin * vz;
+            for (int c = 0; c < 8; ++c) rec[1 + c] += h.pot[(size_t)c * n + i] * vz;
+        }
+    }
+    for (int r = 0; r < h.nreg; ++r) {   // :1020-1330 collision (virial) part
+        double* rec = out + (size_t)r * PGK_HF_NCOL;
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 8; ++c)
+                rec[9 + c] += h.W[widx(o, c, r, 0, i)] * o.atmvel[3 * i]
+                            + h.W[widx(o, c, r, 1, i)] * o.atmvel[3 * i + 1]
+                            + h.W[widx(o, c, r, 2, i)] * o.atmvel[3 * i + 2];
+    }
+    double area_inv = (1.0 / o.box[0]) * (1.0 / o.box[1]);
+    for (int r = 0; r < h.nreg; ++r) {   // :1331-1460
+        double vol_inv = area_inv / (h.z2[r] - h.z1[r]);
+        double* rec = out + (size_t)r * PGK_HF_NCOL;
+        double tot = 0.0;
+        for (int c = 0; c < 17; ++c) { rec[c] = rec[c] * vol_inv; tot += rec[c]; }
+        rec[17] = tot;
+    }
+}
+
+// ---- counter-based normal deviates for langevin_region ----------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC 2011), counter (atom, step lo, step hi, draw), key = seed.
+// The reference draws from SFMT (genrand_res53); the device engine uses the
+// same counter-based stream as this restatement, so the two agree draw for
+// draw and the reference agrees in distribution.
+void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+// uniform on (0, 1] with 53 random bits
+inline double u53(uint32_t a, uint32_t b) {
+    return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6) + 1.0) * (1.0 / 9007199254740992.0);
+}
+void lt_draw(uint64_t seed, long long step, int atom, double* u) {
+    for (int call = 0; call < 2; ++call) {
+        uint32_t c[4] = {(uint32_t)atom, (uint32_t)(uint64_t)step, (uint32_t)((uint64_t)step >> 32), (uint32_t)call};
+        philox4x32(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        u[2 * call] = u53(c[0], c[1]);
+        u[2 * call + 1] = u53(c[2], c[3]);
+    }
+}
+
+// langevin_regist.F90:8-360: region of each atom (first matching region)
+bool lt_inside(const Oracle::HF& h, int r, const double* g, const double* box) {
+    auto in = [](double lo, double hi, double x, double L) {
+        return (lo <= x && x < hi) || (lo <= x - L && x - L < hi);
+    };
+    return in(h.lx1[r], h.lx2[r], g[0], box[0]) && in(h.ly1[r], h.ly2[r], g[1], box[1]) &&
+           in(h.lz1[r], h.lz2[r], g[2], box[2]);
+}
+void langevin_regist(Oracle& o) {
+    Oracle::HF& h = o.hf;
+    h.ltreg.assign(o.natom, -1);
+    int nm = (int)o.molidx.size() - 1;
+    for (int m = 0; m < nm; ++m) {
+        int b = o.molidx[m], e = o.molidx[m + 1];
+        if (h.ltmole[m] && e - b > 1) {
+            double mass = 0.0, g[3] = {0, 0, 0};
+            for (int q = b; q < e; ++q) {
+                int i = o.mollist[q];
+                mass = mass + o.atmmass[i];
+                for (int d = 0; d < 3; ++d) g[d] = g[d] + o.atmmass[i] * o.atmcor[3 * i + d];
+            }
+            for (int d = 0; d < 3; ++d) g[d] = wrap1(g[d] / mass, o.box[d]);
+            for (int r = 0; r < h.nlt; ++r)
+                if (lt_inside(h, r, g, o.box)) {
+                    for (int q = b; q < e; ++q) h.ltreg[o.mollist[q]] = r;
+                    break;
+                }
+        } else {
+            for (int q = b; q < e; ++q) {
+                int i = o.mollist[q];
+                double g[3];
+                for (int d = 0; d < 3; ++d) g[d] = wrap1(o.atmcor[3 * i + d], o.box[d]);
+                for (int r = 0; r < h.nlt; ++r)
+                    if (lt_inside(h, r, g, o.box)) { h.ltreg[i] = r; break; }
+            }
+        }
+    }
+}
+
+// langevin_region.F90:8-203 (streaming velocity zero)
+void langevin_region(Oracle& o, double dt, long long step, bool former) {
+    Oracle::HF& h = o.hf;
+    int n = o.natom;
+    double ek0[8] = {0}, ek1[8] = {0};
+    if (h.ifoutthc)
+        for (int i = 0; i < n; ++i) {
+            int r = h.ltreg[i];
+            if (r < 0) continue;
+            const double* v = &o.atmvel[3 * i];
+            ek0[r] += o.atmmass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+    const double pi = std::acos(-1.0);
+    if (former) {
+        h.frand.assign((size_t)3 * n, 0.0);
+        for (int i = 0; i < n; ++i) {
+            int r = h.ltreg[i];
+            if (r < 0) continue;
+            double var = 2.0 * h.ldamp[r] * h.ltemp[r] / dt * o.atmmass[i];
+            double u[4];
+            lt_draw(h.seed, step, i, u);
+            double a = std::sqrt(-2.0 * std::log(u[0]) * var);
+            double f0 = a * std::cos(2.0 * pi * u[1]);
+            double f1 = a * std::sin(2.0 * pi * u[1]);
+            double f2 = std::sqrt(-2.0 * std::log(u[2]) * var) * std::cos(2.0 * pi * u[3]);
+            h.frand[3 * i] = f0 / o.atmmass[i];
+            h.frand[3 * i + 1] = f1 / o.atmmass[i];
+            h.frand[3 * i + 2] = f2 / o.atmmass[i];
+        }
+        for (int i = 0; i < n; ++i) {
+            int r = h.ltreg[i];
+            if (r < 0) continue;
+            double ex = std::exp(-0.5 * dt * h.ldamp[r]);
+            for (int d = 0; d < 3; ++d) {
+                o.atmvel[3 * i + d] = o.atmvel[3 * i + d] + 0.5 * dt * h.frand[3 * i + d];
+                o.atmvel[3 * i + d] = o.atmvel[3 * i + d] * ex;
+            }
+        }
+    } else {
+        for (int i = 0; i < n; ++i) {
+            int r = h.ltreg[i];
+            if (r < 0) continue;
+            double ex = std::exp(-0.5 * dt * h.ldamp[r]);
+            for (int d = 0; d < 3; ++d) {
+                o.atmvel[3 * i + d] = o.atmvel[3 * i + d] * ex;
+                o.atmvel[3 * i + d] = o.atmvel[3 * i + d] + 0.5 * dt * h.frand[3 * i + d];
+            }
+        }
+    }
+    if (h.ifoutthc) {
+        for (int i = 0; i < n; ++i) {
+            int r = h.ltreg[i];
+            if (r < 0) continue;
+            const double* v = &o.atmvel[3 * i];
+            ek1[r] += o.atmmass[i] * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        }
+        for (int r = 0; r < h.nlt; ++r) h.dekin[r] += 0.5 * (ek1[r] - ek0[r]);
+    }
+}
+
+bool hf_step(const Oracle& o, long long step) {
+    return o.hf.nreg > 0 && step > 0 && (o.hf.heatfinterval == 1 || step % o.hf.heatfinterval == 1);
+}
+
+// moldyn_hf.F90:1405-2480: NVE XO-RESPA + region Langevin + heat flux
+int moldyn_hf(Oracle& o, long long ini, long long end, const pgk_mdparams& md, pgk_energies* eout,
+              std::vector<double>* records) {
+    int n = o.natom;
+    Forces& F = o.F;
+    double dtl = md.dt_long_cal, dts = md.dt_long_cal / (double)md.nstep_short;
+    std::vector<double> old((size_t)3 * n);
+    if (F.fl.size() != (size_t)3 * n) { F.fl.assign((size_t)3 * n, 0.0); F.fs.assign((size_t)3 * n, 0.0); }
+    auto force_eval = [&](int flag) {
+        if (flag == PGK_MTS_LONG) { calforce(o, flag, F.fl.data(), &F.el, &F.vl); accforce(o, F.fl); }
+        else { calforce(o, flag, F.fs.data(), &F.es, &F.vs); accforce(o, F.fs); }
+    };
+    bool lt = o.hf.nlt > 0;
+    for (long long step = ini; step <= end; ++step) {
+        if (step % md_nbook(o) == 1 || md_nbook(o) == 1 || step == 0) transcor(o);
+        if (step % md_nbook(o) == 0 || md_nbook(o) == 1) mklist(o);
+        bool hfs = hf_step(o, step);
+        if (step == 0) {
+            if (lt) langevin_regist(o);
+            force_eval(PGK_MTS_SHORT);
+            force_eval(PGK_MTS_LONG);
+        } else {
+            if (lt) langevin_region(o, dtl, step, true);
+            for (int is = 1; is <= md.nstep_short; ++is) {
+                if (is == 1) for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dtl * F.fl[k];
+                for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dts * F.fs[k];
+                if (md.ifrattle && o.ci.size()) old = o.atmcor;
+                for (int k = 0; k < 3 * n; ++k) o.atmcor[k] = o.atmcor[k] + dts * o.atmvel[k];
+                if (md.ifrattle && o.ci.size()) {
+                    int s = rattle_pos(o, old.data(), md.eps_rattle, dts, nullptr);
+                    if (s) return s;
+                }
+                force_eval(PGK_MTS_SHORT);
+                if (is == md.nstep_short) {
+                    force_eval(PGK_MTS_LONG);
+                    if (hfs) calforce_hf_atm(o);
+                }
+                for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dts * F.fs[k];
+                if (is == md.nstep_short)
+                    for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dtl * F.fl[k];
+                if (md.ifrattle && o.ci.size()) {
+                    int s = rattlep_v(o, md.eps_rattle);
+                    if (s) return s;
+                }
+            }
+            if (lt) { langevin_regist(o); langevin_region(o, dtl, step, false); }
+            if (hfs && records) {
+                size_t b = records->size();
+                records->resize(b + (size_t)o.hf.nreg * PGK_HF_NCOL);
+                calheatf(o, records->data() + b);
+            }
+        }
+        if (eout && (md.outinterval <= 0 ? step == end : step % md.outinterval == 0)) {
+            pgk_energies e{};
+            e.pot_vdw = F.el.pot_vdw + F.es.pot_vdw; e.pot_elc = F.el.pot_elc + F.es.pot_elc;
+            e.pot_ewk = F.el.pot_ewk + F.es.pot_ewk; e.pot_ewc = F.el.pot_ewc + F.es.pot_ewc;
+            e.pot_ewnq = F.el.pot_ewnq + F.es.pot_ewnq;
+            e.pot_vdw14 = F.el.pot_vdw14 + F.es.pot_vdw14; e.pot_elc14 = F.el.pot_elc14 + F.es.pot_elc14;
+            e.pot_bond = F.el.pot_bond + F.es.pot_bond; e.pot_angl = F.el.pot_angl + F.es.pot_angl;
+            e.pot_tors = F.el.pot_tors + F.es.pot_tors; e.pot_torsrb = F.el.pot_torsrb + F.es.pot_torsrb;
+            e.pot_nonbon = F.el.pot_nonbon + F.es.pot_nonbon; e.pot_tot = F.el.pot_tot + F.es.pot_tot;
+            *eout = e;
+        }
+    }
+    return PGK_OK;
+}
 }  // namespace
 
 // ============================================================================
@@ -1416,4 +1969,74 @@ int orc_moldyn(void* h, int kind, long long ini, long long end, const pgk_mdpara
     return moldyn(o, kind, ini, end, *md, e, o.F);
 }
 
+
+int orc_set_hf(void* h, const pgk_hfparams* p) {
+    Oracle* o = (Oracle*)h;
+    Oracle::HF& f = o->hf;
+    if (p->nhfregion < 0 || p->nhfregion > PGK_HF_MAX_REGIONS || p->nlangeregion < 0 ||
+        p->nlangeregion > PGK_LT_MAX_REGIONS || (p->nhfregion > 0 && p->ifhfvol != 1))
+        return PGK_E_INVALID;
+    f.set = true;
+    f.nreg = p->nhfregion;
+    f.heatfinterval = p->heatfinterval > 0 ? p->heatfinterval : 1;
+    f.nlt = p->nlangeregion;
+    f.ifoutthc = p->ifoutthc;
+    f.seed = p->seed;
+    for (int r = 0; r < PGK_HF_MAX_REGIONS; ++r) { f.z1[r] = p->hfzpos1[r]; f.z2[r] = p->hfzpos2[r]; }
+    for (int r = 0; r < PGK_LT_MAX_REGIONS; ++r) {
+        f.lx1[r] = p->ltxpos1[r]; f.lx2[r] = p->ltxpos2[r]; f.ly1[r] = p->ltypos1[r]; f.ly2[r] = p->ltypos2[r];
+        f.lz1[r] = p->ltzpos1[r]; f.lz2[r] = p->ltzpos2[r]; f.ltemp[r] = p->r_ltemp[r]; f.ldamp[r] = p->r_ltdamp[r];
+        f.dekin[r] = 0.0;
+    }
+    int n = o->natom, nm = (int)o->molidx.size() - 1;
+    f.hftyp.assign(n, PGK_HFTYP_ATOM);
+    if (p->hftyp_atm) for (int i = 0; i < n; ++i) f.hftyp[i] = p->hftyp_atm[i];
+    f.molof.assign(n, 0);
+    for (int m = 0; m < nm; ++m)
+        for (int q = o->molidx[m]; q < o->molidx[m + 1]; ++q) f.molof[o->mollist[q]] = m;
+    f.ltmole.assign(nm, 0);
+    if (p->lt_mole_based) for (int m = 0; m < nm; ++m) f.ltmole[m] = p->lt_mole_based[m];
+    f.frand.assign((size_t)3 * n, 0.0);
+    if (f.nlt > 0) langevin_regist(*o);
+    return PGK_OK;
+}
+int orc_calheatf(void* h, double* out) {
+    Oracle* o = (Oracle*)h;
+    if (!o->hf.set || o->hf.nreg < 1) return PGK_E_INVALID;
+    if (o->nb_index.empty()) mklist(*o);
+    calforce_hf_atm(*o);
+    calheatf(*o, out);
+    return PGK_OK;
+}
+int orc_get_hf_atm(void* h, double* pot, double* W) {
+    Oracle* o = (Oracle*)h;
+    if (pot) std::copy(o->hf.pot.begin(), o->hf.pot.end(), pot);
+    if (W) std::copy(o->hf.W.begin(), o->hf.W.end(), W);
+    return PGK_OK;
+}
+int orc_moldyn_hf(void* h, long long ini, long long end, const pgk_mdparams* md, pgk_energies* e, double* rec,
+                  long long cap, long long* nrec) {
+    Oracle* o = (Oracle*)h;
+    std::vector<double> r;
+    int s = moldyn_hf(*o, ini, end, *md, e, &r);
+    long long per = (long long)o->hf.nreg * PGK_HF_NCOL;
+    long long nr = per > 0 ? (long long)r.size() / per : 0;
+    if (rec) std::copy(r.begin(), r.begin() + (size_t)std::min(nr, cap) * per, rec);
+    if (nrec) *nrec = nr;
+    return s;
+}
+void orc_langevin_dekin(void* h, double* out) {
+    Oracle* o = (Oracle*)h;
+    for (int r = 0; r < o->hf.nlt; ++r) { out[r] = o->hf.dekin[r]; o->hf.dekin[r] = 0.0; }
+}
+void orc_lt_regions(void* h, int* out) {
+    Oracle* o = (Oracle*)h;
+    std::copy(o->hf.ltreg.begin(), o->hf.ltreg.end(), out);
+}
+void orc_philox(uint64_t seed, long long step, int atom, double* u) { lt_draw(seed, step, atom, u); }
+void orc_philox_raw(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox4x32(c, key[0], key[1]);
+    for (int q = 0; q < 4; ++q) out[q] = c[q];
+}
 }  // extern "C"

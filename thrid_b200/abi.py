@@ -110,6 +110,71 @@ class ChainStruct(C.Structure):
     ]
 
 
+HF_MAX_REGIONS, LT_MAX_REGIONS, HF_NCOL = 32, 8, 18
+HFTYP_ATOM, HFTYP_MOLE = 1, 2
+HF_BO, HF_AN, HF_TO, HF_14, HF_ELIN, HF_LJIN, HF_ELC, HF_VDW = range(8)
+HF_COLUMNS = ("hfkin", "hfpotbo", "hfpotan", "hfpotto", "hfpot14", "hfpotelin", "hfpotljin", "hfpotelc",
+              "hfpotlj", "hfviribo", "hfvirian", "hfvirito", "hfviri14", "hfvirielin", "hfviriljin",
+              "hfvirielc", "hfvirilj", "hftot")
+
+
+class HfParamsStruct(C.Structure):
+    _fields_ = [
+        ("nhfregion", C.c_int32), ("ifhfvol", C.c_int32), ("heatfinterval", C.c_int32),
+        ("nlangeregion", C.c_int32),
+        ("hfzpos1", C.c_double * HF_MAX_REGIONS), ("hfzpos2", C.c_double * HF_MAX_REGIONS),
+        ("hftyp_atm", _pi), ("lt_mole_based", _pi),
+        ("ltxpos1", C.c_double * LT_MAX_REGIONS), ("ltxpos2", C.c_double * LT_MAX_REGIONS),
+        ("ltypos1", C.c_double * LT_MAX_REGIONS), ("ltypos2", C.c_double * LT_MAX_REGIONS),
+        ("ltzpos1", C.c_double * LT_MAX_REGIONS), ("ltzpos2", C.c_double * LT_MAX_REGIONS),
+        ("r_ltemp", C.c_double * LT_MAX_REGIONS), ("r_ltdamp", C.c_double * LT_MAX_REGIONS),
+        ("seed", C.c_uint64), ("ifoutthc", C.c_int32), ("_pad", C.c_int32),
+    ]
+
+
+class CHfParams:
+    """Owns the arrays behind an HfParamsStruct built from a dict:
+    regions=[(z1, z2), ...], heatfinterval, hftyp (per-atom array or None),
+    langevin=[dict(box=((x1,x2),(y1,y2),(z1,z2)), temp=T_reduced, damp=g_reduced)],
+    lt_mole (per-molecule array or None), seed, ifoutthc."""
+
+    def __init__(self, d):
+        st = HfParamsStruct()
+        regs = d.get("regions", [])
+        st.nhfregion = len(regs)
+        st.ifhfvol = int(d.get("ifhfvol", 1))
+        st.heatfinterval = int(d.get("heatfinterval", 1))
+        for k, (a, b) in enumerate(regs):
+            st.hfzpos1[k] = a
+            st.hfzpos2[k] = b
+        keep = {}
+        if d.get("hftyp") is not None:
+            keep["t"] = np.ascontiguousarray(np.asarray(d["hftyp"], dtype=np.int32))
+            st.hftyp_atm = _ptr(keep["t"], C.c_int32)
+        else:
+            st.hftyp_atm = _pi()
+        if d.get("lt_mole") is not None:
+            keep["m"] = np.ascontiguousarray(np.asarray(d["lt_mole"], dtype=np.int32))
+            st.lt_mole_based = _ptr(keep["m"], C.c_int32)
+        else:
+            st.lt_mole_based = _pi()
+        lts = d.get("langevin", [])
+        st.nlangeregion = len(lts)
+        for k, l in enumerate(lts):
+            (x1, x2), (y1, y2), (z1, z2) = l["box"]
+            st.ltxpos1[k], st.ltxpos2[k] = x1, x2
+            st.ltypos1[k], st.ltypos2[k] = y1, y2
+            st.ltzpos1[k], st.ltzpos2[k] = z1, z2
+            st.r_ltemp[k] = l["temp"]
+            st.r_ltdamp[k] = l["damp"]
+        st.seed = int(d.get("seed", 12345))
+        st.ifoutthc = int(d.get("ifoutthc", 0))
+        self.struct = st
+        self._keep = keep
+        self.nreg = len(regs)
+        self.nlt = len(lts)
+
+
 def _ptr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype)) if a is not None and a.size else C.POINTER(ctype)()
 

@@ -43,88 +43,131 @@ __global__ void k_drift(double* __restrict__ pos, double* __restrict__ old, cons
 
 // rattle_c / rattle_cmtk: one thread per constraint group, Gauss-Seidel sweeps
 // in the reference order, at most 300 sweeps (bounded; failure -> status bit).
-__global__ void k_rattle_pos(double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ old,
-                             const double* __restrict__ mass, const int* __restrict__ gidx,
-                             const int* __restrict__ glist, const int2* __restrict__ cij, const double* __restrict__ cd,
-                             int ngroup, double eps, double dt, int use_rv, const DynState* __restrict__ dyn,
-                             unsigned* status) {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngroup) return;
-    int i1 = gidx[g], i2 = gidx[g + 1];
-    double rvi[3] = {1.0, 1.0, 1.0};
-    if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+// The group's atoms (a contiguous span of at most RATTLE_LOCAL atoms) are
+// staged in thread-local arrays, so the sweeps run from L1 instead of
+// re-reading global memory; longer spans use the global arrays directly.
+#define RATTLE_LOCAL 16
+
+struct RattleAcc {   // atom storage of one group: local copy or the global arrays
+    double* x; double* v; const double* o; const double* im; int stride_lo;
+};
+
+__device__ __forceinline__ bool rattle_pos_sweeps(double* X, double* V, const double* O, const double* IM,
+                                                  int lo, const int* __restrict__ glist, const int2* __restrict__ cij,
+                                                  const double* __restrict__ cd, int i1, int i2, double eps,
+                                                  double dt, const double* rvi) {
     bool finished = false;
     for (int it = 0; it < 300 && !finished; ++it) {
         finished = true;
         for (int ii = i1; ii < i2; ++ii) {
             int nc = glist[ii];
-            int ib = cij[nc].x, jb = cij[nc].y;
+            int ib = cij[nc].x - lo, jb = cij[nc].y - lo;
             double dij = cd[nc];
-            double R0 = pos[3 * ib] - pos[3 * jb], R1 = pos[3 * ib + 1] - pos[3 * jb + 1],
-                   R2 = pos[3 * ib + 2] - pos[3 * jb + 2];
+            double R0 = X[3 * ib] - X[3 * jb], R1 = X[3 * ib + 1] - X[3 * jb + 1], R2 = X[3 * ib + 2] - X[3 * jb + 2];
             double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
             double d2 = dij * dij;
             double delta = fabs(Rsq - d2) / d2;
             if (delta < eps) continue;
             finished = false;
-            double O0 = old[3 * ib] - old[3 * jb], O1 = old[3 * ib + 1] - old[3 * jb + 1],
-                   O2 = old[3 * ib + 2] - old[3 * jb + 2];
+            double O0 = O[3 * ib] - O[3 * jb], O1 = O[3 * ib + 1] - O[3 * jb + 1], O2 = O[3 * ib + 2] - O[3 * jb + 2];
             double RR = R0 * O0 + R1 * O1 + R2 * O2;
-            double mi = 1.0 / mass[ib], mj = 1.0 / mass[jb];
+            double mi = IM[ib], mj = IM[jb];
             double gij = (Rsq - d2) / (2.0 * RR * (mi + mj) * dt);
             double G[3] = {gij * O0, gij * O1, gij * O2};
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                pos[3 * ib + d] = pos[3 * ib + d] - mi * G[d] * dt;
-                pos[3 * jb + d] = pos[3 * jb + d] + mj * G[d] * dt;
+                X[3 * ib + d] = X[3 * ib + d] - mi * G[d] * dt;
+                X[3 * jb + d] = X[3 * jb + d] + mj * G[d] * dt;
             }
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 double Gv = G[d] * rvi[d];
-                vel[3 * ib + d] = vel[3 * ib + d] - mi * Gv;
-                vel[3 * jb + d] = vel[3 * jb + d] + mj * Gv;
+                V[3 * ib + d] = V[3 * ib + d] - mi * Gv;
+                V[3 * jb + d] = V[3 * jb + d] + mj * Gv;
             }
         }
+    }
+    return finished;
+}
+
+__global__ void k_rattle_pos(double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ old,
+                             const double* __restrict__ invm, const int* __restrict__ gidx,
+                             const int* __restrict__ glist, const int2* __restrict__ cij, const double* __restrict__ cd,
+                             const int2* __restrict__ span, int ngroup, double eps, double dt, int use_rv,
+                             const DynState* __restrict__ dyn, unsigned* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroup) return;
+    int i1 = gidx[g], i2 = gidx[g + 1];
+    double rvi[3] = {1.0, 1.0, 1.0};
+    if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+    const int lo = span[g].x, na = span[g].y;
+    bool finished;
+    if (na <= RATTLE_LOCAL) {
+        double X[3 * RATTLE_LOCAL], V[3 * RATTLE_LOCAL], O[3 * RATTLE_LOCAL], IM[RATTLE_LOCAL];
+        for (int k = 0; k < 3 * na; ++k) { X[k] = pos[3 * lo + k]; V[k] = vel[3 * lo + k]; O[k] = old[3 * lo + k]; }
+        for (int k = 0; k < na; ++k) IM[k] = invm[lo + k];
+        finished = rattle_pos_sweeps(X, V, O, IM, lo, glist, cij, cd, i1, i2, eps, dt, rvi);
+        for (int k = 0; k < 3 * na; ++k) { pos[3 * lo + k] = X[k]; vel[3 * lo + k] = V[k]; }
+    } else {
+        finished = rattle_pos_sweeps(pos, vel, old, invm, 0, glist, cij, cd, i1, i2, eps, dt, rvi);
     }
     if (!finished) atomicOr(status, ST_RATTLE_NOCONV);
 }
 
-// rattlep_v (rattle_mtk.F90:278-542)
-__global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ mass,
-                             const int* __restrict__ gidx, const int* __restrict__ glist, const int2* __restrict__ cij,
-                             const double* __restrict__ cd, int ngroup, double eps, unsigned* status) {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngroup) return;
-    int i1 = gidx[g], i2 = gidx[g + 1];
+__device__ __forceinline__ bool rattle_vel_sweeps(const double* X, double* V, const double* IM, int lo,
+                                                  const int* __restrict__ glist, const int2* __restrict__ cij,
+                                                  const double* __restrict__ cd, int i1, int i2, double eps) {
     double eps2 = eps * eps;
     bool finished = false;
     for (int it = 0; it < 300 && !finished; ++it) {
         finished = true;
         for (int ii = i1; ii < i2; ++ii) {
             int nc = glist[ii];
-            int ib = cij[nc].x, jb = cij[nc].y;
+            int ib = cij[nc].x - lo, jb = cij[nc].y - lo;
             double dij = cd[nc];
-            double R[3], V[3];
+            double R[3], W[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                R[d] = pos[3 * ib + d] - pos[3 * jb + d];
-                V[d] = vel[3 * ib + d] - vel[3 * jb + d];
+                R[d] = X[3 * ib + d] - X[3 * jb + d];
+                W[d] = V[3 * ib + d] - V[3 * jb + d];
             }
-            double RV = R[0] * V[0] + R[1] * V[1] + R[2] * V[2];
+            double RV = R[0] * W[0] + R[1] * W[1] + R[2] * W[2];
             double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
-            double V2 = V[0] * V[0] + V[1] * V[1] + V[2] * V[2];
+            double V2 = W[0] * W[0] + W[1] * W[1] + W[2] * W[2];
             double phi = RV * RV / R2 * V2;   // precedence as in the reference
             if (phi < eps2) continue;
             finished = false;
-            double mi = 1.0 / mass[ib], mj = 1.0 / mass[jb];
+            double mi = IM[ib], mj = IM[jb];
             double kij = RV / (dij * dij * (mi + mj));
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 double KR = kij * R[d];
-                vel[3 * ib + d] = vel[3 * ib + d] - mi * KR;
-                vel[3 * jb + d] = vel[3 * jb + d] + mj * KR;
+                V[3 * ib + d] = V[3 * ib + d] - mi * KR;
+                V[3 * jb + d] = V[3 * jb + d] + mj * KR;
             }
         }
+    }
+    return finished;
+}
+
+// rattlep_v (rattle_mtk.F90:278-542)
+__global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ invm,
+                             const int* __restrict__ gidx, const int* __restrict__ glist, const int2* __restrict__ cij,
+                             const double* __restrict__ cd, const int2* __restrict__ span, int ngroup, double eps,
+                             unsigned* status) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroup) return;
+    int i1 = gidx[g], i2 = gidx[g + 1];
+    const int lo = span[g].x, na = span[g].y;
+    bool finished;
+    if (na <= RATTLE_LOCAL) {
+        double X[3 * RATTLE_LOCAL], V[3 * RATTLE_LOCAL], IM[RATTLE_LOCAL];
+        for (int k = 0; k < 3 * na; ++k) { X[k] = pos[3 * lo + k]; V[k] = vel[3 * lo + k]; }
+        for (int k = 0; k < na; ++k) IM[k] = invm[lo + k];
+        finished = rattle_vel_sweeps(X, V, IM, lo, glist, cij, cd, i1, i2, eps);
+        for (int k = 0; k < 3 * na; ++k) vel[3 * lo + k] = V[k];
+    } else {
+        finished = rattle_vel_sweeps(pos, vel, invm, 0, glist, cij, cd, i1, i2, eps);
     }
     if (!finished) atomicOr(status, ST_RATTLEV_NOCONV);
 }
@@ -439,9 +482,9 @@ pgk_status launch_drift(pgk_ctx* c, bool save_old) {
 
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
     if (c->ncgroup == 0) return PGK_OK;
-    k_rattle_pos<<<(c->ncgroup + 127) / 128, 128, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->mass, c->cg_idx,
-                                                               c->cg_list, c->c_ij, c->c_d, c->ncgroup, eps, dt,
-                                                               use_rv ? 1 : 0, c->dyn, c->status);
+    k_rattle_pos<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->cg_idx,
+                                                           c->cg_list, c->c_ij, c->c_d, c->cg_span, c->ncgroup, eps,
+                                                           dt, use_rv ? 1 : 0, c->dyn, c->status);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -449,8 +492,8 @@ pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
 
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
     if (c->ncgroup == 0) return PGK_OK;
-    k_rattle_vel<<<(c->ncgroup + 127) / 128, 128, 0, c->st>>>(c->pos, c->vel, c->mass, c->cg_idx, c->cg_list, c->c_ij,
-                                                               c->c_d, c->ncgroup, eps, c->status);
+    k_rattle_vel<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->invmass, c->cg_idx, c->cg_list, c->c_ij,
+                                                           c->c_d, c->cg_span, c->ncgroup, eps, c->status);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;

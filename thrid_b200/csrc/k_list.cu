@@ -1,18 +1,22 @@
 // k_list.cu -- bookkeeping pair list (mklist_cell.F90:8-352 / mklist.F90:8-234)
 // and molecule wrap (transcor.F90) on the device.
 //
-// The device list keeps, for every atom in cell-sorted order, the FULL set of
-// partners j != i with r^2 < rcut_book^2 (exact FP64 test, no FMA, Fortran
-// dnint min image) minus the mkexcl exclusions.  Its i<j half is, pair for
-// pair, the reference list; pgk_get_nblist() writes it back in the reference
-// CSR layout and row order.  The full rows let the pair kernel accumulate the
-// force of atom i without atomics on j.
+// Layout.  Atoms are counting-sorted into the reference's cells
+// (cellcount = INT(L/rcut_book), cell = MOD(INT((x+L)/cellsize), n),
+// mklist_cell.F90:114-180); inside a cell by (4x4x4 sub-cell, atom index), and
+// each cell's segment is padded with dummy slots (perm = -1) to a multiple of
+// 8, so every 8-slot CLUSTER lies inside one cell.
 //
-// Cells: cellcount = INT(L/rcut_book), cell = MOD(INT((x+L)/cellsize), n)
-// exactly as mklist_cell.F90:114-180.  When the reference would refuse the
-// cell index (rdscript.F90:1595-1610) the same cells are scanned as distinct
-// neighbour cells, which covers every pair of the all-pair mklist2a test
-// because cellsize >= rcut_book.
+// List.  For every i-cluster the row holds each atom j that is a partner of
+// at least one of the cluster's atoms, as (mask << 24 | j): bit b of the mask
+// says that j is in the list of cluster atom b.  Membership is the reference
+// test pair for pair: exact FP64 r^2 < rcut_book^2 (no FMA, Fortran dnint
+// minimum image) minus the mkexcl exclusions, both directions (j != i), so
+// the i<j half of the bits is the reference list; pgk_get_nblist() writes it
+// back in the reference CSR layout and row order.  When the reference would
+// refuse the cell index (rdscript.F90:1595-1610) the same cells are scanned
+// as distinct neighbour cells, which covers every pair of the all-pair
+// mklist2a test because cellsize >= rcut_book.
 #include <algorithm>
 #include <cstdio>
 #include <vector>
@@ -20,6 +24,7 @@
 #include "pgk_ctx.cuh"
 
 #define MAX_CELL_ATOMS 4096
+#define SUBKEY_SHIFT 25
 
 // transcor.F90: wrap each molecule by its first atom into [0, L)
 __global__ void k_transcor(double* __restrict__ pos, const int* __restrict__ mol_idx,
@@ -49,19 +54,34 @@ __device__ __forceinline__ int cell_coord(double x, double L, double cs, int nc)
     return c < 0 ? c + nc : c;
 }
 
+// cell of each atom (reference rule) and its sort key inside the cell: the
+// 4x4x4 sub-cell (Morton order) above the atom index
 __global__ void k_cell_assign(const double* __restrict__ pos, int n, const DynState* __restrict__ dyn,
-                              int* __restrict__ cell_of, int* __restrict__ cell_cnt) {
+                              int* __restrict__ cell_of, int* __restrict__ cell_cnt, int* __restrict__ subkey) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int c[3];
+    int c[3], sc[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) c[d] = cell_coord(pos[3 * i + d], dyn->box[d], dyn->cellsize[d], dyn->ncell[d]);
+    for (int d = 0; d < 3; ++d) {
+        double L = dyn->box[d], cs = dyn->cellsize[d];
+        c[d] = cell_coord(pos[3 * i + d], L, cs, dyn->ncell[d]);
+        double u = __ddiv_rn(__dadd_rn(pos[3 * i + d], L), cs);
+        double fr = u - floor(u);
+        int q = (int)(fr * 4.0);
+        sc[d] = q < 0 ? 0 : (q > 3 ? 3 : q);
+    }
     int key = c[0] + dyn->ncell[0] * (c[1] + dyn->ncell[1] * c[2]);
     cell_of[i] = key;
+    int morton = 0;
+#pragma unroll
+    for (int b = 0; b < 2; ++b)
+        morton |= (((sc[0] >> b) & 1) << (3 * b)) | (((sc[1] >> b) & 1) << (3 * b + 1)) |
+                  (((sc[2] >> b) & 1) << (3 * b + 2));
+    subkey[i] = (morton << SUBKEY_SHIFT) | i;
     atomicAdd(&cell_cnt[key], 1);
 }
 
-// exclusive scan of the cell counts (one CTA; ncells <= a few 10^4)
+// exclusive scan of the padded cell sizes (one CTA; ncells <= a few 10^4)
 __global__ void k_cell_scan(const int* __restrict__ cnt, int* __restrict__ start, int* __restrict__ fill,
                             int ncells, unsigned* status) {
     __shared__ int part[1024];
@@ -69,7 +89,7 @@ __global__ void k_cell_scan(const int* __restrict__ cnt, int* __restrict__ start
     int per = (ncells + nt - 1) / nt;
     int b = t * per, e = min(ncells, b + per);
     int s = 0, mx = 0;
-    for (int k = b; k < e; ++k) { s += cnt[k]; mx = max(mx, cnt[k]); }
+    for (int k = b; k < e; ++k) { s += (cnt[k] + 7) & ~7; mx = max(mx, cnt[k]); }
     part[t] = s;
     if (mx > MAX_CELL_ATOMS) atomicOr(status, ST_CELL_OVERFLOW);
     __syncthreads();
@@ -80,7 +100,7 @@ __global__ void k_cell_scan(const int* __restrict__ cnt, int* __restrict__ start
     }
     __syncthreads();
     int run = part[t];
-    for (int k = b; k < e; ++k) { start[k] = run; fill[k] = run; run += cnt[k]; }
+    for (int k = b; k < e; ++k) { start[k] = run; fill[k] = run; run += (cnt[k] + 7) & ~7; }
 }
 
 __global__ void k_cell_place(const int* __restrict__ cell_of, int n, int* __restrict__ fill, int* __restrict__ perm) {
@@ -90,16 +110,19 @@ __global__ void k_cell_place(const int* __restrict__ cell_of, int n, int* __rest
     perm[p] = i;
 }
 
-// stable order inside each cell: ascending original index (bitonic sort)
-__global__ void k_cell_sort(int* __restrict__ perm, const int* __restrict__ start, int ncells) {
+// deterministic order inside each cell: ascending (sub-cell, atom index);
+// the padding slots at the end of the segment get perm = -1
+__global__ void k_cell_sort(int* __restrict__ perm, const int* __restrict__ start, const int* __restrict__ cnt,
+                            const int* __restrict__ subkey, int ncells) {
     __shared__ int v[MAX_CELL_ATOMS];
     int cell = blockIdx.x;
     if (cell >= ncells) return;
-    int b = start[cell], n = start[cell + 1] - b;
-    if (n <= 1 || n > MAX_CELL_ATOMS) return;
+    int b = start[cell], n = cnt[cell], npad = start[cell + 1] - b;
+    for (int k = n + threadIdx.x; k < npad; k += blockDim.x) perm[b + k] = -1;
+    if (n <= 0 || n > MAX_CELL_ATOMS) return;
     int np = 1;
     while (np < n) np <<= 1;
-    for (int k = threadIdx.x; k < np; k += blockDim.x) v[k] = k < n ? perm[b + k] : 0x7fffffff;
+    for (int k = threadIdx.x; k < np; k += blockDim.x) v[k] = k < n ? subkey[perm[b + k]] : 0x7fffffff;
     __syncthreads();
     for (int size = 2; size <= np; size <<= 1)
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
@@ -113,15 +136,20 @@ __global__ void k_cell_sort(int* __restrict__ perm, const int* __restrict__ star
             }
             __syncthreads();
         }
-    for (int k = threadIdx.x; k < n; k += blockDim.x) perm[b + k] = v[k];
+    for (int k = threadIdx.x; k < n; k += blockDim.x) perm[b + k] = v[k] & ((1 << SUBKEY_SHIFT) - 1);
 }
 
-__global__ void k_sorted_gather(const int* __restrict__ perm, int n, const double* __restrict__ pos,
+__global__ void k_sorted_gather(const int* __restrict__ perm, int npad, const double* __restrict__ pos,
                                 const int* __restrict__ typ, int* __restrict__ iperm, double* __restrict__ pos_s,
                                 int* __restrict__ typ_s) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= npad) return;
     int i = perm[s];
+    if (i < 0) {
+        pos_s[3 * s + 0] = 0.0; pos_s[3 * s + 1] = 0.0; pos_s[3 * s + 2] = 0.0;
+        typ_s[s] = 0;
+        return;
+    }
     iperm[i] = s;
     pos_s[3 * s + 0] = pos[3 * i + 0];
     pos_s[3 * s + 1] = pos[3 * i + 1];
@@ -140,28 +168,39 @@ __device__ __forceinline__ bool is_excluded(const int* __restrict__ exs_idx, con
     return false;
 }
 
-// one warp per sorted atom: scan the distinct neighbour cells, keep the
-// exact-test pairs, drop exclusions, append to the row.
-__global__ void __launch_bounds__(256) k_build_list(
+// one warp per i-cluster: scan the distinct neighbour cells of the cluster's
+// cell; for each real candidate j test all 8 cluster atoms (exact FP64 test,
+// exclusions) and append (mask << 24 | j) when any bit is set.
+__global__ void __launch_bounds__(256) k_build_clist(
         const double* __restrict__ pos_s, const int* __restrict__ perm, const int* __restrict__ cell_of,
-        const int* __restrict__ cell_start, const int* __restrict__ exs_idx, const int* __restrict__ exs_list,
-        int n, int cap, double sqcut, const DynState* __restrict__ dyn,
-        int* __restrict__ nbr, int* __restrict__ ncnt, unsigned long long* __restrict__ counters,
+        const int* __restrict__ cell_start, const int* __restrict__ cell_cnt, const int* __restrict__ exs_idx,
+        const int* __restrict__ exs_list, int n, int ncl, int ccap, double sqcut, const DynState* __restrict__ dyn,
+        int* __restrict__ clist, int* __restrict__ ccnt, unsigned long long* __restrict__ counters,
         unsigned* __restrict__ status) {
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    int s = warp;
-    int io = perm[s];
-    double xi = pos_s[3 * s], yi = pos_s[3 * s + 1], zi = pos_s[3 * s + 2];
-    double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
-    double B0 = 1.0 / L0, B1 = 1.0 / L1, B2 = 1.0 / L2;
-    int nc0 = dyn->ncell[0], nc1 = dyn->ncell[1], nc2 = dyn->ncell[2];
-    int key = cell_of[io];
-    int cx = key % nc0, cy = (key / nc0) % nc1, cz = key / (nc0 * nc1);
-    int nz = nc2 >= 3 ? 3 : nc2, ny = nc1 >= 3 ? 3 : nc1, nx = nc0 >= 3 ? 3 : nc0;
-    int count = 0, half = 0;
-    int* row = nbr + (size_t)s * cap;
+    __shared__ double spi[8][3 * 8];
+    __shared__ int sio[8][8];
+    const int wib = threadIdx.x >> 5;
+    const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (cl >= ncl) return;
+    const int s0 = 8 * cl;
+    if (lane < 8) {
+        int io = perm[s0 + lane];
+        sio[wib][lane] = io;
+        spi[wib][3 * lane] = pos_s[3 * (s0 + lane)];
+        spi[wib][3 * lane + 1] = pos_s[3 * (s0 + lane) + 1];
+        spi[wib][3 * lane + 2] = pos_s[3 * (s0 + lane) + 2];
+    }
+    __syncwarp();
+    const double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
+    const double B0 = 1.0 / L0, B1 = 1.0 / L1, B2 = 1.0 / L2;
+    const int nc0 = dyn->ncell[0], nc1 = dyn->ncell[1], nc2 = dyn->ncell[2];
+    const int key = cell_of[sio[wib][0]];
+    const int cx = key % nc0, cy = (key / nc0) % nc1, cz = key / (nc0 * nc1);
+    const int nz = nc2 >= 3 ? 3 : nc2, ny = nc1 >= 3 ? 3 : nc1, nx = nc0 >= 3 ? 3 : nc0;
+    int count = 0;
+    int full[8] = {0, 0, 0, 0, 0, 0, 0, 0}, half[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int* row = clist + (size_t)cl * ccap;
     for (int a = 0; a < nz; ++a) {
         int z = nc2 >= 3 ? (cz + a - 1 + nc2) % nc2 : a;
         for (int b = 0; b < ny; ++b) {
@@ -169,38 +208,58 @@ __global__ void __launch_bounds__(256) k_build_list(
             for (int c = 0; c < nx; ++c) {
                 int x = nc0 >= 3 ? (cx + c - 1 + nc0) % nc0 : c;
                 int cell = x + nc0 * (y + nc1 * z);
-                int t0 = cell_start[cell], t1 = cell_start[cell + 1];
+                int t0 = cell_start[cell], t1 = t0 + cell_cnt[cell];
                 for (int tb = t0; tb < t1; tb += 32) {
                     int t = tb + lane;
-                    bool keep = false;
-                    int jo = -1;
-                    if (t < t1 && t != s) {
-                        double r0 = mi_exact(__dsub_rn(xi, pos_s[3 * t]), L0, B0);
-                        double r1 = mi_exact(__dsub_rn(yi, pos_s[3 * t + 1]), L1, B1);
-                        double r2 = mi_exact(__dsub_rn(zi, pos_s[3 * t + 2]), L2, B2);
-                        double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)), __dmul_rn(r2, r2));
-                        if (dr < sqcut) {
-                            jo = perm[t];
-                            keep = !is_excluded(exs_idx, exs_list, io, jo);
+                    unsigned mask = 0;
+                    if (t < t1) {
+                        const double xj = pos_s[3 * t], yj = pos_s[3 * t + 1], zj = pos_s[3 * t + 2];
+                        const int jo = perm[t];
+#pragma unroll
+                        for (int ii = 0; ii < 8; ++ii) {
+                            const int io = sio[wib][ii];
+                            if (io < 0 || t == s0 + ii) continue;
+                            double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L0, B0);
+                            double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L1, B1);
+                            double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L2, B2);
+                            double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)), __dmul_rn(r2, r2));
+                            if (dr < sqcut && !is_excluded(exs_idx, exs_list, io, jo)) {
+                                mask |= 1u << ii;
+                                full[ii] += 1;
+                                if (jo > io) half[ii] += 1;
+                            }
                         }
                     }
-                    unsigned m = __ballot_sync(0xffffffffu, keep);
-                    unsigned mh = __ballot_sync(0xffffffffu, keep && jo > io);
-                    if (keep) {
+                    unsigned m = __ballot_sync(0xffffffffu, mask != 0);
+                    if (mask) {
                         int off = count + __popc(m & ((1u << lane) - 1u));
-                        if (off < cap) row[off] = t;
+                        if (off < ccap) row[off] = (int)((mask << 24) | (unsigned)t);
                     }
                     count += __popc(m);
-                    half += __popc(mh);
                 }
             }
         }
     }
+#pragma unroll
+    for (int ii = 0; ii < 8; ++ii) {
+        full[ii] = warp_sum(full[ii]);
+        half[ii] = warp_sum(half[ii]);
+    }
     if (lane == 0) {
-        ncnt[s] = min(count, cap);
-        if (count > cap) atomicOr(status, ST_LIST_OVERFLOW);
+        ccnt[cl] = min(count, ccap);
+        if (count > ccap) atomicOr(status, ST_LIST_OVERFLOW);
         atomicMax(&counters[1], (unsigned long long)count);
-        if (io < n - 1) atomicAdd(&counters[0], (unsigned long long)(half > 0 ? half : 1));
+        unsigned long long nl = 0;
+        int mx = 0;
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            int io = sio[wib][ii];
+            if (io < 0) continue;
+            mx = max(mx, full[ii]);
+            if (io < n - 1) nl += (unsigned long long)(half[ii] > 0 ? half[ii] : 1);
+        }
+        atomicAdd(&counters[0], nl);
+        atomicMax(&counters[3], (unsigned long long)mx);
     }
 }
 
@@ -221,6 +280,28 @@ static int list_mode_for(const pgk_ctx* c, const double* box, int* nc) {
     return PGK_LIST_CELL;
 }
 
+// (re)allocate the sorted/padded arrays for up to npad_cap slots
+static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
+    if (npad_cap <= c->npad_cap) return PGK_OK;
+    cudaFree(c->perm); cudaFree(c->pos_s); cudaFree(c->typ_s); cudaFree(c->xq); cudaFree(c->xq64);
+    cudaFree(c->ccnt); cudaFree(c->clist);
+    c->perm = nullptr; c->pos_s = nullptr; c->typ_s = nullptr; c->xq = nullptr; c->xq64 = nullptr;
+    c->ccnt = nullptr; c->clist = nullptr;
+    int ncl = npad_cap / 8;
+    PGK_CUDA(c, cudaMalloc(&c->perm, sizeof(int) * npad_cap));
+    PGK_CUDA(c, cudaMalloc(&c->pos_s, sizeof(double) * 3 * npad_cap));
+    PGK_CUDA(c, cudaMalloc(&c->typ_s, sizeof(int) * npad_cap));
+    if (c->mixed()) PGK_CUDA(c, cudaMalloc(&c->xq, sizeof(int4) * npad_cap));
+    else PGK_CUDA(c, cudaMalloc(&c->xq64, sizeof(double4) * npad_cap));
+    PGK_CUDA(c, cudaMalloc(&c->ccnt, sizeof(int) * ncl));
+    if (cudaMalloc(&c->clist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {
+        c->clist = nullptr;
+        return pgk_fail(c, PGK_E_NOMEM, "cluster pair list exceeds device memory");
+    }
+    c->npad_cap = npad_cap;
+    return PGK_OK;
+}
+
 pgk_status launch_mklist(pgk_ctx* c) {
     int n = c->natom;
     // the box may have changed on the device (MTK): read it back
@@ -239,48 +320,55 @@ pgk_status launch_mklist(pgk_ctx* c) {
         PGK_CUDA(c, cudaMalloc(&c->cell_start, sizeof(int) * (ncells + 1)));
         PGK_CUDA(c, cudaMalloc(&c->cell_fill, sizeof(int) * (ncells + 1)));
     }
+    long long npad_max = (long long)n + 7 * ncells;
+    if (npad_max >= (1 << 24)) return pgk_fail(c, PGK_E_UNSUPPORTED, "more than 2^24 padded atom slots");
+    pgk_status s;
+    if ((s = ensure_sorted_capacity(c, (int)((npad_max + 7) / 8 * 8)))) return s;
     DynState& h = c->hdyn;
     for (int d = 0; d < 3; ++d) { h.ncell[d] = nc[d]; h.cellsize[d] = h.box[d] / (double)nc[d]; }
     h.list_mode_used = mode;
     PGK_CUDA(c, cudaMemcpyAsync(c->dyn, &h, sizeof(DynState), cudaMemcpyHostToDevice, c->st));
     for (int attempt = 0; attempt < 3; ++attempt) {
         PGK_CUDA(c, cudaMemsetAsync(c->cell_cnt, 0, sizeof(int) * (ncells + 1), c->st));
-        PGK_CUDA(c, cudaMemsetAsync(c->counters, 0, 2 * sizeof(unsigned long long), c->st));
+        PGK_CUDA(c, cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->st));
         int tb = 256, nb = (n + tb - 1) / tb;
-        k_cell_assign<<<nb, tb, 0, c->st>>>(c->pos, n, c->dyn, c->cell_of, c->cell_cnt);
+        k_cell_assign<<<nb, tb, 0, c->st>>>(c->pos, n, c->dyn, c->cell_of, c->cell_cnt, c->subkey);
         k_cell_scan<<<1, 1024, 0, c->st>>>(c->cell_cnt, c->cell_start, c->cell_fill, (int)ncells, c->status);
         k_cell_place<<<nb, tb, 0, c->st>>>(c->cell_of, n, c->cell_fill, c->perm);
-        k_cell_sort<<<(int)ncells, 512, 0, c->st>>>(c->perm, c->cell_start, (int)ncells);
-        k_sorted_gather<<<nb, tb, 0, c->st>>>(c->perm, n, c->pos, c->typ, c->iperm, c->pos_s, c->typ_s);
+        k_cell_sort<<<(int)ncells, 512, 0, c->st>>>(c->perm, c->cell_start, c->cell_cnt, c->subkey, (int)ncells);
+        int npad = 0;
+        PGK_CUDA(c, cudaMemcpyAsync(&npad, c->cell_start + ncells, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        PGK_CUDA(c, cudaStreamSynchronize(c->st));
+        c->npad = npad;
+        c->ncl = npad / 8;
+        k_sorted_gather<<<(npad + 255) / 256, 256, 0, c->st>>>(c->perm, npad, c->pos, c->typ, c->iperm, c->pos_s,
+                                                               c->typ_s);
         double sq = c->prm.rcut_book * c->prm.rcut_book;
-        long long threads = (long long)n * 32;
-        k_build_list<<<(unsigned)((threads + 255) / 256), 256, 0, c->st>>>(
-            c->pos_s, c->perm, c->cell_of, c->cell_start, c->exs_idx, c->exs_list, n, c->cap, sq, c->dyn,
-            c->nbr, c->ncnt, c->counters, c->status);
+        long long threads = (long long)c->ncl * 32;
+        k_build_clist<<<(unsigned)((threads + 255) / 256), 256, 0, c->st>>>(
+            c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, n, c->ncl, c->ccap,
+            sq, c->dyn, c->clist, c->ccnt, c->counters, c->status);
         c->launches += 6;
         PGK_CUDA(c, cudaGetLastError());
-        unsigned long long cnt[2];
+        unsigned long long cnt[4];
         unsigned st;
         PGK_CUDA(c, cudaMemcpyAsync(cnt, c->counters, sizeof(cnt), cudaMemcpyDeviceToHost, c->st));
         PGK_CUDA(c, cudaMemcpyAsync(&st, c->status, sizeof(st), cudaMemcpyDeviceToHost, c->st));
         PGK_CUDA(c, cudaStreamSynchronize(c->st));
-        if (st & ST_CELL_OVERFLOW) return pgk_fail(c, PGK_E_CELL_OVERFLOW, "number of atoms in a cell exceeds the device maximum");
+        if (st & ST_CELL_OVERFLOW)
+            return pgk_fail(c, PGK_E_CELL_OVERFLOW, "number of atoms in a cell exceeds the device maximum");
         if (st & ST_LIST_OVERFLOW) {
-            // grow the rows and rebuild (the reference STOPs here)
-            int need = (int)((cnt[1] + 63) / 32 * 32);
+            // grow the cluster rows and rebuild (the reference STOPs here)
             unsigned zero = 0;
             PGK_CUDA(c, cudaMemcpy(c->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
-            size_t bytes = (size_t)n * need * sizeof(int);
-            cudaFree(c->nbr);
-            if (cudaMalloc(&c->nbr, bytes) != cudaSuccess) {
-                c->nbr = nullptr;
-                return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list exceeds device memory");
-            }
-            c->cap = need;
+            c->ccap = (int)((cnt[1] + 63) / 32 * 32);
+            int capslots = c->npad_cap;
+            c->npad_cap = 0;
+            if ((s = ensure_sorted_capacity(c, capslots))) return s;
             continue;
         }
         h.nlistnball = (long long)cnt[0];
-        h.nmaxrow = (int)cnt[1];
+        h.nmaxrow = (int)cnt[3];
         PGK_CUDA(c, cudaMemcpyAsync(&c->dyn->nlistnball, &h.nlistnball, sizeof(long long),
                                     cudaMemcpyHostToDevice, c->st));
         c->list_valid = true;
@@ -289,17 +377,17 @@ pgk_status launch_mklist(pgk_ctx* c) {
     return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list overflow after regrowth");
 }
 
-// Reference CSR (nb_indexall / nb_listall) from the device rows.
+// Reference CSR (nb_indexall / nb_listall) from the device cluster rows.
 pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_t cap, int64_t* nl) {
     if (!c->list_valid) return pgk_fail(c, PGK_E_INVALID, "no pair list has been built");
-    int n = c->natom;
-    std::vector<int> ncnt(n), perm(n), iperm(n), cell_of(n);
-    std::vector<int> rows((size_t)n * c->cap);
-    PGK_CUDA(c, cudaMemcpyAsync(ncnt.data(), c->ncnt, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
-    PGK_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
+    int n = c->natom, npad = c->npad, ncl = c->ncl;
+    std::vector<int> ccnt(ncl), perm(npad), iperm(n), cell_of(n);
+    std::vector<int> rows((size_t)ncl * c->ccap);
+    PGK_CUDA(c, cudaMemcpyAsync(ccnt.data(), c->ccnt, sizeof(int) * ncl, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm, sizeof(int) * npad, cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(iperm.data(), c->iperm, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(cell_of.data(), c->cell_of, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
-    PGK_CUDA(c, cudaMemcpyAsync(rows.data(), c->nbr, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaMemcpyAsync(rows.data(), c->clist, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaStreamSynchronize(c->st));
     const DynState& h = c->hdyn;
@@ -308,12 +396,14 @@ pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_
     long long pos = 0;
     std::vector<std::pair<long long, int>> tmp;
     for (int i = 0; i < n - 1; ++i) {
-        int s = iperm[i];
+        int s = iperm[i], cl = s / 8, bit = s % 8;
         tmp.clear();
         int ki = cell_of[i];
         int ix = ki % nc0, iy = (ki / nc0) % nc1, iz = ki / (nc0 * nc1);
-        for (int k = 0; k < ncnt[s]; ++k) {
-            int j = perm[rows[(size_t)s * c->cap + k]];
+        for (int k = 0; k < ccnt[cl]; ++k) {
+            unsigned e = (unsigned)rows[(size_t)cl * c->ccap + k];
+            if (!((e >> (24 + bit)) & 1u)) continue;
+            int j = perm[e & 0xFFFFFFu];
             if (j <= i) continue;
             long long ord = j;
             if (cellmode) {   // 27-cell scan order z, y, x (mklist_cell.F90:218-273)

@@ -1,34 +1,39 @@
 // k_nonbond.cu -- real-space LJ + Ewald pair kernel (ewaldrp, ewaldr.F90:404-838)
 //
-// Work decomposition: one warp per atom i of the cell-sorted order, lanes
-// stride over i's full neighbour row (j != i, both directions), so the force
-// on i is a register sum closed by a warp shuffle reduction -- no atomics on
-// j, and a fixed summation order.  Every pair is therefore evaluated twice;
-// energies and virials carry a factor 1/2.
+// Work decomposition: one warp per 8-atom i-cluster of the cell-sorted order.
+// The cluster's row holds entries (mask << 24 | j); bit b of the mask says
+// that j is a list partner of cluster atom b.  One gather of j serves up to 8
+// pairs, and the index stream is one 4-byte entry per (cluster, j) instead of
+// one per pair.  Rows hold both directions (j != i), so the force on each
+// cluster atom is a register sum closed by warp shuffles -- no atomics on j
+// and a fixed summation order.  Every pair is evaluated twice; energies and
+// virials carry a factor 1/2.
 //
 // Mixed precision: positions enter as 32-bit fractional fixed point per box
 // axis (x/L * 2^32); the wrapped integer difference is the minimum-image
 // displacement, converted to FP32 with the box scale.  The displacement error
 // is ~L/2^32 (3e-8 A at L = 130 A) instead of the 8e-6 A of FP32 absolute
 // coordinates.  Pair arithmetic is FP32 with the reference's natural cubic
-// spline tables (spline_interp.F90) staged in shared memory; the per-atom
+// spline tables (spline_interp.F90) staged in shared memory; each atom's
 // force is converted once to int64 fixed point (2^32) and added to the group
 // accumulator.  FP64 precision runs the same structure in double with the
 // reference's dnint minimum image.
 //
 // Roofline: FP32 pipe (61 algorithmic flop per interacting pair) plus one
-// 4-byte index and one 16-byte (32-byte FP64) gather per list entry.
+// 4-byte entry, one 16-byte (32-byte FP64) position and one 4-byte type
+// gather per (cluster, j) entry.
 #include <vector>
 
 #include "pgk_ctx.cuh"
 
-// ---- pack: sorted positions for the pair kernel -------------------------------
+// ---- pack: sorted (padded) positions for the pair kernel ---------------------
 __global__ void k_pack_mixed(const double* __restrict__ pos, const double* __restrict__ chrg,
-                             const int* __restrict__ perm, int n, const DynState* __restrict__ dyn,
+                             const int* __restrict__ perm, int npad, const DynState* __restrict__ dyn,
                              int4* __restrict__ xq) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= npad) return;
     int i = perm[s];
+    if (i < 0) { xq[s] = make_int4(0, 0, 0, 0); return; }
     unsigned u[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -40,15 +45,16 @@ __global__ void k_pack_mixed(const double* __restrict__ pos, const double* __res
 }
 
 __global__ void k_pack_fp64(const double* __restrict__ pos, const double* __restrict__ chrg,
-                            const int* __restrict__ perm, int n, double4* __restrict__ xq) {
+                            const int* __restrict__ perm, int npad, double4* __restrict__ xq) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
+    if (s >= npad) return;
     int i = perm[s];
-    xq[s] = make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], chrg[i]);
+    xq[s] = i < 0 ? make_double4(0, 0, 0, 0) : make_double4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], chrg[i]);
 }
 
 pgk_status launch_pack(pgk_ctx* c) {
-    int n = c->natom;
+    int n = c->npad;
+    if (n <= 0) return PGK_OK;
     if (c->mixed())
         k_pack_mixed<<<(n + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->perm, n, c->dyn, c->xq);
     else
@@ -58,22 +64,23 @@ pgk_status launch_pack(pgk_ctx* c) {
     return PGK_OK;
 }
 
-// ---- pair kernel, mixed precision ------------------------------------------
 struct PairArgs {
-    const int* nbr; const int* ncnt; int cap; int n;
+    const int* clist; const int* ccnt; int ccap; int ncl;
     const int* typ_s; const int* perm;
     int ntyp; int nspl; double h, inv_h;
     double rr2, rl2, rmax2, rrcut;
     void* facc; long long* acc;
 };
 
-template <bool ENE, bool VIR>
-__device__ __forceinline__ void pair_term(const int4 pi, const float qi, const int ti, const int4 pj, const int tj,
+// ---- one pair, mixed precision -----------------------------------------------
+template <int MODE>
+__device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int4 pj, const int tj,
                                           const float sx, const float sy, const float sz, const float rmax2,
                                           const float rr2, const float rl2, const float inv_h, const float h,
                                           const float4* __restrict__ sf, const float4* __restrict__ sp,
                                           const float2* __restrict__ slj, float& fx, float& fy, float& fz,
                                           float& ev, float& ee, float* wc, float* wl) {
+    constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     const float dx = (float)(pi.x - pj.x) * sx;
     const float dy = (float)(pi.y - pj.y) * sy;
     const float dz = (float)(pi.z - pj.z) * sz;
@@ -84,12 +91,17 @@ __device__ __forceinline__ void pair_term(const int4 pi, const float qi, const i
     float fc = 0.f, fl = 0.f;
     if (r2 <= rr2) {
         const float r = r2 * rinv;
-        const float qq = qi * __int_as_float(pj.w);
-        const int idx = (int)(r * inv_h);
-        const float d = fmaf(-(float)idx, h, r);
+        const float qq = __int_as_float(pi.w) * __int_as_float(pj.w);
+        // floor(r/h) on the FP32/ALU pipes (r/h < 2^22): round to nearest via
+        // the 2^23 magic constant, step down when it rounded up
+        const float tf = r * inv_h;
+        float fm = (tf + 8388608.0f) - 8388608.0f;
+        fm = fm > tf ? fm - 1.0f : fm;
+        const int idx = __float_as_int(fm + 8388608.0f) - 0x4B000000;
+        const float d = fmaf(-fm, h, r);
         const float4 c = sf[idx];
         fc = qq * fmaf(d, fmaf(d, fmaf(d, c.w, c.z), c.y), c.x);
-        if (ENE || VIR) {
+        if (ENE) {
             const float4 p = sp[idx];
             ee = fmaf(qq, fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x), ee);
         }
@@ -100,13 +112,18 @@ __device__ __forceinline__ void pair_term(const int4 pi, const float qi, const i
         const float t6 = t2 * t2 * t2;
         const float t12 = t6 * t6;
         fl = 12.f * lp.y * (t12 - t6) * rinv2;
-        if (ENE || VIR) ev = fmaf(lp.y, t12 - 2.f * t6, ev);
+        if (ENE) ev = fmaf(lp.y, t12 - 2.f * t6, ev);
     }
     const float fs = fc + fl;
     fx = fmaf(fs, dx, fx);
     fy = fmaf(fs, dy, fy);
     fz = fmaf(fs, dz, fz);
-    if (VIR) {
+    if (MODE == PM_TENS) {
+        const float cx = fs * dx, cy = fs * dy, cz = fs * dz;
+        wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
+        wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
+    }
+    if (MODE == PM_FULL) {
         const float cx = fc * dx, cy = fc * dy, cz = fc * dz;
         wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
         wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
@@ -116,22 +133,36 @@ __device__ __forceinline__ void pair_term(const int4 pi, const float qi, const i
     }
 }
 
-// Each lane walks entries lane, lane+32, ... of the row; the next entry's
-// index, position and type are loaded before the current pair is evaluated
-// (two gathers in flight per lane).  Per-lane energy/virial sums stay in
-// FP32 registers across all atoms of the warp and are reduced once per block.
-template <bool ENE, bool VIR>
-__global__ void __launch_bounds__(256, 4) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
+// MODE: PM_FORCE forces only; PM_ENE + pot_vdw, pot_elc; PM_TENS + the
+// combined (Coulomb + LJ) virial tensor only (what the anisotropic MTK
+// barostat reads every step: diag(pintt)); PM_FULL + energies, split tensors
+// and the scalar virials of ewaldrp.
+//
+// Each lane walks entries lane, lane+32, ... of the cluster's row; for each
+// entry it evaluates the pairs with the cluster atoms whose mask bit is set
+// (cluster atoms in shared memory) and keeps the 8 atoms' forces in
+// registers, closed by warp shuffles after the row.  The next entry and its j
+// record are loaded before the current entry's pairs are evaluated.
+//
+// Block b owns the contiguous cluster range [b*chunk, (b+1)*chunk); its
+// warps take every 8th cluster of it, so they read overlapping j ranges at
+// the same time (shared L1 lines).  Per-lane energy/virial sums stay in FP32
+// registers across the block's clusters and are reduced once per block.
+template <int MODE>
+__global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
                                                        const float2* __restrict__ lj_g,
                                                        const float4* __restrict__ spl_g,
                                                        const DynState* __restrict__ dyn) {
+    constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     extern __shared__ float4 sm[];
     float4* sf = sm;                        // force table  (spline 0)
-    float4* sp = sm + a.nspl;               // pot table    (spline 1), ENE/VIR only
-    float2* slj = (float2*)(sm + (ENE || VIR ? 2 : 1) * a.nspl);
+    float4* sp = sm + a.nspl;               // pot table    (spline 1), ENE only
+    float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
+    __shared__ int4 si[8][8];
+    __shared__ int sti[8][8];
     for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) {
         sf[k] = spl_g[k];
-        if (ENE || VIR) sp[k] = spl_g[a.nspl + k];
+        if (ENE) sp[k] = spl_g[a.nspl + k];
     }
     for (int k = threadIdx.x; k < a.ntyp * a.ntyp; k += blockDim.x) slj[k] = lj_g[k];
     __syncthreads();
@@ -141,55 +172,74 @@ __global__ void __launch_bounds__(256, 4) k_pair_mixed(const int4* __restrict__ 
     const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
     const float rr2 = (float)a.rr2, rl2 = (float)a.rl2, rmax2 = (float)a.rmax2;
     const float inv_h = (float)a.inv_h, h = (float)a.h;
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
+    const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
     const int* __restrict__ typ_s = a.typ_s;
     float ev = 0.f, ee = 0.f;
     float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
-    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.n; s += nwarps) {
-        const int4 pi = __ldg(xq + s);
-        const float qi = __int_as_float(pi.w);
-        const int ti = __ldg(typ_s + s) * a.ntyp;
-        const int cnt = __ldg(a.ncnt + s);
-        const int* __restrict__ row = a.nbr + (size_t)s * a.cap;
-        float fx = 0.f, fy = 0.f, fz = 0.f;
+    for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
+        __syncwarp();
+        if (lane < 8) {
+            si[warp][lane] = __ldg(xq + 8 * cl + lane);
+            sti[warp][lane] = __ldg(typ_s + 8 * cl + lane) * a.ntyp;
+        }
+        __syncwarp();
+        const int cnt = __ldg(a.ccnt + cl);
+        const int* __restrict__ row = a.clist + (size_t)cl * a.ccap;
+        float f[8][3];
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) { f[ii][0] = 0.f; f[ii][1] = 0.f; f[ii][2] = 0.f; }
         int k = lane;
-        int j = k < cnt ? __ldg(row + k) : s;
-        int4 pj = __ldg(xq + j);
-        int tj = __ldg(typ_s + j);
+        unsigned e = k < cnt ? (unsigned)__ldg(row + k) : 0u;
+        int4 pj = __ldg(xq + (e & 0xFFFFFFu));
+        int tj = __ldg(typ_s + (e & 0xFFFFFFu));
         while (k < cnt) {
             const int kn = k + 32;
-            const int jn = kn < cnt ? __ldg(row + kn) : s;
-            const int4 pjn = __ldg(xq + jn);
-            const int tjn = __ldg(typ_s + jn);
-            pair_term<ENE, VIR>(pi, qi, ti, pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h, sf, sp, slj,
-                                fx, fy, fz, ev, ee, wc, wl);
-            k = kn; pj = pjn; tj = tjn;
+            const unsigned en = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
+            const int4 pjn = __ldg(xq + (en & 0xFFFFFFu));
+            const int tjn = __ldg(typ_s + (en & 0xFFFFFFu));
+            const unsigned m = e >> 24;
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii)
+                if ((m >> ii) & 1u)
+                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h, sf,
+                                    sp, slj, f[ii][0], f[ii][1], f[ii][2], ev, ee, wc, wl);
+            k = kn; e = en; pj = pjn; tj = tjn;
         }
-        fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
-        if (lane == 0) force_add<true>(a.facc, a.perm[s], (double)fx, (double)fy, (double)fz);
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
+            if (lane == ii) {
+                const int io = a.perm[8 * cl + ii];
+                if (io >= 0) force_add<true>(a.facc, io, (double)fx, (double)fy, (double)fz);
+            }
+        }
     }
-    if (ENE || VIR) {
-        // pairs were counted from both sides: factor 1/2.  Tensor (a,b) -> 3*b + a.
+    // pairs were counted from both sides: factor 1/2.  Tensor (a,b) -> 3*b + a,
+    // stored as its lower triangle.
+    if (MODE == PM_FULL) {
         double v[16] = {0.5 * ev, 0.5 * ee, 0.5 * ee,
                         0.5 * wc[0], 0.5 * wc[1], 0.5 * wc[2], 0.5 * wc[3], 0.5 * wc[4], 0.5 * wc[5],
                         0.5 * wl[0], 0.5 * wl[1], 0.5 * wl[2], 0.5 * wl[3], 0.5 * wl[4], 0.5 * wl[5],
                         0.5 * ((double)wl[0] + (double)wl[3] + (double)wl[5])};
-        if (VIR) {
-            const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
-                                 A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
-            block_acc<16>(v, a.acc, idx, false);
-        } else {
-            double v2[2] = {v[0], v[1]};
-            const int idx[2] = {A_VDW, A_ELC};
-            block_acc<2>(v2, a.acc, idx, false);
-        }
+        const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
+                             A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
+        block_acc<16>(v, a.acc, idx, false);
+    } else if (MODE == PM_TENS) {
+        double v[6] = {0.5 * wc[0], 0.5 * wc[1], 0.5 * wc[2], 0.5 * wc[3], 0.5 * wc[4], 0.5 * wc[5]};
+        const int idx[6] = {A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
+        block_acc<6>(v, a.acc, idx, false);
+    } else if (MODE == PM_ENE) {
+        double v[2] = {0.5 * ev, 0.5 * ee};
+        const int idx[2] = {A_VDW, A_ELC};
+        block_acc<2>(v, a.acc, idx, false);
     }
 }
 
 // ---- pair kernel, FP64 (parity path) ---------------------------------------
-template <bool ENE, bool VIR>
+template <bool ENE>
 __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict__ xq, PairArgs a,
                                                       const double2* __restrict__ lj_g,
                                                       const double4* __restrict__ spl_g,
@@ -198,63 +248,86 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
     double4* sf = smd;
     double4* sp = smd + a.nspl;
     double2* slj = (double2*)(smd + 2 * a.nspl);
+    __shared__ double4 si[8][8];
+    __shared__ int sti[8][8];
     for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) { sf[k] = spl_g[k]; sp[k] = spl_g[a.nspl + k]; }
     for (int k = threadIdx.x; k < a.ntyp * a.ntyp; k += blockDim.x) slj[k] = lj_g[k];
     __syncthreads();
     const double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
     const double B0 = 1.0 / L0, B1 = 1.0 / L1, B2 = 1.0 / L2;
-    const int lane = threadIdx.x & 31;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
+    const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
     double e_vdw = 0, e_elc = 0, vc[6] = {0, 0, 0, 0, 0, 0}, vl[6] = {0, 0, 0, 0, 0, 0};
-    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.n; s += nwarps) {
-        const double4 pi = xq[s];
-        const int ti = a.typ_s[s] * a.ntyp;
-        const int cnt = a.ncnt[s];
-        const int* row = a.nbr + (size_t)s * a.cap;
-        double fx = 0, fy = 0, fz = 0;
+    for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
+        __syncwarp();
+        if (lane < 8) {
+            si[warp][lane] = xq[8 * cl + lane];
+            sti[warp][lane] = a.typ_s[8 * cl + lane] * a.ntyp;
+        }
+        __syncwarp();
+        const int cnt = a.ccnt[cl];
+        const int* row = a.clist + (size_t)cl * a.ccap;
+        double f[8][3];
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) { f[ii][0] = 0; f[ii][1] = 0; f[ii][2] = 0; }
         for (int k = lane; k < cnt; k += 32) {
-            const int j = __ldg(row + k);
+            const unsigned e = (unsigned)__ldg(row + k);
+            const int j = (int)(e & 0xFFFFFFu);
             const double4 pj = xq[j];
-            double dx = pi.x - pj.x; dx = dx - L0 * round(dx * B0);
-            double dy = pi.y - pj.y; dy = dy - L1 * round(dy * B1);
-            double dz = pi.z - pj.z; dz = dz - L2 * round(dz * B2);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > a.rmax2) continue;
-            const double rinv2 = 1.0 / r2;
-            double fc = 0, fl = 0;
-            const double r = sqrt(r2);
-            if (r <= a.rrcut) {
-                const double qq = pi.w * pj.w;
-                const int idx = (int)(r / a.h);
-                const double d = r - (double)idx * a.h;
-                const double4 c = sf[idx];
-                fc = (c.x + d * (c.y + d * (c.z + d * c.w))) * qq;
-                if (ENE || VIR) {
-                    const double4 p = sp[idx];
-                    e_elc += 0.5 * ((p.x + d * (p.y + d * (p.z + d * p.w))) * qq);
+            const int tj = a.typ_s[j];
+            const unsigned m = e >> 24;
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii) {
+                if (!((m >> ii) & 1u)) continue;
+                const double4 pi = si[warp][ii];
+                double dx = pi.x - pj.x; dx = dx - L0 * round(dx * B0);
+                double dy = pi.y - pj.y; dy = dy - L1 * round(dy * B1);
+                double dz = pi.z - pj.z; dz = dz - L2 * round(dz * B2);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > a.rmax2) continue;
+                const double rinv2 = 1.0 / r2;
+                double fc = 0, fl = 0;
+                const double r = sqrt(r2);
+                if (r <= a.rrcut) {
+                    const double qq = pi.w * pj.w;
+                    const int idx = (int)(r / a.h);
+                    const double d = r - (double)idx * a.h;
+                    const double4 c = sf[idx];
+                    fc = (c.x + d * (c.y + d * (c.z + d * c.w))) * qq;
+                    if (ENE) {
+                        const double4 p = sp[idx];
+                        e_elc += 0.5 * ((p.x + d * (p.y + d * (p.z + d * p.w))) * qq);
+                    }
+                }
+                if (r2 <= a.rl2) {
+                    const double2 lp = slj[sti[warp][ii] + tj];
+                    const double t2 = rinv2 * lp.x;
+                    const double t6 = t2 * t2 * t2, t12 = t6 * t6;
+                    fl = 12.0 * lp.y * (t12 - t6) * rinv2;
+                    if (ENE) e_vdw += 0.5 * (lp.y * (t12 - 2.0 * t6));
+                }
+                f[ii][0] += fc * dx + fl * dx;
+                f[ii][1] += fc * dy + fl * dy;
+                f[ii][2] += fc * dz + fl * dz;
+                if (ENE) {
+                    vc[0] += fc * dx * dx; vc[1] += fc * dx * dy; vc[2] += fc * dx * dz;
+                    vc[3] += fc * dy * dy; vc[4] += fc * dy * dz; vc[5] += fc * dz * dz;
+                    vl[0] += fl * dx * dx; vl[1] += fl * dx * dy; vl[2] += fl * dx * dz;
+                    vl[3] += fl * dy * dy; vl[4] += fl * dy * dz; vl[5] += fl * dz * dz;
                 }
             }
-            if (r2 <= a.rl2) {
-                const double2 lp = slj[ti + a.typ_s[j]];
-                const double t2 = rinv2 * lp.x;
-                const double t6 = t2 * t2 * t2, t12 = t6 * t6;
-                fl = 12.0 * lp.y * (t12 - t6) * rinv2;
-                if (ENE || VIR) e_vdw += 0.5 * (lp.y * (t12 - 2.0 * t6));
-            }
-            fx += fc * dx + fl * dx;
-            fy += fc * dy + fl * dy;
-            fz += fc * dz + fl * dz;
-            if (VIR) {
-                vc[0] += fc * dx * dx; vc[1] += fc * dx * dy; vc[2] += fc * dx * dz;
-                vc[3] += fc * dy * dy; vc[4] += fc * dy * dz; vc[5] += fc * dz * dz;
-                vl[0] += fl * dx * dx; vl[1] += fl * dx * dy; vl[2] += fl * dx * dz;
-                vl[3] += fl * dy * dy; vl[4] += fl * dy * dz; vl[5] += fl * dz * dz;
+        }
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            const double fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
+            if (lane == ii) {
+                const int io = a.perm[8 * cl + ii];
+                if (io >= 0) force_add<false>(a.facc, io, fx, fy, fz);
             }
         }
-        fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
-        if (lane == 0) force_add<false>(a.facc, a.perm[s], fx, fy, fz);
     }
-    if (ENE || VIR) {
+    if (ENE) {
         double v[16] = {e_vdw, e_elc, e_elc,
                         0.5 * vc[0], 0.5 * vc[1], 0.5 * vc[2], 0.5 * vc[3], 0.5 * vc[4], 0.5 * vc[5],
                         0.5 * vl[0], 0.5 * vl[1], 0.5 * vl[2], 0.5 * vl[3], 0.5 * vl[4], 0.5 * vl[5],
@@ -265,9 +338,19 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
     }
 }
 
-pgk_status launch_pair(pgk_ctx* c, int group, bool ene, bool vir) {
+template <int MODE>
+static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
+    constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
+    size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
+    cudaFuncSetAttribute(k_pair_mixed<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_pair_mixed<MODE><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+}
+
+// vmode: PM_FORCE / PM_ENE / PM_TENS / PM_FULL (see above)
+pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
+    if (c->ncl <= 0) return PGK_OK;
     PairArgs a;
-    a.nbr = c->nbr; a.ncnt = c->ncnt; a.cap = c->cap; a.n = c->natom;
+    a.clist = c->clist; a.ccnt = c->ccnt; a.ccap = c->ccap; a.ncl = c->ncl;
     a.typ_s = c->typ_s; a.perm = c->perm; a.ntyp = c->ntyp; a.nspl = c->nspl;
     a.h = c->hspl; a.inv_h = 1.0 / c->hspl;
     a.rrcut = c->prm.rrcut;
@@ -276,31 +359,26 @@ pgk_status launch_pair(pgk_ctx* c, int group, bool ene, bool vir) {
     a.rmax2 = a.rr2 > a.rl2 ? a.rr2 : a.rl2;
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
-    int warps_per_block = 8;
-    int blocks = c->nsm * 4;
-    long long need = (c->natom + warps_per_block - 1) / warps_per_block;
+    const int warps_per_block = 8;
+    int blocks = c->nsm * (c->mixed() ? 3 : 2);
+    long long need = (c->ncl + warps_per_block - 1) / warps_per_block;
     if (blocks > need) blocks = (int)need;
     if (blocks < 1) blocks = 1;
     if (c->mixed()) {
-        size_t sm = (size_t)((ene || vir) ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-        if (vir) {
-            cudaFuncSetAttribute(k_pair_mixed<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_pair_mixed<true, true><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
-        } else if (ene) {
-            cudaFuncSetAttribute(k_pair_mixed<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_pair_mixed<true, false><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
-        } else {
-            cudaFuncSetAttribute(k_pair_mixed<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_pair_mixed<false, false><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+        switch (vmode) {
+            case PM_FULL: pair_mixed_launch<PM_FULL>(c, a, blocks); break;
+            case PM_TENS: pair_mixed_launch<PM_TENS>(c, a, blocks); break;
+            case PM_ENE: pair_mixed_launch<PM_ENE>(c, a, blocks); break;
+            default: pair_mixed_launch<PM_FORCE>(c, a, blocks); break;
         }
     } else {
         size_t sm = (size_t)2 * c->nspl * sizeof(double4) + c->ntyp * c->ntyp * sizeof(double2);
-        if (vir || ene) {
-            cudaFuncSetAttribute(k_pair_fp64<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_pair_fp64<true, true><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
+        if (vmode != PM_FORCE) {
+            cudaFuncSetAttribute(k_pair_fp64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_pair_fp64<true><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
         } else {
-            cudaFuncSetAttribute(k_pair_fp64<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-            k_pair_fp64<false, false><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
+            cudaFuncSetAttribute(k_pair_fp64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_pair_fp64<false><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
         }
     }
     PGK_LAUNCHED(c);
@@ -308,115 +386,50 @@ pgk_status launch_pair(pgk_ctx* c, int group, bool ene, bool vir) {
     return PGK_OK;
 }
 
-// ---- excluded-pair correction (ewaldr.F90:756-826): thread per pair -------------
-template <bool MIXED>
-__global__ void k_excl(const double* __restrict__ pos, const double* __restrict__ chrg,
-                       const int2* __restrict__ pairs, int npair, const double4* __restrict__ spl64,
-                       const float4* __restrict__ spl32, int nspl, double h, const DynState* __restrict__ dyn,
-                       void* facc, long long* acc, int want) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    double e = 0, t[6] = {0, 0, 0, 0, 0, 0};
-    if (k < npair) {
-        int i = pairs[k].x, j = pairs[k].y;
-        double r[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double v = pos[3 * i + d] - pos[3 * j + d];
-            r[d] = v - dyn->box[d] * round(v * dyn->boxinv[d]);
-        }
-        double qq = chrg[i] * chrg[j];
-        double fx, fy, fz, pot = 0.0;
-        if (MIXED) {
-            float rx = (float)r[0], ry = (float)r[1], rz = (float)r[2];
-            float rr = sqrtf(rx * rx + ry * ry + rz * rz);
-            float hf = (float)h;
-            int idx = (int)(rr / hf);
-            float fs = 0.f, ps = 0.f;
-            if (idx < nspl - 1) {
-                float d = rr - (float)idx * hf;
-                float4 c = spl32[2 * nspl + idx];
-                fs = -(c.x + d * (c.y + d * (c.z + d * c.w))) * (float)qq;
-                float4 p = spl32[3 * nspl + idx];
-                ps = (p.x + d * (p.y + d * (p.z + d * p.w))) * (float)qq;
-            }
-            fx = (double)(fs * rx); fy = (double)(fs * ry); fz = (double)(fs * rz);
-            pot = ps;
-        } else {
-            double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-            double fs = 0.0;
-            if (rr < h * (double)(nspl - 1)) {
-                int idx = (int)(rr / h);
-                double d = rr - (double)idx * h;
-                double4 c = spl64[2 * nspl + idx];
-                fs = -(c.x + d * (c.y + d * (c.z + d * c.w))) * qq;
-                double4 p = spl64[3 * nspl + idx];
-                pot = (p.x + d * (p.y + d * (p.z + d * p.w))) * qq;
-            }
-            fx = fs * r[0]; fy = fs * r[1]; fz = fs * r[2];
-        }
-        force_add<MIXED>(facc, i, fx, fy, fz);
-        force_add<MIXED>(facc, j, -fx, -fy, -fz);
-        e = pot;
-        t[0] = fx * r[0]; t[1] = fx * r[1]; t[2] = fx * r[2];
-        t[3] = fy * r[1]; t[4] = fy * r[2]; t[5] = fz * r[2];
-    }
-    if (want) {
-        double v[8] = {-e, -e, t[0], t[1], t[2], t[3], t[4], t[5]};
-        const int idx[8] = {A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
-        block_acc<8>(v, acc, idx, !MIXED);
-    }
-}
-
-pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir) {
-    if (c->nexpair == 0) return PGK_OK;
-    int nb = (c->nexpair + 255) / 256;
-    long long* acc = c->acc + (size_t)group * NACC;
-    if (c->mixed())
-        k_excl<true><<<nb, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64, c->spl32, c->nspl,
-                                            c->hspl, c->dyn, c->facc[group], acc, ene || vir);
-    else
-        k_excl<false><<<nb, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64, c->spl32, c->nspl,
-                                             c->hspl, c->dyn, c->facc[group], acc, ene || vir);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
-// ---- diagnostic: number of unique pairs inside the interaction cutoff --------
-// (the algorithmic work unit of the pair kernel; run outside any timed region)
-__global__ void k_count_pairs(const double* __restrict__ pos_s, const int* __restrict__ nbr,
-                              const int* __restrict__ ncnt, int cap, int n, double rmax2,
+// ---- diagnostic: unique pairs inside the interaction cutoff, list entries ----
+// (the algorithmic work units of the pair kernel; run outside any timed region)
+__global__ void k_count_pairs(const double* __restrict__ pos_s, const int* __restrict__ clist,
+                              const int* __restrict__ ccnt, int ccap, int ncl, double rmax2,
                               const DynState* __restrict__ dyn, unsigned long long* out) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    unsigned long long c = 0;
+    int cl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cl >= ncl) return;
+    unsigned long long np = 0, bits = 0;
     const double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
-    for (int k = 0; k < ncnt[s]; ++k) {
-        int t = nbr[(size_t)s * cap + k];
-        if (t <= s) continue;
-        double dx = pos_s[3 * s] - pos_s[3 * t]; dx -= L0 * round(dx / L0);
-        double dy = pos_s[3 * s + 1] - pos_s[3 * t + 1]; dy -= L1 * round(dy / L1);
-        double dz = pos_s[3 * s + 2] - pos_s[3 * t + 2]; dz -= L2 * round(dz / L2);
-        if (dx * dx + dy * dy + dz * dz <= rmax2) ++c;
+    const int cnt = ccnt[cl];
+    for (int k = 0; k < cnt; ++k) {
+        unsigned e = (unsigned)clist[(size_t)cl * ccap + k];
+        int t = (int)(e & 0xFFFFFFu);
+        for (int ii = 0; ii < 8; ++ii) {
+            if (!((e >> (24 + ii)) & 1u)) continue;
+            ++bits;
+            int s = 8 * cl + ii;
+            if (t <= s) continue;
+            double dx = pos_s[3 * s] - pos_s[3 * t]; dx -= L0 * round(dx / L0);
+            double dy = pos_s[3 * s + 1] - pos_s[3 * t + 1]; dy -= L1 * round(dy / L1);
+            double dz = pos_s[3 * s + 2] - pos_s[3 * t + 2]; dz -= L2 * round(dz / L2);
+            if (dx * dx + dy * dy + dz * dz <= rmax2) ++np;
+        }
     }
-    atomicAdd(out, c);
+    atomicAdd(out, np);
+    atomicAdd(out + 1, bits);
+    atomicAdd(out + 2, (unsigned long long)cnt);
 }
 
-pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries) {
-    unsigned long long* d = c->counters + 2;
-    PGK_CUDA(c, cudaMemsetAsync(d, 0, sizeof(unsigned long long), c->st));
+// npair: unique pairs inside max(rrcut, rcut); nbits: list pairs, both
+// directions (pair evaluations); nentries: (cluster, j) entries read
+pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long long* nbits) {
+    if (c->ncl <= 0) { *npair = 0; *nentries = 0; if (nbits) *nbits = 0; return PGK_OK; }
+    unsigned long long* d = c->counters + 4;
+    PGK_CUDA(c, cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), c->st));
     double rr2 = c->prm.rrcut * c->prm.rrcut, rl2 = c->prm.rcut * c->prm.rcut;
-    k_count_pairs<<<(c->natom + 255) / 256, 256, 0, c->st>>>(c->pos_s, c->nbr, c->ncnt, c->cap, c->natom,
-                                                              rr2 > rl2 ? rr2 : rl2, c->dyn, d);
+    k_count_pairs<<<(c->ncl + 127) / 128, 128, 0, c->st>>>(c->pos_s, c->clist, c->ccnt, c->ccap, c->ncl,
+                                                            rr2 > rl2 ? rr2 : rl2, c->dyn, d);
     PGK_CUDA(c, cudaGetLastError());
-    unsigned long long h = 0;
-    PGK_CUDA(c, cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c->st));
-    std::vector<int> cnt(c->natom);
-    PGK_CUDA(c, cudaMemcpyAsync(cnt.data(), c->ncnt, sizeof(int) * c->natom, cudaMemcpyDeviceToHost, c->st));
+    unsigned long long h[3] = {0, 0, 0};
+    PGK_CUDA(c, cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaStreamSynchronize(c->st));
-    long long e = 0;
-    for (int v : cnt) e += v;
-    *npair = (long long)h;
-    *nentries = e;
+    *npair = (long long)h[0];
+    *nentries = (long long)h[2];
+    if (nbits) *nbits = (long long)h[1];
     return PGK_OK;
 }

@@ -52,11 +52,16 @@ __device__ __forceinline__ void frac_coord(double x, double recip, int K, int& b
     w = fr - trunc(fr);
 }
 
+// order (may be NULL): atoms in cell-sorted order, so that neighbouring
+// threads touch neighbouring grid points (L2 locality of the atomics)
 template <bool MIXED, int P>
 __global__ void k_spread(const double* __restrict__ pos, const double* __restrict__ chrg, int n,
-                         const DynState* __restrict__ dyn, int K1, int K2, int K3, void* __restrict__ qacc) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n) return;
+                         const DynState* __restrict__ dyn, int K1, int K2, int K3, void* __restrict__ qacc,
+                         const int* __restrict__ order) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int a = order ? order[t] : t;
+    if (a < 0) return;   // padding slot of the cell-sorted order
     double th[3][P], dth[3][P];
     int base[3];
     const int Kd[3] = {K1, K2, K3};
@@ -153,19 +158,141 @@ __device__ __forceinline__ void dft_r(T2* v, int R, T sg) {
     }
 }
 
+// radix chain of a length (4s first, then 2, 3, 5), usable at compile time
+__host__ __device__ constexpr int pick_radix(int m) {
+    return m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 3 == 0 ? 3 : (m % 5 == 0 ? 5 : 0)));
+}
+__host__ __device__ constexpr int stage_radix(int n, int s) {
+    int m = n;
+    for (int k = 0; k < s; ++k) m /= pick_radix(m);
+    return pick_radix(m);
+}
+__host__ __device__ constexpr int stage_ns(int n, int s) {
+    int m = n, ns = 1;
+    for (int k = 0; k < s; ++k) { int r = pick_radix(m); ns *= r; m /= r; }
+    return ns;
+}
+__host__ __device__ constexpr int nstages(int n) {
+    int c = 0;
+    while (n > 1) { n /= pick_radix(n); ++c; }
+    return c;
+}
+
+// one Stockham stage on P pencils of length n held in shared memory
+template <typename T, typename T2>
+__device__ __forceinline__ void fft_stage(const T2* __restrict__ src, T2* __restrict__ dst, int P, int n, int R,
+                                          int Ns, const T2* __restrict__ tw, T sg) {
+    const int nr = n / R;
+    const int twstep = n / (Ns * R);
+    for (int w = threadIdx.x; w < P * nr; w += blockDim.x) {
+        int p = w / nr, j = w - p * nr;
+        int k = j % Ns;
+        T2 v[5];
+        const T2* sp = src + p * n;
+#pragma unroll
+        for (int r = 0; r < 5; ++r)
+            if (r < R) {
+                T2 x = sp[j + r * nr];
+                if (r > 0 && k > 0) {
+                    T2 t = tw[r * k * twstep];
+                    if (sg > 0) t.y = -t.y;
+                    x = cmul(x, t);
+                }
+                v[r] = x;
+            }
+        dft_r<T, T2>(v, R, sg);
+        int o = (j / Ns) * Ns * R + k;
+        T2* dp = dst + p * n;
+#pragma unroll
+        for (int r = 0; r < 5; ++r)
+            if (r < R) dp[o + r * Ns] = v[r];
+    }
+}
+
+// all stages; NC > 0 makes the length and radix chain compile-time constants
+template <typename T, typename T2, int NC, int S = 0>
+struct FftStages {
+    static __device__ __forceinline__ void run(T2*& src, T2*& dst, int P, int n, const FftDev& plan, T sg) {
+        if (NC == 0) {
+            int Ns = 1;
+            for (int s = 0; s < plan.nstage; ++s) {
+                fft_stage<T, T2>(src, dst, P, n, plan.radix[s], Ns, (const T2*)plan.tw, sg);
+                __syncthreads();
+                T2* t = src; src = dst; dst = t;
+                Ns *= plan.radix[s];
+            }
+        } else if (S < nstages(NC)) {
+            fft_stage<T, T2>(src, dst, P, NC, stage_radix(NC, S), stage_ns(NC, S), (const T2*)plan.tw, sg);
+            __syncthreads();
+            T2* t = src; src = dst; dst = t;
+            FftStages<T, T2, NC, (S < 12 ? S + 1 : S)>::run(src, dst, P, n, plan, sg);
+        }
+    }
+};
+template <typename T, typename T2, int NC>
+struct FftStages<T, T2, NC, 12> {
+    static __device__ __forceinline__ void run(T2*&, T2*&, int, int, const FftDev&, T) {}
+};
+
+// influence function of one grid point (scalar_sum, fft_pme.F90:590-680)
+struct ConvArgs {
+    const double* bsp; double alpha, netchrgsq; int corr; long long* acc; int want;
+};
+
+__device__ __forceinline__ double conv_point(int k1, int k2, int k3, int K1, int K2, int K3, double s2,
+                                             const ConvArgs& ca, const DynState* __restrict__ dyn, double& en,
+                                             double& vs, double* vt) {
+    const double pi = 3.14159265358979323846;
+    int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
+    int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
+    int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
+    int m1 = k1 < nf1 ? k1 : k1 - K1;
+    int m2 = k2 < nf2 ? k2 : k2 - K2;
+    int m3 = k3 < nf3 ? k3 : k3 - K3;
+    double h1 = dyn->boxinv[0] * m1, h2 = dyn->boxinv[1] * m2, h3 = dyn->boxinv[2] * m3;
+    double msq = h1 * h1 + h2 * h2 + h3 * h3;
+    if (msq > dyn->rkcut * dyn->rkcut) return 0.0;
+    const double fac = pi * pi / (ca.alpha * ca.alpha);
+    const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    double denom = pi * vol * ca.bsp[k1] * ca.bsp[K1 + k2] * ca.bsp[K1 + K2 + k3] * msq;
+    double ex = exp(-fac * msq);
+    double eterm = ex / denom;
+    if (ca.want) {
+        double vterm = 2.0 * (fac * msq + 1.0) / msq;
+        double es = eterm * s2;
+        en += es;
+        if (ca.corr) {
+            double e2 = ex * ca.netchrgsq / (pi * vol * msq);
+            vs += e2 * (-1.0 + 2.0 * fac * msq);
+            es -= e2;
+        }
+        vt[0] += es * (vterm * h1 * h1 - 1.0);
+        vt[1] += es * (vterm * h1 * h2);
+        vt[2] += es * (vterm * h1 * h3);
+        vt[3] += es * (vterm * h2 * h2 - 1.0);
+        vt[4] += es * (vterm * h2 * h3);
+        vt[5] += es * (vterm * h3 * h3 - 1.0);
+    }
+    return eterm;
+}
+
 // AXIS 0: pencils along x (contiguous); 1: along y; 2: along z.
 // SRC: 0 = complex grid in place, 1 = int64 fixed-point accumulation grid,
 //      2 = double accumulation grid (both real, first forward pass).
-template <typename T, int AXIS, int SRC>
+// CONV (AXIS 2 only): forward z transform, influence function (scalar_sum)
+//      and backward z transform in one pass over the grid.
+template <typename T, int AXIS, int SRC, int NC, bool CONV>
 __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ data, const void* __restrict__ acc,
-                                             int K1, int K2, int K3, FftDev plan, int P, T sg) {
+                                             int K1, int K2, int K3, FftDev plan, int P, T sg, ConvArgs ca,
+                                             const DynState* __restrict__ dyn) {
     typedef typename C2<T>::t T2;
     extern __shared__ unsigned char smraw[];
     T2* bufA = (T2*)smraw;
-    T2* bufB = bufA + P * plan.n;
-    const int n = plan.n;
+    const int n = NC > 0 ? NC : plan.n;
+    T2* bufB = bufA + P * n;
     size_t base;
     size_t stride;
+    int yz = 0;
     if (AXIS == 0) {
         base = (size_t)blockIdx.x * P * K1;
         stride = 1;
@@ -179,16 +306,18 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         int y = blockIdx.x / nxb, x0 = (blockIdx.x % nxb) * P;
         base = (size_t)x0 + (size_t)K1 * y;
         stride = (size_t)K1 * K2;
+        yz = y;
     }
     const int tot = P * n;
     const int npen_total = AXIS == 0 ? K2 * K3 : K1;
+    const int x0 = AXIS == 0 ? 0 : (int)(base % K1);
     for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
         int p, m;
-        if (AXIS == 0) { p = idx / n; m = idx % n; } else { m = idx / P; p = idx % P; }
-        int pg = AXIS == 0 ? blockIdx.x * P + p : (int)(base % K1) + p;
+        if (AXIS == 0) { p = idx / n; m = idx - p * n; } else { m = idx / P; p = idx - m * P; }
+        int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
         T2 v;
         v.x = 0; v.y = 0;
-        bool ok = AXIS == 0 ? pg < npen_total : pg < K1;
+        bool ok = pg < npen_total;
         if (ok) {
             size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
             if (SRC == 0) v = data[off];
@@ -198,47 +327,38 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         bufA[p * n + m] = v;
     }
     __syncthreads();
-    const T2* tw = (const T2*)plan.tw;
     T2* src = bufA;
     T2* dst = bufB;
-    int Ns = 1;
-    for (int s = 0; s < plan.nstage; ++s) {
-        const int R = plan.radix[s];
-        const int nr = n / R;
-        const int twstep = n / (Ns * R);
-        for (int w = threadIdx.x; w < P * nr; w += blockDim.x) {
-            int p = w / nr, j = w % nr;
-            int k = j % Ns;
-            T2 v[5];
-            const T2* sp = src + p * n;
-#pragma unroll
-            for (int r = 0; r < 5; ++r)
-                if (r < R) {
-                    T2 x = sp[j + r * nr];
-                    if (r > 0 && k > 0) {
-                        T2 t = tw[r * k * twstep];
-                        if (sg > 0) t.y = -t.y;
-                        x = cmul(x, t);
-                    }
-                    v[r] = x;
-                }
-            dft_r<T, T2>(v, R, sg);
-            int o = (j / Ns) * Ns * R + k;
-            T2* dp = dst + p * n;
-#pragma unroll
-            for (int r = 0; r < 5; ++r)
-                if (r < R) dp[o + r * Ns] = v[r];
+    FftStages<T, T2, NC>::run(src, dst, P, n, plan, sg);
+    if (CONV) {
+        double en = 0, vs = 0, vt[6] = {0, 0, 0, 0, 0, 0};
+        for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+            int p = idx / n, m = idx - p * n;
+            int k1 = x0 + p;
+            if (k1 >= K1) continue;
+            if (k1 == 0 && yz == 0 && m == 0) continue;   // m = 0 is skipped by scalar_sum
+            T2 v = src[idx];
+            double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+            double et = conv_point(k1, yz, m, K1, K2, K3, s2, ca, dyn, en, vs, vt);
+            v.x = (T)((double)v.x * et);
+            v.y = (T)((double)v.y * et);
+            src[idx] = v;
         }
         __syncthreads();
-        T2* t = src; src = dst; dst = t;
-        Ns *= R;
+        FftStages<T, T2, NC>::run(src, dst, P, n, plan, -sg);
+        if (ca.want) {
+            double out[9] = {0.5 * en, 0.5 * en + 0.5 * vs, 0.5 * vs,
+                             -0.5 * vt[0], -0.5 * vt[1], -0.5 * vt[2], -0.5 * vt[3], -0.5 * vt[4], -0.5 * vt[5]};
+            const int idx9[9] = {A_EWK, A_VC, A_VSCA, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5,
+                                 A_VTC + 8};
+            block_acc<9>(out, ca.acc, idx9, sizeof(T) == 8);
+        }
     }
     for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
         int p, m;
-        if (AXIS == 0) { p = idx / n; m = idx % n; } else { m = idx / P; p = idx % P; }
-        int pg = AXIS == 0 ? blockIdx.x * P + p : (int)(base % K1) + p;
-        bool ok = AXIS == 0 ? pg < npen_total : pg < K1;
-        if (ok) {
+        if (AXIS == 0) { p = idx / n; m = idx - p * n; } else { m = idx / P; p = idx - m * P; }
+        int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
+        if (pg < npen_total) {
             size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
             data[off] = src[p * n + m];
         }
@@ -313,11 +433,13 @@ __global__ void k_scalar(typename C2<T>::t* __restrict__ q, int K1, int K2, int 
 template <bool MIXED, int P>
 __global__ void k_gather(const double* __restrict__ pos, const double* __restrict__ chrg, int n,
                          const DynState* __restrict__ dyn, int K1, int K2, int K3, const void* __restrict__ qc,
-                         void* facc) {
+                         void* facc, const int* __restrict__ order) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     typedef typename C2<T>::t T2;
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n) return;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int a = order ? order[t] : t;
+    if (a < 0) return;   // padding slot of the cell-sorted order
     T th[3][P], dth[3][P];
     int base[3];
     const int Kd[3] = {K1, K2, K3};
@@ -440,8 +562,16 @@ pgk_status spme_setup(pgk_ctx* c) {
     return PGK_OK;
 }
 
-template <typename T, int AXIS, int SRC>
-static pgk_status fft_pass(pgk_ctx* c, int sign) {
+template <typename T, int AXIS, int SRC, int NC, bool CONV>
+static void fft_launch(pgk_ctx* c, const FftDev& fd, int grid, int P, size_t sm, int sign, const ConvArgs& ca) {
+    typedef typename C2<T>::t T2;
+    cudaFuncSetAttribute(k_fft<T, AXIS, SRC, NC, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, c->qacc, c->K[0], c->K[1], c->K[2], fd, P,
+                                                            (T)sign, ca, c->dyn);
+}
+
+template <typename T, int AXIS, int SRC, bool CONV = false>
+static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) {
     typedef typename C2<T>::t T2;
     const FftPlan& pl = c->plan[AXIS];
     FftDev fd;
@@ -456,8 +586,15 @@ static pgk_status fft_pass(pgk_ctx* c, int sign) {
     else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3;
     else grid = ((K1 + P - 1) / P) * K2;
     size_t sm = (size_t)2 * P * pl.n * sizeof(T2);
-    cudaFuncSetAttribute(k_fft<T, AXIS, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_fft<T, AXIS, SRC><<<grid, 256, sm, c->st>>>((T2*)c->qc, c->qacc, K1, K2, K3, fd, P, (T)sign);
+    ConvArgs ca{};
+    if (cap) ca = *cap;
+    switch (pl.n) {   // compile-time lengths of the configured grids; others run the generic stage loop
+        case 32: fft_launch<T, AXIS, SRC, 32, CONV>(c, fd, grid, P, sm, sign, ca); break;
+        case 64: fft_launch<T, AXIS, SRC, 64, CONV>(c, fd, grid, P, sm, sign, ca); break;
+        case 128: fft_launch<T, AXIS, SRC, 128, CONV>(c, fd, grid, P, sm, sign, ca); break;
+        case 192: fft_launch<T, AXIS, SRC, 192, CONV>(c, fd, grid, P, sm, sign, ca); break;
+        default: fft_launch<T, AXIS, SRC, 0, CONV>(c, fd, grid, P, sm, sign, ca); break;
+    }
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -477,15 +614,32 @@ static pgk_status fft3(pgk_ctx* c, int sign, bool first) {
     return fft_pass<T, 2, 0>(c, sign);
 }
 
+// forward x, y; fused [forward z, influence function, backward z]; backward y, x
+template <typename T>
+static pgk_status fft_convolve(pgk_ctx* c, long long* acc, int want) {
+    pgk_status s;
+    ConvArgs ca;
+    ca.bsp = c->bsp; ca.alpha = c->prm.alpha; ca.netchrgsq = c->netchrgsq; ca.corr = c->prm.ifnetqcorrp;
+    ca.acc = acc; ca.want = want;
+    if (sizeof(T) == 4) s = fft_pass<T, 0, 1>(c, -1);
+    else s = fft_pass<T, 0, 2>(c, -1);
+    if (s) return s;
+    if ((s = fft_pass<T, 1, 0>(c, -1))) return s;
+    if ((s = fft_pass<T, 2, 0, true>(c, -1, &ca))) return s;
+    if ((s = fft_pass<T, 1, 0>(c, +1))) return s;
+    return fft_pass<T, 0, 0>(c, +1);
+}
+
 template <bool MIXED, int P>
 static void spread_gather(pgk_ctx* c, bool gather, int group) {
-    int n = c->natom;
+    const int* order = c->list_valid ? c->perm : nullptr;
+    int n = order ? c->npad : c->natom;     // sorted order runs over the padded slots
     if (!gather)
         k_spread<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
-                                                               c->K[2], c->qacc);
+                                                               c->K[2], c->qacc, order);
     else
         k_gather<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
-                                                               c->K[2], c->qc, c->facc[group]);
+                                                               c->K[2], c->qc, c->facc[group], order);
     PGK_LAUNCHED(c);
 }
 
@@ -510,22 +664,13 @@ pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir) {
     pgk_status s;
     long long* acc = c->acc + (size_t)group * NACC;
     int want = (ene || vir) ? 1 : 0;
-    int blocks = c->nsm * 4;
     if (c->mixed()) {
         if ((s = dispatch_sg<true>(c, false, group))) return s;
-        if ((s = fft3<float>(c, -1, true))) return s;
-        k_scalar<float><<<blocks, 256, 0, c->st>>>((float2*)c->qc, c->K[0], c->K[1], c->K[2], c->bsp, c->dyn,
-                                                   c->prm.alpha, c->netchrgsq, c->prm.ifnetqcorrp, acc, want);
-        PGK_LAUNCHED(c);
-        if ((s = fft3<float>(c, +1, false))) return s;
+        if ((s = fft_convolve<float>(c, acc, want))) return s;
         if ((s = dispatch_sg<true>(c, true, group))) return s;
     } else {
         if ((s = dispatch_sg<false>(c, false, group))) return s;
-        if ((s = fft3<double>(c, -1, true))) return s;
-        k_scalar<double><<<blocks, 256, 0, c->st>>>((double2*)c->qc, c->K[0], c->K[1], c->K[2], c->bsp, c->dyn,
-                                                    c->prm.alpha, c->netchrgsq, c->prm.ifnetqcorrp, acc, want);
-        PGK_LAUNCHED(c);
-        if ((s = fft3<double>(c, +1, false))) return s;
+        if ((s = fft_convolve<double>(c, acc, want))) return s;
         if ((s = dispatch_sg<false>(c, true, group))) return s;
     }
     PGK_CUDA(c, cudaGetLastError());
@@ -637,10 +782,14 @@ static cudaError_t noalloc_fft_pass(unsigned char* base, const FftPlan& pl, int 
     if (AXIS == 0) P = std::max(1, 1024 / K1);
     int grid = AXIS == 0 ? (K2 * K3 + P - 1) / P : ((K1 + P - 1) / P) * (AXIS == 1 ? K3 : K2);
     size_t sm = (size_t)2 * P * pl.n * sizeof(double2);
-    cudaError_t e = cudaFuncSetAttribute(k_fft<double, AXIS, SRC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(k_fft<double, AXIS, SRC, 0, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    k_fft<double, AXIS, SRC><<<grid, 256, sm, st>>>((double2*)(base + NOALLOC_OFF_QC), base + NOALLOC_OFF_QACC,
-                                                    K1, K2, K3, fd, P, (double)sign);
+    ConvArgs ca{};
+    k_fft<double, AXIS, SRC, 0, false><<<grid, 256, sm, st>>>((double2*)(base + NOALLOC_OFF_QC),
+                                                              base + NOALLOC_OFF_QACC, K1, K2, K3, fd, P,
+                                                              (double)sign, ca,
+                                                              (const DynState*)(base + NOALLOC_OFF_DYN));
     return cudaGetLastError();
 }
 
@@ -649,10 +798,11 @@ static void noalloc_sg(unsigned char* base, const double* pos, const double* chr
                        double* force, bool gather, cudaStream_t st) {
     const DynState* dyn = (const DynState*)(base + NOALLOC_OFF_DYN);
     if (!gather)
-        k_spread<false, P><<<(n + 127) / 128, 128, 0, st>>>(pos, chrg, n, dyn, K1, K2, K3, base + NOALLOC_OFF_QACC);
+        k_spread<false, P><<<(n + 127) / 128, 128, 0, st>>>(pos, chrg, n, dyn, K1, K2, K3, base + NOALLOC_OFF_QACC,
+                                                            nullptr);
     else
         k_gather<false, P><<<(n + 127) / 128, 128, 0, st>>>(pos, chrg, n, dyn, K1, K2, K3, base + NOALLOC_OFF_QC,
-                                                            force);
+                                                            force, nullptr);
 }
 
 static void noalloc_sg_order(int order, unsigned char* base, const double* pos, const double* chrg, int n, int K1,

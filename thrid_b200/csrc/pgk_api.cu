@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -73,20 +74,24 @@ pgk_status read_status(pgk_ctx* c) {
     return pgk_fail(c, PGK_E_CUDA, "unknown device status");
 }
 
-// one MTS group of calforce (calforce.F90:8-1073)
-pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir) {
+// one MTS group of calforce (calforce.F90:8-1073); tensor_only selects the
+// pair kernel's combined-tensor mode (anisotropic MTK steps without output)
+pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_only = false) {
     int g = flag == PGK_MTS_LONG ? 0 : 1;
     pgk_status s;
     if ((s = launch_zero_group(c, g))) return s;
     if (c->prm.mts_vdw == flag) {
         if (!c->list_valid && (s = launch_mklist(c))) return s;
         if ((s = launch_pack(c))) return s;
-        if ((s = launch_pair(c, g, ene, vir))) return s;
-        if ((s = launch_excl(c, g, ene, vir))) return s;
+        int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
+        if ((s = launch_pair(c, g, vmode))) return s;
     }
     if (c->prm.ifspme && c->prm.mts_ewk == flag)
         if ((s = launch_spme(c, g, ene, vir))) return s;
-    return launch_bonded(c, g, ene, vir, false);
+    int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
+               (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
+               (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (c->prm.mts_vdw == flag ? 32 : 0);
+    return launch_intra(c, g, mask, ene || vir);
 }
 
 double accv(const pgk_ctx* c, long long v) {
@@ -197,6 +202,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     if (!s || !p || !out) return PGK_E_INVALID;
     *out = nullptr;
     int n = s->natom;
+    if (n >= (1 << 25)) return PGK_E_INVALID;   // sort key packs the atom index in 25 bits
     if (n < 2 || !s->atmmass || !s->atmchrg || !s->atmindex || !s->index_excl || !s->list_excl)
         return PGK_E_INVALID;
     if (p->precision != PGK_PREC_FP64 && p->precision != PGK_PREC_MIXED) return PGK_E_INVALID;
@@ -223,6 +229,11 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         if (typ[i] < 0 || typ[i] >= s->ntyp) { pgk_free(c); return PGK_E_INVALID; }
     }
     TRY(upload(c, &c->mass, mass));
+    {
+        std::vector<double> im(n);
+        for (int i = 0; i < n; ++i) im[i] = 1.0 / mass[i];   // rattle.F90: one/atmmass(ib)
+        TRY(upload(c, &c->invmass, im));
+    }
     TRY(upload(c, &c->chrg, chrg));
     TRY(upload(c, &c->typ, typ));
     double q = 0, q2 = 0;
@@ -284,6 +295,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         TRY(upload(c, &c->spl64, s64));
         TRY(upload(c, &c->spl32, s32));
     }
+    HostTerms ht;
+    std::vector<int> mol_idx_h, mol_list_h;
     // ---- exclusions ----
     {
         std::vector<std::vector<int>> part(n);
@@ -312,8 +325,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         if (lst.empty()) lst.push_back(-1);
         TRY(upload(c, &c->exs_idx, idx));
         TRY(upload(c, &c->exs_list, lst));
-        c->nexpair = (int)pairs.size();
-        TRY(upload(c, &c->expair, pairs));
+        ht.ex = pairs;
     }
     // ---- molecules ----
     {
@@ -324,64 +336,52 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
             for (int k = 0; k < mi[s->nmole]; ++k) ml.push_back(s->molept_list[k] - 1);
             TRY(upload(c, &c->mol_idx, mi));
             TRY(upload(c, &c->mol_list, ml));
+            mol_idx_h = mi;
+            mol_list_h = ml;
         } else {
             c->nmole = 0;
         }
     }
-    // ---- bonded ----
+    // ---- bonded (uploaded in chunk order by bonded_setup) ----
     {
-        std::vector<int2> bij; std::vector<double2> bp;
         for (int k = 0; k < s->nbond; ++k) {
-            bij.push_back(make_int2(s->ibond[k] - 1, s->jbond[k] - 1));
-            bp.push_back(make_double2(s->para_cbond[k], s->para_eqbond[k]));
+            ht.bij.push_back(make_int2(s->ibond[k] - 1, s->jbond[k] - 1));
+            ht.bp.push_back(make_double2(s->para_cbond[k], s->para_eqbond[k]));
         }
-        c->nbond = s->nbond;
-        TRY(upload(c, &c->bond_ij, bij)); TRY(upload(c, &c->bond_p, bp));
-        std::vector<int4> aijk; std::vector<double2> ap;
         for (int k = 0; k < s->nangl; ++k) {
-            aijk.push_back(make_int4(s->iangl[k] - 1, s->jangl[k] - 1, s->kangl[k] - 1, 0));
-            ap.push_back(make_double2(s->para_cangl[k], s->para_eqangl[k]));
+            ht.aijk.push_back(make_int4(s->iangl[k] - 1, s->jangl[k] - 1, s->kangl[k] - 1, 0));
+            ht.ap.push_back(make_double2(s->para_cangl[k], s->para_eqangl[k]));
         }
-        c->nangl = s->nangl;
-        TRY(upload(c, &c->angl_ijk, aijk)); TRY(upload(c, &c->angl_p, ap));
-        std::vector<int4> tij; std::vector<double4> tp;
-        std::vector<int2> p14; std::vector<double2> f14;
         for (int k = 0; k < s->ntors; ++k) {
-            tij.push_back(make_int4(s->itors[k] - 1, s->jtors[k] - 1, s->ktors[k] - 1, s->ltors[k] - 1));
-            tp.push_back(make_double4(s->para_barhig[k] / (double)s->para_divfac[k], s->para_phsang[k],
-                                      std::fabs(s->para_period[k]), std::cos(s->para_phsang[k])));
-            // caltors divides inside the force term as barhig*period/divfac; same value
+            ht.tij.push_back(make_int4(s->itors[k] - 1, s->jtors[k] - 1, s->ktors[k] - 1, s->ltors[k] - 1));
+            // caltors: barhig/divfac, phase, |period|, cos(phase) (calijkl force uses cos(phsang))
+            ht.tp.push_back(make_double4(s->para_barhig[k] / (double)s->para_divfac[k], s->para_phsang[k],
+                                         std::fabs(s->para_period[k]), std::cos(s->para_phsang[k])));
         }
-        c->ntors = s->ntors;
-        TRY(upload(c, &c->tors_ijkl, tij)); TRY(upload(c, &c->tors_p, tp));
-        std::vector<int4> rij; std::vector<double> rc;
         for (int k = 0; k < s->ntorsrb; ++k) {
-            rij.push_back(make_int4(s->itorsrb[k] - 1, s->jtorsrb[k] - 1, s->ktorsrb[k] - 1, s->ltorsrb[k] - 1));
-            for (int qq = 0; qq < 6; ++qq) rc.push_back(s->para_barhigrb[6 * k + qq]);
+            ht.rij.push_back(make_int4(s->itorsrb[k] - 1, s->jtorsrb[k] - 1, s->ktorsrb[k] - 1, s->ltorsrb[k] - 1));
+            for (int qq = 0; qq < 6; ++qq) ht.rc.push_back(s->para_barhigrb[6 * k + qq]);
         }
-        c->ntorsrb = s->ntorsrb;
-        TRY(upload(c, &c->rb_ijkl, rij)); TRY(upload(c, &c->rb_c, rc));
         // 1-4 pairs in calnon14p order: periodic torsions, then RB torsions
         if (s->ifcalnonb14)
             for (int k = 0; k < s->ntors; ++k) {
                 if (!s->ifcalnonb14[k]) continue;
                 int i = s->itors[k] - 1, j = s->ltors[k] - 1;
                 if (i == j) continue;
-                p14.push_back(make_int2(i, j));
-                f14.push_back(make_double2(1.0 / s->para_divfac_elc[k] * s->ring14[k],
-                                           1.0 / s->para_divfac_vdw[k] * s->ring14[k]));
+                ht.p14.push_back(make_int2(i, j));
+                ht.f14.push_back(make_double2(1.0 / s->para_divfac_elc[k] * s->ring14[k],
+                                              1.0 / s->para_divfac_vdw[k] * s->ring14[k]));
             }
         if (s->ifcalnonb14_rb)
             for (int k = 0; k < s->ntorsrb; ++k) {
                 if (!s->ifcalnonb14_rb[k]) continue;
                 int i = s->itorsrb[k] - 1, j = s->ltorsrb[k] - 1;
                 if (i == j) continue;
-                p14.push_back(make_int2(i, j));
-                f14.push_back(make_double2(1.0 / s->para_divfac_elcrb[k] * s->ring14_rb[k],
-                                           1.0 / s->para_divfac_vdwrb[k] * s->ring14_rb[k]));
+                ht.p14.push_back(make_int2(i, j));
+                ht.f14.push_back(make_double2(1.0 / s->para_divfac_elcrb[k] * s->ring14_rb[k],
+                                              1.0 / s->para_divfac_vdwrb[k] * s->ring14_rb[k]));
             }
-        c->n14 = (int)p14.size();
-        TRY(upload(c, &c->p14_ij, p14)); TRY(upload(c, &c->p14_f, f14));
+        TRY(bonded_setup(c, ht, mol_idx_h, mol_list_h));
     }
     // ---- constraints ----
     {
@@ -396,28 +396,38 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
                 cij.push_back(make_int2(s->iconst[k] - 1, s->jconst[k] - 1));
                 cd.push_back(s->dconst[k]);
             }
+            std::vector<int2> span(s->nconst);
+            for (int g = 0; g < s->nconst; ++g) {
+                int lo = n, hi = -1;
+                for (int k = gi[g]; k < gi[g + 1]; ++k) {
+                    int2 p2 = cij[gl[k]];
+                    lo = std::min(lo, std::min(p2.x, p2.y));
+                    hi = std::max(hi, std::max(p2.x, p2.y));
+                }
+                span[g] = hi >= lo ? make_int2(lo, hi - lo + 1) : make_int2(0, 0);
+            }
             TRY(upload(c, &c->cg_idx, gi)); TRY(upload(c, &c->cg_list, gl));
             TRY(upload(c, &c->c_ij, cij)); TRY(upload(c, &c->c_d, cd));
+            TRY(upload(c, &c->cg_span, span));
         }
     }
-    // ---- pair list buffers ----
+    // ---- pair list buffers (sorted slots and cluster rows grow at list time) ----
     {
         double vol = p->xcel * p->ycel * p->zcel;
         double rb = p->rcut_book;
-        double expect = (double)n / vol * 4.0 / 3.0 * std::acos(-1.0) * rb * rb * rb;
-        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(1.25 * expect + 96);
+        // partners of an 8-atom cluster: the sphere of radius rcut_book swept
+        // over the cluster's extent (~ 2 A); rows regrow on overflow
+        double rs = rb + 2.0;
+        double expect = (double)n / vol * 4.0 / 3.0 * std::acos(-1.0) * rs * rs * rs;
+        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(1.3 * expect + 128);
         cap = std::min(cap, ((n + 31) / 32) * 32);
         cap = ((cap + 31) / 32) * 32;
-        c->cap = std::max(cap, 32);
-        if (cudaMalloc(&c->nbr, (size_t)n * c->cap * sizeof(int)) || cudaMalloc(&c->ncnt, n * sizeof(int)) ||
-            cudaMalloc(&c->perm, n * sizeof(int)) || cudaMalloc(&c->iperm, n * sizeof(int)) ||
-            cudaMalloc(&c->cell_of, n * sizeof(int)) || cudaMalloc(&c->pos_s, n3 * 8) ||
-            cudaMalloc(&c->typ_s, n * sizeof(int)) || cudaMalloc(&c->counters, 4 * sizeof(unsigned long long))) {
+        c->ccap = std::max(cap, 32);
+        if (cudaMalloc(&c->iperm, n * sizeof(int)) || cudaMalloc(&c->cell_of, n * sizeof(int)) ||
+            cudaMalloc(&c->subkey, n * sizeof(int)) || cudaMalloc(&c->counters, 8 * sizeof(unsigned long long))) {
             pgk_free(c);
             return PGK_E_NOMEM;
         }
-        if (c->mixed()) { if (cudaMalloc(&c->xq, n * sizeof(int4))) { pgk_free(c); return PGK_E_NOMEM; } }
-        else { if (cudaMalloc(&c->xq64, n * sizeof(double4))) { pgk_free(c); return PGK_E_NOMEM; } }
     }
     // ---- SPME ----
     if (p->ifspme) TRY(spme_setup(c));
@@ -452,9 +462,11 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list,
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
-                    c->cell_of, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->nbr,
-                    c->ncnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
-                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout};
+                    c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
+                    c->ccnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
+                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->chunk_atom, c->chunk_term, c->cg_span, c->chunk_slot, c->inc_start, c->inc_slot,
+                    c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
+                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -539,7 +551,9 @@ pgk_status pgk_ewaldr(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v
     bool want = e || v;
     if ((s = launch_zero_group(c, 0))) return s;
     if (!c->list_valid && (s = launch_mklist(c))) return s;
-    if ((s = launch_pack(c)) || (s = launch_pair(c, 0, want, want)) || (s = launch_excl(c, 0, want, want))) return s;
+    if ((s = launch_pack(c)) || (s = launch_pair(c, 0, want ? PM_FULL : PM_FORCE)) ||
+        (s = launch_intra(c, 0, 32, want)))
+        return s;
     if (force && (s = force_to_host(c, 0, force, true))) return s;
     if (want && (s = read_acc(c, 1, e, v, false))) return s;
     return read_status(c);
@@ -560,7 +574,7 @@ pgk_status pgk_calbonded(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials
     if (!c) return PGK_E_INVALID;
     pgk_status s;
     bool want = e || v;
-    if ((s = launch_zero_group(c, 0)) || (s = launch_bonded(c, 0, want, want, true))) return s;
+    if ((s = launch_zero_group(c, 0)) || (s = launch_intra(c, 0, 31, want))) return s;
     if (force && (s = force_to_host(c, 0, force, true))) return s;
     if (want && (s = read_acc(c, 1, e, v, false))) return s;
     return read_status(c);
@@ -624,7 +638,7 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
     PGK_CUDA(c, cudaEventCreate(&e1));
     auto one = [&]() -> pgk_status {
         switch (which) {
-            case 0: return launch_pair(c, 0, true, true);
+            case 0: return launch_pair(c, 0, PM_TENS);
             case 1: return spme_bench(c, 1);
             case 2: return spme_bench(c, 2);
             case 3: return spme_bench(c, 3);
@@ -649,30 +663,44 @@ void* pgk_stream(const pgk_ctx* c) { return c ? (void*)c->st : nullptr; }
 }  // extern "C"
 
 // ---- stage drivers ---------------------------------------------------------------
-static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* eo) {
+// kind: 0 NVE (moldyn.F90), 1 NHC (moldyn_nhc.F90), 2 MTK (moldyn_mtk.F90),
+// 3 NVE + region Langevin + heat flux (moldyn_hf.F90); hf records go to the
+// device buffer c->hf_rec (kind 3), *nrec counts them
+static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* eo,
+                         long long* nrec = nullptr) {
     if (!c || !md || md->nstep_short < 1 || md->dt_long_cal <= 0) return PGK_E_INVALID;
-    if (kind >= 1 && (md->mchain < 2 || md->mchain > 8 || md->nyosh < 1 || md->nyosh > 8 || md->next < 1))
+    if (kind == 3 && !c->hf_set) return pgk_fail(c, PGK_E_INVALID, "pgk_set_hf has not been called");
+    if ((kind == 1 || kind == 2) && (md->mchain < 2 || md->mchain > 8 || md->nyosh < 1 || md->nyosh > 8 || md->next < 1))
         return pgk_fail(c, PGK_E_INVALID, "chain parameters");
     const int nb = c->prm.nstep_book > 0 ? c->prm.nstep_book : 1;
     const double dts = md->dt_long_cal / (double)md->nstep_short;
     const bool rattle = md->ifrattle && c->ncgroup > 0;
     const bool mtk = kind == 2;
     const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);
+    const bool hfdrv = kind == 3;
+    const bool lt = hfdrv && c->hfp.nlangeregion > 0;
+    const int hfi = c->hfp.heatfinterval > 0 ? c->hfp.heatfinterval : 1;
+    const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
+    long long nr = 0;
     pgk_status s;
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
     for (int64_t step = ini; step <= end; ++step) {
         bool out = md->outinterval > 0 ? (step % md->outinterval == 0) : (step == end);
         bool ene = out && eo;
         bool vir = mtk;
+        bool tens = mtk && md->pcont_axis != PGK_PCONT_ISO && !ene;   // nhcpanisoint reads diag(pintt) only
         if (step % nb == 1 || nb == 1 || step == 0) RUN(launch_transcor(c));
         if (step % nb == 0 || nb == 1) RUN(launch_mklist(c));
+        const bool hfs = hfdrv && per > 0 && step > 0 && (hfi == 1 || step % hfi == 1);
         if (step == 0) {
-            RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir));
-            RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir));
+            if (lt) RUN(launch_lt_regist(c));
+            RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
+            RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
         } else {
-            if (kind >= 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-            RUN(launch_coeffs(c, kind, *md, 0));
+            if (lt) RUN(launch_langevin(c, md->dt_long_cal, step, true));
+            if (kind == 1 || kind == 2) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
+            RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
             for (int is = 1; is <= md->nstep_short; ++is) {
                 bool last = is == md->nstep_short;
                 if (is == 1) RUN(launch_kick_long(c));
@@ -680,10 +708,11 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                 RUN(launch_drift(c, rattle));
                 if (mtk) RUN(launch_box_update(c, kind, *md));
                 if (rattle) RUN(launch_rattle_pos(c, md->eps_rattle, dts, mtk));
-                RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir));
+                RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
                 if (last) {
                     if (mtk && c->prm.mts_ewk == PGK_MTS_LONG) RUN(launch_rkcut(c));
-                    RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir));
+                    RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
+                    if (hfs) RUN(launch_hf_atm(c));
                 }
                 RUN(launch_kick_short(c));
                 if (last) RUN(launch_kick_long(c));
@@ -691,10 +720,16 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             }
             if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); RUN(launch_chain(c, chain_kind, *md)); }
+            if (lt) { RUN(launch_lt_regist(c)); RUN(launch_langevin(c, md->dt_long_cal, step, false)); }
+            if (hfs) {
+                if (nr < c->hf_rec_cap) RUN(launch_heatf(c, c->hf_rec + nr * per));
+                ++nr;
+            }
         }
         if (ene) RUN(read_acc(c, 3, eo, nullptr, true));
     }
 #undef RUN
+    if (nrec) *nrec = nr;
     return read_status(c);
 }
 
@@ -707,5 +742,73 @@ pgk_status pgk_moldyn_nhc(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdpara
 }
 pgk_status pgk_moldyn_mtk(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e) {
     return run_md(c, 2, ini, end, md, e);
+}
+
+pgk_status pgk_set_hf(pgk_ctx* c, const pgk_hfparams* hf) {
+    if (!c || !hf) return PGK_E_INVALID;
+    return hf_setup(c, hf);
+}
+
+pgk_status pgk_moldyn_hf(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e,
+                         double* hf_out, int64_t cap_records, int64_t* nrecords) {
+    if (!c || !md || cap_records < 0) return PGK_E_INVALID;
+    if (!c->hf_set) return pgk_fail(c, PGK_E_INVALID, "pgk_set_hf has not been called");
+    const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
+    const int hfi = c->hfp.heatfinterval > 0 ? c->hfp.heatfinterval : 1;
+    long long expect = 0;
+    if (per > 0)
+        for (int64_t st = std::max<int64_t>(ini, 1); st <= end; ++st) expect += (hfi == 1 || st % hfi == 1) ? 1 : 0;
+    long long want = hf_out ? std::min<long long>(expect, cap_records) : 0;
+    if (per > 0 && want > c->hf_rec_cap) {
+        cudaFree(c->hf_rec);
+        c->hf_rec = nullptr;
+        PGK_CUDA(c, cudaMalloc(&c->hf_rec, sizeof(double) * per * want));
+        c->hf_rec_cap = want;
+    }
+    long long cap_save = c->hf_rec_cap;
+    c->hf_rec_cap = want;
+    long long nr = 0;
+    pgk_status s = run_md(c, 3, ini, end, md, e, &nr);
+    c->hf_rec_cap = std::max(cap_save, 1LL);
+    if (s) return s;
+    if (hf_out && want > 0)
+        PGK_CUDA(c, cudaMemcpy(hf_out, c->hf_rec, sizeof(double) * per * std::min(nr, want), cudaMemcpyDeviceToHost));
+    if (nrecords) *nrecords = nr;
+    return PGK_OK;
+}
+
+pgk_status pgk_calheatf(pgk_ctx* c, double* hf) {
+    if (!c || !hf) return PGK_E_INVALID;
+    if (!c->hf_set || c->hfp.nhfregion < 1) return pgk_fail(c, PGK_E_INVALID, "no heat-flux regions set");
+    pgk_status s;
+    if (!c->list_valid && (s = launch_mklist(c))) return s;
+    if ((s = launch_pack(c)) || (s = launch_hf_atm(c)) || (s = launch_heatf(c, c->hf_rec))) return s;
+    PGK_CUDA(c, cudaMemcpyAsync(hf, c->hf_rec, sizeof(double) * c->hfp.nhfregion * PGK_HF_NCOL,
+                                cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return read_status(c);
+}
+
+pgk_status pgk_get_hf_atm(pgk_ctx* c, double* pot_atm, double* viri_atm) {
+    if (!c) return PGK_E_INVALID;
+    if (!c->hf_set) return pgk_fail(c, PGK_E_INVALID, "pgk_set_hf has not been called");
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    size_t n = (size_t)c->natom;
+    if (pot_atm) PGK_CUDA(c, cudaMemcpy(pot_atm, c->hf_pot, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost));
+    if (viri_atm && c->hfp.nhfregion > 0)
+        PGK_CUDA(c, cudaMemcpy(viri_atm, c->hf_W, sizeof(double) * 8 * c->hfp.nhfregion * 3 * n,
+                               cudaMemcpyDeviceToHost));
+    return PGK_OK;
+}
+
+pgk_status pgk_langevin_dekin(pgk_ctx* c, double* out) {
+    if (!c || !out) return PGK_E_INVALID;
+    if (!c->hf_set) return pgk_fail(c, PGK_E_INVALID, "pgk_set_hf has not been called");
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    double h[PGK_LT_MAX_REGIONS];
+    PGK_CUDA(c, cudaMemcpy(h, c->lt_dekin, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int r = 0; r < c->hfp.nlangeregion; ++r) out[r] = h[r];
+    PGK_CUDA(c, cudaMemset(c->lt_dekin, 0, sizeof(h)));
+    return PGK_OK;
 }
 }

@@ -18,6 +18,16 @@ struct FftPlan {              // one axis of the 3-D transform
     void* tw;                 // complex twiddles exp(-2 pi i m / n), m < n (T2)
 };
 
+// bonded-term arrays on the host before chunk ordering / upload (0-based atoms)
+struct HostTerms {
+    std::vector<int2> bij; std::vector<double2> bp;
+    std::vector<int4> aijk; std::vector<double2> ap;
+    std::vector<int4> tij; std::vector<double4> tp;
+    std::vector<int4> rij; std::vector<double> rc;
+    std::vector<int2> p14; std::vector<double2> f14;
+    std::vector<int2> ex;
+};
+
 struct pgk_ctx {
     int natom = 0;
     int prec = PGK_PREC_FP64;
@@ -68,24 +78,40 @@ struct pgk_ctx {
     int ntorsrb = 0; int4* rb_ijkl = nullptr; double* rb_c = nullptr;       // [6*n]
     int n14 = 0; int2* p14_ij = nullptr; double2* p14_f = nullptr;          // (elc fac, vdw fac)
 
+    // ---- fused intramolecular kernel (chunks of whole molecules) ----
+    bool intra_ok = false;
+    int nchunk = 0;
+    int* chunk_atom = nullptr;    // [nchunk+1]
+    int* chunk_term = nullptr;    // [6][nchunk+1]
+    int* chunk_slot = nullptr;    // [6][nchunk] slot base of each term type inside its chunk
+    int* inc_start = nullptr;     // [natom+1] slot incidence CSR
+    unsigned short* inc_slot = nullptr;
+
     // ---- constraints ----
     int ncgroup = 0, nconstraint = 0;
     int *cg_idx = nullptr, *cg_list = nullptr;
     int2* c_ij = nullptr; double* c_d = nullptr;
+    int2* cg_span = nullptr;      // (first atom, atom count) of each group's contiguous span
 
     // ---- pair list ----
     int maxcells = 0;
     int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
-    int* perm = nullptr;          // sorted -> original
-    int* iperm = nullptr;         // original -> sorted
-    double* pos_s = nullptr;      // sorted FP64 positions at list time (3N)
-    int* nbr = nullptr;           // [N*cap]
-    int* ncnt = nullptr;          // [N]
-    int cap = 0;
+    int* subkey = nullptr;        // (sub-cell << 25) | atom, sort key inside a cell
+    // Sorted order: each cell's atoms start on a multiple of 8 (8-atom
+    // clusters); slots past a cell's count are padding (perm = -1).
+    int npad = 0;                 // sorted slots in use (multiple of 8)
+    int npad_cap = 0;             // allocated sorted slots
+    int ncl = 0;                  // clusters = npad / 8
+    int* perm = nullptr;          // sorted slot -> original atom, -1 = padding
+    int* iperm = nullptr;         // original -> sorted slot
+    double* pos_s = nullptr;      // sorted FP64 positions at list time (3*npad)
+    int* clist = nullptr;         // [ncl * ccap] entries (mask << 24) | j-slot
+    int* ccnt = nullptr;          // [ncl]
+    int ccap = 0;
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
     double4* xq64 = nullptr;      // fp64: x,y,z,q sorted
     int* typ_s = nullptr;
-    unsigned long long* counters = nullptr;   // [0] nlistnball, [1] max row
+    unsigned long long* counters = nullptr;   // [0] nlistnball, [1] max cluster row, [3] max atom row
     bool list_valid = false;
 
     // ---- SPME ----
@@ -95,6 +121,27 @@ struct pgk_ctx {
     void* qc = nullptr;           // complex grid (float2 / double2)
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
+
+    // ---- heat flux and region Langevin thermostat (k_heatf.cu) ----
+    bool hf_set = false;
+    pgk_hfparams hfp{};           // host copy (pointer members cleared)
+    int* mol_of = nullptr;        // [N] molecule of each atom
+    int* hftyp = nullptr;         // [N] PGK_HFTYP_*
+    double* molecom = nullptr;    // [3*nmole] calcom.F90 centres at the last heat-flux evaluation
+    double* molevel = nullptr;    // [3*nmole]
+    double* hf_pot = nullptr;     // [8][N]
+    double* hf_W = nullptr;       // [8][nreg][3][N]
+    double* hf_part = nullptr;    // [hf_nblk][nreg][17] calheatf block partials
+    double* hf_rec = nullptr;     // device heat-flux records
+    long long hf_rec_cap = 1;     // records hf_rec holds
+    int hf_nblk = 0;
+    double* hf_zs = nullptr;      // [npad_cap] heat-flux z of each sorted slot
+    int* hf_ms = nullptr;         // [npad_cap] molecule tag of each sorted slot
+    int hf_slots_cap = 0;
+    int* lt_mole = nullptr;       // [nmole] register by centre of mass
+    int* lt_reg = nullptr;        // [N] Langevin region (-1: none)
+    double* lt_frand = nullptr;   // [3N] random accelerations of the former half step
+    double* lt_dekin = nullptr;   // [8] det_ene_kin
 
     // ---- CUDA graphs ----
     std::map<long long, cudaGraphExec_t> graphs;
@@ -121,16 +168,31 @@ pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_
 
 // ---- launchers (k_nonbond.cu) ----
 pgk_status launch_pack(pgk_ctx* c);
-pgk_status launch_pair(pgk_ctx* c, int group, bool ene, bool vir);
+#define PM_FORCE 0
+#define PM_ENE 1
+#define PM_TENS 2
+#define PM_FULL 3
+pgk_status launch_pair(pgk_ctx* c, int group, int vmode);
 pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir);
-pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries);
+pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long long* nbits = nullptr);
 
 // ---- launchers (k_spme.cu) ----
 pgk_status spme_setup(pgk_ctx* c);
 pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir);
 
 // ---- launchers (k_bonded.cu) ----
+pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>& mol_idx, const std::vector<int>& mol_list);
 pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_all);
+pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want);
+
+// ---- launchers (k_heatf.cu, heat flux + region Langevin) ----
+struct HfDev;
+pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p);
+pgk_status launch_hf_atm(pgk_ctx* c);
+pgk_status launch_heatf(pgk_ctx* c, double* dst);
+pgk_status launch_lt_regist(pgk_ctx* c);
+pgk_status launch_langevin(pgk_ctx* c, double dt, long long step, bool former);
+pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h);   // k_bonded.cu
 
 // ---- launchers (k_integrate.cu) ----
 pgk_status launch_zero_group(pgk_ctx* c, int group);

@@ -75,6 +75,12 @@ def lib():
     L.pgk_stream.restype = vp
     L.pgk_stream.argtypes = [vp]
     L.pgk_bench_kernel.argtypes = [vp, C.c_int32, C.c_int32, pd, pd, pd]
+    L.pgk_set_hf.argtypes = [vp, C.POINTER(abi.HfParamsStruct)]
+    L.pgk_moldyn_hf.argtypes = [vp, C.c_int64, C.c_int64, C.POINTER(abi.MdParamsStruct), E, pd, C.c_int64,
+                                C.POINTER(C.c_int64)]
+    L.pgk_calheatf.argtypes = [vp, pd]
+    L.pgk_get_hf_atm.argtypes = [vp, pd, pd]
+    L.pgk_langevin_dekin.argtypes = [vp, pd]
     _lib = L
     return L
 
@@ -202,6 +208,36 @@ class PgkEngine:
 
     def moldyn_mtk(self, ini, end, md):
         return self._md(self.L.pgk_moldyn_mtk, ini, end, md)
+
+    # ---- heat flux + region Langevin (moldyn_hf.F90, calheatf.F90) ----
+    def set_hf(self, hfd):
+        """hfd: dict understood by abi.CHfParams (regions, heatfinterval,
+        hftyp, langevin, lt_mole, seed, ifoutthc)."""
+        self._hf = abi.CHfParams(hfd)
+        self._check(self.L.pgk_set_hf(self.h, C.byref(self._hf.struct)))
+
+    def calheatf(self):
+        out = np.zeros((self._hf.nreg, abi.HF_NCOL))
+        self._check(self.L.pgk_calheatf(self.h, _p(out)))
+        return out
+
+    def hf_atm(self):
+        n = self.sys.natom
+        pot = np.zeros((8, n)); W = np.zeros((8, max(self._hf.nreg, 1), 3, n))
+        self._check(self.L.pgk_get_hf_atm(self.h, _p(pot), _p(W)))
+        return pot, W[:, :self._hf.nreg]
+
+    def moldyn_hf(self, ini, end, md, cap=100000):
+        e = abi.EnergiesStruct()
+        rec = np.zeros((max(cap, 1), max(self._hf.nreg, 1), abi.HF_NCOL))
+        nr = C.c_int64(0)
+        self._check(self.L.pgk_moldyn_hf(self.h, ini, end, C.byref(md), C.byref(e), _p(rec), cap, C.byref(nr)))
+        return e.as_dict(), rec[:min(nr.value, cap), :self._hf.nreg]
+
+    def langevin_dekin(self):
+        out = np.zeros(abi.LT_MAX_REGIONS)
+        self._check(self.L.pgk_langevin_dekin(self.h, _p(out)))
+        return out[:self._hf.nlt]
 
     def sync(self):
         self._check(self.L.pgk_sync(self.h))

@@ -577,6 +577,60 @@ def small_box(kind="propanol", nside=3, spacing=5.2, seed=7, precision=PREC_FP64
     return build_system(f"{kind}_small", [(mol, nside ** 3)], (box, box, box), fn, seed + 2, 300.0, p)
 
 
+def slab_box(seed=99, nxy_w=16, nlay_w=32, nwater=8000, nxy_p=10, nlay_p=8, lxy=50.0, dz_w=3.1, dz_p=6.6,
+             vacuum=15.0, rcut=12.0, nfft=(64, 64, 192), order=4, precision=PREC_MIXED, hf_width=10.0,
+             t_hot=320.0, t_cold=280.0, damp_per_ps=1.0):
+    """Two-sided alcohol/water interface slab: rigid waters in the centre,
+    propanol (long axis along z, chain placer) on each face, vacuum above and
+    below, periodic in x, y, z.  Water is laid on an nxy_w^2 x nlay_w lattice
+    (first `nwater` sites), propanol on nxy_p^2 x nlay_p per face.  The box
+    height follows from the layer stacks plus 2 x vacuum; the default makes
+    8000 waters + 2 x 800 propanol (43,200 atoms) at liquid spacing, which
+    needs Lz ~ 205 A (a 150 A box cannot hold that many molecules at liquid
+    density).  Heat-flux regions: z slabs of `hf_width`; Langevin heat source
+    and sink: 10 A water slabs at t_hot and t_cold, a quarter of the water
+    stack from each end.  Water is molecule-based for the heat flux and the
+    thermostat, propanol atom-based."""
+    rng = np.random.default_rng(seed)
+    wat = water_template()
+    prop = propanol_template(np.random.default_rng(seed + 1))
+    hw = nlay_w * dz_w
+    hp = nlay_p * dz_p
+    lz = hw + 2.0 * hp + 2.0 * vacuum
+    z0w = vacuum + hp                                   # water stack start
+    gw = (np.arange(nxy_w) + 0.5) * (lxy / nxy_w)
+    wsites = np.array([(x, y, z0w + (k + 0.5) * dz_w) for k in range(nlay_w) for y in gw for x in gw])[:nwater]
+    rots = [_rot_matrix(rng) for _ in range(len(wsites))]
+    gp = (np.arange(nxy_p) + 0.5) * (lxy / nxy_p)
+    psites = [(x, y, vacuum + (k + 0.5) * dz_p) for k in range(nlay_p) for y in gp for x in gp]
+    psites += [(x, y, z0w + hw + (k + 0.5) * dz_p) for k in range(nlay_p) for y in gp for x in gp]
+    psites = np.array(psites)
+    placer = _chain_placer(psites, np.random.default_rng(seed + 2), axis=(0.0, 0.0, 1.0), tilt_deg=10.0)
+
+    def fn(mol, m):
+        if mol.name == wat.name:
+            return mol.coords @ rots[m].T + wsites[m]
+        return placer(mol, m)
+    box = (lxy, lxy, lz)
+    p = default_params(box, rcut=rcut, rrcut=rcut, alpha=3.4 / rcut, nfft=nfft, pme_order=order,
+                       precision=precision)
+    sysobj = build_system(f"slab_{nwater * 3 + len(psites) * 12}", [(wat, len(wsites)), (prop, len(psites))], box,
+                          fn, seed + 3, 300.0, p)
+    nw, npm = len(wsites), len(psites)
+    hftyp = np.concatenate([np.full(3 * nw, 2, np.int32), np.ones(12 * npm, np.int32)])
+    lt_mole = np.concatenate([np.ones(nw, np.int32), np.zeros(npm, np.int32)])
+    nreg = max(1, int(lz // hf_width))
+    regions = [(k * lz / nreg, (k + 1) * lz / nreg) for k in range(nreg)]
+    zq = z0w + 0.25 * hw
+    zq2 = z0w + 0.75 * hw
+    gam = damp_per_ps * 1.0e12 * TIMEREF
+    lang = [dict(box=((0.0, lxy), (0.0, lxy), (zq - 5.0, zq + 5.0)), temp=kelvin_to_reduced(t_hot), damp=gam),
+            dict(box=((0.0, lxy), (0.0, lxy), (zq2 - 5.0, zq2 + 5.0)), temp=kelvin_to_reduced(t_cold), damp=gam)]
+    sysobj.regions = dict(hf=dict(regions=regions, heatfinterval=1, hftyp=hftyp, langevin=lang, lt_mole=lt_mole,
+                                  seed=seed, ifoutthc=1))
+    return sysobj
+
+
 def ion_template(sign):
     q = np.array([1.0 if sign > 0 else -1.0])
     return Molecule("ion+" if sign > 0 else "ion-", ["IP" if sign > 0 else "IM"], q, np.zeros((1, 3)),
