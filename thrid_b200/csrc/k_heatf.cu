@@ -17,10 +17,10 @@
 //
 // k_hf_pair walks the same 8-atom cluster rows as the pair kernel: one warp
 // per cluster, one lane per (cluster, j) entry, a loop over the cluster atoms
-// whose mask bit is set.  Each pair contributes only to its cluster atom (the
-// j side is evaluated when j's cluster is processed; calvirihf is symmetric
-// in that sense), so the per-atom sums collect in per-warp shared memory and
-// are written with plain stores -- every atom belongs to one cluster slot.
+// whose mask bit is set; every list pair is stored once.  The cluster atom's
+// shares collect in per-warp shared memory and are flushed once per cluster;
+// j's shares go straight to the global arrays.  Both use FP64 atomics, since
+// other warps add j shares to the same atoms.
 // Pair arithmetic is FP32 in mixed precision and FP64 otherwise; region
 // geometry and all sums are FP64 in global memory.
 #include <algorithm>
@@ -74,20 +74,26 @@ struct HfPairArgs {
     double rrcut, rr2, rl2, rmax2;
 };
 
-// shared-memory accumulators of one cluster atom: pot[4] then W[4][nreg][3]
+// calvirihf of one list pair: both atoms receive f_ij * fact (fact = sign(zi -
+// zj) * frag / 2 per region); the cluster atom's share goes to its shared-
+// memory accumulators wi[nreg][3], j's share to the global array (stride N).
 // (pair categories ELIN, LJIN, ELC, VDW = PGK_HF_ELIN + 0..3)
 template <typename T>
-__device__ __forceinline__ void hf_pair_regions(T* w, int nreg, const HfDev& h, double zi, double zj, double rz,
-                                                double az, T fx, T fy, T fz) {
+__device__ __forceinline__ void hf_pair_regions(T* wi, double* wj, size_t N, int nreg, const HfDev& h, double zi,
+                                                double zj, double rz, double az, T fx, T fy, T fz) {
     const double zlo = fmin(zi, zj), zhi = fmax(zi, zj);
     for (int r = 0; r < nreg; ++r) {
         if (zhi < h.z1[r] || zlo > h.z2[r]) continue;
         double frag;
         if (!hf_frag(zi, zj, h.z1[r], h.z2[r], az, frag)) continue;
         const T fact = (T)(rz >= 0.0 ? frag * 0.5 : -frag * 0.5);
-        atomicAdd(w + 3 * r + 0, fx * fact);
-        atomicAdd(w + 3 * r + 1, fy * fact);
-        atomicAdd(w + 3 * r + 2, fz * fact);
+        const T vx = fx * fact, vy = fy * fact, vz = fz * fact;
+        atomicAdd(wi + 3 * r + 0, vx);
+        atomicAdd(wi + 3 * r + 1, vy);
+        atomicAdd(wi + 3 * r + 2, vz);
+        atomicAdd(wj + (3 * r + 0) * N, (double)vx);
+        atomicAdd(wj + (3 * r + 1) * N, (double)vy);
+        atomicAdd(wj + (3 * r + 2) * N, (double)vz);
     }
 }
 
@@ -120,6 +126,7 @@ __global__ void __launch_bounds__(128) k_hf_pair(const int4* __restrict__ xq, co
             const double zj = a.zs[j];
             const int mj = a.ms[j];
             const int tj = a.typ_s[j];
+            const int oj = a.perm[j];
             int4 qj = make_int4(0, 0, 0, 0);
             double4 pj = make_double4(0, 0, 0, 0);
             if (MIXED) qj = xq[j]; else pj = xq64[j];
@@ -155,8 +162,9 @@ __global__ void __launch_bounds__(128) k_hf_pair(const int4* __restrict__ xq, co
                     const T ft = phi * rinv2;
                     const int cat = same ? 0 : 2;
                     atomicAdd(w + cat, (T)0.5 * phi);
-                    if (vir) hf_pair_regions<T>(w + 4 + cat * 3 * nreg, nreg, h, zi, zj, rz, az, ft * dx, ft * dy,
-                                                ft * dz);
+                    atomicAdd(h.pot + (PGK_HF_ELIN + cat) * N + oj, (double)((T)0.5 * phi));
+                    if (vir) hf_pair_regions<T>(w + 4 + cat * 3 * nreg, h.W + (size_t)(PGK_HF_ELIN + cat) * nreg * 3 * N + oj,
+                                                N, nreg, h, zi, zj, rz, az, ft * dx, ft * dy, ft * dz);
                 }
                 if (r2 <= rl2) {                      // ewaldr_hf.F90:376-470
                     T R2, E;
@@ -167,8 +175,9 @@ __global__ void __launch_bounds__(128) k_hf_pair(const int4* __restrict__ xq, co
                     const T ft = (T)12 * E * (t12 - t6) * rinv2;
                     const int cat = same ? 1 : 3;
                     atomicAdd(w + cat, (T)0.5 * phi);
-                    if (vir) hf_pair_regions<T>(w + 4 + cat * 3 * nreg, nreg, h, zi, zj, rz, az, ft * dx, ft * dy,
-                                                ft * dz);
+                    atomicAdd(h.pot + (PGK_HF_ELIN + cat) * N + oj, (double)((T)0.5 * phi));
+                    if (vir) hf_pair_regions<T>(w + 4 + cat * 3 * nreg, h.W + (size_t)(PGK_HF_ELIN + cat) * nreg * 3 * N + oj,
+                                                N, nreg, h, zi, zj, rz, az, ft * dx, ft * dy, ft * dz);
                 }
             }
         }
@@ -180,10 +189,10 @@ __global__ void __launch_bounds__(128) k_hf_pair(const int4* __restrict__ xq, co
             const int io = a.perm[8 * cl + ii];
             if (io < 0 || v == (T)0) continue;
             if (w < 4) {
-                h.pot[(size_t)(PGK_HF_ELIN + w) * N + io] += (double)v;
+                atomicAdd(h.pot + (size_t)(PGK_HF_ELIN + w) * N + io, (double)v);
             } else {
                 const int u = w - 4, cat = u / (3 * nreg), rem = u - cat * 3 * nreg;
-                h.W[((size_t)(PGK_HF_ELIN + cat) * nreg * 3 + rem) * N + io] += (double)v;
+                atomicAdd(h.W + ((size_t)(PGK_HF_ELIN + cat) * nreg * 3 + rem) * N + io, (double)v);
             }
         }
         __syncwarp();

@@ -7,13 +7,14 @@
 // each cell's segment is padded with dummy slots (perm = -1) to a multiple of
 // 8, so every 8-slot CLUSTER lies inside one cell.
 //
-// List.  For every i-cluster the row holds each atom j that is a partner of
-// at least one of the cluster's atoms, as (mask << 24 | j): bit b of the mask
-// says that j is in the list of cluster atom b.  Membership is the reference
-// test pair for pair: exact FP64 r^2 < rcut_book^2 (no FMA, Fortran dnint
-// minimum image) minus the mkexcl exclusions, both directions (j != i), so
-// the i<j half of the bits is the reference list; pgk_get_nblist() writes it
-// back in the reference CSR layout and row order.  When the reference would
+// List.  For every i-cluster the row holds each atom slot t that is a
+// partner of at least one of the cluster's atoms s with t > s, as
+// (mask << 24 | t): bit b of the mask says that (8*cluster + b, t) is a list
+// pair.  Every pair is therefore stored once, in the row of its lower slot.
+// Membership is the reference test pair for pair: exact FP64
+// r^2 < rcut_book^2 (no FMA, Fortran dnint minimum image) minus the mkexcl
+// exclusions; pgk_get_nblist() writes the pairs back in the reference CSR
+// layout and row order.  When the reference would
 // refuse the cell index (rdscript.F90:1595-1610) the same cells are scanned
 // as distinct neighbour cells, which covers every pair of the all-pair
 // mklist2a test because cellsize >= rcut_book.
@@ -224,7 +225,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
                             double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L2, B2);
                             double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)), __dmul_rn(r2, r2));
                             if (dr < sqcut && !is_excluded(exs_idx, exs_list, io, jo)) {
-                                mask |= 1u << ii;
+                                if (t > s0 + ii) mask |= 1u << ii;   // each pair once: lower slot's row
                                 full[ii] += 1;
                                 if (jo > io) half[ii] += 1;
                             }
@@ -377,15 +378,16 @@ pgk_status launch_mklist(pgk_ctx* c) {
     return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list overflow after regrowth");
 }
 
-// Reference CSR (nb_indexall / nb_listall) from the device cluster rows.
+// Reference CSR (nb_indexall / nb_listall) from the device cluster rows:
+// every stored pair goes to the row of its lower original index, then each
+// row is ordered like the reference (27-cell z-y-x scan or ascending j).
 pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_t cap, int64_t* nl) {
     if (!c->list_valid) return pgk_fail(c, PGK_E_INVALID, "no pair list has been built");
     int n = c->natom, npad = c->npad, ncl = c->ncl;
-    std::vector<int> ccnt(ncl), perm(npad), iperm(n), cell_of(n);
+    std::vector<int> ccnt(ncl), perm(npad), cell_of(n);
     std::vector<int> rows((size_t)ncl * c->ccap);
     PGK_CUDA(c, cudaMemcpyAsync(ccnt.data(), c->ccnt, sizeof(int) * ncl, cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(perm.data(), c->perm, sizeof(int) * npad, cudaMemcpyDeviceToHost, c->st));
-    PGK_CUDA(c, cudaMemcpyAsync(iperm.data(), c->iperm, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(cell_of.data(), c->cell_of, sizeof(int) * n, cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(rows.data(), c->clist, sizeof(int) * rows.size(), cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
@@ -393,18 +395,24 @@ pgk_status export_nblist(pgk_ctx* c, int32_t* nb_index, int32_t* nb_list, int64_
     const DynState& h = c->hdyn;
     int nc0 = h.ncell[0], nc1 = h.ncell[1], nc2 = h.ncell[2];
     bool cellmode = h.list_mode_used == PGK_LIST_CELL;
+    std::vector<std::vector<int>> part(n);
+    for (int cl = 0; cl < ncl; ++cl)
+        for (int k = 0; k < ccnt[cl]; ++k) {
+            unsigned e = (unsigned)rows[(size_t)cl * c->ccap + k];
+            int j = perm[e & 0xFFFFFFu];
+            for (int b = 0; b < 8; ++b) {
+                if (!((e >> (24 + b)) & 1u)) continue;
+                int i = perm[8 * cl + b];
+                if (i < j) part[i].push_back(j); else part[j].push_back(i);
+            }
+        }
     long long pos = 0;
     std::vector<std::pair<long long, int>> tmp;
     for (int i = 0; i < n - 1; ++i) {
-        int s = iperm[i], cl = s / 8, bit = s % 8;
         tmp.clear();
         int ki = cell_of[i];
         int ix = ki % nc0, iy = (ki / nc0) % nc1, iz = ki / (nc0 * nc1);
-        for (int k = 0; k < ccnt[cl]; ++k) {
-            unsigned e = (unsigned)rows[(size_t)cl * c->ccap + k];
-            if (!((e >> (24 + bit)) & 1u)) continue;
-            int j = perm[e & 0xFFFFFFu];
-            if (j <= i) continue;
+        for (int j : part[i]) {
             long long ord = j;
             if (cellmode) {   // 27-cell scan order z, y, x (mklist_cell.F90:218-273)
                 int kj = cell_of[j];

@@ -2,12 +2,14 @@
 //
 // Work decomposition: one warp per 8-atom i-cluster of the cell-sorted order.
 // The cluster's row holds entries (mask << 24 | j); bit b of the mask says
-// that j is a list partner of cluster atom b.  One gather of j serves up to 8
-// pairs, and the index stream is one 4-byte entry per (cluster, j) instead of
-// one per pair.  Rows hold both directions (j != i), so the force on each
-// cluster atom is a register sum closed by warp shuffles -- no atomics on j
-// and a fixed summation order.  Every pair is evaluated twice; energies and
-// virials carry a factor 1/2.
+// that (cluster atom b, j) is a list pair, and every pair is stored once (in
+// the row of its lower slot).  One gather of j serves up to 8 pairs, and the
+// index stream is one 4-byte entry per (cluster, j) instead of one per pair.
+// Each evaluation serves both atoms (Newton's third law): the cluster atoms'
+// forces are register sums closed by warp shuffles, j's force is summed over
+// the entry's bits and added once per entry.  In mixed precision all force
+// sums are int64 fixed point, so the integer atomics on j are exact and the
+// result does not depend on their order.
 //
 // Mixed precision: positions enter as 32-bit fractional fixed point per box
 // axis (x/L * 2^32); the wrapped integer difference is the minimum-image
@@ -140,9 +142,13 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
 //
 // Each lane walks entries lane, lane+32, ... of the cluster's row; for each
 // entry it evaluates the pairs with the cluster atoms whose mask bit is set
-// (cluster atoms in shared memory) and keeps the 8 atoms' forces in
-// registers, closed by warp shuffles after the row.  The next entry and its j
-// record are loaded before the current entry's pairs are evaluated.
+// (cluster atoms in shared memory).  Every pair is stored once, so each
+// evaluation serves both atoms: the force on cluster atom ii accumulates in
+// registers (closed by warp shuffles after the row), the opposite force on j
+// accumulates over the entry's bits and is added once per entry to j's int64
+// fixed-point accumulator -- integer atomics, so the sum is exact and
+// independent of their order.  The next entry and its j record are loaded
+// before the current entry's pairs are evaluated.
 //
 // Block b owns the contiguous cluster range [b*chunk, (b+1)*chunk); its
 // warps take every 8th cluster of it, so they read overlapping j ranges at
@@ -176,6 +182,8 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
     const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
     const int* __restrict__ typ_s = a.typ_s;
+    const int* __restrict__ perm = a.perm;
+    long long* __restrict__ facc = (long long*)a.facc;
     float ev = 0.f, ee = 0.f;
     float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
@@ -195,44 +203,52 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
         unsigned e = k < cnt ? (unsigned)__ldg(row + k) : 0u;
         int4 pj = __ldg(xq + (e & 0xFFFFFFu));
         int tj = __ldg(typ_s + (e & 0xFFFFFFu));
+        int oj = __ldg(perm + (e & 0xFFFFFFu));
         while (k < cnt) {
             const int kn = k + 32;
             const unsigned en = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
             const int4 pjn = __ldg(xq + (en & 0xFFFFFFu));
             const int tjn = __ldg(typ_s + (en & 0xFFFFFFu));
+            const int ojn = __ldg(perm + (en & 0xFFFFFFu));
             const unsigned m = e >> 24;
+            float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii)
-                if ((m >> ii) & 1u)
-                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h, sf,
-                                    sp, slj, f[ii][0], f[ii][1], f[ii][2], ev, ee, wc, wl);
-            k = kn; e = en; pj = pjn; tj = tjn;
+                if ((m >> ii) & 1u) {
+                    float fx = 0.f, fy = 0.f, fz = 0.f;
+                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h,
+                                    sf, sp, slj, fx, fy, fz, ev, ee, wc, wl);
+                    f[ii][0] += fx; f[ii][1] += fy; f[ii][2] += fz;
+                    gx -= fx; gy -= fy; gz -= fz;
+                }
+            long long* fj = facc + 3 * (size_t)oj;
+            atomicAdd((unsigned long long*)fj, (unsigned long long)__double2ll_rn((double)gx * PGK_FORCE_SCALE));
+            atomicAdd((unsigned long long*)fj + 1, (unsigned long long)__double2ll_rn((double)gy * PGK_FORCE_SCALE));
+            atomicAdd((unsigned long long*)fj + 2, (unsigned long long)__double2ll_rn((double)gz * PGK_FORCE_SCALE));
+            k = kn; e = en; pj = pjn; tj = tjn; oj = ojn;
         }
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
             if (lane == ii) {
-                const int io = a.perm[8 * cl + ii];
+                const int io = perm[8 * cl + ii];
                 if (io >= 0) force_add<true>(a.facc, io, (double)fx, (double)fy, (double)fz);
             }
         }
     }
-    // pairs were counted from both sides: factor 1/2.  Tensor (a,b) -> 3*b + a,
-    // stored as its lower triangle.
+    // every pair evaluated once.  Tensor (a,b) -> 3*b + a, stored as its lower triangle.
     if (MODE == PM_FULL) {
-        double v[16] = {0.5 * ev, 0.5 * ee, 0.5 * ee,
-                        0.5 * wc[0], 0.5 * wc[1], 0.5 * wc[2], 0.5 * wc[3], 0.5 * wc[4], 0.5 * wc[5],
-                        0.5 * wl[0], 0.5 * wl[1], 0.5 * wl[2], 0.5 * wl[3], 0.5 * wl[4], 0.5 * wl[5],
-                        0.5 * ((double)wl[0] + (double)wl[3] + (double)wl[5])};
+        double v[16] = {ev, ee, ee, wc[0], wc[1], wc[2], wc[3], wc[4], wc[5],
+                        wl[0], wl[1], wl[2], wl[3], wl[4], wl[5], (double)wl[0] + (double)wl[3] + (double)wl[5]};
         const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
                              A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
         block_acc<16>(v, a.acc, idx, false);
     } else if (MODE == PM_TENS) {
-        double v[6] = {0.5 * wc[0], 0.5 * wc[1], 0.5 * wc[2], 0.5 * wc[3], 0.5 * wc[4], 0.5 * wc[5]};
+        double v[6] = {wc[0], wc[1], wc[2], wc[3], wc[4], wc[5]};
         const int idx[6] = {A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
         block_acc<6>(v, a.acc, idx, false);
     } else if (MODE == PM_ENE) {
-        double v[2] = {0.5 * ev, 0.5 * ee};
+        double v[2] = {ev, ee};
         const int idx[2] = {A_VDW, A_ELC};
         block_acc<2>(v, a.acc, idx, false);
     }
@@ -277,6 +293,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
             const double4 pj = xq[j];
             const int tj = a.typ_s[j];
             const unsigned m = e >> 24;
+            double gx = 0, gy = 0, gz = 0;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii) {
                 if (!((m >> ii) & 1u)) continue;
@@ -297,7 +314,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
                     fc = (c.x + d * (c.y + d * (c.z + d * c.w))) * qq;
                     if (ENE) {
                         const double4 p = sp[idx];
-                        e_elc += 0.5 * ((p.x + d * (p.y + d * (p.z + d * p.w))) * qq);
+                        e_elc += (p.x + d * (p.y + d * (p.z + d * p.w))) * qq;
                     }
                 }
                 if (r2 <= a.rl2) {
@@ -305,11 +322,11 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
                     const double t2 = rinv2 * lp.x;
                     const double t6 = t2 * t2 * t2, t12 = t6 * t6;
                     fl = 12.0 * lp.y * (t12 - t6) * rinv2;
-                    if (ENE) e_vdw += 0.5 * (lp.y * (t12 - 2.0 * t6));
+                    if (ENE) e_vdw += lp.y * (t12 - 2.0 * t6);
                 }
-                f[ii][0] += fc * dx + fl * dx;
-                f[ii][1] += fc * dy + fl * dy;
-                f[ii][2] += fc * dz + fl * dz;
+                const double fx = fc * dx + fl * dx, fy = fc * dy + fl * dy, fz = fc * dz + fl * dz;
+                f[ii][0] += fx; f[ii][1] += fy; f[ii][2] += fz;
+                gx -= fx; gy -= fy; gz -= fz;
                 if (ENE) {
                     vc[0] += fc * dx * dx; vc[1] += fc * dx * dy; vc[2] += fc * dx * dz;
                     vc[3] += fc * dy * dy; vc[4] += fc * dy * dz; vc[5] += fc * dz * dz;
@@ -317,6 +334,7 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
                     vl[3] += fl * dy * dy; vl[4] += fl * dy * dz; vl[5] += fl * dz * dz;
                 }
             }
+            force_add<false>(a.facc, a.perm[j], gx, gy, gz);
         }
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
@@ -328,10 +346,8 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
         }
     }
     if (ENE) {
-        double v[16] = {e_vdw, e_elc, e_elc,
-                        0.5 * vc[0], 0.5 * vc[1], 0.5 * vc[2], 0.5 * vc[3], 0.5 * vc[4], 0.5 * vc[5],
-                        0.5 * vl[0], 0.5 * vl[1], 0.5 * vl[2], 0.5 * vl[3], 0.5 * vl[4], 0.5 * vl[5],
-                        0.5 * (vl[0] + vl[3] + vl[5])};
+        double v[16] = {e_vdw, e_elc, e_elc, vc[0], vc[1], vc[2], vc[3], vc[4], vc[5],
+                        vl[0], vl[1], vl[2], vl[3], vl[4], vl[5], vl[0] + vl[3] + vl[5]};
         const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
                              A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
         block_acc<16>(v, a.acc, idx, true);

@@ -416,10 +416,11 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         double vol = p->xcel * p->ycel * p->zcel;
         double rb = p->rcut_book;
         // partners of an 8-atom cluster: the sphere of radius rcut_book swept
-        // over the cluster's extent (~ 2 A); rows regrow on overflow
+        // over the cluster's extent (~ 2 A), about half of them stored (each
+        // pair once, in its lower slot's row); rows regrow on overflow
         double rs = rb + 2.0;
         double expect = (double)n / vol * 4.0 / 3.0 * std::acos(-1.0) * rs * rs * rs;
-        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(1.3 * expect + 128);
+        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(0.75 * expect + 128);
         cap = std::min(cap, ((n + 31) / 32) * 32);
         cap = ((cap + 31) / 32) * 32;
         c->ccap = std::max(cap, 32);

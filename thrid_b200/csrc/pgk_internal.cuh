@@ -8,10 +8,13 @@
 //                       int64 fixed point (scale 2^32) in mixed precision,
 //                       double in FP64 precision
 //   acc   int64[2][NACC] energy / virial / kinetic accumulators (fixed 2^32)
-//   sorted copies for the pair kernel (cell order): perm[N] (sorted -> orig),
+//   sorted copies for the pair kernel (cell order, each cell padded to a
+//     multiple of 8 slots): perm[npad] (slot -> original atom, -1 padding),
 //     xq (int4: fractional fixed-point x,y,z + float bits of q, mixed) or
-//     xq64 (double4: x,y,z,q, FP64), typ_s[N]
-//   nbr   int32[N*cap]  full neighbour rows (sorted indices), ncnt[N]
+//     xq64 (double4: x,y,z,q, FP64), typ_s[npad]
+//   clist int32[ncl*ccap] rows of 8-atom clusters, entries (mask << 24 | j),
+//     ccnt[ncl]
+//   heat flux: pot[8][N], W[8][nreg][3][N] (k_heatf.cu)
 //   SPME  qacc (8-byte[K3*K2*K1]) + qc (complex[K3*K2*K1])
 //   dyn   DynState      box and integrator coefficients read by every kernel,
 //                       so that a whole MD step can be captured in a CUDA graph
