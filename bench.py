@@ -162,6 +162,8 @@ def run_ours(args, rank, world, local_rank):
     e2e = None if args.no_e2e else e2e_leg(eng, s, md, step0 + args.steps, max(3, args.steps // 4), world)
     # ---- dominant kernel roofline (pair kernel), measured live ----
     roof = roofline(eng)
+    # ---- the all-FP64 device path on the same state (north-star comparison) ----
+    fp64 = None if args.no_fp64 else fp64_leg(eng, s, md, step0 + args.steps + 1000, stream)
     eng.close()
     natom = s.natom
     value = world * natom * args.steps / (ms_max / 1e3)
@@ -174,13 +176,45 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas{world}", "nstep_book": NSTEP_BOOK,
                    "l2": "working set > L2 (pair list ~0.6 GB), no flush"},
         "ns_per_day": ns_per_day(args.steps / (ms_max / 1e3)),
-        "e2e": e2e, "gpu_launches": launches, "roofline": roof,
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "fp64_path": fp64,
         "energies_last": {k: ene[k] for k in ("pot_tot", "pot_vdw", "pot_elc", "pot_ewk")} if ene else None,
     }
     out["clocks"] = clk.summary()
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
+
+
+def fp64_leg(eng, s, md, start, stream, nsteps=10):
+    """The FP64 device path (the parity path) on the mixed run's current state:
+    force RMS relative error of the mixed path against it (both MTS groups,
+    same positions) and its own MD throughput on the same workload."""
+    import torch
+    from thrid_b200 import abi
+    from thrid_b200.pgk import PgkEngine
+    cor, vel, box = eng.download_state()
+    ch = eng.get_chain()
+    fm = eng.calforce(abi.MTS_LONG)[0] + eng.calforce(abi.MTS_SHORT)[0]
+    e64 = PgkEngine(s, dict(s.params, precision=abi.PREC_FP64), upload=False)
+    try:
+        e64.upload_state(cor, vel, box)
+        e64.set_chain(ch)
+        f64 = e64.calforce(abi.MTS_LONG)[0] + e64.calforce(abi.MTS_SHORT)[0]
+        err = float(np.sqrt(((fm - f64) ** 2).sum() / (f64 ** 2).sum()))
+        st64 = torch.cuda.ExternalStream(e64.stream)
+        e64.moldyn_mtk(start, start + 2, md)
+        e64.sync()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st64)
+        e64.moldyn_mtk(start + 3, start + 2 + nsteps, md)
+        b.record(st64)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / nsteps
+    finally:
+        e64.close()
+    return {"value": s.natom / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": nsteps,
+            "force_rel_rms_mixed_vs_fp64": err}
 
 
 def e2e_leg(eng, s, md, start, nsteps, world):
@@ -308,6 +342,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_init()

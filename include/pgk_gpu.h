@@ -134,7 +134,7 @@ typedef struct pgk_params {
     int32_t mts_ewk;              /* gates fft_pme                             */
     int32_t mts_vdw14, mts_elc14; /* calnon14 runs when both equal the flag    */
     int32_t ifnetqcorrp;          /* net-charge correction for pressure        */
-    int32_t max_nbr;              /* per-atom capacity of the device pair list (0 = auto) */
+    int32_t max_nbr;              /* entries per 8-atom cluster row of the device pair list (0 = auto) */
 } pgk_params;
 
 /* ---- integrator parameters (moldyn_*.F90 arguments) ---------------------- */
@@ -353,12 +353,56 @@ void* pgk_stream(const pgk_ctx* ctx);
  * path `iters` times back to back on the context's stream, bracketed by CUDA
  * events, and return the mean device time per launch in *ms.  which:
  *   0 = real-space pair kernel (ewaldrp) with virials, 1 = SPME spread,
- *   2 = SPME gather, 3 = one forward 3-D FFT (three axis passes).
+ *   2 = SPME gather, 3 = one forward 3-D FFT (three axis passes),
+ *   64 + m = the fused intramolecular kernel with term mask m (bit 0 bonds,
+ *   1 angles, 2 torsions, 3 RB torsions, 4 1-4 pairs, 5 excluded pairs).
  * *units receives the algorithmic work of one launch: unique pairs inside
- * the cutoff (0), atoms (1, 2) or grid points (3); *entries the number of
- * full-list entries the pair kernel reads. */
+ * the cutoff (0), atoms (1, 2, 64+), or grid points (3); *entries the number
+ * of (cluster, j) list entries the pair kernel reads. */
 pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
                             double* entries);
+
+/* ---- replica server (continuous batching) --------------------------------
+ * No counterpart in the reference, which runs one system per process.
+ * Independent replicas (different sizes and topologies) are queued with
+ * pgk_server_submit and admitted while earlier ones run, in arrival order,
+ * as worker slots and the device-memory budget allow (pgk_estimate_bytes;
+ * a request larger than the whole budget runs alone).  Each admitted replica
+ * keeps its state resident in its own context and non-blocking CUDA stream;
+ * one host worker per slot runs it (captured step graphs), so the replicas'
+ * kernels overlap on the device.  In mixed precision a replica's results are
+ * bit-identical to a run of it alone (integer force sums, private buffers).
+ * The server copies every input at submit. */
+typedef struct pgk_server pgk_server;
+typedef struct pgk_request {
+    const pgk_system*   sys;
+    const pgk_params*   prm;
+    const pgk_mdparams* md;
+    int32_t kind;                 /* 0 moldyn (NVE), 1 moldyn_nhc, 2 moldyn_mtk, 3 moldyn_hf */
+    int32_t _pad;
+    const pgk_hfparams* hf;       /* required for kind 3, else may be NULL    */
+    const double* atmcor;         /* (3,natom) initial coordinates            */
+    const double* atmvel;         /* (3,natom) initial velocities, NULL = 0   */
+    const double* box;            /* NULL = (xcel, ycel, zcel) of prm         */
+    const pgk_chain* chain;       /* NULL = zero chain                        */
+    int64_t nsteps;               /* runs steps 0 .. nsteps                   */
+} pgk_request;
+
+/* Device bytes one context of this system needs (estimate with margin). */
+int64_t pgk_estimate_bytes(const pgk_system* sys, const pgk_params* prm);
+/* max_slots worker slots on the current device; budget <= 0 = 80 % of free memory. */
+pgk_status pgk_server_create(int32_t max_slots, int64_t hbm_budget_bytes, pgk_server** out);
+pgk_status pgk_server_submit(pgk_server* sv, const pgk_request* req, int64_t* id);
+pgk_status pgk_server_poll(pgk_server* sv, int64_t id, int32_t* done);
+pgk_status pgk_server_wait(pgk_server* sv, int64_t id);
+/* Final state, last energies, heat-flux records (kind 3) and the request's
+ * submit / start / finish times in seconds (steady clock) in times3. */
+pgk_status pgk_server_result(pgk_server* sv, int64_t id, double* atmcor, double* atmvel, double* box,
+                             pgk_energies* ene, double* hf_out, int64_t cap_records, int64_t* nrecords,
+                             double* times3);
+pgk_status pgk_server_release(pgk_server* sv, int64_t id);
+/* Finishes every queued request, then stops the workers. */
+pgk_status pgk_server_free(pgk_server* sv);
 
 /* Allocation-free SPME reciprocal force.  No counterpart in the reference.
  * For callers that must not allocate device memory during a run -- a host

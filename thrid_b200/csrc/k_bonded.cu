@@ -376,8 +376,8 @@ __global__ void k_excl(const double* __restrict__ pos, const double* __restrict_
 // fixed order (precomputed incidence list), so the result is deterministic in
 // both precisions.  Chunks are whole molecules with at most INTRA_ATOMS atoms
 // and INTRA_SLOTS slots.
-#define INTRA_ATOMS 128
-#define INTRA_SLOTS 4096
+#define INTRA_ATOMS 64
+#define INTRA_SLOTS 2048
 
 struct IntraArgs {
     const int* chunk_atom;          // [nchunk+1] first atom of each chunk
@@ -411,13 +411,21 @@ __global__ void __launch_bounds__(256) k_intra(const double* __restrict__ pos, I
                                                const DynState* __restrict__ dyn) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     __shared__ double sp[3 * INTRA_ATOMS];
+    __shared__ unsigned short s_inc[INTRA_SLOTS];     // the chunk's incidence lists
+    __shared__ int s_start[INTRA_ATOMS + 1];
+    __shared__ double s_q[INTRA_ATOMS];                // charges and LJ types of the chunk
+    __shared__ int s_t[INTRA_ATOMS];
     extern __shared__ unsigned char slot_raw[];
     T* sx = (T*)slot_raw;
     T* sy = sx + INTRA_SLOTS;
     T* sz = sy + INTRA_SLOTS;
     const int c = blockIdx.x;
     const int a0 = a.chunk_atom[c], na = a.chunk_atom[c + 1] - a0;
+    const int i0 = a.inc_start[a0], ni = a.inc_start[a0 + na] - i0;
     for (int k = threadIdx.x; k < 3 * na; k += blockDim.x) sp[k] = pos[3 * (size_t)a0 + k];
+    for (int k = threadIdx.x; k <= na; k += blockDim.x) s_start[k] = a.inc_start[a0 + k] - i0;
+    for (int k = threadIdx.x; k < ni; k += blockDim.x) s_inc[k] = a.inc_slot[i0 + k];
+    for (int k = threadIdx.x; k < na; k += blockDim.x) { s_q[k] = a.chrg[a0 + k]; s_t[k] = a.typ[a0 + k]; }
     __syncthreads();
     const int stride = a.nchunk + 1;
     const int* cs = a.chunk_slot;
@@ -497,7 +505,7 @@ __global__ void __launch_bounds__(256) k_intra(const double* __restrict__ pos, I
         for (int t = t0 + threadIdx.x; t < a.chunk_term[4 * stride + c + 1]; t += blockDim.x) {
             int gi = a.p14_ij[t].x, gj = a.p14_ij[t].y;
             double F[3], rd[3], de, dv;
-            eval_14<T>(sp, gi - a0, gj - a0, a.chrg[gi] * a.chrg[gj], a.lj64[a.typ[gi] * a.ntyp + a.typ[gj]],
+            eval_14<T>(sp, gi - a0, gj - a0, s_q[gi - a0] * s_q[gj - a0], a.lj64[s_t[gi - a0] * a.ntyp + s_t[gj - a0]],
                        a.p14_f[t], dyn, F, rd, de, dv);
             int sl = cs[4 * a.nchunk + c] + 2 * (t - t0);
             put(sx, sy, sz, sl, F, 1.0);
@@ -517,7 +525,7 @@ __global__ void __launch_bounds__(256) k_intra(const double* __restrict__ pos, I
         for (int t = t0 + threadIdx.x; t < a.chunk_term[5 * stride + c + 1]; t += blockDim.x) {
             int gi = a.expair[t].x, gj = a.expair[t].y;
             double F[3], rd[3], e;
-            eval_excl<MIXED>(sp, gi - a0, gj - a0, a.chrg[gi] * a.chrg[gj], a.spl64, a.spl32, a.nspl, a.h, dyn,
+            eval_excl<MIXED>(sp, gi - a0, gj - a0, s_q[gi - a0] * s_q[gj - a0], a.spl64, a.spl32, a.nspl, a.h, dyn,
                              F, rd, e);
             int sl = cs[5 * a.nchunk + c] + 2 * (t - t0);
             put(sx, sy, sz, sl, F, 1.0);
@@ -542,8 +550,8 @@ __global__ void __launch_bounds__(256) k_intra(const double* __restrict__ pos, I
     }
     for (int l = threadIdx.x; l < na; l += blockDim.x) {
         double fx = 0, fy = 0, fz = 0;
-        for (int k = a.inc_start[a0 + l]; k < a.inc_start[a0 + l + 1]; ++k) {
-            const int sl = a.inc_slot[k];
+        for (int k = s_start[l]; k < s_start[l + 1]; ++k) {
+            const int sl = s_inc[k];
             bool on = false;
 #pragma unroll
             for (int ty = 0; ty < 6; ++ty) on |= (sl >= lo[ty] && sl < hi[ty]);

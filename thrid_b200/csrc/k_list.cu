@@ -170,14 +170,20 @@ __device__ __forceinline__ bool is_excluded(const int* __restrict__ exs_idx, con
 }
 
 // one warp per i-cluster: scan the distinct neighbour cells of the cluster's
-// cell; for each real candidate j test all 8 cluster atoms (exact FP64 test,
-// exclusions) and append (mask << 24 | j) when any bit is set.
+// cell, candidates t above the cluster's first slot only (each pair is stored
+// in its lower slot's row).  A candidate farther than rcut_book (+ margin)
+// from the bounding box of the cluster's atoms is skipped; otherwise all 8
+// cluster atoms get the exact reference test (FP64, exclusions) and the entry
+// (mask << 24 | t) is appended when any bit is set.
+// nlistnball (the reference's row count, one sentinel per empty row) is the
+// number of pairs plus the atoms i < n-1 without a partner of higher index;
+// hasup[i] = 1 marks the atoms that have one.
 __global__ void __launch_bounds__(256) k_build_clist(
         const double* __restrict__ pos_s, const int* __restrict__ perm, const int* __restrict__ cell_of,
         const int* __restrict__ cell_start, const int* __restrict__ cell_cnt, const int* __restrict__ exs_idx,
-        const int* __restrict__ exs_list, int n, int ncl, int ccap, double sqcut, const DynState* __restrict__ dyn,
-        int* __restrict__ clist, int* __restrict__ ccnt, unsigned long long* __restrict__ counters,
-        unsigned* __restrict__ status) {
+        const int* __restrict__ exs_list, int n, int ncl, int ccap, double sqcut, double rbox,
+        const DynState* __restrict__ dyn, int* __restrict__ clist, int* __restrict__ ccnt,
+        unsigned char* __restrict__ hasup, unsigned long long* __restrict__ counters, unsigned* __restrict__ status) {
     __shared__ double spi[8][3 * 8];
     __shared__ int sio[8][8];
     const int wib = threadIdx.x >> 5;
@@ -193,14 +199,31 @@ __global__ void __launch_bounds__(256) k_build_clist(
         spi[wib][3 * lane + 2] = pos_s[3 * (s0 + lane) + 2];
     }
     __syncwarp();
-    const double L0 = dyn->box[0], L1 = dyn->box[1], L2 = dyn->box[2];
-    const double B0 = 1.0 / L0, B1 = 1.0 / L1, B2 = 1.0 / L2;
+    const double L[3] = {dyn->box[0], dyn->box[1], dyn->box[2]};
+    const double B[3] = {1.0 / L[0], 1.0 / L[1], 1.0 / L[2]};
     const int nc0 = dyn->ncell[0], nc1 = dyn->ncell[1], nc2 = dyn->ncell[2];
+    // bounding box of the real cluster atoms, minimum image relative to atom 0
+    double ctr[3], hw[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double lo = 0.0, hi = 0.0;
+        const double x0 = spi[wib][d];
+        for (int ii = 1; ii < 8; ++ii) {
+            if (sio[wib][ii] < 0) continue;
+            double r = spi[wib][3 * ii + d] - x0;
+            r -= L[d] * rint(r * B[d]);
+            lo = fmin(lo, r); hi = fmax(hi, r);
+        }
+        ctr[d] = x0 + 0.5 * (lo + hi);
+        hw[d] = 0.5 * (hi - lo);
+    }
+    const double rb2 = rbox * rbox;
     const int key = cell_of[sio[wib][0]];
     const int cx = key % nc0, cy = (key / nc0) % nc1, cz = key / (nc0 * nc1);
     const int nz = nc2 >= 3 ? 3 : nc2, ny = nc1 >= 3 ? 3 : nc1, nx = nc0 >= 3 ? 3 : nc0;
     int count = 0;
-    int full[8] = {0, 0, 0, 0, 0, 0, 0, 0}, half[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned long long npair = 0;
+    unsigned up = 0;                                   // bit ii: cluster atom ii has a higher-index partner
     int* row = clist + (size_t)cl * ccap;
     for (int a = 0; a < nz; ++a) {
         int z = nc2 >= 3 ? (cz + a - 1 + nc2) % nc2 : a;
@@ -210,25 +233,42 @@ __global__ void __launch_bounds__(256) k_build_clist(
                 int x = nc0 >= 3 ? (cx + c - 1 + nc0) % nc0 : c;
                 int cell = x + nc0 * (y + nc1 * z);
                 int t0 = cell_start[cell], t1 = t0 + cell_cnt[cell];
+                if (t1 <= s0 + 1) continue;             // every slot of the cell is below the cluster
+                t0 = max(t0, s0 + 1);
                 for (int tb = t0; tb < t1; tb += 32) {
                     int t = tb + lane;
                     unsigned mask = 0;
                     if (t < t1) {
                         const double xj = pos_s[3 * t], yj = pos_s[3 * t + 1], zj = pos_s[3 * t + 2];
-                        const int jo = perm[t];
+                        const double pj[3] = {xj, yj, zj};
+                        double e2 = 0.0;
 #pragma unroll
-                        for (int ii = 0; ii < 8; ++ii) {
-                            const int io = sio[wib][ii];
-                            if (io < 0 || t == s0 + ii) continue;
-                            double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L0, B0);
-                            double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L1, B1);
-                            double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L2, B2);
-                            double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)), __dmul_rn(r2, r2));
-                            if (dr < sqcut && !is_excluded(exs_idx, exs_list, io, jo)) {
-                                if (t > s0 + ii) mask |= 1u << ii;   // each pair once: lower slot's row
-                                full[ii] += 1;
-                                if (jo > io) half[ii] += 1;
+                        for (int d = 0; d < 3; ++d) {
+                            double r = pj[d] - ctr[d];
+                            r -= L[d] * rint(r * B[d]);
+                            double ex = fmax(fabs(r) - hw[d], 0.0);
+                            e2 += ex * ex;
+                        }
+                        if (e2 <= rb2) {
+                            const int jo = perm[t];
+                            bool jlow = false;
+#pragma unroll
+                            for (int ii = 0; ii < 8; ++ii) {
+                                const int io = sio[wib][ii];
+                                if (io < 0 || t <= s0 + ii) continue;
+                                double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L[0], B[0]);
+                                double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L[1], B[1]);
+                                double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
+                                double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)),
+                                                      __dmul_rn(r2, r2));
+                                if (dr < sqcut && !is_excluded(exs_idx, exs_list, io, jo)) {
+                                    mask |= 1u << ii;
+                                    if (jo > io) up |= 1u << ii;
+                                    else jlow = true;
+                                }
                             }
+                            if (jlow) hasup[jo] = 1;
+                            npair += (unsigned long long)__popc(mask);
                         }
                     }
                     unsigned m = __ballot_sync(0xffffffffu, mask != 0);
@@ -241,27 +281,23 @@ __global__ void __launch_bounds__(256) k_build_clist(
             }
         }
     }
-#pragma unroll
-    for (int ii = 0; ii < 8; ++ii) {
-        full[ii] = warp_sum(full[ii]);
-        half[ii] = warp_sum(half[ii]);
-    }
+    up = __reduce_or_sync(0xffffffffu, up);
+    npair = warp_sum(npair);
+    if (lane < 8 && ((up >> lane) & 1u)) hasup[sio[wib][lane]] = 1;
     if (lane == 0) {
         ccnt[cl] = min(count, ccap);
         if (count > ccap) atomicOr(status, ST_LIST_OVERFLOW);
         atomicMax(&counters[1], (unsigned long long)count);
-        unsigned long long nl = 0;
-        int mx = 0;
-#pragma unroll
-        for (int ii = 0; ii < 8; ++ii) {
-            int io = sio[wib][ii];
-            if (io < 0) continue;
-            mx = max(mx, full[ii]);
-            if (io < n - 1) nl += (unsigned long long)(half[ii] > 0 ? half[ii] : 1);
-        }
-        atomicAdd(&counters[0], nl);
-        atomicMax(&counters[3], (unsigned long long)mx);
+        atomicAdd(&counters[0], npair);
     }
+}
+
+// atoms i < n-1 without a partner of higher index (one sentinel row each)
+__global__ void k_count_noup(const unsigned char* __restrict__ hasup, int m, unsigned long long* counters) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned v = (i < m && !hasup[i]) ? 1u : 0u;
+    unsigned w = __popc(__ballot_sync(0xffffffffu, v));
+    if ((threadIdx.x & 31) == 0 && w) atomicAdd(&counters[2], (unsigned long long)w);
 }
 
 pgk_status launch_transcor(pgk_ctx* c) {
@@ -346,10 +382,12 @@ pgk_status launch_mklist(pgk_ctx* c) {
                                                                c->typ_s);
         double sq = c->prm.rcut_book * c->prm.rcut_book;
         long long threads = (long long)c->ncl * 32;
+        PGK_CUDA(c, cudaMemsetAsync(c->hasup, 0, (size_t)n, c->st));
         k_build_clist<<<(unsigned)((threads + 255) / 256), 256, 0, c->st>>>(
             c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, n, c->ncl, c->ccap,
-            sq, c->dyn, c->clist, c->ccnt, c->counters, c->status);
-        c->launches += 6;
+            sq, c->prm.rcut_book + 0.05, c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
+        if (n > 1) k_count_noup<<<(n - 1 + 255) / 256, 256, 0, c->st>>>(c->hasup, n - 1, c->counters);
+        c->launches += 7;
         PGK_CUDA(c, cudaGetLastError());
         unsigned long long cnt[4];
         unsigned st;
@@ -368,11 +406,12 @@ pgk_status launch_mklist(pgk_ctx* c) {
             if ((s = ensure_sorted_capacity(c, capslots))) return s;
             continue;
         }
-        h.nlistnball = (long long)cnt[0];
-        h.nmaxrow = (int)cnt[3];
+        h.nlistnball = (long long)(cnt[0] + cnt[2]);
+        h.nmaxrow = (int)cnt[1];
         PGK_CUDA(c, cudaMemcpyAsync(&c->dyn->nlistnball, &h.nlistnball, sizeof(long long),
                                     cudaMemcpyHostToDevice, c->st));
         c->list_valid = true;
+        ++c->list_epoch;
         return PGK_OK;
     }
     return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list overflow after regrowth");

@@ -179,16 +179,20 @@ __host__ __device__ constexpr int nstages(int n) {
 }
 
 // one Stockham stage on P pencils of length n held in shared memory
+// pencils are stored with pitch ld = n + 1 elements, so that the strided
+// loads and stores of the y and z passes (consecutive threads on consecutive
+// pencils) fall into different shared-memory banks
 template <typename T, typename T2>
 __device__ __forceinline__ void fft_stage(const T2* __restrict__ src, T2* __restrict__ dst, int P, int n, int R,
                                           int Ns, const T2* __restrict__ tw, T sg) {
+    const int ld = n + 1;
     const int nr = n / R;
     const int twstep = n / (Ns * R);
     for (int w = threadIdx.x; w < P * nr; w += blockDim.x) {
         int p = w / nr, j = w - p * nr;
         int k = j % Ns;
         T2 v[5];
-        const T2* sp = src + p * n;
+        const T2* sp = src + p * ld;
 #pragma unroll
         for (int r = 0; r < 5; ++r)
             if (r < R) {
@@ -202,7 +206,7 @@ __device__ __forceinline__ void fft_stage(const T2* __restrict__ src, T2* __rest
             }
         dft_r<T, T2>(v, R, sg);
         int o = (j / Ns) * Ns * R + k;
-        T2* dp = dst + p * n;
+        T2* dp = dst + p * ld;
 #pragma unroll
         for (int r = 0; r < 5; ++r)
             if (r < R) dp[o + r * Ns] = v[r];
@@ -289,7 +293,8 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
     extern __shared__ unsigned char smraw[];
     T2* bufA = (T2*)smraw;
     const int n = NC > 0 ? NC : plan.n;
-    T2* bufB = bufA + P * n;
+    const int ld = n + 1;                 // padded pencil pitch (bank-conflict free strided access)
+    T2* bufB = bufA + P * ld;
     size_t base;
     size_t stride;
     int yz = 0;
@@ -324,7 +329,7 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
             else if (SRC == 1) v.x = (T)((double)((const long long*)acc)[off] * PGK_GRID_ISCALE);
             else v.x = (T)((const double*)acc)[off];
         }
-        bufA[p * n + m] = v;
+        bufA[p * ld + m] = v;
     }
     __syncthreads();
     T2* src = bufA;
@@ -334,15 +339,16 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         double en = 0, vs = 0, vt[6] = {0, 0, 0, 0, 0, 0};
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
             int p = idx / n, m = idx - p * n;
+            const int sidx = p * ld + m;
             int k1 = x0 + p;
             if (k1 >= K1) continue;
             if (k1 == 0 && yz == 0 && m == 0) continue;   // m = 0 is skipped by scalar_sum
-            T2 v = src[idx];
+            T2 v = src[sidx];
             double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
             double et = conv_point(k1, yz, m, K1, K2, K3, s2, ca, dyn, en, vs, vt);
             v.x = (T)((double)v.x * et);
             v.y = (T)((double)v.y * et);
-            src[idx] = v;
+            src[sidx] = v;
         }
         __syncthreads();
         FftStages<T, T2, NC>::run(src, dst, P, n, plan, -sg);
@@ -360,7 +366,7 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
         if (pg < npen_total) {
             size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
-            data[off] = src[p * n + m];
+            data[off] = src[p * ld + m];
         }
     }
 }
@@ -585,7 +591,7 @@ static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) 
     if (AXIS == 0) grid = (K2 * K3 + P - 1) / P;
     else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3;
     else grid = ((K1 + P - 1) / P) * K2;
-    size_t sm = (size_t)2 * P * pl.n * sizeof(T2);
+    size_t sm = (size_t)2 * P * (pl.n + 1) * sizeof(T2);
     ConvArgs ca{};
     if (cap) ca = *cap;
     switch (pl.n) {   // compile-time lengths of the configured grids; others run the generic stage loop
@@ -781,7 +787,7 @@ static cudaError_t noalloc_fft_pass(unsigned char* base, const FftPlan& pl, int 
     int P = 8;
     if (AXIS == 0) P = std::max(1, 1024 / K1);
     int grid = AXIS == 0 ? (K2 * K3 + P - 1) / P : ((K1 + P - 1) / P) * (AXIS == 1 ? K3 : K2);
-    size_t sm = (size_t)2 * P * pl.n * sizeof(double2);
+    size_t sm = (size_t)2 * P * (pl.n + 1) * sizeof(double2);
     cudaError_t e = cudaFuncSetAttribute(k_fft<double, AXIS, SRC, 0, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;

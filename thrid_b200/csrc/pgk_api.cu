@@ -211,6 +211,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return PGK_E_CUDA;
     pgk_ctx* c = new pgk_ctx();
+    if (const char* gv = getenv("PGK_GRAPHS")) c->use_graphs = atoi(gv) != 0;   // 0: launch MD steps eagerly
     c->natom = n;
     c->prec = p->precision;
     c->prm = *p;
@@ -425,7 +426,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         cap = ((cap + 31) / 32) * 32;
         c->ccap = std::max(cap, 32);
         if (cudaMalloc(&c->iperm, n * sizeof(int)) || cudaMalloc(&c->cell_of, n * sizeof(int)) ||
-            cudaMalloc(&c->subkey, n * sizeof(int)) || cudaMalloc(&c->counters, 8 * sizeof(unsigned long long))) {
+            cudaMalloc(&c->subkey, n * sizeof(int)) || cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)) ||
+            cudaMalloc(&c->hasup, std::max(n, 1))) {
             pgk_free(c);
             return PGK_E_NOMEM;
         }
@@ -458,7 +460,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
 pgk_status pgk_free(pgk_ctx* c) {
     if (!c) return PGK_OK;
     if (c->st) cudaStreamSynchronize(c->st);
-    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+    for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
                     c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list,
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
@@ -467,7 +469,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->ccnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->chunk_atom, c->chunk_term, c->cg_span, c->chunk_slot, c->inc_start, c->inc_slot,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
-                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin};
+                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -633,7 +635,7 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
     } else if (units) {
         *units = which == 3 ? (double)c->K[0] * c->K[1] * c->K[2] : (double)c->natom;
     }
-    if (which >= 1 && !c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
+    if (which >= 1 && which <= 3 && !c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
     cudaEvent_t e0, e1;
     PGK_CUDA(c, cudaEventCreate(&e0));
     PGK_CUDA(c, cudaEventCreate(&e1));
@@ -643,7 +645,9 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
             case 1: return spme_bench(c, 1);
             case 2: return spme_bench(c, 2);
             case 3: return spme_bench(c, 3);
-            default: return pgk_fail(c, PGK_E_INVALID, "unknown kernel id");
+            default:
+                if (which >= 64 && which < 128) return launch_intra(c, 0, which - 64, true);
+                return pgk_fail(c, PGK_E_INVALID, "unknown kernel id");
         }
     };
     if ((s = launch_zero_group(c, 0)) || (s = one())) return s;    // warm-up launch
@@ -664,6 +668,9 @@ void* pgk_stream(const pgk_ctx* c) { return c ? (void*)c->st : nullptr; }
 }  // extern "C"
 
 // ---- stage drivers ---------------------------------------------------------------
+static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
+                               bool tens, bool hfs, bool lt);
+
 // kind: 0 NVE (moldyn.F90), 1 NHC (moldyn_nhc.F90), 2 MTK (moldyn_mtk.F90),
 // 3 NVE + region Langevin + heat flux (moldyn_hf.F90); hf records go to the
 // device buffer c->hf_rec (kind 3), *nrec counts them
@@ -674,15 +681,16 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     if ((kind == 1 || kind == 2) && (md->mchain < 2 || md->mchain > 8 || md->nyosh < 1 || md->nyosh > 8 || md->next < 1))
         return pgk_fail(c, PGK_E_INVALID, "chain parameters");
     const int nb = c->prm.nstep_book > 0 ? c->prm.nstep_book : 1;
-    const double dts = md->dt_long_cal / (double)md->nstep_short;
-    const bool rattle = md->ifrattle && c->ncgroup > 0;
     const bool mtk = kind == 2;
-    const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);
     const bool hfdrv = kind == 3;
     const bool lt = hfdrv && c->hfp.nlangeregion > 0;
     const int hfi = c->hfp.heatfinterval > 0 ? c->hfp.heatfinterval : 1;
     const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
     long long nr = 0;
+    const bool graphs = c->use_graphs;
+    auto step_body = [&](int64_t st, bool e_, bool v_, bool t_, bool h_, bool l_) {
+        return md_step_body(c, kind, st, md, e_, v_, t_, h_, l_);
+    };
     pgk_status s;
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
     for (int64_t step = ini; step <= end; ++step) {
@@ -698,29 +706,56 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
-        } else {
-            if (lt) RUN(launch_langevin(c, md->dt_long_cal, step, true));
-            if (kind == 1 || kind == 2) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-            RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
-            for (int is = 1; is <= md->nstep_short; ++is) {
-                bool last = is == md->nstep_short;
-                if (is == 1) RUN(launch_kick_long(c));
-                RUN(launch_kick_short(c));
-                RUN(launch_drift(c, rattle));
-                if (mtk) RUN(launch_box_update(c, kind, *md));
-                if (rattle) RUN(launch_rattle_pos(c, md->eps_rattle, dts, mtk));
-                RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
-                if (last) {
-                    if (mtk && c->prm.mts_ewk == PGK_MTS_LONG) RUN(launch_rkcut(c));
-                    RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
-                    if (hfs) RUN(launch_hf_atm(c));
-                }
-                RUN(launch_kick_short(c));
-                if (last) RUN(launch_kick_long(c));
-                if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
+        } else if (graphs && c->list_valid && !hfs && !lt) {
+            // the step's kernel sequence depends only on (ene, vir, tens) and the
+            // list build; replay a captured CUDA graph of it
+            const int key = 8 * kind + ((ene ? 1 : 0) | (vir ? 2 : 0) | (tens ? 4 : 0));
+            if (memcmp(&c->graph_md, md, sizeof(pgk_mdparams)) != 0) {
+                for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
+                c->graphs.clear();
+                c->graph_md = *md;
             }
-            if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-            if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); RUN(launch_chain(c, chain_kind, *md)); }
+            auto it = c->graphs.find(key);
+            if (it == c->graphs.end() || it->second.epoch != c->list_epoch) {
+                // capture the step; a graph of an earlier list build is updated in
+                // place (same topology, new launch parameters), else instantiated
+                cudaGraph_t g = nullptr;
+                const long long l0 = c->launches;
+                PGK_CUDA(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+                pgk_status bs = step_body(step, ene, vir, tens, false, false);
+                cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+                if (bs) { if (g) cudaGraphDestroy(g); return bs; }
+                PGK_CUDA(c, ce);
+                const long long nl = c->launches - l0;
+                c->launches = l0;
+                bool updated = false;
+                if (it != c->graphs.end()) {
+                    cudaGraphExecUpdateResultInfo info;
+                    updated = cudaGraphExecUpdate(it->second.exec, g, &info) == cudaSuccess;
+                    if (!updated) {
+                        cudaGetLastError();
+                        cudaGraphExecDestroy(it->second.exec);
+                        c->graphs.erase(it);
+                    }
+                }
+                if (updated) {
+                    it->second.epoch = c->list_epoch;
+                    it->second.launches = nl;
+                    cudaGraphDestroy(g);
+                } else {
+                    cudaGraphExec_t ex = nullptr;
+                    cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                    cudaGraphDestroy(g);
+                    PGK_CUDA(c, ie);
+                    it = c->graphs.emplace(key, pgk_ctx::GraphEntry{ex, nl, c->list_epoch}).first;
+                }
+            }
+            PGK_CUDA(c, cudaGraphLaunch(it->second.exec, c->st));
+            c->launches += it->second.launches;
+        } else {
+            RUN(step_body(step, ene, vir, tens, hfs, lt));
+        }
+        if (step > 0) {
             if (lt) { RUN(launch_lt_regist(c)); RUN(launch_langevin(c, md->dt_long_cal, step, false)); }
             if (hfs) {
                 if (nr < c->hf_rec_cap) RUN(launch_heatf(c, c->hf_rec + nr * per));
@@ -732,6 +767,43 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
 #undef RUN
     if (nrec) *nrec = nr;
     return read_status(c);
+}
+
+// one MD step (step > 0) of run_md: the thermostat / barostat half steps and
+// the XO-RESPA loop with its force evaluations
+static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
+                               bool tens, bool hfs, bool lt) {
+    const double dts = md->dt_long_cal / (double)md->nstep_short;
+    const bool rattle = md->ifrattle && c->ncgroup > 0;
+    const bool mtk = kind == 2;
+    const bool hfdrv = kind == 3;
+    const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);
+    pgk_status s;
+#define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
+    if (lt) RUN(launch_langevin(c, md->dt_long_cal, step, true));
+    if (kind == 1 || kind == 2) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
+    RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
+    for (int is = 1; is <= md->nstep_short; ++is) {
+        bool last = is == md->nstep_short;
+        if (is == 1) RUN(launch_kick_long(c));
+        RUN(launch_kick_short(c));
+        RUN(launch_drift(c, rattle));
+        if (mtk) RUN(launch_box_update(c, kind, *md));
+        if (rattle) RUN(launch_rattle_pos(c, md->eps_rattle, dts, mtk));
+        RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
+        if (last) {
+            if (mtk && c->prm.mts_ewk == PGK_MTS_LONG) RUN(launch_rkcut(c));
+            RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
+            if (hfs) RUN(launch_hf_atm(c));
+        }
+        RUN(launch_kick_short(c));
+        if (last) RUN(launch_kick_long(c));
+        if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
+    }
+    if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
+    if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); RUN(launch_chain(c, chain_kind, *md)); }
+#undef RUN
+    return PGK_OK;
 }
 
 extern "C" {

@@ -111,8 +111,11 @@ struct pgk_ctx {
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
     double4* xq64 = nullptr;      // fp64: x,y,z,q sorted
     int* typ_s = nullptr;
-    unsigned long long* counters = nullptr;   // [0] nlistnball, [1] max cluster row, [3] max atom row
+    unsigned long long* counters = nullptr;   // [0] list pairs, [1] longest cluster row, [2] rows without
+                                              //  a higher-index partner; [4..6] count_pairs scratch
+    unsigned char* hasup = nullptr;           // [N] atom has a list partner of higher index
     bool list_valid = false;
+    long long list_epoch = 0;     // incremented by every list build (invalidates captured graphs)
 
     // ---- SPME ----
     int K[3] = {0, 0, 0};
@@ -143,8 +146,11 @@ struct pgk_ctx {
     double* lt_frand = nullptr;   // [3N] random accelerations of the former half step
     double* lt_dekin = nullptr;   // [8] det_ene_kin
 
-    // ---- CUDA graphs ----
-    std::map<long long, cudaGraphExec_t> graphs;
+    // ---- CUDA graphs of captured MD steps (key: driver kind and step flags);
+    //      valid for one list build and one set of integrator parameters ----
+    struct GraphEntry { cudaGraphExec_t exec; long long launches; long long epoch; };
+    std::map<int, GraphEntry> graphs;
+    pgk_mdparams graph_md{};
     bool use_graphs = true;
 
     // ---- scratch for host transfers ----

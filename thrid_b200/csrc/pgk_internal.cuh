@@ -66,7 +66,7 @@ struct DynState {
     double cellsize[3];
     int    list_mode_used;
     long long nlistnball;         // reference-format count of the last build
-    int    nmaxrow;               // longest full row of the last build
+    int    nmaxrow;               // longest cluster row of the last build (entries)
 };
 
 struct ChainDev {                 // device mirror of pgk_chain + derived
