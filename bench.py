@@ -334,6 +334,82 @@ def dist_max(x, world):
     return float(x)
 
 
+def serve_replica(rng, k, precision):
+    """One replica of the serving workload: a water or propanol box of 1.5k-30k
+    atoms (log-uniform), rc <= 10 A, SPME at ~1 A grid spacing."""
+    from thrid_b200 import systems as S
+    natom = float(np.exp(rng.uniform(np.log(1500.0), np.log(30000.0))))
+    if rng.random() < 0.5:
+        nside = max(6, int(round((natom / 3.0) ** (1.0 / 3.0))))
+        s = S.small_box("water", nside=nside, spacing=3.1, precision=precision, seed=100 + k,
+                        nfft=_nfft(nside * 3.1), order=4, rcut=min(10.0, nside * 3.1 / 2.0 - 2.2))
+    else:
+        nside = max(3, int(round((natom / 12.0) ** (1.0 / 3.0))))
+        s = S.small_box("propanol", nside=nside, spacing=5.2, precision=precision, seed=100 + k,
+                        nfft=_nfft(nside * 5.2), order=4, rcut=min(10.0, nside * 5.2 / 2.0 - 2.2))
+    return s
+
+
+def _nfft(L):
+    for k in (16, 20, 24, 32, 40, 48, 64, 80, 96, 128):
+        if k >= L:
+            return k
+    return 128
+
+
+def run_serve(args):
+    """Continuous batching of independent replicas (the serving configuration):
+    Poisson arrivals, admission by slots and memory, per-replica latency."""
+    import torch
+    from thrid_b200 import abi
+    from thrid_b200 import systems as S
+    from thrid_b200.serve import ReplicaServer
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(args.serve_seed)
+    reps = [serve_replica(rng, k, abi.PREC_MIXED) for k in range(args.serve_replicas)]
+    md = abi.md_struct(S.fs_to_reduced(1.0), ifrattle=1, outinterval=0)
+    work = sum(s.natom for s in reps) * args.serve_steps
+
+    def run(slots, arrivals):
+        srv = ReplicaServer(max_slots=slots)
+        t0 = time.perf_counter()
+        ids = []
+        for s, ta in zip(reps, arrivals):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(srv.submit(s, md, kind=0, nsteps=args.serve_steps))
+        res = [srv.result(i) for i in ids]
+        srv.close()
+        t = np.array([r[5] for r in res])
+        lat = t[:, 2] - t[:, 0]
+        span = t[:, 2].max() - t[:, 0].min()
+        return lat, span
+
+    # warm-up (library load, first context)
+    srv = ReplicaServer(max_slots=1)
+    srv.result(srv.submit(reps[0], md, kind=0, nsteps=5))
+    srv.close()
+    seq_lat, seq_span = run(1, [0.0] * len(reps))               # one at a time, all queued at t=0
+    mean_service = seq_span / len(reps)
+    gaps = rng.exponential(mean_service / args.serve_load * 1.0, size=len(reps))
+    arrivals = np.cumsum(gaps) - gaps[0]
+    lat, span = run(args.serve_slots, arrivals)
+    return {
+        "metric": "replica serving: aggregate atom-steps/s and p50/p99 latency (mixed precision)",
+        "value": work / span, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "config": {"workload": "poisson_replicas_water_or_propanol_1.5k-30k_nve", "replicas": len(reps),
+                   "steps_per_replica": args.serve_steps, "slots": args.serve_slots,
+                   "offered_load": args.serve_load, "natom_total": int(sum(s.natom for s in reps))},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "one_at_a_time": {"value": work / seq_span, "unit": UNIT,
+                          "latency_p50_s": float(np.percentile(seq_lat, 50)),
+                          "latency_p99_s": float(np.percentile(seq_lat, 99))},
+        "data": "synthetic (seeded lattices)",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,8 +419,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison leg")
+    ap.add_argument("--serve", action="store_true", help="replica-serving benchmark instead of the main line")
+    ap.add_argument("--serve-replicas", type=int, default=32)
+    ap.add_argument("--serve-steps", type=int, default=1000)
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-load", type=float, default=4.0, help="arrival rate / one-at-a-time service rate")
+    ap.add_argument("--serve-seed", type=int, default=2025)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.serve:
+        print(json.dumps(run_serve(args)))
+        return
     rank, world, local = dist_init()
     if args.impl == "reference":
         out = run_reference(args, rank, world)

@@ -400,6 +400,8 @@ pgk_status pgk_server_wait(pgk_server* sv, int64_t id);
 pgk_status pgk_server_result(pgk_server* sv, int64_t id, double* atmcor, double* atmvel, double* box,
                              pgk_energies* ene, double* hf_out, int64_t cap_records, int64_t* nrecords,
                              double* times3);
+/* Error text of a failed request ("" when it succeeded). */
+const char* pgk_server_error(pgk_server* sv, int64_t id);
 pgk_status pgk_server_release(pgk_server* sv, int64_t id);
 /* Finishes every queued request, then stops the workers. */
 pgk_status pgk_server_free(pgk_server* sv);

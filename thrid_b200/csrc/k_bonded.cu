@@ -932,11 +932,11 @@ pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want) {
     a.facc = c->facc[group]; a.acc = c->acc + (size_t)group * NACC; a.status = c->status;
     if (c->mixed()) {
         size_t sm = (size_t)3 * INTRA_SLOTS * sizeof(float);
-        cudaFuncSetAttribute(k_intra<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_limit(k_intra<true>, sm);
         k_intra<true><<<c->nchunk, 128, sm, c->st>>>(c->pos, a, c->dyn);
     } else {
         size_t sm = (size_t)3 * INTRA_SLOTS * sizeof(double);
-        cudaFuncSetAttribute(k_intra<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        smem_limit(k_intra<false>, sm);
         k_intra<false><<<c->nchunk, 128, sm, c->st>>>(c->pos, a, c->dyn);
     }
     PGK_LAUNCHED(c);

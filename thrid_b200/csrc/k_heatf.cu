@@ -440,6 +440,7 @@ pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p) {
 
 static pgk_status ensure_hf_slots(pgk_ctx* c) {
     if (c->hf_slots_cap >= c->npad_cap) return PGK_OK;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     cudaFree(c->hf_zs); cudaFree(c->hf_ms);
     c->hf_zs = nullptr; c->hf_ms = nullptr;
     PGK_CUDA(c, cudaMalloc(&c->hf_zs, sizeof(double) * c->npad_cap));
@@ -480,11 +481,11 @@ pgk_status launch_hf_atm(pgk_ctx* c) {
         int blocks = std::min((c->ncl + 3) / 4, c->nsm * 8);
         if (c->mixed()) {
             size_t sm = (size_t)4 * 8 * per * sizeof(float);
-            cudaFuncSetAttribute(k_hf_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            smem_limit(k_hf_pair<true>, sm);
             k_hf_pair<true><<<blocks, 128, sm, c->st>>>(c->xq, nullptr, a, c->lj32, c->lj64, h, c->dyn);
         } else {
             size_t sm = (size_t)4 * 8 * per * sizeof(double);
-            cudaFuncSetAttribute(k_hf_pair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            smem_limit(k_hf_pair<false>, sm);
             k_hf_pair<false><<<blocks, 128, sm, c->st>>>(nullptr, c->xq64, a, c->lj32, c->lj64, h, c->dyn);
         }
         PGK_LAUNCHED(c);

@@ -340,6 +340,7 @@ static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
 }
 
 pgk_status launch_mklist(pgk_ctx* c) {
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);   // may grow the list arrays
     int n = c->natom;
     // the box may have changed on the device (MTK): read it back
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));

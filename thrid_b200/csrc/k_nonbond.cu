@@ -358,7 +358,7 @@ template <int MODE>
 static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-    cudaFuncSetAttribute(k_pair_mixed<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    smem_limit(k_pair_mixed<MODE>, sm);
     k_pair_mixed<MODE><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
 }
 
@@ -390,10 +390,10 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
     } else {
         size_t sm = (size_t)2 * c->nspl * sizeof(double4) + c->ntyp * c->ntyp * sizeof(double2);
         if (vmode != PM_FORCE) {
-            cudaFuncSetAttribute(k_pair_fp64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            smem_limit(k_pair_fp64<true>, sm);
             k_pair_fp64<true><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
         } else {
-            cudaFuncSetAttribute(k_pair_fp64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            smem_limit(k_pair_fp64<false>, sm);
             k_pair_fp64<false><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
         }
     }

@@ -571,7 +571,7 @@ pgk_status spme_setup(pgk_ctx* c) {
 template <typename T, int AXIS, int SRC, int NC, bool CONV>
 static void fft_launch(pgk_ctx* c, const FftDev& fd, int grid, int P, size_t sm, int sign, const ConvArgs& ca) {
     typedef typename C2<T>::t T2;
-    cudaFuncSetAttribute(k_fft<T, AXIS, SRC, NC, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    smem_limit(k_fft<T, AXIS, SRC, NC, CONV>, sm);
     k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, c->qacc, c->K[0], c->K[1], c->K[2], fd, P,
                                                             (T)sign, ca, c->dyn);
 }
@@ -788,8 +788,7 @@ static cudaError_t noalloc_fft_pass(unsigned char* base, const FftPlan& pl, int 
     if (AXIS == 0) P = std::max(1, 1024 / K1);
     int grid = AXIS == 0 ? (K2 * K3 + P - 1) / P : ((K1 + P - 1) / P) * (AXIS == 1 ? K3 : K2);
     size_t sm = (size_t)2 * P * (pl.n + 1) * sizeof(double2);
-    cudaError_t e = cudaFuncSetAttribute(k_fft<double, AXIS, SRC, 0, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = smem_limit(k_fft<double, AXIS, SRC, 0, false>, sm);
     if (e != cudaSuccess) return e;
     ConvArgs ca{};
     k_fft<double, AXIS, SRC, 0, false><<<grid, 256, sm, st>>>((double2*)(base + NOALLOC_OFF_QC),

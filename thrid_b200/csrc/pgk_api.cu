@@ -11,6 +11,19 @@
 
 #include "pgk_ctx.cuh"
 
+std::shared_mutex g_alloc_mu;   // see pgk_ctx.cuh
+
+cudaError_t smem_limit(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<const void*, size_t> limit;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = limit[kernel];
+    if (bytes <= cur) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 pgk_status launch_rkcut(pgk_ctx* c);
 pgk_status spme_bench(pgk_ctx* c, int which);
 
@@ -200,6 +213,7 @@ extern "C" {
 
 pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     if (!s || !p || !out) return PGK_E_INVALID;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     *out = nullptr;
     int n = s->natom;
     if (n >= (1 << 25)) return PGK_E_INVALID;   // sort key packs the atom index in 25 bits
@@ -459,6 +473,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
 
 pgk_status pgk_free(pgk_ctx* c) {
     if (!c) return PGK_OK;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     if (c->st) cudaStreamSynchronize(c->st);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
@@ -687,7 +702,6 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     const int hfi = c->hfp.heatfinterval > 0 ? c->hfp.heatfinterval : 1;
     const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
     long long nr = 0;
-    const bool graphs = c->use_graphs;
     auto step_body = [&](int64_t st, bool e_, bool v_, bool t_, bool h_, bool l_) {
         return md_step_body(c, kind, st, md, e_, v_, t_, h_, l_);
     };
@@ -706,7 +720,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
-        } else if (graphs && c->list_valid && !hfs && !lt) {
+        } else if (c->use_graphs && c->list_valid && !hfs && !lt) {
             // the step's kernel sequence depends only on (ene, vir, tens) and the
             // list build; replay a captured CUDA graph of it
             const int key = 8 * kind + ((ene ? 1 : 0) | (vir ? 2 : 0) | (tens ? 4 : 0));
@@ -721,11 +735,24 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                 // place (same topology, new launch parameters), else instantiated
                 cudaGraph_t g = nullptr;
                 const long long l0 = c->launches;
+                std::shared_lock<std::shared_mutex> capture_lock(g_alloc_mu);
                 PGK_CUDA(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
                 pgk_status bs = step_body(step, ene, vir, tens, false, false);
                 cudaError_t ce = cudaStreamEndCapture(c->st, &g);
-                if (bs) { if (g) cudaGraphDestroy(g); return bs; }
-                PGK_CUDA(c, ce);
+                capture_lock.unlock();
+                if (bs != PGK_OK || ce != cudaSuccess) {
+                    // nothing of the step ran during the failed capture: run it
+                    // eagerly and stop capturing on this context
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                    c->launches = l0;
+                    c->use_graphs = false;
+                    c->graph_fail = std::string(cudaGetErrorString(ce)) + (bs ? " / " + c->err : "");
+                    fprintf(stderr, "pgk: step capture failed (%s); this context runs its steps without graphs\n",
+                            c->graph_fail.c_str());
+                    RUN(step_body(step, ene, vir, tens, false, false));
+                    goto step_done;
+                }
                 const long long nl = c->launches - l0;
                 c->launches = l0;
                 bool updated = false;
@@ -752,6 +779,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             }
             PGK_CUDA(c, cudaGraphLaunch(it->second.exec, c->st));
             c->launches += it->second.launches;
+        step_done:;
         } else {
             RUN(step_body(step, ene, vir, tens, hfs, lt));
         }
@@ -819,6 +847,7 @@ pgk_status pgk_moldyn_mtk(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdpara
 
 pgk_status pgk_set_hf(pgk_ctx* c, const pgk_hfparams* hf) {
     if (!c || !hf) return PGK_E_INVALID;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     return hf_setup(c, hf);
 }
 
@@ -833,6 +862,7 @@ pgk_status pgk_moldyn_hf(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparam
         for (int64_t st = std::max<int64_t>(ini, 1); st <= end; ++st) expect += (hfi == 1 || st % hfi == 1) ? 1 : 0;
     long long want = hf_out ? std::min<long long>(expect, cap_records) : 0;
     if (per > 0 && want > c->hf_rec_cap) {
+        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
         cudaFree(c->hf_rec);
         c->hf_rec = nullptr;
         PGK_CUDA(c, cudaMalloc(&c->hf_rec, sizeof(double) * per * want));

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 #include <map>
+#include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
@@ -152,10 +154,25 @@ struct pgk_ctx {
     std::map<int, GraphEntry> graphs;
     pgk_mdparams graph_md{};
     bool use_graphs = true;
+    std::string graph_fail;       // why capture was switched off (empty: never failed)
 
     // ---- scratch for host transfers ----
     std::vector<double> hbuf;
 };
+
+// Device allocation and stream capture across host threads (replica server):
+// cudaMalloc/cudaFree may synchronise the device, which would invalidate a
+// capture running on another thread, so allocating code takes this mutex
+// exclusively and captures take it shared.
+extern std::shared_mutex g_alloc_mu;
+
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is a process-wide property of the kernel, shared by every context
+// and host thread, so it only ever grows (a lower value set by one replica
+// would make another replica's larger launch fail).
+cudaError_t smem_limit(const void* kernel, size_t bytes);
+template <typename K>
+inline cudaError_t smem_limit(K* kernel, size_t bytes) { return smem_limit((const void*)kernel, bytes); }
 
 // error helpers
 pgk_status pgk_fail(pgk_ctx* c, pgk_status s, const std::string& msg);

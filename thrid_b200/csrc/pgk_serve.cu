@@ -155,7 +155,7 @@ static void run_job(pgk_server* sv, Job* j) {
         j->v.resize(j->v0.size());
         s = pgk_download_state(c, j->x.data(), j->v.data(), j->box);
     }
-    if (s != PGK_OK && c) j->err = pgk_last_error(c);
+    if (s != PGK_OK) j->err = c ? pgk_last_error(c) : pgk_status_string(s);
     if (c) pgk_free(c);
     j->status = s;
 }
@@ -315,6 +315,14 @@ pgk_status pgk_server_result(pgk_server* sv, int64_t id, double* atmcor, double*
     }
     if (times3) { times3[0] = j->t_submit; times3[1] = j->t_start; times3[2] = j->t_done; }
     return PGK_OK;
+}
+
+const char* pgk_server_error(pgk_server* sv, int64_t id) {
+    if (!sv) return "";
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(id);
+    if (it == sv->jobs.end()) return "unknown request id";
+    return it->second->err.c_str();
 }
 
 pgk_status pgk_server_release(pgk_server* sv, int64_t id) {
