@@ -335,6 +335,19 @@ pgk_status pgk_get_hf_atm(pgk_ctx* ctx, double* pot_atm, double* viri_atm);
  * (-) per Langevin region) summed since the last call, then reset. */
 pgk_status pgk_langevin_dekin(pgk_ctx* ctx, double* det_ene_kin);
 
+/* ---- device-side output records (outene / outpre of output_data.F90) ----
+ * With a capacity set, every output step of the stage drivers (outinterval)
+ * appends one record to a device buffer instead of reading the accumulators
+ * back (no host synchronisation per output step); pgk_get_output copies the
+ * records out and clears the buffer.  Record layout (PGK_OUT_NCOL doubles):
+ *   [0] step, [1..13] the pgk_energies fields in struct order,
+ *   [14] sum(m v^2), [15] pint, [16..24] pintt (column-major), [25..27] box.
+ * pint/pintt are the barostat's values (moldyn_mtk); other drivers leave the
+ * last ones set.  Records beyond the capacity are counted but not kept. */
+#define PGK_OUT_NCOL 28
+pgk_status pgk_set_output(pgk_ctx* ctx, int64_t cap_records);
+pgk_status pgk_get_output(pgk_ctx* ctx, double* out, int64_t cap_records, int64_t* nrecords);
+
 /* Kinetic energy sum(m v^2) and atomic pressure tensor (calpress.F90, atomic
  * branch) of the current device state; press9 may be NULL. */
 pgk_status pgk_calpress(pgk_ctx* ctx, double* kint, double* pressatm_tot, double* press9);

@@ -576,3 +576,38 @@ pgk_status launch_copy_force(pgk_ctx* c, int group, double* dst) {
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
+
+// ---- output record (outene / outpre values) of the current step ----------------
+// Sums both MTS groups' accumulators like the host read-back does, adds the
+// Ewald self and net-charge constants, and stores one PGK_OUT_NCOL record.
+__global__ void k_out_record(const long long* __restrict__ acc, const DynState* __restrict__ dyn,
+                             const ChainDev* __restrict__ ch, int dbl, double pot_ewc, double alpha, double netchrgsq,
+                             int ifspme, long long step, double* __restrict__ r) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    auto S = [&](int k) { return acc_get(acc, k, dbl != 0) + acc_get(acc + NACC, k, dbl != 0); };
+    const double pi = 3.14159265358979323846;
+    const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    const double a1 = -pi / (alpha * alpha * vol);
+    double e_vdw = S(A_VDW), e_elc = S(A_ELC), e_ewk = S(A_EWK), e_v14 = S(A_VDW14), e_e14 = S(A_ELC14);
+    double e_b = S(A_BOND), e_a = S(A_ANGL), e_t = S(A_TORS), e_rb = S(A_TORSRB);
+    double e_ewc = ifspme ? pot_ewc : 0.0, e_nq = ifspme ? 0.5 * a1 * netchrgsq : 0.0;
+    double nonbon = e_vdw + e_elc + e_ewk + e_ewc + e_nq + e_v14 + e_e14;
+    double tot = e_b + e_a + e_t + e_rb + nonbon;
+    r[0] = (double)step;
+    r[1] = tot; r[2] = nonbon; r[3] = e_vdw; r[4] = e_elc; r[5] = e_ewk; r[6] = e_ewc; r[7] = e_nq;
+    r[8] = e_v14; r[9] = e_e14; r[10] = e_b; r[11] = e_a; r[12] = e_t; r[13] = e_rb;
+    r[14] = acc_get(acc, A_KE, dbl != 0);
+    r[15] = ch->pint;
+    for (int k = 0; k < 9; ++k) r[16 + k] = ch->pintt[k];
+    for (int d = 0; d < 3; ++d) r[25 + d] = dyn->box[d];
+}
+
+pgk_status launch_out_record(pgk_ctx* c, long long step, double* dst) {
+    pgk_status s;
+    if ((s = launch_kinetic(c, 0))) return s;
+    k_out_record<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, c->mixed() ? 0 : 1, c->pot_ewc, c->prm.alpha,
+                                      c->netchrgsq, c->prm.ifspme, step, dst);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}

@@ -484,7 +484,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->ccnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->chunk_atom, c->chunk_term, c->cg_span, c->chunk_slot, c->inc_start, c->inc_slot,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
-                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup};
+                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -702,6 +702,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     const int hfi = c->hfp.heatfinterval > 0 ? c->hfp.heatfinterval : 1;
     const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
     long long nr = 0;
+    long long last_rec = -1;
     auto step_body = [&](int64_t st, bool e_, bool v_, bool t_, bool h_, bool l_) {
         return md_step_body(c, kind, st, md, e_, v_, t_, h_, l_);
     };
@@ -709,7 +710,8 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
     for (int64_t step = ini; step <= end; ++step) {
         bool out = md->outinterval > 0 ? (step % md->outinterval == 0) : (step == end);
-        bool ene = out && eo;
+        const bool rec = out && c->out_cap > 0;         // device-side output record
+        bool ene = out && (eo || rec);
         bool vir = mtk;
         bool tens = mtk && md->pcont_axis != PGK_PCONT_ISO && !ene;   // nhcpanisoint reads diag(pintt) only
         if (step % nb == 1 || nb == 1 || step == 0) RUN(launch_transcor(c));
@@ -790,9 +792,24 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                 ++nr;
             }
         }
-        if (ene) RUN(read_acc(c, 3, eo, nullptr, true));
+        if (rec) {
+            if (c->out_n < c->out_cap) {
+                RUN(launch_out_record(c, step, c->out_rec + c->out_n * PGK_OUT_NCOL));
+                last_rec = c->out_n;
+            }
+            ++c->out_n;
+        } else if (ene) {
+            RUN(read_acc(c, 3, eo, nullptr, true));
+        }
     }
 #undef RUN
+    if (eo && last_rec >= 0) {          // energies of the last recorded output step
+        double r[PGK_OUT_NCOL];
+        PGK_CUDA(c, cudaMemcpyAsync(r, c->out_rec + last_rec * PGK_OUT_NCOL, sizeof(r), cudaMemcpyDeviceToHost,
+                                    c->st));
+        PGK_CUDA(c, cudaStreamSynchronize(c->st));
+        memcpy(eo, r + 1, sizeof(pgk_energies));
+    }
     if (nrec) *nrec = nr;
     return read_status(c);
 }
@@ -843,6 +860,35 @@ pgk_status pgk_moldyn_nhc(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdpara
 }
 pgk_status pgk_moldyn_mtk(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e) {
     return run_md(c, 2, ini, end, md, e);
+}
+
+pgk_status pgk_set_output(pgk_ctx* c, int64_t cap) {
+    if (!c || cap < 0) return PGK_E_INVALID;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    if (c->out_rec) { cudaFree(c->out_rec); c->out_rec = nullptr; }
+    c->out_cap = 0;
+    c->out_n = 0;
+    if (cap > 0) {
+        if (cudaMalloc(&c->out_rec, sizeof(double) * PGK_OUT_NCOL * (size_t)cap) != cudaSuccess) {
+            c->out_rec = nullptr;
+            return pgk_fail(c, PGK_E_NOMEM, "output record buffer");
+        }
+        c->out_cap = cap;
+    }
+    return PGK_OK;
+}
+
+pgk_status pgk_get_output(pgk_ctx* c, double* out, int64_t cap, int64_t* n) {
+    if (!c || cap < 0) return PGK_E_INVALID;
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    long long have = std::min<long long>(c->out_n, c->out_cap);
+    if (out && cap > 0 && have > 0)
+        PGK_CUDA(c, cudaMemcpy(out, c->out_rec, sizeof(double) * PGK_OUT_NCOL * std::min<long long>(have, cap),
+                               cudaMemcpyDeviceToHost));
+    if (n) *n = c->out_n;
+    c->out_n = 0;
+    return PGK_OK;
 }
 
 pgk_status pgk_set_hf(pgk_ctx* c, const pgk_hfparams* hf) {

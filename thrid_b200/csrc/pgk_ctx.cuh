@@ -127,6 +127,10 @@ struct pgk_ctx {
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
 
+    // ---- device-side output records ----
+    double* out_rec = nullptr;    // [out_cap][PGK_OUT_NCOL]
+    long long out_cap = 0, out_n = 0;
+
     // ---- heat flux and region Langevin thermostat (k_heatf.cu) ----
     bool hf_set = false;
     pgk_hfparams hfp{};           // host copy (pointer members cleared)
@@ -230,3 +234,4 @@ pgk_status launch_press(pgk_ctx* c);
 pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int phase);
 pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md);
 pgk_status launch_copy_force(pgk_ctx* c, int group, double* dst_dev);
+pgk_status launch_out_record(pgk_ctx* c, long long step, double* dst);

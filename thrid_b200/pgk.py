@@ -76,6 +76,8 @@ def lib():
     L.pgk_stream.argtypes = [vp]
     L.pgk_bench_kernel.argtypes = [vp, C.c_int32, C.c_int32, pd, pd, pd]
     L.pgk_set_hf.argtypes = [vp, C.POINTER(abi.HfParamsStruct)]
+    L.pgk_set_output.argtypes = [vp, C.c_int64]
+    L.pgk_get_output.argtypes = [vp, pd, C.c_int64, C.POINTER(C.c_int64)]
     L.pgk_moldyn_hf.argtypes = [vp, C.c_int64, C.c_int64, C.POINTER(abi.MdParamsStruct), E, pd, C.c_int64,
                                 C.POINTER(C.c_int64)]
     L.pgk_calheatf.argtypes = [vp, pd]
@@ -208,6 +210,21 @@ class PgkEngine:
 
     def moldyn_mtk(self, ini, end, md):
         return self._md(self.L.pgk_moldyn_mtk, ini, end, md)
+
+    # ---- device-side output records (outene / outpre) ----
+    OUT_COLUMNS = ("step",) + tuple(n for n, _ in abi.EnergiesStruct._fields_) + (
+        "kint", "pint") + tuple(f"pintt{k}" for k in range(9)) + ("xcel", "ycel", "zcel")
+
+    def set_output(self, cap_records):
+        self._check(self.L.pgk_set_output(self.h, int(cap_records)))
+        self._out_cap = int(cap_records)
+
+    def get_output(self):
+        cap = getattr(self, "_out_cap", 0)
+        out = np.zeros((max(cap, 1), len(self.OUT_COLUMNS)))
+        n = C.c_int64()
+        self._check(self.L.pgk_get_output(self.h, _p(out), cap, C.byref(n)))
+        return out[:min(n.value, cap)]
 
     # ---- heat flux + region Langevin (moldyn_hf.F90, calheatf.F90) ----
     def set_hf(self, hfd):
