@@ -181,7 +181,7 @@ __device__ __forceinline__ bool is_excluded(const int* __restrict__ exs_idx, con
 __global__ void __launch_bounds__(256) k_build_clist(
         const double* __restrict__ pos_s, const int* __restrict__ perm, const int* __restrict__ cell_of,
         const int* __restrict__ cell_start, const int* __restrict__ cell_cnt, const int* __restrict__ exs_idx,
-        const int* __restrict__ exs_list, int n, int ncl, int ccap, double sqcut, double rbox,
+        const int* __restrict__ exs_list, int n, int ncl, int ccap, int sort_rows, double sqcut, double rbox,
         const DynState* __restrict__ dyn, int* __restrict__ clist, int* __restrict__ ccnt,
         unsigned char* __restrict__ hasup, unsigned long long* __restrict__ counters, unsigned* __restrict__ status) {
     __shared__ double spi[8][3 * 8];
@@ -279,6 +279,44 @@ __global__ void __launch_bounds__(256) k_build_clist(
                     count += __popc(m);
                 }
             }
+        }
+    }
+    // Group the row's entries by mask (stable counting sort in shared memory):
+    // 32 consecutive entries then mostly share one mask, so the pair kernel's
+    // loop over the mask bits is uniform across the warp.  Entries keep their
+    // candidate (spatial) order inside a mask group; the result is the same on
+    // every build of the same positions.
+    if (sort_rows && count <= ccap) {
+        extern __shared__ int srow_raw[];
+        int* buf = srow_raw + (size_t)wib * (ccap + 256);
+        int* bin = buf + ccap;
+        for (int q = lane; q < 256; q += 32) bin[q] = 0;
+        __syncwarp();
+        for (int k = lane; k < count; k += 32) {
+            const int e = row[k];
+            buf[k] = e;
+            atomicAdd(&bin[(unsigned)e >> 24], 1);
+        }
+        __syncwarp();
+        if (lane == 0) {                        // exclusive scan of the 256 bins
+            int run = 0;
+            for (int q = 0; q < 256; ++q) { int v = bin[q]; bin[q] = run; run += v; }
+        }
+        __syncwarp();
+        for (int k0 = 0; k0 < count; k0 += 32) {
+            const int k = k0 + lane;
+            const bool ok = k < count;
+            const int e = ok ? buf[k] : 0;
+            const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(grp & ((1u << lane) - 1u));
+            const int base = ok ? bin[key] : 0;
+            __syncwarp();
+            if (ok) {
+                row[base + rank] = e;
+                if (rank == 0) bin[key] = base + __popc(grp);
+            }
+            __syncwarp();
         }
     }
     up = __reduce_or_sync(0xffffffffu, up);
@@ -384,9 +422,13 @@ pgk_status launch_mklist(pgk_ctx* c) {
         double sq = c->prm.rcut_book * c->prm.rcut_book;
         long long threads = (long long)c->ncl * 32;
         PGK_CUDA(c, cudaMemsetAsync(c->hasup, 0, (size_t)n, c->st));
-        k_build_clist<<<(unsigned)((threads + 255) / 256), 256, 0, c->st>>>(
+        // rows are grouped by mask in shared memory when 8 rows fit (<= 160 KB)
+        const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
+        const int sort_rows = sort_sm <= 160 * 1024 ? 1 : 0;
+        if (sort_rows) PGK_CUDA(c, smem_limit(k_build_clist, sort_sm));
+        k_build_clist<<<(unsigned)((threads + 255) / 256), 256, sort_rows ? sort_sm : 0, c->st>>>(
             c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, n, c->ncl, c->ccap,
-            sq, c->prm.rcut_book + 0.05, c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
+            sort_rows, sq, c->prm.rcut_book + 0.05, c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
         if (n > 1) k_count_noup<<<(n - 1 + 255) / 256, 256, 0, c->st>>>(c->hasup, n - 1, c->counters);
         c->launches += 7;
         PGK_CUDA(c, cudaGetLastError());
