@@ -6,13 +6,13 @@
 //   calnon14p  calnon14.F90:249-521     scaled 1-4 Coulomb + LJ
 //   ewaldrp excluded-pair erf correction (ewaldr.F90:756-826)
 //
-// Hot path: k_intra, one CTA per chunk of whole molecules (atoms contiguous):
-// the chunk's positions are staged in shared memory, every term writes the
-// force on each of its atoms into its own shared-memory slot, and each atom
-// then sums its slots in a fixed order -- no atomics inside the chunk,
-// deterministic in both precisions -- before one global add per atom
-// component.  The per-term-type kernels (k_bond, k_angl, k_tors, k_non14,
-// k_excl) serve systems whose molecules are not contiguous or too large.
+// Layout: every term type writes the force on each of its atoms into its own
+// slot of one global slot array (slot = base[type] + K*term + q, SoA x|y|z),
+// one thread per term and one kernel per type, with no atomics; then
+// k_slot_gather sums each atom's slots in a fixed order (a precomputed
+// incidence list) and adds the total to the group's force accumulator once.
+// The result is deterministic in both precisions and needs no assumption on
+// molecule layout.  Energies and virials are block-reduced per type.
 //
 // Displacements are formed in FP64 from the master positions (Fortran anint
 // minimum image); the remaining arithmetic runs in T (float for mixed).
@@ -59,6 +59,28 @@ __device__ __forceinline__ void vir_abs(double* v, const double* f, const double
     for (int b = 0; b < 3; ++b)
 #pragma unroll
         for (int a = 0; a < 3; ++a) v[1 + a + 3 * b] += f[a] * x[b];
+}
+
+// where a term kernel puts its forces: the slot array (slot = base + K*term + q)
+// or, when slot is null, the force accumulator (atomics)
+struct TermOut {
+    void* facc;
+    void* slot;          // [3][S] of T
+    long long S, base;
+};
+template <bool MIXED>
+__device__ __forceinline__ void put_force(const TermOut& o, int term, int K, int q, int atom, const double* F,
+                                          double sgn) {
+    typedef typename std::conditional<MIXED, float, double>::type T;
+    if (o.slot) {
+        T* sl = (T*)o.slot;
+        const size_t k = (size_t)o.base + (size_t)K * term + q;
+        sl[k] = (T)(sgn * F[0]);
+        sl[o.S + k] = (T)(sgn * F[1]);
+        sl[2 * o.S + k] = (T)(sgn * F[2]);
+    } else {
+        force_add<MIXED>(o.facc, atom, sgn * F[0], sgn * F[1], sgn * F[2]);
+    }
 }
 
 // ---- term evaluators (P = positions, indices into P) ------------------------
@@ -249,18 +271,17 @@ __device__ __forceinline__ void eval_excl(const double* P, int i, int j, double 
 // ---- per-term-type kernels (general path) -------------------------------------
 template <bool MIXED>
 __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ ij, const double2* __restrict__ par,
-                       int nterm, const DynState* __restrict__ dyn, void* facc, long long* acc, int want) {
+                       int nterm, const DynState* __restrict__ dyn, TermOut out, long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
     if (k < nterm) {
-        double F[3], rd[3], e;
+        double F[3] = {0, 0, 0}, rd[3], e;
         int i = ij[k].x, j = ij[k].y;
-        if (eval_bond<T>(pos, i, j, par[k], dyn, F, rd, e)) {
-            force_add<MIXED>(facc, i, F[0], F[1], F[2]);
-            force_add<MIXED>(facc, j, -F[0], -F[1], -F[2]);
-            if (want) { v[0] = e; vir_pair(v + 1, F, rd); }
-        }
+        const bool on = eval_bond<T>(pos, i, j, par[k], dyn, F, rd, e);
+        put_force<MIXED>(out, k, 2, 0, i, F, 1.0);
+        put_force<MIXED>(out, k, 2, 1, j, F, -1.0);
+        if (want && on) { v[0] = e; vir_pair(v + 1, F, rd); }
     }
     if (want) {
         const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
@@ -271,21 +292,20 @@ __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ 
 
 template <bool MIXED>
 __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ ijk, const double2* __restrict__ par,
-                       int nterm, const DynState* __restrict__ dyn, void* facc, long long* acc, int want) {
+                       int nterm, const DynState* __restrict__ dyn, TermOut out, long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
     if (n < nterm) {
-        double F[3][3], e;
+        double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
         int at[3] = {ijk[n].x, ijk[n].y, ijk[n].z};
-        if (eval_angl<T>(pos, at[0], at[1], at[2], par[n], dyn, F, e)) {
+        const bool on = eval_angl<T>(pos, at[0], at[1], at[2], par[n], dyn, F, e);
 #pragma unroll
-            for (int q = 0; q < 3; ++q) force_add<MIXED>(facc, at[q], F[q][0], F[q][1], F[q][2]);
-            if (want) {
-                v[0] = e;
+        for (int q = 0; q < 3; ++q) put_force<MIXED>(out, n, 3, q, at[q], F[q], 1.0);
+        if (want && on) {
+            v[0] = e;
 #pragma unroll
-                for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], pos, at[q]);
-            }
+            for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], pos, at[q]);
         }
     }
     if (want) {
@@ -297,7 +317,7 @@ __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ 
 
 template <bool MIXED, bool RB>
 __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ ijkl, const double4* __restrict__ par,
-                       const double* __restrict__ rbc, int nterm, const DynState* __restrict__ dyn, void* facc,
+                       const double* __restrict__ rbc, int nterm, const DynState* __restrict__ dyn, TermOut out,
                        long long* acc, int want, unsigned* status) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -308,7 +328,7 @@ __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ 
         eval_tors<T, RB>(pos, at[0], at[1], at[2], at[3], RB ? make_double4(0, 0, 0, 0) : par[n],
                          RB ? rbc + 6 * (size_t)n : nullptr, dyn, F, e, status);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) force_add<MIXED>(facc, at[q], F[q][0], F[q][1], F[q][2]);
+        for (int q = 0; q < 4; ++q) put_force<MIXED>(out, n, 4, q, at[q], F[q], 1.0);
         if (want) {
             v[0] = e;
 #pragma unroll
@@ -325,7 +345,7 @@ __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ 
 template <bool MIXED>
 __global__ void k_non14(const double* __restrict__ pos, const double* __restrict__ chrg, const int* __restrict__ typ,
                         const int2* __restrict__ ij, const double2* __restrict__ fac, int nterm, int ntyp,
-                        const double2* __restrict__ lj64, const DynState* __restrict__ dyn, void* facc,
+                        const double2* __restrict__ lj64, const DynState* __restrict__ dyn, TermOut out,
                         long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -334,8 +354,8 @@ __global__ void k_non14(const double* __restrict__ pos, const double* __restrict
         int i = ij[n].x, j = ij[n].y;
         double F[3], rd[3], de, dv;
         eval_14<T>(pos, i, j, chrg[i] * chrg[j], lj64[typ[i] * ntyp + typ[j]], fac[n], dyn, F, rd, de, dv);
-        force_add<MIXED>(facc, i, F[0], F[1], F[2]);
-        force_add<MIXED>(facc, j, -F[0], -F[1], -F[2]);
+        put_force<MIXED>(out, n, 2, 0, i, F, 1.0);
+        put_force<MIXED>(out, n, 2, 1, j, F, -1.0);
         if (want) { v[0] = de; v[1] = dv; vir_pair(v + 2, F, rd); }
     }
     if (want) {
@@ -349,15 +369,15 @@ template <bool MIXED>
 __global__ void k_excl(const double* __restrict__ pos, const double* __restrict__ chrg,
                        const int2* __restrict__ pairs, int npair, const double4* __restrict__ spl64,
                        const float4* __restrict__ spl32, int nspl, double h, const DynState* __restrict__ dyn,
-                       void* facc, long long* acc, int want) {
+                       TermOut out, long long* acc, int want) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
     if (k < npair) {
         int i = pairs[k].x, j = pairs[k].y;
         double F[3], rd[3], e;
         eval_excl<MIXED>(pos, i, j, chrg[i] * chrg[j], spl64, spl32, nspl, h, dyn, F, rd, e);
-        force_add<MIXED>(facc, i, F[0], F[1], F[2]);
-        force_add<MIXED>(facc, j, -F[0], -F[1], -F[2]);
+        put_force<MIXED>(out, k, 2, 0, i, F, 1.0);
+        put_force<MIXED>(out, k, 2, 1, j, F, -1.0);
         v[0] = -e;
         vir_pair(v + 1, F, rd);
     }
@@ -369,197 +389,31 @@ __global__ void k_excl(const double* __restrict__ pos, const double* __restrict_
     }
 }
 
-// ---- fused intramolecular kernel ----------------------------------------------
-// Gather formulation, no atomics inside the chunk: every term writes the force
-// on each of its atoms into its own slot (slots of a term type are laid out
-// term by term, k slots per k-atom term); then each atom sums its slots in a
-// fixed order (precomputed incidence list), so the result is deterministic in
-// both precisions.  Chunks are whole molecules with at most INTRA_ATOMS atoms
-// and INTRA_SLOTS slots.
-#define INTRA_ATOMS 64
-#define INTRA_SLOTS 2048
-
-struct IntraArgs {
-    const int* chunk_atom;          // [nchunk+1] first atom of each chunk
-    const int* chunk_term;          // [6][nchunk+1] term ranges per type
-    const int* chunk_slot;          // [6][nchunk] slot base of each type inside its chunk
-    const int* inc_start;           // [natom+1] incidence CSR (chunk-local slot ids)
-    const unsigned short* inc_slot;
-    int nchunk;
-    int mask;                       // bit t: evaluate term type t (0 bond,1 angl,2 tors,3 torsrb,4 1-4,5 excl)
-    int want;
-    const int2* bond_ij; const double2* bond_p;
-    const int4* angl_ijk; const double2* angl_p;
-    const int4* tors_ijkl; const double4* tors_p;
-    const int4* rb_ijkl; const double* rb_c;
-    const int2* p14_ij; const double2* p14_f;
-    const int2* expair;
-    const double* chrg; const int* typ; int ntyp; const double2* lj64;
-    const double4* spl64; const float4* spl32; int nspl; double h;
-    void* facc; long long* acc; unsigned* status;
-};
-
-template <typename T>
-__device__ __forceinline__ void put(T* sx, T* sy, T* sz, int slot, const double* F, double sign) {
-    sx[slot] = (T)(sign * F[0]);
-    sy[slot] = (T)(sign * F[1]);
-    sz[slot] = (T)(sign * F[2]);
-}
+// ---- per-atom sum of the slot forces --------------------------------------------
+// type of a slot from the type bases; only the types in `mask` were written by
+// this evaluation, the others hold another MTS group's values and are skipped
+struct SlotTypes { long long base[7]; };
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_intra(const double* __restrict__ pos, IntraArgs a,
-                                               const DynState* __restrict__ dyn) {
+__global__ void k_slot_gather(const int* __restrict__ inc_start, const int* __restrict__ inc_slot,
+                              const void* __restrict__ slot, SlotTypes ty, int mask, int n, void* facc) {
     typedef typename std::conditional<MIXED, float, double>::type T;
-    __shared__ double sp[3 * INTRA_ATOMS];
-    __shared__ unsigned short s_inc[INTRA_SLOTS];     // the chunk's incidence lists
-    __shared__ int s_start[INTRA_ATOMS + 1];
-    __shared__ double s_q[INTRA_ATOMS];                // charges and LJ types of the chunk
-    __shared__ int s_t[INTRA_ATOMS];
-    extern __shared__ unsigned char slot_raw[];
-    T* sx = (T*)slot_raw;
-    T* sy = sx + INTRA_SLOTS;
-    T* sz = sy + INTRA_SLOTS;
-    const int c = blockIdx.x;
-    const int a0 = a.chunk_atom[c], na = a.chunk_atom[c + 1] - a0;
-    const int i0 = a.inc_start[a0], ni = a.inc_start[a0 + na] - i0;
-    for (int k = threadIdx.x; k < 3 * na; k += blockDim.x) sp[k] = pos[3 * (size_t)a0 + k];
-    for (int k = threadIdx.x; k <= na; k += blockDim.x) s_start[k] = a.inc_start[a0 + k] - i0;
-    for (int k = threadIdx.x; k < ni; k += blockDim.x) s_inc[k] = a.inc_slot[i0 + k];
-    for (int k = threadIdx.x; k < na; k += blockDim.x) { s_q[k] = a.chrg[a0 + k]; s_t[k] = a.typ[a0 + k]; }
-    __syncthreads();
-    const int stride = a.nchunk + 1;
-    const int* cs = a.chunk_slot;
-    if (a.mask & 1) {   // bonds (2 slots)
-        double v[11] = {0};
-        const int t0 = a.chunk_term[c];
-        for (int t = t0 + threadIdx.x; t < a.chunk_term[c + 1]; t += blockDim.x) {
-            int i = a.bond_ij[t].x - a0, j = a.bond_ij[t].y - a0;
-            double F[3] = {0, 0, 0}, rd[3], e;
-            bool on = eval_bond<T>(sp, i, j, a.bond_p[t], dyn, F, rd, e);
-            int sl = cs[c] + 2 * (t - t0);
-            put(sx, sy, sz, sl, F, 1.0);
-            put(sx, sy, sz, sl + 1, F, -1.0);
-            if (a.want && on) { v[0] += e; vir_pair(v + 1, F, rd); }
-        }
-        if (a.want) {
-            const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
-                                 A_VTB + 6, A_VTB + 7, A_VTB + 8};
-            block_acc<11>(v, a.acc, idx, !MIXED);
-            __syncthreads();
-        }
-    }
-    if (a.mask & 2) {   // angles (3 slots)
-        double v[11] = {0};
-        const int t0 = a.chunk_term[stride + c];
-        for (int t = t0 + threadIdx.x; t < a.chunk_term[stride + c + 1]; t += blockDim.x) {
-            const int at[3] = {a.angl_ijk[t].x - a0, a.angl_ijk[t].y - a0, a.angl_ijk[t].z - a0};
-            double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
-            bool on = eval_angl<T>(sp, at[0], at[1], at[2], a.angl_p[t], dyn, F, e);
-            int sl = cs[a.nchunk + c] + 3 * (t - t0);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long S = ty.base[6];
+    const T* sx = (const T*)slot;
+    const T* sy = sx + S;
+    const T* sz = sy + S;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int k = inc_start[i]; k < inc_start[i + 1]; ++k) {
+        const int sl = inc_slot[k];
+        int t = 0;
 #pragma unroll
-            for (int q = 0; q < 3; ++q) put(sx, sy, sz, sl + q, F[q], 1.0);
-            if (a.want && on) {
-                v[0] += e;
-#pragma unroll
-                for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], sp, at[q]);
-            }
-        }
-        if (a.want) {
-            const int idx[11] = {A_ANGL, A_VA, A_VTA + 0, A_VTA + 1, A_VTA + 2, A_VTA + 3, A_VTA + 4, A_VTA + 5,
-                                 A_VTA + 6, A_VTA + 7, A_VTA + 8};
-            block_acc<11>(v, a.acc, idx, !MIXED);
-            __syncthreads();
-        }
+        for (int q = 1; q < 6; ++q) t += sl >= ty.base[q] ? 1 : 0;
+        if (!((mask >> t) & 1)) continue;
+        fx += (double)sx[sl]; fy += (double)sy[sl]; fz += (double)sz[sl];
     }
-    for (int rb = 0; rb < 2; ++rb) {   // periodic (type 2) and Ryckaert-Bellemans (type 3) torsions (4 slots)
-        if (!(a.mask & (4 << rb))) continue;
-        double v[11] = {0};
-        const int ty = 2 + rb;
-        const int t0 = a.chunk_term[ty * stride + c];
-        for (int t = t0 + threadIdx.x; t < a.chunk_term[ty * stride + c + 1]; t += blockDim.x) {
-            const int4 q4 = rb ? a.rb_ijkl[t] : a.tors_ijkl[t];
-            const int at[4] = {q4.x - a0, q4.y - a0, q4.z - a0, q4.w - a0};
-            double F[4][3], e;
-            if (rb) eval_tors<T, true>(sp, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0),
-                                       a.rb_c + 6 * (size_t)t, dyn, F, e, a.status);
-            else eval_tors<T, false>(sp, at[0], at[1], at[2], at[3], a.tors_p[t], nullptr, dyn, F, e, a.status);
-            int sl = cs[ty * a.nchunk + c] + 4 * (t - t0);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) put(sx, sy, sz, sl + q, F[q], 1.0);
-            if (a.want) {
-                v[0] += e;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) vir_abs(v + 1, F[q], sp, at[q]);
-            }
-        }
-        if (a.want) {
-            const int idx[11] = {rb ? A_TORSRB : A_TORS, A_VT, A_VTT + 0, A_VTT + 1, A_VTT + 2, A_VTT + 3,
-                                 A_VTT + 4, A_VTT + 5, A_VTT + 6, A_VTT + 7, A_VTT + 8};
-            block_acc<11>(v, a.acc, idx, !MIXED);
-            __syncthreads();
-        }
-    }
-    if (a.mask & 16) {  // 1-4 pairs (2 slots)
-        double v[12] = {0};
-        const int t0 = a.chunk_term[4 * stride + c];
-        for (int t = t0 + threadIdx.x; t < a.chunk_term[4 * stride + c + 1]; t += blockDim.x) {
-            int gi = a.p14_ij[t].x, gj = a.p14_ij[t].y;
-            double F[3], rd[3], de, dv;
-            eval_14<T>(sp, gi - a0, gj - a0, s_q[gi - a0] * s_q[gj - a0], a.lj64[s_t[gi - a0] * a.ntyp + s_t[gj - a0]],
-                       a.p14_f[t], dyn, F, rd, de, dv);
-            int sl = cs[4 * a.nchunk + c] + 2 * (t - t0);
-            put(sx, sy, sz, sl, F, 1.0);
-            put(sx, sy, sz, sl + 1, F, -1.0);
-            if (a.want) { v[0] += de; v[1] += dv; vir_pair(v + 2, F, rd); }
-        }
-        if (a.want) {
-            const int idx[12] = {A_ELC14, A_VDW14, A_V14, A_VT14 + 0, A_VT14 + 1, A_VT14 + 2, A_VT14 + 3,
-                                 A_VT14 + 4, A_VT14 + 5, A_VT14 + 6, A_VT14 + 7, A_VT14 + 8};
-            block_acc<12>(v, a.acc, idx, !MIXED);
-            __syncthreads();
-        }
-    }
-    if (a.mask & 32) {  // excluded-pair Ewald correction (2 slots)
-        double v[11] = {0};
-        const int t0 = a.chunk_term[5 * stride + c];
-        for (int t = t0 + threadIdx.x; t < a.chunk_term[5 * stride + c + 1]; t += blockDim.x) {
-            int gi = a.expair[t].x, gj = a.expair[t].y;
-            double F[3], rd[3], e;
-            eval_excl<MIXED>(sp, gi - a0, gj - a0, s_q[gi - a0] * s_q[gj - a0], a.spl64, a.spl32, a.nspl, a.h, dyn,
-                             F, rd, e);
-            int sl = cs[5 * a.nchunk + c] + 2 * (t - t0);
-            put(sx, sy, sz, sl, F, 1.0);
-            put(sx, sy, sz, sl + 1, F, -1.0);
-            if (a.want) { v[0] -= e; vir_pair(v + 1, F, rd); }
-        }
-        if (a.want) {
-            double w[8] = {v[0], v[0], v[2], v[3], v[4], v[6], v[7], v[10]};
-            const int idx[8] = {A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
-            block_acc<8>(w, a.acc, idx, !MIXED);
-        }
-    }
-    __syncthreads();
-    // each atom sums its slots in the precomputed order (slots of term types
-    // that are off for this MTS group are skipped by their type ranges)
-    int lo[6], hi[6];
-#pragma unroll
-    for (int ty = 0; ty < 6; ++ty) {
-        const int k = ty == 0 ? 2 : ty == 1 ? 3 : ty <= 3 ? 4 : 2;
-        lo[ty] = (a.mask >> ty) & 1 ? cs[ty * a.nchunk + c] : 0;
-        hi[ty] = (a.mask >> ty) & 1 ? lo[ty] + k * (a.chunk_term[ty * stride + c + 1] - a.chunk_term[ty * stride + c]) : 0;
-    }
-    for (int l = threadIdx.x; l < na; l += blockDim.x) {
-        double fx = 0, fy = 0, fz = 0;
-        for (int k = s_start[l]; k < s_start[l + 1]; ++k) {
-            const int sl = s_inc[k];
-            bool on = false;
-#pragma unroll
-            for (int ty = 0; ty < 6; ++ty) on |= (sl >= lo[ty] && sl < hi[ty]);
-            if (!on) continue;
-            fx += (double)sx[sl]; fy += (double)sy[sl]; fz += (double)sz[sl];
-        }
-        if (fx != 0.0 || fy != 0.0 || fz != 0.0) force_add<MIXED>(a.facc, a0 + l, fx, fy, fz);
-    }
+    if (fx != 0.0 || fy != 0.0 || fz != 0.0) force_add<MIXED>(facc, i, fx, fy, fz);
 }
 
 // ---- host side -------------------------------------------------------------------
@@ -578,98 +432,37 @@ static pgk_status up(pgk_ctx* c, T** dst, const std::vector<T>& v) {
     return PGK_OK;
 }
 
-// Chunks of whole molecules (contiguous atom ranges, <= INTRA_ATOMS atoms and
-// <= INTRA_SLOTS term-atom slots), terms ordered by chunk, plus the per-atom
-// slot incidence lists; falls back to the per-type kernels when a molecule is
-// not contiguous, is too large for a chunk, or a term spans two molecules.
-pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>& mol_idx, const std::vector<int>& mol_list) {
-    int n = c->natom;
-    bool ok = !mol_idx.empty();
+// Term arrays ordered by their lowest atom (locality of the position gathers
+// and slot writes), the global slot layout and each atom's slot incidence
+// list (by type, then term), and the slot array itself.
+pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const std::vector<int>&) {
+    const int n = c->natom;
     const int K[6] = {2, 3, 4, 4, 2, 2};
-    // slots contributed by each molecule (terms are assigned to the molecule of their first atom)
-    std::vector<int> mol_of(n, -1);
-    int nmol = ok ? (int)mol_idx.size() - 1 : 0;
-    for (int m = 0; m < nmol && ok; ++m) {
-        int b = mol_idx[m], e = mol_idx[m + 1];
-        for (int q = b; q < e; ++q) {
-            if (mol_list[q] != mol_list[b] + (q - b)) ok = false;
-            else mol_of[mol_list[q]] = m;
-        }
-        if (m > 0 && mol_list[b] != mol_list[mol_idx[m - 1]] + (mol_idx[m] - mol_idx[m - 1])) ok = false;
-        if (e - b > INTRA_ATOMS) ok = false;
-    }
-    if (ok && (nmol == 0 || mol_list[mol_idx[0]] != 0 || mol_idx[nmol] != n)) ok = false;
-    std::vector<long long> mslots(nmol, 0);
-    auto add_slots = [&](int first, int k) { if (ok) { int m = mol_of[first]; if (m < 0) ok = false; else mslots[m] += k; } };
-    for (auto& x : t.bij) add_slots(x.x, 2);
-    for (auto& x : t.aijk) add_slots(x.x, 3);
-    for (auto& x : t.tij) add_slots(x.x, 4);
-    for (auto& x : t.rij) add_slots(x.x, 4);
-    for (auto& x : t.p14) add_slots(x.x, 2);
-    for (auto& x : t.ex) add_slots(x.x, 2);
-    std::vector<int> atom_chunk(n, -1), chunk_atom(1, 0);
-    if (ok) {
-        int natoms = 0; long long nslots = 0;
-        for (int m = 0; m < nmol && ok; ++m) {
-            int na = mol_idx[m + 1] - mol_idx[m];
-            if (mslots[m] > INTRA_SLOTS) { ok = false; break; }
-            if (natoms + na > INTRA_ATOMS || nslots + mslots[m] > INTRA_SLOTS) {
-                chunk_atom.push_back(chunk_atom.back() + natoms);
-                natoms = 0; nslots = 0;
-            }
-            natoms += na; nslots += mslots[m];
-        }
-        if (ok) {
-            chunk_atom.push_back(n);
-            int nch = (int)chunk_atom.size() - 1;
-            for (int k = 0; k < nch; ++k)
-                for (int a2 = chunk_atom[k]; a2 < chunk_atom[k + 1]; ++a2) atom_chunk[a2] = k;
-        }
-    }
-    int nch = ok ? (int)chunk_atom.size() - 1 : 0;
-    std::vector<int> ranges;
-    auto sort_type = [&](int count, auto atoms_of, auto apply) {
-        std::vector<int> order(count), ch(count);
-        for (int k = 0; k < count && ok; ++k) {
-            int cc = -1;
-            for (int at : atoms_of(k)) {
-                int x = atom_chunk[at];
-                if (cc < 0) cc = x;
-                else if (x != cc) ok = false;
-            }
-            ch[k] = cc;
-        }
-        if (!ok) return;
+    auto sort_type = [&](int count, auto first_atom, auto apply) {
+        std::vector<int> order(count);
         for (int k = 0; k < count; ++k) order[k] = k;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return ch[x] < ch[y]; });
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return first_atom(x) < first_atom(y); });
         apply(order);
-        std::vector<int> r(nch + 1, 0);
-        for (int k = 0; k < count; ++k) r[ch[k] + 1]++;
-        for (int k = 0; k < nch; ++k) r[k + 1] += r[k];
-        ranges.insert(ranges.end(), r.begin(), r.end());
     };
-    if (ok) {
-        sort_type((int)t.bij.size(), [&](int k) { return std::vector<int>{t.bij[k].x, t.bij[k].y}; },
-                  [&](const std::vector<int>& o) { reorder(t.bij, o); reorder(t.bp, o); });
-        sort_type((int)t.aijk.size(), [&](int k) { return std::vector<int>{t.aijk[k].x, t.aijk[k].y, t.aijk[k].z}; },
-                  [&](const std::vector<int>& o) { reorder(t.aijk, o); reorder(t.ap, o); });
-        sort_type((int)t.tij.size(),
-                  [&](int k) { return std::vector<int>{t.tij[k].x, t.tij[k].y, t.tij[k].z, t.tij[k].w}; },
-                  [&](const std::vector<int>& o) { reorder(t.tij, o); reorder(t.tp, o); });
-        sort_type((int)t.rij.size(),
-                  [&](int k) { return std::vector<int>{t.rij[k].x, t.rij[k].y, t.rij[k].z, t.rij[k].w}; },
-                  [&](const std::vector<int>& o) {
-                      std::vector<double> rc2(t.rc.size());
-                      for (size_t k = 0; k < o.size(); ++k)
-                          for (int q = 0; q < 6; ++q) rc2[6 * k + q] = t.rc[6 * o[k] + q];
-                      reorder(t.rij, o);
-                      t.rc.swap(rc2);
-                  });
-        sort_type((int)t.p14.size(), [&](int k) { return std::vector<int>{t.p14[k].x, t.p14[k].y}; },
-                  [&](const std::vector<int>& o) { reorder(t.p14, o); reorder(t.f14, o); });
-        sort_type((int)t.ex.size(), [&](int k) { return std::vector<int>{t.ex[k].x, t.ex[k].y}; },
-                  [&](const std::vector<int>& o) { reorder(t.ex, o); });
-    }
+    auto mn = [](std::initializer_list<int> v) { return std::min(v); };
+    sort_type((int)t.bij.size(), [&](int k) { return mn({t.bij[k].x, t.bij[k].y}); },
+              [&](const std::vector<int>& o) { reorder(t.bij, o); reorder(t.bp, o); });
+    sort_type((int)t.aijk.size(), [&](int k) { return mn({t.aijk[k].x, t.aijk[k].y, t.aijk[k].z}); },
+              [&](const std::vector<int>& o) { reorder(t.aijk, o); reorder(t.ap, o); });
+    sort_type((int)t.tij.size(), [&](int k) { return mn({t.tij[k].x, t.tij[k].y, t.tij[k].z, t.tij[k].w}); },
+              [&](const std::vector<int>& o) { reorder(t.tij, o); reorder(t.tp, o); });
+    sort_type((int)t.rij.size(), [&](int k) { return mn({t.rij[k].x, t.rij[k].y, t.rij[k].z, t.rij[k].w}); },
+              [&](const std::vector<int>& o) {
+                  std::vector<double> rc2(t.rc.size());
+                  for (size_t k = 0; k < o.size(); ++k)
+                      for (int q = 0; q < 6; ++q) rc2[6 * k + q] = t.rc[6 * o[k] + q];
+                  reorder(t.rij, o);
+                  t.rc.swap(rc2);
+              });
+    sort_type((int)t.p14.size(), [&](int k) { return mn({t.p14[k].x, t.p14[k].y}); },
+              [&](const std::vector<int>& o) { reorder(t.p14, o); reorder(t.f14, o); });
+    sort_type((int)t.ex.size(), [&](int k) { return mn({t.ex[k].x, t.ex[k].y}); },
+              [&](const std::vector<int>& o) { reorder(t.ex, o); });
     pgk_status s;
     c->nbond = (int)t.bij.size(); c->nangl = (int)t.aijk.size(); c->ntors = (int)t.tij.size();
     c->ntorsrb = (int)t.rij.size(); c->n14 = (int)t.p14.size(); c->nexpair = (int)t.ex.size();
@@ -678,88 +471,41 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>& mol_id
         (s = up(c, &c->rb_ijkl, t.rij)) || (s = up(c, &c->rb_c, t.rc)) || (s = up(c, &c->p14_ij, t.p14)) ||
         (s = up(c, &c->p14_f, t.f14)) || (s = up(c, &c->expair, t.ex)))
         return s;
-    c->intra_ok = ok && nch > 0;
-    if (!c->intra_ok) return PGK_OK;
-    c->nchunk = nch;
-    // slot bases per type per chunk, and the incidence lists
-    std::vector<int> slot_base(6 * (size_t)nch, 0);
-    std::vector<std::vector<unsigned short>> inc(n);
-    auto atom_list = [&](int ty, int k) -> std::vector<int> {
+    const long long cnt[6] = {c->nbond, c->nangl, c->ntors, c->ntorsrb, c->n14, c->nexpair};
+    c->slot_base[0] = 0;
+    for (int ty = 0; ty < 6; ++ty) c->slot_base[ty + 1] = c->slot_base[ty] + K[ty] * cnt[ty];
+    const long long S = c->slot_base[6];
+    if (S >= (1LL << 31)) return pgk_fail(c, PGK_E_UNSUPPORTED, "more than 2^31 bonded term slots");
+    std::vector<int> deg(n + 1, 0);
+    auto atoms_of = [&](int ty, long long k, int* at) {
         switch (ty) {
-            case 0: return {t.bij[k].x, t.bij[k].y};
-            case 1: return {t.aijk[k].x, t.aijk[k].y, t.aijk[k].z};
-            case 2: return {t.tij[k].x, t.tij[k].y, t.tij[k].z, t.tij[k].w};
-            case 3: return {t.rij[k].x, t.rij[k].y, t.rij[k].z, t.rij[k].w};
-            case 4: return {t.p14[k].x, t.p14[k].y};
-            default: return {t.ex[k].x, t.ex[k].y};
+            case 0: at[0] = t.bij[k].x; at[1] = t.bij[k].y; break;
+            case 1: at[0] = t.aijk[k].x; at[1] = t.aijk[k].y; at[2] = t.aijk[k].z; break;
+            case 2: at[0] = t.tij[k].x; at[1] = t.tij[k].y; at[2] = t.tij[k].z; at[3] = t.tij[k].w; break;
+            case 3: at[0] = t.rij[k].x; at[1] = t.rij[k].y; at[2] = t.rij[k].z; at[3] = t.rij[k].w; break;
+            case 4: at[0] = t.p14[k].x; at[1] = t.p14[k].y; break;
+            default: at[0] = t.ex[k].x; at[1] = t.ex[k].y; break;
         }
     };
-    for (int ch = 0; ch < nch; ++ch) {
-        int base = 0;
-        for (int ty = 0; ty < 6; ++ty) {
-            slot_base[(size_t)ty * nch + ch] = base;
-            int t0 = ranges[(size_t)ty * (nch + 1) + ch], t1 = ranges[(size_t)ty * (nch + 1) + ch + 1];
-            for (int k = t0; k < t1; ++k) {
-                std::vector<int> at = atom_list(ty, k);
-                for (int q = 0; q < K[ty]; ++q) inc[at[q]].push_back((unsigned short)(base + K[ty] * (k - t0) + q));
-            }
-            base += K[ty] * (t1 - t0);
+    int at[4];
+    for (int ty = 0; ty < 6; ++ty)
+        for (long long k = 0; k < cnt[ty]; ++k) {
+            atoms_of(ty, k, at);
+            for (int q = 0; q < K[ty]; ++q) deg[at[q] + 1]++;
         }
-        if (base > INTRA_SLOTS) { c->intra_ok = false; return PGK_OK; }
+    for (int i = 0; i < n; ++i) deg[i + 1] += deg[i];
+    std::vector<int> inc((size_t)std::max<long long>(S, 1)), fill(deg.begin(), deg.end() - 1);
+    for (int ty = 0; ty < 6; ++ty)
+        for (long long k = 0; k < cnt[ty]; ++k) {
+            atoms_of(ty, k, at);
+            for (int q = 0; q < K[ty]; ++q) inc[fill[at[q]]++] = (int)(c->slot_base[ty] + K[ty] * k + q);
+        }
+    if ((s = up(c, &c->inc_start, deg)) || (s = up(c, &c->inc_slot, inc))) return s;
+    if (S > 0) {
+        const size_t bytes = (size_t)3 * S * (c->mixed() ? sizeof(float) : sizeof(double));
+        PGK_CUDA(c, cudaMalloc(&c->slot_f, bytes));
+        PGK_CUDA(c, cudaMemset(c->slot_f, 0, bytes));
     }
-    std::vector<int> inc_start(n + 1, 0);
-    std::vector<unsigned short> inc_slot;
-    for (int i = 0; i < n; ++i) {
-        inc_start[i] = (int)inc_slot.size();
-        inc_slot.insert(inc_slot.end(), inc[i].begin(), inc[i].end());
-    }
-    inc_start[n] = (int)inc_slot.size();
-    if (inc_slot.empty()) inc_slot.push_back(0);
-    if ((s = up(c, &c->chunk_atom, chunk_atom)) || (s = up(c, &c->chunk_term, ranges)) ||
-        (s = up(c, &c->chunk_slot, slot_base)) || (s = up(c, &c->inc_start, inc_start)) ||
-        (s = up(c, &c->inc_slot, inc_slot)))
-        return s;
-    return PGK_OK;
-}
-
-template <bool MIXED>
-static void bonded_impl(pgk_ctx* c, int group, bool want, bool all) {
-    void* f = c->facc[group];
-    long long* acc = c->acc + (size_t)group * NACC;
-    int w = want ? 1 : 0;
-    const int tb = 128;
-    auto on = [&](int mts) { return all || mts == (group == 0 ? PGK_MTS_LONG : PGK_MTS_SHORT); };
-    if (c->nbond && on(c->prm.mts_bond)) {
-        k_bond<MIXED><<<(c->nbond + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->bond_ij, c->bond_p, c->nbond, c->dyn,
-                                                                   f, acc, w);
-        PGK_LAUNCHED(c);
-    }
-    if (c->nangl && on(c->prm.mts_angl)) {
-        k_angl<MIXED><<<(c->nangl + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->angl_ijk, c->angl_p, c->nangl, c->dyn,
-                                                                   f, acc, w);
-        PGK_LAUNCHED(c);
-    }
-    if (c->ntors && on(c->prm.mts_tors)) {
-        k_tors<MIXED, false><<<(c->ntors + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->tors_ijkl, c->tors_p, nullptr,
-                                                                          c->ntors, c->dyn, f, acc, w, c->status);
-        PGK_LAUNCHED(c);
-    }
-    if (c->ntorsrb && on(c->prm.mts_torsrb)) {
-        k_tors<MIXED, true><<<(c->ntorsrb + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->rb_ijkl, nullptr, c->rb_c,
-                                                                           c->ntorsrb, c->dyn, f, acc, w, c->status);
-        PGK_LAUNCHED(c);
-    }
-    if (c->n14 && (all || (on(c->prm.mts_vdw14) && c->prm.mts_vdw14 == c->prm.mts_elc14))) {
-        k_non14<MIXED><<<(c->n14 + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij, c->p14_f, c->n14,
-                                                                  c->ntyp, c->lj64, c->dyn, f, acc, w);
-        PGK_LAUNCHED(c);
-    }
-}
-
-pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_all) {
-    if (c->mixed()) bonded_impl<true>(c, group, ene || vir, force_all);
-    else bonded_impl<false>(c, group, ene || vir, force_all);
-    PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
 
@@ -863,83 +609,77 @@ pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h) {
     return PGK_OK;
 }
 
-pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir) {
-    if (c->nexpair == 0) return PGK_OK;
-    int nb = (c->nexpair + 255) / 256;
+// One MTS group's bonded terms (mask bits: 0 bond, 1 angle, 2 periodic
+// torsion, 3 RB torsion, 4 1-4 pairs, 5 excluded-pair Ewald correction): one
+// kernel per active type writing the slots, then the per-atom gather.
+template <bool MIXED>
+static void terms_impl(pgk_ctx* c, int group, int mask, bool want) {
     long long* acc = c->acc + (size_t)group * NACC;
-    if (c->mixed())
-        k_excl<true><<<nb, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64, c->spl32, c->nspl,
-                                            c->hspl, c->dyn, c->facc[group], acc, ene || vir);
-    else
-        k_excl<false><<<nb, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64, c->spl32, c->nspl,
-                                             c->hspl, c->dyn, c->facc[group], acc, ene || vir);
-    PGK_LAUNCHED(c);
+    const int w = want ? 1 : 0;
+    const int tb = 128;
+    const long long S = c->slot_base[6];
+    auto out = [&](int ty) { return TermOut{c->facc[group], c->slot_f, S, c->slot_base[ty]}; };
+    if ((mask & 1) && c->nbond) {
+        k_bond<MIXED><<<(c->nbond + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->bond_ij, c->bond_p, c->nbond, c->dyn,
+                                                                   out(0), acc, w);
+        PGK_LAUNCHED(c);
+    }
+    if ((mask & 2) && c->nangl) {
+        k_angl<MIXED><<<(c->nangl + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->angl_ijk, c->angl_p, c->nangl, c->dyn,
+                                                                   out(1), acc, w);
+        PGK_LAUNCHED(c);
+    }
+    if ((mask & 4) && c->ntors) {
+        k_tors<MIXED, false><<<(c->ntors + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->tors_ijkl, c->tors_p, nullptr,
+                                                                          c->ntors, c->dyn, out(2), acc, w, c->status);
+        PGK_LAUNCHED(c);
+    }
+    if ((mask & 8) && c->ntorsrb) {
+        k_tors<MIXED, true><<<(c->ntorsrb + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->rb_ijkl, nullptr, c->rb_c,
+                                                                           c->ntorsrb, c->dyn, out(3), acc, w,
+                                                                           c->status);
+        PGK_LAUNCHED(c);
+    }
+    if ((mask & 16) && c->n14) {
+        k_non14<MIXED><<<(c->n14 + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij, c->p14_f, c->n14,
+                                                                  c->ntyp, c->lj64, c->dyn, out(4), acc, w);
+        PGK_LAUNCHED(c);
+    }
+    if ((mask & 32) && c->nexpair) {
+        k_excl<MIXED><<<(c->nexpair + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64,
+                                                                    c->spl32, c->nspl, c->hspl, c->dyn, out(5), acc,
+                                                                    w);
+        PGK_LAUNCHED(c);
+    }
+    if (S > 0) {
+        SlotTypes ty;
+        for (int q = 0; q < 7; ++q) ty.base[q] = c->slot_base[q];
+        k_slot_gather<MIXED><<<(c->natom + 255) / 256, 256, 0, c->st>>>(c->inc_start, c->inc_slot, c->slot_f, ty,
+                                                                         mask, c->natom, c->facc[group]);
+        PGK_LAUNCHED(c);
+    }
+}
+
+pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want) {
+    const long long cnt[6] = {c->nbond, c->nangl, c->ntors, c->ntorsrb, c->n14, c->nexpair};
+    int active = 0;
+    for (int ty = 0; ty < 6; ++ty) if (((mask >> ty) & 1) && cnt[ty] > 0) active |= 1 << ty;
+    if (!active) return PGK_OK;
+    if (c->mixed()) terms_impl<true>(c, group, active, want);
+    else terms_impl<false>(c, group, active, want);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
 
-// mask bits: 0 bond, 1 angle, 2 periodic torsion, 3 RB torsion, 4 1-4, 5 excluded pairs
-pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want) {
-    if (!mask) return PGK_OK;
-    if (!c->intra_ok) {   // general path: one kernel per term type
-        pgk_status s = PGK_OK;
-        if (mask & 31) {
-            int g = group;
-            void* f = c->facc[g];
-            long long* acc = c->acc + (size_t)g * NACC;
-            int w = want ? 1 : 0;
-            const int tb = 128;
-            if ((mask & 1) && c->nbond) {
-                if (c->mixed()) k_bond<true><<<(c->nbond + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->bond_ij, c->bond_p, c->nbond, c->dyn, f, acc, w);
-                else k_bond<false><<<(c->nbond + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->bond_ij, c->bond_p, c->nbond, c->dyn, f, acc, w);
-                PGK_LAUNCHED(c);
-            }
-            if ((mask & 2) && c->nangl) {
-                if (c->mixed()) k_angl<true><<<(c->nangl + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->angl_ijk, c->angl_p, c->nangl, c->dyn, f, acc, w);
-                else k_angl<false><<<(c->nangl + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->angl_ijk, c->angl_p, c->nangl, c->dyn, f, acc, w);
-                PGK_LAUNCHED(c);
-            }
-            if ((mask & 4) && c->ntors) {
-                if (c->mixed()) k_tors<true, false><<<(c->ntors + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->tors_ijkl, c->tors_p, nullptr, c->ntors, c->dyn, f, acc, w, c->status);
-                else k_tors<false, false><<<(c->ntors + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->tors_ijkl, c->tors_p, nullptr, c->ntors, c->dyn, f, acc, w, c->status);
-                PGK_LAUNCHED(c);
-            }
-            if ((mask & 8) && c->ntorsrb) {
-                if (c->mixed()) k_tors<true, true><<<(c->ntorsrb + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->rb_ijkl, nullptr, c->rb_c, c->ntorsrb, c->dyn, f, acc, w, c->status);
-                else k_tors<false, true><<<(c->ntorsrb + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->rb_ijkl, nullptr, c->rb_c, c->ntorsrb, c->dyn, f, acc, w, c->status);
-                PGK_LAUNCHED(c);
-            }
-            if ((mask & 16) && c->n14) {
-                if (c->mixed()) k_non14<true><<<(c->n14 + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij, c->p14_f, c->n14, c->ntyp, c->lj64, c->dyn, f, acc, w);
-                else k_non14<false><<<(c->n14 + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij, c->p14_f, c->n14, c->ntyp, c->lj64, c->dyn, f, acc, w);
-                PGK_LAUNCHED(c);
-            }
-        }
-        if (mask & 32) s = launch_excl(c, group, want, want);
-        if (s) return s;
-        PGK_CUDA(c, cudaGetLastError());
-        return PGK_OK;
-    }
-    IntraArgs a;
-    a.chunk_atom = c->chunk_atom; a.chunk_term = c->chunk_term; a.chunk_slot = c->chunk_slot;
-    a.inc_start = c->inc_start; a.inc_slot = c->inc_slot; a.nchunk = c->nchunk;
-    a.mask = mask; a.want = want ? 1 : 0;
-    a.bond_ij = c->bond_ij; a.bond_p = c->bond_p; a.angl_ijk = c->angl_ijk; a.angl_p = c->angl_p;
-    a.tors_ijkl = c->tors_ijkl; a.tors_p = c->tors_p; a.rb_ijkl = c->rb_ijkl; a.rb_c = c->rb_c;
-    a.p14_ij = c->p14_ij; a.p14_f = c->p14_f; a.expair = c->expair;
-    a.chrg = c->chrg; a.typ = c->typ; a.ntyp = c->ntyp; a.lj64 = c->lj64;
-    a.spl64 = c->spl64; a.spl32 = c->spl32; a.nspl = c->nspl; a.h = c->hspl;
-    a.facc = c->facc[group]; a.acc = c->acc + (size_t)group * NACC; a.status = c->status;
-    if (c->mixed()) {
-        size_t sm = (size_t)3 * INTRA_SLOTS * sizeof(float);
-        smem_limit(k_intra<true>, sm);
-        k_intra<true><<<c->nchunk, 128, sm, c->st>>>(c->pos, a, c->dyn);
-    } else {
-        size_t sm = (size_t)3 * INTRA_SLOTS * sizeof(double);
-        smem_limit(k_intra<false>, sm);
-        k_intra<false><<<c->nchunk, 128, sm, c->st>>>(c->pos, a, c->dyn);
-    }
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
+// all bonded terms (the MTS assignment ignored) or only those of the group
+pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_all) {
+    auto on = [&](int mts) { return force_all || mts == (group == 0 ? PGK_MTS_LONG : PGK_MTS_SHORT); };
+    const int mask = (on(c->prm.mts_bond) ? 1 : 0) | (on(c->prm.mts_angl) ? 2 : 0) | (on(c->prm.mts_tors) ? 4 : 0) |
+                     (on(c->prm.mts_torsrb) ? 8 : 0) |
+                     ((force_all || (on(c->prm.mts_vdw14) && c->prm.mts_vdw14 == c->prm.mts_elc14)) ? 16 : 0);
+    return launch_intra(c, group, mask, ene || vir);
+}
+
+pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir) {
+    return launch_intra(c, group, 32, ene || vir);
 }

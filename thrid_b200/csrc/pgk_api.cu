@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -400,19 +401,55 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     }
     // ---- constraints ----
     {
-        c->ncgroup = s->nconst;
         c->nconstraint = s->nconstraint;
+        c->ncgroup = 0;
         if (s->nconst > 0) {
-            std::vector<int> gi(s->nconst + 1), gl;
-            for (int g = 0; g <= s->nconst; ++g) gi[g] = s->index_mconst[g] - 1;
-            for (int k = 0; k < gi[s->nconst]; ++k) gl.push_back(s->list_mconst[k] - 1);
+            std::vector<int> gi0(s->nconst + 1), gl0;
+            for (int g = 0; g <= s->nconst; ++g) gi0[g] = s->index_mconst[g] - 1;
+            for (int k = 0; k < gi0[s->nconst]; ++k) gl0.push_back(s->list_mconst[k] - 1);
             std::vector<int2> cij; std::vector<double> cd;
             for (int k = 0; k < s->nconstraint; ++k) {
                 cij.push_back(make_int2(s->iconst[k] - 1, s->jconst[k] - 1));
                 cd.push_back(s->dconst[k]);
             }
-            std::vector<int2> span(s->nconst);
+            // Split every group into its connected components (constraints that
+            // share no atom, e.g. the X-H bonds of different carbons), keeping
+            // the reference order inside each.  The Gauss-Seidel sweeps of
+            // rattle_c / rattlep_v give the same result either way: a component
+            // only moves its own atoms, and once converged its constraints are
+            // skipped by every further sweep of the group.
+            std::vector<int> gi(1, 0), gl;
+            std::map<int, int> parent;
+            std::function<int(int)> find = [&](int a) {
+                int r = a;
+                while (parent[r] != r) r = parent[r];
+                while (parent[a] != r) { int nx = parent[a]; parent[a] = r; a = nx; }
+                return r;
+            };
             for (int g = 0; g < s->nconst; ++g) {
+                parent.clear();
+                for (int k = gi0[g]; k < gi0[g + 1]; ++k) {
+                    int2 p2 = cij[gl0[k]];
+                    if (!parent.count(p2.x)) parent[p2.x] = p2.x;
+                    if (!parent.count(p2.y)) parent[p2.y] = p2.y;
+                    int ra = find(p2.x), rb = find(p2.y);
+                    if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+                }
+                std::vector<int> roots;
+                std::map<int, std::vector<int>> comp;
+                for (int k = gi0[g]; k < gi0[g + 1]; ++k) {
+                    int r = find(cij[gl0[k]].x);
+                    if (!comp.count(r)) roots.push_back(r);
+                    comp[r].push_back(gl0[k]);
+                }
+                for (int r : roots) {
+                    gl.insert(gl.end(), comp[r].begin(), comp[r].end());
+                    gi.push_back((int)gl.size());
+                }
+            }
+            c->ncgroup = (int)gi.size() - 1;
+            std::vector<int2> span(c->ncgroup);
+            for (int g = 0; g < c->ncgroup; ++g) {
                 int lo = n, hi = -1;
                 for (int k = gi[g]; k < gi[g + 1]; ++k) {
                     int2 p2 = cij[gl[k]];
@@ -482,7 +519,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
                     c->ccnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
-                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->chunk_atom, c->chunk_term, c->cg_span, c->chunk_slot, c->inc_start, c->inc_slot,
+                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->slot_f, c->inc_start, c->inc_slot,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};
     for (void* b : bufs) if (b) cudaFree(b);

@@ -80,14 +80,11 @@ struct pgk_ctx {
     int ntorsrb = 0; int4* rb_ijkl = nullptr; double* rb_c = nullptr;       // [6*n]
     int n14 = 0; int2* p14_ij = nullptr; double2* p14_f = nullptr;          // (elc fac, vdw fac)
 
-    // ---- fused intramolecular kernel (chunks of whole molecules) ----
-    bool intra_ok = false;
-    int nchunk = 0;
-    int* chunk_atom = nullptr;    // [nchunk+1]
-    int* chunk_term = nullptr;    // [6][nchunk+1]
-    int* chunk_slot = nullptr;    // [6][nchunk] slot base of each term type inside its chunk
+    // ---- bonded force slots (one slot per term atom) and their gather ----
+    long long slot_base[7] = {0, 0, 0, 0, 0, 0, 0};   // per term type: bond, angle, tors, RB, 1-4, excl
+    void* slot_f = nullptr;       // [3][nslot] slot forces (float mixed / double FP64)
     int* inc_start = nullptr;     // [natom+1] slot incidence CSR
-    unsigned short* inc_slot = nullptr;
+    int* inc_slot = nullptr;      // global slot ids, per atom by type then term
 
     // ---- constraints ----
     int ncgroup = 0, nconstraint = 0;
