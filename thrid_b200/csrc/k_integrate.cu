@@ -107,7 +107,16 @@ __global__ void k_rattle_pos(double* __restrict__ pos, double* __restrict__ vel,
         for (int k = 0; k < 3 * na; ++k) { X[k] = pos[3 * lo + k]; V[k] = vel[3 * lo + k]; O[k] = old[3 * lo + k]; }
         for (int k = 0; k < na; ++k) IM[k] = invm[lo + k];
         finished = rattle_pos_sweeps(X, V, O, IM, lo, glist, cij, cd, i1, i2, eps, dt, rvi);
-        for (int k = 0; k < 3 * na; ++k) { pos[3 * lo + k] = X[k]; vel[3 * lo + k] = V[k]; }
+        // write back only this group's own atoms: the spans of groups split
+        // from one molecule interleave, and other threads own the rest
+        for (int ii = i1; ii < i2; ++ii) {
+            const int2 p2 = cij[glist[ii]];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pos[3 * p2.x + d] = X[3 * (p2.x - lo) + d]; vel[3 * p2.x + d] = V[3 * (p2.x - lo) + d];
+                pos[3 * p2.y + d] = X[3 * (p2.y - lo) + d]; vel[3 * p2.y + d] = V[3 * (p2.y - lo) + d];
+            }
+        }
     } else {
         finished = rattle_pos_sweeps(pos, vel, old, invm, 0, glist, cij, cd, i1, i2, eps, dt, rvi);
     }
@@ -165,7 +174,14 @@ __global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict_
         for (int k = 0; k < 3 * na; ++k) { X[k] = pos[3 * lo + k]; V[k] = vel[3 * lo + k]; }
         for (int k = 0; k < na; ++k) IM[k] = invm[lo + k];
         finished = rattle_vel_sweeps(X, V, IM, lo, glist, cij, cd, i1, i2, eps);
-        for (int k = 0; k < 3 * na; ++k) vel[3 * lo + k] = V[k];
+        for (int ii = i1; ii < i2; ++ii) {
+            const int2 p2 = cij[glist[ii]];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                vel[3 * p2.x + d] = V[3 * (p2.x - lo) + d];
+                vel[3 * p2.y + d] = V[3 * (p2.y - lo) + d];
+            }
+        }
     } else {
         finished = rattle_vel_sweeps(pos, vel, invm, 0, glist, cij, cd, i1, i2, eps);
     }
