@@ -96,6 +96,52 @@ __global__ void k_spread(const double* __restrict__ pos, const double* __restric
     }
 }
 
+// Row-cooperative spread (the path the engine runs): P lanes per atom, lane
+// i1 adds the points (i1, i2, i3) of all (i2, i3), so each atomic instruction
+// of a warp covers 32/P atoms x P consecutive grid points -- a few L2 sectors
+// per instruction instead of one sector per lane.  Each contribution is the
+// same product th0 * (th1 * (th2 * q)) as in k_spread, so the mixed grid
+// (integer sums) is bit-identical to k_spread's.
+template <bool MIXED, int P>
+__global__ void __launch_bounds__(256) k_spread_rows(const double* __restrict__ pos, const double* __restrict__ chrg,
+                                                     int n, const DynState* __restrict__ dyn, int K1, int K2, int K3,
+                                                     void* __restrict__ qacc, const int* __restrict__ order) {
+    constexpr int G = 32 / P;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / P, i1 = lane - g * P;
+    const int t = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G + g;
+    if (g >= G || t >= n) return;
+    const int a = order ? order[t] : t;
+    if (a < 0) return;   // padding slot of the cell-sorted order
+    double th[3][P], dth[3][P];
+    int base[3];
+    const int Kd[3] = {K1, K2, K3};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w;
+        frac_coord(pos[3 * a + d], dyn->boxinv[d], Kd[d], base[d], w);
+        fill_bspline_d<double, P>(w, th[d], dth[d]);
+    }
+    double t0 = 0.0;
+#pragma unroll
+    for (int q = 0; q < P; ++q) t0 = q == i1 ? th[0][q] : t0;
+    const double q = chrg[a];
+    int i = base[0] - P + 1 + i1; i = i < 0 ? i + K1 : i;
+#pragma unroll
+    for (int i3 = 0; i3 < P; ++i3) {
+        int k = base[2] - P + 1 + i3; k = k < 0 ? k + K3 : k;
+        const double p1 = th[2][i3] * q;
+#pragma unroll
+        for (int i2 = 0; i2 < P; ++i2) {
+            int j = base[1] - P + 1 + i2; j = j < 0 ? j + K2 : j;
+            const double v = t0 * (th[1][i2] * p1);
+            const size_t at = (size_t)K1 * (j + (size_t)K2 * k) + i;
+            if (MIXED) atomicAdd((unsigned long long*)qacc + at, (unsigned long long)__double2ll_rn(v * PGK_GRID_SCALE));
+            else atomicAdd((double*)qacc + at, v);
+        }
+    }
+}
+
 // ---- FFT --------------------------------------------------------------------
 template <typename T> struct C2;
 template <> struct C2<float> { typedef float2 t; };
@@ -482,6 +528,68 @@ __global__ void k_gather(const double* __restrict__ pos, const double* __restric
                      dyn->boxinv[2] * (double)f2);
 }
 
+// Row-cooperative gather: P lanes per atom, lane i1 sums the points with
+// first index i1; the P partial forces are then added in lane order by the
+// group's first lane (fixed order: deterministic).
+template <bool MIXED, int P>
+__global__ void __launch_bounds__(256) k_gather_rows(const double* __restrict__ pos, const double* __restrict__ chrg,
+                                                     int n, const DynState* __restrict__ dyn, int K1, int K2, int K3,
+                                                     const void* __restrict__ qc, void* facc,
+                                                     const int* __restrict__ order) {
+    typedef typename std::conditional<MIXED, float, double>::type T;
+    typedef typename C2<T>::t T2;
+    constexpr int G = 32 / P;
+    const int lane = threadIdx.x & 31;
+    const int g = lane / P, i1 = lane - g * P;
+    const int t = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G + g;
+    const int a = (g < G && t < n) ? (order ? order[t] : t) : -1;
+    T f0 = 0, f1 = 0, f2 = 0;
+    if (a >= 0) {
+        T th[3][P], dth[3][P];
+        int base[3];
+        const int Kd[3] = {K1, K2, K3};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double w;
+            frac_coord(pos[3 * a + d], dyn->boxinv[d], Kd[d], base[d], w);
+            fill_bspline_d<T, P>((T)w, th[d], dth[d]);
+        }
+        T t0 = 0, d0 = 0;
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            t0 = q == i1 ? th[0][q] : t0;
+            d0 = q == i1 ? dth[0][q] : d0;
+        }
+        const T2* Q = (const T2*)qc;
+        const T q = (T)chrg[a];
+        int i = base[0] - P + 1 + i1; i = i < 0 ? i + K1 : i;
+#pragma unroll
+        for (int i3 = 0; i3 < P; ++i3) {
+            int k = base[2] - P + 1 + i3; k = k < 0 ? k + K3 : k;
+#pragma unroll
+            for (int i2 = 0; i2 < P; ++i2) {
+                int j = base[1] - P + 1 + i2; j = j < 0 ? j + K2 : j;
+                const T term = q * Q[(size_t)K1 * (j + (size_t)K2 * k) + i].x;
+                f0 = f0 - (T)K1 * term * d0 * th[1][i2] * th[2][i3];
+                f1 = f1 - (T)K2 * term * t0 * dth[1][i2] * th[2][i3];
+                f2 = f2 - (T)K3 * term * t0 * th[1][i2] * dth[2][i3];
+            }
+        }
+    }
+    // lane g*P collects its group's partials in lane order
+    T s0 = f0, s1 = f1, s2 = f2;
+#pragma unroll
+    for (int q = 1; q < P; ++q) {
+        const int src = (lane - i1 + q) & 31;
+        const T o0 = __shfl_sync(0xffffffffu, f0, src), o1 = __shfl_sync(0xffffffffu, f1, src),
+                o2 = __shfl_sync(0xffffffffu, f2, src);
+        s0 += o0; s1 += o1; s2 += o2;
+    }
+    if (a >= 0 && i1 == 0)
+        force_add<MIXED>(facc, a, dyn->boxinv[0] * (double)s0, dyn->boxinv[1] * (double)s1,
+                         dyn->boxinv[2] * (double)s2);
+}
+
 // ---- host side ------------------------------------------------------------------
 static void fill_bspline_h(double w, int order, double* arr, double* darr) {
     arr[order - 1] = 0.0; arr[1] = w; arr[0] = 1.0 - w;
@@ -639,13 +747,14 @@ static pgk_status fft_convolve(pgk_ctx* c, long long* acc, int want) {
 template <bool MIXED, int P>
 static void spread_gather(pgk_ctx* c, bool gather, int group) {
     const int* order = c->list_valid ? c->perm : nullptr;
-    int n = order ? c->npad : c->natom;     // sorted order runs over the padded slots
+    const int n = order ? c->npad : c->natom;     // sorted order runs over the padded slots
+    const int warps = (n + 32 / P - 1) / (32 / P);
     if (!gather)
-        k_spread<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
-                                                               c->K[2], c->qacc, order);
+        k_spread_rows<MIXED, P><<<(warps + 7) / 8, 256, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
+                                                                    c->K[2], c->qacc, order);
     else
-        k_gather<MIXED, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
-                                                               c->K[2], c->qc, c->facc[group], order);
+        k_gather_rows<MIXED, P><<<(warps + 7) / 8, 256, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
+                                                                    c->K[2], c->qc, c->facc[group], order);
     PGK_LAUNCHED(c);
 }
 
