@@ -367,10 +367,12 @@ void* pgk_stream(const pgk_ctx* ctx);
  * events, and return the mean device time per launch in *ms.  which:
  *   0 = real-space pair kernel (ewaldrp) with virials, 1 = SPME spread,
  *   2 = SPME gather, 3 = one forward 3-D FFT (three axis passes),
- *   64 + m = the fused intramolecular kernel with term mask m (bit 0 bonds,
- *   1 angles, 2 torsions, 3 RB torsions, 4 1-4 pairs, 5 excluded pairs).
+ *   64 + m = the bonded terms with term mask m (bit 0 bonds, 1 angles,
+ *   2 torsions, 3 RB torsions, 4 1-4 pairs, 5 excluded pairs) with energies
+ *   and per-type virials, 128 + m = the same with only the total virial
+ *   tensor (the anisotropic MTK step without output).
  * *units receives the algorithmic work of one launch: unique pairs inside
- * the cutoff (0), atoms (1, 2, 64+), or grid points (3); *entries the number
+ * the cutoff (0), atoms (1, 2, 64+, 128+), or grid points (3); *entries the number
  * of (cluster, j) list entries the pair kernel reads. */
 pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
                             double* entries);

@@ -6,13 +6,17 @@
 //   calnon14p  calnon14.F90:249-521     scaled 1-4 Coulomb + LJ
 //   ewaldrp excluded-pair erf correction (ewaldr.F90:756-826)
 //
-// Layout: every term type writes the force on each of its atoms into its own
-// slot of one global slot array (slot = base[type] + K*term + q, SoA x|y|z),
-// one thread per term and one kernel per type, with no atomics; then
-// k_slot_gather sums each atom's slots in a fixed order (a precomputed
-// incidence list) and adds the total to the group's force accumulator once.
-// The result is deterministic in both precisions and needs no assumption on
-// molecule layout.  Energies and virials are block-reduced per type.
+// Layout: bonded_setup cuts the atoms into blocks of consecutive atoms; block
+// b owns the terms whose lowest atom lies in its range (terms sorted by lowest
+// atom), stages the positions of its local atoms (owned range plus the
+// higher atoms its terms reach) in shared memory, evaluates its terms with
+// one thread per term, writes each term atom's force into a shared-memory
+// slot, and then sums every local atom's slots in a fixed order (a
+// precomputed per-block incidence list) and adds the total to the group's
+// force accumulator once per block.  No atomics inside the block; the
+// per-atom sums are deterministic.  Terms spanning BLK_FAR_SPAN atoms or more
+// (rare: e.g. a disulfide bond) run in the per-type kernels with force
+// atomics.  Energies and virials are block-reduced per type.
 //
 // Displacements are formed in FP64 from the master positions (Fortran anint
 // minimum image); the remaining arithmetic runs in T (float for mixed).
@@ -23,6 +27,14 @@
 
 #include "pgk_ctx.cuh"
 #include "pgk_hf.cuh"
+
+// block plan limits: local atoms per block, the atom span from which a term
+// is "far", threads per block, slots per block (shared-memory slot planes)
+#define BLK_LOC_MAX 512
+#define BLK_FAR_SPAN 256
+#define BLK_THREADS 256
+#define BLK_SLOT_CAP_MAX 4096
+static inline int blk_slot_cap(bool mixed) { return mixed ? BLK_SLOT_CAP_MAX : 2048; }
 
 
 template <typename T>
@@ -61,26 +73,10 @@ __device__ __forceinline__ void vir_abs(double* v, const double* f, const double
         for (int a = 0; a < 3; ++a) v[1 + a + 3 * b] += f[a] * x[b];
 }
 
-// where a term kernel puts its forces: the slot array (slot = base + K*term + q)
-// or, when slot is null, the force accumulator (atomics)
-struct TermOut {
-    void* facc;
-    void* slot;          // [3][S] of T
-    long long S, base;
-};
+// the per-type kernels (far terms) add their forces with atomics
 template <bool MIXED>
-__device__ __forceinline__ void put_force(const TermOut& o, int term, int K, int q, int atom, const double* F,
-                                          double sgn) {
-    typedef typename std::conditional<MIXED, float, double>::type T;
-    if (o.slot) {
-        T* sl = (T*)o.slot;
-        const size_t k = (size_t)o.base + (size_t)K * term + q;
-        sl[k] = (T)(sgn * F[0]);
-        sl[o.S + k] = (T)(sgn * F[1]);
-        sl[2 * o.S + k] = (T)(sgn * F[2]);
-    } else {
-        force_add<MIXED>(o.facc, atom, sgn * F[0], sgn * F[1], sgn * F[2]);
-    }
+__device__ __forceinline__ void put_force(void* facc, int atom, const double* F, double sgn) {
+    force_add<MIXED>(facc, atom, sgn * F[0], sgn * F[1], sgn * F[2]);
 }
 
 // ---- term evaluators (P = positions, indices into P) ------------------------
@@ -271,7 +267,7 @@ __device__ __forceinline__ void eval_excl(const double* P, int i, int j, double 
 // ---- per-term-type kernels (general path) -------------------------------------
 template <bool MIXED>
 __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ ij, const double2* __restrict__ par,
-                       int nterm, const DynState* __restrict__ dyn, TermOut out, long long* acc, int want) {
+                       int nterm, const DynState* __restrict__ dyn, void* facc, long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
@@ -279,8 +275,8 @@ __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ 
         double F[3] = {0, 0, 0}, rd[3], e;
         int i = ij[k].x, j = ij[k].y;
         const bool on = eval_bond<T>(pos, i, j, par[k], dyn, F, rd, e);
-        put_force<MIXED>(out, k, 2, 0, i, F, 1.0);
-        put_force<MIXED>(out, k, 2, 1, j, F, -1.0);
+        put_force<MIXED>(facc, i, F, 1.0);
+        put_force<MIXED>(facc, j, F, -1.0);
         if (want && on) { v[0] = e; vir_pair(v + 1, F, rd); }
     }
     if (want) {
@@ -292,7 +288,7 @@ __global__ void k_bond(const double* __restrict__ pos, const int2* __restrict__ 
 
 template <bool MIXED>
 __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ ijk, const double2* __restrict__ par,
-                       int nterm, const DynState* __restrict__ dyn, TermOut out, long long* acc, int want) {
+                       int nterm, const DynState* __restrict__ dyn, void* facc, long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
@@ -301,7 +297,7 @@ __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ 
         int at[3] = {ijk[n].x, ijk[n].y, ijk[n].z};
         const bool on = eval_angl<T>(pos, at[0], at[1], at[2], par[n], dyn, F, e);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) put_force<MIXED>(out, n, 3, q, at[q], F[q], 1.0);
+        for (int q = 0; q < 3; ++q) put_force<MIXED>(facc, at[q], F[q], 1.0);
         if (want && on) {
             v[0] = e;
 #pragma unroll
@@ -317,7 +313,7 @@ __global__ void k_angl(const double* __restrict__ pos, const int4* __restrict__ 
 
 template <bool MIXED, bool RB>
 __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ ijkl, const double4* __restrict__ par,
-                       const double* __restrict__ rbc, int nterm, const DynState* __restrict__ dyn, TermOut out,
+                       const double* __restrict__ rbc, int nterm, const DynState* __restrict__ dyn, void* facc,
                        long long* acc, int want, unsigned* status) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -328,7 +324,7 @@ __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ 
         eval_tors<T, RB>(pos, at[0], at[1], at[2], at[3], RB ? make_double4(0, 0, 0, 0) : par[n],
                          RB ? rbc + 6 * (size_t)n : nullptr, dyn, F, e, status);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) put_force<MIXED>(out, n, 4, q, at[q], F[q], 1.0);
+        for (int q = 0; q < 4; ++q) put_force<MIXED>(facc, at[q], F[q], 1.0);
         if (want) {
             v[0] = e;
 #pragma unroll
@@ -345,7 +341,7 @@ __global__ void k_tors(const double* __restrict__ pos, const int4* __restrict__ 
 template <bool MIXED>
 __global__ void k_non14(const double* __restrict__ pos, const double* __restrict__ chrg, const int* __restrict__ typ,
                         const int2* __restrict__ ij, const double2* __restrict__ fac, int nterm, int ntyp,
-                        const double2* __restrict__ lj64, const DynState* __restrict__ dyn, TermOut out,
+                        const double2* __restrict__ lj64, const DynState* __restrict__ dyn, void* facc,
                         long long* acc, int want) {
     typedef typename std::conditional<MIXED, float, double>::type T;
     int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -354,8 +350,8 @@ __global__ void k_non14(const double* __restrict__ pos, const double* __restrict
         int i = ij[n].x, j = ij[n].y;
         double F[3], rd[3], de, dv;
         eval_14<T>(pos, i, j, chrg[i] * chrg[j], lj64[typ[i] * ntyp + typ[j]], fac[n], dyn, F, rd, de, dv);
-        put_force<MIXED>(out, n, 2, 0, i, F, 1.0);
-        put_force<MIXED>(out, n, 2, 1, j, F, -1.0);
+        put_force<MIXED>(facc, i, F, 1.0);
+        put_force<MIXED>(facc, j, F, -1.0);
         if (want) { v[0] = de; v[1] = dv; vir_pair(v + 2, F, rd); }
     }
     if (want) {
@@ -369,15 +365,15 @@ template <bool MIXED>
 __global__ void k_excl(const double* __restrict__ pos, const double* __restrict__ chrg,
                        const int2* __restrict__ pairs, int npair, const double4* __restrict__ spl64,
                        const float4* __restrict__ spl32, int nspl, double h, const DynState* __restrict__ dyn,
-                       TermOut out, long long* acc, int want) {
+                       void* facc, long long* acc, int want) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double v[11] = {0};
     if (k < npair) {
         int i = pairs[k].x, j = pairs[k].y;
         double F[3], rd[3], e;
         eval_excl<MIXED>(pos, i, j, chrg[i] * chrg[j], spl64, spl32, nspl, h, dyn, F, rd, e);
-        put_force<MIXED>(out, k, 2, 0, i, F, 1.0);
-        put_force<MIXED>(out, k, 2, 1, j, F, -1.0);
+        put_force<MIXED>(facc, i, F, 1.0);
+        put_force<MIXED>(facc, j, F, -1.0);
         v[0] = -e;
         vir_pair(v + 1, F, rd);
     }
@@ -389,31 +385,234 @@ __global__ void k_excl(const double* __restrict__ pos, const double* __restrict_
     }
 }
 
-// ---- per-atom sum of the slot forces --------------------------------------------
-// type of a slot from the type bases; only the types in `mask` were written by
-// this evaluation, the others hold another MTS group's values and are skipped
-struct SlotTypes { long long base[7]; };
+// ---- block kernel (near terms) ---------------------------------------------------
+struct TermsDev {
+    const int2* bond_ij; const double2* bond_p;
+    const int4* angl_ijk; const double2* angl_p;
+    const int4* tors_ijkl; const double4* tors_p;
+    const int4* rb_ijkl; const double* rb_c;
+    const int2* p14_ij; const double2* p14_f;
+    const int2* expair;
+    const double* chrg; const int* typ; const double2* lj64; int ntyp;
+    const double4* spl64; const float4* spl32; int nspl; double hspl;
+};
+struct BlkDev {
+    const int* a0; const int* nloc; const int* t; const int* soff; const int* ip; const int* incp;
+    const unsigned short* inc;
+    int nblk, smax;
+};
 
-template <bool MIXED>
-__global__ void k_slot_gather(const int* __restrict__ inc_start, const int* __restrict__ inc_slot,
-                              const void* __restrict__ slot, SlotTypes ty, int mask, int n, void* facc) {
+// TENS: the steps that need only the total bonded virial tensor (anisotropic
+// MTK steps without output): one 9-entry tensor summed over all types into
+// the bond tensor slot, no energies, one block reduction.  Otherwise every
+// type's energy, scalar virial and tensor, reduced per type.
+template <bool MIXED, bool TENS>
+__global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __restrict__ pos, TermsDev D, BlkDev K,
+                                                              const DynState* __restrict__ dyn, void* facc,
+                                                              long long* acc, int mask, int want, unsigned* status) {
     typedef typename std::conditional<MIXED, float, double>::type T;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const long long S = ty.base[6];
-    const T* sx = (const T*)slot;
-    const T* sy = sx + S;
-    const T* sz = sy + S;
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int k = inc_start[i]; k < inc_start[i + 1]; ++k) {
-        const int sl = inc_slot[k];
-        int t = 0;
+    extern __shared__ __align__(16) double sh[];
+    __shared__ int so[8];
+    const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    const int a0 = K.a0[b], nloc = K.nloc[b];
+    double* P = sh;                                          // [BLK_LOC_MAX][3] local positions
+    T* SX = (T*)(sh + 3 * BLK_LOC_MAX);                      // [3][smax] slot forces
+    T* SY = SX + K.smax;
+    T* SZ = SY + K.smax;
+    int* IP = (int*)(SZ + K.smax);                           // [BLK_LOC_MAX+1] incidence pointers
+    unsigned short* INC = (unsigned short*)(IP + BLK_LOC_MAX + 4);   // [smax] incidence (16-byte aligned)
+    const int* ipg = K.incp + K.ip[b];
+    const int inc0 = ipg[0], ninc = ipg[nloc] - inc0;
+    {
+        // staging: every load of a thread is issued before its stores (the
+        // sizes are bounded: 3*BLK_LOC_MAX doubles, BLK_LOC_MAX+1 pointers,
+        // smax slot ids stored as 16-byte groups from a 16-byte aligned start)
+        constexpr int NP = (3 * BLK_LOC_MAX + BLK_THREADS - 1) / BLK_THREADS;
+        constexpr int NI = (BLK_LOC_MAX + 1 + BLK_THREADS - 1) / BLK_THREADS;
+        constexpr int NV = (BLK_SLOT_CAP_MAX / 8 + BLK_THREADS - 1) / BLK_THREADS;
+        double rp[NP];
+        int ri[NI];
+        uint4 rv[NV];
+        const uint4* incv = (const uint4*)(K.inc + inc0);
+        const int nv = (ninc + 7) / 8;
 #pragma unroll
-        for (int q = 1; q < 6; ++q) t += sl >= ty.base[q] ? 1 : 0;
-        if (!((mask >> t) & 1)) continue;
-        fx += (double)sx[sl]; fy += (double)sy[sl]; fz += (double)sz[sl];
+        for (int q = 0; q < NP; ++q) { const int l = tid + q * nt; if (l < 3 * nloc) rp[q] = pos[3 * (size_t)a0 + l]; }
+#pragma unroll
+        for (int q = 0; q < NI; ++q) { const int l = tid + q * nt; if (l <= nloc) ri[q] = ipg[l]; }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) { const int l = tid + q * nt; if (l < nv) rv[q] = incv[l]; }
+        if (tid < 8) so[tid] = K.soff[8 * b + tid];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) { const int l = tid + q * nt; if (l < 3 * nloc) P[l] = rp[q]; }
+#pragma unroll
+        for (int q = 0; q < NI; ++q) { const int l = tid + q * nt; if (l <= nloc) IP[l] = ri[q] - inc0; }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) { const int l = tid + q * nt; if (l < nv) ((uint4*)INC)[l] = rv[q]; }
     }
-    if (fx != 0.0 || fy != 0.0 || fz != 0.0) force_add<MIXED>(facc, i, fx, fy, fz);
+    __syncthreads();
+    auto range = [&](int ty, int& t0, int& t1) {
+        t0 = K.t[ty * (K.nblk + 1) + b];
+        t1 = K.t[ty * (K.nblk + 1) + b + 1];
+    };
+    auto put = [&](int sl, const double* F, double sg) {
+        SX[sl] = (T)(sg * F[0]); SY[sl] = (T)(sg * F[1]); SZ[sl] = (T)(sg * F[2]);
+    };
+    double tv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};               // TENS: total tensor (a + 3b)
+    auto tens_pair = [&](const double* F, const double* r) {
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa) tv[aa + 3 * bb] += F[aa] * r[bb];
+    };
+    auto tens_abs = [&](const double* F, int l) {
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa) tv[aa + 3 * bb] += F[aa] * P[3 * l + bb];
+    };
+    const bool full = want && !TENS;
+    if (mask & 1) {
+        int t0, t1; range(0, t0, t1);
+        double v[11] = {0};
+        for (int k = t0 + tid; k < t1; k += nt) {
+            double F[3] = {0, 0, 0}, rd[3], e;
+            const int2 ij = D.bond_ij[k];
+            const bool on = eval_bond<T>(P, ij.x - a0, ij.y - a0, D.bond_p[k], dyn, F, rd, e);
+            const int sl = so[0] + 2 * (k - t0);
+            put(sl, F, 1.0); put(sl + 1, F, -1.0);
+            if (TENS && on) tens_pair(F, rd);
+            if (full && on) { v[0] += e; vir_pair(v + 1, F, rd); }
+        }
+        if (full) {
+            const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
+                                 A_VTB + 6, A_VTB + 7, A_VTB + 8};
+            block_acc<11>(v, acc, idx, !MIXED);
+            __syncthreads();
+        }
+    }
+    if (mask & 2) {
+        int t0, t1; range(1, t0, t1);
+        double v[11] = {0};
+        for (int k = t0 + tid; k < t1; k += nt) {
+            double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
+            const int4 q4 = D.angl_ijk[k];
+            const int at[3] = {q4.x - a0, q4.y - a0, q4.z - a0};
+            const bool on = eval_angl<T>(P, at[0], at[1], at[2], D.angl_p[k], dyn, F, e);
+            const int sl = so[1] + 3 * (k - t0);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) put(sl + q, F[q], 1.0);
+            if (TENS && on) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) tens_abs(F[q], at[q]);
+            }
+            if (full && on) {
+                v[0] += e;
+#pragma unroll
+                for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], P, at[q]);
+            }
+        }
+        if (full) {
+            const int idx[11] = {A_ANGL, A_VA, A_VTA + 0, A_VTA + 1, A_VTA + 2, A_VTA + 3, A_VTA + 4, A_VTA + 5,
+                                 A_VTA + 6, A_VTA + 7, A_VTA + 8};
+            block_acc<11>(v, acc, idx, !MIXED);
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int rb = 0; rb < 2; ++rb) {
+        if (!(mask & (4 << rb))) continue;
+        int t0, t1; range(2 + rb, t0, t1);
+        double v[11] = {0};
+        for (int k = t0 + tid; k < t1; k += nt) {
+            const int4 q4 = rb ? D.rb_ijkl[k] : D.tors_ijkl[k];
+            const int at[4] = {q4.x - a0, q4.y - a0, q4.z - a0, q4.w - a0};
+            double F[4][3], e;
+            if (rb) eval_tors<T, true>(P, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0), D.rb_c + 6 * (size_t)k,
+                                       dyn, F, e, status);
+            else eval_tors<T, false>(P, at[0], at[1], at[2], at[3], D.tors_p[k], nullptr, dyn, F, e, status);
+            const int sl = so[2 + rb] + 4 * (k - t0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) put(sl + q, F[q], 1.0);
+            if (TENS) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) tens_abs(F[q], at[q]);
+            }
+            if (full) {
+                v[0] += e;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) vir_abs(v + 1, F[q], P, at[q]);
+            }
+        }
+        if (full) {
+            const int idx[11] = {rb ? A_TORSRB : A_TORS, A_VT, A_VTT + 0, A_VTT + 1, A_VTT + 2, A_VTT + 3,
+                                 A_VTT + 4, A_VTT + 5, A_VTT + 6, A_VTT + 7, A_VTT + 8};
+            block_acc<11>(v, acc, idx, !MIXED);
+            __syncthreads();
+        }
+    }
+    if (mask & 16) {
+        int t0, t1; range(4, t0, t1);
+        double v[12] = {0};
+        for (int k = t0 + tid; k < t1; k += nt) {
+            const int2 ij = D.p14_ij[k];
+            double F[3], rd[3], de, dv;
+            eval_14<T>(P, ij.x - a0, ij.y - a0, D.chrg[ij.x] * D.chrg[ij.y], D.lj64[D.typ[ij.x] * D.ntyp + D.typ[ij.y]],
+                       D.p14_f[k], dyn, F, rd, de, dv);
+            const int sl = so[4] + 2 * (k - t0);
+            put(sl, F, 1.0); put(sl + 1, F, -1.0);
+            if (TENS) tens_pair(F, rd);
+            if (full) { v[0] += de; v[1] += dv; vir_pair(v + 2, F, rd); }
+        }
+        if (full) {
+            const int idx[12] = {A_ELC14, A_VDW14, A_V14, A_VT14 + 0, A_VT14 + 1, A_VT14 + 2, A_VT14 + 3,
+                                 A_VT14 + 4, A_VT14 + 5, A_VT14 + 6, A_VT14 + 7, A_VT14 + 8};
+            block_acc<12>(v, acc, idx, !MIXED);
+            __syncthreads();
+        }
+    }
+    if (mask & 32) {
+        int t0, t1; range(5, t0, t1);
+        double v[11] = {0};
+        for (int k = t0 + tid; k < t1; k += nt) {
+            const int2 ij = D.expair[k];
+            double F[3], rd[3], e;
+            eval_excl<MIXED>(P, ij.x - a0, ij.y - a0, D.chrg[ij.x] * D.chrg[ij.y], D.spl64, D.spl32, D.nspl, D.hspl,
+                             dyn, F, rd, e);
+            const int sl = so[5] + 2 * (k - t0);
+            put(sl, F, 1.0); put(sl + 1, F, -1.0);
+            if (TENS) tens_pair(F, rd);
+            if (full) { v[0] -= e; vir_pair(v + 1, F, rd); }
+        }
+        if (full) {
+            // pot_elc -= potij; pot_viri_coul -= potij; tensor (lower triangle) += f r
+            double w[8] = {v[0], v[0], v[2], v[3], v[4], v[6], v[7], v[10]};
+            const int idx[8] = {A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
+            block_acc<8>(w, acc, idx, !MIXED);
+        }
+    }
+    if (TENS && want) {
+        const int idx[9] = {A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5, A_VTB + 6, A_VTB + 7,
+                            A_VTB + 8};
+        block_acc<9>(tv, acc, idx, !MIXED);
+    }
+    __syncthreads();
+    // per local atom: its slots in incidence order (types outside mask hold
+    // nothing of this evaluation and are skipped)
+    for (int l = tid; l < nloc; l += nt) {
+        const int p0 = IP[l], p1 = IP[l + 1];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        bool any = false;
+        for (int p = p0; p < p1; ++p) {
+            const int sl = INC[p];
+            int ty = 0;
+#pragma unroll
+            for (int q = 1; q < 6; ++q) ty += sl >= so[q] ? 1 : 0;
+            if (!((mask >> ty) & 1)) continue;
+            fx += (double)SX[sl]; fy += (double)SY[sl]; fz += (double)SZ[sl];
+            any = true;
+        }
+        if (any) force_add<MIXED>(facc, a0 + l, fx, fy, fz);
+    }
 }
 
 // ---- host side -------------------------------------------------------------------
@@ -432,51 +631,15 @@ static pgk_status up(pgk_ctx* c, T** dst, const std::vector<T>& v) {
     return PGK_OK;
 }
 
-// Term arrays ordered by their lowest atom (locality of the position gathers
-// and slot writes), the global slot layout and each atom's slot incidence
-// list (by type, then term), and the slot array itself.
+// Term arrays: per type the near terms (atom span < BLK_FAR_SPAN) first,
+// ordered by their lowest atom, then the far ones.  Block plan: consecutive
+// lowest atoms are gathered into blocks while the block's slots fit the
+// shared-memory slot planes and its local atom range fits BLK_LOC_MAX; each
+// block's incidence list gives every local atom its slots by type, term and
+// position in the term.
 pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const std::vector<int>&) {
     const int n = c->natom;
     const int K[6] = {2, 3, 4, 4, 2, 2};
-    auto sort_type = [&](int count, auto first_atom, auto apply) {
-        std::vector<int> order(count);
-        for (int k = 0; k < count; ++k) order[k] = k;
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return first_atom(x) < first_atom(y); });
-        apply(order);
-    };
-    auto mn = [](std::initializer_list<int> v) { return std::min(v); };
-    sort_type((int)t.bij.size(), [&](int k) { return mn({t.bij[k].x, t.bij[k].y}); },
-              [&](const std::vector<int>& o) { reorder(t.bij, o); reorder(t.bp, o); });
-    sort_type((int)t.aijk.size(), [&](int k) { return mn({t.aijk[k].x, t.aijk[k].y, t.aijk[k].z}); },
-              [&](const std::vector<int>& o) { reorder(t.aijk, o); reorder(t.ap, o); });
-    sort_type((int)t.tij.size(), [&](int k) { return mn({t.tij[k].x, t.tij[k].y, t.tij[k].z, t.tij[k].w}); },
-              [&](const std::vector<int>& o) { reorder(t.tij, o); reorder(t.tp, o); });
-    sort_type((int)t.rij.size(), [&](int k) { return mn({t.rij[k].x, t.rij[k].y, t.rij[k].z, t.rij[k].w}); },
-              [&](const std::vector<int>& o) {
-                  std::vector<double> rc2(t.rc.size());
-                  for (size_t k = 0; k < o.size(); ++k)
-                      for (int q = 0; q < 6; ++q) rc2[6 * k + q] = t.rc[6 * o[k] + q];
-                  reorder(t.rij, o);
-                  t.rc.swap(rc2);
-              });
-    sort_type((int)t.p14.size(), [&](int k) { return mn({t.p14[k].x, t.p14[k].y}); },
-              [&](const std::vector<int>& o) { reorder(t.p14, o); reorder(t.f14, o); });
-    sort_type((int)t.ex.size(), [&](int k) { return mn({t.ex[k].x, t.ex[k].y}); },
-              [&](const std::vector<int>& o) { reorder(t.ex, o); });
-    pgk_status s;
-    c->nbond = (int)t.bij.size(); c->nangl = (int)t.aijk.size(); c->ntors = (int)t.tij.size();
-    c->ntorsrb = (int)t.rij.size(); c->n14 = (int)t.p14.size(); c->nexpair = (int)t.ex.size();
-    if ((s = up(c, &c->bond_ij, t.bij)) || (s = up(c, &c->bond_p, t.bp)) || (s = up(c, &c->angl_ijk, t.aijk)) ||
-        (s = up(c, &c->angl_p, t.ap)) || (s = up(c, &c->tors_ijkl, t.tij)) || (s = up(c, &c->tors_p, t.tp)) ||
-        (s = up(c, &c->rb_ijkl, t.rij)) || (s = up(c, &c->rb_c, t.rc)) || (s = up(c, &c->p14_ij, t.p14)) ||
-        (s = up(c, &c->p14_f, t.f14)) || (s = up(c, &c->expair, t.ex)))
-        return s;
-    const long long cnt[6] = {c->nbond, c->nangl, c->ntors, c->ntorsrb, c->n14, c->nexpair};
-    c->slot_base[0] = 0;
-    for (int ty = 0; ty < 6; ++ty) c->slot_base[ty + 1] = c->slot_base[ty] + K[ty] * cnt[ty];
-    const long long S = c->slot_base[6];
-    if (S >= (1LL << 31)) return pgk_fail(c, PGK_E_UNSUPPORTED, "more than 2^31 bonded term slots");
-    std::vector<int> deg(n + 1, 0);
     auto atoms_of = [&](int ty, long long k, int* at) {
         switch (ty) {
             case 0: at[0] = t.bij[k].x; at[1] = t.bij[k].y; break;
@@ -487,25 +650,131 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
             default: at[0] = t.ex[k].x; at[1] = t.ex[k].y; break;
         }
     };
-    int at[4];
-    for (int ty = 0; ty < 6; ++ty)
-        for (long long k = 0; k < cnt[ty]; ++k) {
-            atoms_of(ty, k, at);
-            for (int q = 0; q < K[ty]; ++q) deg[at[q] + 1]++;
+    auto lo_hi = [&](int ty, long long k, int& lo, int& hi) {
+        int at[4];
+        atoms_of(ty, k, at);
+        lo = hi = at[0];
+        for (int q = 1; q < K[ty]; ++q) { lo = std::min(lo, at[q]); hi = std::max(hi, at[q]); }
+    };
+    const int count0[6] = {(int)t.bij.size(), (int)t.aijk.size(), (int)t.tij.size(), (int)t.rij.size(),
+                           (int)t.p14.size(), (int)t.ex.size()};
+    for (int ty = 0; ty < 6; ++ty) {
+        std::vector<long long> key(count0[ty]);
+        int nnear = 0;
+        for (int k = 0; k < count0[ty]; ++k) {
+            int lo, hi;
+            lo_hi(ty, k, lo, hi);
+            const bool far = hi - lo >= BLK_FAR_SPAN;
+            key[k] = ((long long)(far ? 1 : 0) << 32) | (long long)lo;
+            nnear += far ? 0 : 1;
         }
-    for (int i = 0; i < n; ++i) deg[i + 1] += deg[i];
-    std::vector<int> inc((size_t)std::max<long long>(S, 1)), fill(deg.begin(), deg.end() - 1);
-    for (int ty = 0; ty < 6; ++ty)
-        for (long long k = 0; k < cnt[ty]; ++k) {
-            atoms_of(ty, k, at);
-            for (int q = 0; q < K[ty]; ++q) inc[fill[at[q]]++] = (int)(c->slot_base[ty] + K[ty] * k + q);
+        std::vector<int> o(count0[ty]);
+        for (int k = 0; k < count0[ty]; ++k) o[k] = k;
+        std::stable_sort(o.begin(), o.end(), [&](int x, int y) { return key[x] < key[y]; });
+        switch (ty) {
+            case 0: reorder(t.bij, o); reorder(t.bp, o); break;
+            case 1: reorder(t.aijk, o); reorder(t.ap, o); break;
+            case 2: reorder(t.tij, o); reorder(t.tp, o); break;
+            case 3: {
+                std::vector<double> rc2(t.rc.size());
+                for (size_t k = 0; k < o.size(); ++k)
+                    for (int q = 0; q < 6; ++q) rc2[6 * k + q] = t.rc[6 * o[k] + q];
+                reorder(t.rij, o);
+                t.rc.swap(rc2);
+                break;
+            }
+            case 4: reorder(t.p14, o); reorder(t.f14, o); break;
+            default: reorder(t.ex, o); break;
         }
-    if ((s = up(c, &c->inc_start, deg)) || (s = up(c, &c->inc_slot, inc))) return s;
-    if (S > 0) {
-        const size_t bytes = (size_t)3 * S * (c->mixed() ? sizeof(float) : sizeof(double));
-        PGK_CUDA(c, cudaMalloc(&c->slot_f, bytes));
-        PGK_CUDA(c, cudaMemset(c->slot_f, 0, bytes));
+        c->nnear[ty] = nnear;
     }
+    pgk_status s;
+    c->nbond = count0[0]; c->nangl = count0[1]; c->ntors = count0[2];
+    c->ntorsrb = count0[3]; c->n14 = count0[4]; c->nexpair = count0[5];
+    if ((s = up(c, &c->bond_ij, t.bij)) || (s = up(c, &c->bond_p, t.bp)) || (s = up(c, &c->angl_ijk, t.aijk)) ||
+        (s = up(c, &c->angl_p, t.ap)) || (s = up(c, &c->tors_ijkl, t.tij)) || (s = up(c, &c->tors_p, t.tp)) ||
+        (s = up(c, &c->rb_ijkl, t.rij)) || (s = up(c, &c->rb_c, t.rc)) || (s = up(c, &c->p14_ij, t.p14)) ||
+        (s = up(c, &c->p14_f, t.f14)) || (s = up(c, &c->expair, t.ex)))
+        return s;
+
+    // ---- block plan ----
+    const int cap = blk_slot_cap(c->mixed());
+    std::vector<int> a0v, nlocv, soffv, ipv, incp;
+    std::vector<int> tst[6];
+    std::vector<unsigned short> inc;
+    int ptr[6] = {0, 0, 0, 0, 0, 0};
+    int cur_a0 = -1, cur_hi = -1, cur_slots = 0;
+    int start[6];
+    auto close_block = [&](const int* end) {
+        const int b0 = cur_a0, nloc = cur_hi - cur_a0 + 1;
+        int off[8];
+        off[0] = 0;
+        for (int ty = 0; ty < 6; ++ty) off[ty + 1] = off[ty] + K[ty] * (end[ty] - start[ty]);
+        off[7] = 0;
+        a0v.push_back(b0);
+        nlocv.push_back(nloc);
+        for (int q = 0; q < 8; ++q) soffv.push_back(off[q]);
+        for (int ty = 0; ty < 6; ++ty) tst[ty].push_back(start[ty]);
+        ipv.push_back((int)incp.size());
+        std::vector<int> deg(nloc + 1, 0);
+        int at[4];
+        for (int ty = 0; ty < 6; ++ty)
+            for (int k = start[ty]; k < end[ty]; ++k) {
+                atoms_of(ty, k, at);
+                for (int q = 0; q < K[ty]; ++q) deg[at[q] - b0 + 1]++;
+            }
+        for (int l = 0; l < nloc; ++l) deg[l + 1] += deg[l];
+        const int base = (int)inc.size();            // a multiple of 8: 16-byte aligned groups
+        for (int l = 0; l <= nloc; ++l) incp.push_back(base + deg[l]);
+        inc.resize(base + ((deg[nloc] + 7) & ~7), 0);
+        std::vector<int> fill(deg.begin(), deg.end() - 1);
+        for (int ty = 0; ty < 6; ++ty)
+            for (int k = start[ty]; k < end[ty]; ++k) {
+                atoms_of(ty, k, at);
+                for (int q = 0; q < K[ty]; ++q)
+                    inc[base + fill[at[q] - b0]++] = (unsigned short)(off[ty] + K[ty] * (k - start[ty]) + q);
+            }
+    };
+    for (int a = 0; a < n; ++a) {
+        int end[6], slots = 0, hi = -1;
+        for (int ty = 0; ty < 6; ++ty) {
+            int k = ptr[ty];
+            for (; k < c->nnear[ty]; ++k) {
+                int lo, h;
+                lo_hi(ty, k, lo, h);
+                if (lo != a) break;
+                slots += K[ty];
+                hi = std::max(hi, h);
+            }
+            end[ty] = k;
+        }
+        if (slots == 0) continue;
+        if (slots > cap)
+            return pgk_fail(c, PGK_E_UNSUPPORTED, "too many bonded terms share one lowest atom");
+        if (cur_a0 >= 0 && (cur_slots + slots > cap || std::max(cur_hi, hi) - cur_a0 + 1 > BLK_LOC_MAX)) {
+            close_block(ptr);
+            cur_a0 = -1;
+        }
+        if (cur_a0 < 0) {
+            cur_a0 = a; cur_hi = hi; cur_slots = 0;
+            for (int ty = 0; ty < 6; ++ty) start[ty] = ptr[ty];
+        }
+        cur_slots += slots;
+        cur_hi = std::max(cur_hi, hi);
+        for (int ty = 0; ty < 6; ++ty) ptr[ty] = end[ty];
+    }
+    if (cur_a0 >= 0) close_block(ptr);
+    c->nblk = (int)a0v.size();
+    if (c->nblk == 0) return PGK_OK;
+    std::vector<int> tall;
+    for (int ty = 0; ty < 6; ++ty) {
+        tall.insert(tall.end(), tst[ty].begin(), tst[ty].end());
+        tall.push_back(ptr[ty]);          // end of the last block
+    }
+    if ((s = up(c, &c->blk_a0, a0v)) || (s = up(c, &c->blk_nloc, nlocv)) || (s = up(c, &c->blk_t, tall)) ||
+        (s = up(c, &c->blk_soff, soffv)) || (s = up(c, &c->blk_ip, ipv)) || (s = up(c, &c->blk_incp, incp)) ||
+        (s = up(c, &c->blk_inc, inc)))
+        return s;
     return PGK_OK;
 }
 
@@ -610,63 +879,77 @@ pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h) {
 }
 
 // One MTS group's bonded terms (mask bits: 0 bond, 1 angle, 2 periodic
-// torsion, 3 RB torsion, 4 1-4 pairs, 5 excluded-pair Ewald correction): one
-// kernel per active type writing the slots, then the per-atom gather.
+// torsion, 3 RB torsion, 4 1-4 pairs, 5 excluded-pair Ewald correction): the
+// block kernel for the near terms, the per-type kernels for the far ones.
 template <bool MIXED>
-static void terms_impl(pgk_ctx* c, int group, int mask, bool want) {
+static void terms_impl(pgk_ctx* c, int group, int mask, bool want, bool tens) {
     long long* acc = c->acc + (size_t)group * NACC;
+    void* facc = c->facc[group];
     const int w = want ? 1 : 0;
-    const int tb = 128;
-    const long long S = c->slot_base[6];
-    auto out = [&](int ty) { return TermOut{c->facc[group], c->slot_f, S, c->slot_base[ty]}; };
-    if ((mask & 1) && c->nbond) {
-        k_bond<MIXED><<<(c->nbond + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->bond_ij, c->bond_p, c->nbond, c->dyn,
-                                                                   out(0), acc, w);
-        PGK_LAUNCHED(c);
-    }
-    if ((mask & 2) && c->nangl) {
-        k_angl<MIXED><<<(c->nangl + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->angl_ijk, c->angl_p, c->nangl, c->dyn,
-                                                                   out(1), acc, w);
-        PGK_LAUNCHED(c);
-    }
-    if ((mask & 4) && c->ntors) {
-        k_tors<MIXED, false><<<(c->ntors + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->tors_ijkl, c->tors_p, nullptr,
-                                                                          c->ntors, c->dyn, out(2), acc, w, c->status);
-        PGK_LAUNCHED(c);
-    }
-    if ((mask & 8) && c->ntorsrb) {
-        k_tors<MIXED, true><<<(c->ntorsrb + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->rb_ijkl, nullptr, c->rb_c,
-                                                                           c->ntorsrb, c->dyn, out(3), acc, w,
+    if (c->nblk > 0) {
+        TermsDev D{c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl, c->tors_p, c->rb_ijkl, c->rb_c,
+                   c->p14_ij, c->p14_f, c->expair, c->chrg, c->typ, c->lj64, c->ntyp, c->spl64, c->spl32, c->nspl,
+                   c->hspl};
+        const int cap = blk_slot_cap(MIXED);
+        BlkDev K{c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff, c->blk_ip, c->blk_incp, c->blk_inc, c->nblk, cap};
+        const size_t sm = 3 * BLK_LOC_MAX * sizeof(double) + 3 * (size_t)cap * (MIXED ? sizeof(float) : sizeof(double)) +
+                          (BLK_LOC_MAX + 4) * sizeof(int) + (size_t)cap * sizeof(unsigned short);
+        if (tens) {
+            smem_limit(k_intra_blk<MIXED, true>, sm);
+            k_intra_blk<MIXED, true><<<c->nblk, BLK_THREADS, sm, c->st>>>(c->pos, D, K, c->dyn, facc, acc, mask, w,
+                                                                          c->status);
+        } else {
+            smem_limit(k_intra_blk<MIXED, false>, sm);
+            k_intra_blk<MIXED, false><<<c->nblk, BLK_THREADS, sm, c->st>>>(c->pos, D, K, c->dyn, facc, acc, mask, w,
                                                                            c->status);
+        }
         PGK_LAUNCHED(c);
     }
-    if ((mask & 16) && c->n14) {
-        k_non14<MIXED><<<(c->n14 + tb - 1) / tb, tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij, c->p14_f, c->n14,
-                                                                  c->ntyp, c->lj64, c->dyn, out(4), acc, w);
+    const int tb = 128;
+    auto nb = [&](int m) { return (m + tb - 1) / tb; };
+    int f = c->nnear[0], m = c->nbond - f;
+    if ((mask & 1) && m > 0) {
+        k_bond<MIXED><<<nb(m), tb, 0, c->st>>>(c->pos, c->bond_ij + f, c->bond_p + f, m, c->dyn, facc, acc, w);
         PGK_LAUNCHED(c);
     }
-    if ((mask & 32) && c->nexpair) {
-        k_excl<MIXED><<<(c->nexpair + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->expair, c->nexpair, c->spl64,
-                                                                    c->spl32, c->nspl, c->hspl, c->dyn, out(5), acc,
-                                                                    w);
+    f = c->nnear[1]; m = c->nangl - f;
+    if ((mask & 2) && m > 0) {
+        k_angl<MIXED><<<nb(m), tb, 0, c->st>>>(c->pos, c->angl_ijk + f, c->angl_p + f, m, c->dyn, facc, acc, w);
         PGK_LAUNCHED(c);
     }
-    if (S > 0) {
-        SlotTypes ty;
-        for (int q = 0; q < 7; ++q) ty.base[q] = c->slot_base[q];
-        k_slot_gather<MIXED><<<(c->natom + 255) / 256, 256, 0, c->st>>>(c->inc_start, c->inc_slot, c->slot_f, ty,
-                                                                         mask, c->natom, c->facc[group]);
+    f = c->nnear[2]; m = c->ntors - f;
+    if ((mask & 4) && m > 0) {
+        k_tors<MIXED, false><<<nb(m), tb, 0, c->st>>>(c->pos, c->tors_ijkl + f, c->tors_p + f, nullptr, m, c->dyn,
+                                                      facc, acc, w, c->status);
+        PGK_LAUNCHED(c);
+    }
+    f = c->nnear[3]; m = c->ntorsrb - f;
+    if ((mask & 8) && m > 0) {
+        k_tors<MIXED, true><<<nb(m), tb, 0, c->st>>>(c->pos, c->rb_ijkl + f, nullptr, c->rb_c + 6 * (size_t)f, m,
+                                                     c->dyn, facc, acc, w, c->status);
+        PGK_LAUNCHED(c);
+    }
+    f = c->nnear[4]; m = c->n14 - f;
+    if ((mask & 16) && m > 0) {
+        k_non14<MIXED><<<nb(m), tb, 0, c->st>>>(c->pos, c->chrg, c->typ, c->p14_ij + f, c->p14_f + f, m, c->ntyp,
+                                                c->lj64, c->dyn, facc, acc, w);
+        PGK_LAUNCHED(c);
+    }
+    f = c->nnear[5]; m = c->nexpair - f;
+    if ((mask & 32) && m > 0) {
+        k_excl<MIXED><<<nb(m), tb, 0, c->st>>>(c->pos, c->chrg, c->expair + f, m, c->spl64, c->spl32, c->nspl,
+                                               c->hspl, c->dyn, facc, acc, w);
         PGK_LAUNCHED(c);
     }
 }
 
-pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want) {
+pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want, bool tens) {
     const long long cnt[6] = {c->nbond, c->nangl, c->ntors, c->ntorsrb, c->n14, c->nexpair};
     int active = 0;
     for (int ty = 0; ty < 6; ++ty) if (((mask >> ty) & 1) && cnt[ty] > 0) active |= 1 << ty;
     if (!active) return PGK_OK;
-    if (c->mixed()) terms_impl<true>(c, group, active, want);
-    else terms_impl<false>(c, group, active, want);
+    if (c->mixed()) terms_impl<true>(c, group, active, want, tens && want);
+    else terms_impl<false>(c, group, active, want, tens && want);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }

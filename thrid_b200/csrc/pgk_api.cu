@@ -105,7 +105,7 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
     int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
                (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
                (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (c->prm.mts_vdw == flag ? 32 : 0);
-    return launch_intra(c, g, mask, ene || vir);
+    return launch_intra(c, g, mask, ene || vir, vir && tensor_only);
 }
 
 double accv(const pgk_ctx* c, long long v) {
@@ -519,7 +519,8 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
                     c->ccnt, c->xq, c->xq64, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
-                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->slot_f, c->inc_start, c->inc_slot,
+                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
+                    c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};
     for (void* b : bufs) if (b) cudaFree(b);
@@ -699,6 +700,7 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
             case 3: return spme_bench(c, 3);
             default:
                 if (which >= 64 && which < 128) return launch_intra(c, 0, which - 64, true);
+                if (which >= 128 && which < 192) return launch_intra(c, 0, which - 128, true, true);
                 return pgk_fail(c, PGK_E_INVALID, "unknown kernel id");
         }
     };

@@ -80,11 +80,21 @@ struct pgk_ctx {
     int ntorsrb = 0; int4* rb_ijkl = nullptr; double* rb_c = nullptr;       // [6*n]
     int n14 = 0; int2* p14_ij = nullptr; double2* p14_f = nullptr;          // (elc fac, vdw fac)
 
-    // ---- bonded force slots (one slot per term atom) and their gather ----
-    long long slot_base[7] = {0, 0, 0, 0, 0, 0, 0};   // per term type: bond, angle, tors, RB, 1-4, excl
-    void* slot_f = nullptr;       // [3][nslot] slot forces (float mixed / double FP64)
-    int* inc_start = nullptr;     // [natom+1] slot incidence CSR
-    int* inc_slot = nullptr;      // global slot ids, per atom by type then term
+    // ---- bonded block plan ----
+    // Per type (bond, angle, tors, RB, 1-4, excl) the terms [0, nnear) are the
+    // "near" ones (atom span < BLK_FAR_SPAN), sorted by their lowest atom; the
+    // rest [nnear, n) go through the per-type kernels with force atomics.
+    // Block b owns the near terms whose lowest atom lies in its atom range;
+    // its local atoms are [a0, a0 + nloc).
+    int nnear[6] = {0, 0, 0, 0, 0, 0};
+    int nblk = 0;
+    int* blk_a0 = nullptr;        // [nblk]
+    int* blk_nloc = nullptr;      // [nblk]
+    int* blk_t = nullptr;         // [6][nblk+1] first term of each block, per type
+    int* blk_soff = nullptr;      // [nblk][8] local slot offset per type, [6] = slot count
+    int* blk_ip = nullptr;        // [nblk] offset of the block's nloc+1 pointers in blk_incp
+    int* blk_incp = nullptr;      // per block and local atom: range in blk_inc
+    unsigned short* blk_inc = nullptr;   // local slot ids, per atom by type, term, position
 
     // ---- constraints ----
     int ncgroup = 0, nconstraint = 0;
@@ -207,7 +217,9 @@ pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir);
 // ---- launchers (k_bonded.cu) ----
 pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>& mol_idx, const std::vector<int>& mol_list);
 pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_all);
-pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want);
+// tens: only the total bonded virial tensor is wanted (it goes to the bond
+// tensor slot; no energies), as in the anisotropic MTK steps without output
+pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want, bool tens = false);
 
 // ---- launchers (k_heatf.cu, heat flux + region Langevin) ----
 struct HfDev;
