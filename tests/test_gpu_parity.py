@@ -32,6 +32,7 @@ def case(name):
             "propanol_cells": lambda: S.propanol_box(nside=11, box=57.2),    # mklist_cell, 4^3 cells
             "butane_small": lambda: S.small_box("butane", nside=5, spacing=5.4, nfft=24, order=5),
             "nacl": lambda: _jittered(S.nacl_lattice()),
+            "propanol_scattered": lambda: _scattered(S.small_box("propanol", nside=4, spacing=5.6)),
         }[name]()
     return _cache[name]
 
@@ -40,6 +41,33 @@ def _jittered(s, amp=0.05, seed=11):
     """Perfect lattices have ~0 net force; displace ions so forces are O(1)."""
     s.atmcor = s.atmcor + np.random.default_rng(seed).normal(0.0, amp, s.atmcor.shape)
     return s
+
+
+def _scattered(s):
+    """The same system with the atoms of its second half of molecules
+    interleaved (atom k of molecule m -> far from atom k+1): their bonded
+    terms span hundreds of atom indices, the first half's stay compact, so
+    both bonded paths (per-block and per-type) run."""
+    import dataclasses
+    nm = s.nmole
+    mols = [list(s.molept_list[s.molept_index[m]:s.molept_index[m + 1]]) for m in range(nm)]
+    order = [a for m in mols[:nm // 2] for a in m]
+    rest = mols[nm // 2:]
+    for k in range(max(len(m) for m in rest)):
+        order += [m[k] for m in rest if k < len(m)]
+    new_of = np.empty(s.natom, dtype=np.int64)
+    new_of[np.asarray(order)] = np.arange(s.natom)
+    old = np.asarray(order)
+    mp = lambda a: new_of[np.asarray(a, dtype=np.int64)] if len(a) else np.asarray(a)
+    bonds, angles, tors, torsrb = mp(s.bonds), mp(s.angles), mp(s.tors), mp(s.torsrb)
+    index_excl, list_excl = S._mkexcl(s.natom, bonds, angles, tors, torsrb)
+    return dataclasses.replace(
+        s, name=s.name + "_scattered", atmcor=s.atmcor[old].copy(), atmvel=s.atmvel[old].copy(),
+        atmmass=s.atmmass[old].copy(), atmchrg=s.atmchrg[old].copy(), atmindex=s.atmindex[old].copy(),
+        molept_list=mp(s.molept_list).astype(s.molept_list.dtype), index_excl=index_excl, list_excl=list_excl,
+        bonds=bonds.astype(s.bonds.dtype), angles=angles.astype(s.angles.dtype), tors=tors.astype(s.tors.dtype),
+        torsrb=torsrb.astype(s.torsrb.dtype) if len(s.torsrb) else s.torsrb,
+        const_ij=mp(s.const_ij).astype(s.const_ij.dtype) if len(s.const_ij) else s.const_ij)
 
 
 def engine(s, prec, **over):
@@ -115,7 +143,7 @@ def _ref_terms(oracle_mod, s):
     return o, o.ewaldrp(), o.fft_pmep(), o.bonded()
 
 
-@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl"])
+@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl", "propanol_scattered"])
 def test_fp64_forces_energies_virials(oracle_mod, name):
     s = case(name)
     o, (rf, re, rv), (kf, ke, kv), (bf, be, bv) = _ref_terms(oracle_mod, s)
@@ -141,7 +169,7 @@ def test_fp64_forces_energies_virials(oracle_mod, name):
             assert erel(vi[k], bv[k]) < 1e-9, k
 
 
-@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl"])
+@pytest.mark.parametrize("name", ["water", "propanol_small", "butane_small", "nacl", "propanol_scattered"])
 def test_mixed_forces_within_1e5(oracle_mod, name):
     s = case(name)
     o, (rf, re, rv), (kf, ke, kv), (bf, be, bv) = _ref_terms(oracle_mod, s)

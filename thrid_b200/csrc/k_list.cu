@@ -359,14 +359,18 @@ static int list_mode_for(const pgk_ctx* c, const double* box, int* nc) {
 static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     if (npad_cap <= c->npad_cap) return PGK_OK;
     cudaFree(c->perm); cudaFree(c->pos_s); cudaFree(c->typ_s); cudaFree(c->xq); cudaFree(c->xq64);
-    cudaFree(c->ccnt); cudaFree(c->clist);
+    cudaFree(c->ccnt); cudaFree(c->clist); cudaFree(c->fsort);
     c->perm = nullptr; c->pos_s = nullptr; c->typ_s = nullptr; c->xq = nullptr; c->xq64 = nullptr;
-    c->ccnt = nullptr; c->clist = nullptr;
+    c->ccnt = nullptr; c->clist = nullptr; c->fsort = nullptr;
     int ncl = npad_cap / 8;
     PGK_CUDA(c, cudaMalloc(&c->perm, sizeof(int) * npad_cap));
     PGK_CUDA(c, cudaMalloc(&c->pos_s, sizeof(double) * 3 * npad_cap));
     PGK_CUDA(c, cudaMalloc(&c->typ_s, sizeof(int) * npad_cap));
-    if (c->mixed()) PGK_CUDA(c, cudaMalloc(&c->xq, sizeof(int4) * npad_cap));
+    if (c->mixed()) {
+        PGK_CUDA(c, cudaMalloc(&c->xq, sizeof(int4) * npad_cap));
+        PGK_CUDA(c, cudaMalloc(&c->fsort, sizeof(long long) * 3 * (size_t)npad_cap));
+        PGK_CUDA(c, cudaMemsetAsync(c->fsort, 0, sizeof(long long) * 3 * (size_t)npad_cap, c->st));
+    }
     else PGK_CUDA(c, cudaMalloc(&c->xq64, sizeof(double4) * npad_cap));
     PGK_CUDA(c, cudaMalloc(&c->ccnt, sizeof(int) * ncl));
     if (cudaMalloc(&c->clist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {

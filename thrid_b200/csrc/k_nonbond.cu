@@ -72,63 +72,66 @@ struct PairArgs {
     int ntyp; int nspl; double h, inv_h;
     double rr2, rl2, rmax2, rrcut;
     void* facc; long long* acc;
+    long long* fsort; int fstride;     // mixed: forces by sorted slot (SoA, stride fstride)
 };
 
 // ---- one pair, mixed precision -----------------------------------------------
+// Branch-free: every pair of an entry's mask is evaluated to the end and the
+// cutoffs select zero (the spline index is clamped into the table), so the
+// lanes of a warp never diverge inside the pair arithmetic.  The force on
+// cluster atom fi and the opposite force on j (g) accumulate directly.
 template <int MODE>
 __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int4 pj, const int tj,
-                                          const float sx, const float sy, const float sz, const float rmax2,
-                                          const float rr2, const float rl2, const float inv_h, const float h,
+                                          const float sx, const float sy, const float sz, const float rr2,
+                                          const float rl2, const float inv_h, const float h, const int nsplm1,
                                           const float4* __restrict__ sf, const float4* __restrict__ sp,
-                                          const float2* __restrict__ slj, float& fx, float& fy, float& fz,
-                                          float& ev, float& ee, float* wc, float* wl) {
+                                          const float2* __restrict__ slj, float (&fi)[3], float& gx, float& gy,
+                                          float& gz, float& ev, float& ee, float* wc, float* wl) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     const float dx = (float)(pi.x - pj.x) * sx;
     const float dy = (float)(pi.y - pj.y) * sy;
     const float dz = (float)(pi.z - pj.z) * sz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    if (r2 > rmax2) return;
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
-    float fc = 0.f, fl = 0.f;
-    if (r2 <= rr2) {
-        const float r = r2 * rinv;
-        const float qq = __int_as_float(pi.w) * __int_as_float(pj.w);
-        // floor(r/h) on the FP32/ALU pipes (r/h < 2^22): round to nearest via
-        // the 2^23 magic constant, step down when it rounded up
-        const float tf = r * inv_h;
-        float fm = (tf + 8388608.0f) - 8388608.0f;
-        fm = fm > tf ? fm - 1.0f : fm;
-        const int idx = __float_as_int(fm + 8388608.0f) - 0x4B000000;
-        const float d = fmaf(-fm, h, r);
-        const float4 c = sf[idx];
-        fc = qq * fmaf(d, fmaf(d, fmaf(d, c.w, c.z), c.y), c.x);
-        if (ENE) {
-            const float4 p = sp[idx];
-            ee = fmaf(qq, fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x), ee);
-        }
+    const float r = r2 * rinv;
+    const float qq = __int_as_float(pi.w) * __int_as_float(pj.w);
+    // floor(r/h) on the FP32/ALU pipes (r/h < 2^22): round to nearest via
+    // the 2^23 magic constant, step down when it rounded up
+    const float tf = r * inv_h;
+    float fm = (tf + 8388608.0f) - 8388608.0f;
+    fm = fm > tf ? fm - 1.0f : fm;
+    int idx = __float_as_int(fm + 8388608.0f) - 0x4B000000;
+    idx = min(idx, nsplm1);
+    const float d = fmaf(-fm, h, r);
+    const float4 c = sf[idx];
+    const bool inr = r2 <= rr2, inl = r2 <= rl2;
+    float fc = qq * fmaf(d, fmaf(d, fmaf(d, c.w, c.z), c.y), c.x);
+    fc = inr ? fc : 0.f;
+    if (ENE) {
+        const float4 p = sp[idx];
+        const float pe = qq * fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x);
+        ee += inr ? pe : 0.f;
     }
-    if (r2 <= rl2) {
-        const float2 lp = slj[ti + tj];
-        const float t2 = rinv2 * lp.x;
-        const float t6 = t2 * t2 * t2;
-        const float t12 = t6 * t6;
-        fl = 12.f * lp.y * (t12 - t6) * rinv2;
-        if (ENE) ev = fmaf(lp.y, t12 - 2.f * t6, ev);
-    }
+    const float2 lp = slj[ti + tj];
+    const float t2 = rinv2 * lp.x;
+    const float t6 = t2 * t2 * t2;
+    const float t12 = t6 * t6;
+    float fl = 12.f * lp.y * (t12 - t6) * rinv2;
+    fl = inl ? fl : 0.f;
+    if (ENE) ev += inl ? lp.y * (t12 - 2.f * t6) : 0.f;
     const float fs = fc + fl;
-    fx = fmaf(fs, dx, fx);
-    fy = fmaf(fs, dy, fy);
-    fz = fmaf(fs, dz, fz);
+    const float cx = fs * dx, cy = fs * dy, cz = fs * dz;
+    fi[0] += cx; fi[1] += cy; fi[2] += cz;
+    gx -= cx; gy -= cy; gz -= cz;
     if (MODE == PM_TENS) {
-        const float cx = fs * dx, cy = fs * dy, cz = fs * dz;
         wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
         wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
     }
     if (MODE == PM_FULL) {
-        const float cx = fc * dx, cy = fc * dy, cz = fc * dz;
-        wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
-        wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
+        const float ax = fc * dx, ay = fc * dy, az = fc * dz;
+        wc[0] = fmaf(ax, dx, wc[0]); wc[1] = fmaf(ax, dy, wc[1]); wc[2] = fmaf(ax, dz, wc[2]);
+        wc[3] = fmaf(ay, dy, wc[3]); wc[4] = fmaf(ay, dz, wc[4]); wc[5] = fmaf(az, dz, wc[5]);
         const float lx = fl * dx, ly = fl * dy, lz = fl * dz;
         wl[0] = fmaf(lx, dx, wl[0]); wl[1] = fmaf(lx, dy, wl[1]); wl[2] = fmaf(lx, dz, wl[2]);
         wl[3] = fmaf(ly, dy, wl[3]); wl[4] = fmaf(ly, dz, wl[4]); wl[5] = fmaf(lz, dz, wl[5]);
@@ -176,14 +179,15 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
     const float sy = (float)(dyn->box[1] * (1.0 / 4294967296.0));
     const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
-    const float rr2 = (float)a.rr2, rl2 = (float)a.rl2, rmax2 = (float)a.rmax2;
+    const float rr2 = (float)a.rr2, rl2 = (float)a.rl2;
+    const int nsplm1 = a.nspl - 1;
     const float inv_h = (float)a.inv_h, h = (float)a.h;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
     const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
     const int* __restrict__ typ_s = a.typ_s;
-    const int* __restrict__ perm = a.perm;
-    long long* __restrict__ facc = (long long*)a.facc;
+    long long* __restrict__ fs0 = a.fsort;
+    const int fst = a.fstride;
     float ev = 0.f, ee = 0.f;
     float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
@@ -203,36 +207,33 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
         unsigned e = k < cnt ? (unsigned)__ldg(row + k) : 0u;
         int4 pj = __ldg(xq + (e & 0xFFFFFFu));
         int tj = __ldg(typ_s + (e & 0xFFFFFFu));
-        int oj = __ldg(perm + (e & 0xFFFFFFu));
         while (k < cnt) {
             const int kn = k + 32;
             const unsigned en = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
             const int4 pjn = __ldg(xq + (en & 0xFFFFFFu));
             const int tjn = __ldg(typ_s + (en & 0xFFFFFFu));
-            const int ojn = __ldg(perm + (en & 0xFFFFFFu));
             const unsigned m = e >> 24;
+            const int sj = e & 0xFFFFFFu;
             float gx = 0.f, gy = 0.f, gz = 0.f;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii)
-                if ((m >> ii) & 1u) {
-                    float fx = 0.f, fy = 0.f, fz = 0.f;
-                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rmax2, rr2, rl2, inv_h, h,
-                                    sf, sp, slj, fx, fy, fz, ev, ee, wc, wl);
-                    f[ii][0] += fx; f[ii][1] += fy; f[ii][2] += fz;
-                    gx -= fx; gy -= fy; gz -= fz;
-                }
-            long long* fj = facc + 3 * (size_t)oj;
-            atomicAdd((unsigned long long*)fj, (unsigned long long)__double2ll_rn((double)gx * PGK_FORCE_SCALE));
-            atomicAdd((unsigned long long*)fj + 1, (unsigned long long)__double2ll_rn((double)gy * PGK_FORCE_SCALE));
-            atomicAdd((unsigned long long*)fj + 2, (unsigned long long)__double2ll_rn((double)gz * PGK_FORCE_SCALE));
-            k = kn; e = en; pj = pjn; tj = tjn; oj = ojn;
+                if ((m >> ii) & 1u)
+                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rr2, rl2, inv_h, h, nsplm1,
+                                    sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl);
+            unsigned long long* fj = (unsigned long long*)fs0 + sj;
+            atomicAdd(fj, (unsigned long long)__double2ll_rn((double)gx * PGK_FORCE_SCALE));
+            atomicAdd(fj + fst, (unsigned long long)__double2ll_rn((double)gy * PGK_FORCE_SCALE));
+            atomicAdd(fj + 2 * fst, (unsigned long long)__double2ll_rn((double)gz * PGK_FORCE_SCALE));
+            k = kn; e = en; pj = pjn; tj = tjn;
         }
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
-            if (lane == ii) {
-                const int io = perm[8 * cl + ii];
-                if (io >= 0) force_add<true>(a.facc, io, (double)fx, (double)fy, (double)fz);
+            if (lane == ii) {     // padding slots get zero sums (no mask bits)
+                unsigned long long* fi = (unsigned long long*)fs0 + 8 * cl + ii;
+                atomicAdd(fi, (unsigned long long)__double2ll_rn((double)fx * PGK_FORCE_SCALE));
+                atomicAdd(fi + fst, (unsigned long long)__double2ll_rn((double)fy * PGK_FORCE_SCALE));
+                atomicAdd(fi + 2 * fst, (unsigned long long)__double2ll_rn((double)fz * PGK_FORCE_SCALE));
             }
         }
     }
@@ -354,12 +355,28 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
     }
 }
 
+// sorted-slot pair forces -> the group accumulator (one thread per slot: the
+// atom's only writer here), leaving the slot buffer zero for the next call
+__global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __restrict__ perm, int npad,
+                         long long* __restrict__ facc) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= npad) return;
+    const int i = perm[s];
+    const long long vx = fsort[s], vy = fsort[s + fst], vz = fsort[s + 2 * (size_t)fst];
+    if (i >= 0 && (vx | vy | vz)) {
+        facc[3 * (size_t)i] += vx; facc[3 * (size_t)i + 1] += vy; facc[3 * (size_t)i + 2] += vz;
+    }
+    if (vx | vy | vz) { fsort[s] = 0; fsort[s + fst] = 0; fsort[s + 2 * (size_t)fst] = 0; }
+}
+
 template <int MODE>
 static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
     smem_limit(k_pair_mixed<MODE>, sm);
     k_pair_mixed<MODE><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+    PGK_LAUNCHED(c);
+    k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
 }
 
 // vmode: PM_FORCE / PM_ENE / PM_TENS / PM_FULL (see above)
@@ -375,6 +392,7 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
     a.rmax2 = a.rr2 > a.rl2 ? a.rr2 : a.rl2;
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
+    a.fsort = c->fsort; a.fstride = c->npad_cap;
     const int warps_per_block = 8;
     int blocks = c->nsm * (c->mixed() ? 3 : 2);
     long long need = (c->ncl + warps_per_block - 1) / warps_per_block;

@@ -118,6 +118,7 @@ struct pgk_ctx {
     int* ccnt = nullptr;          // [ncl]
     int ccap = 0;
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
+    long long* fsort = nullptr;   // mixed: pair forces by sorted slot, [3][npad_cap] int64 fixed point (kept zero between uses)
     double4* xq64 = nullptr;      // fp64: x,y,z,q sorted
     int* typ_s = nullptr;
     unsigned long long* counters = nullptr;   // [0] list pairs, [1] longest cluster row, [2] rows without
