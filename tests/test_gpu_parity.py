@@ -324,3 +324,26 @@ def test_list_rebuild_inside_md_run(oracle_mod):
     ox, _, _ = o.get_state()
     gx, _, _ = e.download_state()
     assert np.abs(gx - ox).max() < 1e-9
+
+
+# ------------------------------------------------------- pruned pair list ---
+def test_mixed_pruned_list_keeps_every_pair(monkeypatch):
+    """The mixed pair kernel reads a pruned copy of the book list (pairs
+    inside cutoff + buffer, re-pruned when atoms have moved half the buffer).
+    With a thin buffer it re-prunes every few steps; after an MD run its
+    forces must equal those of an engine whose list was just built at the
+    same positions (every pair inside the cutoff present in both)."""
+    s = case("propanol_cells")
+    md = _md(s, kind="nve")
+    monkeypatch.setenv("PGK_PRUNE_BUFFER", "0.3")
+    e1 = engine(s, abi.PREC_MIXED)
+    e1.moldyn_nve(0, 40, md)
+    x, v, _ = e1.download_state()
+    f1, en1, _ = e1.calforce(abi.MTS_LONG)
+    monkeypatch.setenv("PGK_PRUNE_BUFFER", "0")
+    e2 = engine(s, abi.PREC_MIXED)
+    e2.upload_state(x, v)
+    e2.mklist_cell()
+    f2, en2, _ = e2.calforce(abi.MTS_LONG)
+    assert rel_rms(f1, f2) < 1e-6
+    assert erel(en1["pot_nonbon"], en2["pot_nonbon"]) < 1e-6

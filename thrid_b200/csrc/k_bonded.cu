@@ -240,7 +240,7 @@ __device__ __forceinline__ void eval_excl(const double* P, int i, int j, double 
         float hf = (float)h;
         int idx = (int)(rr / hf);
         float fs = 0.f, ps = 0.f;
-        if (idx < nspl - 1) {
+        if (rr == rr && idx >= 0 && idx < nspl - 1) {     // a non-finite distance reads no table
             float d = rr - (float)idx * hf;
             float4 c = spl32[2 * nspl + idx];
             fs = -(c.x + d * (c.y + d * (c.z + d * c.w))) * (float)qq;

@@ -359,9 +359,11 @@ static int list_mode_for(const pgk_ctx* c, const double* box, int* nc) {
 static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     if (npad_cap <= c->npad_cap) return PGK_OK;
     cudaFree(c->perm); cudaFree(c->pos_s); cudaFree(c->typ_s); cudaFree(c->xq); cudaFree(c->xq64);
-    cudaFree(c->ccnt); cudaFree(c->clist); cudaFree(c->fsort);
+    cudaFree(c->ccnt); cudaFree(c->clist); cudaFree(c->fsort); cudaFree(c->plist); cudaFree(c->pcnt);
+    cudaFree(c->xq_prune);
     c->perm = nullptr; c->pos_s = nullptr; c->typ_s = nullptr; c->xq = nullptr; c->xq64 = nullptr;
-    c->ccnt = nullptr; c->clist = nullptr; c->fsort = nullptr;
+    c->ccnt = nullptr; c->clist = nullptr; c->fsort = nullptr; c->plist = nullptr; c->pcnt = nullptr;
+    c->xq_prune = nullptr;
     int ncl = npad_cap / 8;
     PGK_CUDA(c, cudaMalloc(&c->perm, sizeof(int) * npad_cap));
     PGK_CUDA(c, cudaMalloc(&c->pos_s, sizeof(double) * 3 * npad_cap));
@@ -376,6 +378,15 @@ static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     if (cudaMalloc(&c->clist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {
         c->clist = nullptr;
         return pgk_fail(c, PGK_E_NOMEM, "cluster pair list exceeds device memory");
+    }
+    if (c->prune_buffer > 0.f) {
+        if (cudaMalloc(&c->plist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {
+            c->plist = nullptr;
+            return pgk_fail(c, PGK_E_NOMEM, "pruned pair list exceeds device memory");
+        }
+        PGK_CUDA(c, cudaMalloc(&c->pcnt, sizeof(int) * ncl));
+        PGK_CUDA(c, cudaMalloc(&c->xq_prune, sizeof(int4) * npad_cap));
+        PGK_CUDA(c, cudaMemsetAsync(c->xq_prune, 0, sizeof(int4) * npad_cap, c->st));
     }
     c->npad_cap = npad_cap;
     return PGK_OK;
@@ -459,6 +470,7 @@ pgk_status launch_mklist(pgk_ctx* c) {
                                     cudaMemcpyHostToDevice, c->st));
         c->list_valid = true;
         ++c->list_epoch;
+        if (c->prune_buffer > 0.f) PGK_CUDA(c, cudaMemsetAsync(&c->prune->force, 1, 1, c->st));   // re-prune
         return PGK_OK;
     }
     return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list overflow after regrowth");

@@ -24,6 +24,7 @@
 // Roofline: FP32 pipe (61 algorithmic flop per interacting pair) plus one
 // 4-byte entry, one 16-byte (32-byte FP64) position and one 4-byte type
 // gather per (cluster, j) entry.
+#include <cmath>
 #include <vector>
 
 #include "pgk_ctx.cuh"
@@ -31,19 +32,34 @@
 // ---- pack: sorted (padded) positions for the pair kernel ---------------------
 __global__ void k_pack_mixed(const double* __restrict__ pos, const double* __restrict__ chrg,
                              const int* __restrict__ perm, int npad, const DynState* __restrict__ dyn,
-                             int4* __restrict__ xq) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= npad) return;
-    int i = perm[s];
-    if (i < 0) { xq[s] = make_int4(0, 0, 0, 0); return; }
-    unsigned u[3];
+                             int4* __restrict__ xq, const int4* __restrict__ xq_prune, PruneDev* __restrict__ P) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = s < npad ? perm[s] : -1;
+    int4 v = make_int4(0, 0, 0, 0);
+    if (i >= 0) {
+        unsigned u[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double f = pos[3 * i + d] * dyn->boxinv[d];
-        f -= floor(f);
-        u[d] = (unsigned)(unsigned long long)(f * 4294967296.0);
+        for (int d = 0; d < 3; ++d) {
+            double f = pos[3 * i + d] * dyn->boxinv[d];
+            f -= floor(f);
+            u[d] = (unsigned)(unsigned long long)(f * 4294967296.0);
+        }
+        v = make_int4((int)u[0], (int)u[1], (int)u[2], __float_as_int((float)chrg[i]));
     }
-    xq[s] = make_int4((int)u[0], (int)u[1], (int)u[2], __float_as_int((float)chrg[i]));
+    if (s < npad) xq[s] = v;
+    if (P) {
+        // displacement since the last prune (minimum image, current box)
+        float dd = 0.f;
+        if (i >= 0) {
+            const int4 o = xq_prune[s];
+            const float dx = (float)(v.x - o.x) * (float)(dyn->box[0] * (1.0 / 4294967296.0));
+            const float dy = (float)(v.y - o.y) * (float)(dyn->box[1] * (1.0 / 4294967296.0));
+            const float dz = (float)(v.z - o.z) * (float)(dyn->box[2] * (1.0 / 4294967296.0));
+            dd = sqrtf(dx * dx + dy * dy + dz * dz);
+        }
+        const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(dd));
+        if ((threadIdx.x & 31) == 0 && m) atomicMax(&P->dmax, m);
+    }
 }
 
 __global__ void k_pack_fp64(const double* __restrict__ pos, const double* __restrict__ chrg,
@@ -58,7 +74,8 @@ pgk_status launch_pack(pgk_ctx* c) {
     int n = c->npad;
     if (n <= 0) return PGK_OK;
     if (c->mixed())
-        k_pack_mixed<<<(n + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->perm, n, c->dyn, c->xq);
+        k_pack_mixed<<<(n + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->perm, n, c->dyn, c->xq, c->xq_prune,
+                                                          c->prune_buffer > 0.f ? c->prune : nullptr);
     else
         k_pack_fp64<<<(n + 255) / 256, 256, 0, c->st>>>(c->pos, c->chrg, c->perm, n, c->xq64);
     PGK_LAUNCHED(c);
@@ -102,7 +119,7 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
     float fm = (tf + 8388608.0f) - 8388608.0f;
     fm = fm > tf ? fm - 1.0f : fm;
     int idx = __float_as_int(fm + 8388608.0f) - 0x4B000000;
-    idx = min(idx, nsplm1);
+    idx = (int)min((unsigned)idx, (unsigned)nsplm1);      // into the table whatever r is (NaN included)
     const float d = fmaf(-fm, h, r);
     const float4 c = sf[idx];
     const bool inr = r2 <= rr2, inl = r2 <= rl2;
@@ -355,6 +372,115 @@ __global__ void __launch_bounds__(256, 2) k_pair_fp64(const double4* __restrict_
     }
 }
 
+// ---- pruned list -------------------------------------------------------------
+// decision for this pair evaluation (one thread; see PruneDev)
+__global__ void k_prune_decide(PruneDev* __restrict__ P, const DynState* __restrict__ dyn, float buffer,
+                               float rprune) {
+    if (threadIdx.x || blockIdx.x) return;
+    const float dmax = __uint_as_float(P->dmax);
+    double bt = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) bt = fmax(bt, fabs(dyn->box[d] / P->box[d] - 1.0));
+    const bool keep = !P->force && (2.0 * (double)dmax + (double)rprune * bt < (double)buffer);   // NaN -> prune
+    P->do_prune = keep ? 0 : 1;
+    if (!keep) {
+        P->dmax = 0u;
+        P->force = 0;
+        for (int d = 0; d < 3; ++d) P->box[d] = dyn->box[d];
+        P->nprune += 1ull;
+    }
+}
+
+// Rows of the book list with the masks cut to the pairs inside rprune at the
+// current positions (entries left without pairs dropped), regrouped by mask
+// like the book rows; the cluster's slots record their positions as the new
+// displacement origin.  One warp per row; no-op unless a prune was decided.
+__global__ void __launch_bounds__(256) k_prune(const int4* __restrict__ xq, int4* __restrict__ xq_prune,
+                                               const int* __restrict__ clist, const int* __restrict__ ccnt,
+                                               int ccap, int ncl, int* __restrict__ plist, int* __restrict__ pcnt,
+                                               const PruneDev* __restrict__ P, const DynState* __restrict__ dyn,
+                                               float rp2, int sort_rows) {
+    if (!P->do_prune) return;
+    __shared__ int4 si[8][8];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (cl >= ncl) return;
+    const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
+    const float sy = (float)(dyn->box[1] * (1.0 / 4294967296.0));
+    const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
+    if (lane < 8) {
+        const int4 v = xq[8 * cl + lane];
+        si[wib][lane] = v;
+        xq_prune[8 * cl + lane] = v;
+    }
+    __syncwarp();
+    const int cnt = ccnt[cl];
+    const int* __restrict__ row = clist + (size_t)cl * ccap;
+    int* out = plist + (size_t)cl * ccap;
+    extern __shared__ int prow_raw[];
+    int* buf = sort_rows ? prow_raw + (size_t)wib * (ccap + 256) : out;
+    int count = 0;
+    unsigned e = lane < cnt ? (unsigned)row[lane] : 0u;
+    int4 pj = xq[e & 0xFFFFFFu];
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int kn = k0 + 32 + lane;          // next chunk's entry and j, loaded ahead
+        const unsigned en = kn < cnt ? (unsigned)row[kn] : 0u;
+        const int4 pjn = xq[en & 0xFFFFFFu];
+        const unsigned m = e >> 24;
+        unsigned nm = 0;
+        if (m) {
+            // per-pair minimum image from the wrapped fixed-point difference,
+            // exactly as the pair kernel forms it
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii) {
+                const int4 pi = si[wib][ii];
+                const float dx = (float)(pi.x - pj.x) * sx;
+                const float dy = (float)(pi.y - pj.y) * sy;
+                const float dz = (float)(pi.z - pj.z) * sz;
+                const bool in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rp2;
+                nm |= (in && ((m >> ii) & 1u)) ? 1u << ii : 0u;
+            }
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, nm != 0);
+        if (nm) buf[count + __popc(b & ((1u << lane) - 1u))] = (int)((nm << 24) | (e & 0xFFFFFFu));
+        count += __popc(b);
+        e = en; pj = pjn;
+    }
+    if (sort_rows) {          // stable counting sort by mask (as the book rows)
+        int* bin = buf + ccap;
+        for (int q = lane; q < 256; q += 32) bin[q] = 0;
+        __syncwarp();
+        for (int k0 = 0; k0 < count; k0 += 32) {
+            const int k = k0 + lane;
+            const unsigned key = k < count ? ((unsigned)buf[k] >> 24) : 256u + lane;
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int run = 0;
+            for (int q = 0; q < 256; ++q) { const int v = bin[q]; bin[q] = run; run += v; }
+        }
+        __syncwarp();
+        for (int k0 = 0; k0 < count; k0 += 32) {
+            const int k = k0 + lane;
+            const bool ok = k < count;
+            const int e = ok ? buf[k] : 0;
+            const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(grp & ((1u << lane) - 1u));
+            const int base = ok ? bin[key] : 0;
+            __syncwarp();
+            if (ok) {
+                out[base + rank] = e;
+                if (rank == 0) bin[key] = base + __popc(grp);
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) pcnt[cl] = count;
+}
+
 // sorted-slot pair forces -> the group accumulator (one thread per slot: the
 // atom's only writer here), leaving the slot buffer zero for the next call
 __global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __restrict__ perm, int npad,
@@ -393,6 +519,20 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
     a.fsort = c->fsort; a.fstride = c->npad_cap;
+    if (c->mixed() && c->prune_buffer > 0.f) {
+        const float rmax = (float)std::sqrt(a.rmax2);
+        const float rp = rmax + c->prune_buffer;
+        k_prune_decide<<<1, 32, 0, c->st>>>(c->prune, c->dyn, c->prune_buffer, rp);
+        const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
+        const int sort_rows = sort_sm <= 160 * 1024 ? 1 : 0;
+        if (sort_rows) smem_limit(k_prune, sort_sm);
+        const long long threads = (long long)c->ncl * 32;
+        k_prune<<<(unsigned)((threads + 255) / 256), 256, sort_rows ? sort_sm : 0, c->st>>>(
+            c->xq, c->xq_prune, c->clist, c->ccnt, c->ccap, c->ncl, c->plist, c->pcnt, c->prune, c->dyn, rp * rp,
+            sort_rows);
+        c->launches += 2;
+        a.clist = c->plist; a.ccnt = c->pcnt;
+    }
     const int warps_per_block = 8;
     int blocks = c->nsm * (c->mixed() ? 3 : 2);
     long long need = (c->ncl + warps_per_block - 1) / warps_per_block;

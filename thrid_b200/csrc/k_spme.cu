@@ -48,7 +48,7 @@ __device__ __forceinline__ void frac_coord(double x, double recip, int K, int& b
     double f = x * recip;
     f = f - floor(f);
     double fr = (double)K * f;
-    base = (int)fr;
+    base = min(max((int)fr, 0), K - 1);     // in range even for non-finite coordinates
     w = fr - trunc(fr);
 }
 

@@ -476,6 +476,18 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         cap = std::min(cap, ((n + 31) / 32) * 32);
         cap = ((cap + 31) / 32) * 32;
         c->ccap = std::max(cap, 32);
+        // pruned list buffer (mixed): PGK_PRUNE_BUFFER overrides the 1 A default; 0
+        // disables pruning, as does a book skin too thin for the buffer
+        if (c->mixed()) {
+            const char* pb = getenv("PGK_PRUNE_BUFFER");
+            const double buf = pb ? atof(pb) : 1.0;
+            const double rmax = std::max(p->rcut, p->rrcut);
+            c->prune_buffer = (buf > 0.0 && rmax + buf < p->rcut_book) ? (float)buf : 0.f;
+            if (cudaMalloc(&c->prune, sizeof(PruneDev)) || cudaMemset(c->prune, 0, sizeof(PruneDev))) {
+                pgk_free(c);
+                return PGK_E_NOMEM;
+            }
+        }
         if (cudaMalloc(&c->iperm, n * sizeof(int)) || cudaMalloc(&c->cell_of, n * sizeof(int)) ||
             cudaMalloc(&c->subkey, n * sizeof(int)) || cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)) ||
             cudaMalloc(&c->hasup, std::max(n, 1))) {
@@ -518,7 +530,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
-                    c->ccnt, c->xq, c->xq64, c->fsort, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
+                    c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,

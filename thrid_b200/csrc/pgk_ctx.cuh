@@ -116,6 +116,12 @@ struct pgk_ctx {
     double* pos_s = nullptr;      // sorted FP64 positions at list time (3*npad)
     int* clist = nullptr;         // [ncl * ccap] entries (mask << 24) | j-slot
     int* ccnt = nullptr;          // [ncl]
+    // pruned copy of the rows (mixed precision, see PruneDev)
+    int* plist = nullptr;         // [ncl * ccap]
+    int* pcnt = nullptr;          // [ncl]
+    int4* xq_prune = nullptr;     // xq at the last prune
+    PruneDev* prune = nullptr;
+    float prune_buffer = 0.f;     // A; 0 = no pruning (pair kernel reads the book rows)
     int ccap = 0;
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
     long long* fsort = nullptr;   // mixed: pair forces by sorted slot, [3][npad_cap] int64 fixed point (kept zero between uses)

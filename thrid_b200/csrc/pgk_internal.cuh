@@ -53,6 +53,22 @@ enum AccIdx {
 #define ST_RATTLEV_NOCONV  (1u << 4)
 #define ST_UNSUPPORTED     (1u << 5)
 
+// Pruned pair list state (mixed precision): the pair kernel reads a copy of
+// the book list whose masks keep only pairs inside rprune = cutoff + buffer
+// at the last prune.  dmax tracks the largest atom displacement since then
+// (float bits, atomicMax); the list is re-pruned before a pair evaluation
+// when 2*dmax plus the box-scaling term reaches the buffer, or when the book
+// list was rebuilt (force), so no pair of the book list that comes inside
+// the cutoff is ever missing from the pruned list.
+struct PruneDev {
+    unsigned dmax;
+    int force;
+    int do_prune;
+    int pad;
+    double box[3];                // box at the last prune
+    unsigned long long nprune;    // prunes done (diagnostic)
+};
+
 struct DynState {
     double box[3], boxinv[3];
     double rkcut;
