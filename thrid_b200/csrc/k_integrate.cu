@@ -94,9 +94,10 @@ __global__ void k_rattle_pos(double* __restrict__ pos, double* __restrict__ vel,
                              const double* __restrict__ invm, const int* __restrict__ gidx,
                              const int* __restrict__ glist, const int2* __restrict__ cij, const double* __restrict__ cd,
                              const int2* __restrict__ span, int ngroup, double eps, double dt, int use_rv,
-                             const DynState* __restrict__ dyn, unsigned* status) {
+                             const DynState* __restrict__ dyn, unsigned* status,
+                             const unsigned char* __restrict__ fit) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngroup) return;
+    if (g >= ngroup || (fit && fit[g >> 5])) return;      // staged groups run in k_rattle_warp
     int i1 = gidx[g], i2 = gidx[g + 1];
     double rvi[3] = {1.0, 1.0, 1.0};
     if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
@@ -163,9 +164,9 @@ __device__ __forceinline__ bool rattle_vel_sweeps(const double* X, double* V, co
 __global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict__ vel, const double* __restrict__ invm,
                              const int* __restrict__ gidx, const int* __restrict__ glist, const int2* __restrict__ cij,
                              const double* __restrict__ cd, const int2* __restrict__ span, int ngroup, double eps,
-                             unsigned* status) {
+                             unsigned* status, const unsigned char* __restrict__ fit) {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ngroup) return;
+    if (g >= ngroup || (fit && fit[g >> 5])) return;      // staged groups run in k_rattle_warp
     int i1 = gidx[g], i2 = gidx[g + 1];
     const int lo = span[g].x, na = span[g].y;
     bool finished;
@@ -496,21 +497,185 @@ pgk_status launch_drift(pgk_ctx* c, bool save_old) {
     return PGK_OK;
 }
 
+// Warp-staged RATTLE: the 32 groups of a warp (consecutive groups cover a
+// compact atom range) stage the union of their atom spans and their
+// constraints in shared memory with coalesced loads; each lane then runs its
+// group's sweeps (same arithmetic, same order as rattle_*_sweeps) from shared
+// memory and writes back its own atoms.  Warps whose union span or
+// constraint counts exceed the staging limits run the per-thread kernels.
+#define RATTLE_WSPAN 192          // atoms staged per warp
+#define RATTLE_WCON 8             // constraints per group
+#define RATTLE_WARPS 4
+
+struct RattleStage {
+    double x[3 * RATTLE_WSPAN], v[3 * RATTLE_WSPAN], o[3 * RATTLE_WSPAN], im[RATTLE_WSPAN];
+    int2 ij[32 * RATTLE_WCON];
+    double d2[32 * RATTLE_WCON];
+};
+
+template <bool POS>
+__global__ void __launch_bounds__(32 * RATTLE_WARPS) k_rattle_warp(double* __restrict__ pos, double* __restrict__ vel,
+                                                                  const double* __restrict__ old,
+                                                                  const double* __restrict__ invm,
+                                                                  const int* __restrict__ gidx,
+                                                                  const int* __restrict__ glist,
+                                                                  const int2* __restrict__ cij,
+                                                                  const double* __restrict__ cd,
+                                                                  const int2* __restrict__ span, int ngroup,
+                                                                  double eps, double dt, int use_rv,
+                                                                  const DynState* __restrict__ dyn,
+                                                                  unsigned* status,
+                                                                  const unsigned char* __restrict__ fit) {
+    extern __shared__ __align__(16) unsigned char rsm_raw[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gw = (blockIdx.x * RATTLE_WARPS + w) * 32;
+    if (gw >= ngroup || !fit[gw >> 5]) return;                  // warp-uniform; others: per-thread kernel
+    RattleStage& S = ((RattleStage*)rsm_raw)[w];
+    const int g = gw + lane;
+    const bool has = g < ngroup;
+    const int i1 = has ? gidx[g] : 0, i2 = has ? gidx[g + 1] : 0;
+    const int2 sp = has ? span[g] : make_int2(0x7fffffff, 0);
+    const int lo = __reduce_min_sync(0xffffffffu, has ? sp.x : 0x7fffffff);
+    const int hi = __reduce_max_sync(0xffffffffu, has ? sp.x + sp.y : 0);
+    const int nsp = hi - lo;                                    // <= RATTLE_WSPAN (fit)
+#pragma unroll 4
+    for (int k = lane; k < 3 * nsp; k += 32) {
+        S.x[k] = pos[3 * (size_t)lo + k];
+        S.v[k] = vel[3 * (size_t)lo + k];
+        if (POS) S.o[k] = old[3 * (size_t)lo + k];
+    }
+    for (int k = lane; k < nsp; k += 32) S.im[k] = invm[lo + k];
+    const int ncon = i2 - i1;
+    for (int q = 0; q < ncon; ++q) {
+        const int nc = glist[i1 + q];
+        const int2 p = cij[nc];
+        const double dij = cd[nc];
+        S.ij[lane * RATTLE_WCON + q] = make_int2(p.x - lo, p.y - lo);
+        S.d2[lane * RATTLE_WCON + q] = dij * dij;
+    }
+    __syncwarp();
+    double* X = S.x; double* V = S.v; const double* O = S.o; const double* IM = S.im;
+    const int2* C = S.ij + lane * RATTLE_WCON;
+    const double* D2 = S.d2 + lane * RATTLE_WCON;
+    bool finished = false;
+    if (POS) {
+        double rvi[3] = {1.0, 1.0, 1.0};
+        if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+            for (int q = 0; q < ncon; ++q) {
+                const int ib = C[q].x, jb = C[q].y;
+                const double d2 = D2[q];
+                double R0 = X[3 * ib] - X[3 * jb], R1 = X[3 * ib + 1] - X[3 * jb + 1], R2 = X[3 * ib + 2] - X[3 * jb + 2];
+                double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
+                double delta = fabs(Rsq - d2) / d2;
+                if (delta < eps) continue;
+                finished = false;
+                double O0 = O[3 * ib] - O[3 * jb], O1 = O[3 * ib + 1] - O[3 * jb + 1], O2 = O[3 * ib + 2] - O[3 * jb + 2];
+                double RR = R0 * O0 + R1 * O1 + R2 * O2;
+                double mi = IM[ib], mj = IM[jb];
+                double gij = (Rsq - d2) / (2.0 * RR * (mi + mj) * dt);
+                double G[3] = {gij * O0, gij * O1, gij * O2};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    X[3 * ib + d] = X[3 * ib + d] - mi * G[d] * dt;
+                    X[3 * jb + d] = X[3 * jb + d] + mj * G[d] * dt;
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double Gv = G[d] * rvi[d];
+                    V[3 * ib + d] = V[3 * ib + d] - mi * Gv;
+                    V[3 * jb + d] = V[3 * jb + d] + mj * Gv;
+                }
+            }
+        }
+    } else {
+        const double eps2 = eps * eps;
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+            for (int q = 0; q < ncon; ++q) {
+                const int ib = C[q].x, jb = C[q].y;
+                const double dd = D2[q];          // dij * dij
+                double R[3], W[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    R[d] = X[3 * ib + d] - X[3 * jb + d];
+                    W[d] = V[3 * ib + d] - V[3 * jb + d];
+                }
+                double RV = R[0] * W[0] + R[1] * W[1] + R[2] * W[2];
+                double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+                double V2 = W[0] * W[0] + W[1] * W[1] + W[2] * W[2];
+                double phi = RV * RV / R2 * V2;   // precedence as in the reference
+                if (phi < eps2) continue;
+                finished = false;
+                double mi = IM[ib], mj = IM[jb];
+                double kij = RV / (dd * (mi + mj));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double KR = kij * R[d];
+                    V[3 * ib + d] = V[3 * ib + d] - mi * KR;
+                    V[3 * jb + d] = V[3 * jb + d] + mj * KR;
+                }
+            }
+        }
+    }
+    if (has) {
+        for (int q = 0; q < ncon; ++q) {
+            const int ib = C[q].x, jb = C[q].y;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                if (POS) { pos[3 * ((size_t)lo + ib) + d] = X[3 * ib + d]; pos[3 * ((size_t)lo + jb) + d] = X[3 * jb + d]; }
+                vel[3 * ((size_t)lo + ib) + d] = V[3 * ib + d];
+                vel[3 * ((size_t)lo + jb) + d] = V[3 * jb + d];
+            }
+        }
+        if (!finished) atomicOr(status, POS ? ST_RATTLE_NOCONV : ST_RATTLEV_NOCONV);
+    }
+}
+
+static void rattle_warp_launch(pgk_ctx* c, bool pos, double eps, double dt, bool use_rv) {
+    const int nwarp = (c->ncgroup + 31) / 32;
+    const int blocks = (nwarp + RATTLE_WARPS - 1) / RATTLE_WARPS;
+    const size_t sm = RATTLE_WARPS * sizeof(RattleStage);
+    if (pos) {
+        smem_limit(k_rattle_warp<true>, sm);
+        k_rattle_warp<true><<<blocks, 32 * RATTLE_WARPS, sm, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass,
+                                                                     c->cg_idx, c->cg_list, c->c_ij, c->c_d,
+                                                                     c->cg_span, c->ncgroup, eps, dt, use_rv ? 1 : 0,
+                                                                     c->dyn, c->status, c->cg_fit);
+    } else {
+        smem_limit(k_rattle_warp<false>, sm);
+        k_rattle_warp<false><<<blocks, 32 * RATTLE_WARPS, sm, c->st>>>(c->pos, c->vel, nullptr, c->invmass,
+                                                                      c->cg_idx, c->cg_list, c->c_ij, c->c_d,
+                                                                      c->cg_span, c->ncgroup, eps, 0.0, 0, c->dyn,
+                                                                      c->status, c->cg_fit);
+    }
+    PGK_LAUNCHED(c);
+}
+
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
     if (c->ncgroup == 0) return PGK_OK;
-    k_rattle_pos<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->cg_idx,
-                                                           c->cg_list, c->c_ij, c->c_d, c->cg_span, c->ncgroup, eps,
-                                                           dt, use_rv ? 1 : 0, c->dyn, c->status);
-    PGK_LAUNCHED(c);
+    if (c->cg_nfit > 0) rattle_warp_launch(c, true, eps, dt, use_rv);
+    if (c->cg_nfit < (c->ncgroup + 31) / 32) {
+        k_rattle_pos<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->cg_idx,
+                                                               c->cg_list, c->c_ij, c->c_d, c->cg_span, c->ncgroup,
+                                                               eps, dt, use_rv ? 1 : 0, c->dyn, c->status,
+                                                               c->cg_nfit > 0 ? c->cg_fit : nullptr);
+        PGK_LAUNCHED(c);
+    }
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
 
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
     if (c->ncgroup == 0) return PGK_OK;
-    k_rattle_vel<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->invmass, c->cg_idx, c->cg_list, c->c_ij,
-                                                           c->c_d, c->cg_span, c->ncgroup, eps, c->status);
-    PGK_LAUNCHED(c);
+    if (c->cg_nfit > 0) rattle_warp_launch(c, false, eps, 0.0, false);
+    if (c->cg_nfit < (c->ncgroup + 31) / 32) {
+        k_rattle_vel<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->invmass, c->cg_idx, c->cg_list,
+                                                               c->c_ij, c->c_d, c->cg_span, c->ncgroup, eps, c->status,
+                                                               c->cg_nfit > 0 ? c->cg_fit : nullptr);
+        PGK_LAUNCHED(c);
+    }
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }

@@ -461,6 +461,23 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
             TRY(upload(c, &c->cg_idx, gi)); TRY(upload(c, &c->cg_list, gl));
             TRY(upload(c, &c->c_ij, cij)); TRY(upload(c, &c->c_d, cd));
             TRY(upload(c, &c->cg_span, span));
+            // warps of 32 consecutive groups whose atoms and constraints fit the
+            // shared-memory staging of k_rattle_warp (192 atoms, 8 constraints per group)
+            const int nw = (c->ncgroup + 31) / 32;
+            std::vector<unsigned char> fit(nw, 0);
+            c->cg_nfit = 0;
+            for (int w = 0; w < nw; ++w) {
+                int lo = INT32_MAX, hi = 0;
+                bool ok = true;
+                for (int g = 32 * w; g < std::min(c->ncgroup, 32 * w + 32); ++g) {
+                    lo = std::min(lo, span[g].x);
+                    hi = std::max(hi, span[g].x + span[g].y);
+                    ok = ok && gi[g + 1] - gi[g] <= 8;
+                }
+                fit[w] = (ok && hi - lo <= 192) ? 1 : 0;
+                c->cg_nfit += fit[w];
+            }
+            TRY(upload(c, &c->cg_fit, fit));
         }
     }
     // ---- pair list buffers (sorted slots and cluster rows grow at list time) ----
@@ -531,7 +548,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
                     c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
-                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
+                    c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->cg_fit, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};

@@ -101,6 +101,8 @@ struct pgk_ctx {
     int *cg_idx = nullptr, *cg_list = nullptr;
     int2* c_ij = nullptr; double* c_d = nullptr;
     int2* cg_span = nullptr;      // (first atom, atom count) of each group's contiguous span
+    unsigned char* cg_fit = nullptr;   // per 32 groups: 1 = staged in shared memory (k_rattle_warp)
+    int cg_nfit = 0;
 
     // ---- pair list ----
     int maxcells = 0;
