@@ -262,26 +262,27 @@ __device__ __forceinline__ void fft_stage(const T2* __restrict__ src, T2* __rest
 // all stages; NC > 0 makes the length and radix chain compile-time constants
 template <typename T, typename T2, int NC, int S = 0>
 struct FftStages {
-    static __device__ __forceinline__ void run(T2*& src, T2*& dst, int P, int n, const FftDev& plan, T sg) {
+    static __device__ __forceinline__ void run(T2*& src, T2*& dst, int P, int n, const FftDev& plan, T sg,
+                                               const T2* tw) {
         if (NC == 0) {
             int Ns = 1;
             for (int s = 0; s < plan.nstage; ++s) {
-                fft_stage<T, T2>(src, dst, P, n, plan.radix[s], Ns, (const T2*)plan.tw, sg);
+                fft_stage<T, T2>(src, dst, P, n, plan.radix[s], Ns, tw, sg);
                 __syncthreads();
                 T2* t = src; src = dst; dst = t;
                 Ns *= plan.radix[s];
             }
         } else if (S < nstages(NC)) {
-            fft_stage<T, T2>(src, dst, P, NC, stage_radix(NC, S), stage_ns(NC, S), (const T2*)plan.tw, sg);
+            fft_stage<T, T2>(src, dst, P, NC, stage_radix(NC, S), stage_ns(NC, S), tw, sg);
             __syncthreads();
             T2* t = src; src = dst; dst = t;
-            FftStages<T, T2, NC, (S < 12 ? S + 1 : S)>::run(src, dst, P, n, plan, sg);
+            FftStages<T, T2, NC, (S < 12 ? S + 1 : S)>::run(src, dst, P, n, plan, sg, tw);
         }
     }
 };
 template <typename T, typename T2, int NC>
 struct FftStages<T, T2, NC, 12> {
-    static __device__ __forceinline__ void run(T2*&, T2*&, int, int, const FftDev&, T) {}
+    static __device__ __forceinline__ void run(T2*&, T2*&, int, int, const FftDev&, T, const T2*) {}
 };
 
 // influence function of one grid point (scalar_sum, fft_pme.F90:590-680)
@@ -341,6 +342,8 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
     const int n = NC > 0 ? NC : plan.n;
     const int ld = n + 1;                 // padded pencil pitch (bank-conflict free strided access)
     T2* bufB = bufA + P * ld;
+    T2* tws = bufB + P * ld;              // twiddle table (n entries) staged in shared memory
+    for (int k = threadIdx.x; k < n; k += blockDim.x) tws[k] = ((const T2*)plan.tw)[k];
     size_t base;
     size_t stride;
     int yz = 0;
@@ -362,25 +365,43 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
     const int tot = P * n;
     const int npen_total = AXIS == 0 ? K2 * K3 : K1;
     const int x0 = AXIS == 0 ? 0 : (int)(base % K1);
-    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    // load: each thread issues its first FFT_LQ loads before any shared store
+    // (one memory latency per block instead of one per element)
+    auto load_one = [&](int idx, T2& v) {
         int p, m;
         if (AXIS == 0) { p = idx / n; m = idx - p * n; } else { m = idx / P; p = idx - m * P; }
-        int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
-        T2 v;
+        const int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
         v.x = 0; v.y = 0;
-        bool ok = pg < npen_total;
-        if (ok) {
-            size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
+        if (pg < npen_total) {
+            const size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
             if (SRC == 0) v = data[off];
             else if (SRC == 1) v.x = (T)((double)((const long long*)acc)[off] * PGK_GRID_ISCALE);
             else v.x = (T)((const double*)acc)[off];
         }
-        bufA[p * ld + m] = v;
+        return p * ld + m;
+    };
+    {
+        constexpr int FFT_LQ = 8;
+        T2 rv[FFT_LQ];
+        int ri[FFT_LQ];
+#pragma unroll
+        for (int q = 0; q < FFT_LQ; ++q) {
+            const int idx = threadIdx.x + q * blockDim.x;
+            ri[q] = idx < tot ? load_one(idx, rv[q]) : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < FFT_LQ; ++q)
+            if (ri[q] >= 0) bufA[ri[q]] = rv[q];
+        for (int idx = threadIdx.x + FFT_LQ * blockDim.x; idx < tot; idx += blockDim.x) {
+            T2 v;
+            const int si = load_one(idx, v);
+            bufA[si] = v;
+        }
     }
     __syncthreads();
     T2* src = bufA;
     T2* dst = bufB;
-    FftStages<T, T2, NC>::run(src, dst, P, n, plan, sg);
+    FftStages<T, T2, NC>::run(src, dst, P, n, plan, sg, tws);
     if (CONV) {
         double en = 0, vs = 0, vt[6] = {0, 0, 0, 0, 0, 0};
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
@@ -397,7 +418,7 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
             src[sidx] = v;
         }
         __syncthreads();
-        FftStages<T, T2, NC>::run(src, dst, P, n, plan, -sg);
+        FftStages<T, T2, NC>::run(src, dst, P, n, plan, -sg, tws);
         if (ca.want) {
             double out[9] = {0.5 * en, 0.5 * en + 0.5 * vs, 0.5 * vs,
                              -0.5 * vt[0], -0.5 * vt[1], -0.5 * vt[2], -0.5 * vt[3], -0.5 * vt[4], -0.5 * vt[5]};
@@ -699,7 +720,7 @@ static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) 
     if (AXIS == 0) grid = (K2 * K3 + P - 1) / P;
     else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3;
     else grid = ((K1 + P - 1) / P) * K2;
-    size_t sm = (size_t)2 * P * (pl.n + 1) * sizeof(T2);
+    size_t sm = ((size_t)2 * P * (pl.n + 1) + pl.n) * sizeof(T2);   // two pencil buffers + twiddles
     ConvArgs ca{};
     if (cap) ca = *cap;
     switch (pl.n) {   // compile-time lengths of the configured grids; others run the generic stage loop
@@ -896,7 +917,7 @@ static cudaError_t noalloc_fft_pass(unsigned char* base, const FftPlan& pl, int 
     int P = 8;
     if (AXIS == 0) P = std::max(1, 1024 / K1);
     int grid = AXIS == 0 ? (K2 * K3 + P - 1) / P : ((K1 + P - 1) / P) * (AXIS == 1 ? K3 : K2);
-    size_t sm = (size_t)2 * P * (pl.n + 1) * sizeof(double2);
+    size_t sm = ((size_t)2 * P * (pl.n + 1) + pl.n) * sizeof(double2);   // two pencil buffers + twiddles
     cudaError_t e = smem_limit(k_fft<double, AXIS, SRC, 0, false>, sm);
     if (e != cudaSuccess) return e;
     ConvArgs ca{};
