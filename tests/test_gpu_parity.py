@@ -316,6 +316,22 @@ def test_mixed_md_tracks_fp64(oracle_mod):
     assert erel(ge["pot_tot"], oe["pot_tot"]) < 1e-4 * max(1.0, abs(oe["pot_tot"]))
 
 
+def test_mixed_mtk_aniso_tracks_fp64(oracle_mod):
+    """Anisotropic MTK in mixed precision: the steps without output read only
+    the total virial tensor (tensor-only pair and bonded kernels); the
+    pressure tensor, box and positions track the FP64 oracle."""
+    s = case("propanol_small")
+    md = _md(s, kind="mtk", pext_pa=1.0e5, axis=abi.PCONT_ANISO)
+    o, e, oe, ge = _run_pair(oracle_mod, s, "mtk", md, 6, prec=abi.PREC_MIXED)
+    ox, _, ob = o.get_state()
+    gx, _, gb = e.download_state()
+    assert np.abs(gx - ox).max() < 1e-4
+    assert np.abs(gb - ob).max() < 1e-6 * np.abs(ob).max()
+    oc, gc = o.get_chain(), e.get_chain()
+    op, gp = np.array(oc.pintt[:]), np.array(gc.pintt[:])
+    assert np.abs(gp - op).max() < 1e-4 * np.abs(op).max()
+
+
 def test_list_rebuild_inside_md_run(oracle_mod):
     s = case("water")
     md = _md(s, kind="nve")

@@ -221,6 +221,99 @@ __device__ __forceinline__ void eval_14(const double* P, int i, int j, double qq
     dv_out = (double)dv;
 }
 
+// ---- mixed-precision force-and-tensor forms (tensor-only steps) ---------------
+// Same forces as eval_angl / eval_tors in FP32 without the energy: no inverse
+// trigonometry in the torsion (the force factor is a polynomial in cos phi,
+// sin^2 phi = 1 - cos^2 phi), sin(theta) = sqrt(1 - cos^2 theta) in the angle,
+// reciprocals instead of divisions.  The caller forms the virial from lever
+// arms relative to the term's first atom (the term forces sum to zero), so the
+// FP32 tensor sums do not cancel absolute coordinates.
+__device__ __forceinline__ void angl_force_f(const double* P, int i, int j, int k, double2 p,
+                                             const DynState* dyn, float (&F)[3][3], float (&arm)[3][3]) {
+    float rij[3], rkj[3];
+    disp<float>(P, j, i, dyn, rij);
+    disp<float>(P, j, k, dyn, rkj);
+    const float ia = rsqrtf(dt3(rij, rij)), ib = rsqrtf(dt3(rkj, rkj));
+    float c = dt3(rij, rkj) * ia * ib;
+    c = fminf(fmaxf(c, -1.f), 1.f);
+    const float th = acosf(c);
+    const float s = sqrtf(fmaxf(1.f - c * c, 0.f));
+    const float dth = th - (float)p.y;
+    float fi[3] = {0, 0, 0}, fk[3] = {0, 0, 0};
+    if (s > 1.0e-7f) {
+        const float ft = -2.f * (float)p.x * dth / s;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            fi[d] = ft * ((rkj[d] * ib - rij[d] * c * ia) * ia);
+            fk[d] = ft * ((rij[d] * ia - rkj[d] * c * ib) * ib);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        F[0][d] = fi[d]; F[1][d] = -fi[d] - fk[d]; F[2][d] = fk[d];
+        arm[0][d] = 0.f; arm[1][d] = rij[d]; arm[2][d] = rij[d] - rkj[d];   // x_q - x_i
+    }
+}
+
+template <bool RB>
+__device__ __forceinline__ void tors_force_f(const double* P, int i, int j, int k, int l, double4 p,
+                                             const double* __restrict__ C, const DynState* dyn, float (&F)[4][3],
+                                             float (&arm)[4][3], unsigned* status) {
+    float rij[3], rkj[3], rkl[3];
+    disp<float>(P, j, i, dyn, rij); disp<float>(P, j, k, dyn, rkj); disp<float>(P, l, k, dyn, rkl);
+    float rik[3], rjl[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { rik[d] = rij[d] - rkj[d]; rjl[d] = rkl[d] - rkj[d]; }
+    float ni[3], nl[3];
+    crs(rij, rkj, ni);
+    crs(rkj, rkl, nl);
+    const float iai = rsqrtf(dt3(ni, ni)), ial = rsqrtf(dt3(nl, nl));
+    float c = dt3(ni, nl) * iai * ial;
+    c = fminf(fmaxf(c, -1.f), 1.f);
+    float b[3], cc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float a = ni[d] * iai, e = nl[d] * ial;
+        b[d] = (e - c * a) * iai;
+        cc[d] = (a - c * e) * ial;
+    }
+    float fa;
+    if (RB) {
+        const float bt[6] = {(float)C[0], -(float)C[1], (float)C[2], -(float)C[3], (float)C[4], -(float)C[5]};
+        float dp = bt[5];
+        fa = 0.f;
+#pragma unroll
+        for (int q = 4; q >= 0; --q) { fa = fa * c + dp; dp = dp * c + bt[q]; }
+        fa = -fa;
+    } else {
+        const int np = (int)lround(p.z);
+        if (np == 1) fa = 1.f;
+        else if (np == 2) fa = 2.f * c;
+        else if (np == 3) fa = 4.f * c * c - 1.f;          // -4 sin^2 + 3
+        else if (np == 4) fa = 4.f * c * (2.f * c * c - 1.f);
+        else if (np == 5) { fa = 4.f * c * c; fa = fa * (fa - 3.f) + 1.f; }
+        else if (np == 6) { fa = 4.f * c * c; fa = 2.f * c * (fa - 3.f) * (fa - 1.f); }
+        else { fa = 0.f; atomicOr(status, ST_UNSUPPORTED); }
+        fa = -fa * (float)p.w * (float)p.x * (float)p.z;
+    }
+    float t1[3], t2[3];
+    crs(b, rkj, t1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[0][d] = fa * t1[d];
+    crs(cc, rkl, t1); crs(b, rik, t2);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[1][d] = fa * (-t1[d] + t2[d]);
+    crs(b, rij, t1); crs(cc, rjl, t2);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) F[2][d] = fa * (-t1[d] + t2[d]);
+    crs(cc, rkj, t1);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        F[3][d] = fa * t1[d];
+        arm[0][d] = 0.f; arm[1][d] = rij[d]; arm[2][d] = rik[d]; arm[3][d] = rik[d] + rkl[d];   // x_q - x_i
+    }
+}
+
 // excluded-pair erf correction: spline tables 2 (force) and 3 (potential)
 template <bool MIXED>
 __device__ __forceinline__ void eval_excl(const double* P, int i, int j, double qq, const double4* __restrict__ spl64,
@@ -458,11 +551,22 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         SX[sl] = (T)(sg * F[0]); SY[sl] = (T)(sg * F[1]); SZ[sl] = (T)(sg * F[2]);
     };
     double tv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};               // TENS: total tensor (a + 3b)
+    float tvf[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};               // mixed TENS: FP32 sums of lever-arm terms
+    constexpr bool FAST = MIXED && TENS;
     auto tens_pair = [&](const double* F, const double* r) {
 #pragma unroll
         for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
-            for (int aa = 0; aa < 3; ++aa) tv[aa + 3 * bb] += F[aa] * r[bb];
+            for (int aa = 0; aa < 3; ++aa) {
+                if (FAST) tvf[aa + 3 * bb] = fmaf((float)F[aa], (float)r[bb], tvf[aa + 3 * bb]);
+                else tv[aa + 3 * bb] += F[aa] * r[bb];
+            }
+    };
+    auto tens_arm = [&](const float* F, const float* r) {
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+            for (int aa = 0; aa < 3; ++aa) tvf[aa + 3 * bb] = fmaf(F[aa], r[bb], tvf[aa + 3 * bb]);
     };
     auto tens_abs = [&](const double* F, int l) {
 #pragma unroll
@@ -494,11 +598,23 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         int t0, t1; range(1, t0, t1);
         double v[11] = {0};
         for (int k = t0 + tid; k < t1; k += nt) {
-            double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
             const int4 q4 = D.angl_ijk[k];
             const int at[3] = {q4.x - a0, q4.y - a0, q4.z - a0};
-            const bool on = eval_angl<T>(P, at[0], at[1], at[2], D.angl_p[k], dyn, F, e);
             const int sl = so[1] + 3 * (k - t0);
+            if (FAST) {
+                const double2 pp = D.angl_p[k];
+                float Ff[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, arm[3][3];
+                if (fabs(pp.x) >= 1.0e-32) {
+                    angl_force_f(P, at[0], at[1], at[2], pp, dyn, Ff, arm);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) tens_arm(Ff[q], arm[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 3; ++q) { SX[sl + q] = Ff[q][0]; SY[sl + q] = Ff[q][1]; SZ[sl + q] = Ff[q][2]; }
+                continue;
+            }
+            double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
+            const bool on = eval_angl<T>(P, at[0], at[1], at[2], D.angl_p[k], dyn, F, e);
 #pragma unroll
             for (int q = 0; q < 3; ++q) put(sl + q, F[q], 1.0);
             if (TENS && on) {
@@ -526,6 +642,19 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         for (int k = t0 + tid; k < t1; k += nt) {
             const int4 q4 = rb ? D.rb_ijkl[k] : D.tors_ijkl[k];
             const int at[4] = {q4.x - a0, q4.y - a0, q4.z - a0, q4.w - a0};
+            if (FAST) {
+                float Ff[4][3], arm[4][3];
+                if (rb) tors_force_f<true>(P, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0),
+                                           D.rb_c + 6 * (size_t)k, dyn, Ff, arm, status);
+                else tors_force_f<false>(P, at[0], at[1], at[2], at[3], D.tors_p[k], nullptr, dyn, Ff, arm, status);
+                const int slf = so[2 + rb] + 4 * (k - t0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    tens_arm(Ff[q], arm[q]);
+                    SX[slf + q] = Ff[q][0]; SY[slf + q] = Ff[q][1]; SZ[slf + q] = Ff[q][2];
+                }
+                continue;
+            }
             double F[4][3], e;
             if (rb) eval_tors<T, true>(P, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0), D.rb_c + 6 * (size_t)k,
                                        dyn, F, e, status);
@@ -593,6 +722,10 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     if (TENS && want) {
         const int idx[9] = {A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5, A_VTB + 6, A_VTB + 7,
                             A_VTB + 8};
+        if (FAST) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) tv[q] = (double)tvf[q];
+        }
         block_acc<9>(tv, acc, idx, !MIXED);
     }
     __syncthreads();
