@@ -181,11 +181,13 @@ __device__ __forceinline__ bool is_excluded(const int* __restrict__ exs_idx, con
 __global__ void __launch_bounds__(256) k_build_clist(
         const double* __restrict__ pos_s, const int* __restrict__ perm, const int* __restrict__ cell_of,
         const int* __restrict__ cell_start, const int* __restrict__ cell_cnt, const int* __restrict__ exs_idx,
-        const int* __restrict__ exs_list, int n, int ncl, int ccap, int sort_rows, double sqcut, double rbox,
+        const int* __restrict__ exs_list, const int2* __restrict__ exs_rng, int n, int ncl, int ccap, int sort_rows,
+        double sqcut, double rbox,
         const DynState* __restrict__ dyn, int* __restrict__ clist, int* __restrict__ ccnt,
         unsigned char* __restrict__ hasup, unsigned long long* __restrict__ counters, unsigned* __restrict__ status) {
     __shared__ double spi[8][3 * 8];
     __shared__ int sio[8][8];
+    __shared__ int2 srng[8][8];
     const int wib = threadIdx.x >> 5;
     const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
     if (lane < 8) {
         int io = perm[s0 + lane];
         sio[wib][lane] = io;
+        srng[wib][lane] = io >= 0 ? exs_rng[io] : make_int2(INT_MAX, -1);
         spi[wib][3 * lane] = pos_s[3 * (s0 + lane)];
         spi[wib][3 * lane + 1] = pos_s[3 * (s0 + lane) + 1];
         spi[wib][3 * lane + 2] = pos_s[3 * (s0 + lane) + 2];
@@ -261,7 +264,9 @@ __global__ void __launch_bounds__(256) k_build_clist(
                                 double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
                                 double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)),
                                                       __dmul_rn(r2, r2));
-                                if (dr < sqcut && !is_excluded(exs_idx, exs_list, io, jo)) {
+                                const int2 rg = srng[wib][ii];
+                                if (dr < sqcut &&
+                                    !(jo >= rg.x && jo <= rg.y && is_excluded(exs_idx, exs_list, io, jo))) {
                                     mask |= 1u << ii;
                                     if (jo > io) up |= 1u << ii;
                                     else jlow = true;
@@ -442,7 +447,8 @@ pgk_status launch_mklist(pgk_ctx* c) {
         const int sort_rows = sort_sm <= 160 * 1024 ? 1 : 0;
         if (sort_rows) PGK_CUDA(c, smem_limit(k_build_clist, sort_sm));
         k_build_clist<<<(unsigned)((threads + 255) / 256), 256, sort_rows ? sort_sm : 0, c->st>>>(
-            c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, n, c->ncl, c->ccap,
+            c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, c->exs_rng, n, c->ncl,
+            c->ccap,
             sort_rows, sq, c->prm.rcut_book + 0.05, c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
         if (n > 1) k_count_noup<<<(n - 1 + 255) / 256, 256, 0, c->st>>>(c->hasup, n - 1, c->counters);
         c->launches += 7;

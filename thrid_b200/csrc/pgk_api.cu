@@ -338,9 +338,15 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
             c->max_excl = std::max(c->max_excl, (int)part[i].size());
         }
         idx[n] = (int)lst.size();
+        // (lowest, highest) partner of each atom: the list builder looks a pair
+        // up only when j falls inside its atom's range
+        std::vector<int2> rng(n);
+        for (int i = 0; i < n; ++i)
+            rng[i] = part[i].empty() ? make_int2(INT32_MAX, -1) : make_int2(part[i].front(), part[i].back());
         if (lst.empty()) lst.push_back(-1);
         TRY(upload(c, &c->exs_idx, idx));
         TRY(upload(c, &c->exs_list, lst));
+        TRY(upload(c, &c->exs_rng, rng));
         ht.ex = pairs;
     }
     // ---- molecules ----
@@ -543,7 +549,7 @@ pgk_status pgk_free(pgk_ctx* c) {
     if (c->st) cudaStreamSynchronize(c->st);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
-                    c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list,
+                    c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list, c->exs_rng,
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,

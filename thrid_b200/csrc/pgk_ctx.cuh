@@ -66,6 +66,7 @@ struct pgk_ctx {
 
     // ---- exclusions ----
     int *exs_idx = nullptr, *exs_list = nullptr;   // symmetric, 0-based, sorted
+    int2* exs_rng = nullptr;                        // per atom: (lowest, highest) partner
     int2* expair = nullptr; int nexpair = 0;        // reference pairs i<j
     int max_excl = 0;
 
