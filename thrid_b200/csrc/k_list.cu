@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
         const double* __restrict__ pos_s, const int* __restrict__ perm, const int* __restrict__ cell_of,
         const int* __restrict__ cell_start, const int* __restrict__ cell_cnt, const int* __restrict__ exs_idx,
         const int* __restrict__ exs_list, const int2* __restrict__ exs_rng, int n, int ncl, int ccap, int sort_rows,
-        double sqcut, double rbox,
+        double sqcut, double rbox, float sqlo, float sqhi,
         const DynState* __restrict__ dyn, int* __restrict__ clist, int* __restrict__ ccnt,
         unsigned char* __restrict__ hasup, unsigned long long* __restrict__ counters, unsigned* __restrict__ status) {
     __shared__ double spi[8][3 * 8];
@@ -221,6 +221,14 @@ __global__ void __launch_bounds__(256) k_build_clist(
         hw[d] = 0.5 * (hi - lo);
     }
     const double rb2 = rbox * rbox;
+    // FP32 copies for the screening tests: a pair whose FP32 squared distance
+    // is below sqlo (above sqhi) is inside (outside) rcut_book whatever the
+    // rounding; only pairs between the two take the exact FP64 test
+    const float Lf[3] = {(float)L[0], (float)L[1], (float)L[2]};
+    const float Bf[3] = {(float)B[0], (float)B[1], (float)B[2]};
+    const float ctrf[3] = {(float)ctr[0], (float)ctr[1], (float)ctr[2]};
+    const float hwf[3] = {(float)hw[0], (float)hw[1], (float)hw[2]};
+    const float rb2f = (float)rb2 * 1.0001f + 1.0e-3f;
     const int key = cell_of[sio[wib][0]];
     const int cx = key % nc0, cy = (key / nc0) % nc1, cz = key / (nc0 * nc1);
     const int nz = nc2 >= 3 ? 3 : nc2, ny = nc1 >= 3 ? 3 : nc1, nx = nc0 >= 3 ? 3 : nc0;
@@ -243,29 +251,41 @@ __global__ void __launch_bounds__(256) k_build_clist(
                     unsigned mask = 0;
                     if (t < t1) {
                         const double xj = pos_s[3 * t], yj = pos_s[3 * t + 1], zj = pos_s[3 * t + 2];
-                        const double pj[3] = {xj, yj, zj};
-                        double e2 = 0.0;
+                        const float pjf[3] = {(float)xj, (float)yj, (float)zj};
+                        float e2 = 0.f;
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
-                            double r = pj[d] - ctr[d];
-                            r -= L[d] * rint(r * B[d]);
-                            double ex = fmax(fabs(r) - hw[d], 0.0);
+                            float r = pjf[d] - ctrf[d];
+                            r -= Lf[d] * rintf(r * Bf[d]);
+                            const float ex = fmaxf(fabsf(r) - hwf[d], 0.f);
                             e2 += ex * ex;
                         }
-                        if (e2 <= rb2) {
+                        if (e2 <= rb2f) {
                             const int jo = perm[t];
                             bool jlow = false;
 #pragma unroll
                             for (int ii = 0; ii < 8; ++ii) {
                                 const int io = sio[wib][ii];
                                 if (io < 0 || t <= s0 + ii) continue;
-                                double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L[0], B[0]);
-                                double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L[1], B[1]);
-                                double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
-                                double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)),
-                                                      __dmul_rn(r2, r2));
+                                float q2 = 0.f;
+#pragma unroll
+                                for (int d = 0; d < 3; ++d) {
+                                    float r = (float)spi[wib][3 * ii + d] - pjf[d];
+                                    r -= Lf[d] * rintf(r * Bf[d]);
+                                    q2 = fmaf(r, r, q2);
+                                }
+                                if (q2 > sqhi) continue;
+                                bool in = q2 < sqlo;
+                                if (!in) {       // near rcut_book: the reference's exact FP64 test decides
+                                    double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L[0], B[0]);
+                                    double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L[1], B[1]);
+                                    double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
+                                    double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)),
+                                                          __dmul_rn(r2, r2));
+                                    in = dr < sqcut;
+                                }
                                 const int2 rg = srng[wib][ii];
-                                if (dr < sqcut &&
+                                if (in &&
                                     !(jo >= rg.x && jo <= rg.y && is_excluded(exs_idx, exs_list, io, jo))) {
                                     mask |= 1u << ii;
                                     if (jo > io) up |= 1u << ii;
@@ -440,6 +460,11 @@ pgk_status launch_mklist(pgk_ctx* c) {
         k_sorted_gather<<<(npad + 255) / 256, 256, 0, c->st>>>(c->perm, npad, c->pos, c->typ, c->iperm, c->pos_s,
                                                                c->typ_s);
         double sq = c->prm.rcut_book * c->prm.rcut_book;
+        // screening margin on r^2: FP32 coordinates (up to twice the box) carry
+        // 2^-24 relative error each, a distance component up to 4x that
+        const double lmax = std::max(h.box[0], std::max(h.box[1], h.box[2]));
+        const double eps_pos = 4.0 * 5.96e-8 * 2.0 * lmax;
+        const double scr = std::max(0.01, 2.0 * 2.0 * c->prm.rcut_book * 1.7321 * eps_pos + 1.0e-3);
         long long threads = (long long)c->ncl * 32;
         PGK_CUDA(c, cudaMemsetAsync(c->hasup, 0, (size_t)n, c->st));
         // rows are grouped by mask in shared memory when 8 rows fit (<= 160 KB)
@@ -449,7 +474,8 @@ pgk_status launch_mklist(pgk_ctx* c) {
         k_build_clist<<<(unsigned)((threads + 255) / 256), 256, sort_rows ? sort_sm : 0, c->st>>>(
             c->pos_s, c->perm, c->cell_of, c->cell_start, c->cell_cnt, c->exs_idx, c->exs_list, c->exs_rng, n, c->ncl,
             c->ccap,
-            sort_rows, sq, c->prm.rcut_book + 0.05, c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
+            sort_rows, sq, c->prm.rcut_book + 0.05, (float)(sq * (1.0 - 1.0e-5) - scr),
+            (float)(sq * (1.0 + 1.0e-5) + scr), c->dyn, c->clist, c->ccnt, c->hasup, c->counters, c->status);
         if (n > 1) k_count_noup<<<(n - 1 + 255) / 256, 256, 0, c->st>>>(c->hasup, n - 1, c->counters);
         c->launches += 7;
         PGK_CUDA(c, cudaGetLastError());
