@@ -41,6 +41,28 @@ __global__ void k_drift(double* __restrict__ pos, double* __restrict__ old, cons
     pos[k] = x * dyn->dr_a[d] + vel[k] * dyn->dr_b[d];
 }
 
+// Kicks and drift of one short step in one pass over the atoms (the same
+// arithmetic as k_kick_long, k_kick_short and k_drift, in the order the KD_*
+// flags give).
+template <bool MIXED>
+__global__ void k_kick_drift(double* __restrict__ vel, double* __restrict__ pos, double* __restrict__ old,
+                             const void* __restrict__ fl, const void* __restrict__ fs,
+                             const double* __restrict__ mass, int n, const DynState* __restrict__ dyn, int flags) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    const int d = k % 3;
+    double v = vel[k];
+    if ((flags & KD_SHORT) && (flags & KD_SHORT_FIRST)) v = v + dyn->ks_b * (force_get<MIXED>(fs, k) / mass[k / 3]);
+    if (flags & KD_LONG) v = v * dyn->kl_s[d] + (force_get<MIXED>(fl, k) / mass[k / 3]) * dyn->kl_b[d];
+    if ((flags & KD_SHORT) && !(flags & KD_SHORT_FIRST)) v = v + dyn->ks_b * (force_get<MIXED>(fs, k) / mass[k / 3]);
+    vel[k] = v;
+    if (flags & KD_DRIFT) {
+        const double x = pos[k];
+        if (flags & KD_SAVE) old[k] = x;
+        pos[k] = x * dyn->dr_a[d] + v * dyn->dr_b[d];
+    }
+}
+
 // rattle_c / rattle_cmtk: one thread per constraint group, Gauss-Seidel sweeps
 // in the reference order, at most 300 sweeps (bounded; failure -> status bit).
 // The group's atoms (a contiguous span of at most RATTLE_LOCAL atoms) are
@@ -239,8 +261,7 @@ __device__ void chain_tail(ChainDev& c, const pgk_mdparams& md, double* glogs, d
     }
 }
 
-__global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs a) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restrict__ acc, const ChainArgs& a) {
     ChainDev c = *chain;
     const pgk_mdparams& md = a.md;
     int M = md.mchain;
@@ -314,12 +335,15 @@ __global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restric
     *chain = c;
 }
 
+__global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs a) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) chain_run(chain, acc, a);
+}
+
 // kick / drift coefficients of the step (moldyn_*.F90 at istep_short == 1)
 // kind: 0 NVE, 1 NHC, 2 MTK
 struct CoefArgs { pgk_mdparams md; int degfree; int kind; };
 
-__global__ void k_coeffs(DynState* __restrict__ dyn, const ChainDev* __restrict__ chain, CoefArgs a) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void coeffs_run(DynState* __restrict__ dyn, const ChainDev* __restrict__ chain, const CoefArgs& a) {
     const pgk_mdparams& md = a.md;
     const double dtl = md.dt_long_cal, dts = md.dt_long_cal / (double)md.nstep_short;
     const double e2 = 1.0 / 6.0, e4 = e2 / 20.0, e6 = e4 / 42.0, e8 = e6 / 72.0;
@@ -379,6 +403,18 @@ __global__ void k_coeffs(DynState* __restrict__ dyn, const ChainDev* __restrict_
     }
 }
 
+__global__ void k_coeffs(DynState* __restrict__ dyn, const ChainDev* __restrict__ chain, CoefArgs a) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) coeffs_run(dyn, chain, a);
+}
+
+// chain update followed by the step's coefficients (start of an NHC / MTK step)
+__global__ void k_chain_coeffs(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs ca,
+                               DynState* __restrict__ dyn, CoefArgs cf) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    chain_run(chain, acc, ca);
+    coeffs_run(dyn, chain, cf);
+}
+
 // erf_corr_cutoff.F90:28-62 (the reference's min-ish rule kept)
 __device__ double rkcut_of(const double* box, int n1, int n2, int n3) {
     double m1 = 0.5 * (n1 / box[0]);
@@ -423,9 +459,8 @@ __global__ void k_rkcut(DynState* __restrict__ dyn, int n1, int n2, int n3) {
 // sums and both groups' virials (+ self and net-charge terms)
 struct PressArgs { double pot_ewc, netchrgsq, alpha; int ifspme, ifnetqcorrp, dbl; };
 
-__global__ void k_press(const long long* __restrict__ acc, const DynState* __restrict__ dyn, ChainDev* chain,
-                        PressArgs a) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ void press_run(const long long* __restrict__ acc, const DynState* __restrict__ dyn, ChainDev* chain,
+                          const PressArgs& a) {
     const long long* A = acc;              // kinetic sums live in group 0
     const bool dbl = a.dbl != 0;
     double K = acc_get(A, A_KE, dbl);
@@ -458,6 +493,19 @@ __global__ void k_press(const long long* __restrict__ acc, const DynState* __res
     for (int k = 0; k < 9; ++k) chain->pintt[k] = 1.0 * b3 * (acc_get(A, A_KET + k, dbl) + Wt[k]);
 }
 
+__global__ void k_press(const long long* __restrict__ acc, const DynState* __restrict__ dyn, ChainDev* chain,
+                        PressArgs a) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) press_run(acc, dyn, chain, a);
+}
+
+// pressure of the step end followed by the chain update (end of an MTK step)
+__global__ void k_press_chain(const long long* __restrict__ acc, const DynState* __restrict__ dyn,
+                              ChainDev* chain, PressArgs pa, ChainArgs ca) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    press_run(acc, dyn, chain, pa);
+    chain_run(chain, acc, ca);
+}
+
 template <bool MIXED>
 __global__ void k_copy_force(const void* __restrict__ f, double* __restrict__ out, int n3) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -484,6 +532,20 @@ pgk_status launch_kick_short(pgk_ctx* c) {
     int n3 = 3 * c->natom;
     if (c->mixed()) k_kick_short<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
     else k_kick_short<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_kick_drift(pgk_ctx* c, int flags) {
+    if (!flags) return PGK_OK;
+    const int n3 = 3 * c->natom;
+    if (c->mixed())
+        k_kick_drift<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->pos, c->pos_old, c->facc[0], c->facc[1],
+                                                               c->mass, c->natom, c->dyn, flags);
+    else
+        k_kick_drift<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->pos, c->pos_old, c->facc[0], c->facc[1],
+                                                                c->mass, c->natom, c->dyn, flags);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -703,6 +765,22 @@ pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md) {
     return PGK_OK;
 }
 
+pgk_status launch_chain_coeffs(pgk_ctx* c, int chain_kind, int coef_kind, const pgk_mdparams& md) {
+    ChainArgs ca;
+    ca.md = md;
+    ca.degfree = c->degfree;
+    ca.dbl = c->mixed() ? 0 : 1;
+    ca.kind = chain_kind;
+    CoefArgs cf;
+    cf.md = md;
+    cf.degfree = c->degfree;
+    cf.kind = coef_kind;
+    k_chain_coeffs<<<1, 32, 0, c->st>>>(c->chain, c->acc, ca, c->dyn, cf);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
 pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int) {
     CoefArgs a;
     a.md = md;
@@ -714,14 +792,14 @@ pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int) {
     return PGK_OK;
 }
 
-pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md) {
+pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md, bool with_rkcut) {
     BoxArgs a;
     a.dts = md.dt_long_cal / (double)md.nstep_short;
     a.rcut = c->prm.rcut;
     a.rcut_book = c->prm.rcut_book;
     a.aniso = (kind == 2 && md.pcont_axis != PGK_PCONT_ISO) ? 1 : 0;
     a.nfft1 = c->prm.nfft1; a.nfft2 = c->prm.nfft2; a.nfft3 = c->prm.nfft3;
-    a.update_rk = c->prm.mts_ewk == PGK_MTS_SHORT ? 1 : 0;
+    a.update_rk = (with_rkcut || c->prm.mts_ewk == PGK_MTS_SHORT) ? 1 : 0;
     k_box<<<1, 32, 0, c->st>>>(c->dyn, c->chain, a, c->status);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
@@ -744,6 +822,25 @@ pgk_status launch_press(pgk_ctx* c) {
     a.ifnetqcorrp = c->prm.ifnetqcorrp;
     a.dbl = c->mixed() ? 0 : 1;
     k_press<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, a);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+pgk_status launch_press_chain(pgk_ctx* c, int chain_kind, const pgk_mdparams& md) {
+    PressArgs pa;
+    pa.pot_ewc = c->pot_ewc;
+    pa.netchrgsq = c->netchrgsq;
+    pa.alpha = c->prm.alpha;
+    pa.ifspme = c->prm.ifspme;
+    pa.ifnetqcorrp = c->prm.ifnetqcorrp;
+    pa.dbl = c->mixed() ? 0 : 1;
+    ChainArgs ca;
+    ca.md = md;
+    ca.degfree = c->degfree;
+    ca.dbl = c->mixed() ? 0 : 1;
+    ca.kind = chain_kind;
+    k_press_chain<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, pa, ca);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;

@@ -230,6 +230,11 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     c->natom = n;
     c->prec = p->precision;
     c->prm = *p;
+    {
+        const int S = PGK_MTS_SHORT;
+        c->short_empty = p->mts_bond != S && p->mts_angl != S && p->mts_tors != S && p->mts_torsrb != S &&
+                         p->mts_vdw != S && p->mts_ewk != S && p->mts_vdw14 != S && p->mts_elc14 != S;
+    }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -899,28 +904,32 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
     const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);
     pgk_status s;
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
+    // An empty short group (every term in the long group) has zero forces: its
+    // evaluation and kicks are skipped (they would add exact zeros).
+    const int kshort = c->short_empty ? 0 : KD_SHORT;
     if (lt) RUN(launch_langevin(c, md->dt_long_cal, step, true));
-    if (kind == 1 || kind == 2) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-    RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
+    if (kind == 1 || kind == 2) {
+        RUN(launch_kinetic(c, 0));
+        RUN(launch_chain_coeffs(c, chain_kind, hfdrv ? 0 : kind, *md));
+    } else {
+        RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
+    }
     for (int is = 1; is <= md->nstep_short; ++is) {
         bool last = is == md->nstep_short;
-        if (is == 1) RUN(launch_kick_long(c));
-        RUN(launch_kick_short(c));
-        RUN(launch_drift(c, rattle));
-        if (mtk) RUN(launch_box_update(c, kind, *md));
+        RUN(launch_kick_drift(c, (is == 1 ? KD_LONG : 0) | kshort | KD_DRIFT | (rattle ? KD_SAVE : 0)));
+        // the box update also refreshes the Ewald k cutoff for the long group's SPME
+        if (mtk) RUN(launch_box_update(c, kind, *md, last));
         if (rattle) RUN(launch_rattle_pos(c, md->eps_rattle, dts, mtk));
-        RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
+        if (!c->short_empty) RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
         if (last) {
-            if (mtk && c->prm.mts_ewk == PGK_MTS_LONG) RUN(launch_rkcut(c));
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (hfs) RUN(launch_hf_atm(c));
         }
-        RUN(launch_kick_short(c));
-        if (last) RUN(launch_kick_long(c));
+        RUN(launch_kick_drift(c, kshort | KD_SHORT_FIRST | (last ? KD_LONG : 0)));
         if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
     }
     if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-    if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); RUN(launch_chain(c, chain_kind, *md)); }
+    if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press_chain(c, chain_kind, *md)); }
 #undef RUN
     return PGK_OK;
 }

@@ -98,6 +98,7 @@ struct pgk_ctx {
     unsigned short* blk_inc = nullptr;   // local slot ids, per atom by type, term, position
 
     // ---- constraints ----
+    bool short_empty = false;     // no term in the short MTS group
     int ncgroup = 0, nconstraint = 0;
     int *cg_idx = nullptr, *cg_list = nullptr;
     int2* c_ij = nullptr; double* c_d = nullptr;
@@ -245,12 +246,23 @@ pgk_status launch_zero_group(pgk_ctx* c, int group);
 pgk_status launch_kick_long(pgk_ctx* c);
 pgk_status launch_kick_short(pgk_ctx* c);
 pgk_status launch_drift(pgk_ctx* c, bool save_old);
+// k_kick_drift flags: KD_LONG long kick, KD_SHORT short kick, KD_SHORT_FIRST
+// short kick before the long one (second half step), KD_DRIFT drift, KD_SAVE
+// keep the positions before the drift (RATTLE)
+#define KD_LONG 1
+#define KD_SHORT 2
+#define KD_DRIFT 4
+#define KD_SAVE 8
+#define KD_SHORT_FIRST 16
+pgk_status launch_kick_drift(pgk_ctx* c, int flags);
+pgk_status launch_chain_coeffs(pgk_ctx* c, int chain_kind, int coef_kind, const pgk_mdparams& md);
+pgk_status launch_press_chain(pgk_ctx* c, int chain_kind, const pgk_mdparams& md);
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rvinv);
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps);
 pgk_status launch_kinetic(pgk_ctx* c, int group);
 pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md);
 pgk_status launch_press(pgk_ctx* c);
 pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int phase);
-pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md);
+pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md, bool with_rkcut = false);
 pgk_status launch_copy_force(pgk_ctx* c, int group, double* dst_dev);
 pgk_status launch_out_record(pgk_ctx* c, long long step, double* dst);
