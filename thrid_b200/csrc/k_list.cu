@@ -381,6 +381,22 @@ static int list_mode_for(const pgk_ctx* c, const double* box, int* nc) {
 }
 
 // (re)allocate the sorted/padded arrays for up to npad_cap slots
+// cluster rows (book and pruned) for npad_cap/8 clusters of ccap entries
+static pgk_status alloc_rows(pgk_ctx* c) {
+    cudaFree(c->clist); cudaFree(c->plist);
+    c->clist = nullptr; c->plist = nullptr;
+    const size_t bytes = sizeof(int) * (size_t)(c->npad_cap / 8) * c->ccap;
+    if (cudaMalloc(&c->clist, bytes) != cudaSuccess) {
+        c->clist = nullptr;
+        return pgk_fail(c, PGK_E_NOMEM, "cluster pair list exceeds device memory");
+    }
+    if (c->prune_buffer > 0.f && cudaMalloc(&c->plist, bytes) != cudaSuccess) {
+        c->plist = nullptr;
+        return pgk_fail(c, PGK_E_NOMEM, "pruned pair list exceeds device memory");
+    }
+    return PGK_OK;
+}
+
 static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     if (npad_cap <= c->npad_cap) return PGK_OK;
     cudaFree(c->perm); cudaFree(c->pos_s); cudaFree(c->typ_s); cudaFree(c->xq); cudaFree(c->xq64);
@@ -400,21 +416,13 @@ static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     }
     else PGK_CUDA(c, cudaMalloc(&c->xq64, sizeof(double4) * npad_cap));
     PGK_CUDA(c, cudaMalloc(&c->ccnt, sizeof(int) * ncl));
-    if (cudaMalloc(&c->clist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {
-        c->clist = nullptr;
-        return pgk_fail(c, PGK_E_NOMEM, "cluster pair list exceeds device memory");
-    }
     if (c->prune_buffer > 0.f) {
-        if (cudaMalloc(&c->plist, sizeof(int) * (size_t)ncl * c->ccap) != cudaSuccess) {
-            c->plist = nullptr;
-            return pgk_fail(c, PGK_E_NOMEM, "pruned pair list exceeds device memory");
-        }
         PGK_CUDA(c, cudaMalloc(&c->pcnt, sizeof(int) * ncl));
         PGK_CUDA(c, cudaMalloc(&c->xq_prune, sizeof(int4) * npad_cap));
         PGK_CUDA(c, cudaMemsetAsync(c->xq_prune, 0, sizeof(int4) * npad_cap, c->st));
     }
     c->npad_cap = npad_cap;
-    return PGK_OK;
+    return alloc_rows(c);
 }
 
 pgk_status launch_mklist(pgk_ctx* c) {
@@ -490,10 +498,10 @@ pgk_status launch_mklist(pgk_ctx* c) {
             // grow the cluster rows and rebuild (the reference STOPs here)
             unsigned zero = 0;
             PGK_CUDA(c, cudaMemcpy(c->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
-            c->ccap = (int)((cnt[1] + 63) / 32 * 32);
-            int capslots = c->npad_cap;
-            c->npad_cap = 0;
-            if ((s = ensure_sorted_capacity(c, capslots))) return s;
+            // a quarter of headroom above the longest row, so the rows of
+            // later builds (density fluctuations) rarely force another regrowth
+            c->ccap = (int)(((long long)cnt[1] * 5 / 4 + 32 + 31) / 32 * 32);
+            if ((s = alloc_rows(c))) return s;
             continue;
         }
         h.nlistnball = (long long)(cnt[0] + cnt[2]);

@@ -327,6 +327,45 @@ __device__ __forceinline__ double conv_point(int k1, int k2, int k3, int K1, int
     return eterm;
 }
 
+// The same influence function in FP32 (mixed precision; the grid itself is
+// FP32 there): exp and divisions on the FP32 pipes, energy and virial sums
+// still accumulated in FP64.
+struct ConvF { float bi[3], rk2, fac, pivol; };
+
+__device__ __forceinline__ float conv_point_f(int k1, int k2, int k3, int K1, int K2, int K3, float s2,
+                                              const ConvArgs& ca, const ConvF& cf, double& en, double& vs,
+                                              double* vt) {
+    int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
+    int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
+    int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
+    const int m1 = k1 < nf1 ? k1 : k1 - K1;
+    const int m2 = k2 < nf2 ? k2 : k2 - K2;
+    const int m3 = k3 < nf3 ? k3 : k3 - K3;
+    const float h1 = cf.bi[0] * (float)m1, h2 = cf.bi[1] * (float)m2, h3 = cf.bi[2] * (float)m3;
+    const float msq = h1 * h1 + h2 * h2 + h3 * h3;
+    if (msq > cf.rk2) return 0.f;
+    const float denom = cf.pivol * (float)ca.bsp[k1] * (float)ca.bsp[K1 + k2] * (float)ca.bsp[K1 + K2 + k3] * msq;
+    const float ex = expf(-cf.fac * msq);
+    const float eterm = ex / denom;
+    if (ca.want) {
+        const float vterm = 2.f * (cf.fac * msq + 1.f) / msq;
+        float es = eterm * s2;
+        en += (double)es;
+        if (ca.corr) {
+            const float e2 = ex * (float)ca.netchrgsq / (cf.pivol * msq);
+            vs += (double)(e2 * (-1.f + 2.f * cf.fac * msq));
+            es -= e2;
+        }
+        vt[0] += (double)(es * (vterm * h1 * h1 - 1.f));
+        vt[1] += (double)(es * (vterm * h1 * h2));
+        vt[2] += (double)(es * (vterm * h1 * h3));
+        vt[3] += (double)(es * (vterm * h2 * h2 - 1.f));
+        vt[4] += (double)(es * (vterm * h2 * h3));
+        vt[5] += (double)(es * (vterm * h3 * h3 - 1.f));
+    }
+    return eterm;
+}
+
 // AXIS 0: pencils along x (contiguous); 1: along y; 2: along z.
 // SRC: 0 = complex grid in place, 1 = int64 fixed-point accumulation grid,
 //      2 = double accumulation grid (both real, first forward pass).
@@ -404,6 +443,14 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
     FftStages<T, T2, NC>::run(src, dst, P, n, plan, sg, tws);
     if (CONV) {
         double en = 0, vs = 0, vt[6] = {0, 0, 0, 0, 0, 0};
+        ConvF cf;
+        {
+            const double pi = 3.14159265358979323846;
+            for (int d = 0; d < 3; ++d) cf.bi[d] = (float)dyn->boxinv[d];
+            cf.rk2 = (float)(dyn->rkcut * dyn->rkcut);
+            cf.fac = (float)(pi * pi / (ca.alpha * ca.alpha));
+            cf.pivol = (float)(pi * dyn->box[0] * dyn->box[1] * dyn->box[2]);
+        }
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
             int p = idx / n, m = idx - p * n;
             const int sidx = p * ld + m;
@@ -411,10 +458,17 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
             if (k1 >= K1) continue;
             if (k1 == 0 && yz == 0 && m == 0) continue;   // m = 0 is skipped by scalar_sum
             T2 v = src[sidx];
-            double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
-            double et = conv_point(k1, yz, m, K1, K2, K3, s2, ca, dyn, en, vs, vt);
-            v.x = (T)((double)v.x * et);
-            v.y = (T)((double)v.y * et);
+            if (sizeof(T) == 4) {
+                const float et = conv_point_f(k1, yz, m, K1, K2, K3, (float)v.x * (float)v.x + (float)v.y * (float)v.y,
+                                              ca, cf, en, vs, vt);
+                v.x = (T)((float)v.x * et);
+                v.y = (T)((float)v.y * et);
+            } else {
+                double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
+                double et = conv_point(k1, yz, m, K1, K2, K3, s2, ca, dyn, en, vs, vt);
+                v.x = (T)((double)v.x * et);
+                v.y = (T)((double)v.y * et);
+            }
             src[sidx] = v;
         }
         __syncthreads();

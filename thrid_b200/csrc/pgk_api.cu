@@ -500,7 +500,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         // pair once, in its lower slot's row); rows regrow on overflow
         double rs = rb + 2.0;
         double expect = (double)n / vol * 4.0 / 3.0 * std::acos(-1.0) * rs * rs * rs;
-        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(0.75 * expect + 128);
+        int cap = p->max_nbr > 0 ? p->max_nbr : (int)(expect + 128);
         cap = std::min(cap, ((n + 31) / 32) * 32);
         cap = ((cap + 31) / 32) * 32;
         c->ccap = std::max(cap, 32);
