@@ -90,6 +90,11 @@ struct PairArgs {
     double rr2, rl2, rmax2, rrcut;
     void* facc; long long* acc;
     long long* fsort; int fstride;     // mixed: forces by sorted slot (SoA, stride fstride)
+    // pruned rows (mixed; P null = none): on a prune step (P->do_prune) the
+    // kernel reads the book rows (blist/bcnt), writes each entry's pairs inside
+    // rprune (rp2) compacted into plist/pcnt and the new displacement origin
+    // xq_prune; otherwise it reads plist/pcnt
+    const PruneDev* P; const int* blist; const int* bcnt; int* plist; int* pcnt; int4* xq_prune; float rp2;
 };
 
 // ---- one pair, mixed precision -----------------------------------------------
@@ -103,12 +108,13 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
                                           const float rl2, const float inv_h, const float h, const int nsplm1,
                                           const float4* __restrict__ sf, const float4* __restrict__ sp,
                                           const float2* __restrict__ slj, float (&fi)[3], float& gx, float& gy,
-                                          float& gz, float& ev, float& ee, float* wc, float* wl) {
+                                          float& gz, float& ev, float& ee, float* wc, float* wl, float& r2o) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     const float dx = (float)(pi.x - pj.x) * sx;
     const float dy = (float)(pi.y - pj.y) * sy;
     const float dz = (float)(pi.z - pj.z) * sz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    r2o = r2;
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
     const float r = r2 * rinv;
@@ -208,41 +214,61 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     float ev = 0.f, ee = 0.f;
     float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
+    const bool prune = a.P != nullptr && a.P->do_prune;         // block-uniform
+    const int* __restrict__ rows = prune ? a.blist : a.clist;
+    const int* __restrict__ rcnt = prune ? a.bcnt : a.ccnt;
+    const float rp2 = a.rp2;
+
     for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
         __syncwarp();
         if (lane < 8) {
-            si[warp][lane] = __ldg(xq + 8 * cl + lane);
+            const int4 v = __ldg(xq + 8 * cl + lane);
+            si[warp][lane] = v;
             sti[warp][lane] = __ldg(typ_s + 8 * cl + lane) * a.ntyp;
+            if (prune) a.xq_prune[8 * cl + lane] = v;
         }
         __syncwarp();
-        const int cnt = __ldg(a.ccnt + cl);
-        const int* __restrict__ row = a.clist + (size_t)cl * a.ccap;
+        const int cnt = __ldg(rcnt + cl);
+        const int* __restrict__ row = rows + (size_t)cl * a.ccap;
+        int* __restrict__ prow = a.plist + (size_t)cl * a.ccap;
+        int pcount = 0;
         float f[8][3];
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) { f[ii][0] = 0.f; f[ii][1] = 0.f; f[ii][2] = 0.f; }
-        int k = lane;
-        unsigned e = k < cnt ? (unsigned)__ldg(row + k) : 0u;
+        unsigned e = lane < cnt ? (unsigned)__ldg(row + lane) : 0u;
         int4 pj = __ldg(xq + (e & 0xFFFFFFu));
         int tj = __ldg(typ_s + (e & 0xFFFFFFu));
-        while (k < cnt) {
-            const int kn = k + 32;
+        for (int k0 = 0; k0 < cnt; k0 += 32) {          // warp-uniform trip count
+            const int kn = k0 + 32 + lane;
             const unsigned en = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
             const int4 pjn = __ldg(xq + (en & 0xFFFFFFu));
             const int tjn = __ldg(typ_s + (en & 0xFFFFFFu));
             const unsigned m = e >> 24;
             const int sj = e & 0xFFFFFFu;
             float gx = 0.f, gy = 0.f, gz = 0.f;
+            unsigned nm = 0;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii)
-                if ((m >> ii) & 1u)
+                if ((m >> ii) & 1u) {
+                    float r2;
                     pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rr2, rl2, inv_h, h, nsplm1,
-                                    sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl);
-            unsigned long long* fj = (unsigned long long*)fs0 + sj;
-            atomicAdd(fj, (unsigned long long)__double2ll_rn((double)gx * PGK_FORCE_SCALE));
-            atomicAdd(fj + fst, (unsigned long long)__double2ll_rn((double)gy * PGK_FORCE_SCALE));
-            atomicAdd(fj + 2 * fst, (unsigned long long)__double2ll_rn((double)gz * PGK_FORCE_SCALE));
-            k = kn; e = en; pj = pjn; tj = tjn;
+                                    sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
+                    nm |= r2 < rp2 ? 1u << ii : 0u;
+                }
+            if (m) {
+                unsigned long long* fj = (unsigned long long*)fs0 + sj;
+                atomicAdd(fj, (unsigned long long)__float2ll_rn(gx * (float)PGK_FORCE_SCALE));
+                atomicAdd(fj + fst, (unsigned long long)__float2ll_rn(gy * (float)PGK_FORCE_SCALE));
+                atomicAdd(fj + 2 * fst, (unsigned long long)__float2ll_rn(gz * (float)PGK_FORCE_SCALE));
+            }
+            if (prune) {       // compact the entries that keep a pair inside rprune
+                const unsigned b = __ballot_sync(0xffffffffu, nm != 0);
+                if (nm) prow[pcount + __popc(b & ((1u << lane) - 1u))] = (int)((nm << 24) | (unsigned)sj);
+                pcount += __popc(b);
+            }
+            e = en; pj = pjn; tj = tjn;
         }
+        if (prune && lane == 0) a.pcnt[cl] = pcount;
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
@@ -391,94 +417,52 @@ __global__ void k_prune_decide(PruneDev* __restrict__ P, const DynState* __restr
     }
 }
 
-// Rows of the book list with the masks cut to the pairs inside rprune at the
-// current positions (entries left without pairs dropped), regrouped by mask
-// like the book rows; the cluster's slots record their positions as the new
-// displacement origin.  One warp per row; no-op unless a prune was decided.
-__global__ void __launch_bounds__(256) k_prune(const int4* __restrict__ xq, int4* __restrict__ xq_prune,
-                                               const int* __restrict__ clist, const int* __restrict__ ccnt,
-                                               int ccap, int ncl, int* __restrict__ plist, int* __restrict__ pcnt,
-                                               const PruneDev* __restrict__ P, const DynState* __restrict__ dyn,
-                                               float rp2, int sort_rows) {
+// After a prune step: regroup each pruned row by mask (stable counting sort
+// in shared memory, as the book rows), so the pair kernel's loops over the
+// mask bits stay uniform across a warp.  One warp per row; no-op unless a
+// prune was decided.
+__global__ void __launch_bounds__(256) k_prune_sort(int* __restrict__ plist, const int* __restrict__ pcnt, int ccap,
+                                                    int ncl, const PruneDev* __restrict__ P) {
     if (!P->do_prune) return;
-    __shared__ int4 si[8][8];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (cl >= ncl) return;
-    const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
-    const float sy = (float)(dyn->box[1] * (1.0 / 4294967296.0));
-    const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
-    if (lane < 8) {
-        const int4 v = xq[8 * cl + lane];
-        si[wib][lane] = v;
-        xq_prune[8 * cl + lane] = v;
+    extern __shared__ int prow_raw[];
+    int* buf = prow_raw + (size_t)wib * (ccap + 256);
+    int* bin = buf + ccap;
+    int* out = plist + (size_t)cl * ccap;
+    const int count = pcnt[cl];
+    for (int q = lane; q < 256; q += 32) bin[q] = 0;
+    __syncwarp();
+    for (int k0 = 0; k0 < count; k0 += 32) {
+        const int k = k0 + lane;
+        const int e = k < count ? out[k] : 0;
+        if (k < count) buf[k] = e;
+        const unsigned key = k < count ? ((unsigned)e >> 24) : 256u + lane;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
     }
     __syncwarp();
-    const int cnt = ccnt[cl];
-    const int* __restrict__ row = clist + (size_t)cl * ccap;
-    int* out = plist + (size_t)cl * ccap;
-    extern __shared__ int prow_raw[];
-    int* buf = sort_rows ? prow_raw + (size_t)wib * (ccap + 256) : out;
-    int count = 0;
-    unsigned e = lane < cnt ? (unsigned)row[lane] : 0u;
-    int4 pj = xq[e & 0xFFFFFFu];
-    for (int k0 = 0; k0 < cnt; k0 += 32) {
-        const int kn = k0 + 32 + lane;          // next chunk's entry and j, loaded ahead
-        const unsigned en = kn < cnt ? (unsigned)row[kn] : 0u;
-        const int4 pjn = xq[en & 0xFFFFFFu];
-        const unsigned m = e >> 24;
-        unsigned nm = 0;
-        if (m) {
-            // per-pair minimum image from the wrapped fixed-point difference,
-            // exactly as the pair kernel forms it
-#pragma unroll
-            for (int ii = 0; ii < 8; ++ii) {
-                const int4 pi = si[wib][ii];
-                const float dx = (float)(pi.x - pj.x) * sx;
-                const float dy = (float)(pi.y - pj.y) * sy;
-                const float dz = (float)(pi.z - pj.z) * sz;
-                const bool in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < rp2;
-                nm |= (in && ((m >> ii) & 1u)) ? 1u << ii : 0u;
-            }
-        }
-        const unsigned b = __ballot_sync(0xffffffffu, nm != 0);
-        if (nm) buf[count + __popc(b & ((1u << lane) - 1u))] = (int)((nm << 24) | (e & 0xFFFFFFu));
-        count += __popc(b);
-        e = en; pj = pjn;
+    if (lane == 0) {
+        int run = 0;
+        for (int q = 0; q < 256; ++q) { const int v = bin[q]; bin[q] = run; run += v; }
     }
-    if (sort_rows) {          // stable counting sort by mask (as the book rows)
-        int* bin = buf + ccap;
-        for (int q = lane; q < 256; q += 32) bin[q] = 0;
+    __syncwarp();
+    for (int k0 = 0; k0 < count; k0 += 32) {
+        const int k = k0 + lane;
+        const bool ok = k < count;
+        const int e = ok ? buf[k] : 0;
+        const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int rank = __popc(grp & ((1u << lane) - 1u));
+        const int base = ok ? bin[key] : 0;
         __syncwarp();
-        for (int k0 = 0; k0 < count; k0 += 32) {
-            const int k = k0 + lane;
-            const unsigned key = k < count ? ((unsigned)buf[k] >> 24) : 256u + lane;
-            const unsigned grp = __match_any_sync(0xffffffffu, key);
-            if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
+        if (ok) {
+            out[base + rank] = e;
+            if (rank == 0) bin[key] = base + __popc(grp);
         }
         __syncwarp();
-        if (lane == 0) {
-            int run = 0;
-            for (int q = 0; q < 256; ++q) { const int v = bin[q]; bin[q] = run; run += v; }
-        }
-        __syncwarp();
-        for (int k0 = 0; k0 < count; k0 += 32) {
-            const int k = k0 + lane;
-            const bool ok = k < count;
-            const int e = ok ? buf[k] : 0;
-            const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
-            const unsigned grp = __match_any_sync(0xffffffffu, key);
-            const int rank = __popc(grp & ((1u << lane) - 1u));
-            const int base = ok ? bin[key] : 0;
-            __syncwarp();
-            if (ok) {
-                out[base + rank] = e;
-                if (rank == 0) bin[key] = base + __popc(grp);
-            }
-            __syncwarp();
-        }
     }
-    if (lane == 0) pcnt[cl] = count;
 }
 
 // sorted-slot pair forces -> the group accumulator (one thread per slot: the
@@ -503,6 +487,15 @@ static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     k_pair_mixed<MODE><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
     PGK_LAUNCHED(c);
     k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
+    if (a.P) {
+        const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
+        if (sort_sm <= 160 * 1024 && smem_limit(k_prune_sort, sort_sm) == cudaSuccess) {
+            PGK_LAUNCHED(c);
+            const long long threads = (long long)c->ncl * 32;
+            k_prune_sort<<<(unsigned)((threads + 255) / 256), 256, sort_sm, c->st>>>(c->plist, c->pcnt, c->ccap,
+                                                                                     c->ncl, c->prune);
+        }
+    }
 }
 
 // vmode: PM_FORCE / PM_ENE / PM_TENS / PM_FULL (see above)
@@ -519,18 +512,15 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
     a.fsort = c->fsort; a.fstride = c->npad_cap;
-    if (c->mixed() && c->prune_buffer > 0.f) {
-        const float rmax = (float)std::sqrt(a.rmax2);
-        const float rp = rmax + c->prune_buffer;
+    a.P = nullptr; a.blist = nullptr; a.bcnt = nullptr; a.plist = nullptr; a.pcnt = nullptr; a.xq_prune = nullptr;
+    a.rp2 = 0.f;
+    const bool pruned = c->mixed() && c->prune_buffer > 0.f;
+    if (pruned) {
+        const float rp = (float)std::sqrt(a.rmax2) + c->prune_buffer;
         k_prune_decide<<<1, 32, 0, c->st>>>(c->prune, c->dyn, c->prune_buffer, rp);
-        const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
-        const int sort_rows = sort_sm <= 160 * 1024 ? 1 : 0;
-        if (sort_rows) smem_limit(k_prune, sort_sm);
-        const long long threads = (long long)c->ncl * 32;
-        k_prune<<<(unsigned)((threads + 255) / 256), 256, sort_rows ? sort_sm : 0, c->st>>>(
-            c->xq, c->xq_prune, c->clist, c->ccnt, c->ccap, c->ncl, c->plist, c->pcnt, c->prune, c->dyn, rp * rp,
-            sort_rows);
-        c->launches += 2;
+        c->launches += 1;
+        a.P = c->prune; a.blist = c->clist; a.bcnt = c->ccnt; a.plist = c->plist; a.pcnt = c->pcnt;
+        a.xq_prune = c->xq_prune; a.rp2 = rp * rp;
         a.clist = c->plist; a.ccnt = c->pcnt;
     }
     const int warps_per_block = 8;
