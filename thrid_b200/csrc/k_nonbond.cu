@@ -180,11 +180,15 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
 // warps take every 8th cluster of it, so they read overlapping j ranges at
 // the same time (shared L1 lines).  Per-lane energy/virial sums stay in FP32
 // registers across the block's clusters and are reduced once per block.
-template <int MODE>
+// PRUNE: the instance that runs on prune steps (reads the book rows, writes
+// the pruned ones); the other instance runs on all other steps.  Both are
+// launched; each returns at once when the step is not its kind.
+template <int MODE, bool PRUNE>
 __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
                                                        const float2* __restrict__ lj_g,
                                                        const float4* __restrict__ spl_g,
                                                        const DynState* __restrict__ dyn) {
+    if (PRUNE ? (a.P == nullptr || !a.P->do_prune) : (a.P != nullptr && a.P->do_prune)) return;   // other step kind
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     extern __shared__ float4 sm[];
     float4* sf = sm;                        // force table  (spline 0)
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     float ev = 0.f, ee = 0.f;
     float wc[6] = {0, 0, 0, 0, 0, 0}, wl[6] = {0, 0, 0, 0, 0, 0};
 
-    const bool prune = a.P != nullptr && a.P->do_prune;         // block-uniform
+    const bool prune = PRUNE;
     const int* __restrict__ rows = prune ? a.blist : a.clist;
     const int* __restrict__ rcnt = prune ? a.bcnt : a.ccnt;
     const float rp2 = a.rp2;
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
                     float r2;
                     pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rr2, rl2, inv_h, h, nsplm1,
                                     sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
-                    nm |= r2 < rp2 ? 1u << ii : 0u;
+                    if (PRUNE) nm |= r2 < rp2 ? 1u << ii : 0u;
                 }
             if (m) {
                 unsigned long long* fj = (unsigned long long*)fs0 + sj;
@@ -483,9 +487,14 @@ template <int MODE>
 static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-    smem_limit(k_pair_mixed<MODE>, sm);
-    k_pair_mixed<MODE><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+    smem_limit(k_pair_mixed<MODE, false>, sm);
+    k_pair_mixed<MODE, false><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
     PGK_LAUNCHED(c);
+    if (a.P) {
+        smem_limit(k_pair_mixed<MODE, true>, sm);
+        k_pair_mixed<MODE, true><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+        PGK_LAUNCHED(c);
+    }
     k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
     if (a.P) {
         const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
