@@ -323,10 +323,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
             atomicAdd(&bin[(unsigned)e >> 24], 1);
         }
         __syncwarp();
-        if (lane == 0) {                        // exclusive scan of the 256 bins
-            int run = 0;
-            for (int q = 0; q < 256; ++q) { int v = bin[q]; bin[q] = run; run += v; }
-        }
+        warp_scan256(bin, lane);                 // exclusive scan of the 256 bins
         __syncwarp();
         for (int k0 = 0; k0 < count; k0 += 32) {
             const int k = k0 + lane;

@@ -447,10 +447,7 @@ __global__ void __launch_bounds__(256) k_prune_sort(int* __restrict__ plist, con
         if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
     }
     __syncwarp();
-    if (lane == 0) {
-        int run = 0;
-        for (int q = 0; q < 256; ++q) { const int v = bin[q]; bin[q] = run; run += v; }
-    }
+    warp_scan256(bin, lane);                 // exclusive scan of the 256 bins
     __syncwarp();
     for (int k0 = 0; k0 < count; k0 += 32) {
         const int k = k0 + lane;

@@ -159,6 +159,22 @@ __device__ __forceinline__ double force_get(const void* facc, size_t k) {
 }
 
 // Fortran dnint/anint (round half away from zero), exact FP64 min image
+// exclusive prefix sum of 256 shared-memory bins by one warp (8 bins a lane)
+__device__ __forceinline__ void warp_scan256(int* bin, int lane) {
+    int v[8], t = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { v[q] = bin[8 * lane + q]; t += v[q]; }
+    int incl = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    int run = incl - t;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) { bin[8 * lane + q] = run; run += v[q]; }
+}
+
 __device__ __forceinline__ double mi_exact(double r, double box, double binv) {
     return __dsub_rn(r, __dmul_rn(box, round(__dmul_rn(r, binv))));
 }
