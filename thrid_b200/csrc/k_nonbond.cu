@@ -425,7 +425,7 @@ __global__ void k_prune_decide(PruneDev* __restrict__ P, const DynState* __restr
 // in shared memory, as the book rows), so the pair kernel's loops over the
 // mask bits stay uniform across a warp.  One warp per row; no-op unless a
 // prune was decided.
-__global__ void __launch_bounds__(256) k_prune_sort(int* __restrict__ plist, const int* __restrict__ pcnt, int ccap,
+__global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, const int* __restrict__ pcnt, int ccap,
                                                     int ncl, const PruneDev* __restrict__ P) {
     if (!P->do_prune) return;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -437,12 +437,18 @@ __global__ void __launch_bounds__(256) k_prune_sort(int* __restrict__ plist, con
     int* out = plist + (size_t)cl * ccap;
     const int count = pcnt[cl];
     for (int q = lane; q < 256; q += 32) bin[q] = 0;
+    // stage the row: eight loads in flight per lane
+    for (int k0 = 0; k0 < count; k0 += 256) {
+        int r[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) { const int k = k0 + 32 * q + lane; r[q] = k < count ? out[k] : 0; }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) { const int k = k0 + 32 * q + lane; if (k < count) buf[k] = r[q]; }
+    }
     __syncwarp();
     for (int k0 = 0; k0 < count; k0 += 32) {
         const int k = k0 + lane;
-        const int e = k < count ? out[k] : 0;
-        if (k < count) buf[k] = e;
-        const unsigned key = k < count ? ((unsigned)e >> 24) : 256u + lane;
+        const unsigned key = k < count ? ((unsigned)buf[k] >> 24) : 256u + lane;
         const unsigned grp = __match_any_sync(0xffffffffu, key);
         if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
     }
@@ -494,11 +500,11 @@ static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     }
     k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
     if (a.P) {
-        const size_t sort_sm = (size_t)8 * (c->ccap + 256) * sizeof(int);
+        const size_t sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each
         if (sort_sm <= 160 * 1024 && smem_limit(k_prune_sort, sort_sm) == cudaSuccess) {
             PGK_LAUNCHED(c);
             const long long threads = (long long)c->ncl * 32;
-            k_prune_sort<<<(unsigned)((threads + 255) / 256), 256, sort_sm, c->st>>>(c->plist, c->pcnt, c->ccap,
+            k_prune_sort<<<(unsigned)((threads + 127) / 128), 128, sort_sm, c->st>>>(c->plist, c->pcnt, c->ccap,
                                                                                      c->ncl, c->prune);
         }
     }
