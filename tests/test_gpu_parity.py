@@ -373,3 +373,32 @@ def test_mixed_pruned_list_keeps_every_pair(monkeypatch):
     f2, en2, _ = e2.calforce(abi.MTS_LONG)
     assert rel_rms(f1, f2) < 1e-6
     assert erel(en1["pot_nonbon"], en2["pot_nonbon"]) < 1e-6
+
+
+# ------------------------------------------------------------ cluster frame ---
+def test_mixed_cluster_frame_matches_per_pair_image(monkeypatch):
+    """Boxes wide enough for the cluster frame (here 93.6 A, 70k atoms): the
+    pair kernel takes displacements as FP32 offsets from each cluster's first
+    atom and the tensor-only virial from the atom forces.  Anisotropic MTK
+    steps (tensor-only between outputs) must match the per-pair minimum-image
+    kernel to FP32 rounding and track the FP64 device path."""
+    s = S.propanol_box(nside=18, box=93.6)
+    md = _md(s, kind="mtk", pext_pa=1.0e5, axis=abi.PCONT_ANISO)
+    res = {}
+    for tag, prec, frame in (("frame", abi.PREC_MIXED, "1"), ("pair", abi.PREC_MIXED, "0"), ("fp64", abi.PREC_FP64, "1")):
+        monkeypatch.setenv("PGK_PAIR_FRAME", frame)
+        e = engine(s, prec)
+        e.set_chain(abi.chain_init(s.box))
+        en = e.moldyn_mtk(0, 4, md)
+        x, _, b = e.download_state()
+        res[tag] = (x, b, en["pot_tot"], np.array(e.get_chain().vboxg[:]))
+        e.close()
+    xf, bf, pf, vf = res["frame"]
+    xp, bp, pp, vp = res["pair"]
+    x6, b6, p6, v6 = res["fp64"]
+    assert np.abs(xf - xp).max() < 1e-5
+    assert np.abs(bf - bp).max() < 1e-9 * np.abs(bp).max()
+    assert erel(pf, pp) < 1e-6 * max(1.0, abs(pp))
+    assert np.abs(vf - vp).max() < 1e-2 * max(np.abs(v6).max(), 1e-12)      # barostat velocity: the virial
+    assert np.abs(xf - x6).max() < 1e-4
+    assert erel(pf, p6) < 1e-5 * max(1.0, abs(p6))

@@ -102,23 +102,22 @@ struct PairArgs {
 // cutoffs select zero (the spline index is clamped into the table), so the
 // lanes of a warp never diverge inside the pair arithmetic.  The force on
 // cluster atom fi and the opposite force on j (g) accumulate directly.
-template <int MODE>
-__device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int4 pj, const int tj,
-                                          const float sx, const float sy, const float sz, const float rr2,
-                                          const float rl2, const float inv_h, const float h, const int nsplm1,
-                                          const float4* __restrict__ sf, const float4* __restrict__ sp,
-                                          const float2* __restrict__ slj, float (&fi)[3], float& gx, float& gy,
-                                          float& gz, float& ev, float& ee, float* wc, float* wl, float& r2o) {
+// (dx, dy, dz) = x_i - x_j (minimum image), qq = q_i q_j, tij = LJ table row
+// of the pair.  PAIRVIR: the tensor-only virial is summed per pair here (else
+// the caller forms it from the atom forces in the cluster frame).
+template <int MODE, bool PAIRVIR>
+__device__ __forceinline__ void pair_term(const float dx, const float dy, const float dz, const float qq,
+                                          const int tij, const float rr2, const float rl2, const float inv_h,
+                                          const float h, const int nsplm1, const float4* __restrict__ sf,
+                                          const float4* __restrict__ sp, const float2* __restrict__ slj,
+                                          float (&fi)[3], float& gx, float& gy, float& gz, float& ev, float& ee,
+                                          float* wc, float* wl, float& r2o) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
-    const float dx = (float)(pi.x - pj.x) * sx;
-    const float dy = (float)(pi.y - pj.y) * sy;
-    const float dz = (float)(pi.z - pj.z) * sz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     r2o = r2;
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
     const float r = r2 * rinv;
-    const float qq = __int_as_float(pi.w) * __int_as_float(pj.w);
     // floor(r/h) on the FP32/ALU pipes (r/h < 2^22): round to nearest via
     // the 2^23 magic constant, step down when it rounded up
     const float tf = r * inv_h;
@@ -136,7 +135,7 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
         const float pe = qq * fmaf(d, fmaf(d, fmaf(d, p.w, p.z), p.y), p.x);
         ee += inr ? pe : 0.f;
     }
-    const float2 lp = slj[ti + tj];
+    const float2 lp = slj[tij];
     const float t2 = rinv2 * lp.x;
     const float t6 = t2 * t2 * t2;
     const float t12 = t6 * t6;
@@ -147,7 +146,7 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
     const float cx = fs * dx, cy = fs * dy, cz = fs * dz;
     fi[0] += cx; fi[1] += cy; fi[2] += cz;
     gx -= cx; gy -= cy; gz -= cz;
-    if (MODE == PM_TENS) {
+    if (MODE == PM_TENS && PAIRVIR) {
         wc[0] = fmaf(cx, dx, wc[0]); wc[1] = fmaf(cx, dy, wc[1]); wc[2] = fmaf(cx, dz, wc[2]);
         wc[3] = fmaf(cy, dy, wc[3]); wc[4] = fmaf(cy, dz, wc[4]); wc[5] = fmaf(cz, dz, wc[5]);
     }
@@ -183,7 +182,13 @@ __device__ __forceinline__ void pair_term(const int4 pi, const int ti, const int
 // PRUNE: the instance that runs on prune steps (reads the book rows, writes
 // the pruned ones); the other instance runs on all other steps.  Both are
 // launched; each returns at once when the step is not its kind.
-template <int MODE, bool PRUNE>
+// FRAME (boxes wide enough that the cluster atoms and every listed j, each
+// taken as its minimum image from cluster atom 0, never wrap against each
+// other): positions enter as FP32 offsets from cluster atom 0, so a pair's
+// displacement is three subtractions, and the tensor-only virial is summed
+// as sum_a F_a (x) x_a over the cluster atoms and the entries' j (equal to
+// sum over pairs f (x) r, with the lever arms of the cluster frame).
+template <int MODE, bool PRUNE, bool FRAME>
 __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
                                                        const float2* __restrict__ lj_g,
                                                        const float4* __restrict__ spl_g,
@@ -195,6 +200,7 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     float4* sp = sm + a.nspl;               // pot table    (spline 1), ENE only
     float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
     __shared__ int4 si[8][8];
+    __shared__ float4 sif[8][8];          // FRAME: offsets from cluster atom 0 (A) and charge
     __shared__ int sti[8][8];
     for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) {
         sf[k] = spl_g[k];
@@ -225,9 +231,13 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
 
     for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
         __syncwarp();
+        const int4 p0 = __ldg(xq + 8 * cl);
         if (lane < 8) {
             const int4 v = __ldg(xq + 8 * cl + lane);
             si[warp][lane] = v;
+            if (FRAME)
+                sif[warp][lane] = make_float4((float)(v.x - p0.x) * sx, (float)(v.y - p0.y) * sy,
+                                              (float)(v.z - p0.z) * sz, __int_as_float(v.w));
             sti[warp][lane] = __ldg(typ_s + 8 * cl + lane) * a.ntyp;
             if (prune) a.xq_prune[8 * cl + lane] = v;
         }
@@ -251,14 +261,31 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
             const int sj = e & 0xFFFFFFu;
             float gx = 0.f, gy = 0.f, gz = 0.f;
             unsigned nm = 0;
+            const float jx = FRAME ? (float)(pj.x - p0.x) * sx : 0.f;
+            const float jy = FRAME ? (float)(pj.y - p0.y) * sy : 0.f;
+            const float jz = FRAME ? (float)(pj.z - p0.z) * sz : 0.f;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii)
                 if ((m >> ii) & 1u) {
-                    float r2;
-                    pair_term<MODE>(si[warp][ii], sti[warp][ii], pj, tj, sx, sy, sz, rr2, rl2, inv_h, h, nsplm1,
-                                    sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
+                    float r2, dx, dy, dz, qq;
+                    if (FRAME) {
+                        const float4 pi = sif[warp][ii];
+                        dx = pi.x - jx; dy = pi.y - jy; dz = pi.z - jz;
+                        qq = pi.w * __int_as_float(pj.w);
+                    } else {
+                        const int4 pi = si[warp][ii];
+                        dx = (float)(pi.x - pj.x) * sx; dy = (float)(pi.y - pj.y) * sy;
+                        dz = (float)(pi.z - pj.z) * sz;
+                        qq = __int_as_float(pi.w) * __int_as_float(pj.w);
+                    }
+                    pair_term<MODE, !FRAME>(dx, dy, dz, qq, sti[warp][ii] + tj, rr2, rl2, inv_h, h, nsplm1, sf, sp,
+                                            slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
                     if (PRUNE) nm |= r2 < rp2 ? 1u << ii : 0u;
                 }
+            if (FRAME && MODE == PM_TENS && m) {     // j's share of sum F (x) x (frame coordinates)
+                wc[0] = fmaf(gx, jx, wc[0]); wc[1] = fmaf(gx, jy, wc[1]); wc[2] = fmaf(gx, jz, wc[2]);
+                wc[3] = fmaf(gy, jy, wc[3]); wc[4] = fmaf(gy, jz, wc[4]); wc[5] = fmaf(gz, jz, wc[5]);
+            }
             if (m) {
                 unsigned long long* fj = (unsigned long long*)fs0 + sj;
                 atomicAdd(fj, (unsigned long long)__float2ll_rn(gx * (float)PGK_FORCE_SCALE));
@@ -276,6 +303,11 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
+            if (FRAME && MODE == PM_TENS && lane == ii) {      // cluster atom's share of sum F (x) x
+                const float4 pi = sif[warp][ii];
+                wc[0] = fmaf(fx, pi.x, wc[0]); wc[1] = fmaf(fx, pi.y, wc[1]); wc[2] = fmaf(fx, pi.z, wc[2]);
+                wc[3] = fmaf(fy, pi.y, wc[3]); wc[4] = fmaf(fy, pi.z, wc[4]); wc[5] = fmaf(fz, pi.z, wc[5]);
+            }
             if (lane == ii) {     // padding slots get zero sums (no mask bits)
                 unsigned long long* fi = (unsigned long long*)fs0 + 8 * cl + ii;
                 atomicAdd(fi, (unsigned long long)__double2ll_rn((double)fx * PGK_FORCE_SCALE));
@@ -486,18 +518,36 @@ __global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __re
     if (vx | vy | vz) { fsort[s] = 0; fsort[s + fst] = 0; fsort[s + 2 * (size_t)fst] = 0; }
 }
 
-template <int MODE>
-static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
+template <int MODE, bool FRAME>
+static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a, int blocks) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-    smem_limit(k_pair_mixed<MODE, false>, sm);
-    k_pair_mixed<MODE, false><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+    smem_limit(k_pair_mixed<MODE, false, FRAME>, sm);
+    k_pair_mixed<MODE, false, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
     PGK_LAUNCHED(c);
     if (a.P) {
-        smem_limit(k_pair_mixed<MODE, true>, sm);
-        k_pair_mixed<MODE, true><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+        smem_limit(k_pair_mixed<MODE, true, FRAME>, sm);
+        k_pair_mixed<MODE, true, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
         PGK_LAUNCHED(c);
     }
+}
+
+// The cluster frame is exact when no cluster atom or listed j, taken as its
+// minimum image from cluster atom 0, can lie half a box away: cluster atoms
+// stay within a list cell (plus drift), listed j within rcut_book (plus drift)
+// of a cluster atom.
+static bool frame_ok(const pgk_ctx* c) {
+    const DynState& h = c->hdyn;
+    double cs = 0.0, lmin = 1e300;
+    for (int d = 0; d < 3; ++d) { cs = std::max(cs, h.cellsize[d]); lmin = std::min(lmin, h.box[d]); }
+    if (h.list_mode_used != PGK_LIST_CELL) return false;
+    return 0.5 * lmin > std::sqrt(3.0) * cs + c->prm.rcut_book + 4.0;
+}
+
+template <int MODE>
+static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
+    if (frame_ok(c) && !c->no_frame) pair_mixed_launch2<MODE, true>(c, a, blocks);
+    else pair_mixed_launch2<MODE, false>(c, a, blocks);
     k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
     if (a.P) {
         const size_t sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each

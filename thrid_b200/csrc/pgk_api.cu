@@ -507,6 +507,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         // pruned list buffer (mixed): PGK_PRUNE_BUFFER overrides the 1 A default; 0
         // disables pruning, as does a book skin too thin for the buffer
         if (c->mixed()) {
+            const char* pf = getenv("PGK_PAIR_FRAME");
+            c->no_frame = pf && atoi(pf) == 0;
             const char* pb = getenv("PGK_PRUNE_BUFFER");
             const double buf = pb ? atof(pb) : 1.0;
             const double rmax = std::max(p->rcut, p->rrcut);

@@ -126,6 +126,7 @@ struct pgk_ctx {
     int4* xq_prune = nullptr;     // xq at the last prune
     PruneDev* prune = nullptr;
     float prune_buffer = 0.f;     // A; 0 = no pruning (pair kernel reads the book rows)
+    bool no_frame = false;        // PGK_PAIR_FRAME=0: always the per-pair minimum image
     int ccap = 0;
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
     long long* fsort = nullptr;   // mixed: pair forces by sorted slot, [3][npad_cap] int64 fixed point (kept zero between uses)
