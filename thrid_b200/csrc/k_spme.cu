@@ -368,7 +368,9 @@ __device__ __forceinline__ float conv_point_f(int k1, int k2, int k3, int K1, in
 
 // AXIS 0: pencils along x (contiguous); 1: along y; 2: along z.
 // SRC: 0 = complex grid in place, 1 = int64 fixed-point accumulation grid,
-//      2 = double accumulation grid (both real, first forward pass).
+//      2 = double accumulation grid (both real, first forward pass),
+//      3 = complex grid in, real part out to the real grid `acc` (last
+//      backward pass; the gather reads only the real part).
 // CONV (AXIS 2 only): forward z transform, influence function (scalar_sum)
 //      and backward z transform in one pass over the grid.
 template <typename T, int AXIS, int SRC, int NC, bool CONV>
@@ -413,7 +415,7 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         v.x = 0; v.y = 0;
         if (pg < npen_total) {
             const size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
-            if (SRC == 0) v = data[off];
+            if (SRC == 0 || SRC == 3) v = data[off];
             else if (SRC == 1) v.x = (T)((double)((const long long*)acc)[off] * PGK_GRID_ISCALE);
             else v.x = (T)((const double*)acc)[off];
         }
@@ -487,7 +489,8 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
         int pg = AXIS == 0 ? blockIdx.x * P + p : x0 + p;
         if (pg < npen_total) {
             size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
-            data[off] = src[p * ld + m];
+            if (SRC == 3) ((T*)acc)[off] = src[p * ld + m].x;     // real part only (what the gather reads)
+            else data[off] = src[p * ld + m];
         }
     }
 }
@@ -635,7 +638,7 @@ __global__ void __launch_bounds__(256) k_gather_rows(const double* __restrict__ 
             t0 = q == i1 ? th[0][q] : t0;
             d0 = q == i1 ? dth[0][q] : d0;
         }
-        const T2* Q = (const T2*)qc;
+        const T* Q = (const T*)qc;       // real grid
         const T q = (T)chrg[a];
         int i = base[0] - P + 1 + i1; i = i < 0 ? i + K1 : i;
 #pragma unroll
@@ -644,7 +647,7 @@ __global__ void __launch_bounds__(256) k_gather_rows(const double* __restrict__ 
 #pragma unroll
             for (int i2 = 0; i2 < P; ++i2) {
                 int j = base[1] - P + 1 + i2; j = j < 0 ? j + K2 : j;
-                const T term = q * Q[(size_t)K1 * (j + (size_t)K2 * k) + i].x;
+                const T term = q * Q[(size_t)K1 * (j + (size_t)K2 * k) + i];
                 f0 = f0 - (T)K1 * term * d0 * th[1][i2] * th[2][i3];
                 f1 = f1 - (T)K2 * term * t0 * dth[1][i2] * th[2][i3];
                 f2 = f2 - (T)K3 * term * t0 * th[1][i2] * dth[2][i3];
@@ -703,6 +706,8 @@ pgk_status spme_setup(pgk_ctx* c) {
     size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
     PGK_CUDA(c, cudaMalloc(&c->qacc, KK * 8));
     PGK_CUDA(c, cudaMalloc(&c->qc, KK * (c->mixed() ? sizeof(float2) : sizeof(double2))));
+    PGK_CUDA(c, cudaMalloc(&c->qr, KK * (c->mixed() ? sizeof(float) : sizeof(double))));
+    PGK_CUDA(c, cudaMemset(c->qr, 0, KK * (c->mixed() ? sizeof(float) : sizeof(double))));
     // B-spline moduli (DFTMOD, fft_pme_init.F90:263-289)
     double arr[16], darr[16];
     fill_bspline_h(0.0, c->order, arr, darr);
@@ -755,8 +760,8 @@ template <typename T, int AXIS, int SRC, int NC, bool CONV>
 static void fft_launch(pgk_ctx* c, const FftDev& fd, int grid, int P, size_t sm, int sign, const ConvArgs& ca) {
     typedef typename C2<T>::t T2;
     smem_limit(k_fft<T, AXIS, SRC, NC, CONV>, sm);
-    k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, c->qacc, c->K[0], c->K[1], c->K[2], fd, P,
-                                                            (T)sign, ca, c->dyn);
+    k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, SRC == 3 ? c->qr : c->qacc, c->K[0], c->K[1],
+                                                            c->K[2], fd, P, (T)sign, ca, c->dyn);
 }
 
 template <typename T, int AXIS, int SRC, bool CONV = false>
@@ -816,7 +821,7 @@ static pgk_status fft_convolve(pgk_ctx* c, long long* acc, int want) {
     if ((s = fft_pass<T, 1, 0>(c, -1))) return s;
     if ((s = fft_pass<T, 2, 0, true>(c, -1, &ca))) return s;
     if ((s = fft_pass<T, 1, 0>(c, +1))) return s;
-    return fft_pass<T, 0, 0>(c, +1);
+    return fft_pass<T, 0, 3>(c, +1);
 }
 
 template <bool MIXED, int P>
@@ -829,7 +834,7 @@ static void spread_gather(pgk_ctx* c, bool gather, int group) {
                                                                     c->K[2], c->qacc, order);
     else
         k_gather_rows<MIXED, P><<<(warps + 7) / 8, 256, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1],
-                                                                    c->K[2], c->qc, c->facc[group], order);
+                                                                    c->K[2], c->qr, c->facc[group], order);
     PGK_LAUNCHED(c);
 }
 

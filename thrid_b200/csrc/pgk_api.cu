@@ -560,7 +560,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
                     c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
-                    c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->bsp,
+                    c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->qr, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->cg_fit, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
@@ -765,7 +765,7 @@ void* pgk_stream(const pgk_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 // ---- stage drivers ---------------------------------------------------------------
 static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
-                               bool tens, bool hfs, bool lt);
+                               bool tens, bool hfs, bool lt, bool ke_ready);
 
 // kind: 0 NVE (moldyn.F90), 1 NHC (moldyn_nhc.F90), 2 MTK (moldyn_mtk.F90),
 // 3 NVE + region Langevin + heat flux (moldyn_hf.F90); hf records go to the
@@ -784,8 +784,12 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     const long long per = (long long)c->hfp.nhfregion * PGK_HF_NCOL;
     long long nr = 0;
     long long last_rec = -1;
+    // ke_ready: the kinetic sums of the current velocities are in the
+    // accumulators (the previous step of this run ended with them), so the
+    // step's first chain half reuses them instead of summing again
+    bool ke_ready = false;
     auto step_body = [&](int64_t st, bool e_, bool v_, bool t_, bool h_, bool l_) {
-        return md_step_body(c, kind, st, md, e_, v_, t_, h_, l_);
+        return md_step_body(c, kind, st, md, e_, v_, t_, h_, l_, ke_ready);
     };
     pgk_status s;
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
@@ -803,10 +807,11 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             RUN(force_group(c, PGK_MTS_SHORT, ene || vir, vir, tens));
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
+            ke_ready = mtk;
         } else if (c->use_graphs && c->list_valid && !hfs && !lt) {
             // the step's kernel sequence depends only on (ene, vir, tens) and the
             // list build; replay a captured CUDA graph of it
-            const int key = 8 * kind + ((ene ? 1 : 0) | (vir ? 2 : 0) | (tens ? 4 : 0));
+            const int key = 16 * kind + ((ene ? 1 : 0) | (vir ? 2 : 0) | (tens ? 4 : 0) | (ke_ready ? 8 : 0));
             if (memcmp(&c->graph_md, md, sizeof(pgk_mdparams)) != 0) {
                 for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
                 c->graphs.clear();
@@ -866,6 +871,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
         } else {
             RUN(step_body(step, ene, vir, tens, hfs, lt));
         }
+        if (step > 0) ke_ready = kind == 1 || kind == 2;
         if (step > 0) {
             if (lt) { RUN(launch_lt_regist(c)); RUN(launch_langevin(c, md->dt_long_cal, step, false)); }
             if (hfs) {
@@ -898,7 +904,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
 // one MD step (step > 0) of run_md: the thermostat / barostat half steps and
 // the XO-RESPA loop with its force evaluations
 static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
-                               bool tens, bool hfs, bool lt) {
+                               bool tens, bool hfs, bool lt, bool ke_ready) {
     const double dts = md->dt_long_cal / (double)md->nstep_short;
     const bool rattle = md->ifrattle && c->ncgroup > 0;
     const bool mtk = kind == 2;
@@ -911,7 +917,7 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
     const int kshort = c->short_empty ? 0 : KD_SHORT;
     if (lt) RUN(launch_langevin(c, md->dt_long_cal, step, true));
     if (kind == 1 || kind == 2) {
-        RUN(launch_kinetic(c, 0));
+        if (!ke_ready) RUN(launch_kinetic(c, 0));
         RUN(launch_chain_coeffs(c, chain_kind, hfdrv ? 0 : kind, *md));
     } else {
         RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));

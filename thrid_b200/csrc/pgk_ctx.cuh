@@ -143,6 +143,7 @@ struct pgk_ctx {
     int order = 0;
     void* qacc = nullptr;         // accumulation grid (int64 fixed / double)
     void* qc = nullptr;           // complex grid (float2 / double2)
+    void* qr = nullptr;           // real part after the backward transform (float / double), read by the gather
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
 
