@@ -236,6 +236,56 @@ __global__ void __launch_bounds__(256) k_build_clist(
     unsigned long long npair = 0;
     unsigned up = 0;                                   // bit ii: cluster atom ii has a higher-index partner
     int* row = clist + (size_t)cl * ccap;
+    // Candidates that pass the bounding-box test queue up (in scan order) and
+    // are tested against the 8 cluster atoms 32 at a time, so the exact tests
+    // run on full warps.  Entries come out in the same order as a direct scan.
+    __shared__ int squeue[8][32 + 4 * 32];
+    int* queue = squeue[wib];
+    int qn = 0;
+    auto test_batch = [&](int t) {          // t < 0: idle lane
+        unsigned mask = 0;
+        if (t >= 0) {
+            const double xj = pos_s[3 * t], yj = pos_s[3 * t + 1], zj = pos_s[3 * t + 2];
+            const float pjf[3] = {(float)xj, (float)yj, (float)zj};
+            const int jo = perm[t];
+            bool jlow = false;
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii) {
+                const int io = sio[wib][ii];
+                if (io < 0 || t <= s0 + ii) continue;
+                float q2 = 0.f;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    float r = (float)spi[wib][3 * ii + d] - pjf[d];
+                    r -= Lf[d] * rintf(r * Bf[d]);
+                    q2 = fmaf(r, r, q2);
+                }
+                if (q2 > sqhi) continue;
+                bool in = q2 < sqlo;
+                if (!in) {       // near rcut_book: the reference's exact FP64 test decides
+                    double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L[0], B[0]);
+                    double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L[1], B[1]);
+                    double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
+                    double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)), __dmul_rn(r2, r2));
+                    in = dr < sqcut;
+                }
+                const int2 rg = srng[wib][ii];
+                if (in && !(jo >= rg.x && jo <= rg.y && is_excluded(exs_idx, exs_list, io, jo))) {
+                    mask |= 1u << ii;
+                    if (jo > io) up |= 1u << ii;
+                    else jlow = true;
+                }
+            }
+            if (jlow) hasup[jo] = 1;
+            npair += (unsigned long long)__popc(mask);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, mask != 0);
+        if (mask) {
+            const int off = count + __popc(m & ((1u << lane) - 1u));
+            if (off < ccap) row[off] = (int)((mask << 24) | (unsigned)t);
+        }
+        count += __popc(m);
+    };
     for (int a = 0; a < nz; ++a) {
         int z = nc2 >= 3 ? (cz + a - 1 + nc2) % nc2 : a;
         for (int b = 0; b < ny; ++b) {
@@ -246,65 +296,54 @@ __global__ void __launch_bounds__(256) k_build_clist(
                 int t0 = cell_start[cell], t1 = t0 + cell_cnt[cell];
                 if (t1 <= s0 + 1) continue;             // every slot of the cell is below the cluster
                 t0 = max(t0, s0 + 1);
-                for (int tb = t0; tb < t1; tb += 32) {
-                    int t = tb + lane;
-                    unsigned mask = 0;
-                    if (t < t1) {
-                        const double xj = pos_s[3 * t], yj = pos_s[3 * t + 1], zj = pos_s[3 * t + 2];
-                        const float pjf[3] = {(float)xj, (float)yj, (float)zj};
-                        float e2 = 0.f;
+                for (int tb = t0; tb < t1; tb += 128) {
+                    // four candidates a lane: their positions load together
+                    double px[4][3];
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            float r = pjf[d] - ctrf[d];
-                            r -= Lf[d] * rintf(r * Bf[d]);
-                            const float ex = fmaxf(fabsf(r) - hwf[d], 0.f);
-                            e2 += ex * ex;
-                        }
-                        if (e2 <= rb2f) {
-                            const int jo = perm[t];
-                            bool jlow = false;
+                    for (int u = 0; u < 4; ++u) {
+                        const int t = tb + 32 * u + lane;
 #pragma unroll
-                            for (int ii = 0; ii < 8; ++ii) {
-                                const int io = sio[wib][ii];
-                                if (io < 0 || t <= s0 + ii) continue;
-                                float q2 = 0.f;
+                        for (int d = 0; d < 3; ++d) px[u][d] = t < t1 ? pos_s[3 * t + d] : 0.0;
+                    }
 #pragma unroll
-                                for (int d = 0; d < 3; ++d) {
-                                    float r = (float)spi[wib][3 * ii + d] - pjf[d];
-                                    r -= Lf[d] * rintf(r * Bf[d]);
-                                    q2 = fmaf(r, r, q2);
-                                }
-                                if (q2 > sqhi) continue;
-                                bool in = q2 < sqlo;
-                                if (!in) {       // near rcut_book: the reference's exact FP64 test decides
-                                    double r0 = mi_exact(__dsub_rn(spi[wib][3 * ii], xj), L[0], B[0]);
-                                    double r1 = mi_exact(__dsub_rn(spi[wib][3 * ii + 1], yj), L[1], B[1]);
-                                    double r2 = mi_exact(__dsub_rn(spi[wib][3 * ii + 2], zj), L[2], B[2]);
-                                    double dr = __dadd_rn(__dadd_rn(__dmul_rn(r0, r0), __dmul_rn(r1, r1)),
-                                                          __dmul_rn(r2, r2));
-                                    in = dr < sqcut;
-                                }
-                                const int2 rg = srng[wib][ii];
-                                if (in &&
-                                    !(jo >= rg.x && jo <= rg.y && is_excluded(exs_idx, exs_list, io, jo))) {
-                                    mask |= 1u << ii;
-                                    if (jo > io) up |= 1u << ii;
-                                    else jlow = true;
-                                }
+                    for (int u = 0; u < 4; ++u) {
+                        const int t = tb + 32 * u + lane;
+                        bool acc = false;
+                        if (t < t1) {
+                            float e2 = 0.f;
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) {
+                                float r = (float)px[u][d] - ctrf[d];
+                                r -= Lf[d] * rintf(r * Bf[d]);
+                                const float ex = fmaxf(fabsf(r) - hwf[d], 0.f);
+                                e2 += ex * ex;
                             }
-                            if (jlow) hasup[jo] = 1;
-                            npair += (unsigned long long)__popc(mask);
+                            acc = e2 <= rb2f;
                         }
+                        const unsigned ba = __ballot_sync(0xffffffffu, acc);
+                        if (acc) queue[qn + __popc(ba & ((1u << lane) - 1u))] = t;
+                        qn += __popc(ba);
                     }
-                    unsigned m = __ballot_sync(0xffffffffu, mask != 0);
-                    if (mask) {
-                        int off = count + __popc(m & ((1u << lane) - 1u));
-                        if (off < ccap) row[off] = (int)((mask << 24) | (unsigned)t);
+                    __syncwarp();
+                    while (qn >= 32) {
+                        const int tq = queue[lane];
+                        int rest[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) rest[u] = qn - 32 > 32 * u + lane ? queue[32 + 32 * u + lane] : -1;
+                        __syncwarp();
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) if (rest[u] >= 0) queue[32 * u + lane] = rest[u];
+                        qn -= 32;
+                        __syncwarp();
+                        test_batch(tq);
                     }
-                    count += __popc(m);
                 }
             }
         }
+    }
+    if (qn > 0) {
+        const int tq = lane < qn ? queue[lane] : -1;
+        test_batch(tq);
     }
     // Group the row's entries by mask (stable counting sort in shared memory):
     // 32 consecutive entries then mostly share one mask, so the pair kernel's
