@@ -256,7 +256,8 @@ def roofline(eng):
     clk = peaks.get("sm_max_mhz", 1965.0)
     peak = 148 * 128 * 2 * clk * 1e6 / 1e12           # FP32 CUDA-core FMA peak at the max SM clock
     traffic = profiled_traffic()
-    return {"kernel": "k_pair_mixed<PM_TENS>", "bound": "fp32", "achieved": achieved, "peak": peak,
+    return {"kernel": "k_pair_mixed<PM_TENS> (regular instance on the pruned rows)", "bound": "fp32",
+            "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
             "peak_source": f"nominal FP32 FMA peak 148 SM x 128 lanes x 2 x {clk:.0f} MHz "
                            "(MEASURED_PEAKS.json has no FP32 CUDA-core figure)",
