@@ -100,11 +100,26 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
         if ((s = launch_pair(c, g, vmode))) return s;
     }
-    if (c->prm.ifspme && c->prm.mts_ewk == flag)
-        if ((s = launch_spme(c, g, ene, vir))) return s;
     int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
                (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
                (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (c->prm.mts_vdw == flag ? 32 : 0);
+    const bool spme = c->prm.ifspme && c->prm.mts_ewk == flag;
+    if (spme && mask && c->st2) {
+        // bonded terms on the second stream beside the SPME chain (both latency
+        // bound); the pair forces are already in the accumulator
+        PGK_CUDA(c, cudaEventRecord(c->ev_fork, c->st));
+        PGK_CUDA(c, cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+        cudaStream_t main_st = c->st;
+        c->st = c->st2;
+        s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+        c->st = main_st;
+        if (s) return s;
+        PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
+        if ((s = launch_spme(c, g, ene, vir))) return s;
+        PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
+        return PGK_OK;
+    }
+    if (spme && (s = launch_spme(c, g, ene, vir))) return s;
     return launch_intra(c, g, mask, ene || vir, vir && tensor_only);
 }
 
@@ -239,6 +254,12 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return PGK_E_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        pgk_free(c);
+        return PGK_E_CUDA;
+    }
     c->degfree = s->degfree_all;
     pgk_status st;
 #define TRY(x) do { if ((st = (x)) != PGK_OK) { pgk_free(c); return st; } } while (0)
@@ -566,6 +587,9 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};
     for (void* b : bufs) if (b) cudaFree(b);
+    if (c->st2) { cudaStreamSynchronize(c->st2); cudaStreamDestroy(c->st2); }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return PGK_OK;

@@ -36,6 +36,11 @@ struct pgk_ctx {
     bool mixed() const { return prec == PGK_PREC_MIXED; }
     pgk_params prm{};
     cudaStream_t st = nullptr;
+    // second stream of the force evaluation: the bonded terms run on it beside
+    // the SPME chain (fork and join through the two events; integer or FP64
+    // atomics on the shared force and energy accumulators commute)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
     int nsm = 148;
