@@ -504,16 +504,18 @@ __global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, con
     }
 }
 
-// sorted-slot pair forces -> the group accumulator (one thread per slot: the
-// atom's only writer here), leaving the slot buffer zero for the next call
+// sorted-slot pair forces -> the group accumulator, leaving the slot buffer
+// zero for the next call
 __global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __restrict__ perm, int npad,
                          long long* __restrict__ facc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= npad) return;
     const int i = perm[s];
     const long long vx = fsort[s], vy = fsort[s + fst], vz = fsort[s + 2 * (size_t)fst];
-    if (i >= 0 && (vx | vy | vz)) {
-        facc[3 * (size_t)i] += vx; facc[3 * (size_t)i + 1] += vy; facc[3 * (size_t)i + 2] += vz;
+    if (i >= 0 && (vx | vy | vz)) {     // atomic: other force kernels may run beside it
+        atomicAdd((unsigned long long*)facc + 3 * (size_t)i, (unsigned long long)vx);
+        atomicAdd((unsigned long long*)facc + 3 * (size_t)i + 1, (unsigned long long)vy);
+        atomicAdd((unsigned long long*)facc + 3 * (size_t)i + 2, (unsigned long long)vz);
     }
     if (vx | vy | vz) { fsort[s] = 0; fsort[s + fst] = 0; fsort[s + 2 * (size_t)fst] = 0; }
 }
@@ -548,20 +550,32 @@ template <int MODE>
 static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
     if (frame_ok(c) && !c->no_frame) pair_mixed_launch2<MODE, true>(c, a, blocks);
     else pair_mixed_launch2<MODE, false>(c, a, blocks);
-    k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(a.fsort, a.fstride, c->perm, c->npad, (long long*)a.facc);
-    if (a.P) {
+}
+
+// After the mixed pair kernel: the sorted-slot forces into the group
+// accumulator and, after a prune step, the mask regrouping of the pruned
+// rows.  Runs on the context's current stream (the force evaluation may put
+// it beside the SPME chain: the accumulator adds are atomic).
+pgk_status launch_pair_finish(pgk_ctx* c, int group) {
+    if (c->ncl <= 0 || !c->mixed()) return PGK_OK;
+    k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(c->fsort, c->npad_cap, c->perm, c->npad,
+                                                       (long long*)c->facc[group]);
+    PGK_LAUNCHED(c);
+    if (c->prune_buffer > 0.f) {
         const size_t sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each
         if (sort_sm <= 160 * 1024 && smem_limit(k_prune_sort, sort_sm) == cudaSuccess) {
-            PGK_LAUNCHED(c);
             const long long threads = (long long)c->ncl * 32;
             k_prune_sort<<<(unsigned)((threads + 127) / 128), 128, sort_sm, c->st>>>(c->plist, c->pcnt, c->ccap,
                                                                                      c->ncl, c->prune);
+            PGK_LAUNCHED(c);
         }
     }
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
 }
 
 // vmode: PM_FORCE / PM_ENE / PM_TENS / PM_FULL (see above)
-pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
+pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
     if (c->ncl <= 0) return PGK_OK;
     PairArgs a;
     a.clist = c->clist; a.ccnt = c->ccnt; a.ccap = c->ccap; a.ncl = c->ncl;
@@ -606,10 +620,10 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode) {
             smem_limit(k_pair_fp64<false>, sm);
             k_pair_fp64<false><<<blocks, 256, sm, c->st>>>(c->xq64, a, c->lj64, c->spl64, c->dyn);
         }
+        PGK_LAUNCHED(c);
     }
-    PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
+    return finish ? launch_pair_finish(c, group) : PGK_OK;
 }
 
 // ---- diagnostic: unique pairs inside the interaction cutoff, list entries ----

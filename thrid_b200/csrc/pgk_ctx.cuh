@@ -224,7 +224,10 @@ pgk_status launch_pack(pgk_ctx* c);
 #define PM_ENE 1
 #define PM_TENS 2
 #define PM_FULL 3
-pgk_status launch_pair(pgk_ctx* c, int group, int vmode);
+// finish = false: the caller launches launch_pair_finish itself (mixed: the
+// sorted-slot forces into the accumulator, the pruned-row regrouping)
+pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish = true);
+pgk_status launch_pair_finish(pgk_ctx* c, int group);
 pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir);
 pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long long* nbits = nullptr);
 
