@@ -12,38 +12,10 @@
 
 #include "pgk_ctx.cuh"
 
-template <bool MIXED>
-__global__ void k_kick_long(double* __restrict__ vel, const void* __restrict__ fl, const double* __restrict__ mass,
-                            int n, const DynState* __restrict__ dyn) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * n) return;
-    int d = k % 3;
-    double a = force_get<MIXED>(fl, k) / mass[k / 3];
-    vel[k] = vel[k] * dyn->kl_s[d] + a * dyn->kl_b[d];
-}
-
-template <bool MIXED>
-__global__ void k_kick_short(double* __restrict__ vel, const void* __restrict__ fs, const double* __restrict__ mass,
-                             int n, const DynState* __restrict__ dyn) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * n) return;
-    double a = force_get<MIXED>(fs, k) / mass[k / 3];
-    vel[k] = vel[k] + dyn->ks_b * a;
-}
-
-__global__ void k_drift(double* __restrict__ pos, double* __restrict__ old, const double* __restrict__ vel, int n,
-                        const DynState* __restrict__ dyn, int save) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * n) return;
-    int d = k % 3;
-    double x = pos[k];
-    if (save) old[k] = x;
-    pos[k] = x * dyn->dr_a[d] + vel[k] * dyn->dr_b[d];
-}
-
-// Kicks and drift of one short step in one pass over the atoms (the same
-// arithmetic as k_kick_long, k_kick_short and k_drift, in the order the KD_*
-// flags give).
+// Kicks and drift of one short step in one pass over the atoms (moldyn*.F90
+// array statements): long kick v = v*kl_s + (F_long/m)*kl_b, short kick
+// v = v + ks_b*(F_short/m), drift x = x*dr_a + v*dr_b, in the order the KD_*
+// flags give (coefficients from the chain kernels in DynState).
 template <bool MIXED>
 __global__ void k_kick_drift(double* __restrict__ vel, double* __restrict__ pos, double* __restrict__ old,
                              const void* __restrict__ fl, const void* __restrict__ fs,
@@ -451,10 +423,6 @@ __global__ void k_box(DynState* __restrict__ dyn, ChainDev* __restrict__ chain, 
     if (a.update_rk) dyn->rkcut = rkcut_of(b, a.nfft1, a.nfft2, a.nfft3);
 }
 
-__global__ void k_rkcut(DynState* __restrict__ dyn, int n1, int n2, int n3) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) dyn->rkcut = rkcut_of(dyn->box, n1, n2, n3);
-}
-
 // calpress, atomic branch: pint / pintt of the current state from the kinetic
 // sums and both groups' virials (+ self and net-charge terms)
 struct PressArgs { double pot_ewc, netchrgsq, alpha; int ifspme, ifnetqcorrp, dbl; };
@@ -519,24 +487,6 @@ pgk_status launch_zero_group(pgk_ctx* c, int g) {
     return PGK_OK;
 }
 
-pgk_status launch_kick_long(pgk_ctx* c) {
-    int n3 = 3 * c->natom;
-    if (c->mixed()) k_kick_long<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[0], c->mass, c->natom, c->dyn);
-    else k_kick_long<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[0], c->mass, c->natom, c->dyn);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
-pgk_status launch_kick_short(pgk_ctx* c) {
-    int n3 = 3 * c->natom;
-    if (c->mixed()) k_kick_short<true><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
-    else k_kick_short<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->facc[1], c->mass, c->natom, c->dyn);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
 pgk_status launch_kick_drift(pgk_ctx* c, int flags) {
     if (!flags) return PGK_OK;
     const int n3 = 3 * c->natom;
@@ -546,14 +496,6 @@ pgk_status launch_kick_drift(pgk_ctx* c, int flags) {
     else
         k_kick_drift<false><<<(n3 + 255) / 256, 256, 0, c->st>>>(c->vel, c->pos, c->pos_old, c->facc[0], c->facc[1],
                                                                 c->mass, c->natom, c->dyn, flags);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
-pgk_status launch_drift(pgk_ctx* c, bool save_old) {
-    int n3 = 3 * c->natom;
-    k_drift<<<(n3 + 255) / 256, 256, 0, c->st>>>(c->pos, c->pos_old, c->vel, c->natom, c->dyn, save_old ? 1 : 0);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -801,13 +743,6 @@ pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md, bool 
     a.nfft1 = c->prm.nfft1; a.nfft2 = c->prm.nfft2; a.nfft3 = c->prm.nfft3;
     a.update_rk = (with_rkcut || c->prm.mts_ewk == PGK_MTS_SHORT) ? 1 : 0;
     k_box<<<1, 32, 0, c->st>>>(c->dyn, c->chain, a, c->status);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
-pgk_status launch_rkcut(pgk_ctx* c) {
-    k_rkcut<<<1, 32, 0, c->st>>>(c->dyn, c->prm.nfft1, c->prm.nfft2, c->prm.nfft3);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;

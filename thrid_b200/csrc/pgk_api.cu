@@ -25,7 +25,6 @@ cudaError_t smem_limit(const void* kernel, size_t bytes) {
     return e;
 }
 
-pgk_status launch_rkcut(pgk_ctx* c);
 pgk_status spme_bench(pgk_ctx* c, int which);
 
 pgk_status pgk_fail(pgk_ctx* c, pgk_status s, const std::string& msg) {

@@ -253,9 +253,6 @@ pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h);   // k_bonded.cu
 
 // ---- launchers (k_integrate.cu) ----
 pgk_status launch_zero_group(pgk_ctx* c, int group);
-pgk_status launch_kick_long(pgk_ctx* c);
-pgk_status launch_kick_short(pgk_ctx* c);
-pgk_status launch_drift(pgk_ctx* c, bool save_old);
 // k_kick_drift flags: KD_LONG long kick, KD_SHORT short kick, KD_SHORT_FIRST
 // short kick before the long one (second half step), KD_DRIFT drift, KD_SAVE
 // keep the positions before the drift (RATTLE)
