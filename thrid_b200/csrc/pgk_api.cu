@@ -89,42 +89,41 @@ pgk_status read_status(pgk_ctx* c) {
 
 // one MTS group of calforce (calforce.F90:8-1073); tensor_only selects the
 // pair kernel's combined-tensor mode (anisotropic MTK steps without output)
+// Two streams: the SPME chain runs on the second stream beside the pair
+// kernel, its finishing kernels and the bonded terms (the pair kernel is
+// issue-bound, the SPME kernels latency-bound, so they fill each other's idle
+// issue slots).  Every add into the shared force and energy accumulators is
+// atomic (int64 in mixed precision: exact and independent of the interleaving).
 pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_only = false) {
     int g = flag == PGK_MTS_LONG ? 0 : 1;
     pgk_status s;
-    bool pair_pending = false;          // launch_pair_finish still to run
     if ((s = launch_zero_group(c, g))) return s;
-    if (c->prm.mts_vdw == flag) {
-        if (!c->list_valid && (s = launch_mklist(c))) return s;
-        if ((s = launch_pack(c))) return s;
-        int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
-        if ((s = launch_pair(c, g, vmode, false))) return s;
-        pair_pending = true;
-    }
-    int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
-               (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
-               (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (c->prm.mts_vdw == flag ? 32 : 0);
+    const bool pairs = c->prm.mts_vdw == flag;
+    if (pairs && !c->list_valid && (s = launch_mklist(c))) return s;
+    const int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
+                     (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
+                     (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (pairs ? 32 : 0);
     const bool spme = c->prm.ifspme && c->prm.mts_ewk == flag;
-    if (spme && mask && c->st2) {
-        // the pair kernel's finishing kernels and the bonded terms on the
-        // second stream beside the SPME chain (all latency bound; every add
-        // into the shared accumulators is atomic)
+    const bool fork = spme && c->st2 && (pairs || mask);
+    if (fork) {
         PGK_CUDA(c, cudaEventRecord(c->ev_fork, c->st));
         PGK_CUDA(c, cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
         cudaStream_t main_st = c->st;
         c->st = c->st2;
-        s = pair_pending ? launch_pair_finish(c, g) : PGK_OK;
-        if (!s) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+        s = launch_spme(c, g, ene, vir);
         c->st = main_st;
         if (s) return s;
         PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
-        if ((s = launch_spme(c, g, ene, vir))) return s;
-        PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
-        return PGK_OK;
     }
-    if (pair_pending && (s = launch_pair_finish(c, g))) return s;
-    if (spme && (s = launch_spme(c, g, ene, vir))) return s;
-    return launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+    if (pairs) {
+        if ((s = launch_pack(c))) return s;
+        const int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
+        if ((s = launch_pair(c, g, vmode))) return s;
+    }
+    if (spme && !fork && (s = launch_spme(c, g, ene, vir))) return s;
+    if ((s = launch_intra(c, g, mask, ene || vir, vir && tensor_only))) return s;
+    if (fork) PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
+    return PGK_OK;
 }
 
 double accv(const pgk_ctx* c, long long v) {

@@ -36,9 +36,9 @@ struct pgk_ctx {
     bool mixed() const { return prec == PGK_PREC_MIXED; }
     pgk_params prm{};
     cudaStream_t st = nullptr;
-    // second stream of the force evaluation: the bonded terms run on it beside
-    // the SPME chain (fork and join through the two events; integer or FP64
-    // atomics on the shared force and energy accumulators commute)
+    // second stream of the force evaluation: the SPME chain runs on it beside
+    // the pair and bonded kernels (fork and join through the two events;
+    // integer or FP64 atomics on the shared force and energy accumulators)
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
