@@ -89,10 +89,10 @@ pgk_status read_status(pgk_ctx* c) {
 
 // one MTS group of calforce (calforce.F90:8-1073); tensor_only selects the
 // pair kernel's combined-tensor mode (anisotropic MTK steps without output)
-// Two streams: the SPME chain runs on the second stream beside the pair
-// kernel, its finishing kernels and the bonded terms (the pair kernel is
-// issue-bound, the SPME kernels latency-bound, so they fill each other's idle
-// issue slots).  Every add into the shared force and energy accumulators is
+// Two streams: the SPME chain and then the bonded terms run on the second
+// stream beside the pair kernel and its finishing kernels (the pair kernel is
+// issue-bound, the SPME and bonded kernels latency-bound, so they fill each
+// other's idle issue slots).  Every add into the shared force and energy accumulators is
 // atomic (int64 in mixed precision: exact and independent of the interleaving).
 pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_only = false) {
     int g = flag == PGK_MTS_LONG ? 0 : 1;
@@ -111,6 +111,7 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         cudaStream_t main_st = c->st;
         c->st = c->st2;
         s = launch_spme(c, g, ene, vir);
+        if (!s) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
         c->st = main_st;
         if (s) return s;
         PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
@@ -120,10 +121,12 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         const int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
         if ((s = launch_pair(c, g, vmode))) return s;
     }
-    if (spme && !fork && (s = launch_spme(c, g, ene, vir))) return s;
-    if ((s = launch_intra(c, g, mask, ene || vir, vir && tensor_only))) return s;
-    if (fork) PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
-    return PGK_OK;
+    if (fork) {
+        PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
+        return PGK_OK;
+    }
+    if (spme && (s = launch_spme(c, g, ene, vir))) return s;
+    return launch_intra(c, g, mask, ene || vir, vir && tensor_only);
 }
 
 double accv(const pgk_ctx* c, long long v) {
