@@ -211,15 +211,16 @@ int64_t pgk_estimate_bytes(const pgk_system* s, const pgk_params* p) {
                       std::max(1.0, std::floor(p->zcel / p->rcut_book));
     const double npad = n + 7.0 * nc;
     const double rs = p->rcut_book + 2.0;
-    double cap = 0.75 * n / vol * 4.0 / 3.0 * 3.14159265358979 * rs * rs * rs + 128;
+    double cap = (n / vol * 4.0 / 3.0 * 3.14159265358979 * rs * rs * rs + 128) * 1.25;   // rows regrow with headroom
     if (p->max_nbr > 0) cap = p->max_nbr;
+    const double rows = mixed ? 2.0 : 1.0;                                 // book + pruned rows (mixed)
     double bytes = n * (3 * 24 + 3 * 8 + 4 + 2 * 24 + 12 + 1 + 24)       // state, forces, list keys
-                 + npad * (4 + 24 + 4 + (mixed ? 16 : 32))                 // sorted copies
-                 + npad / 8.0 * (cap + 1) * 4                              // cluster rows
+                 + npad * (4 + 24 + 4 + (mixed ? 16 + 24 + 16 : 32))       // sorted copies, slot forces, prune origin
+                 + rows * npad / 8.0 * (cap + 1) * 4                       // cluster rows
                  + n * 400.0;                                              // bonded terms and incidence
     if (p->ifspme) {
         const double K = (double)p->nfft1 * p->nfft2 * p->nfft3;
-        bytes += K * (8 + (mixed ? 8 : 16));
+        bytes += K * (8 + (mixed ? 8 + 4 : 16 + 8));                       // accumulation, complex and real grids
     }
     bytes = bytes * 1.25 + 16.0 * (1 << 20);                               // regrowth margin + fixed
     return (int64_t)bytes;
