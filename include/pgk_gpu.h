@@ -359,7 +359,10 @@ pgk_status pgk_sync(pgk_ctx* ctx);
 int64_t pgk_kernel_launches(const pgk_ctx* ctx);
 
 /* CUDA stream of the context (cudaStream_t as void*), for callers that time
- * the context's kernels with their own events. */
+ * the context's kernels with their own events.  A force evaluation also uses
+ * a second, internal stream (the SPME chain and bonded terms run beside the
+ * pair kernel); its work is always joined back to this stream, so events and
+ * synchronisation on this stream cover everything the context launched. */
 void* pgk_stream(const pgk_ctx* ctx);
 
 /* Instrumentation (no reference counterpart): launch one kernel of the force
