@@ -411,6 +411,80 @@ def run_serve(args):
     }
 
 
+EWK_WORKLOAD = "water_12288_box49.66_alpha0.32_ewaldkp_hf"
+EWK_FLOPS = {"k_ewk_sfac": 16, "k_ewk_atom": 34}   # FP64 flops per (atom, wave)
+EWK_FLOPS_PER_PAIR = sum(EWK_FLOPS.values())
+FP64_NOMINAL_TFLOPS = 37.0   # B200 (HGX) datasheet FP64; no FP64 peak is measured on this pool
+
+
+def run_ewk(args):
+    """ewaldkp_hf (per-atom standard-Ewald k-space term of the bulk heat flux)
+    on 4,096 rigid waters (12,288 atoms, 49.66 A cube, alpha 0.32) at
+    kmax = --ewk-hf: device time of the whole kernel chain per evaluation;
+    the same end to end through the C ABI (positions up from host memory,
+    force, per-atom energy and tensor down); the oracle on one host core at a
+    smaller kmax, per (atom, wave) pair."""
+    import ctypes as C
+    from oracle import oracle as orc
+    from thrid_b200 import abi
+    from thrid_b200 import systems as S
+    from thrid_b200.pgk import PgkEngine
+    kmax = args.ewk_hf
+    s = S.water_box(nside=16, box=49.66)
+    eng = PgkEngine(s, dict(s.params, precision=abi.PREC_FP64))
+    ms, units = C.c_double(0.0), C.c_double(0.0)
+    launches0 = eng.kernel_launches
+    r = eng.ewaldkp_hf(kmax)
+    launches = eng.kernel_launches - launches0       # kernels of one evaluation
+    with ClockSampler(0) as clk:
+        st = eng.L.pgk_bench_kernel(eng.h, 256 + kmax, args.steps, C.byref(ms), C.byref(units), None)
+    if st:
+        raise RuntimeError(f"pgk_bench_kernel status {st}: {eng.L.pgk_last_error(eng.h)}")
+    pairs = units.value
+    kern = {}
+    for name, base in (("k_ewk_sfac", 512), ("k_ewk_atom", 768)):
+        km = C.c_double(0.0)
+        st = eng.L.pgk_bench_kernel(eng.h, base + kmax, args.steps, C.byref(km), None, None)
+        if st:
+            raise RuntimeError(f"pgk_bench_kernel status {st}: {eng.L.pgk_last_error(eng.h)}")
+        kern[name] = {"ms": km.value, "share": km.value / ms.value,
+                      "fp64_tflops": EWK_FLOPS[name] * pairs / (km.value * 1e-3) * 1e-12}
+    top = max(kern, key=lambda k: kern[k]["ms"])
+    for _ in range(args.warmup):
+        eng.upload_state(s.atmcor)
+        r = eng.ewaldkp_hf(kmax)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.upload_state(s.atmcor)
+        r = eng.ewaldkp_hf(kmax)
+    e2e = (time.perf_counter() - t0) / args.steps
+    n = s.natom
+    kc = max(2, kmax // 2)
+    o = orc.Oracle(s)
+    t0 = time.perf_counter()
+    rc = o.ewaldkp_hf(kc)
+    tc = time.perf_counter() - t0
+    dev = ms.value * 1e-3
+    return {
+        "metric": "ewaldkp_hf (atom, wave) pairs/s", "value": pairs / dev, "unit": "pairs/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms.value, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic (seeded water lattice)",
+        "config": {"workload": EWK_WORKLOAD, "natom": n, "kmax": kmax, "nwave": r["nwave"],
+                   "l2": "working set (tables 12 MB) inside L2; device timing back to back"},
+        "fp64_tflops": EWK_FLOPS_PER_PAIR * pairs / dev * 1e-12,
+        "kernels": kern,
+        "roofline": {"bound": "fp64", "kernel": top, "achieved": kern[top]["fp64_tflops"],
+                     "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                     "frac": kern[top]["fp64_tflops"] / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal (datasheet)",
+                     "traffic": None},
+        "e2e": {"value": pairs / e2e, "unit": "pairs/s", "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 8 * 13 * n + 8 * 11},
+        "cpu_baseline": {"value": n * (rc["nwave"] - 1) / tc, "unit": "pairs/s", "cores": 1, "kind": "port",
+                         "sample": f"one oracle evaluation of the same system at kmax {kc} ({rc['nwave']} waves)"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,8 +500,13 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-load", type=float, default=4.0, help="arrival rate / one-at-a-time service rate")
     ap.add_argument("--serve-seed", type=int, default=2025)
+    ap.add_argument("--ewk-hf", type=int, default=0, metavar="KMAX",
+                    help="ewaldkp_hf benchmark at this kmax instead of the main line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.ewk_hf:
+        print(json.dumps(run_ewk(args)))
+        return
     if args.serve:
         print(json.dumps(run_serve(args)))
         return

@@ -331,6 +331,38 @@ pgk_status pgk_calheatf(pgk_ctx* ctx, double* hf);
  * viri*_atm(a,3,i,r).  Either pointer may be NULL. */
 pgk_status pgk_get_hf_atm(pgk_ctx* ctx, double* pot_atm, double* viri_atm);
 
+/* ewaldkp_hf (ewaldk_hf.F90:8-304): the standard-Ewald k-space force, energy
+ * and virial with their per-atom split, which the -D_HF_BULK_EWK build runs
+ * in place of the reciprocal term on heat-flux steps (calforce_hf.F90:1046-1067),
+ * at the context's current positions and box.  Wave vectors as prepewk /
+ * upewk (prepewk.F90:100-155): integer (nx,ny,nz) != 0 with |nx| <= kmax,
+ * |ny| <= kmax*ny0, |nz| <= kmax*nz0 and nx^2 + ny^2/ny0^2 + nz^2/nz0^2 <=
+ * kmax^2, where ny0, nz0 = anint(ycel/xcel), anint(zcel/xcel) of the
+ * context's initial box (rdscript.F90:1494); K = (nx/xcel, ny/ycel, nz/zcel)
+ * at the current box.  alpha, ifnetqcorrp and (sum q)^2 come from the context.
+ * The host arrays receive this term alone (the reference's in/out arrays add
+ * it); each may be NULL:
+ *   force        (3,natom)   2 q_i / V * sum_k A(K) (bck sin_i - bsk cos_i) K,
+ *                            added by the reference to force and for_viri_coul;
+ *   pot_elc_atm  (natom)     per-atom energy, with the self term
+ *                            -alpha/sqrt(pi) q_i^2 (ewaldk_hf.F90:295-299);
+ *   virielct_atm (3,3,natom) per-atom virial tensor, [a + 3*b + 9*i] (the
+ *                            reference's region-1 slice virielct_atm(:,:,i,1)).
+ * With ifnetqcorrp every atom's tensor carries -pot_fact*A(K)*netchrgsq per
+ * wave (ewaldk_hf.F90:257-272), so the atom tensors then do not sum to the
+ * total tensor.  kmax >= 1; ny0, nz0 >= 1; at most 253 table rows
+ * (kmax*(1 + ny0 + nz0) <= 250). */
+typedef struct pgk_ewk_hf {
+    double  pot_ewk;              /* k-space energy                            */
+    double  pot_ewk_cc;           /* net-charge correction (0 without ifnetqcorrp);
+                                     pot_viri_coul += pot_ewk + pot_ewk_cc      */
+    double  pot_virit_coul[9];    /* k-space virial tensor t[a + 3*b]           */
+    int32_t nwave;                /* wave vectors, (0,0,0) included (nwave of prepewk) */
+    int32_t _pad;
+} pgk_ewk_hf;
+pgk_status pgk_ewaldkp_hf(pgk_ctx* ctx, int32_t kmax, double* force, double* pot_elc_atm,
+                          double* virielct_atm, pgk_ewk_hf* out);
+
 /* det_ene_kin of langevin_region.F90 (kinetic energy put in (+) or taken out
  * (-) per Langevin region) summed since the last call, then reset. */
 pgk_status pgk_langevin_dekin(pgk_ctx* ctx, double* det_ene_kin);
@@ -373,9 +405,12 @@ void* pgk_stream(const pgk_ctx* ctx);
  *   64 + m = the bonded terms with term mask m (bit 0 bonds, 1 angles,
  *   2 torsions, 3 RB torsions, 4 1-4 pairs, 5 excluded pairs) with energies
  *   and per-type virials, 128 + m = the same with only the total virial
- *   tensor (the anisotropic MTK step without output).
+ *   tensor (the anisotropic MTK step without output), 256 + kmax = one
+ *   ewaldkp_hf evaluation (the whole kernel chain), 512 + kmax / 768 + kmax
+ *   = its structure-factor / per-atom kernel alone (kmax < 256).
  * *units receives the algorithmic work of one launch: unique pairs inside
- * the cutoff (0), atoms (1, 2, 64+, 128+), or grid points (3); *entries the number
+ * the cutoff (0), atoms (1, 2, 64+, 128+), grid points (3), or (atom, wave)
+ * pairs without (0,0,0) (256+); *entries the number
  * of (cluster, j) list entries the pair kernel reads. */
 pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
                             double* entries);

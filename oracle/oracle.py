@@ -73,8 +73,22 @@ def lib():
         L.orc_langevin_dekin.argtypes = [vp, pd]
         L.orc_lt_regions.argtypes = [vp, pi]
         L.orc_philox.argtypes = [C.c_uint64, C.c_longlong, C.c_int, pd]
+        L.orc_ewk_nvec.argtypes = [C.c_int, C.c_double, C.c_double, pi, C.c_int, pi]
+        L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
         _lib = L
     return _lib
+
+
+def ewk_nvec(kmax, yratio=1.0, zratio=1.0):
+    """prepewk.F90:100-135 wave-vector integers (nwave, 3), (0,0,0) first."""
+    L = lib()
+    nw = C.c_int(0)
+    st = L.orc_ewk_nvec(kmax, yratio, zratio, None, 0, C.byref(nw))
+    if st:
+        raise RuntimeError(f"orc_ewk_nvec status {st}")
+    out = np.zeros((nw.value, 3), np.int32)
+    L.orc_ewk_nvec(kmax, yratio, zratio, out.ctypes.data_as(C.POINTER(C.c_int32)), nw.value, C.byref(nw))
+    return out
 
 
 def _p(a):
@@ -197,6 +211,19 @@ class Oracle:
         nr = C.c_longlong(0)
         st = self.L.orc_moldyn_hf(self.h, ini, end, C.byref(md), C.byref(e), _p(rec), cap, C.byref(nr))
         return st, e.as_dict(), rec[:min(nr.value, cap)]
+
+    def ewaldkp_hf(self, kmax):
+        """ewaldkp_hf (ewaldk_hf.F90:8-304): dict with force (N,3), pot_atm (N),
+        viri_atm (N,3,3) with viri_atm[i, b, a] = virielct_atm(a,b,i,1), the
+        scalars pot_ewk, pot_ewk_cc, pot_virit_coul (3,3) [b, a] and nwave."""
+        n = self.sys.natom
+        f = np.zeros((n, 3)); pot = np.zeros(n); vir = np.zeros((n, 3, 3)); sc = np.zeros(11)
+        nw = C.c_int(0)
+        st = self.L.orc_ewaldkp_hf(self.h, kmax, _p(f), _p(pot), _p(vir), _p(sc), C.byref(nw))
+        if st:
+            raise RuntimeError(f"orc_ewaldkp_hf status {st}")
+        return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=sc[0], pot_ewk_cc=sc[1],
+                    pot_virit_coul=sc[2:].reshape(3, 3), nwave=nw.value)
 
     def langevin_dekin(self):
         out = np.zeros(abi.LT_MAX_REGIONS)

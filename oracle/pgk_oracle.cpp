@@ -1793,6 +1793,107 @@ int moldyn_hf(Oracle& o, long long ini, long long end, const pgk_mdparams& md, p
     }
     return PGK_OK;
 }
+
+// prepewk.F90:100-135: integer wave vectors in the reference's kx, ky, kz loop
+// order, (0,0,0) first (nwave = 1 is reserved for it); yratio and zratio are
+// the initial box ratios (rdscript.F90:1494)
+int ewk_nvec(int kmax, double yratio, double zratio, std::vector<int>& nv) {
+    const int ny0 = (int)std::round(yratio), nz0 = (int)std::round(zratio);   // anint, prepewk.F90:73-76
+    if (kmax < 1 || ny0 < 1 || nz0 < 1) return PGK_E_INVALID;
+    const int yk = kmax * ny0, zk = kmax * nz0;
+    nv.assign(3, 0);
+    for (int kx = -kmax; kx <= kmax; ++kx)
+        for (int ky = -yk; ky <= yk; ++ky)
+            for (int kz = -zk; kz <= zk; ++kz) {
+                if (kx == 0 && ky == 0 && kz == 0) continue;
+                double a2 = (double)(kx * kx) + (double)(ky * ky) / (double)(ny0 * ny0) +
+                            (double)(kz * kz) / (double)(nz0 * nz0);
+                if (a2 <= (double)(kmax * kmax)) { nv.push_back(kx); nv.push_back(ky); nv.push_back(kz); }
+            }
+    return PGK_OK;
+}
+
+// ewaldkp_hf (ewaldk_hf.F90:8-304) with kwave/awave of prepewk.F90:137-155 at
+// the current box.  Outputs hold this term alone: force (3,N), pot_atm (N)
+// with the self term, viri (3,3,N) = virielct_atm(:,:,i,1), sc = pot_ewk,
+// pot_ewk_cc, pot_virit_coul(3,3).
+int ewaldkp_hf(Oracle& o, int kmax, double* force, double* pot_atm, double* viri, double* sc, int* nwave_out) {
+    std::vector<int> nv;
+    int s = ewk_nvec(kmax, o.prm.ycel / o.prm.xcel, o.prm.zcel / o.prm.xcel, nv);
+    if (s) return s;
+    const int n = o.natom, nwave = (int)nv.size() / 3;
+    const double pi = std::acos(-1.0), pi2 = 2.0 * pi;
+    const double* box = o.box;
+    const double vol = box[0] * box[1] * box[2];
+    const double pot_fact = 0.5 / pi / vol, inv_vol = 1.0 / vol;
+    const double alpha = o.prm.alpha, fac_vir = 2.0 * pi * pi * (1.0 / (alpha * alpha));
+    const double alpha_sqrtpi = alpha / std::sqrt(pi);
+    const double coeff = (pi / alpha) * (pi / alpha);
+    const bool cc = o.prm.ifnetqcorrp != 0;
+    std::vector<double> kw((size_t)3 * nwave), aw(nwave, 0.0);
+    for (int k = 0; k < nwave; ++k) {
+        for (int d = 0; d < 3; ++d) kw[3 * k + d] = (double)nv[3 * k + d] / box[d];
+        if (k == 0) continue;
+        double x = (double)nv[3 * k] / box[0], y = (double)nv[3 * k + 1] / box[1], z = (double)nv[3 * k + 2] / box[2];
+        double a2 = x * x + y * y + z * z;
+        aw[k] = std::exp(-coeff * a2) / a2;
+    }
+    std::vector<double> fi((size_t)3 * n, 0.0), pa(n, 0.0), va((size_t)9 * n, 0.0), sini(n), cosi(n);
+    double pot_ewk = 0.0, pot_ewk_cc = 0.0, vt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double* r = o.atmcor.data();
+    const double* q = o.atmchrg.data();
+    for (int k = 0; k < nwave; ++k) {
+        const double* K = &kw[3 * k];
+        double bsk = 0.0, bck = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double th = K[0] * r[3 * i] + K[1] * r[3 * i + 1] + K[2] * r[3 * i + 2];
+            th = pi2 * th;
+            sini[i] = std::sin(th);
+            cosi[i] = std::cos(th);
+            bsk = bsk + q[i] * sini[i];
+            bck = bck + q[i] * cosi[i];
+        }
+        const double pfa = pot_fact * aw[k];
+        const double poti = pfa * (bsk * bsk + bck * bck);
+        pot_ewk = pot_ewk + poti;
+        for (int i = 0; i < n; ++i) pa[i] = pa[i] + pfa * q[i] * (sini[i] * bsk + cosi[i] * bck);
+        double csk[3], cck[3];
+        for (int d = 0; d < 3; ++d) { csk[d] = aw[k] * bsk * K[d]; cck[d] = aw[k] * bck * K[d]; }
+        for (int i = 0; i < n; ++i)
+            for (int d = 0; d < 3; ++d) fi[3 * i + d] = fi[3 * i + d] + cck[d] * sini[i] - csk[d] * cosi[i];
+        if (k == 0) continue;   // ewaldk_hf.F90:186
+        const double k2 = K[0] * K[0] + K[1] * K[1] + K[2] * K[2];
+        double fac3 = 0.0;
+        if (cc) {   // ewaldk_hf.F90:236-240
+            fac3 = pfa * o.netchrgsq;
+            pot_ewk_cc = pot_ewk_cc + fac3 * (-1.0 + fac_vir * k2);
+        }
+        // k_fact(a,b) = (delta_ab - (2/|K|^2 + fac_vir) K_a K_b) * factor
+        auto kfact = [&](double f, double* dst) {
+            for (int b = 0; b < 3; ++b) {
+                double col[3];
+                for (int a = 0; a < 3; ++a) col[a] = -1.0 * (2.0 / k2 + fac_vir) * K[a] * K[b];
+                col[b] = col[b] + 1.0;
+                for (int a = 0; a < 3; ++a) dst[a + 3 * b] = dst[a + 3 * b] + col[a] * f;
+            }
+        };
+        kfact(poti - fac3, vt);
+        for (int i = 0; i < n; ++i) kfact(pfa * q[i] * (sini[i] * bsk + cosi[i] * bck) - fac3, &va[(size_t)9 * i]);
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int d = 0; d < 3; ++d) fi[3 * i + d] = 2.0 * q[i] * inv_vol * fi[3 * i + d];
+        pa[i] = pa[i] - alpha_sqrtpi * (q[i] * q[i]);
+    }
+    if (force) std::copy(fi.begin(), fi.end(), force);
+    if (pot_atm) std::copy(pa.begin(), pa.end(), pot_atm);
+    if (viri) std::copy(va.begin(), va.end(), viri);
+    if (sc) {
+        sc[0] = pot_ewk; sc[1] = pot_ewk_cc;
+        for (int t = 0; t < 9; ++t) sc[2 + t] = vt[t];
+    }
+    if (nwave_out) *nwave_out = nwave;
+    return PGK_OK;
+}
 }  // namespace
 
 // ============================================================================
@@ -2034,6 +2135,17 @@ void orc_lt_regions(void* h, int* out) {
     std::copy(o->hf.ltreg.begin(), o->hf.ltreg.end(), out);
 }
 void orc_philox(uint64_t seed, long long step, int atom, double* u) { lt_draw(seed, step, atom, u); }
+int orc_ewk_nvec(int kmax, double yratio, double zratio, int* out, int cap, int* nwave) {
+    std::vector<int> nv;
+    int s = ewk_nvec(kmax, yratio, zratio, nv);
+    if (s) return s;
+    *nwave = (int)nv.size() / 3;
+    if (out) std::copy(nv.begin(), nv.begin() + std::min((size_t)3 * cap, nv.size()), out);
+    return PGK_OK;
+}
+int orc_ewaldkp_hf(void* h, int kmax, double* force, double* pot_atm, double* viri, double* sc, int* nwave) {
+    return ewaldkp_hf(*(Oracle*)h, kmax, force, pot_atm, viri, sc, nwave);
+}
 void orc_philox_raw(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
     uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
     philox4x32(c, key[0], key[1]);

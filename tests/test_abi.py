@@ -36,9 +36,9 @@ def test_struct_sizes_match_the_header():
     # compile a tiny C probe of the header's struct sizes with gcc
     here = os.path.dirname(os.path.abspath(__file__))
     inc = os.path.join(here, "..", "include")
-    src = ('#include "pgk_gpu.h"\n#include <stdio.h>\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu\\n",'
+    src = ('#include "pgk_gpu.h"\n#include <stdio.h>\nint main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n",'
            'sizeof(pgk_system),sizeof(pgk_params),sizeof(pgk_mdparams),sizeof(pgk_energies),'
-           'sizeof(pgk_virials),sizeof(pgk_chain),sizeof(pgk_hfparams));return 0;}\n')
+           'sizeof(pgk_virials),sizeof(pgk_chain),sizeof(pgk_hfparams),sizeof(pgk_ewk_hf));return 0;}\n')
     import tempfile
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "p.c")
@@ -48,5 +48,5 @@ def test_struct_sizes_match_the_header():
         sizes = [int(x) for x in subprocess.check_output([exe]).split()]
     want = [ctypes.sizeof(t) for t in (abi.SystemStruct, abi.ParamsStruct, abi.MdParamsStruct,
                                        abi.EnergiesStruct, abi.VirialsStruct, abi.ChainStruct,
-                                       abi.HfParamsStruct)]
+                                       abi.HfParamsStruct, abi.EwkHfStruct)]
     assert sizes == want

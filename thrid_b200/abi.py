@@ -132,6 +132,12 @@ class HfParamsStruct(C.Structure):
     ]
 
 
+class EwkHfStruct(C.Structure):
+    """pgk_ewk_hf: scalars of ewaldkp_hf (ewaldk_hf.F90:8-304)."""
+    _fields_ = [("pot_ewk", C.c_double), ("pot_ewk_cc", C.c_double), ("pot_virit_coul", C.c_double * 9),
+                ("nwave", C.c_int32), ("_pad", C.c_int32)]
+
+
 class CHfParams:
     """Owns the arrays behind an HfParamsStruct built from a dict:
     regions=[(z1, z2), ...], heatfinterval, hftyp (per-atom array or None),

@@ -591,7 +591,8 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->cg_fit, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
-                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec};
+                    c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec,
+                    c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st2) { cudaStreamSynchronize(c->st2); cudaStreamDestroy(c->st2); }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -698,6 +699,32 @@ pgk_status pgk_fft_pme(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* 
     return read_status(c);
 }
 
+pgk_status pgk_ewaldkp_hf(pgk_ctx* c, int32_t kmax, double* force, double* pot_atm, double* viri_atm,
+                          pgk_ewk_hf* out) {
+    if (!c) return PGK_E_INVALID;
+    int nw = 0;
+    pgk_status s = launch_ewk_hf(c, kmax, &nw);
+    if (s) return s;
+    const size_t n = (size_t)c->natom;
+    if (force) PGK_CUDA(c, cudaMemcpyAsync(force, c->ewk_out, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    if (pot_atm)
+        PGK_CUDA(c, cudaMemcpyAsync(pot_atm, c->ewk_out + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    if (viri_atm)
+        PGK_CUDA(c, cudaMemcpyAsync(viri_atm, c->ewk_out + 4 * n, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost,
+                                    c->st));
+    double sc[11];
+    PGK_CUDA(c, cudaMemcpyAsync(sc, c->ewk_out + 13 * n, sizeof(sc), cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    if (out) {
+        out->pot_ewk = sc[0];
+        out->pot_ewk_cc = sc[1];
+        for (int t = 0; t < 9; ++t) out->pot_virit_coul[t] = sc[2 + t];
+        out->nwave = nw;
+        out->_pad = 0;
+    }
+    return read_status(c);
+}
+
 pgk_status pgk_calbonded(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
     if (!c) return PGK_E_INVALID;
     pgk_status s;
@@ -760,6 +787,11 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
     } else if (units) {
         *units = which == 3 ? (double)c->K[0] * c->K[1] * c->K[2] : (double)c->natom;
     }
+    if (which >= 256 && which < 1024) {
+        int nw = 0;
+        if ((s = launch_ewk_hf(c, (which - 256) & 255, &nw))) return s;
+        if (units) *units = (double)c->natom * (nw - 1);
+    }
     if (which >= 1 && which <= 3 && !c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
     cudaEvent_t e0, e1;
     PGK_CUDA(c, cudaEventCreate(&e0));
@@ -771,6 +803,8 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
             case 2: return spme_bench(c, 2);
             case 3: return spme_bench(c, 3);
             default:
+                if (which >= 256 && which < 1024)
+                    return launch_ewk_hf(c, (which - 256) & 255, nullptr, (which - 256) >> 8);
                 if (which >= 64 && which < 128) return launch_intra(c, 0, which - 64, true);
                 if (which >= 128 && which < 192) return launch_intra(c, 0, which - 128, true, true);
                 return pgk_fail(c, PGK_E_INVALID, "unknown kernel id");

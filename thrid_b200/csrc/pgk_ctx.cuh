@@ -177,6 +177,18 @@ struct pgk_ctx {
     double* lt_frand = nullptr;   // [3N] random accelerations of the former half step
     double* lt_dekin = nullptr;   // [8] det_ene_kin
 
+    // ---- standard-Ewald k-space of the bulk heat flux (k_ewald.cu) ----
+    int ewk_kmax = 0;             // wave set held in ewk_nv (0: none)
+    int ewk_nwave = 0;            // waves, (0,0,0) first
+    int ewk_nmax[3] = {0, 0, 0};  // largest |n| per axis
+    int4* ewk_nv = nullptr;       // [nwave] (nx, ny, nz, 0)
+    double2* ewk_tab = nullptr;   // [rows][N] exp(2 pi i n r_d / L_d), rows = n 0..nmax of x, y, z
+    double2* ewk_part = nullptr;  // [nchunk][nwave] structure-factor partial sums (cos, sin)
+    double* ewk_coef = nullptr;   // [nwave][EWK_NCOEF] per-wave coefficients
+    double* ewk_red = nullptr;    // [wave blocks][8] energy / tensor partials
+    double* ewk_out = nullptr;    // force 3N | energy N | tensor 9N | scalars 11
+    size_t ewk_bytes[5] = {0, 0, 0, 0, 0};   // allocated sizes of tab, part, coef, red, out
+
     // ---- CUDA graphs of captured MD steps (key: driver kind and step flags);
     //      valid for one list build and one set of integrator parameters ----
     struct GraphEntry { cudaGraphExec_t exec; long long launches; long long epoch; };
@@ -250,6 +262,12 @@ pgk_status launch_heatf(pgk_ctx* c, double* dst);
 pgk_status launch_lt_regist(pgk_ctx* c);
 pgk_status launch_langevin(pgk_ctx* c, double dt, long long step, bool former);
 pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h);   // k_bonded.cu
+
+// ---- launchers (k_ewald.cu, ewaldkp_hf) ----
+// one evaluation at the current positions into c->ewk_out (device); nwave out.
+// only = 1 / 2: launch k_ewk_sfac / k_ewk_atom alone on the buffers of the
+// last full call with this kmax (instrumentation)
+pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave, int only = 0);
 
 // ---- launchers (k_integrate.cu) ----
 pgk_status launch_zero_group(pgk_ctx* c, int group);

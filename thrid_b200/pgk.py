@@ -83,6 +83,7 @@ def lib():
     L.pgk_calheatf.argtypes = [vp, pd]
     L.pgk_get_hf_atm.argtypes = [vp, pd, pd]
     L.pgk_langevin_dekin.argtypes = [vp, pd]
+    L.pgk_ewaldkp_hf.argtypes = [vp, C.c_int32, pd, pd, pd, C.POINTER(abi.EwkHfStruct)]
     _lib = L
     return L
 
@@ -250,6 +251,18 @@ class PgkEngine:
         nr = C.c_int64(0)
         self._check(self.L.pgk_moldyn_hf(self.h, ini, end, C.byref(md), C.byref(e), _p(rec), cap, C.byref(nr)))
         return e.as_dict(), rec[:min(nr.value, cap), :self._hf.nreg]
+
+    def ewaldkp_hf(self, kmax):
+        """ewaldkp_hf (ewaldk_hf.F90:8-304) at the current positions: dict with
+        force (N,3), pot_atm (N), viri_atm (N,3,3) with viri_atm[i, b, a] =
+        virielct_atm(a,b,i,1), pot_ewk, pot_ewk_cc, pot_virit_coul (3,3) [b, a]
+        and nwave."""
+        n = self.sys.natom
+        f = np.zeros((n, 3)); pot = np.zeros(n); vir = np.zeros((n, 3, 3))
+        o = abi.EwkHfStruct()
+        self._check(self.L.pgk_ewaldkp_hf(self.h, kmax, _p(f), _p(pot), _p(vir), C.byref(o)))
+        return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=o.pot_ewk, pot_ewk_cc=o.pot_ewk_cc,
+                    pot_virit_coul=np.array(o.pot_virit_coul[:]).reshape(3, 3), nwave=o.nwave)
 
     def langevin_dekin(self):
         out = np.zeros(abi.LT_MAX_REGIONS)
