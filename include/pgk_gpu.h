@@ -114,6 +114,14 @@ typedef struct pgk_system {
     const double  *dconst;
 
     int32_t degfree_all;          /* prepmd.F90:250-330                          */
+
+    /* Morse pairs (morse.F90, rdpara.F90:680-720): type pairs whose
+     * inter_inttyp is 2 (INTTYPE_MOR, md_global.inc:120) interact by
+     * D (exp(-2a(r-r0)) - 2 exp(-a(r-r0))) instead of LJ.  [ntyp*ntyp]
+     * column-major like vdw_radij; NULL = no Morse pairs.  The device engine
+     * does not build Morse yet: pgk_init returns PGK_E_UNSUPPORTED when a
+     * Morse pair type is present (the oracle restates it). */
+    const double  *para_welmor, *para_radmor, *para_alphamor;
 } pgk_system;
 
 /* ---- run-time parameters (peachgk.ini keywords after calbase) ----------- */
@@ -135,6 +143,10 @@ typedef struct pgk_params {
     int32_t mts_vdw14, mts_elc14; /* calnon14 runs when both equal the flag    */
     int32_t ifnetqcorrp;          /* net-charge correction for pressure        */
     int32_t max_nbr;              /* entries per 8-atom cluster row of the device pair list (0 = auto) */
+    double  rcutmor;              /* Morse cutoff                              */
+    double  rcut_bookmor;         /* Morse list radius (mklist_mor*.F90)       */
+    int32_t mts_mor;              /* gates morsep (PGK_MTS_*)                   */
+    int32_t _pad_mor;
 } pgk_params;
 
 /* ---- integrator parameters (moldyn_*.F90 arguments) ---------------------- */
@@ -161,6 +173,7 @@ typedef struct pgk_energies {
     double pot_vdw, pot_elc, pot_ewk, pot_ewc, pot_ewnq;
     double pot_vdw14, pot_elc14;
     double pot_bond, pot_angl, pot_tors, pot_torsrb;
+    double pot_mor;               /* Morse energy (in pot_tot, not pot_nonbon; calforce.F90:1060-1070) */
 } pgk_energies;
 
 /* ---- virials (ewaldrp / fft_pmep / cal*p OUTPUT names), tensors (3,3)
@@ -170,6 +183,7 @@ typedef struct pgk_virials {
     double pot_virit_coul[9], pot_virit_lj[9];
     double atm_viri_bond, atm_viri_angl, atm_viri_tors, atm_viri_14;
     double atm_virit_bond[9], atm_virit_angl[9], atm_virit_tors[9], atm_virit_14[9];
+    double pot_viri_mor, pot_virit_mor[9];   /* morsep */
 } pgk_virials;
 
 /* ---- thermostat / barostat state (md_global.inc xlogs, vlogs, ...) ------- */

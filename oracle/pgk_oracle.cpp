@@ -4,12 +4,17 @@
 // library (libpgkgpu.so) never links or calls it.
 //
 // Parity status: the reference is Fortran 90 and no Fortran compiler exists in
-// this image, so the reference cannot be built or run here, and the reference
-// tree holds no golden vectors for this path.  Parity of this restatement is
-// therefore "unpinned" against the reference binary; it is pinned instead by
-// analytical known answers in tests/ (two-body LJ/Coulomb, Madelung constant of
-// a NaCl lattice, B-spline partition of unity, FFT vs direct DFT, spline vs
-// erfc, finite-difference forces, constraint residuals, conserved NHC energy).
+// this image, so the reference cannot be built or run here.  The restatement
+// is pinned against the reference's own recorded run instead: the reference
+// tree keeps the step-1 positions (out_pos.dat) and energies (out_ene.dat) of
+// its Pt/Morse sample, and tests/test_golden_pt_morse.py reproduces every
+// recorded energy term of calforce (LJ, real-space and SPME Coulomb, self
+// term, 1-4, bond, angle, torsion, RB torsion, Morse, total) from those
+// positions within the precision the recorded files carry (1e-5 .. 1e-9).
+// Analytical known answers in tests/ add what a recorded energy cannot show
+// (forces by finite differences, two-body LJ/Coulomb, Madelung constant,
+// B-spline partition of unity, FFT vs direct DFT, spline vs erfc, constraint
+// residuals, conserved NHC energy).
 //
 // Every routine cites the reference file:line it restates.  Arithmetic follows
 // the reference order (left-to-right sums, dnint = round-half-away) and is
@@ -102,6 +107,10 @@ struct Oracle {
     int ntyp = 0;
     std::vector<double> radij, welij;  // [i + ntyp*j]
     std::vector<int> inttyp;
+    // Morse pairs (rdpara.F90:680-720), column-major (i,j) like radij
+    std::vector<double> welmor, radmor, almor;
+    std::vector<int> mor_atoms;            // nmorselist (linkbond.F90), 0-based
+    std::vector<int> mor_idx, mor_list;    // mklist2a_mor rows: [mor_atoms+1] starts, 0-based partners
     std::vector<int> molidx, mollist;  // 0-based
     std::vector<int> excl_idx, excl_list;  // reference CSR kept 1-based values
     // bonded
@@ -313,7 +322,40 @@ int choose_list_mode(const Oracle& o) {
     return PGK_LIST_CELL;
 }
 
+// mklist2a_mor (mklist_mor.F90:30-120): for each Morse atom, the later Morse
+// atoms of a Morse type pair inside rcut_bookmor (minimum image).  The cell
+// variant (mklist_mor_cell.F90) keeps j > i by atom index from the 27-cell
+// stencil when the rdscript.F90:1620-1635 rule allows it: the same pair set,
+// partners in another order.  Without a list radius the half-box diagonal
+// is the radius (mklist_mor.F90:30-34).
+void mklist_mor(Oracle& o) {
+    double sqcut = o.prm.rcut_bookmor * o.prm.rcut_bookmor;
+    if (o.prm.rcut_bookmor <= 0.0)
+        sqcut = (o.box[0] / 2.0) * (o.box[0] / 2.0) + (o.box[1] / 2.0) * (o.box[1] / 2.0) +
+                (o.box[2] / 2.0) * (o.box[2] / 2.0);
+    const int nm = (int)o.mor_atoms.size();
+    o.mor_idx.assign((size_t)nm + 1, 0);
+    o.mor_list.clear();
+    for (int m1 = 0; m1 < nm; ++m1) {
+        o.mor_idx[m1] = (int)o.mor_list.size();
+        const int i = o.mor_atoms[m1], it = o.atmindex[i];
+        for (int m2 = m1 + 1; m2 < nm; ++m2) {
+            const int j = o.mor_atoms[m2], jt = o.atmindex[j];
+            if (o.inttyp[it + o.ntyp * jt] != 2) continue;
+            double rij[3];
+            for (int d = 0; d < 3; ++d) {
+                double v = o.atmcor[3 * i + d] - o.atmcor[3 * j + d];
+                rij[d] = v - o.box[d] * dnint(v * (1.0 / o.box[d]));
+            }
+            double dr = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+            if (dr < sqcut) o.mor_list.push_back(j);
+        }
+    }
+    o.mor_idx[nm] = (int)o.mor_list.size();
+}
+
 void mklist(Oracle& o) {
+    if (!o.welmor.empty()) mklist_mor(o);
     int n = o.natom;
     double sqcut = o.prm.rcut_book * o.prm.rcut_book;
     int mode = choose_list_mode(o);
@@ -821,6 +863,35 @@ void calnon14p(Oracle& o, double* force, double& pe, double& pv, double& vs, dou
     }
 }
 
+// morsep (morse.F90:206-414): Morse energy, forces and virials over the
+// Morse list, pairs beyond rcutmor skipped; forces summed in fmor first
+void morsep(Oracle& o, double* force, double& pot, double& vir, double* virt) {
+    const int n = o.natom, nm = (int)o.mor_atoms.size();
+    const double sqcut = o.prm.rcutmor * o.prm.rcutmor;
+    std::vector<double> fm((size_t)3 * n, 0.0);
+    for (int m1 = 0; m1 + 1 < nm; ++m1) {
+        const int i = o.mor_atoms[m1], it = o.atmindex[i];
+        for (int q = o.mor_idx[m1]; q < o.mor_idx[m1 + 1]; ++q) {
+            const int j = o.mor_list[q], jt = o.atmindex[j];
+            double rij[3]; mi(o, i, j, rij);
+            double r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+            if (r2 > sqcut) continue;
+            double r = std::sqrt(r2), ri1 = 1.0 / r;
+            const size_t t = (size_t)it + (size_t)o.ntyp * jt;
+            double rt1 = std::exp(-1.0 * (r - o.radmor[t]) * o.almor[t]);
+            double rt2 = rt1 * rt1;
+            double ftmp = 2.0 * o.almor[t] * o.welmor[t] * (rt2 - rt1) * ri1;
+            double potij = o.welmor[t] * (rt2 - 2.0 * rt1);
+            pot = pot + potij;
+            double fij[3] = {ftmp * rij[0], ftmp * rij[1], ftmp * rij[2]};
+            for (int d = 0; d < 3; ++d) { fm[3 * i + d] += fij[d]; fm[3 * j + d] -= fij[d]; }
+            for (int nn = 0; nn < 3; ++nn) for (int a = 0; a < 3; ++a) virt[a + 3 * nn] += fij[a] * rij[nn];
+            vir = vir + fij[0] * rij[0] + fij[1] * rij[1] + fij[2] * rij[2];
+        }
+    }
+    for (size_t k = 0; k < fm.size(); ++k) force[k] = force[k] + fm[k];
+}
+
 // calforce (calforce.F90:8-1073) for one MTS group; force overwritten
 void calforce(Oracle& o, int flag, double* force, pgk_energies* e, pgk_virials* v) {
     std::fill(force, force + 3 * o.natom, 0.0);
@@ -833,6 +904,7 @@ void calforce(Oracle& o, int flag, double* force, pgk_energies* e, pgk_virials* 
     if (o.prm.mts_torsrb == flag) caltorsrbp(o, force, E.pot_torsrb, V.atm_viri_tors, V.atm_virit_tors);
     if (o.prm.mts_vdw14 == flag && o.prm.mts_elc14 == flag)
         calnon14p(o, force, E.pot_elc14, E.pot_vdw14, V.atm_viri_14, V.atm_virit_14);
+    if (!o.welmor.empty() && o.prm.mts_mor == flag) morsep(o, force, E.pot_mor, V.pot_viri_mor, V.pot_virit_mor);
     if (flag == PGK_MTS_LONG && o.prm.ifspme) {   // :1018-1050 net charge
         double pi = std::acos(-1.0);
         double a1 = -pi / (o.prm.alpha * o.prm.alpha * o.box[0] * o.box[1] * o.box[2]);
@@ -846,7 +918,7 @@ void calforce(Oracle& o, int flag, double* force, pgk_energies* e, pgk_virials* 
         E.pot_ewc = o.pot_ewc;
     }
     E.pot_nonbon = E.pot_vdw + E.pot_elc + E.pot_ewk + E.pot_ewc + E.pot_ewnq + E.pot_vdw14 + E.pot_elc14;
-    E.pot_tot = E.pot_bond + E.pot_angl + E.pot_tors + E.pot_torsrb + E.pot_nonbon;
+    E.pot_tot = E.pot_bond + E.pot_angl + E.pot_tors + E.pot_torsrb + E.pot_mor + E.pot_nonbon;
     if (e) *e = E;
     if (v) *v = V;
 }
@@ -1061,11 +1133,13 @@ void calpress(Oracle& o, const pgk_virials& vl, const pgk_virials& vs, double* p
     double W = vl.pot_viri_coul + vs.pot_viri_coul + ewc + ewnq + vl.pot_viri_lj + vs.pot_viri_lj;
     W += vl.atm_viri_bond + vs.atm_viri_bond + vl.atm_viri_angl + vs.atm_viri_angl +
          vl.atm_viri_tors + vs.atm_viri_tors + vl.atm_viri_14 + vs.atm_viri_14;
+    W += vl.pot_viri_mor + vs.pot_viri_mor;   // calpress.F90:146-151
     double Wt[9];
     for (int k = 0; k < 9; ++k)
         Wt[k] = vl.pot_virit_coul[k] + vs.pot_virit_coul[k] + vl.pot_virit_lj[k] + vs.pot_virit_lj[k] +
                 vl.atm_virit_bond[k] + vs.atm_virit_bond[k] + vl.atm_virit_angl[k] + vs.atm_virit_angl[k] +
-                vl.atm_virit_tors[k] + vs.atm_virit_tors[k] + vl.atm_virit_14[k] + vs.atm_virit_14[k];
+                vl.atm_virit_tors[k] + vs.atm_virit_tors[k] + vl.atm_virit_14[k] + vs.atm_virit_14[k] +
+                vl.pot_virit_mor[k] + vs.pot_virit_mor[k];
     double binv = 1.0 / o.box[0] * (1.0 / o.box[1]) * (1.0 / o.box[2]);
     double b3 = (1.0 / o.box[0]) * (1.0 / o.box[1]) * (1.0 / o.box[2]);
     (void)binv;
@@ -1248,6 +1322,7 @@ int moldyn(Oracle& o, int kind, long long ini, long long end, const pgk_mdparams
             e.pot_vdw14 = F.el.pot_vdw14 + F.es.pot_vdw14; e.pot_elc14 = F.el.pot_elc14 + F.es.pot_elc14;
             e.pot_bond = F.el.pot_bond + F.es.pot_bond; e.pot_angl = F.el.pot_angl + F.es.pot_angl;
             e.pot_tors = F.el.pot_tors + F.es.pot_tors; e.pot_torsrb = F.el.pot_torsrb + F.es.pot_torsrb;
+            e.pot_mor = F.el.pot_mor + F.es.pot_mor;
             e.pot_nonbon = F.el.pot_nonbon + F.es.pot_nonbon; e.pot_tot = F.el.pot_tot + F.es.pot_tot;
             *eout = e;
         }
@@ -1787,6 +1862,7 @@ int moldyn_hf(Oracle& o, long long ini, long long end, const pgk_mdparams& md, p
             e.pot_vdw14 = F.el.pot_vdw14 + F.es.pot_vdw14; e.pot_elc14 = F.el.pot_elc14 + F.es.pot_elc14;
             e.pot_bond = F.el.pot_bond + F.es.pot_bond; e.pot_angl = F.el.pot_angl + F.es.pot_angl;
             e.pot_tors = F.el.pot_tors + F.es.pot_tors; e.pot_torsrb = F.el.pot_torsrb + F.es.pot_torsrb;
+            e.pot_mor = F.el.pot_mor + F.es.pot_mor;
             e.pot_nonbon = F.el.pot_nonbon + F.es.pot_nonbon; e.pot_tot = F.el.pot_tot + F.es.pot_tot;
             *eout = e;
         }
@@ -1914,6 +1990,21 @@ void* orc_create(const pgk_system* s, const pgk_params* p) {
     o->radij.assign(s->vdw_radij, s->vdw_radij + s->ntyp * s->ntyp);
     o->welij.assign(s->vdw_welij, s->vdw_welij + s->ntyp * s->ntyp);
     if (s->inter_inttyp) o->inttyp.assign(s->inter_inttyp, s->inter_inttyp + s->ntyp * s->ntyp);
+    if (s->inter_inttyp && s->para_welmor && s->para_radmor && s->para_alphamor) {
+        const int t2 = s->ntyp * s->ntyp;
+        bool any = false;
+        for (int k = 0; k < t2; ++k) any = any || s->inter_inttyp[k] == 2;
+        if (any) {
+            o->welmor.assign(s->para_welmor, s->para_welmor + t2);
+            o->radmor.assign(s->para_radmor, s->para_radmor + t2);
+            o->almor.assign(s->para_alphamor, s->para_alphamor + t2);
+            std::vector<char> mt(s->ntyp, 0);   // types with a Morse partner
+            for (int a = 0; a < s->ntyp; ++a)
+                for (int b = 0; b < s->ntyp; ++b) mt[a] = mt[a] || s->inter_inttyp[a + s->ntyp * b] == 2;
+            for (int i = 0; i < n; ++i)
+                if (mt[s->atmindex[i] - 1]) o->mor_atoms.push_back(i);
+        }
+    }
     o->molidx.resize(s->nmole + 1);
     for (int m = 0; m <= s->nmole; ++m) o->molidx[m] = s->molept_index[m] - 1;
     o->mollist.resize(o->molidx[s->nmole]);

@@ -46,6 +46,7 @@ class SystemStruct(C.Structure):
         ("nconst", C.c_int32), ("index_mconst", _pi), ("list_mconst", _pi),
         ("nconstraint", C.c_int32), ("iconst", _pi), ("jconst", _pi), ("dconst", _pd),
         ("degfree_all", C.c_int32),
+        ("para_welmor", _pd), ("para_radmor", _pd), ("para_alphamor", _pd),
     ]
 
 
@@ -59,7 +60,11 @@ class ParamsStruct(C.Structure):
         ("mts_bond", C.c_int32), ("mts_angl", C.c_int32), ("mts_tors", C.c_int32), ("mts_torsrb", C.c_int32),
         ("mts_vdw", C.c_int32), ("mts_ewk", C.c_int32), ("mts_vdw14", C.c_int32), ("mts_elc14", C.c_int32),
         ("ifnetqcorrp", C.c_int32), ("max_nbr", C.c_int32),
+        ("rcutmor", C.c_double), ("rcut_bookmor", C.c_double), ("mts_mor", C.c_int32), ("_pad_mor", C.c_int32),
     ]
+
+# run-time parameters a system may leave out (no Morse pairs)
+PARAM_DEFAULTS = {"rcutmor": 0.0, "rcut_bookmor": 0.0, "mts_mor": 0, "_pad_mor": 0}
 
 
 class MdParamsStruct(C.Structure):
@@ -73,7 +78,7 @@ class MdParamsStruct(C.Structure):
 
 
 ENERGY_NAMES = ["pot_tot", "pot_nonbon", "pot_vdw", "pot_elc", "pot_ewk", "pot_ewc", "pot_ewnq",
-                "pot_vdw14", "pot_elc14", "pot_bond", "pot_angl", "pot_tors", "pot_torsrb"]
+                "pot_vdw14", "pot_elc14", "pot_bond", "pot_angl", "pot_tors", "pot_torsrb", "pot_mor"]
 
 
 class EnergiesStruct(C.Structure):
@@ -91,6 +96,7 @@ class VirialsStruct(C.Structure):
         ("atm_viri_tors", C.c_double), ("atm_viri_14", C.c_double),
         ("atm_virit_bond", C.c_double * 9), ("atm_virit_angl", C.c_double * 9),
         ("atm_virit_tors", C.c_double * 9), ("atm_virit_14", C.c_double * 9),
+        ("pot_viri_mor", C.c_double), ("pot_virit_mor", C.c_double * 9),
     ]
 
     def as_dict(self):
@@ -208,7 +214,8 @@ class CSystem:
         st.ntyp = ntyp
         st.vdw_radij = d("R", s.vdw_radij.T)      # column-major (i,j)
         st.vdw_welij = d("E", s.vdw_welij.T)
-        st.inter_inttyp = C.POINTER(C.c_int32)()
+        inttyp = getattr(s, "inttyp", None)
+        st.inter_inttyp = i("it", inttyp.T) if inttyp is not None else C.POINTER(C.c_int32)()
         st.nmole = s.nmole
         st.molept_index = i("mi", s.molept_index, 1)
         st.molept_list = i("ml", s.molept_list, 1)
@@ -241,6 +248,9 @@ class CSystem:
         st.iconst = i("cii", s.const_ij[:, 0], 1); st.jconst = i("cjj", s.const_ij[:, 1], 1)
         st.dconst = d("cd", s.const_d)
         st.degfree_all = int(s.degfree_all)
+        if getattr(s, "mor_wel", None) is not None:
+            st.para_welmor = d("mw", s.mor_wel.T); st.para_radmor = d("mr", s.mor_rad.T)
+            st.para_alphamor = d("ma", s.mor_alpha.T)
         self.struct = st
         self._keep = keep
 
@@ -248,7 +258,7 @@ class CSystem:
 def params_struct(p: dict) -> ParamsStruct:
     ps = ParamsStruct()
     for name, _ in ParamsStruct._fields_:
-        setattr(ps, name, p[name])
+        setattr(ps, name, p[name] if name in p or name not in PARAM_DEFAULTS else PARAM_DEFAULTS[name])
     return ps
 
 

@@ -243,7 +243,9 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         return PGK_E_INVALID;
     if (p->precision != PGK_PREC_FP64 && p->precision != PGK_PREC_MIXED) return PGK_E_INVALID;
     if (p->rcut_book <= 0 || p->rcut <= 0 || p->rrcut <= 0) return PGK_E_INVALID;
-    if (p->mts_vdw != p->mts_vdw) return PGK_E_INVALID;
+    if (s->inter_inttyp && s->para_welmor)   // Morse pairs (morse.F90): restated by the oracle, not on the device
+        for (int k = 0; k < s->ntyp * s->ntyp; ++k)
+            if (s->inter_inttyp[k] == 2) return PGK_E_UNSUPPORTED;
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return PGK_E_CUDA;
     pgk_ctx* c = new pgk_ctx();
@@ -959,7 +961,8 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
         PGK_CUDA(c, cudaMemcpyAsync(r, c->out_rec + last_rec * PGK_OUT_NCOL, sizeof(r), cudaMemcpyDeviceToHost,
                                     c->st));
         PGK_CUDA(c, cudaStreamSynchronize(c->st));
-        memcpy(eo, r + 1, sizeof(pgk_energies));
+        memset(eo, 0, sizeof(pgk_energies));
+        memcpy(eo, r + 1, offsetof(pgk_energies, pot_mor));   // record: the energies before pot_mor
     }
     if (nrec) *nrec = nr;
     return read_status(c);

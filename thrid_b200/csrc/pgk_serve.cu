@@ -48,6 +48,8 @@ struct SystemCopy {
         s.atmmass = cd(x.atmmass, n); s.atmchrg = cd(x.atmchrg, n); s.atmindex = ci(x.atmindex, n);
         s.vdw_radij = cd(x.vdw_radij, t2); s.vdw_welij = cd(x.vdw_welij, t2);
         s.inter_inttyp = ci(x.inter_inttyp, t2);
+        s.para_welmor = cd(x.para_welmor, t2); s.para_radmor = cd(x.para_radmor, t2);
+        s.para_alphamor = cd(x.para_alphamor, t2);
         s.molept_index = ci(x.molept_index, (size_t)x.nmole + 1);
         s.molept_list = ci(x.molept_list, x.molept_index ? (size_t)(x.molept_index[x.nmole] - 1) : 0);
         s.index_excl = ci(x.index_excl, n + 1);

@@ -353,6 +353,10 @@ class System:
     degfree_all: int
     params: dict                     # peachgk.ini-like run parameters (reduced)
     regions: dict = dataclasses.field(default_factory=dict)
+    inttyp: np.ndarray = None        # (ntyp,ntyp) inter_inttyp (1 LJ, 2 Morse); None = all LJ
+    mor_wel: np.ndarray = None       # (ntyp,ntyp) Morse D, r0, alpha (rdpara.F90:680-720)
+    mor_rad: np.ndarray = None
+    mor_alpha: np.ndarray = None
 
     @property
     def nmole(self):
