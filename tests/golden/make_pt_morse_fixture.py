@@ -6,7 +6,8 @@ of step 1 in out_ene.dat (output_data.F90 outene, SI units, E15.8) and the
 positions of the same step in out_pos.dat (outpos, output_data.F90:345-394,
 Fortran unformatted records, single precision unless -D_DOUBLE_OUTPOS).  This
 script restates the reference's input processing for that system and stores
-every array the oracle needs, in reduced units, beside the recorded energies:
+every array the oracle needs, in reduced units, beside the recorded energies
+and the virials of the same step (out_pre.dat, outpre):
 
   * rdpara.F90:100-760     <ATOM>, <BOND>, <ANGLE>, <TORSION>, <TORSION_RB>,
                            <MORSE>, <VDW_SP> of para_bond.dat; para_vdw_s.dat;
@@ -280,6 +281,11 @@ def main(ref):
     ene = [r for r in read_out_ene(os.path.join(ref, "out_ene.dat")) if int(r["nstep"]) == step]
     if len(ene) != 1:
         raise ValueError("no out_ene.dat record for the out_pos.dat step")
+    # outpre (same layout as outene): virials [J] and pressure tensors of the step
+    pre = [r for r in read_out_ene(os.path.join(ref, "out_pre.dat")) if int(r["nstep"]) == step]
+    if len(pre) != 1:
+        raise ValueError("no out_pre.dat record for the out_pos.dat step")
+    pre_keys = [k for k in pre[0] if k.startswith(("pot_viri", "atm_viri", "preatmt_vtot"))]
     ini = b["ini"]
     g = b["g"]
     an, mref = 6.0221367e23, 1.99431e-26                       # rdpara.F90:64, main_md.F90:395
@@ -299,6 +305,7 @@ def main(ref):
         mol_sizes=np.array(b["mol_sizes"], np.int32),
         params_keys=np.array(list(params)), params_vals=np.array(list(params.values()), float),
         ene_keys=np.array(ENE_KEYS), ene_joule=np.array([ene[0][k] for k in ENE_KEYS]), eref=EREF, xref=XREF,
+        pre_keys=np.array(pre_keys), pre_joule=np.array([pre[0][k] for k in pre_keys]),
         **b["fix"])
     print("wrote", OUT, "natom", len(tix), "step", step)
 

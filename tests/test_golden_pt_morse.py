@@ -68,25 +68,30 @@ def load_pt_morse(precision=abi.PREC_FP64):
         degfree_all=3 * natom, params=params,
         inttyp=z["inttyp"], mor_wel=z["mor_wel"], mor_rad=z["mor_rad"], mor_alpha=z["mor_alpha"])
     want = {str(k): float(v) / float(z["eref"]) for k, v in zip(z["ene_keys"], z["ene_joule"])}
+    want.update({str(k): float(v) / float(z["eref"]) for k, v in zip(z["pre_keys"], z["pre_joule"])})
     return s, want
 
 
-def oracle_energies(oracle_mod, s):
+def oracle_energies(oracle_mod, s, virials=False):
     o = oracle_mod.Oracle(s, threads=os.cpu_count() or 1)
     o.mklist()
-    _, el, _ = o.calforce(abi.MTS_LONG)
-    _, es, _ = o.calforce(abi.MTS_SHORT)
-    return {k: el[k] + es[k] for k in el}
+    _, el, vl = o.calforce(abi.MTS_LONG)
+    _, es, vs = o.calforce(abi.MTS_SHORT)
+    e = {k: el[k] + es[k] for k in el}
+    if not virials:
+        return e
+    return e, {k: np.asarray(vl[k]) + np.asarray(vs[k]) for k in vl}
 
 
 @pytest.fixture(scope="module")
 def pt_morse(oracle_mod):
     s, want = load_pt_morse()
-    return s, want, oracle_energies(oracle_mod, s)
+    e, v = oracle_energies(oracle_mod, s, virials=True)
+    return s, want, e, v
 
 
 def test_fixture_shape(pt_morse):
-    s, want, _ = pt_morse
+    s, want, _, _ = pt_morse
     assert s.natom == 6364 and len(s.bonds) == 2580 and len(s.angles) == 4750
     assert len(s.tors) == 210 and len(s.torsrb) == 5130
     # the reference's ring14_rb reset covers only the first ntors RB torsions
@@ -95,9 +100,39 @@ def test_fixture_shape(pt_morse):
 
 @pytest.mark.parametrize("term", sorted(TOL))
 def test_oracle_matches_recorded_energy(pt_morse, term):
-    _, want, got = pt_morse
+    _, want, got, _ = pt_morse
     w, g = want[term], got[term]
     assert abs(g - w) <= TOL[term] * abs(w), f"{term}: oracle {g!r} recorded {w!r} rel {abs(g - w) / abs(w):.2e}"
+
+
+# recorded virial (calpress.F90 outputs) -> the oracle's sum, relative tolerance;
+# measured: lj 1.3e-6, mor 7.2e-6, coulomb 8.9e-9, bond 1.3e-5, 1-4 4.9e-7
+VIR = {"pot_virilj_all": (("pot_viri_lj",), 1e-5), "pot_virimor_all": (("pot_viri_mor",), 5e-5),
+       "atm_viribo_all": (("atm_viri_bond",), 1e-4), "atm_viri14_all": (("atm_viri_14",), 5e-6)}
+
+
+@pytest.mark.parametrize("term", sorted(VIR))
+def test_oracle_matches_recorded_virial(pt_morse, term):
+    _, want, _, vir = pt_morse
+    keys, tol = VIR[term]
+    g = sum(float(vir[k]) for k in keys)
+    assert abs(g - want[term]) <= tol * abs(want[term]), (term, g, want[term])
+
+
+def test_oracle_matches_recorded_coulomb_virial_and_tensor(pt_morse):
+    _, want, e, vir = pt_morse
+    # pot_viric_all: real-space + SPME virial with the self and net-charge terms
+    g = float(vir["pot_viri_coul"]) + e["pot_ewc"] + e["pot_ewnq"]
+    assert abs(g - want["pot_viric_all"]) <= 1e-7 * abs(want["pot_viric_all"])
+    # angle and torsion forces carry no scalar virial (recorded ~1e-32 J)
+    assert abs(float(vir["atm_viri_angl"])) < 1e-12 * abs(want["atm_viribo_all"])
+    assert abs(float(vir["atm_viri_tors"])) < 1e-12 * abs(want["atm_viribo_all"])
+    # preatmt_vtot: the virial tensor of every term; measured within 9.2e-6 of its largest entry
+    # (the zz entry, dominated by the Morse slab, is the most sensitive to the rounded positions)
+    tens = sum(vir[k] for k in ("pot_virit_coul", "pot_virit_lj", "pot_virit_mor", "atm_virit_bond",
+                                "atm_virit_angl", "atm_virit_tors", "atm_virit_14")).reshape(3, 3).T
+    rec = np.array([[want[f"preatmt_vtot{i}{j}"] for j in (1, 2, 3)] for i in (1, 2, 3)])
+    assert np.abs(tens - rec).max() <= 3e-5 * np.abs(rec).max()
 
 
 def test_ring14_rb_reset_is_what_the_reference_ran(oracle_mod):
