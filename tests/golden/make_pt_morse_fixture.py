@@ -47,7 +47,7 @@ EPS0 = 8.854187817e-12
 EPS0REF = QREF ** 2 / EREF / XREF              # calbase.F90:71
 CHARGE_SCALE = 1.0 / math.sqrt(4.0 * math.pi * (EPS0 / EPS0REF))   # prepmd.F90:241
 
-ENE_KEYS = ("pot_tot", "pot_nonbon", "pot_bon", "pot_coul", "pot_vdw", "pot_elc", "pot_ewk", "pot_ewc",
+ENE_KEYS = ("ene_kin", "pot_tot", "pot_nonbon", "pot_bon", "pot_coul", "pot_vdw", "pot_elc", "pot_ewk", "pot_ewc",
             "pot_ewnq", "pot_vdw14", "pot_elc14", "pot_bond", "pot_angl", "pot_tors", "pot_torsrb", "pot_mor")
 
 
@@ -119,7 +119,8 @@ def read_records(path):
 
 
 def read_out_pos(path):
-    """outpos (output_data.F90:381-385): step, then (i, x, y, z, atmtyp) per atom, REAL*4 [m]."""
+    """outpos / outvel (output_data.F90:381-385, :430-436): step, then
+    (i, x, y, z, atmtyp) per atom, REAL*4 [m] or [m/s]."""
     recs = read_records(path)
     step = struct.unpack("<i", recs[0])[0]
     idx, xyz, typ = [], [], []
@@ -278,6 +279,9 @@ def main(ref):
     step, pos_m, ptyp = read_out_pos(os.path.join(ref, "out_pos.dat"))
     if ptyp != b["atmtyp"]:
         raise ValueError("atom types of out_pos.dat differ from the topology order")
+    vstep, vel_ms, vtyp = read_out_pos(os.path.join(ref, "out_vel.dat"))   # outvel: same record layout [m/s]
+    if vstep != step or vtyp != ptyp:
+        raise ValueError("out_vel.dat does not match out_pos.dat")
     ene = [r for r in read_out_ene(os.path.join(ref, "out_ene.dat")) if int(r["nstep"]) == step]
     if len(ene) != 1:
         raise ValueError("no out_ene.dat record for the out_pos.dat step")
@@ -289,6 +293,7 @@ def main(ref):
     ini = b["ini"]
     g = b["g"]
     an, mref = 6.0221367e23, 1.99431e-26                       # rdpara.F90:64, main_md.F90:395
+    vref = math.sqrt(EREF / mref)                              # calbase.F90:66
     names = b["names"]
     tix = np.array([names.index(t) + 1 for t in b["atmtyp"]], np.int32)
     params = dict(xcel=g("xcel") / XREF, ycel=g("ycel") / XREF, zcel=g("zcel") / XREF,
@@ -298,13 +303,13 @@ def main(ref):
                   rcutmor=g("rcutmor") / XREF, rcut_bookmor=g("rcut_bookmor") / XREF,
                   ifnetqcorrp=int(ini["ifnetqcorrp"][0][0].lower().startswith(".t")))
     np.savez_compressed(
-        OUT, step=step, pos_m=pos_m, atmindex=tix, type_names=np.array(names),
+        OUT, step=step, pos_m=pos_m, vel_ms=vel_ms, atmindex=tix, type_names=np.array(names),
         mass_t=b["mass_t"] * 1.0e-3 / an / mref, chrg_t=b["chrg_t"] * CHARGE_SCALE,
         vdw_welij=b["welij"], vdw_radij=b["radij"], inttyp=b["inttyp"],
         mor_wel=b["welmor"], mor_rad=b["radmor"], mor_alpha=b["almor"],
         mol_sizes=np.array(b["mol_sizes"], np.int32),
         params_keys=np.array(list(params)), params_vals=np.array(list(params.values()), float),
-        ene_keys=np.array(ENE_KEYS), ene_joule=np.array([ene[0][k] for k in ENE_KEYS]), eref=EREF, xref=XREF,
+        ene_keys=np.array(ENE_KEYS), ene_joule=np.array([ene[0][k] for k in ENE_KEYS]), eref=EREF, xref=XREF, vref=vref,
         pre_keys=np.array(pre_keys), pre_joule=np.array([pre[0][k] for k in pre_keys]),
         **b["fix"])
     print("wrote", OUT, "natom", len(tix), "step", step)

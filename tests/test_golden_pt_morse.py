@@ -50,7 +50,8 @@ def load_pt_morse(precision=abi.PREC_FP64):
     iex, lex = S._mkexcl(natom, z["bonds"], z["angles"], z["tors"], z["torsrb"])
     s = S.System(
         name="pt_morse_6364", natom=natom, box=box,
-        atmcor=z["pos_m"].astype(np.float64) / float(z["xref"]), atmvel=np.zeros((natom, 3)),
+        atmcor=z["pos_m"].astype(np.float64) / float(z["xref"]),
+        atmvel=z["vel_ms"].astype(np.float64) / float(z["vref"]),
         atmmass=z["mass_t"][tix - 1], atmchrg=z["chrg_t"][tix - 1], atmindex=tix,
         type_names=[str(t) for t in z["type_names"]],
         vdw_radij=z["vdw_radij"], vdw_welij=z["vdw_welij"],
@@ -133,6 +134,15 @@ def test_oracle_matches_recorded_coulomb_virial_and_tensor(pt_morse):
                                 "atm_virit_angl", "atm_virit_tors", "atm_virit_14")).reshape(3, 3).T
     rec = np.array([[want[f"preatmt_vtot{i}{j}"] for j in (1, 2, 3)] for i in (1, 2, 3)])
     assert np.abs(tens - rec).max() <= 3e-5 * np.abs(rec).max()
+
+
+def test_oracle_kinetic_energy_matches_recorded(oracle_mod):
+    """ene_kin of out_ene.dat = half the oracle's sum m v^2 (calkin) over the
+    recorded velocities: pins the mass and velocity units (rdpara.F90:461,
+    calbase.F90:66)."""
+    s, want = load_pt_morse()
+    o = oracle_mod.Oracle(s)
+    assert abs(0.5 * o.kint() - want["ene_kin"]) <= 1e-7 * want["ene_kin"]
 
 
 def test_ring14_rb_reset_is_what_the_reference_ran(oracle_mod):
