@@ -134,6 +134,26 @@ def read_out_pos(path):
     return step, np.array(xyz, np.float32), typ
 
 
+def read_state_record(path):
+    """wrsta (wrsta.F90:8-180) state record: '#nstep', and per atom in the
+    #poly / #water / #matom sections: index, x y z [m], vx vy vz [m/s], type."""
+    step, cor, vel, typ, sec = None, [], [], [], None
+    for line in open(path):
+        w = line.split()
+        if not w:
+            continue
+        if w[0].startswith("#"):
+            sec = w[0]
+            if w[0] == "#nstep":
+                step = int(w[1])
+            continue
+        if sec in ("#poly", "#water", "#matom"):
+            cor.append([fnum(q) for q in w[1:4]])
+            vel.append([fnum(q) for q in w[4:7]])
+            typ.append(w[7])
+    return step, np.array(cor), np.array(vel), typ
+
+
 def read_out_ene(path):
     """outene: header line of names, then one line per output step [J]."""
     lines = [ln.split() for ln in open(path) if ln.strip()]
@@ -276,12 +296,22 @@ def build(ref):
 
 def main(ref):
     b = build(ref)
-    step, pos_m, ptyp = read_out_pos(os.path.join(ref, "out_pos.dat"))
+    ini = b["ini"]
+    step, pos32, ptyp = read_out_pos(os.path.join(ref, "out_pos.dat"))
     if ptyp != b["atmtyp"]:
         raise ValueError("atom types of out_pos.dat differ from the topology order")
-    vstep, vel_ms, vtyp = read_out_pos(os.path.join(ref, "out_vel.dat"))   # outvel: same record layout [m/s]
+    vstep, vel32, vtyp = read_out_pos(os.path.join(ref, "out_vel.dat"))    # outvel: same record layout [m/s]
     if vstep != step or vtyp != ptyp:
         raise ValueError("out_vel.dat does not match out_pos.dat")
+    # the state record of the same step holds the same configuration in
+    # double precision (E24.16): use it, after checking it against the
+    # single-precision outputs
+    sstep, pos_m, vel_ms, styp = read_state_record(os.path.join(ref, ini["iostarecname"][0][0]))
+    if sstep != step or styp != ptyp:
+        raise ValueError("state record is not the out_pos.dat step")
+    if np.abs(pos_m - pos32).max() > 1e-6 * np.abs(pos_m).max() or \
+            np.abs(vel_ms - vel32).max() > 1e-6 * np.abs(vel_ms).max():
+        raise ValueError("state record differs from out_pos.dat / out_vel.dat beyond single precision")
     ene = [r for r in read_out_ene(os.path.join(ref, "out_ene.dat")) if int(r["nstep"]) == step]
     if len(ene) != 1:
         raise ValueError("no out_ene.dat record for the out_pos.dat step")
@@ -290,7 +320,6 @@ def main(ref):
     if len(pre) != 1:
         raise ValueError("no out_pre.dat record for the out_pos.dat step")
     pre_keys = [k for k in pre[0] if k.startswith(("pot_viri", "atm_viri", "preatmt_vtot"))]
-    ini = b["ini"]
     g = b["g"]
     an, mref = 6.0221367e23, 1.99431e-26                       # rdpara.F90:64, main_md.F90:395
     vref = math.sqrt(EREF / mref)                              # calbase.F90:66
