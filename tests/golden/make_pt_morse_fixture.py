@@ -306,7 +306,19 @@ def main(ref):
     # the state record of the same step holds the same configuration in
     # double precision (E24.16): use it, after checking it against the
     # single-precision outputs
-    sstep, pos_m, vel_ms, styp = read_state_record(os.path.join(ref, ini["iostarecname"][0][0]))
+    sta_path = os.path.join(ref, ini["iostarecname"][0][0])
+    sstep, pos_m, vel_ms, styp = read_state_record(sta_path)
+    # raw text of the record (wrsta.F90 formats): header, the first and last
+    # atoms of each section and the chain sections, for the format tests
+    raw = open(sta_path).read().split("\n")
+    tags = [i for i, ln in enumerate(raw) if ln.strip().startswith("#")]
+    keep = set(range(0, tags[tags.index(next(i for i in tags if raw[i].strip() == "#poly"))] + 1))
+    for t in tags:
+        if raw[t].strip() in ("#poly", "#water", "#matom"):
+            keep.update(range(t, min(t + 13, len(raw))))
+        if raw[t].strip() == "#nhc":
+            keep.update(range(t - 13, len(raw)))
+    sta_lines = [(i, raw[i]) for i in sorted(keep) if i < len(raw)]
     if sstep != step or styp != ptyp:
         raise ValueError("state record is not the out_pos.dat step")
     if np.abs(pos_m - pos32).max() > 1e-6 * np.abs(pos_m).max() or \
@@ -339,6 +351,7 @@ def main(ref):
         mol_sizes=np.array(b["mol_sizes"], np.int32),
         params_keys=np.array(list(params)), params_vals=np.array(list(params.values()), float),
         ene_keys=np.array(ENE_KEYS), ene_joule=np.array([ene[0][k] for k in ENE_KEYS]), eref=EREF, xref=XREF, vref=vref,
+        sta_line_no=np.array([i for i, _ in sta_lines]), sta_line_text=np.array([t for _, t in sta_lines]),
         pre_keys=np.array(pre_keys), pre_joule=np.array([pre[0][k] for k in pre_keys]),
         **b["fix"])
     print("wrote", OUT, "natom", len(tix), "step", step)

@@ -60,3 +60,36 @@ def test_device_checkpoint_restart(tmp_path):
     xb, vb, boxb = b.download_state()
     np.testing.assert_allclose(xb, x, rtol=2e-15, atol=1e-13)
     np.testing.assert_allclose(vb, v, rtol=2e-15, atol=1e-18)
+
+
+def test_reference_state_record_lines_reproduced():
+    """Lines of the reference's own state record (sta_peachgk-2.0.dat of its
+    Pt/Morse sample, kept in tests/golden/pt_morse_step1.npz) rendered again
+    from their values by the writer's line functions: byte-identical header,
+    section tags, atom lines ('(I10,6E24.16,A3)') and chain sections."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "pt_morse_step1.npz"))
+    lines = dict(zip((int(i) for i in z["sta_line_no"]), (str(t) for t in z["sta_line_text"])))
+    num = R._num
+    box = [num(lines[k].split()[1]) for k in (10, 12, 14)]
+    hdr = R.header_lines(int(lines[0].split()[1]), int(lines[2].split()[1]), int(lines[4].split()[1]),
+                         int(lines[6].split()[1]), int(lines[8].split()[1]), box, int(lines[16].split()[1]))
+    assert hdr == [lines[k] for k in range(18)]
+    tags = {t for t in lines.values() if t.strip() in ("#poly", "#water", "#matom")}
+    assert tags <= {" #poly", "#water", "#matom"} and " #poly" in tags
+    natom_lines = 0
+    for k, t in lines.items():
+        f = t.split()
+        if len(f) == 8 and f[0].isdigit():
+            x = [num(q) for q in f[1:4]]
+            v = [num(q) for q in f[4:7]]
+            assert R.atom_line(int(f[0]), x, v, f[7]) == t
+            natom_lines += 1
+    assert natom_lines >= 20
+    k0 = next(k for k, t in lines.items() if t == "#nhc")
+    nhc = [lines[k].split() for k in range(k0 + 1, k0 + 4)]
+    ander = lines[k0 + 6].split()
+    aniso = lines[k0 + 9].split()
+    got = R.chain_lines([num(a[1]) for a in nhc], [num(a[2]) for a in nhc], num(ander[1]), num(ander[2]),
+                        [num(q) for q in aniso[1:4]], [num(q) for q in aniso[4:13]])
+    assert got == [lines[k] for k in range(k0, k0 + len(got))]

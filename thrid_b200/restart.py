@@ -46,6 +46,35 @@ def _section_atoms(system, npoly_mol):
     return [[int(a) for a in ml[mi[m]:mi[m + 1]]] for m in range(system.nmole)]
 
 
+def header_lines(npoly, nwater, nmatom, natom, mchain, box_si, nstep):
+    """Header of a state record (wrsta.F90:56-73), each line followed by the
+    empty record of a bare list-directed write."""
+    L = [f"#npoly{npoly:8d}", f"#nwater{nwater:8d}", f"#nmatom{nmatom:8d}", f"#natom{natom:10d}",
+         f"#mchain{mchain:3d}", "#xcel" + fortran_e(box_si[0]), "#ycel" + fortran_e(box_si[1]),
+         "#zcel" + fortran_e(box_si[2]), f"#nstep{int(nstep):12d}"]
+    out = []
+    for ln in L:
+        out += [ln, ""]
+    return out
+
+
+def atom_line(k, x_si, v_si, tname):
+    """One atom of a #poly / #water / #matom section, '(I10,6E24.16,A3)'
+    (wrsta.F90:89-96): positions [m], velocities [m/s], type right-justified."""
+    return f"{k:10d}" + "".join(fortran_e(q) for q in (*x_si, *v_si)) + tname[:3].rjust(3)
+
+
+def chain_lines(xlogs, vlogs_si, vlogv_si, pint_si, vboxg_si, pintt_si):
+    """#nhc, #andersen, #andersen_aniso and #end (wrsta.F90:148-175)."""
+    L = ["#nhc"]
+    for i, (a, b) in enumerate(zip(xlogs, vlogs_si)):
+        L.append(f"{i + 1:10d}" + fortran_e(a) + fortran_e(b))
+    L += ["", "#andersen", f"{1:10d}" + fortran_e(vlogv_si) + fortran_e(pint_si), "", "#andersen_aniso",
+          f"{1:10d}" + "".join(fortran_e(q) for q in vboxg_si) + "".join(fortran_e(q) for q in pintt_si),
+          "", "#end"]
+    return L
+
+
 def write_sta(path, system, atmcor, atmvel, box, chain, nstep, mchain=3, npoly=None, nwater=None, nmatom=None):
     """Write a state record.  npoly / nwater / nmatom count the molecules of
     the three sections in topology order (poly first, then water, then
@@ -62,40 +91,20 @@ def write_sta(path, system, atmcor, atmvel, box, chain, nstep, mchain=3, npoly=N
         raise ValueError("npoly + nwater + nmatom must equal the number of molecules")
     xref, vref, tref, pref = S.XREF, S.VREF, S.TIMEREF, S.PREF
     names = system.type_names
-    L = []
-    L.append(f"#npoly{npoly:8d}"); L.append("")
-    L.append(f"#nwater{nwater:8d}"); L.append("")
-    L.append(f"#nmatom{nmatom:8d}"); L.append("")
-    L.append(f"#natom{system.natom:10d}"); L.append("")
-    L.append(f"#mchain{mchain:3d}"); L.append("")
-    for key, v in (("#xcel", box[0]), ("#ycel", box[1]), ("#zcel", box[2])):
-        L.append(key + fortran_e(v * xref)); L.append("")
-    L.append(f"#nstep{int(nstep):12d}"); L.append("")
+    L = header_lines(npoly, nwater, nmatom, system.natom, mchain, [q * xref for q in box], nstep)
     k = 0
-    bounds = (("#poly", 0, npoly), ("#water", npoly, npoly + nwater), ("#matom", npoly + nwater, len(mols)))
+    # section tags as wrsta.F90:79,102,125 write them: '(A6)', so the 5-letter '#poly' is right-justified
+    bounds = ((" #poly", 0, npoly), ("#water", npoly, npoly + nwater), ("#matom", npoly + nwater, len(mols)))
     for tag, m0, m1 in bounds:
         L.append(tag)
         for m in range(m0, m1):
             for a in mols[m]:
                 k += 1
-                x = atmcor[a] * xref
-                v = atmvel[a] * vref
-                tname = names[system.atmindex[a] - 1][:3].rjust(3)
-                L.append(f"{k:10d}" + "".join(fortran_e(q) for q in (*x, *v)) + tname)
+                L.append(atom_line(k, atmcor[a] * xref, atmvel[a] * vref, names[system.atmindex[a] - 1]))
         L.append("")
-    L.append("#nhc")
-    for i in range(mchain):
-        L.append(f"{i + 1:10d}" + fortran_e(chain.xlogs[i]) + fortran_e(chain.vlogs[i] / tref))
-    L.append("")
-    L.append("#andersen")
-    L.append(f"{1:10d}" + fortran_e(chain.vlogv / tref) + fortran_e(chain.pint * pref))
-    L.append("")
-    L.append("#andersen_aniso")
-    pt = [chain.pintt[q] for q in range(9)]
-    L.append(f"{1:10d}" + "".join(fortran_e(chain.vboxg[d] / tref) for d in range(3))
-             + "".join(fortran_e(q * pref) for q in pt))
-    L.append("")
-    L.append("#end")
+    L += chain_lines([chain.xlogs[i] for i in range(mchain)], [chain.vlogs[i] / tref for i in range(mchain)],
+                     chain.vlogv / tref, chain.pint * pref, [chain.vboxg[d] / tref for d in range(3)],
+                     [chain.pintt[q] * pref for q in range(9)])
     with open(path, "w") as f:
         f.write("\n".join(L) + "\n")
 
