@@ -1,9 +1,10 @@
 """Known-answer checks that pin the FP64 CPU oracle (no GPU).
 
-The reference tree has no tests and no golden vectors for this path, and its
-Fortran cannot be compiled here, so the oracle is pinned by analytical
-answers: FFT vs a direct DFT, B-spline partition of unity, spline tables vs
-erfc/erf, the Madelung constant of rock salt, LJ two-body values,
+The reference has no tests and its Fortran cannot be compiled here.  Its
+recorded Pt/Morse run pins every energy and virial term
+(tests/test_golden_pt_morse.py); these analytical answers pin what a recorded
+energy cannot show: FFT vs a direct DFT, B-spline partition of unity, spline
+tables vs erfc/erf, the Madelung constant of rock salt, LJ two-body values,
 finite-difference forces, constraint residuals and energy conservation.
 """
 import math
