@@ -76,7 +76,9 @@ typedef struct pgk_system {
     int32_t        ntyp;
     const double*  vdw_radij;     /* [ntyp*ntyp] column-major (i,j): R_min,ij  */
     const double*  vdw_welij;     /* [ntyp*ntyp] well depth E_ij              */
-    const int32_t* inter_inttyp;  /* [ntyp*ntyp] 1 = INTTYPE_VDW, else no LJ; NULL = all LJ */
+    const int32_t* inter_inttyp;  /* [ntyp*ntyp] 1 = INTTYPE_VDW (LJ), 2 = INTTYPE_MOR (no LJ;
+                                     Morse when switched on); 3..10 (SH, RFH, DOU, RP-VW,
+                                     custom) return PGK_E_UNSUPPORTED; NULL = all LJ */
 
     int32_t        nmole;         /* molecules (transcor.F90, calpress.F90)    */
     const int32_t* molept_index;  /* [nmole+1], 1-based                        */
@@ -120,7 +122,9 @@ typedef struct pgk_system {
      * D (exp(-2a(r-r0)) - 2 exp(-a(r-r0))) instead of LJ.  [ntyp*ntyp]
      * column-major like vdw_radij; NULL = no Morse pairs.  The device engine
      * does not build Morse yet: pgk_init returns PGK_E_UNSUPPORTED when a
-     * Morse pair type is present (the oracle restates it). */
+     * Morse pair type is present and mts_mor is not PGK_MTS_NONE (the oracle
+     * restates it); with mts_mor = PGK_MTS_NONE Morse is switched off, as in
+     * the reference, and those pairs carry neither Morse nor LJ. */
     const double  *para_welmor, *para_radmor, *para_alphamor;
 } pgk_system;
 

@@ -169,3 +169,29 @@ def test_engine_reports_morse_unsupported():
     h = C.c_void_p()
     assert L.pgk_init(C.byref(cs.struct), C.byref(ps), C.byref(h)) == abi.PGK_E_UNSUPPORTED
     assert not h.value
+
+
+def test_engine_input_checks_for_pair_types():
+    """Morse switched off (mts_mor = none) is accepted up to the device check;
+    pair potentials the engine does not build are refused before any device
+    call; an out-of-range type code is invalid."""
+    import ctypes as C
+    from thrid_b200 import pgk
+    L = pgk.lib()
+
+    def init(s):
+        cs = abi.CSystem(s)
+        ps = abi.params_struct(s.params)
+        h = C.c_void_p()
+        st = L.pgk_init(C.byref(cs.struct), C.byref(ps), C.byref(h))
+        if h.value:
+            L.pgk_free(h)
+        return st
+    s, _ = load_pt_morse()
+    for code, want in ((3, abi.PGK_E_UNSUPPORTED), (10, abi.PGK_E_UNSUPPORTED), (11, abi.PGK_E_INVALID)):
+        s.inttyp = s.inttyp.copy()
+        s.inttyp[0, 1] = s.inttyp[1, 0] = code
+        assert init(s) == want
+    s, _ = load_pt_morse()
+    s.params["mts_mor"] = 0                                        # PGK_MTS_NONE: Morse switched off
+    assert init(s) not in (abi.PGK_E_UNSUPPORTED, abi.PGK_E_INVALID)   # passes the pair-type checks

@@ -243,9 +243,13 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         return PGK_E_INVALID;
     if (p->precision != PGK_PREC_FP64 && p->precision != PGK_PREC_MIXED) return PGK_E_INVALID;
     if (p->rcut_book <= 0 || p->rcut <= 0 || p->rrcut <= 0) return PGK_E_INVALID;
-    if (s->inter_inttyp && s->para_welmor)   // Morse pairs (morse.F90): restated by the oracle, not on the device
-        for (int k = 0; k < s->ntyp * s->ntyp; ++k)
-            if (s->inter_inttyp[k] == 2) return PGK_E_UNSUPPORTED;
+    if (s->inter_inttyp)   // pair potentials other than LJ (md_global.inc:119-128) are not on the device
+        for (int k = 0; k < s->ntyp * s->ntyp; ++k) {
+            const int t = s->inter_inttyp[k];
+            if (t < 1 || t > 10) return PGK_E_INVALID;
+            if (t >= 3) return PGK_E_UNSUPPORTED;                            // SH, RFH, DOU, RP-VW, custom
+            if (t == 2 && s->para_welmor && p->mts_mor != PGK_MTS_NONE) return PGK_E_UNSUPPORTED;   // Morse
+        }
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return PGK_E_CUDA;
     pgk_ctx* c = new pgk_ctx();
