@@ -75,6 +75,7 @@ def lib():
         L.orc_philox.argtypes = [C.c_uint64, C.c_longlong, C.c_int, pd]
         L.orc_ewk_nvec.argtypes = [C.c_int, C.c_double, C.c_double, pi, C.c_int, pi]
         L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
+        L.orc_spme_hf_atm.argtypes = [vp, pd, pd]
         _lib = L
     return _lib
 
@@ -224,6 +225,16 @@ class Oracle:
             raise RuntimeError(f"orc_ewaldkp_hf status {st}")
         return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=sc[0], pot_ewk_cc=sc[1],
                     pot_virit_coul=sc[2:].reshape(3, 3), nwave=nw.value)
+
+    def spme_hf_atm(self):
+        """Per-atom split of fft_pmep: pot_atm (N) with the self term and
+        viri_atm (N,3,3), viri_atm[i, b, a] = tensor(a,b) of atom i."""
+        n = self.sys.natom
+        pot = np.zeros(n); vir = np.zeros((n, 3, 3))
+        st = self.L.orc_spme_hf_atm(self.h, _p(pot), _p(vir))
+        if st:
+            raise RuntimeError(f"orc_spme_hf_atm status {st}")
+        return pot, vir
 
     def langevin_dekin(self):
         out = np.zeros(abi.LT_MAX_REGIONS)

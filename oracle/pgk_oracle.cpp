@@ -517,13 +517,13 @@ void ewaldrp(Oracle& o, double* force, pgk_energies* e, pgk_virials* v) {
 // --------------------------------------------------------------------------
 // fft_pmep (fft_pme.F90:144-270) + helpers :273-937
 // --------------------------------------------------------------------------
-void fft_pmep(Oracle& o, double* force, pgk_energies* e, pgk_virials* v) {
+// get_scaled_fractionals + get_bspline_coeffs (fft_pme.F90:273-356): scaled
+// fractional coordinates fr (3,N) and B-spline weights th, dth (p,3,N)
+void spme_bspline(const Oracle& o, std::vector<double>& fr, std::vector<double>& th, std::vector<double>& dth) {
     int n = o.natom, p = o.prm.pme_order;
-    int K1 = o.prm.nfft1, K2 = o.prm.nfft2, K3 = o.prm.nfft3;
+    int Kd[3] = {o.prm.nfft1, o.prm.nfft2, o.prm.nfft3};
     double recip[3] = {1.0 / o.box[0], 1.0 / o.box[1], 1.0 / o.box[2]};
-    double vol = o.box[0] * o.box[1] * o.box[2];
-    std::vector<double> fr((size_t)3 * n), th((size_t)3 * p * n), dth((size_t)3 * p * n);
-    int Kd[3] = {K1, K2, K3};
+    fr.assign((size_t)3 * n, 0.0); th.assign((size_t)3 * p * n, 0.0); dth.assign((size_t)3 * p * n, 0.0);
     for (int a = 0; a < n; ++a)
         for (int d = 0; d < 3; ++d) {
             double w = o.atmcor[3 * a + d] * recip[d];           // get_scaled_fractionals
@@ -532,47 +532,70 @@ void fft_pmep(Oracle& o, double* force, pgk_energies* e, pgk_virials* v) {
             double ww = fr[3 * a + d] - std::trunc(fr[3 * a + d]);  // get_bspline_coeffs (dint)
             fill_bspline(ww, p, &th[((size_t)3 * a + d) * p], &dth[((size_t)3 * a + d) * p]);
         }
-    size_t KK = (size_t)K1 * K2 * K3;
-    std::vector<cplx> Q(KK, cplx(0, 0));
-    auto wrap = [](int k0, int K) { return k0 >= 0 ? k0 : k0 + K; };
-    for (int a = 0; a < n; ++a) {               // fill_charge_grid :359-422
+}
+
+inline int spme_wrap(int k0, int K) { return k0 >= 0 ? k0 : k0 + K; }
+
+// fill_charge_grid (fft_pme.F90:359-422): Q(re) += q theta1 theta2 theta3
+void spme_spread(const Oracle& o, const std::vector<double>& fr, const std::vector<double>& th, std::vector<cplx>& Q) {
+    int n = o.natom, p = o.prm.pme_order;
+    int K1 = o.prm.nfft1, K2 = o.prm.nfft2, K3 = o.prm.nfft3;
+    Q.assign((size_t)K1 * K2 * K3, cplx(0, 0));
+    for (int a = 0; a < n; ++a) {
         const double* t1 = &th[((size_t)3 * a + 0) * p];
         const double* t2 = &th[((size_t)3 * a + 1) * p];
         const double* t3 = &th[((size_t)3 * a + 2) * p];
         int k0 = (int)fr[3 * a + 2] - p;
         for (int i3 = 0; i3 < p; ++i3) {
             k0 += 1;
-            int k = wrap(k0, K3);
+            int k = spme_wrap(k0, K3);
             double prod1 = t3[i3] * o.atmchrg[a];
             int j0 = (int)fr[3 * a + 1] - p;
             for (int i2 = 0; i2 < p; ++i2) {
                 j0 += 1;
-                int j = wrap(j0, K2);
+                int j = spme_wrap(j0, K2);
                 double prod = t2[i2] * prod1;
                 int ii0 = (int)fr[3 * a] - p;
                 for (int i1 = 0; i1 < p; ++i1) {
                     ii0 += 1;
-                    int i = wrap(ii0, K1);
+                    int i = spme_wrap(ii0, K1);
                     Q[(size_t)i + (size_t)K1 * (j + (size_t)K2 * k)] += t1[i1] * prod;
                 }
             }
         }
     }
-    // fft_back = pubz3d(isign=-1): x, y, z passes of cfftf
-    auto pass3 = [&](int sign) {
-        par_chunks(o.nthreads, K3, [&](long long b, long long e_, int) {
-            for (long long k = b; k < e_; ++k)
-                for (int j = 0; j < K2; ++j) fft1d(&Q[(size_t)K1 * (j + (size_t)K2 * k)], K1, 1, sign);
-        });
-        par_chunks(o.nthreads, K3, [&](long long b, long long e_, int) {
-            for (long long k = b; k < e_; ++k)
-                for (int i = 0; i < K1; ++i) fft1d(&Q[(size_t)i + (size_t)K1 * K2 * k], K2, K1, sign);
-        });
-        par_chunks(o.nthreads, K2, [&](long long b, long long e_, int) {
-            for (long long j = b; j < e_; ++j)
-                for (int i = 0; i < K1; ++i) fft1d(&Q[(size_t)i + (size_t)K1 * j], K3, K1 * K2, sign);
-        });
-    };
+}
+
+// pubz3d: x, y, z passes of cfftf (sign -1) or cfftb (sign +1)
+void spme_fft3(const Oracle& o, std::vector<cplx>& Q, int sign) {
+    int K1 = o.prm.nfft1, K2 = o.prm.nfft2, K3 = o.prm.nfft3;
+    par_chunks(o.nthreads, K3, [&](long long b, long long e_, int) {
+        for (long long k = b; k < e_; ++k)
+            for (int j = 0; j < K2; ++j) fft1d(&Q[(size_t)K1 * (j + (size_t)K2 * k)], K1, 1, sign);
+    });
+    par_chunks(o.nthreads, K3, [&](long long b, long long e_, int) {
+        for (long long k = b; k < e_; ++k)
+            for (int i = 0; i < K1; ++i) fft1d(&Q[(size_t)i + (size_t)K1 * K2 * k], K2, K1, sign);
+    });
+    par_chunks(o.nthreads, K2, [&](long long b, long long e_, int) {
+        for (long long j = b; j < e_; ++j)
+            for (int i = 0; i < K1; ++i) fft1d(&Q[(size_t)i + (size_t)K1 * j], K3, K1 * K2, sign);
+    });
+}
+
+void fft_pmep(Oracle& o, double* force, pgk_energies* e, pgk_virials* v) {
+    int n = o.natom, p = o.prm.pme_order;
+    int K1 = o.prm.nfft1, K2 = o.prm.nfft2, K3 = o.prm.nfft3;
+    double recip[3] = {1.0 / o.box[0], 1.0 / o.box[1], 1.0 / o.box[2]};
+    double vol = o.box[0] * o.box[1] * o.box[2];
+    std::vector<double> fr, th, dth;
+    spme_bspline(o, fr, th, dth);
+    size_t KK = (size_t)K1 * K2 * K3;
+    std::vector<cplx> Q;
+    spme_spread(o, fr, th, Q);
+    auto wrap = spme_wrap;
+    auto pass3 = [&](int sign) { spme_fft3(o, Q, sign); };
+    // fft_back = pubz3d(isign=-1)
     pass3(-1);
     // scalar_sum :544-690
     double pi = 3.14159265358979323846;
@@ -670,6 +693,93 @@ void fft_pmep(Oracle& o, double* force, pgk_energies* e, pgk_virials* v) {
         for (int k = 0; k < 9; ++k) v->pot_virit_coul[k] -= 0.5 * vfull[k];
         v->pot_viri_coul += pot_ewk + vsca;
     }
+}
+
+// Per-atom split of fft_pmep's reciprocal energy and virial tensor for the
+// bulk heat flux: the SPME form of ewaldkp_hf's per-atom terms
+// (ewaldk_hf.F90:165-173, :212-230), which the reference has only for
+// standard Ewald.  With S = FFT(Q) and the influence function eterm of
+// scalar_sum (fft_pme.F90:544-690),
+//   pot_atm(i)      = 1/2 q_i sum_g theta_i(g) IFFT(eterm S)(g) - alpha/sqrt(pi) q_i^2
+//   viri_atm(a,b,i) = 1/2 q_i sum_g theta_i(g) IFFT(eterm (delta_ab - vterm h_a h_b) S)(g)
+// so the atoms' energies (less the self term) sum to pot_ewk and their
+// tensors to fft_pmep's pot_virit_coul (before the net-charge terms, which
+// are global and not split).  viri_atm is (3,3,N), [a + 3b + 9i].
+void spme_hf_atm(Oracle& o, double* pot_atm, double* viri_atm) {
+    int n = o.natom, p = o.prm.pme_order;
+    int K1 = o.prm.nfft1, K2 = o.prm.nfft2, K3 = o.prm.nfft3;
+    double recip[3] = {1.0 / o.box[0], 1.0 / o.box[1], 1.0 / o.box[2]};
+    double vol = o.box[0] * o.box[1] * o.box[2];
+    std::vector<double> fr, th, dth;
+    spme_bspline(o, fr, th, dth);
+    std::vector<cplx> Q;
+    spme_spread(o, fr, th, Q);
+    spme_fft3(o, Q, -1);
+    const size_t KK = (size_t)K1 * K2 * K3;
+    // grids: 0 potential, 1..6 tensor xx xy xz yy yz zz
+    std::vector<std::vector<cplx>> G(7, std::vector<cplx>(KK, cplx(0, 0)));
+    const double pi = 3.14159265358979323846;
+    const double rk2 = o.rkcut * o.rkcut, fac = pi * pi / (o.prm.alpha * o.prm.alpha);
+    int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
+    int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
+    int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
+    for (size_t ind = 1; ind < KK; ++ind) {
+        int k3 = (int)(ind / ((size_t)K1 * K2));
+        size_t jnd = ind - (size_t)k3 * K1 * K2;
+        int k2 = (int)(jnd / K1), k1 = (int)(jnd - (size_t)k2 * K1);
+        int m1 = k1 < nf1 ? k1 : k1 - K1;
+        int m2 = k2 < nf2 ? k2 : k2 - K2;
+        int m3 = k3 < nf3 ? k3 : k3 - K3;
+        double h[3] = {recip[0] * m1, recip[1] * m2, recip[2] * m3};
+        double msq = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+        if (msq > rk2) continue;
+        double denom = pi * vol * o.bsp[0][k1] * o.bsp[1][k2] * o.bsp[2][k3] * msq;
+        double eterm = std::exp(-fac * msq) / denom;
+        double vterm = 2.0 * (fac * msq + 1.0) / msq;
+        cplx es = eterm * Q[ind];
+        G[0][ind] = es;
+        const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+        for (int c = 0; c < 6; ++c) {
+            int a = ab[c][0], b = ab[c][1];
+            G[1 + c][ind] = es * ((a == b ? 1.0 : 0.0) - vterm * h[a] * h[b]);
+        }
+    }
+    for (int c = 0; c < 7; ++c) spme_fft3(o, G[c], +1);
+    const double self = o.prm.alpha / std::sqrt(pi);
+    par_chunks(o.nthreads, n, [&](long long b_, long long e_, int) {
+        for (int a = (int)b_; a < (int)e_; ++a) {
+            const double* t1 = &th[((size_t)3 * a + 0) * p];
+            const double* t2 = &th[((size_t)3 * a + 1) * p];
+            const double* t3 = &th[((size_t)3 * a + 2) * p];
+            double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+            int k0 = (int)fr[3 * a + 2] - p;
+            for (int i3 = 0; i3 < p; ++i3) {
+                k0 += 1;
+                int k = spme_wrap(k0, K3);
+                int j0 = (int)fr[3 * a + 1] - p;
+                for (int i2 = 0; i2 < p; ++i2) {
+                    j0 += 1;
+                    int j = spme_wrap(j0, K2);
+                    int ii0 = (int)fr[3 * a] - p;
+                    for (int i1 = 0; i1 < p; ++i1) {
+                        ii0 += 1;
+                        int i = spme_wrap(ii0, K1);
+                        size_t g = (size_t)i + (size_t)K1 * (j + (size_t)K2 * k);
+                        double w = t1[i1] * t2[i2] * t3[i3];
+                        for (int c = 0; c < 7; ++c) acc[c] += w * G[c][g].real();
+                    }
+                }
+            }
+            const double hq = 0.5 * o.atmchrg[a];
+            if (pot_atm) pot_atm[a] = hq * acc[0] - self * (o.atmchrg[a] * o.atmchrg[a]);
+            if (viri_atm) {
+                double* v = viri_atm + (size_t)9 * a;
+                v[0] = hq * acc[1]; v[1] = hq * acc[2]; v[2] = hq * acc[3];
+                v[3] = v[1];        v[4] = hq * acc[4]; v[5] = hq * acc[5];
+                v[6] = v[2];        v[7] = v[5];        v[8] = hq * acc[6];
+            }
+        }
+    });
 }
 
 // --------------------------------------------------------------------------
@@ -2232,6 +2342,12 @@ int orc_ewk_nvec(int kmax, double yratio, double zratio, int* out, int cap, int*
     if (s) return s;
     *nwave = (int)nv.size() / 3;
     if (out) std::copy(nv.begin(), nv.begin() + std::min((size_t)3 * cap, nv.size()), out);
+    return PGK_OK;
+}
+int orc_spme_hf_atm(void* h, double* pot_atm, double* viri) {
+    Oracle* o = (Oracle*)h;
+    if (!o->prm.ifspme) return PGK_E_INVALID;
+    spme_hf_atm(*o, pot_atm, viri);
     return PGK_OK;
 }
 int orc_ewaldkp_hf(void* h, int kmax, double* force, double* pot_atm, double* viri, double* sc, int* nwave) {
