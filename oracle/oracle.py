@@ -76,6 +76,7 @@ def lib():
         L.orc_ewk_nvec.argtypes = [C.c_int, C.c_double, C.c_double, pi, C.c_int, pi]
         L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
         L.orc_spme_hf_atm.argtypes = [vp, pd, pd]
+        L.orc_mor_list.argtypes = [vp, i64p]
         _lib = L
     return _lib
 
@@ -225,6 +226,12 @@ class Oracle:
             raise RuntimeError(f"orc_ewaldkp_hf status {st}")
         return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=sc[0], pot_ewk_cc=sc[1],
                     pot_virit_coul=sc[2:].reshape(3, 3), nwave=nw.value)
+
+    def mor_list(self):
+        """(PGK_LIST_* order, pair count) of the Morse list of the last mklist."""
+        n = C.c_longlong(0)
+        mode = self.L.orc_mor_list(self.h, C.byref(n))
+        return mode, n.value
 
     def spme_hf_atm(self):
         """Per-atom split of fft_pmep: pot_atm (N) with the self term and

@@ -110,7 +110,8 @@ struct Oracle {
     // Morse pairs (rdpara.F90:680-720), column-major (i,j) like radij
     std::vector<double> welmor, radmor, almor;
     std::vector<int> mor_atoms;            // nmorselist (linkbond.F90), 0-based
-    std::vector<int> mor_idx, mor_list;    // mklist2a_mor rows: [mor_atoms+1] starts, 0-based partners
+    std::vector<int> mor_idx, mor_list;    // Morse list rows: [mor_atoms+1] starts, 0-based partners
+    int mor_list_mode = 0;                 // PGK_LIST_* order of the last Morse list
     std::vector<int> molidx, mollist;  // 0-based
     std::vector<int> excl_idx, excl_list;  // reference CSR kept 1-based values
     // bonded
@@ -322,12 +323,14 @@ int choose_list_mode(const Oracle& o) {
     return PGK_LIST_CELL;
 }
 
-// mklist2a_mor (mklist_mor.F90:30-120): for each Morse atom, the later Morse
-// atoms of a Morse type pair inside rcut_bookmor (minimum image).  The cell
-// variant (mklist_mor_cell.F90) keeps j > i by atom index from the 27-cell
-// stencil when the rdscript.F90:1620-1635 rule allows it: the same pair set,
-// partners in another order.  Without a list radius the half-box diagonal
-// is the radius (mklist_mor.F90:30-34).
+// Morse list (rows per Morse atom, partners 0-based).  mklist2a_mor
+// (mklist_mor.F90:30-120): for each Morse atom the later Morse atoms of a
+// Morse type pair inside rcut_bookmor (minimum image), in atom order; without
+// a list radius the half-box diagonal is the radius (mklist_mor.F90:30-34).
+// mklist_mor_cell (mklist_mor_cell.F90:8-327): the same test over the 27-cell
+// stencil (z, y, x order; cell = MOD(INT((x+L)/cs), nc); j > i by atom
+// index), used when every cell count is >= 3 and there are more than 27 cells
+// (rdscript.F90:1616-1632); list_mode forces either order as for the pair list.
 void mklist_mor(Oracle& o) {
     double sqcut = o.prm.rcut_bookmor * o.prm.rcut_bookmor;
     if (o.prm.rcut_bookmor <= 0.0)
@@ -336,19 +339,58 @@ void mklist_mor(Oracle& o) {
     const int nm = (int)o.mor_atoms.size();
     o.mor_idx.assign((size_t)nm + 1, 0);
     o.mor_list.clear();
+    auto test = [&](int i, int j) {
+        if (o.inttyp[o.atmindex[i] + o.ntyp * o.atmindex[j]] != 2) return false;
+        double rij[3];
+        for (int d = 0; d < 3; ++d) {
+            double v = o.atmcor[3 * i + d] - o.atmcor[3 * j + d];
+            rij[d] = v - o.box[d] * dnint(v * (1.0 / o.box[d]));
+        }
+        double dr = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+        return dr < sqcut;
+    };
+    int nc[3] = {0, 0, 0};
+    bool cell = o.prm.rcut_bookmor > 0.0 && o.prm.list_mode != PGK_LIST_ALLPAIR;
+    if (cell) {
+        for (int d = 0; d < 3; ++d) nc[d] = (int)(o.box[d] / o.prm.rcut_bookmor);
+        if (o.prm.list_mode != PGK_LIST_CELL &&
+            (nc[0] < 3 || nc[1] < 3 || nc[2] < 3 || (long long)nc[0] * nc[1] * nc[2] <= 27))
+            cell = false;
+    }
+    o.mor_list_mode = cell ? PGK_LIST_CELL : PGK_LIST_ALLPAIR;
+    if (!cell) {
+        for (int m1 = 0; m1 < nm; ++m1) {
+            o.mor_idx[m1] = (int)o.mor_list.size();
+            const int i = o.mor_atoms[m1];
+            for (int m2 = m1 + 1; m2 < nm; ++m2)
+                if (test(i, o.mor_atoms[m2])) o.mor_list.push_back(o.mor_atoms[m2]);
+        }
+        o.mor_idx[nm] = (int)o.mor_list.size();
+        return;
+    }
+    double cs[3];
+    for (int d = 0; d < 3; ++d) cs[d] = o.box[d] / (double)nc[d];
+    std::vector<int> a2c((size_t)3 * nm);
+    std::vector<std::vector<int>> cellv((size_t)nc[0] * nc[1] * nc[2]);
+    for (int m = 0; m < nm; ++m) {
+        const int i = o.mor_atoms[m];
+        for (int d = 0; d < 3; ++d) a2c[3 * m + d] = ((int)((o.atmcor[3 * i + d] + o.box[d]) / cs[d])) % nc[d];
+        cellv[a2c[3 * m] + (size_t)nc[0] * (a2c[3 * m + 1] + (size_t)nc[1] * a2c[3 * m + 2])].push_back(i);
+    }
     for (int m1 = 0; m1 < nm; ++m1) {
         o.mor_idx[m1] = (int)o.mor_list.size();
-        const int i = o.mor_atoms[m1], it = o.atmindex[i];
-        for (int m2 = m1 + 1; m2 < nm; ++m2) {
-            const int j = o.mor_atoms[m2], jt = o.atmindex[j];
-            if (o.inttyp[it + o.ntyp * jt] != 2) continue;
-            double rij[3];
-            for (int d = 0; d < 3; ++d) {
-                double v = o.atmcor[3 * i + d] - o.atmcor[3 * j + d];
-                rij[d] = v - o.box[d] * dnint(v * (1.0 / o.box[d]));
+        const int i = o.mor_atoms[m1];
+        for (int z1 = a2c[3 * m1 + 2] - 1; z1 <= a2c[3 * m1 + 2] + 1; ++z1) {
+            const int z = (z1 + nc[2]) % nc[2];
+            for (int y1 = a2c[3 * m1 + 1] - 1; y1 <= a2c[3 * m1 + 1] + 1; ++y1) {
+                const int y = (y1 + nc[1]) % nc[1];
+                const size_t posyz = (size_t)y * nc[0] + (size_t)z * nc[0] * nc[1];
+                for (int x1 = a2c[3 * m1] - 1; x1 <= a2c[3 * m1] + 1; ++x1) {
+                    const int x = (x1 + nc[0]) % nc[0];
+                    for (int j : cellv[x + posyz])
+                        if (i < j && test(i, j)) o.mor_list.push_back(j);
+                }
             }
-            double dr = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
-            if (dr < sqcut) o.mor_list.push_back(j);
         }
     }
     o.mor_idx[nm] = (int)o.mor_list.size();
@@ -2343,6 +2385,12 @@ int orc_ewk_nvec(int kmax, double yratio, double zratio, int* out, int cap, int*
     *nwave = (int)nv.size() / 3;
     if (out) std::copy(nv.begin(), nv.begin() + std::min((size_t)3 * cap, nv.size()), out);
     return PGK_OK;
+}
+// Morse list of the last mklist: its order (PGK_LIST_*) and pair count
+int orc_mor_list(void* h, long long* npair) {
+    Oracle* o = (Oracle*)h;
+    if (npair) *npair = (long long)o->mor_list.size();
+    return o->mor_list_mode;
 }
 int orc_spme_hf_atm(void* h, double* pot_atm, double* viri) {
     Oracle* o = (Oracle*)h;

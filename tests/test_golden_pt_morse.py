@@ -195,3 +195,28 @@ def test_engine_input_checks_for_pair_types():
     s, _ = load_pt_morse()
     s.params["mts_mor"] = 0                                        # PGK_MTS_NONE: Morse switched off
     assert init(s) not in (abi.PGK_E_UNSUPPORTED, abi.PGK_E_INVALID)   # passes the pair-type checks
+
+
+def test_morse_cell_list_matches_all_pairs(oracle_mod):
+    """mklist_mor_cell and mklist2a_mor give the same Morse pairs: with
+    rcut_bookmor 12 A the slab has 3 x 3 x 10 cells, so the cell scan runs
+    (rdscript.F90:1616-1632); forcing the all-pairs order changes only the
+    summation order.  The recorded run itself used all pairs (2 x 2 x 9
+    cells at 14 A)."""
+    s, want = load_pt_morse()
+    o = oracle_mod.Oracle(s)
+    o.mklist()
+    assert o.mor_list()[0] == abi.LIST_ALLPAIR
+    out = {}
+    for mode in (abi.LIST_AUTO, abi.LIST_ALLPAIR):
+        s2, _ = load_pt_morse()
+        s2.params.update(rcut_bookmor=12.0, list_mode=mode)
+        o = oracle_mod.Oracle(s2)
+        o.mklist()
+        _, e, _ = o.calforce(abi.MTS_LONG)
+        out[mode] = (o.mor_list(), e["pot_mor"])
+    (m_cell, n_cell), e_cell = out[abi.LIST_AUTO]
+    (m_all, n_all), e_all = out[abi.LIST_ALLPAIR]
+    assert m_cell == abi.LIST_CELL and m_all == abi.LIST_ALLPAIR and n_cell == n_all
+    assert abs(e_cell - e_all) <= 1e-12 * abs(e_all)
+    assert printed(want["pot_mor"], e_cell, want["eref"])
