@@ -164,7 +164,6 @@ def read_out_ene(path):
 
 def build(ref):
     ini = read_ini(os.path.join(ref, "peachgk.ini"))
-    g = lambda k: fnum(ini[k][0][0])
     para = read_sections(os.path.join(ref, ini["iuparabondname"][0][0]))
     vdw = [w for w in (ln.split() for ln in open(os.path.join(ref, ini["iuparavdwname"][0][0])))
            if len(w) >= 5 and not w[0].startswith("#")]
@@ -291,7 +290,8 @@ def build(ref):
             ring14_rb[n] = 0.5
     fix["tors_ring"] = ring14
     fix["torsrb_ring"] = ring14_rb
-    return locals()
+    return dict(ini=ini, atmtyp=atmtyp, mol_sizes=mol_sizes, names=names, mass_t=mass_t, chrg_t=chrg_t,
+                welij=welij, radij=radij, inttyp=inttyp, welmor=welmor, radmor=radmor, almor=almor, fix=fix)
 
 
 def main(ref):
@@ -332,7 +332,7 @@ def main(ref):
     if len(pre) != 1:
         raise ValueError("no out_pre.dat record for the out_pos.dat step")
     pre_keys = [k for k in pre[0] if k.startswith(("pot_viri", "atm_viri", "preatmt_vtot"))]
-    g = b["g"]
+    g = lambda k: fnum(ini[k][0][0])
     an, mref = 6.0221367e23, 1.99431e-26                       # rdpara.F90:64, main_md.F90:395
     vref = math.sqrt(EREF / mref)                              # calbase.F90:66
     names = b["names"]
