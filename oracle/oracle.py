@@ -77,6 +77,7 @@ def lib():
         L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
         L.orc_spme_hf_atm.argtypes = [vp, pd, pd]
         L.orc_mor_list.argtypes = [vp, i64p]
+        L.orc_morse_hf_atm.argtypes = [vp, pd, pd]
         _lib = L
     return _lib
 
@@ -226,6 +227,16 @@ class Oracle:
             raise RuntimeError(f"orc_ewaldkp_hf status {st}")
         return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=sc[0], pot_ewk_cc=sc[1],
                     pot_virit_coul=sc[2:].reshape(3, 3), nwave=nw.value)
+
+    def morse_hf_atm(self):
+        """morsep_hf: per-atom Morse energy (N) and virial W (nreg,3,N) with
+        W[r, a, i] = virimort_atm(a,3,i,r); needs set_hf."""
+        n = self.sys.natom
+        pot = np.zeros(n); W = np.zeros((self._hf.nreg, 3, n))
+        st = self.L.orc_morse_hf_atm(self.h, _p(pot), _p(W))
+        if st:
+            raise RuntimeError(f"orc_morse_hf_atm status {st}")
+        return pot, W
 
     def mor_list(self):
         """(PGK_LIST_* order, pair count) of the Morse list of the last mklist."""

@@ -1527,8 +1527,13 @@ void calcom(Oracle& o, const std::vector<double>& x, std::vector<double>& out) {
 // calvirihf.F90:8-405, local volume-based branch without _HF_ALL_DIR/_HF_BULK:
 // viri(:,3,i,r) += fi * f, viri(:,3,j,r) += -fj * f, f = +-(z length of the
 // i-j segment inside slab r) * nbodycoeff
-void calvirihf(Oracle& o, int i, int j, const double* fi, const double* fj, double nbc, int cat) {
+// dst: a [1][nreg][3][N] array that takes the pair instead of category cat of
+// the per-atom arrays (the Morse term of morsep_hf)
+void calvirihf(Oracle& o, int i, int j, const double* fi, const double* fj, double nbc, int cat,
+               std::vector<double>* dst = nullptr) {
     Oracle::HF& h = o.hf;
+    double* W = dst ? dst->data() : h.W.data();
+    if (dst) cat = 0;
     int atomflag = 0;
     double zi, zj;
     if (h.hftyp[i] == PGK_HFTYP_MOLE) zi = h.molecom[3 * h.molof[i] + 2];
@@ -1558,8 +1563,8 @@ void calvirihf(Oracle& o, int i, int j, const double* fi, const double* fj, doub
         }
         double fact = rz >= 0.0 ? frag * nbc : -frag * nbc;
         for (int a = 0; a < 3; ++a) {
-            h.W[widx(o, cat, r, a, i)] += fi[a] * fact;
-            h.W[widx(o, cat, r, a, j)] += (-fj[a]) * fact;
+            W[widx(o, cat, r, a, i)] += fi[a] * fact;
+            W[widx(o, cat, r, a, j)] += (-fj[a]) * fact;
         }
     }
 }
@@ -1746,6 +1751,39 @@ void calnon14p_hf(Oracle& o) {
         o.hf.pot[(size_t)HF_14 * n + i] += 0.5 * dv;
         o.hf.pot[(size_t)HF_14 * n + j] += 0.5 * dv;
         calvirihf(o, i, j, fv, fv41, 0.5, HF_14);
+    }
+}
+
+// morsep_hf (morse_hf.F90:6-250): morsep's pair loop with half of each pair
+// energy to either atom (pot_mor_atm) and calvirihf (two-body coefficient
+// 1/2) into a Morse virial array [nreg][3][N] (virimort_atm); the centres of
+// mass come from calcom at the current positions.
+void morsep_hf(Oracle& o, double* pot_atm, std::vector<double>& W) {
+    Oracle::HF& h = o.hf;
+    calcom(o, o.atmcor, h.molecom);
+    const int n = o.natom, nm = (int)o.mor_atoms.size();
+    std::fill(pot_atm, pot_atm + n, 0.0);
+    W.assign((size_t)h.nreg * 3 * n, 0.0);
+    const double sqcut = o.prm.rcutmor * o.prm.rcutmor;
+    for (int m1 = 0; m1 + 1 < nm; ++m1) {
+        const int i = o.mor_atoms[m1], it = o.atmindex[i];
+        for (int q = o.mor_idx[m1]; q < o.mor_idx[m1 + 1]; ++q) {
+            const int j = o.mor_list[q], jt = o.atmindex[j];
+            double rij[3]; mi(o, i, j, rij);
+            double r2 = rij[0] * rij[0] + rij[1] * rij[1] + rij[2] * rij[2];
+            if (r2 > sqcut) continue;
+            double r = std::sqrt(r2), ri1 = 1.0 / r;
+            const size_t t = (size_t)it + (size_t)o.ntyp * jt;
+            double rt1 = std::exp(-1.0 * (r - o.radmor[t]) * o.almor[t]);
+            double rt2 = rt1 * rt1;
+            double ftmp = 2.0 * o.almor[t] * o.welmor[t] * (rt2 - rt1) * ri1;
+            double potij = o.welmor[t] * (rt2 - 2.0 * rt1);
+            pot_atm[i] = pot_atm[i] + 0.5 * potij;
+            pot_atm[j] = pot_atm[j] + 0.5 * potij;
+            double fij[3] = {ftmp * rij[0], ftmp * rij[1], ftmp * rij[2]};
+            double fji[3] = {-fij[0], -fij[1], -fij[2]};
+            calvirihf(o, i, j, fij, fji, 0.5, 0, &W);
+        }
     }
 }
 
@@ -2384,6 +2422,17 @@ int orc_ewk_nvec(int kmax, double yratio, double zratio, int* out, int cap, int*
     if (s) return s;
     *nwave = (int)nv.size() / 3;
     if (out) std::copy(nv.begin(), nv.begin() + std::min((size_t)3 * cap, nv.size()), out);
+    return PGK_OK;
+}
+// morsep_hf per-atom Morse energy (N) and virial (:,3,i,r) as W[(r*3 + a)*N + i]
+int orc_morse_hf_atm(void* h, double* pot, double* W) {
+    Oracle* o = (Oracle*)h;
+    if (!o->hf.set || o->welmor.empty()) return PGK_E_INVALID;
+    if (o->nb_index.empty()) mklist(*o);
+    std::vector<double> w, p((size_t)o->natom);
+    morsep_hf(*o, p.data(), w);
+    if (pot) std::copy(p.begin(), p.end(), pot);
+    if (W) std::copy(w.begin(), w.end(), W);
     return PGK_OK;
 }
 // Morse list of the last mklist: its order (PGK_LIST_*) and pair count

@@ -220,3 +220,20 @@ def test_morse_cell_list_matches_all_pairs(oracle_mod):
     assert m_cell == abi.LIST_CELL and m_all == abi.LIST_ALLPAIR and n_cell == n_all
     assert abs(e_cell - e_all) <= 1e-12 * abs(e_all)
     assert printed(want["pot_mor"], e_cell, want["eref"])
+
+
+def test_morse_heat_flux_shares(pt_morse, oracle_mod):
+    """morsep_hf (morse_hf.F90): half of each pair energy to either atom, so
+    the shares sum to pot_mor; with one region over the whole box and every
+    atom atom-based, the per-atom z column of the Morse virial sums to the
+    (a, z) column of the Morse virial tensor (no Morse pair crosses the
+    vacuum gap in z)."""
+    s, want, e, vir = pt_morse
+    o = oracle_mod.Oracle(s, threads=os.cpu_count() or 1)
+    o.set_hf({"regions": [(0.0, s.box[2])], "hftyp": None})
+    o.mklist()
+    pot, W = o.morse_hf_atm()
+    assert abs(pot.sum() - e["pot_mor"]) <= 1e-12 * abs(e["pot_mor"])
+    assert printed(want["pot_mor"], pot.sum(), want["eref"])
+    col = np.asarray(vir["pot_virit_mor"])[6:9]          # t[a + 3*2]: f_a z_ij
+    np.testing.assert_allclose(W[0].sum(axis=1), col, rtol=1e-10, atol=1e-8 * np.abs(col).max())
