@@ -116,9 +116,10 @@ def measured_peaks():
         return {}
 
 
-def profiled_traffic():
-    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_pair_mixed_butane200k.md")
+def profiled_traffic(name="k_pair_mixed_butane200k.md"):
+    """DRAM bytes (read + write) per launch of one kernel from its committed
+    ncu summary under profiles/ (line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", name)
     try:
         for ln in open(p):
             if ln.startswith("traffic_bytes_per_launch:"):
@@ -126,6 +127,18 @@ def profiled_traffic():
     except (OSError, ValueError):
         pass
     return None
+
+
+def period_window(warmup, steps, nb):
+    """Timed window of whole pair-list periods: the first step after the
+    warm-up that opens a period (step % nb == 1) and a length of at least
+    `steps` rounded up to a multiple of nb, so the window holds its list
+    rebuilds (steps % nb == 0) at exactly their natural rate."""
+    n = max(steps, nb)
+    n = -(-n // nb) * nb
+    s0 = warmup + 1
+    s0 += (1 - s0) % nb
+    return s0, n
 
 
 def run_ours(args, rank, world, local_rank):
@@ -139,11 +152,12 @@ def run_ours(args, rank, world, local_rank):
     eng = PgkEngine(s)
     stream = torch.cuda.ExternalStream(eng.stream)
     eng.set_chain(abi.chain_init(s.box))
-    # ---- warm-up: step 0 (initial forces) + W steps ----
-    eng.moldyn_mtk(0, args.warmup, md)
+    step0, nsteps = period_window(args.warmup, args.steps, NSTEP_BOOK)
+    # ---- warm-up: step 0 (initial forces), the W warm-up steps and the rest
+    #      of their list period ----
+    eng.moldyn_mtk(0, step0 - 1, md)
     eng.sync()
     dist_barrier(world)
-    step0 = args.warmup + 1
     launches0 = eng.kernel_launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -151,44 +165,52 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         dist_barrier(world)
         e0.record(stream)
-        ene = eng.moldyn_mtk(step0, step0 + args.steps - 1, md)
+        ene = eng.moldyn_mtk(step0, step0 + nsteps - 1, md)
         e1.record(stream)
         torch.cuda.synchronize()
         dist_barrier(world)
     ms = e0.elapsed_time(e1)
     launches = eng.kernel_launches - launches0
     ms_max = dist_max(ms, world)
+    nxt = step0 + nsteps
     # ---- end to end through the public API with host buffers ----
-    e2e = None if args.no_e2e else e2e_leg(eng, s, md, step0 + args.steps, max(3, args.steps // 4), world)
-    # ---- dominant kernel roofline (pair kernel), measured live ----
-    roof = roofline(eng)
+    e2e = None if args.no_e2e else e2e_leg(eng, s, md, nxt, nsteps, world)
     # ---- the all-FP64 device path on the same state (north-star comparison) ----
-    fp64 = None if args.no_fp64 else fp64_leg(eng, s, md, step0 + args.steps + 1000, stream)
+    fp64 = None if args.no_fp64 else fp64_leg(eng, s, md, stream)
+    # ---- rooflines of the dominant kernel and the HBM-bound kernels, measured
+    #      live (last: the kick/drift launches move the atoms) ----
+    roof, roof_hbm = roofline(eng, s)
     eng.close()
     natom = s.natom
-    value = world * natom * args.steps / (ms_max / 1e3)
+    value = world * natom * nsteps / (ms_max / 1e3)
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": nsteps,
+        "warmup": args.warmup, "ms_per_step": ms_max / nsteps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int64 (pair/SPME/bonded), fp64 (x, v, RATTLE, MTK)",
         "data": "synthetic (seeded butane lattice, OPLS-like parameters)",
         "config": {"workload": WORKLOAD, "natom": natom, "replicas": world, "global_batch": world * natom,
                    "parallelism": f"replicas{world}", "nstep_book": NSTEP_BOOK,
+                   "steps_requested": args.steps,
+                   "timed_window": f"steps {step0}..{step0 + nsteps - 1}: whole pair-list periods, "
+                                   f"{nsteps // NSTEP_BOOK} list rebuilds inside (1 per {NSTEP_BOOK} steps)",
                    "l2": "working set > L2 (pair list ~0.6 GB), no flush"},
-        "ns_per_day": ns_per_day(args.steps / (ms_max / 1e3)),
-        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "fp64_path": fp64,
+        "ns_per_day": ns_per_day(nsteps / (ms_max / 1e3)),
+        "e2e": e2e, "gpu_launches": launches, "roofline": roof, "roofline_hbm": roof_hbm, "fp64_path": fp64,
         "energies_last": {k: ene[k] for k in ("pot_tot", "pot_vdw", "pot_elc", "pot_ewk")} if ene else None,
     }
     out["clocks"] = clk.summary()
+    if rank == 0 and not args.no_configs:
+        out["other_configs"] = other_configs(args)
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
 
 
-def fp64_leg(eng, s, md, start, stream, nsteps=10):
+def fp64_leg(eng, s, md, stream):
     """The FP64 device path (the parity path) on the mixed run's current state:
     force RMS relative error of the mixed path against it (both MTS groups,
-    same positions) and its own MD throughput on the same workload."""
+    same positions) and its own MD throughput on the same workload, timed
+    over one whole pair-list period (its list rebuild included)."""
     import torch
     from thrid_b200 import abi
     from thrid_b200.pgk import PgkEngine
@@ -202,61 +224,87 @@ def fp64_leg(eng, s, md, start, stream, nsteps=10):
         f64 = e64.calforce(abi.MTS_LONG)[0] + e64.calforce(abi.MTS_SHORT)[0]
         err = float(np.sqrt(((fm - f64) ** 2).sum() / (f64 ** 2).sum()))
         st64 = torch.cuda.ExternalStream(e64.stream)
-        e64.moldyn_mtk(start, start + 2, md)
+        s0, nsteps = period_window(3, NSTEP_BOOK, NSTEP_BOOK)
+        e64.moldyn_mtk(0, s0 - 1, md)
         e64.sync()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(st64)
-        e64.moldyn_mtk(start + 3, start + 2 + nsteps, md)
+        e64.moldyn_mtk(s0, s0 + nsteps - 1, md)
         b.record(st64)
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / nsteps
     finally:
         e64.close()
     return {"value": s.natom / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": nsteps,
+            "timed_window": f"steps {s0}..{s0 + nsteps - 1} (one list period, its rebuild inside)",
             "force_rel_rms_mixed_vs_fp64": err}
 
 
 def e2e_leg(eng, s, md, start, nsteps, world):
     """Host-driver ownership of the state (like the Fortran module arrays):
-    every step uploads x, v from pinned host memory, runs one outer step and
-    reads back x, v and the energies."""
+    every step uploads x, v from pinned host memory, runs one outer step
+    through pgk_moldyn_mtk and reads x, v (the step's result) back into
+    pinned host memory.  The window covers whole pair-list periods, like the
+    device-timed one; energies are not read (no output step, as between the
+    reference's outinterval steps)."""
     import torch
+    from thrid_b200 import abi
     n = s.natom
+    md_e2e = abi.MdParamsStruct.from_buffer_copy(md)
+    md_e2e.outinterval = 1 << 30                     # no output step inside the window
     cor = torch.empty((n, 3), dtype=torch.float64).pin_memory()
     vel = torch.empty((n, 3), dtype=torch.float64).pin_memory()
-    c, v, _ = eng.download_state()
-    cor.numpy()[:] = c
-    vel.numpy()[:] = v
     cn, vn = cor.numpy(), vel.numpy()
+    eng.download_state(cn, vn)
+    s0 = start + (1 - start) % NSTEP_BOOK
+    eng.moldyn_mtk(start, s0 - 1, md_e2e)            # reach a period start; capture the step graph
+    eng.download_state(cn, vn)
     torch.cuda.synchronize()
     dist_barrier(world)
     t0 = time.perf_counter()
     for k in range(nsteps):
         eng.upload_state(cn, vn)
-        eng.moldyn_mtk(start + k, start + k, md)
-        c, v, _ = eng.download_state()
-        cn[:] = c
-        vn[:] = v
+        eng.moldyn_mtk(s0 + k, s0 + k, md_e2e)
+        eng.download_state(cn, vn)
     torch.cuda.synchronize()
     dt = dist_max(time.perf_counter() - t0, world)
-    return {"value": world * n * nsteps / dt, "unit": UNIT, "steps": nsteps,
-            "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 2 * 24 * n + 13 * 8}
+    return {"value": world * n * nsteps / dt, "unit": UNIT, "steps": nsteps, "ms_per_step": 1e3 * dt / nsteps,
+            "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 2 * 24 * n,
+            "path": "pgk_upload_state (pinned x, v) -> pgk_moldyn_mtk (1 step) -> pgk_download_state (pinned x, v)"}
 
 
-def roofline(eng):
+# algorithmic bytes per unit of the HBM-bound kernels (SURVEY 8(d) formulas)
+HBM_KERNELS = (
+    # (bench id, name, profile summary, unit, bytes(natom, K3, entries))
+    (1, "k_spread_rows<5> (fill_charge_grid)", "k_spread_rows_butane200k.md",
+     "N*16 + K^3*16", lambda n, k3, e: n * 16 + k3 * 16),
+    (2, "k_gather_rows<5> (grad_sum)", "k_gather_rows_butane200k.md",
+     "N*16 + K^3*4 + N*24", lambda n, k3, e: n * 16 + k3 * 4 + n * 24),
+    (5, "k_kick_drift (long kick + drift)", "k_kick_drift_butane200k.md",
+     "N*(48 + 48 + 24 + 8)", lambda n, k3, e: n * 128),
+    (4, "list build chain (k_cell_* + k_build_clist)", "k_build_clist_butane200k.md",
+     "N*(24 + 16) + 4 * list entries", lambda n, k3, e: n * 40 + 4 * e),
+)
+
+
+def roofline(eng, s):
+    """Pair kernel against the FP32 pipe; spread, gather, kick/drift and the
+    list build against the measured HBM copy bandwidth.  Each kernel is timed
+    with CUDA events on the context's stream (pgk_bench_kernel, 20 launches
+    after one warm-up launch)."""
     import ctypes as C
     ms = C.c_double(); units = C.c_double(); entries = C.c_double()
     st = eng.L.pgk_bench_kernel(eng.h, 0, 20, C.byref(ms), C.byref(units), C.byref(entries))
     if st != 0:
-        return {"error": f"pgk_bench_kernel status {st}"}
+        return {"error": f"pgk_bench_kernel status {st}"}, None
     flop = 61.0 * units.value                       # algorithmic flop per interacting pair
     achieved = flop / (ms.value * 1e-3) / 1e12       # TFLOP/s
     peaks = measured_peaks()
     clk = peaks.get("sm_max_mhz", 1965.0)
     peak = 148 * 128 * 2 * clk * 1e6 / 1e12           # FP32 CUDA-core FMA peak at the max SM clock
     traffic = profiled_traffic()
-    return {"kernel": "k_pair_mixed<PM_TENS> (regular instance on the pruned rows)", "bound": "fp32",
+    pair = {"kernel": "k_pair_mixed<PM_TENS> (regular instance on the pruned rows)", "bound": "fp32",
             "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
             "peak_source": f"nominal FP32 FMA peak 148 SM x 128 lanes x 2 x {clk:.0f} MHz "
@@ -264,11 +312,29 @@ def roofline(eng):
             "ms_per_launch": ms.value, "pairs_per_launch": units.value, "list_entries": entries.value,
             "hbm_gbs_index_stream": entries.value * 4 / (ms.value * 1e-3) / 1e9,
             "hbm_peak_gbs": peaks.get("hbm_gbs")}
+    hbm_peak = peaks.get("hbm_gbs")
+    k3 = float(s.params["nfft1"] * s.params["nfft2"] * s.params["nfft3"])
+    rows = []
+    for kid, name, prof, formula, fbytes in HBM_KERNELS:
+        km = C.c_double()
+        st = eng.L.pgk_bench_kernel(eng.h, kid, 20, C.byref(km), None, None)
+        if st != 0:
+            rows.append({"kernel": name, "error": f"pgk_bench_kernel status {st}"})
+            continue
+        b = float(fbytes(s.natom, k3, entries.value))
+        gbs = b / (km.value * 1e-3) / 1e9
+        rows.append({"kernel": name, "bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": gbs / hbm_peak if hbm_peak else None, "traffic": profiled_traffic(prof),
+                     "algorithmic_bytes": b, "bytes_formula": formula, "ms_per_launch": km.value,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm_peak else None})
+    return pair, rows
 
 
 def cpu_baseline(args, nsteps=None, threads=None):
     """The oracle (C++ FP64 restatement of the reference loops) on the host
-    cores, on a bounded sample of the same workload."""
+    cores, on a bounded sample of the same workload: `nsteps` outer MTK steps
+    timed after step 0, plus the share 1/nstep_book of one timed list build
+    (the reference rebuilds its list every nstep_book steps)."""
     from oracle import oracle as orc
     from thrid_b200 import abi
     threads = threads or os.cpu_count() or 1
@@ -281,11 +347,17 @@ def cpu_baseline(args, nsteps=None, threads=None):
     t_init = time.perf_counter() - t0
     nsteps = nsteps or 3
     t0 = time.perf_counter()
-    st2, _ = o.moldyn(2, 1, nsteps, md)
+    st2, _ = o.moldyn(2, 1, nsteps, md)        # steps 1..nsteps: no list build falls inside
     dt = time.perf_counter() - t0
-    return {"value": s.natom * nsteps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    t0 = time.perf_counter()
+    o.mklist()
+    t_list = time.perf_counter() - t0
+    per_step = dt / nsteps + t_list / NSTEP_BOOK
+    return {"value": s.natom / per_step, "unit": UNIT, "cores": threads, "kind": "port",
+            "steps": nsteps, "ms_per_step": 1e3 * per_step,
             "sample": f"{nsteps} outer MTK steps of the 200,004-atom butane system after step 0 "
-                      f"(step-0 list build + forces took {t_init:.1f} s, untimed)",
+                      f"({1e3 * dt / nsteps:.0f} ms each) plus 1/{NSTEP_BOOK} of one list build "
+                      f"({1e3 * t_list:.0f} ms); step 0 (list + forces, {t_init:.1f} s) untimed",
             "status": int(st2)}
 
 
@@ -293,13 +365,148 @@ def run_reference(args, rank, world):
     if rank != 0:
         return None
     cb = cpu_baseline(args, nsteps=max(1, min(args.steps, 3)))
-    return {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * 200004 / cb["value"], "higher_is_better": True,
+    natom = 200004
+    return {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": cb["steps"],
+            "warmup": args.warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic (seeded butane lattice)",
-            "config": {"workload": WORKLOAD, "natom": 200004, "parallelism": "host threads"},
+            "config": {"workload": WORKLOAD, "natom": natom, "replicas": 1, "global_batch": natom,
+                       "parallelism": "host threads", "nstep_book": NSTEP_BOOK, "steps_requested": args.steps,
+                       "timed_window": cb["sample"], "l2": "host run"},
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "reference Fortran cannot be compiled here (no gfortran); its C++ restatement runs instead"}
+            "note": "reference Fortran cannot be compiled here (no gfortran); its C++ restatement runs instead; "
+                    "each step of the run is a bounded sample (steps = the steps actually timed)"}
+
+
+def _timed_md(eng, kind, s0, n, md, stream):
+    """CUDA-event time (ms) of moldyn steps s0..s0+n-1 on the context's stream."""
+    import torch
+    fn = {"nve": eng.moldyn_nve, "nhc": eng.moldyn_nhc, "mtk": eng.moldyn_mtk}[kind]
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn(s0, s0 + n - 1, md)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def nve_drift(s, prec, nchunk=10, chunk=200):
+    """NVE drift of the total energy (pot_tot + KE) over nchunk*chunk steps at
+    1 fs: least-squares slope per ns, with its standard error, in units of
+    eref per atom and of the mean kinetic energy."""
+    from thrid_b200 import abi
+    from thrid_b200 import systems as S
+    from thrid_b200.pgk import PgkEngine
+    eng = PgkEngine(s, dict(s.params, precision=prec))
+    md = abi.md_struct(S.fs_to_reduced(1.0), ifrattle=1, outinterval=0)
+    eng.moldyn_nve(0, 0, md)
+    t, E, K = [], [], []
+    for k in range(nchunk):
+        e = eng.moldyn_nve(k * chunk + 1, (k + 1) * chunk, md)
+        kint, _, _ = eng.calpress()
+        t.append((k + 1) * chunk * 1e-6)                    # ns
+        E.append(e["pot_tot"] + 0.5 * kint)
+        K.append(0.5 * kint)
+    eng.close()
+    t, E = np.asarray(t), np.asarray(E)
+    (slope, icpt), cov = np.polyfit(t, E, 1, cov=True)
+    se = float(np.sqrt(cov[0, 0]))
+    return {"per_atom_eref_per_ns": slope / s.natom, "stderr_per_atom_eref_per_ns": se / s.natom,
+            "per_mean_ke_per_ns": slope / np.mean(K), "steps": nchunk * chunk}
+
+
+def _md_leg(s, kind, md, prec, warm, n, hf=False):
+    """Throughput of one configuration on its own context: atom-steps/s over
+    steps warm+1..warm+n (whole list periods when n is a multiple of 50)."""
+    import torch
+    from thrid_b200 import abi
+    from thrid_b200.pgk import PgkEngine
+    eng = PgkEngine(s, dict(s.params, precision=prec))
+    st = torch.cuda.ExternalStream(eng.stream)
+    if kind in ("nhc", "mtk"):
+        eng.set_chain(abi.chain_init(s.box))
+    if hf:
+        eng.set_hf(s.regions["hf"])
+        eng.moldyn_hf(0, warm, md, cap=1)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(st)
+        _, rec = eng.moldyn_hf(warm + 1, warm + n, md, cap=n)
+        b.record(st)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        cor, vel, _ = eng.download_state()
+        eng.close()
+        return ms, rec, cor, vel
+    {"nve": eng.moldyn_nve, "nhc": eng.moldyn_nhc, "mtk": eng.moldyn_mtk}[kind](0, warm, md)
+    ms = _timed_md(eng, kind, warm + 1, n, md, st)
+    eng.close()
+    return ms, None, None, None
+
+
+def _zprofile(s, cor, vel, nbin):
+    """z-resolved kinetic temperature (reduced) per slab of the box height."""
+    m = s.atmmass
+    z = np.mod(cor[:, 2], s.box[2])
+    b = np.minimum((z / s.box[2] * nbin).astype(int), nbin - 1)
+    ke = 0.5 * m * (vel ** 2).sum(1)
+    cnt = np.bincount(b, minlength=nbin)
+    kes = np.bincount(b, weights=ke, minlength=nbin)
+    return np.where(cnt > 0, 2.0 * kes / (3.0 * np.maximum(cnt, 1)), 0.0), cnt
+
+
+def other_configs(args):
+    """The other named shapes at 1 GPU, mixed precision (each on its own
+    context, CUDA-event timed, list rebuilds inside the window):
+      C1 rigid water 1536 atoms NVE (+ NVE drift per ns, FP64 and mixed),
+      C2 flexible propanol 12,000 atoms NHC,
+      C3 alcohol/water slab 43,200 atoms, NVE + region Langevin + per-atom
+         heat flux every step (+ J(t) and z temperature profile of the mixed
+         path against the FP64 path over the same steps)."""
+    from thrid_b200 import abi
+    from thrid_b200 import systems as S
+    out = {}
+    dt = S.fs_to_reduced(1.0)
+    c1 = S.water_box(precision=abi.PREC_MIXED)
+    md = abi.md_struct(dt, ifrattle=1, outinterval=0)
+    ms, *_ = _md_leg(c1, "nve", md, abi.PREC_MIXED, 49, 1000)
+    d64 = nve_drift(c1, abi.PREC_FP64)
+    dmx = nve_drift(c1, abi.PREC_MIXED)
+    out["C1_water_1536_nve"] = {"value": c1.natom * 1000 / (ms / 1e3), "unit": UNIT, "steps": 1000,
+                                "ms_per_step": ms / 1000, "ns_per_day": ns_per_day(1000 / (ms / 1e3)),
+                                "nve_drift_fp64": d64, "nve_drift_mixed": dmx}
+    c2 = S.propanol_box(precision=abi.PREC_MIXED)
+    T = S.kelvin_to_reduced(300.0)
+    md2 = abi.md_struct(dt, mchain=3, text=T, tfreq=1.0e13 * S.TIMEREF, degfree=c2.degfree_all, ifrattle=1,
+                        outinterval=0)
+    ms, *_ = _md_leg(c2, "nhc", md2, abi.PREC_MIXED, 49, 200)
+    out["C2_propanol_12000_nhc"] = {"value": c2.natom * 200 / (ms / 1e3), "unit": UNIT, "steps": 200,
+                                    "ms_per_step": ms / 200, "ns_per_day": ns_per_day(200 / (ms / 1e3))}
+    res = {}
+    for prec in (abi.PREC_MIXED, abi.PREC_FP64):
+        c3 = S.slab_box(precision=prec)
+        md3 = abi.md_struct(dt, ifrattle=1, outinterval=0)
+        res[prec] = (c3,) + _md_leg(c3, "nve", md3, prec, 49, 100, hf=True)
+    c3, ms, rec, cor, vel = res[abi.PREC_MIXED]
+    _, ms64, rec64, cor64, vel64 = res[abi.PREC_FP64]
+    vols = np.array([(b - a) for a, b in c3.regions["hf"]["regions"]]) * c3.box[0] * c3.box[1]
+    jt = (rec[:, :, 17] * vols).sum(1)                 # total J_z(t) of the slab, per step
+    jt64 = (rec64[:, :, 17] * vols).sum(1)
+    nbin = len(c3.regions["hf"]["regions"])
+    tp, cnt = _zprofile(c3, cor, vel, nbin)
+    tp64, _ = _zprofile(c3, cor64, vel64, nbin)
+    occ = cnt > 0
+    out["C3_slab_43200_hf_langevin"] = {
+        "value": c3.natom * 100 / (ms / 1e3), "unit": UNIT, "steps": 100, "ms_per_step": ms / 100,
+        "ns_per_day": ns_per_day(100 / (ms / 1e3)), "fp64_ms_per_step": ms64 / 100,
+        "hf_records": int(rec.shape[0]), "regions": nbin,
+        "jz_rel_rms_mixed_vs_fp64": float(np.sqrt(((jt - jt64) ** 2).mean() / (jt64 ** 2).mean())),
+        "tprofile_max_rel_err_mixed_vs_fp64": float(np.max(np.abs(tp[occ] - tp64[occ]) / tp64[occ])),
+        "note": "same seeded start and Langevin stream; 100 steps after a 49-step warm-up"}
+    return out
 
 
 # ---- torch.distributed plumbing (replicas; barrier + max over ranks only) ----
@@ -494,6 +701,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the host-core baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other named shapes (C1-C3, drift)")
     ap.add_argument("--serve", action="store_true", help="replica-serving benchmark instead of the main line")
     ap.add_argument("--serve-replicas", type=int, default=32)
     ap.add_argument("--serve-steps", type=int, default=1000)

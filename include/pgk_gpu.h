@@ -390,11 +390,12 @@ pgk_status pgk_langevin_dekin(pgk_ctx* ctx, double* det_ene_kin);
  * appends one record to a device buffer instead of reading the accumulators
  * back (no host synchronisation per output step); pgk_get_output copies the
  * records out and clears the buffer.  Record layout (PGK_OUT_NCOL doubles):
- *   [0] step, [1..13] the pgk_energies fields in struct order,
- *   [14] sum(m v^2), [15] pint, [16..24] pintt (column-major), [25..27] box.
+ *   [0] step, [1..14] the 14 pgk_energies fields in struct order (pot_tot
+ *   .. pot_mor), [15] sum(m v^2), [16] pint, [17..25] pintt (column-major),
+ *   [26..28] box.
  * pint/pintt are the barostat's values (moldyn_mtk); other drivers leave the
  * last ones set.  Records beyond the capacity are counted but not kept. */
-#define PGK_OUT_NCOL 28
+#define PGK_OUT_NCOL 29
 pgk_status pgk_set_output(pgk_ctx* ctx, int64_t cap_records);
 pgk_status pgk_get_output(pgk_ctx* ctx, double* out, int64_t cap_records, int64_t* nrecords);
 
@@ -420,6 +421,8 @@ void* pgk_stream(const pgk_ctx* ctx);
  * events, and return the mean device time per launch in *ms.  which:
  *   0 = real-space pair kernel (ewaldrp) with virials, 1 = SPME spread,
  *   2 = SPME gather, 3 = one forward 3-D FFT (three axis passes),
+ *   4 = one pair-list build (mklist_cell / mklist2a, every kernel of it),
+ *   5 = one long kick + drift pass (moves the atoms: time it last),
  *   64 + m = the bonded terms with term mask m (bit 0 bonds, 1 angles,
  *   2 torsions, 3 RB torsions, 4 1-4 pairs, 5 excluded pairs) with energies
  *   and per-type virials, 128 + m = the same with only the total virial
@@ -427,7 +430,7 @@ void* pgk_stream(const pgk_ctx* ctx);
  *   ewaldkp_hf evaluation (the whole kernel chain), 512 + kmax / 768 + kmax
  *   = its structure-factor / per-atom kernel alone (kmax < 256).
  * *units receives the algorithmic work of one launch: unique pairs inside
- * the cutoff (0), atoms (1, 2, 64+, 128+), grid points (3), or (atom, wave)
+ * the cutoff (0), atoms (1, 2, 4, 5, 64+, 128+), grid points (3), or (atom, wave)
  * pairs without (0,0,0) (256+); *entries the number
  * of (cluster, j) list entries the pair kernel reads. */
 pgk_status pgk_bench_kernel(pgk_ctx* ctx, int32_t which, int32_t iters, double* ms, double* units,
@@ -490,8 +493,10 @@ pgk_status pgk_server_free(pgk_server* sv);
  *   pot_ewk   host pointer for the reciprocal energy (NULL = not needed;
  *             when given, the call waits for its stream);
  *   stream    cudaStream_t as void* (NULL = default stream).
- * Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256 and a product of 2, 3
- * and 5, 3 <= pme_order <= 8; larger sizes return PGK_E_SCRATCH_LIMIT.
+ * Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256, 3 <= pme_order <= 8;
+ * larger sizes return PGK_E_SCRATCH_LIMIT.  Each nfft must also be a product
+ * of 2, 3 and 5 (else PGK_E_UNSUPPORTED) and at least pme_order (else
+ * PGK_E_INVALID); these checks come before any CUDA call.
  * The first call on a device looks up the array's address on that device;
  * make it before any stream capture.  All calls share the array and keep its
  * last contents: calls that overlap on the GPU race, so serialise them. */

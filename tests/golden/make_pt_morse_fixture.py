@@ -27,7 +27,7 @@ and the virials of the same step (out_pre.dat, outpre):
 
 Run in a checkout that has the reference tree (not needed to run the tests):
 
-    python tests/golden/make_pt_morse_fixture.py [REFERENCE_DIR]
+    python tests/golden/make_pt_morse_fixture.py REFERENCE_DIR
 """
 import math
 import os
@@ -358,4 +358,8 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/peachgk-md")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PEACHGK_MD_DIR")
+    if not ref:
+        sys.exit("usage: make_pt_morse_fixture.py REFERENCE_DIR (the peachgk-md directory of the reference "
+                 "tree; or set PEACHGK_MD_DIR)")
+    main(ref)

@@ -34,7 +34,7 @@ def _noalloc(L):
     return f
 
 
-def test_noalloc_spme_matches_context_entry_point():
+def test_noalloc_spme_matches_context_entry_point(oracle_mod):
     import torch
     s = S.water_box()
     p = dict(s.params)
@@ -42,6 +42,10 @@ def test_noalloc_spme_matches_context_entry_point():
     eng = PgkEngine(s, p)
     ref, ene, _ = eng.fft_pme()
     eng.close()
+    # the oracle's fft_pmep (fft_pme.F90:144-270) on the same state
+    o = oracle_mod.Oracle(s, p)
+    oref, oene, _ = o.fft_pmep()
+    assert rel_rms(ref, oref) < TOL_FORCE
 
     dev = torch.device("cuda:0")
     pos = torch.tensor(s.atmcor.ravel(), dtype=torch.float64, device=dev)
@@ -59,7 +63,9 @@ def test_noalloc_spme_matches_context_entry_point():
         torch.cuda.synchronize()
         got = force.cpu().numpy().reshape(-1, 3)
         assert rel_rms(got, ref) < TOL_FORCE, call
+        assert rel_rms(got, oref) < TOL_FORCE, call
         assert abs(e.value - ene["pot_ewk"]) < TOL_ENERGY * max(1.0, abs(ene["pot_ewk"])), call
+        assert abs(e.value - oene["pot_ewk"]) < TOL_ENERGY * max(1.0, abs(oene["pot_ewk"])), call
 
 
 def test_noalloc_rejects_grids_beyond_its_static_scratch():
@@ -74,4 +80,6 @@ def test_noalloc_rejects_grids_beyond_its_static_scratch():
     st = fn(pos.data_ptr(), chg.data_ptr(), s.natom, box, 0.32, 128, 128, 128, 4, force.data_ptr(), None, None)
     assert st == abi.PGK_E_SCRATCH_LIMIT
     assert lib().pgk_status_string(st).startswith(b"size exceeds")
+    st = fn(pos.data_ptr(), chg.data_ptr(), s.natom, box, 0.32, 32, 32, 4, 6, force.data_ptr(), None, None)
+    assert st == abi.PGK_E_INVALID      # an axis shorter than the B-spline order
     assert float(force.abs().max()) == 0.0

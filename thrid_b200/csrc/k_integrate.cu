@@ -802,18 +802,19 @@ __global__ void k_out_record(const long long* __restrict__ acc, const DynState* 
     const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
     const double a1 = -pi / (alpha * alpha * vol);
     double e_vdw = S(A_VDW), e_elc = S(A_ELC), e_ewk = S(A_EWK), e_v14 = S(A_VDW14), e_e14 = S(A_ELC14);
-    double e_b = S(A_BOND), e_a = S(A_ANGL), e_t = S(A_TORS), e_rb = S(A_TORSRB);
+    double e_b = S(A_BOND), e_a = S(A_ANGL), e_t = S(A_TORS), e_rb = S(A_TORSRB), e_mor = S(A_MOR);
     double e_ewc = ifspme ? pot_ewc : 0.0, e_nq = ifspme ? 0.5 * a1 * netchrgsq : 0.0;
     double nonbon = e_vdw + e_elc + e_ewk + e_ewc + e_nq + e_v14 + e_e14;
-    double tot = e_b + e_a + e_t + e_rb + nonbon;
+    double tot = e_b + e_a + e_t + e_rb + e_mor + nonbon;   // calforce.F90: pot_mor is outside pot_nonbon
     r[0] = (double)step;
     r[1] = tot; r[2] = nonbon; r[3] = e_vdw; r[4] = e_elc; r[5] = e_ewk; r[6] = e_ewc; r[7] = e_nq;
-    r[8] = e_v14; r[9] = e_e14; r[10] = e_b; r[11] = e_a; r[12] = e_t; r[13] = e_rb;
-    r[14] = acc_get(acc, A_KE, dbl != 0);
-    r[15] = ch->pint;
-    for (int k = 0; k < 9; ++k) r[16 + k] = ch->pintt[k];
-    for (int d = 0; d < 3; ++d) r[25 + d] = dyn->box[d];
+    r[8] = e_v14; r[9] = e_e14; r[10] = e_b; r[11] = e_a; r[12] = e_t; r[13] = e_rb; r[14] = e_mor;
+    r[15] = acc_get(acc, A_KE, dbl != 0);
+    r[16] = ch->pint;
+    for (int k = 0; k < 9; ++k) r[17 + k] = ch->pintt[k];
+    for (int d = 0; d < 3; ++d) r[26 + d] = dyn->box[d];
 }
+static_assert(PGK_OUT_NCOL == 29 && sizeof(pgk_energies) == 14 * sizeof(double), "output record layout");
 
 pgk_status launch_out_record(pgk_ctx* c, long long step, double* dst) {
     pgk_status s;

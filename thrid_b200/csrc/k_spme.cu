@@ -703,6 +703,13 @@ pgk_status spme_setup(pgk_ctx* c) {
     c->K[0] = c->prm.nfft1; c->K[1] = c->prm.nfft2; c->K[2] = c->prm.nfft3;
     c->order = c->prm.pme_order;
     if (c->order < 3 || c->order > 8) return pgk_fail(c, PGK_E_UNSUPPORTED, "pme_order must be 3..8");
+    // spread and gather wrap a grid index once (base - order + 1 + i, plus K
+    // when negative), so every axis needs at least pme_order points
+    for (int d = 0; d < 3; ++d)
+        if (c->K[d] < c->order) return pgk_fail(c, PGK_E_INVALID, "every nfft must be at least pme_order");
+    for (int d = 0; d < 3; ++d)
+        if (!factor(c->K[d], c->plan[d]))
+            return pgk_fail(c, PGK_E_UNSUPPORTED, "SPME grid sizes must factor into 2, 3, 5");
     size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
     PGK_CUDA(c, cudaMalloc(&c->qacc, KK * 8));
     PGK_CUDA(c, cudaMalloc(&c->qc, KK * (c->mixed() ? sizeof(float2) : sizeof(double2))));
@@ -891,8 +898,10 @@ pgk_status spme_bench(pgk_ctx* c, int which) {
 // below, of fixed size, which every GPU that loads this library holds until
 // the process exits.
 //
-// Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256 and a product of 2, 3
-// and 5, 3 <= pme_order <= 8.  Larger sizes return PGK_E_SCRATCH_LIMIT.
+// Limits: nfft1*nfft2*nfft3 <= 64^3, each nfft <= 256, 3 <= pme_order <= 8;
+// larger sizes return PGK_E_SCRATCH_LIMIT.  Every nfft must also be a
+// product of 2, 3 and 5 (else PGK_E_UNSUPPORTED) and at least pme_order
+// (else PGK_E_INVALID: spread and gather wrap a grid index only once).
 // The first call on a device looks up the array's device address there
 // (cudaGetSymbolAddress); make that first call before any stream capture.
 // All calls share the one array: calls that overlap on the GPU (two streams,
@@ -1016,14 +1025,15 @@ extern "C" pgk_status pgk_fft_pme_noalloc(const double* d_atmcor, const double* 
                                           int32_t nfft3, int32_t pme_order, double* d_force, double* pot_ewk,
                                           void* stream) {
     if (!d_atmcor || !d_atmchrg || !d_force || !box || natom < 1 || alpha <= 0.0) return PGK_E_INVALID;
-    if (nfft1 < 2 || nfft2 < 2 || nfft3 < 2 || nfft1 > NOALLOC_MAX_N || nfft2 > NOALLOC_MAX_N ||
-        nfft3 > NOALLOC_MAX_N || (long long)nfft1 * nfft2 * nfft3 > NOALLOC_MAX_GRID || pme_order < 3 ||
-        pme_order > 8)
+    if (nfft1 < 2 || nfft2 < 2 || nfft3 < 2 || pme_order < 3) return PGK_E_INVALID;
+    if (nfft1 > NOALLOC_MAX_N || nfft2 > NOALLOC_MAX_N || nfft3 > NOALLOC_MAX_N ||
+        (long long)nfft1 * nfft2 * nfft3 > NOALLOC_MAX_GRID || pme_order > 8)
         return PGK_E_SCRATCH_LIMIT;
+    if (nfft1 < pme_order || nfft2 < pme_order || nfft3 < pme_order) return PGK_E_INVALID;
     FftPlan pl[3];
     const int Kd[3] = {nfft1, nfft2, nfft3};
     for (int d = 0; d < 3; ++d)
-        if (!factor(Kd[d], pl[d])) return PGK_E_SCRATCH_LIMIT;
+        if (!factor(Kd[d], pl[d])) return PGK_E_UNSUPPORTED;
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return PGK_E_CUDA;

@@ -808,6 +808,8 @@ pgk_status pgk_bench_kernel(pgk_ctx* c, int32_t which, int32_t iters, double* ms
             case 1: return spme_bench(c, 1);
             case 2: return spme_bench(c, 2);
             case 3: return spme_bench(c, 3);
+            case 4: return launch_mklist(c);                          // list build chain
+            case 5: return launch_kick_drift(c, KD_LONG | KD_DRIFT);  // long kick + drift (moves the atoms)
             default:
                 if (which >= 256 && which < 1024)
                     return launch_ewk_hf(c, (which - 256) & 255, nullptr, (which - 256) >> 8);
@@ -966,7 +968,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                                     c->st));
         PGK_CUDA(c, cudaStreamSynchronize(c->st));
         memset(eo, 0, sizeof(pgk_energies));
-        memcpy(eo, r + 1, offsetof(pgk_energies, pot_mor));   // record: the energies before pot_mor
+        memcpy(eo, r + 1, sizeof(pgk_energies));   // record columns 1..14: the pgk_energies fields
     }
     if (nrec) *nrec = nr;
     return read_status(c);

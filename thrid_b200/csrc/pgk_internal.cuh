@@ -42,7 +42,10 @@ enum AccIdx {
     A_VSCA = A_VT14 + 9,  // vir_sca of scalar_sum
     A_KE,                 // sum m v^2
     A_KET,                // sum m v_a v_b, 9
-    NACC = A_KET + 9
+    A_MOR = A_KET + 9,    // pot_mor (morsep)
+    A_VMOR,               // pot_viri_mor
+    A_VTMOR,              // pot_virit_mor, 9
+    NACC = A_VTMOR + 9
 };
 
 // status bits (device sticky word)

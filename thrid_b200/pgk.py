@@ -134,9 +134,16 @@ class PgkEngine:
         self._check(self.L.pgk_upload_state(self.h, _p(cor), _p(vel) if vel is not None else None,
                                             _p(bx) if bx is not None else None))
 
-    def download_state(self):
+    def download_state(self, cor=None, vel=None):
+        """Positions, velocities (N,3) and box.  cor / vel: optional
+        C-contiguous float64 (N,3) arrays to fill (e.g. pinned host memory)."""
         n = self.sys.natom
-        cor = np.zeros((n, 3)); vel = np.zeros((n, 3)); box = np.zeros(3)
+        for a in (cor, vel):
+            if a is not None and (a.dtype != np.float64 or a.shape != (n, 3) or not a.flags.c_contiguous):
+                raise ValueError("download_state: out arrays must be C-contiguous float64 (natom, 3)")
+        cor = np.zeros((n, 3)) if cor is None else cor
+        vel = np.zeros((n, 3)) if vel is None else vel
+        box = np.zeros(3)
         self._check(self.L.pgk_download_state(self.h, _p(cor), _p(vel), _p(box)))
         return cor, vel, box
 
