@@ -148,9 +148,11 @@ typedef struct pgk_params {
     int32_t ifnetqcorrp;          /* net-charge correction for pressure        */
     int32_t max_nbr;              /* entries per 8-atom cluster row of the device pair list (0 = auto) */
     double  rcutmor;              /* Morse cutoff                              */
-    double  rcut_bookmor;         /* Morse list radius (mklist_mor*.F90)       */
+    double  rcut_bookmor;         /* Morse list radius (mklist_mor*.F90); <= 0: every Morse
+                                     pair within half the box diagonal (ifbookmor off) */
     int32_t mts_mor;              /* gates morsep (PGK_MTS_*)                   */
-    int32_t _pad_mor;
+    int32_t nstep_bookmor;        /* Morse list rebuild interval of the stage drivers
+                                     (moldyn*.F90; 0 = nstep_book)              */
 } pgk_params;
 
 /* ---- integrator parameters (moldyn_*.F90 arguments) ---------------------- */
@@ -302,6 +304,25 @@ pgk_status pgk_ewaldr(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virial
 pgk_status pgk_fft_pme(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
 /* calbondp/calanglp/caltorsp/caltorsrbp/calnon14p (all terms, no MTS gate). */
 pgk_status pgk_calbonded(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
+/* morsep (morse.F90:206-414): Morse force over the Morse list, pot_mor,
+ * pot_viri_mor, pot_virit_mor (no MTS gate; builds the Morse list if none). */
+pgk_status pgk_morsep(pgk_ctx* ctx, double* force, pgk_energies* ene, pgk_virials* vir);
+
+/* ---- Morse pair list (its own list, as in the reference) ------------------
+ * Morse atoms (nmorselist, linkbond.F90) are the atoms of a type that has a
+ * Morse partner type (inter_inttyp == 2); with mts_mor = PGK_MTS_NONE the
+ * engine holds no Morse list.  mklist_mor_cell (mklist_mor_cell.F90:8-327,
+ * 27-cell scan) or mklist2a_mor (mklist_mor.F90: all later Morse atoms) by
+ * the rule of rdscript.F90:1616-1632 (cells of rcut_bookmor, fewer than 3 per
+ * direction or at most 27 in all -> mklist2a_mor; list_mode forces either).
+ * *nlistmorall receives the reference's count (0 sentinels included). */
+pgk_status pgk_mklist_mor_cell(pgk_ctx* ctx, int64_t* nlistmorall);
+/* The last Morse list in the reference layout: nmorselist[nmorse] (1-based
+ * atoms), mor_indexall[nmorse] (1-based start of row mor1 = 1..nmorse-1;
+ * entry nmorse holds nlistmorall+1), mor_listall[nlistmorall] (1-based j, a 0
+ * for an empty row).  Any array may be NULL; cap = capacity of mor_listall. */
+pgk_status pgk_get_morlist(pgk_ctx* ctx, int32_t* nmorselist, int32_t* mor_indexall, int32_t* mor_listall,
+                           int64_t cap, int64_t* nlistmorall, int32_t* nmorse);
 
 /* rattle_c (rattle.F90:6-272) on the device state, given atmcor_old (3,natom)
  * on the host (copied in).  dt_short = time step used for the correction. */

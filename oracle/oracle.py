@@ -77,6 +77,8 @@ def lib():
         L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
         L.orc_spme_hf_atm.argtypes = [vp, pd, pd]
         L.orc_mor_list.argtypes = [vp, i64p]
+        L.orc_get_mor_list.argtypes = [vp, pi, pi, pi, C.c_longlong, i64p, pi]
+        L.orc_morsep.argtypes = [vp, pd, C.POINTER(abi.EnergiesStruct), C.POINTER(abi.VirialsStruct)]
         L.orc_morse_hf_atm.argtypes = [vp, pd, pd]
         _lib = L
     return _lib
@@ -243,6 +245,23 @@ class Oracle:
         n = C.c_longlong(0)
         mode = self.L.orc_mor_list(self.h, C.byref(n))
         return mode, n.value
+
+    def get_mor_list(self):
+        """(nmorselist, mor_indexall, mor_listall) of the last Morse list,
+        1-based, in the reference layout."""
+        nl = C.c_longlong(0)
+        nm = C.c_int32(0)
+        self.L.orc_get_mor_list(self.h, None, None, None, 0, C.byref(nl), C.byref(nm))
+        atoms = np.zeros(max(nm.value, 1), np.int32)
+        idx = np.zeros(max(nm.value, 1), np.int32)
+        lst = np.zeros(max(nl.value, 1), np.int32)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self.L.orc_get_mor_list(self.h, ip(atoms), ip(idx), ip(lst), nl.value, C.byref(nl), C.byref(nm))
+        return atoms[:nm.value], idx[:nm.value], lst[:nl.value]
+
+    def morsep(self):
+        f, e, v, _ = self._call3(self.L.orc_morsep)
+        return f, e, v
 
     def spme_hf_atm(self):
         """Per-atom split of fft_pmep: pot_atm (N) with the self term and

@@ -2441,6 +2441,43 @@ int orc_mor_list(void* h, long long* npair) {
     if (npair) *npair = (long long)o->mor_list.size();
     return o->mor_list_mode;
 }
+// the Morse list itself in the reference layout (mklist_mor_cell.F90:250-300):
+// nmorselist (1-based atoms), mor_indexall rows 1..nmorse-1 (1-based starts,
+// entry nmorse = nlistmorall + 1), mor_listall (1-based, 0 for an empty row)
+int orc_get_mor_list(void* h, int* nmorselist, int* mor_index, int* mor_list, long long cap, long long* nl,
+                     int* nmorse) {
+    Oracle* o = (Oracle*)h;
+    const int nm = (int)o->mor_atoms.size();
+    if (nmorse) *nmorse = nm;
+    if (nm == 0) { if (nl) *nl = 0; return PGK_OK; }
+    long long icut = 0;
+    for (int m = 0; m + 1 < nm; ++m) {
+        if (mor_index) mor_index[m] = (int)(icut + 1);
+        const int b = o->mor_idx[m], e = o->mor_idx[m + 1];
+        if (b == e) {
+            if (mor_list && icut < cap) mor_list[icut] = 0;
+            ++icut;
+            continue;
+        }
+        for (int q = b; q < e; ++q, ++icut)
+            if (mor_list && icut < cap) mor_list[icut] = o->mor_list[q] + 1;
+    }
+    if (mor_index) mor_index[nm - 1] = (int)(icut + 1);
+    if (nmorselist) for (int m = 0; m < nm; ++m) nmorselist[m] = o->mor_atoms[m] + 1;
+    if (nl) *nl = icut;
+    return PGK_OK;
+}
+// morsep alone at the current positions (force added, energies, virials)
+int orc_morsep(void* h, double* force, pgk_energies* e, pgk_virials* v) {
+    Oracle* o = (Oracle*)h;
+    if (o->welmor.empty()) return PGK_E_INVALID;
+    if (o->mor_idx.empty()) mklist_mor(*o);
+    pgk_energies E{}; pgk_virials V{};
+    morsep(*o, force, E.pot_mor, V.pot_viri_mor, V.pot_virit_mor);
+    if (e) *e = E;
+    if (v) *v = V;
+    return PGK_OK;
+}
 int orc_spme_hf_atm(void* h, double* pot_atm, double* viri) {
     Oracle* o = (Oracle*)h;
     if (!o->prm.ifspme) return PGK_E_INVALID;

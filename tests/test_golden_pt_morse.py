@@ -157,18 +157,26 @@ def test_ring14_rb_reset_is_what_the_reference_ran(oracle_mod):
         assert abs(got[k] * want["eref"] - want[k]) > 5.0 * abs(want[k])
 
 
-def test_engine_reports_morse_unsupported():
-    """The device engine has no Morse kernel yet: pgk_init refuses a system
-    with a Morse type pair before it touches a device (PGK_E_UNSUPPORTED)."""
+def test_engine_accepts_morse_pair_types():
+    """Morse type pairs (inter_inttyp 2) pass pgk_init's input checks (the
+    device evaluates them, k_morse.cu); a Morse pair type without Morse
+    parameters is invalid.  Without a GPU the call ends at the device check."""
     import ctypes as C
     from thrid_b200 import pgk
-    s, _ = load_pt_morse()
     L = pgk.lib()
-    cs = abi.CSystem(s)
-    ps = abi.params_struct(s.params)
-    h = C.c_void_p()
-    assert L.pgk_init(C.byref(cs.struct), C.byref(ps), C.byref(h)) == abi.PGK_E_UNSUPPORTED
-    assert not h.value
+
+    def init(s):
+        cs = abi.CSystem(s)
+        ps = abi.params_struct(s.params)
+        h = C.c_void_p()
+        st = L.pgk_init(C.byref(cs.struct), C.byref(ps), C.byref(h))
+        if h.value:
+            L.pgk_free(h)
+        return st
+    s, _ = load_pt_morse()
+    assert init(s) in (abi.PGK_OK, abi.PGK_E_CUDA)
+    s.mor_wel = None
+    assert init(s) == abi.PGK_E_INVALID
 
 
 def test_engine_input_checks_for_pair_types():

@@ -1,66 +1,75 @@
 """Device engine against the reference's recorded Pt/Morse step.
 
-The engine has no Morse kernel yet, so it runs the recorded state with Morse
-switched off (mts_mor = none: the Pt-Pt pairs carry neither Morse nor LJ) and
-every other printed term of the step is compared with the device result
-(tests/golden/pt_morse_step1.npz, loaded by tests/test_golden_pt_morse.py,
-whose CPU tests pin the oracle to the same values).
+The engine evaluates the recorded state (tests/golden/pt_morse_step1.npz,
+loaded by tests/test_golden_pt_morse.py, whose CPU tests pin the oracle to the
+same values) with both MTS groups, Morse pairs included (k_morse.cu), and
+every printed energy term, the total, the virials and the virial tensor of
+the step are compared with the device result directly.
 """
-import math
-
 import numpy as np
 import pytest
 
+from tests.conftest import rel_rms
 from tests.test_golden_pt_morse import load_pt_morse, printed
 from thrid_b200 import abi
 
-NON_MORSE = ("pot_vdw", "pot_elc", "pot_ewk", "pot_ewc", "pot_vdw14", "pot_elc14", "pot_bond", "pot_angl",
-             "pot_tors", "pot_torsrb")
+TERMS = ("pot_mor", "pot_vdw", "pot_elc", "pot_ewk", "pot_ewc", "pot_vdw14", "pot_elc14", "pot_bond", "pot_angl",
+         "pot_tors", "pot_torsrb", "pot_tot")
 
 
 def _engine_terms(precision):
-    """The device engine on the recorded state with Morse switched off
-    (mts_mor = none: Pt-Pt pairs carry neither Morse nor LJ), both MTS
-    groups summed."""
+    """The device engine on the recorded state, both MTS groups summed
+    (forces, energies, virials)."""
     from thrid_b200.pgk import PgkEngine
     s, want = load_pt_morse(precision)
-    p = dict(s.params)
-    p["mts_mor"] = 0
-    eng = PgkEngine(s, p)
+    eng = PgkEngine(s)
     eng.mklist_cell()
-    _, el, vl = eng.calforce(abi.MTS_LONG)
-    _, es, vs = eng.calforce(abi.MTS_SHORT)
+    fl, el, vl = eng.calforce(abi.MTS_LONG)
+    fs, es, vs = eng.calforce(abi.MTS_SHORT)
+    eng.close()
     e = {k: el[k] + es[k] for k in el}
     v = {k: np.asarray(vl[k]) + np.asarray(vs[k]) for k in vl}
-    return want, e, v
+    return s, want, fl + fs, e, v
 
 
 @pytest.mark.gpu
 def test_engine_fp64_matches_recorded_run():
     """FP64 device path against the reference's printed step-1 values: every
-    energy term but Morse, and the LJ, Coulomb, bond and 1-4 virials, within
-    half a unit of the 8th printed digit (slack 2 for the device sum order)."""
-    want, e, v = _engine_terms(abi.PREC_FP64)
-    assert e["pot_mor"] == 0.0
-    for k in NON_MORSE:
+    energy term (Morse included) and the total, the LJ, Morse, Coulomb, bond
+    and 1-4 virials and the nine entries of the virial tensor, within half a
+    unit of the 8th printed digit (slack 2 for the device sum order)."""
+    _, want, _, e, v = _engine_terms(abi.PREC_FP64)
+    for k in TERMS:
         assert printed(want[k], e[k], want["eref"], slack=2.0), (k, e[k] * want["eref"], want[k])
-    # pot_tot less the Morse term: a difference of two printed values, so the
-    # bound is the sum of their half-units
-    hu = lambda x: 0.5 * 10.0 ** (math.floor(math.log10(abs(x))) + 1 - 8)
-    assert abs(e["pot_tot"] * want["eref"] - (want["pot_tot"] - want["pot_mor"])) <= \
-        2.0 * (hu(want["pot_tot"]) + hu(want["pot_mor"]))
     assert printed(want["pot_virilj_all"], float(v["pot_viri_lj"]), want["eref"], slack=2.0)
+    assert printed(want["pot_virimor_all"], float(v["pot_viri_mor"]), want["eref"], slack=2.0)
     assert printed(want["pot_viric_all"], float(v["pot_viri_coul"]) + e["pot_ewc"] + e["pot_ewnq"],
                    want["eref"], slack=2.0)
     assert printed(want["atm_viribo_all"], float(v["atm_viri_bond"]), want["eref"], slack=2.0)
     assert printed(want["atm_viri14_all"], float(v["atm_viri_14"]), want["eref"], slack=2.0)
+    tens = sum(v[k] for k in ("pot_virit_coul", "pot_virit_lj", "pot_virit_mor", "atm_virit_bond",
+                              "atm_virit_angl", "atm_virit_tors", "atm_virit_14")).reshape(3, 3).T
+    for i in range(3):
+        for j in range(3):
+            assert printed(want[f"preatmt_vtot{i + 1}{j + 1}"], tens[i, j], want["eref"], slack=2.0), (i, j)
 
 
 @pytest.mark.gpu
-def test_engine_mixed_tracks_recorded_run():
-    """Mixed-precision device path against the same printed values, each
-    energy term within 1e-4 of itself (FP32 pair and bonded arithmetic)."""
-    want, e, _ = _engine_terms(abi.PREC_MIXED)
-    for k in NON_MORSE:
+def test_engine_mixed_tracks_recorded_run(oracle_mod):
+    """Mixed-precision device path on the recorded state: force RMS relative
+    error within 1e-5 of the FP64 oracle (whose energies reproduce the
+    printed ones), every printed energy term within 1e-5 of the largest
+    energy term and within 1e-4 of itself."""
+    from tests.test_golden_pt_morse import oracle_energies
+    s, want, f, e, _ = _engine_terms(abi.PREC_MIXED)
+    o = oracle_mod.Oracle(s, threads=8)
+    o.mklist()
+    of = o.calforce(abi.MTS_LONG)[0] + o.calforce(abi.MTS_SHORT)[0]
+    err = rel_rms(f, of)
+    print(f"mixed force RMS relative error on the recorded state: {err:.2e}")
+    assert err < 1e-5
+    scale = max(abs(want[k]) for k in TERMS) / want["eref"]
+    for k in TERMS:
         w = want[k] / want["eref"]
-        assert abs(e[k] - w) <= 1e-4 * abs(w), (k, e[k], w)
+        print(f"{k}: mixed {e[k]:.10e} recorded {w:.10e} rel {abs(e[k] - w) / abs(w):.2e}")
+        assert abs(e[k] - w) <= 1e-5 * scale and abs(e[k] - w) <= 1e-4 * abs(w), (k, e[k], w)

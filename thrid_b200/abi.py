@@ -60,11 +60,11 @@ class ParamsStruct(C.Structure):
         ("mts_bond", C.c_int32), ("mts_angl", C.c_int32), ("mts_tors", C.c_int32), ("mts_torsrb", C.c_int32),
         ("mts_vdw", C.c_int32), ("mts_ewk", C.c_int32), ("mts_vdw14", C.c_int32), ("mts_elc14", C.c_int32),
         ("ifnetqcorrp", C.c_int32), ("max_nbr", C.c_int32),
-        ("rcutmor", C.c_double), ("rcut_bookmor", C.c_double), ("mts_mor", C.c_int32), ("_pad_mor", C.c_int32),
+        ("rcutmor", C.c_double), ("rcut_bookmor", C.c_double), ("mts_mor", C.c_int32), ("nstep_bookmor", C.c_int32),
     ]
 
 # run-time parameters a system may leave out (no Morse pairs)
-PARAM_DEFAULTS = {"rcutmor": 0.0, "rcut_bookmor": 0.0, "mts_mor": 0, "_pad_mor": 0}
+PARAM_DEFAULTS = {"rcutmor": 0.0, "rcut_bookmor": 0.0, "mts_mor": 0, "nstep_bookmor": 0}
 
 
 class MdParamsStruct(C.Structure):

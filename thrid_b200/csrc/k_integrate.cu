@@ -441,13 +441,14 @@ __device__ void press_run(const long long* __restrict__ acc, const DynState* __r
     for (int k = 0; k < 9; ++k) Wt[k] = 0.0;
     for (int g = 0; g < 2; ++g) {
         const long long* G = acc + (size_t)g * NACC;
-        W += acc_get(G, A_VC, dbl) + acc_get(G, A_VLJ, dbl) + acc_get(G, A_VB, dbl) + acc_get(G, A_VA, dbl) + acc_get(G, A_VT, dbl) + acc_get(G, A_V14, dbl);
+        W += acc_get(G, A_VC, dbl) + acc_get(G, A_VLJ, dbl) + acc_get(G, A_VB, dbl) + acc_get(G, A_VA, dbl) + acc_get(G, A_VT, dbl) + acc_get(G, A_V14, dbl) +
+             acc_get(G, A_VMOR, dbl);   // calpress.F90:146-151 (pot_viri_mor)
         for (int k = 0; k < 9; ++k) {
             // coulomb / LJ tensors are stored as their lower triangle
             int r = k % 3, cl = k / 3;
             int ks = r >= cl ? k : cl + 3 * r;
             Wt[k] += acc_get(G, A_VTC + ks, dbl) + acc_get(G, A_VTLJ + ks, dbl) + acc_get(G, A_VTB + k, dbl) + acc_get(G, A_VTA + k, dbl) +
-                     acc_get(G, A_VTT + k, dbl) + acc_get(G, A_VT14 + k, dbl);
+                     acc_get(G, A_VTT + k, dbl) + acc_get(G, A_VT14 + k, dbl) + acc_get(G, A_VTMOR + k, dbl);
         }
     }
     if (a.ifspme && !a.ifnetqcorrp) {      // calforce.F90:1018-1050 (long group)

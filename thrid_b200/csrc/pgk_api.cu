@@ -121,6 +121,7 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         const int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
         if ((s = launch_pair(c, g, vmode))) return s;
     }
+    if (c->nmor && c->prm.mts_mor == flag && (s = launch_morse(c, g, ene || vir))) return s;   // calforce.F90:360-400
     if (fork) {
         PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
         return PGK_OK;
@@ -164,18 +165,21 @@ pgk_status read_acc(pgk_ctx* c, int gmask, pgk_energies* e, pgk_virials* v, bool
         e->pot_vdw = S[A_VDW]; e->pot_elc = S[A_ELC]; e->pot_ewk = S[A_EWK];
         e->pot_vdw14 = S[A_VDW14]; e->pot_elc14 = S[A_ELC14];
         e->pot_bond = S[A_BOND]; e->pot_angl = S[A_ANGL]; e->pot_tors = S[A_TORS]; e->pot_torsrb = S[A_TORSRB];
+        e->pot_mor = S[A_MOR];
         if (add_ewald_consts && c->prm.ifspme) { e->pot_ewc = c->pot_ewc; e->pot_ewnq = 0.5 * a1 * c->netchrgsq; }
         e->pot_nonbon = e->pot_vdw + e->pot_elc + e->pot_ewk + e->pot_ewc + e->pot_ewnq + e->pot_vdw14 + e->pot_elc14;
-        e->pot_tot = e->pot_bond + e->pot_angl + e->pot_tors + e->pot_torsrb + e->pot_nonbon;
+        e->pot_tot = e->pot_bond + e->pot_angl + e->pot_tors + e->pot_torsrb + e->pot_mor + e->pot_nonbon;
     }
     if (v) {
         memset(v, 0, sizeof(*v));
         v->pot_viri_coul = S[A_VC]; v->pot_viri_lj = S[A_VLJ];
         v->atm_viri_bond = S[A_VB]; v->atm_viri_angl = S[A_VA]; v->atm_viri_tors = S[A_VT]; v->atm_viri_14 = S[A_V14];
+        v->pot_viri_mor = S[A_VMOR];
         for (int k = 0; k < 9; ++k) {
             v->pot_virit_coul[k] = S[A_VTC + k]; v->pot_virit_lj[k] = S[A_VTLJ + k];
             v->atm_virit_bond[k] = S[A_VTB + k]; v->atm_virit_angl[k] = S[A_VTA + k];
             v->atm_virit_tors[k] = S[A_VTT + k]; v->atm_virit_14[k] = S[A_VT14 + k];
+            v->pot_virit_mor[k] = S[A_VTMOR + k];
         }
     }
     return PGK_OK;
@@ -248,7 +252,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
             const int t = s->inter_inttyp[k];
             if (t < 1 || t > 10) return PGK_E_INVALID;
             if (t >= 3) return PGK_E_UNSUPPORTED;                            // SH, RFH, DOU, RP-VW, custom
-            if (t == 2 && s->para_welmor && p->mts_mor != PGK_MTS_NONE) return PGK_E_UNSUPPORTED;   // Morse
+            if (t == 2 && p->mts_mor != PGK_MTS_NONE && (!s->para_welmor || !s->para_radmor || !s->para_alphamor))
+                return PGK_E_INVALID;                                        // Morse pair without parameters
         }
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return PGK_E_CUDA;
@@ -319,6 +324,7 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         }
     TRY(upload(c, &c->lj64, lj64));
     TRY(upload(c, &c->lj32, lj32));
+    TRY(morse_setup(c, s));
     // ---- spline tables (spline_interp.F90:14-136) ----
     {
         int ns = p->nspltbl > 0 ? p->nspltbl : 1100;
@@ -598,7 +604,9 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec,
-                    c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out};
+                    c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out,
+                    c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
+                    c->mor_cstart, c->mor_cfill, c->mor_ctr};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st2) { cudaStreamSynchronize(c->st2); cudaStreamDestroy(c->st2); }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -731,6 +739,30 @@ pgk_status pgk_ewaldkp_hf(pgk_ctx* c, int32_t kmax, double* force, double* pot_a
     return read_status(c);
 }
 
+pgk_status pgk_mklist_mor_cell(pgk_ctx* c, int64_t* nl) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s = launch_mklist_mor(c);
+    if (s) return s;
+    return export_morlist(c, nullptr, nullptr, nullptr, 0, nl);
+}
+
+pgk_status pgk_get_morlist(pgk_ctx* c, int32_t* nmorselist, int32_t* mor_indexall, int32_t* mor_listall,
+                           int64_t cap, int64_t* nl, int32_t* nmorse) {
+    if (!c) return PGK_E_INVALID;
+    if (nmorse) *nmorse = c->nmor;
+    return export_morlist(c, nmorselist, mor_indexall, mor_listall, cap, nl);
+}
+
+pgk_status pgk_morsep(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s;
+    bool want = e || v;
+    if ((s = launch_zero_group(c, 0)) || (s = launch_morse(c, 0, want))) return s;
+    if (force && (s = force_to_host(c, 0, force, true))) return s;
+    if (want && (s = read_acc(c, 1, e, v, false))) return s;
+    return read_status(c);
+}
+
 pgk_status pgk_calbonded(pgk_ctx* c, double* force, pgk_energies* e, pgk_virials* v) {
     if (!c) return PGK_E_INVALID;
     pgk_status s;
@@ -849,6 +881,8 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     if ((kind == 1 || kind == 2) && (md->mchain < 2 || md->mchain > 8 || md->nyosh < 1 || md->nyosh > 8 || md->next < 1))
         return pgk_fail(c, PGK_E_INVALID, "chain parameters");
     const int nb = c->prm.nstep_book > 0 ? c->prm.nstep_book : 1;
+    // Morse list cadence (nstep_bookmor; 0 = the pair list's)
+    const int nbm = c->prm.nstep_bookmor > 0 ? c->prm.nstep_bookmor : nb;
     const bool mtk = kind == 2;
     const bool hfdrv = kind == 3;
     const bool lt = hfdrv && c->hfp.nlangeregion > 0;
@@ -873,6 +907,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
         bool tens = mtk && md->pcont_axis != PGK_PCONT_ISO && !ene;   // nhcpanisoint reads diag(pintt) only
         if (step % nb == 1 || nb == 1 || step == 0) RUN(launch_transcor(c));
         if (step % nb == 0 || nb == 1) RUN(launch_mklist(c));
+        if (c->nmor && (step % nbm == 0 || nbm == 1 || !c->mor_valid)) RUN(launch_mklist_mor(c));
         const bool hfs = hfdrv && per > 0 && step > 0 && (hfi == 1 || step % hfi == 1);
         if (step == 0) {
             if (lt) RUN(launch_lt_regist(c));
@@ -880,7 +915,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press(c)); }
             ke_ready = mtk;
-        } else if (c->use_graphs && c->list_valid && !hfs && !lt) {
+        } else if (c->use_graphs && c->list_valid && (c->nmor == 0 || c->mor_valid) && !hfs && !lt) {
             // the step's kernel sequence depends only on (ene, vir, tens) and the
             // list build; replay a captured CUDA graph of it
             const int key = 16 * kind + ((ene ? 1 : 0) | (vir ? 2 : 0) | (tens ? 4 : 0) | (ke_ready ? 8 : 0));
@@ -1057,6 +1092,8 @@ pgk_status pgk_get_output(pgk_ctx* c, double* out, int64_t cap, int64_t* n) {
 
 pgk_status pgk_set_hf(pgk_ctx* c, const pgk_hfparams* hf) {
     if (!c || !hf) return PGK_E_INVALID;
+    if (c->nmor)   // the per-atom Morse shares of morsep_hf (morse_hf.F90) are not built on the device
+        return pgk_fail(c, PGK_E_UNSUPPORTED, "heat flux with Morse pairs (morsep_hf) is not built");
     std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     return hf_setup(c, hf);
 }

@@ -152,6 +152,22 @@ struct pgk_ctx {
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
 
+    // ---- Morse pairs (k_morse.cu): own list (radius rcut_bookmor) and kernel ----
+    int nmor = 0;                 // Morse atoms (0: no Morse pairs or Morse switched off)
+    int* mor_atoms = nullptr;     // [nmor] nmorselist, 0-based ascending
+    double4* mor_par = nullptr;   // [ntyp*ntyp] (D, r0, alpha, Morse type pair) at it + ntyp*jt
+    int mor_cap = 0;              // row capacity (entries)
+    int* mor_rows = nullptr;      // [nmor * mor_cap] partners, reference row order
+    int* mor_cnt = nullptr;       // [nmor]
+    int* mor_cell = nullptr;      // [nmor] cell key (cell mode)
+    int* mor_csort = nullptr;     // [nmor] Morse atoms by cell, ascending inside a cell
+    int *mor_ccnt = nullptr, *mor_cstart = nullptr, *mor_cfill = nullptr;
+    int mor_maxcells = 0;
+    unsigned long long* mor_ctr = nullptr;   // [0] entries, [1] longest row of the last build
+    int mor_mode = 0;             // PGK_LIST_* order of the last build
+    long long mor_entries = 0;
+    bool mor_valid = false;
+
     // ---- device-side output records ----
     double* out_rec = nullptr;    // [out_cap][PGK_OUT_NCOL]
     long long out_cap = 0, out_n = 0;
@@ -253,6 +269,13 @@ pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_a
 // tens: only the total bonded virial tensor is wanted (it goes to the bond
 // tensor slot; no energies), as in the anisotropic MTK steps without output
 pgk_status launch_intra(pgk_ctx* c, int group, int mask, bool want, bool tens = false);
+
+// ---- launchers (k_morse.cu) ----
+pgk_status morse_setup(pgk_ctx* c, const pgk_system* s);
+pgk_status launch_mklist_mor(pgk_ctx* c);
+pgk_status launch_morse(pgk_ctx* c, int group, bool ev);
+pgk_status export_morlist(pgk_ctx* c, int32_t* nmorselist, int32_t* mor_index, int32_t* mor_list, int64_t cap,
+                          int64_t* nl);
 
 // ---- launchers (k_heatf.cu, heat flux + region Langevin) ----
 struct HfDev;

@@ -84,6 +84,9 @@ def lib():
     L.pgk_get_hf_atm.argtypes = [vp, pd, pd]
     L.pgk_langevin_dekin.argtypes = [vp, pd]
     L.pgk_ewaldkp_hf.argtypes = [vp, C.c_int32, pd, pd, pd, C.POINTER(abi.EwkHfStruct)]
+    L.pgk_morsep.argtypes = [vp, pd, E, V]
+    L.pgk_mklist_mor_cell.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.pgk_get_morlist.argtypes = [vp, pi, pi, pi, C.c_int64, C.POINTER(C.c_int64), pi]
     _lib = L
     return L
 
@@ -173,6 +176,28 @@ class PgkEngine:
         self._check(self.L.pgk_get_nblist(self.h, idx.ctypes.data_as(C.POINTER(C.c_int32)),
                                           lst.ctypes.data_as(C.POINTER(C.c_int32)), nl.value, C.byref(nl)))
         return idx, lst[:nl.value]
+
+    def mklist_mor_cell(self):
+        nl = C.c_int64(0)
+        self._check(self.L.pgk_mklist_mor_cell(self.h, C.byref(nl)))
+        return nl.value
+
+    def get_morlist(self):
+        """(nmorselist, mor_indexall, mor_listall) of the last Morse list,
+        1-based, in the reference layout."""
+        nl = C.c_int64(0)
+        nm = C.c_int32(0)
+        self._check(self.L.pgk_get_morlist(self.h, None, None, None, 0, C.byref(nl), C.byref(nm)))
+        atoms = np.zeros(max(nm.value, 1), np.int32)
+        idx = np.zeros(max(nm.value, 1), np.int32)
+        lst = np.zeros(max(nl.value, 1), np.int32)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._check(self.L.pgk_get_morlist(self.h, ip(atoms), ip(idx), ip(lst), nl.value, C.byref(nl),
+                                           C.byref(nm)))
+        return atoms[:nm.value], idx[:nm.value], lst[:nl.value]
+
+    def morsep(self):
+        return self._fev(self.L.pgk_morsep)
 
     def _fev(self, fn, *pre):
         f = np.zeros((self.sys.natom, 3))
