@@ -84,10 +84,15 @@ template <typename T>
 __device__ __forceinline__ bool eval_bond(const double* P, int i, int j, double2 p, const DynState* dyn,
                                           double (&F)[3], double (&rd)[3], double& pot) {
     if (fabs(p.x) < 1.0e-16) return false;
-    T r[3];
-    disp<T>(P, i, j, dyn, r);
-    T rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    T dr = rr - (T)p.y;
+    // the stretch r - r0 is a small difference of two ~1.5 A lengths: formed in
+    // FP64 in both precisions (in FP32 its rounding alone is ~1e-5 of a
+    // thermal stretch); the force arithmetic after it runs in T
+    double r64[3];
+    disp<double>(P, i, j, dyn, r64);
+    const double rr64 = sqrt(r64[0] * r64[0] + r64[1] * r64[1] + r64[2] * r64[2]);
+    const T r[3] = {(T)r64[0], (T)r64[1], (T)r64[2]};
+    const T rr = (T)rr64;
+    const T dr = (T)(rr64 - p.y);
     T fa = T(-2) * (T)p.x * dr;
 #pragma unroll
     for (int d = 0; d < 3; ++d) { F[d] = (double)(fa * r[d] / rr); rd[d] = (double)r[d]; }
