@@ -345,9 +345,10 @@ __global__ void __launch_bounds__(256) k_build_clist(
         const int tq = lane < qn ? queue[lane] : -1;
         test_batch(tq);
     }
-    // Group the row's entries by mask (stable counting sort in shared memory):
-    // 32 consecutive entries then mostly share one mask, so the pair kernel's
-    // loop over the mask bits is uniform across the warp.  Entries keep their
+    // Group the row's entries by mask (stable counting sort in shared memory,
+    // bins in inverse-Gray-code order of the masks): 32 consecutive entries
+    // then mostly share their mask bits, so the pair kernel's loop over the
+    // mask bits is nearly uniform across the warp.  Entries keep their
     // candidate (spatial) order inside a mask group; the result is the same on
     // every build of the same positions.
     if (sort_rows && count <= ccap) {
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
         for (int k = lane; k < count; k += 32) {
             const int e = row[k];
             buf[k] = e;
-            atomicAdd(&bin[(unsigned)e >> 24], 1);
+            atomicAdd(&bin[mask_bin((unsigned)e >> 24)], 1);
         }
         __syncwarp();
         warp_scan256(bin, lane);                 // exclusive scan of the 256 bins
@@ -368,7 +369,7 @@ __global__ void __launch_bounds__(256) k_build_clist(
             const int k = k0 + lane;
             const bool ok = k < count;
             const int e = ok ? buf[k] : 0;
-            const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
+            const unsigned key = ok ? mask_bin((unsigned)e >> 24) : 256u + lane;
             const unsigned grp = __match_any_sync(0xffffffffu, key);
             const int rank = __popc(grp & ((1u << lane) - 1u));
             const int base = ok ? bin[key] : 0;

@@ -118,12 +118,12 @@ __device__ __forceinline__ void pair_term(const float dx, const float dy, const 
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
     const float r = r2 * rinv;
-    // floor(r/h) on the FP32/ALU pipes (r/h < 2^22): round to nearest via
-    // the 2^23 magic constant, step down when it rounded up
+    // floor(r/h) on the FP32/ALU pipes: adding 2^23 rounded toward -inf
+    // leaves floor(r/h) in the low mantissa bits (exact for r/h < 2^23)
     const float tf = r * inv_h;
-    float fm = (tf + 8388608.0f) - 8388608.0f;
-    fm = fm > tf ? fm - 1.0f : fm;
-    int idx = __float_as_int(fm + 8388608.0f) - 0x4B000000;
+    const float fb = __fadd_rd(tf, 8388608.0f);
+    const float fm = fb - 8388608.0f;
+    int idx = __float_as_int(fb) - 0x4B000000;
     idx = (int)min((unsigned)idx, (unsigned)nsplm1);      // into the table whatever r is (NaN included)
     const float d = fmaf(-fm, h, r);
     const float4 c = sf[idx];
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, con
     __syncwarp();
     for (int k0 = 0; k0 < count; k0 += 32) {
         const int k = k0 + lane;
-        const unsigned key = k < count ? ((unsigned)buf[k] >> 24) : 256u + lane;
+        const unsigned key = k < count ? mask_bin((unsigned)buf[k] >> 24) : 256u + lane;
         const unsigned grp = __match_any_sync(0xffffffffu, key);
         if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
     }
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, con
         const int k = k0 + lane;
         const bool ok = k < count;
         const int e = ok ? buf[k] : 0;
-        const unsigned key = ok ? ((unsigned)e >> 24) : 256u + lane;
+        const unsigned key = ok ? mask_bin((unsigned)e >> 24) : 256u + lane;
         const unsigned grp = __match_any_sync(0xffffffffu, key);
         const int rank = __popc(grp & ((1u << lane) - 1u));
         const int base = ok ? bin[key] : 0;

@@ -161,6 +161,17 @@ __device__ __forceinline__ double force_get(const void* facc, size_t k) {
     return ((const double*)facc)[k];
 }
 
+// Sort bin of a cluster-row entry's 8-bit mask: the inverse Gray code, so
+// that masks next to each other in the sorted row differ in few bits (the
+// pair kernel's loop over the mask bits then leaves fewer lanes idle than in
+// numeric mask order)
+__device__ __forceinline__ unsigned mask_bin(unsigned m) {
+    m ^= m >> 1;
+    m ^= m >> 2;
+    m ^= m >> 4;
+    return m & 0xFFu;
+}
+
 // Fortran dnint/anint (round half away from zero), exact FP64 min image
 // exclusive prefix sum of 256 shared-memory bins by one warp (8 bins a lane)
 __device__ __forceinline__ void warp_scan256(int* bin, int lane) {
