@@ -402,6 +402,30 @@ typedef struct pgk_ewk_hf {
 pgk_status pgk_ewaldkp_hf(pgk_ctx* ctx, int32_t kmax, double* force, double* pot_elc_atm,
                           double* virielct_atm, pgk_ewk_hf* out);
 
+/* Per-atom reciprocal term of the bulk heat flux.  PGK_HF_KSPACE_NONE (the
+ * default, as the reference's default heat-flux build: the reciprocal term is
+ * not split per atom); PGK_HF_KSPACE_EWK: the -D_HF_BULK_EWK build
+ * (calforce_hf.F90:1046-1062) -- on heat-flux steps ewaldkp_hf with waves up
+ * to kmax replaces the SPME term (force, pot_ewk, virial) and adds its
+ * per-atom energy and virial; PGK_HF_KSPACE_SPME: the SPME force stays and
+ * the per-atom split of the SPME term (pgk_fft_pme_hf) is added.  Either way
+ * the energy goes to each atom's pot_elc_atm and the (a, z) column of the
+ * tensor to region 1 of virielct_atm (ewaldk_hf.F90:212-230 writes region 1). */
+#define PGK_HF_KSPACE_NONE 0
+#define PGK_HF_KSPACE_EWK  1
+#define PGK_HF_KSPACE_SPME 2
+pgk_status pgk_set_hf_kspace(pgk_ctx* ctx, int32_t mode, int32_t kmax);
+
+/* Per-atom split of fft_pmep's reciprocal energy and virial tensor: the SPME
+ * form of ewaldkp_hf's per-atom terms (ewaldk_hf.F90:165-230, which the
+ * reference has only for standard Ewald).  With S = FFT(Q) and scalar_sum's
+ * influence function eterm: pot_atm[i] = 1/2 q_i sum_g theta_i(g)
+ * IFFT(eterm S)(g) - alpha/sqrt(pi) q_i^2; viri_atm[9i + a + 3b] = 1/2 q_i
+ * sum_g theta_i(g) IFFT(eterm (delta_ab - vterm h_a h_b) S)(g).  The energies
+ * less the self terms sum to pot_ewk and the tensors to pot_virit_coul (the
+ * net-charge terms are global and not split).  FP64 in both precisions. */
+pgk_status pgk_fft_pme_hf(pgk_ctx* ctx, double* pot_atm, double* viri_atm);
+
 /* det_ene_kin of langevin_region.F90 (kinetic energy put in (+) or taken out
  * (-) per Langevin region) summed since the last call, then reset. */
 pgk_status pgk_langevin_dekin(pgk_ctx* ctx, double* det_ene_kin);

@@ -76,6 +76,7 @@ def lib():
         L.orc_ewk_nvec.argtypes = [C.c_int, C.c_double, C.c_double, pi, C.c_int, pi]
         L.orc_ewaldkp_hf.argtypes = [vp, C.c_int, pd, pd, pd, pd, pi]
         L.orc_spme_hf_atm.argtypes = [vp, pd, pd]
+        L.orc_set_hf_kspace.argtypes = [vp, C.c_int, C.c_int]
         L.orc_mor_list.argtypes = [vp, i64p]
         L.orc_get_mor_list.argtypes = [vp, pi, pi, pi, C.c_longlong, i64p, pi]
         L.orc_morsep.argtypes = [vp, pd, C.POINTER(abi.EnergiesStruct), C.POINTER(abi.VirialsStruct)]
@@ -262,6 +263,11 @@ class Oracle:
     def morsep(self):
         f, e, v, _ = self._call3(self.L.orc_morsep)
         return f, e, v
+
+    def set_hf_kspace(self, mode, kmax=0):
+        st = self.L.orc_set_hf_kspace(self.h, int(mode), int(kmax))
+        if st:
+            raise RuntimeError(f"orc_set_hf_kspace status {st}")
 
     def spme_hf_atm(self):
         """Per-atom split of fft_pmep: pot_atm (N) with the self term and

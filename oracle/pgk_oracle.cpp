@@ -160,6 +160,12 @@ struct Oracle {
         std::vector<int> ltreg;    // Langevin region of each atom (-1: none)
         std::vector<double> frand; // 3N accelerations of the former half
         double dekin[8];
+        // per-atom reciprocal term of the bulk heat flux (PGK_HF_KSPACE_*):
+        // EWK = the -D_HF_BULK_EWK build (calforce_hf.F90:1046-1062)
+        int kspace = 0, kmax = 0;
+        bool ewk_now = false;      // this force evaluation is the heat-flux step's
+        bool ewk_fresh = false;    // ewk_pot / ewk_vir hold ewaldkp_hf at the current positions
+        std::vector<double> ewk_pot, ewk_vir;
     } hf;
 };
 
@@ -1015,6 +1021,8 @@ void calnon14p(Oracle& o, double* force, double& pe, double& pv, double& vs, dou
     }
 }
 
+int ewaldkp_hf(Oracle& o, int kmax, double* force, double* pot_atm, double* viri, double* sc, int* nwave_out);
+
 // morsep (morse.F90:206-414): Morse energy, forces and virials over the
 // Morse list, pairs beyond rcutmor skipped; forces summed in fmor first
 void morsep(Oracle& o, double* force, double& pot, double& vir, double* virt) {
@@ -1049,7 +1057,23 @@ void calforce(Oracle& o, int flag, double* force, pgk_energies* e, pgk_virials* 
     std::fill(force, force + 3 * o.natom, 0.0);
     pgk_energies E{}; pgk_virials V{};
     if (o.prm.mts_vdw == flag) ewaldrp(o, force, &E, &V);
-    if (o.prm.mts_ewk == flag && o.prm.ifspme) fft_pmep(o, force, &E, &V);
+    if (o.hf.ewk_now && o.prm.mts_ewk == flag) {
+        // -D_HF_BULK_EWK heat-flux step (calforce_hf.F90:1046-1062): ewaldkp_hf
+        // in place of fft_pmep; pot_viri_coul += pot_ewk + pot_ewk_cc (ewaldk_hf.F90:290)
+        const size_t n = (size_t)o.natom;
+        std::vector<double> f(3 * n, 0.0), sc(11, 0.0);
+        o.hf.ewk_pot.assign(n, 0.0);
+        o.hf.ewk_vir.assign(9 * n, 0.0);
+        int nw = 0;
+        ewaldkp_hf(o, o.hf.kmax, f.data(), o.hf.ewk_pot.data(), o.hf.ewk_vir.data(), sc.data(), &nw);
+        for (size_t k = 0; k < 3 * n; ++k) force[k] += f[k];
+        E.pot_ewk += sc[0];
+        V.pot_viri_coul += sc[0] + sc[1];
+        for (int k = 0; k < 9; ++k) V.pot_virit_coul[k] += sc[2 + k];
+        o.hf.ewk_fresh = true;
+    } else if (o.prm.mts_ewk == flag && o.prm.ifspme) {
+        fft_pmep(o, force, &E, &V);
+    }
     if (o.prm.mts_bond == flag) calbondp(o, force, E.pot_bond, V.atm_viri_bond, V.atm_virit_bond);
     if (o.prm.mts_angl == flag) calanglp(o, force, E.pot_angl, V.atm_viri_angl, V.atm_virit_angl);
     if (o.prm.mts_tors == flag) caltorsp(o, force, E.pot_tors, V.atm_viri_tors, V.atm_virit_tors);
@@ -1801,6 +1825,28 @@ void calforce_hf_atm(Oracle& o) {
     if (on(o.prm.mts_tors)) caltorsp_hf(o);
     if (on(o.prm.mts_torsrb)) caltorsrbp_hf(o);
     if (on(o.prm.mts_vdw14) && o.prm.mts_vdw14 == o.prm.mts_elc14) calnon14p_hf(o);
+    // the per-atom reciprocal term: energy to pot_elc_atm, the (a, z) column of
+    // the tensor to region 1 of virielct_atm (ewaldk_hf.F90:212-230)
+    const size_t n = (size_t)o.natom;
+    std::vector<double> pot, vir;
+    if (h.kspace == PGK_HF_KSPACE_SPME) {
+        pot.assign(n, 0.0); vir.assign(9 * n, 0.0);
+        spme_hf_atm(o, pot.data(), vir.data());
+    } else if (h.kspace == PGK_HF_KSPACE_EWK) {
+        if (!h.ewk_fresh) {
+            std::vector<double> f(3 * n, 0.0), sc(11, 0.0);
+            h.ewk_pot.assign(n, 0.0); h.ewk_vir.assign(9 * n, 0.0);
+            int nw = 0;
+            ewaldkp_hf(o, h.kmax, f.data(), h.ewk_pot.data(), h.ewk_vir.data(), sc.data(), &nw);
+        }
+        pot = h.ewk_pot; vir = h.ewk_vir;
+    }
+    h.ewk_fresh = false;
+    if (!pot.empty())
+        for (size_t i = 0; i < n; ++i) {
+            h.pot[(size_t)PGK_HF_ELC * n + i] += pot[i];
+            for (int a = 0; a < 3; ++a) h.W[((size_t)PGK_HF_ELC * h.nreg * 3 + a) * n + i] += vir[9 * i + a + 6];
+        }
 }
 
 // calheatf.F90:365-1466, volume-based, z components; streaming velocity 0
@@ -2024,11 +2070,13 @@ int moldyn_hf(Oracle& o, long long ini, long long end, const pgk_mdparams& md, p
                     int s = rattle_pos(o, old.data(), md.eps_rattle, dts, nullptr);
                     if (s) return s;
                 }
+                o.hf.ewk_now = hfs && is == md.nstep_short && o.hf.kspace == PGK_HF_KSPACE_EWK;
                 force_eval(PGK_MTS_SHORT);
                 if (is == md.nstep_short) {
                     force_eval(PGK_MTS_LONG);
                     if (hfs) calforce_hf_atm(o);
                 }
+                o.hf.ewk_now = false;
                 for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dts * F.fs[k];
                 if (is == md.nstep_short)
                     for (int k = 0; k < 3 * n; ++k) o.atmvel[k] = o.atmvel[k] + 0.5 * dtl * F.fl[k];
@@ -2476,6 +2524,15 @@ int orc_morsep(void* h, double* force, pgk_energies* e, pgk_virials* v) {
     morsep(*o, force, E.pot_mor, V.pot_viri_mor, V.pot_virit_mor);
     if (e) *e = E;
     if (v) *v = V;
+    return PGK_OK;
+}
+int orc_set_hf_kspace(void* h, int mode, int kmax) {
+    Oracle* o = (Oracle*)h;
+    if (mode < PGK_HF_KSPACE_NONE || mode > PGK_HF_KSPACE_SPME || (mode == PGK_HF_KSPACE_EWK && kmax < 1))
+        return PGK_E_INVALID;
+    o->hf.kspace = mode;
+    o->hf.kmax = kmax;
+    o->hf.ewk_fresh = false;
     return PGK_OK;
 }
 int orc_spme_hf_atm(void* h, double* pot_atm, double* viri) {

@@ -117,6 +117,7 @@ class ChainStruct(C.Structure):
 
 
 HF_MAX_REGIONS, LT_MAX_REGIONS, HF_NCOL = 32, 8, 18
+HF_KSPACE_NONE, HF_KSPACE_EWK, HF_KSPACE_SPME = 0, 1, 2
 HFTYP_ATOM, HFTYP_MOLE = 1, 2
 HF_BO, HF_AN, HF_TO, HF_14, HF_ELIN, HF_LJIN, HF_ELC, HF_VDW = range(8)
 HF_COLUMNS = ("hfkin", "hfpotbo", "hfpotan", "hfpotto", "hfpot14", "hfpotelin", "hfpotljin", "hfpotelc",

@@ -362,3 +362,38 @@ pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave_out, int only) {
     if (nwave_out) *nwave_out = nwave;
     return PGK_OK;
 }
+
+// _HF_BULK_EWK heat-flux step (calforce_hf.F90:1046-1062): ewaldkp_hf's force
+// into group g's accumulator in place of the SPME reciprocal force, pot_ewk,
+// pot_viri_coul += pot_ewk + pot_ewk_cc (ewaldk_hf.F90:290) and the tensor
+// (symmetric; the accumulator keeps the lower triangle)
+template <bool MIXED>
+__global__ void k_ewk_force_add(const double* __restrict__ out, int n, void* __restrict__ facc,
+                                long long* __restrict__ acc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < 3 * n) {
+        if (MIXED) atomicAdd((unsigned long long*)facc + t, (unsigned long long)to_fix(out[t], PGK_FORCE_SCALE));
+        else atomicAdd((double*)facc + t, out[t]);
+    }
+    if (t == 0) {
+        const double* sc = out + 13 * (size_t)n;
+        acc_add(&acc[A_EWK], sc[0], !MIXED);
+        acc_add(&acc[A_VC], sc[0] + sc[1], !MIXED);
+        const int lo[6] = {0, 1, 2, 4, 5, 8};
+        for (int k = 0; k < 6; ++k) acc_add(&acc[A_VTC + lo[k]], sc[2 + lo[k]], !MIXED);
+    }
+}
+
+pgk_status launch_ewk_force(pgk_ctx* c, int group) {
+    int nw = 0;
+    pgk_status s = launch_ewk_hf(c, c->hf_kmax, &nw);
+    if (s) return s;
+    const int n = c->natom;
+    long long* acc = c->acc + (size_t)group * NACC;
+    if (c->mixed()) k_ewk_force_add<true><<<(3 * n + 255) / 256, 256, 0, c->st>>>(c->ewk_out, n, c->facc[group], acc);
+    else k_ewk_force_add<false><<<(3 * n + 255) / 256, 256, 0, c->st>>>(c->ewk_out, n, c->facc[group], acc);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    c->hf_ewk_fresh = true;
+    return PGK_OK;
+}

@@ -451,6 +451,43 @@ static pgk_status ensure_hf_slots(pgk_ctx* c) {
 
 // calforce_hf's per-atom quantities at the current positions (list and the
 // pair kernel's packed coordinates must be current)
+// Per-atom reciprocal terms of the bulk heat flux (pgk_set_hf_kspace) into
+// the intermolecular Coulomb category: each atom's energy, and the (a, z)
+// column of its tensor into region 1 -- ewaldk_hf.F90:212-230 writes
+// virielct_atm(:, :, i, 1), the single region of the bulk builds.
+__global__ void k_hf_kspace_add(const double* __restrict__ pot, const double* __restrict__ vir, int n, int nreg,
+                                double* __restrict__ hf_pot, double* __restrict__ hf_W) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    hf_pot[(size_t)PGK_HF_ELC * n + i] += pot[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        hf_W[((size_t)PGK_HF_ELC * nreg * 3 + a) * n + i] += vir[(size_t)9 * i + a + 6];
+}
+
+pgk_status launch_hf_kspace(pgk_ctx* c) {
+    const int n = c->natom;
+    const double* pot = nullptr;
+    if (c->hf_kspace == PGK_HF_KSPACE_SPME) {
+        pgk_status s = launch_spme_hf_atm(c);
+        if (s) return s;
+        pot = c->hfk_out;
+    } else if (c->hf_kspace == PGK_HF_KSPACE_EWK) {
+        if (!c->hf_ewk_fresh) {       // not yet evaluated at these positions by the force evaluation
+            int nw = 0;
+            pgk_status s = launch_ewk_hf(c, c->hf_kmax, &nw);
+            if (s) return s;
+        }
+        pot = c->ewk_out + 3 * (size_t)n;
+    }
+    c->hf_ewk_fresh = false;
+    if (!pot) return PGK_OK;
+    k_hf_kspace_add<<<(n + 255) / 256, 256, 0, c->st>>>(pot, pot + n, n, c->hfp.nhfregion, c->hf_pot, c->hf_W);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
 pgk_status launch_hf_atm(pgk_ctx* c) {
     if (!c->hf_set || c->hfp.nhfregion < 1) return pgk_fail(c, PGK_E_INVALID, "no heat-flux regions set");
     pgk_status s;
@@ -491,7 +528,8 @@ pgk_status launch_hf_atm(pgk_ctx* c) {
         PGK_LAUNCHED(c);
         PGK_CUDA(c, cudaGetLastError());
     }
-    return launch_bonded_hf(c, h);
+    if ((s = launch_bonded_hf(c, h))) return s;
+    return launch_hf_kspace(c);
 }
 
 // calheatf with the current velocities: one record of nreg * 18 at dst (device)

@@ -463,7 +463,9 @@ static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
 }
 
 pgk_status launch_mklist(pgk_ctx* c) {
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);   // may grow the list arrays
+    // g_alloc_mu is taken only around the (rare) growth of the list arrays, so
+    // the list builds of concurrent replicas (kernels and host round trips)
+    // do not wait for each other
     int n = c->natom;
     // the box may have changed on the device (MTK): read it back
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
@@ -475,6 +477,7 @@ pgk_status launch_mklist(pgk_ctx* c) {
     for (int d = 0; d < 3; ++d) nc[d] = std::max(1, nc[d]);
     long long ncells = (long long)nc[0] * nc[1] * nc[2];
     if (ncells > c->maxcells) {
+        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
         cudaFree(c->cell_cnt); cudaFree(c->cell_start); cudaFree(c->cell_fill);
         c->maxcells = (int)ncells;
         PGK_CUDA(c, cudaMalloc(&c->cell_cnt, sizeof(int) * (ncells + 1)));
@@ -484,7 +487,10 @@ pgk_status launch_mklist(pgk_ctx* c) {
     long long npad_max = (long long)n + 7 * ncells;
     if (npad_max >= (1 << 24)) return pgk_fail(c, PGK_E_UNSUPPORTED, "more than 2^24 padded atom slots");
     pgk_status s;
-    if ((s = ensure_sorted_capacity(c, (int)((npad_max + 7) / 8 * 8)))) return s;
+    if ((npad_max + 7) / 8 * 8 > c->npad_cap) {
+        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
+        if ((s = ensure_sorted_capacity(c, (int)((npad_max + 7) / 8 * 8)))) return s;
+    }
     DynState& h = c->hdyn;
     for (int d = 0; d < 3; ++d) { h.ncell[d] = nc[d]; h.cellsize[d] = h.box[d] / (double)nc[d]; }
     h.list_mode_used = mode;
@@ -538,6 +544,7 @@ pgk_status launch_mklist(pgk_ctx* c) {
             // a quarter of headroom above the longest row, so the rows of
             // later builds (density fluctuations) rarely force another regrowth
             c->ccap = (int)(((long long)cnt[1] * 5 / 4 + 32 + 31) / 32 * 32);
+            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
             if ((s = alloc_rows(c))) return s;
             continue;
         }

@@ -288,7 +288,6 @@ pgk_status morse_setup(pgk_ctx* c, const pgk_system* s) {
 // moldyn*.F90 at mod(step, nstep_bookmor) == 0)
 pgk_status launch_mklist_mor(pgk_ctx* c) {
     if (c->nmor == 0) return PGK_OK;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);   // may grow the rows
     c->mor_valid = false;         // until this build completes
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
     PGK_CUDA(c, cudaStreamSynchronize(c->st));
@@ -314,6 +313,7 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
     if (cell) {
         if (ncells > (1LL << 24)) return pgk_fail(c, PGK_E_UNSUPPORTED, "too many Morse list cells");
         if (ncells > c->mor_maxcells) {
+            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
             cudaFree(c->mor_ccnt); cudaFree(c->mor_cstart); cudaFree(c->mor_cfill);
             c->mor_ccnt = c->mor_cstart = c->mor_cfill = nullptr;
             c->mor_maxcells = (int)ncells;
@@ -335,6 +335,7 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
     }
     for (int attempt = 0; attempt < 3; ++attempt) {
         if (!c->mor_rows) {
+            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
             if (cudaMalloc(&c->mor_rows, sizeof(int) * (size_t)nm * c->mor_cap) != cudaSuccess) {
                 c->mor_rows = nullptr;
                 return pgk_fail(c, PGK_E_NOMEM, "Morse pair list exceeds device memory");
@@ -363,6 +364,7 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
             return pgk_fail(c, PGK_E_CELL_OVERFLOW, "number of atoms in a cell exceeds max (morse)");
         if ((long long)ctr[1] > c->mor_cap) {
             // grow the rows and rebuild (the reference STOPs: "nlistmorall exceed")
+            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
             cudaFree(c->mor_rows);
             c->mor_rows = nullptr;
             c->mor_cap = (int)(((long long)ctr[1] * 5 / 4 + 32 + 31) / 32 * 32);

@@ -88,6 +88,9 @@ struct PairArgs {
     const int* typ_s; const int* perm;
     int ntyp; int nspl; double h, inv_h;
     double rr2, rl2, rmax2, rrcut;
+    // FP32 copies for the mixed kernel, read straight from the parameter
+    // bank inside the pair loop (no registers held for them)
+    float rr2f, rl2f, inv_hf, hf; int nsplm1;
     void* facc; long long* acc;
     long long* fsort; int fstride;     // mixed: forces by sorted slot (SoA, stride fstride)
     // pruned rows (mixed; P null = none): on a prune step (P->do_prune) the
@@ -212,9 +215,6 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
     const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
     const float sy = (float)(dyn->box[1] * (1.0 / 4294967296.0));
     const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
-    const float rr2 = (float)a.rr2, rl2 = (float)a.rl2;
-    const int nsplm1 = a.nspl - 1;
-    const float inv_h = (float)a.inv_h, h = (float)a.h;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
     const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
     const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
@@ -278,7 +278,8 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
                         dz = (float)(pi.z - pj.z) * sz;
                         qq = __int_as_float(pi.w) * __int_as_float(pj.w);
                     }
-                    pair_term<MODE, !FRAME>(dx, dy, dz, qq, sti[warp][ii] + tj, rr2, rl2, inv_h, h, nsplm1, sf, sp,
+                    pair_term<MODE, !FRAME>(dx, dy, dz, qq, sti[warp][ii] + tj, a.rr2f, a.rl2f, a.inv_hf, a.hf,
+                                            a.nsplm1, sf, sp,
                                             slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
                     if (PRUNE) nm |= r2 < rp2 ? 1u << ii : 0u;
                 }
@@ -585,6 +586,8 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
     a.rr2 = c->prm.rrcut * c->prm.rrcut;
     a.rl2 = c->prm.rcut * c->prm.rcut;
     a.rmax2 = a.rr2 > a.rl2 ? a.rr2 : a.rl2;
+    a.rr2f = (float)a.rr2; a.rl2f = (float)a.rl2; a.inv_hf = (float)a.inv_h; a.hf = (float)a.h;
+    a.nsplm1 = c->nspl - 1;
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
     a.fsort = c->fsort; a.fstride = c->npad_cap;

@@ -887,6 +887,202 @@ pgk_status spme_bench(pgk_ctx* c, int which) {
 }
 
 // ============================================================================
+// Per-atom split of the SPME reciprocal energy and virial tensor (bulk heat
+// flux): the SPME form of ewaldkp_hf's per-atom terms (ewaldk_hf.F90:165-230;
+// the reference has them only for standard Ewald).  With S = FFT(Q) and the
+// influence function eterm of scalar_sum (fft_pme.F90:544-690),
+//   pot_atm(i)      = 1/2 q_i sum_g theta_i(g) IFFT(eterm S)(g) - alpha/sqrt(pi) q_i^2
+//   viri_atm(a,b,i) = 1/2 q_i sum_g theta_i(g) IFFT(eterm (delta_ab - vterm h_a h_b) S)(g)
+// FP64 in both precisions (the heat-flux sums are FP64): the charges go into
+// a double grid, one forward transform, k_hf_sgrids writes the seven
+// convolved grids (energy; tensor xx xy xz yy yz zz) as one array of 7 K^3
+// points, whose x and y backward passes run as one K1 x K2 x 7K3 grid and
+// whose z passes run per grid; k_hf_spme_atm gathers the seven real parts
+// with each atom's B-spline weights.
+// Layout: hfk_q double[K3][K2][K1]; hfk_g double2[7][K3][K2][K1];
+// hfk_out double[N] energies | [9N] tensors, (3,3) column-major per atom.
+// ============================================================================
+__global__ void k_hf_sgrids(double2* __restrict__ g, int K1, int K2, int K3, const double* __restrict__ bsp,
+                            double alpha, const DynState* __restrict__ dyn) {
+    const size_t KK = (size_t)K1 * K2 * K3;
+    const double pi = 3.14159265358979323846;
+    const double fac = pi * pi / (alpha * alpha);
+    const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    const double rk2 = dyn->rkcut * dyn->rkcut;
+    int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
+    int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
+    int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
+    for (size_t ind = blockIdx.x * (size_t)blockDim.x + threadIdx.x; ind < KK; ind += (size_t)gridDim.x * blockDim.x) {
+        const int k3 = (int)(ind / ((size_t)K1 * K2));
+        const size_t jnd = ind - (size_t)k3 * K1 * K2;
+        const int k2 = (int)(jnd / K1), k1 = (int)(jnd - (size_t)k2 * K1);
+        const int m1 = k1 < nf1 ? k1 : k1 - K1;
+        const int m2 = k2 < nf2 ? k2 : k2 - K2;
+        const int m3 = k3 < nf3 ? k3 : k3 - K3;
+        const double h[3] = {dyn->boxinv[0] * m1, dyn->boxinv[1] * m2, dyn->boxinv[2] * m3};
+        const double msq = h[0] * h[0] + h[1] * h[1] + h[2] * h[2];
+        double2 es = make_double2(0.0, 0.0);
+        double vterm = 0.0;
+        if (ind != 0 && msq <= rk2) {
+            const double denom = pi * vol * bsp[k1] * bsp[K1 + k2] * bsp[K1 + K2 + k3] * msq;
+            const double eterm = exp(-fac * msq) / denom;
+            vterm = 2.0 * (fac * msq + 1.0) / msq;
+            const double2 S = g[ind];
+            es = make_double2(eterm * S.x, eterm * S.y);
+        }
+        g[ind] = es;
+        const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double f = (ab[c][0] == ab[c][1] ? 1.0 : 0.0) - vterm * h[ab[c][0]] * h[ab[c][1]];
+            g[(size_t)(1 + c) * KK + ind] = make_double2(es.x * f, es.y * f);
+        }
+    }
+}
+
+template <int P>
+__global__ void k_hf_spme_atm(const double* __restrict__ pos, const double* __restrict__ chrg, int n,
+                              const DynState* __restrict__ dyn, int K1, int K2, int K3,
+                              const double2* __restrict__ g, double alpha, double* __restrict__ out) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const size_t KK = (size_t)K1 * K2 * K3;
+    double th[3][P], dth[3][P];
+    int base[3];
+    const int Kd[3] = {K1, K2, K3};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double w;
+        frac_coord(pos[3 * a + d], dyn->boxinv[d], Kd[d], base[d], w);
+        fill_bspline_d<double, P>(w, th[d], dth[d]);
+    }
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int i3 = 0; i3 < P; ++i3) {
+        int k = base[2] - P + 1 + i3;
+        k = k < 0 ? k + K3 : k;
+        for (int i2 = 0; i2 < P; ++i2) {
+            int j = base[1] - P + 1 + i2;
+            j = j < 0 ? j + K2 : j;
+            const size_t row = (size_t)K1 * (j + (size_t)K2 * k);
+            const double w23 = th[1][i2] * th[2][i3];
+#pragma unroll
+            for (int i1 = 0; i1 < P; ++i1) {
+                int i = base[0] - P + 1 + i1;
+                i = i < 0 ? i + K1 : i;
+                const double w = th[0][i1] * w23;
+#pragma unroll
+                for (int c = 0; c < 7; ++c) acc[c] += w * g[(size_t)c * KK + row + i].x;
+            }
+        }
+    }
+    const double q = chrg[a], hq = 0.5 * q;
+    const double self = alpha / sqrt(3.14159265358979323846);
+    out[a] = hq * acc[0] - self * q * q;
+    double* v = out + n + (size_t)9 * a;
+    v[0] = hq * acc[1]; v[1] = hq * acc[2]; v[2] = hq * acc[3];
+    v[3] = v[1];        v[4] = hq * acc[4]; v[5] = hq * acc[5];
+    v[6] = v[2];        v[7] = v[5];        v[8] = hq * acc[6];
+}
+
+// one FP64 pencil pass over an explicit grid (the heat-flux grids)
+template <int AXIS, int SRC>
+static pgk_status hfk_fft_pass(pgk_ctx* c, double2* data, const void* src, int K3e, int sign) {
+    const FftPlan& pl = c->plan[AXIS];
+    FftDev fd;
+    fd.n = pl.n; fd.nstage = pl.nstage;
+    for (int q = 0; q < PGK_MAX_RADIX_STAGES; ++q) fd.radix[q] = pl.radix[q];
+    fd.tw = c->hfk_tw[AXIS];
+    const int K1 = c->K[0], K2 = c->K[1];
+    int P = 8;
+    if (AXIS == 0) P = std::max(1, 1024 / K1);
+    int grid;
+    if (AXIS == 0) grid = (K2 * K3e + P - 1) / P;
+    else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3e;
+    else grid = ((K1 + P - 1) / P) * K2;
+    const size_t sm = ((size_t)2 * P * (pl.n + 1) + pl.n) * sizeof(double2);
+    ConvArgs ca{};
+    PGK_CUDA(c, smem_limit(k_fft<double, AXIS, SRC, 0, false>, sm));
+    k_fft<double, AXIS, SRC, 0, false><<<grid, 256, sm, c->st>>>(data, src, K1, K2, K3e, fd, P, (double)sign, ca,
+                                                                  c->dyn);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+// buffers of the heat-flux SPME split (first use; FP64 twiddles of the
+// context's plans, which hold FP32 twiddles in mixed precision)
+static pgk_status hfk_setup(pgk_ctx* c) {
+    if (c->hfk_g) return PGK_OK;
+    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
+    const size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
+    PGK_CUDA(c, cudaMalloc(&c->hfk_q, KK * sizeof(double)));
+    PGK_CUDA(c, cudaMalloc(&c->hfk_g, 7 * KK * sizeof(double2)));
+    PGK_CUDA(c, cudaMalloc(&c->hfk_out, (size_t)10 * c->natom * sizeof(double)));
+    for (int d = 0; d < 3; ++d) {
+        const int n = c->K[d];
+        std::vector<double2> tw(n);
+        for (int m = 0; m < n; ++m) {
+            const double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
+            tw[m] = make_double2(std::cos(ang), std::sin(ang));
+        }
+        PGK_CUDA(c, cudaMalloc(&c->hfk_tw[d], n * sizeof(double2)));
+        PGK_CUDA(c, cudaMemcpy(c->hfk_tw[d], tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+    return PGK_OK;
+}
+
+template <int P>
+static void hfk_spread_gather(pgk_ctx* c, bool gather) {
+    const int n = c->natom;
+    if (!gather)
+        k_spread<false, P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1], c->K[2],
+                                                               c->hfk_q, nullptr);
+    else
+        k_hf_spme_atm<P><<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->dyn, c->K[0], c->K[1], c->K[2],
+                                                             (const double2*)c->hfk_g, c->prm.alpha, c->hfk_out);
+    PGK_LAUNCHED(c);
+}
+
+// the split at the current positions into c->hfk_out (device)
+pgk_status launch_spme_hf_atm(pgk_ctx* c) {
+    if (!c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
+    pgk_status s;
+    if ((s = hfk_setup(c))) return s;
+    const int K1 = c->K[0], K2 = c->K[1], K3 = c->K[2];
+    const size_t KK = (size_t)K1 * K2 * K3;
+    double2* g = (double2*)c->hfk_g;
+    PGK_CUDA(c, cudaMemsetAsync(c->hfk_q, 0, KK * sizeof(double), c->st));
+    switch (c->order) {
+        case 3: hfk_spread_gather<3>(c, false); break;
+        case 4: hfk_spread_gather<4>(c, false); break;
+        case 5: hfk_spread_gather<5>(c, false); break;
+        case 6: hfk_spread_gather<6>(c, false); break;
+        case 7: hfk_spread_gather<7>(c, false); break;
+        default: hfk_spread_gather<8>(c, false); break;
+    }
+    if ((s = hfk_fft_pass<0, 2>(c, g, c->hfk_q, K3, -1)) || (s = hfk_fft_pass<1, 0>(c, g, nullptr, K3, -1)) ||
+        (s = hfk_fft_pass<2, 0>(c, g, nullptr, K3, -1)))
+        return s;
+    k_hf_sgrids<<<c->nsm * 4, 256, 0, c->st>>>(g, K1, K2, K3, c->bsp, c->prm.alpha, c->dyn);
+    PGK_LAUNCHED(c);
+    for (int q = 0; q < 7; ++q)
+        if ((s = hfk_fft_pass<2, 0>(c, g + (size_t)q * KK, nullptr, K3, +1))) return s;
+    if ((s = hfk_fft_pass<1, 0>(c, g, nullptr, 7 * K3, +1)) || (s = hfk_fft_pass<0, 0>(c, g, nullptr, 7 * K3, +1)))
+        return s;
+    switch (c->order) {
+        case 3: hfk_spread_gather<3>(c, true); break;
+        case 4: hfk_spread_gather<4>(c, true); break;
+        case 5: hfk_spread_gather<5>(c, true); break;
+        case 6: hfk_spread_gather<6>(c, true); break;
+        case 7: hfk_spread_gather<7>(c, true); break;
+        default: hfk_spread_gather<8>(c, true); break;
+    }
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+// ============================================================================
 // Allocation-free SPME reciprocal force: pgk_fft_pme_noalloc.
 //
 // For callers that cannot call cudaMalloc during a run: a host driver or a

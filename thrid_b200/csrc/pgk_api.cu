@@ -103,7 +103,9 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
     const int mask = (c->prm.mts_bond == flag ? 1 : 0) | (c->prm.mts_angl == flag ? 2 : 0) |
                      (c->prm.mts_tors == flag ? 4 : 0) | (c->prm.mts_torsrb == flag ? 8 : 0) |
                      (c->prm.mts_vdw14 == flag && c->prm.mts_elc14 == flag ? 16 : 0) | (pairs ? 32 : 0);
-    const bool spme = c->prm.ifspme && c->prm.mts_ewk == flag;
+    // _HF_BULK_EWK heat-flux step: ewaldkp_hf replaces the SPME term (calforce_hf.F90:1046-1062)
+    const bool ewk_hf = c->hf_ewk_now && c->prm.mts_ewk == flag;
+    const bool spme = c->prm.ifspme && c->prm.mts_ewk == flag && !ewk_hf;
     const bool fork = spme && c->st2 && (pairs || mask);
     if (fork) {
         PGK_CUDA(c, cudaEventRecord(c->ev_fork, c->st));
@@ -127,6 +129,7 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         return PGK_OK;
     }
     if (spme && (s = launch_spme(c, g, ene, vir))) return s;
+    if (ewk_hf && (s = launch_ewk_force(c, g))) return s;
     return launch_intra(c, g, mask, ene || vir, vir && tensor_only);
 }
 
@@ -606,7 +609,8 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec,
                     c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out,
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
-                    c->mor_cstart, c->mor_cfill, c->mor_ctr};
+                    c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
+                    c->hfk_tw[1], c->hfk_tw[2]};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c->st2) { cudaStreamSynchronize(c->st2); cudaStreamDestroy(c->st2); }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -1032,6 +1036,9 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
     }
     for (int is = 1; is <= md->nstep_short; ++is) {
         bool last = is == md->nstep_short;
+        // the standard-Ewald heat-flux option evaluates the reciprocal term of
+        // the last short step of a heat-flux step by ewaldkp_hf
+        c->hf_ewk_now = hfs && last && c->hf_kspace == PGK_HF_KSPACE_EWK;
         RUN(launch_kick_drift(c, (is == 1 ? KD_LONG : 0) | kshort | KD_DRIFT | (rattle ? KD_SAVE : 0)));
         // the box update also refreshes the Ewald k cutoff for the long group's SPME
         if (mtk) RUN(launch_box_update(c, kind, *md, last));
@@ -1041,6 +1048,7 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
             RUN(force_group(c, PGK_MTS_LONG, ene || vir, vir, tens));
             if (hfs) RUN(launch_hf_atm(c));
         }
+        c->hf_ewk_now = false;
         RUN(launch_kick_drift(c, kshort | KD_SHORT_FIRST | (last ? KD_LONG : 0)));
         if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
     }
@@ -1125,6 +1133,30 @@ pgk_status pgk_moldyn_hf(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparam
         PGK_CUDA(c, cudaMemcpy(hf_out, c->hf_rec, sizeof(double) * per * std::min(nr, want), cudaMemcpyDeviceToHost));
     if (nrecords) *nrecords = nr;
     return PGK_OK;
+}
+
+pgk_status pgk_set_hf_kspace(pgk_ctx* c, int32_t mode, int32_t kmax) {
+    if (!c) return PGK_E_INVALID;
+    if (mode == PGK_HF_KSPACE_SPME && !c->prm.ifspme) return pgk_fail(c, PGK_E_INVALID, "ifspme is off");
+    if (mode == PGK_HF_KSPACE_EWK && kmax < 1) return pgk_fail(c, PGK_E_INVALID, "kmax must be at least 1");
+    if (mode != PGK_HF_KSPACE_NONE && mode != PGK_HF_KSPACE_EWK && mode != PGK_HF_KSPACE_SPME)
+        return pgk_fail(c, PGK_E_INVALID, "unknown k-space heat-flux mode");
+    c->hf_kspace = mode;
+    c->hf_kmax = mode == PGK_HF_KSPACE_EWK ? kmax : 0;
+    c->hf_ewk_fresh = false;
+    return PGK_OK;
+}
+
+pgk_status pgk_fft_pme_hf(pgk_ctx* c, double* pot_atm, double* viri_atm) {
+    if (!c) return PGK_E_INVALID;
+    pgk_status s = launch_spme_hf_atm(c);
+    if (s) return s;
+    const size_t n = (size_t)c->natom;
+    if (pot_atm) PGK_CUDA(c, cudaMemcpyAsync(pot_atm, c->hfk_out, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+    if (viri_atm)
+        PGK_CUDA(c, cudaMemcpyAsync(viri_atm, c->hfk_out + n, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    return read_status(c);
 }
 
 pgk_status pgk_calheatf(pgk_ctx* c, double* hf) {

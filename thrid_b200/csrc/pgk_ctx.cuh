@@ -205,6 +205,16 @@ struct pgk_ctx {
     double* ewk_out = nullptr;    // force 3N | energy N | tensor 9N | scalars 11
     size_t ewk_bytes[5] = {0, 0, 0, 0, 0};   // allocated sizes of tab, part, coef, red, out
 
+    // ---- SPME per-atom reciprocal split of the heat flux (k_spme.cu) ----
+    double* hfk_q = nullptr;      // [K^3] double charge grid
+    void* hfk_g = nullptr;        // [7][K^3] double2 convolved grids
+    double* hfk_out = nullptr;    // energies [N] | tensors [9N]
+    void* hfk_tw[3] = {nullptr, nullptr, nullptr};   // FP64 twiddles per axis
+    int hf_kspace = 0;            // PGK_HF_KSPACE_* (pgk_set_hf_kspace)
+    int hf_kmax = 0;              // waves of the standard-Ewald option
+    bool hf_ewk_now = false;      // this force evaluation is the heat-flux step's (standard-Ewald option)
+    bool hf_ewk_fresh = false;    // ewk_out holds ewaldkp_hf at the current positions
+
     // ---- CUDA graphs of captured MD steps (key: driver kind and step flags);
     //      valid for one list build and one set of integrator parameters ----
     struct GraphEntry { cudaGraphExec_t exec; long long launches; long long epoch; };
@@ -263,6 +273,9 @@ pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long l
 pgk_status spme_setup(pgk_ctx* c);
 pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir);
 
+// per-atom split of the SPME reciprocal energy / tensor into c->hfk_out
+pgk_status launch_spme_hf_atm(pgk_ctx* c);
+
 // ---- launchers (k_bonded.cu) ----
 pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>& mol_idx, const std::vector<int>& mol_list);
 pgk_status launch_bonded(pgk_ctx* c, int group, bool ene, bool vir, bool force_all);
@@ -283,6 +296,8 @@ pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p);
 pgk_status launch_hf_atm(pgk_ctx* c);
 pgk_status launch_heatf(pgk_ctx* c, double* dst);
 pgk_status launch_lt_regist(pgk_ctx* c);
+pgk_status launch_hf_kspace(pgk_ctx* c);           // per-atom reciprocal terms (pgk_set_hf_kspace)
+pgk_status launch_ewk_force(pgk_ctx* c, int group); // ewaldkp_hf force in place of SPME (k_ewald.cu)
 pgk_status launch_langevin(pgk_ctx* c, double dt, long long step, bool former);
 pgk_status launch_bonded_hf(pgk_ctx* c, const HfDev& h);   // k_bonded.cu
 

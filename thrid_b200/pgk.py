@@ -85,6 +85,8 @@ def lib():
     L.pgk_langevin_dekin.argtypes = [vp, pd]
     L.pgk_ewaldkp_hf.argtypes = [vp, C.c_int32, pd, pd, pd, C.POINTER(abi.EwkHfStruct)]
     L.pgk_morsep.argtypes = [vp, pd, E, V]
+    L.pgk_set_hf_kspace.argtypes = [vp, C.c_int32, C.c_int32]
+    L.pgk_fft_pme_hf.argtypes = [vp, pd, pd]
     L.pgk_mklist_mor_cell.argtypes = [vp, C.POINTER(C.c_int64)]
     L.pgk_get_morlist.argtypes = [vp, pi, pi, pi, C.c_int64, C.POINTER(C.c_int64), pi]
     _lib = L
@@ -295,6 +297,20 @@ class PgkEngine:
         self._check(self.L.pgk_ewaldkp_hf(self.h, kmax, _p(f), _p(pot), _p(vir), C.byref(o)))
         return dict(force=f, pot_atm=pot, viri_atm=vir, pot_ewk=o.pot_ewk, pot_ewk_cc=o.pot_ewk_cc,
                     pot_virit_coul=np.array(o.pot_virit_coul[:]).reshape(3, 3), nwave=o.nwave)
+
+    def set_hf_kspace(self, mode, kmax=0):
+        """Per-atom reciprocal term of the heat flux: abi.HF_KSPACE_NONE,
+        HF_KSPACE_EWK (ewaldkp_hf on heat-flux steps, waves up to kmax) or
+        HF_KSPACE_SPME (the per-atom split of the SPME term)."""
+        self._check(self.L.pgk_set_hf_kspace(self.h, int(mode), int(kmax)))
+
+    def fft_pme_hf(self):
+        """Per-atom split of fft_pmep: pot_atm (N) with the self term and
+        viri_atm (N,3,3), viri_atm[i, b, a] = tensor(a,b) of atom i."""
+        n = self.sys.natom
+        pot = np.zeros(n); vir = np.zeros((n, 3, 3))
+        self._check(self.L.pgk_fft_pme_hf(self.h, _p(pot), _p(vir)))
+        return pot, vir
 
     def langevin_dekin(self):
         out = np.zeros(abi.LT_MAX_REGIONS)
