@@ -11,9 +11,10 @@
 //                shared memory, two complex products per (atom, wave)
 //   k_ewk_coef   chunk sums in a fixed order, the per-wave coefficients, block
 //                partials of the energy and virial-tensor sums
-//   k_ewk_atom   thread per atom over all waves in the reference's order:
-//                one complex product per wave inside a run of consecutive nz,
-//                force, energy and virial tensor of the atom in registers
+//   k_ewk_atom   thread per atom over a segment of the waves in the
+//                reference's order: one complex product per wave inside a run
+//                of consecutive nz, force, energy and virial tensor of the
+//                atom in registers; k_ewk_atom_sum adds the segments
 //   k_ewk_final  fixed-order sum of the block partials
 // Every sum runs in a fixed order: results are run-to-run identical.
 
@@ -179,10 +180,27 @@ __global__ void __launch_bounds__(EWK_SB) k_ewk_coef(const double2* __restrict__
 // fixed (nx, ny) (nv[w].w = 1 opens a run): the phase is taken from sincospi
 // at the start of a run and advanced by exp(2 pi i z / Lz) inside it, so the
 // atom's state stays in registers.  out: force [3N] | energy [N] | tensor [9N].
+// The wave loop is split into nseg segments (blockIdx.y), so that small
+// systems still fill the SMs; a segment starts its phase from sincospi like a
+// run.  With nseg > 1 each segment writes its 11 sums to seg[(s*11+k)*N + i]
+// and k_ewk_atom_sum adds them in segment order (fixed: run-to-run identical).
+__device__ __forceinline__ void ewk_atom_out(int i, int n, double qi, double pq, double vol, double alpha,
+                                             const double (&r)[11], double* __restrict__ out) {
+    const double pi = 3.14159265358979323846;
+    const double f2 = 2.0 * qi / vol;
+    out[3 * (size_t)i] = f2 * r[0]; out[3 * (size_t)i + 1] = f2 * r[1]; out[3 * (size_t)i + 2] = f2 * r[2];
+    out[3 * (size_t)n + i] = pq * r[3] - alpha / sqrt(pi) * (qi * qi);
+    const double E = r[4], txx = r[5], tyy = r[6], tzz = r[7], txy = r[8], txz = r[9], tyz = r[10];
+    double* v = out + 4 * (size_t)n + 9 * (size_t)i;
+    v[0] = E - txx; v[1] = -txy; v[2] = -txz;
+    v[3] = -txy; v[4] = E - tyy; v[5] = -tyz;
+    v[6] = -txz; v[7] = -tyz; v[8] = E - tzz;
+}
+
 __global__ void __launch_bounds__(128) k_ewk_atom(const double* __restrict__ pos, const double* __restrict__ q,
                                                   int n, const int4* __restrict__ nv, const double* __restrict__ coef,
                                                   int nwave, EwkArgs a, const DynState* __restrict__ dyn,
-                                                  double* __restrict__ out) {
+                                                  double* __restrict__ out, int nseg, double* __restrict__ seg) {
     __shared__ double scf[EWK_CT * EWK_NCOEF];
     __shared__ int4 snv[EWK_CT];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -200,8 +218,11 @@ __global__ void __launch_bounds__(128) k_ewk_atom(const double* __restrict__ pos
     double pc = 1.0, ps_ = 0.0;                                // phase (cos, sin)
     double fx = 0.0, fy = 0.0, fz = 0.0, ps = 0.0, E = 0.0;
     double txx = 0.0, tyy = 0.0, tzz = 0.0, txy = 0.0, txz = 0.0, tyz = 0.0;
-    for (int w0 = 1; w0 < nwave; w0 += EWK_CT) {
-        const int cnt = min(EWK_CT, nwave - w0);
+    const int sgi = blockIdx.y;
+    const int wb = 1 + (int)((long long)(nwave - 1) * sgi / nseg);
+    const int we = 1 + (int)((long long)(nwave - 1) * (sgi + 1) / nseg);
+    for (int w0 = wb; w0 < we; w0 += EWK_CT) {
+        const int cnt = min(EWK_CT, we - w0);
         __syncthreads();
         for (int e = threadIdx.x; e < cnt * EWK_NCOEF; e += blockDim.x) scf[e] = coef[(size_t)w0 * EWK_NCOEF + e];
         for (int e = threadIdx.x; e < cnt; e += blockDim.x) snv[e] = nv[w0 + e];
@@ -209,7 +230,7 @@ __global__ void __launch_bounds__(128) k_ewk_atom(const double* __restrict__ pos
         for (int j = 0; j < cnt; ++j) {
             const double* cf = scf + j * EWK_NCOEF;
             const int4 v = snv[j];
-            if (v.w) {
+            if (v.w || w0 + j == wb) {
                 sincospi(2.0 * ((double)v.x * ux + (double)v.y * uy + (double)v.z * uz), &ps_, &pc);
             } else {
                 const double c2 = pc * zc - ps_ * zs;
@@ -227,13 +248,28 @@ __global__ void __launch_bounds__(128) k_ewk_atom(const double* __restrict__ pos
         }
     }
     if (!live) return;
-    const double f2 = 2.0 * qi / vol;
-    out[3 * (size_t)i] = f2 * fx; out[3 * (size_t)i + 1] = f2 * fy; out[3 * (size_t)i + 2] = f2 * fz;
-    out[3 * (size_t)n + i] = pq * ps - a.alpha / sqrt(pi) * (qi * qi);
-    double* v = out + 4 * (size_t)n + 9 * (size_t)i;
-    v[0] = E - txx; v[1] = -txy; v[2] = -txz;
-    v[3] = -txy; v[4] = E - tyy; v[5] = -tyz;
-    v[6] = -txz; v[7] = -tyz; v[8] = E - tzz;
+    const double r[11] = {fx, fy, fz, ps, E, txx, tyy, tzz, txy, txz, tyz};
+    if (nseg == 1) {
+        ewk_atom_out(i, n, qi, pq, vol, a.alpha, r, out);
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 11; ++k) seg[((size_t)sgi * 11 + k) * n + i] = r[k];
+}
+
+__global__ void k_ewk_atom_sum(const double* __restrict__ q, int n, int nseg, const double* __restrict__ seg,
+                               EwkArgs a, const DynState* __restrict__ dyn, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double r[11];
+#pragma unroll
+    for (int k = 0; k < 11; ++k) r[k] = 0.0;
+    for (int sg = 0; sg < nseg; ++sg)
+#pragma unroll
+        for (int k = 0; k < 11; ++k) r[k] += seg[((size_t)sg * 11 + k) * n + i];
+    const double vol = dyn->box[0] * dyn->box[1] * dyn->box[2];
+    const double qi = q[i], pq = 0.5 / 3.14159265358979323846 / vol * qi;
+    ewk_atom_out(i, n, qi, pq, vol, a.alpha, r, out);
 }
 
 // scalars: pot_ewk, pot_ewk_cc, pot_virit_coul[a + 3b]
@@ -329,6 +365,20 @@ pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave_out, int only) {
         (s = ewk_buf(c, (void**)&c->ewk_red, c->ewk_bytes[3], sizeof(double) * 8 * (size_t)ncb)) ||
         (s = ewk_buf(c, (void**)&c->ewk_out, c->ewk_bytes[4], sizeof(double) * (13 * (size_t)n + 11))))
         return s;
+    // wave segments of the per-atom kernel: about four blocks of 128 per SM
+    const int nab = (n + 127) / 128;
+    const int nseg = std::max(1, std::min(16, std::min((4 * c->nsm + nab - 1) / nab, nwave - 1)));
+    if (nseg > 1 && (s = ewk_buf(c, (void**)&c->ewk_seg, c->ewk_bytes[5], sizeof(double) * 11 * (size_t)nseg * n)))
+        return s;
+    auto atom_kernels = [&]() {
+        k_ewk_atom<<<dim3(nab, nseg), 128, 0, c->st>>>(c->pos, c->chrg, n, c->ewk_nv, c->ewk_coef, nwave, a, c->dyn,
+                                                      c->ewk_out, nseg, c->ewk_seg);
+        PGK_LAUNCHED(c);
+        if (nseg > 1) {
+            k_ewk_atom_sum<<<(n + 255) / 256, 256, 0, c->st>>>(c->chrg, n, nseg, c->ewk_seg, a, c->dyn, c->ewk_out);
+            PGK_LAUNCHED(c);
+        }
+    };
 
     const size_t sm_sfac = sizeof(double2) * EWK_TA * nrp + sizeof(double) * EWK_TA;
     PGK_CUDA(c, smem_limit(k_ewk_sfac, sm_sfac));
@@ -338,9 +388,8 @@ pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave_out, int only) {
             k_ewk_sfac<<<dim3(nkb, nchunk), EWK_SB, sm_sfac, c->st>>>(c->ewk_tab, c->chrg, n, chunk, c->ewk_nv, nwave,
                                                                         a, c->ewk_part);
         else
-            k_ewk_atom<<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->ewk_nv, c->ewk_coef, nwave, a,
-                                                            c->dyn, c->ewk_out);
-        PGK_LAUNCHED(c);
+            atom_kernels();
+        if (only == 1) PGK_LAUNCHED(c);
         PGK_CUDA(c, cudaGetLastError());
         if (nwave_out) *nwave_out = nwave;
         return PGK_OK;
@@ -353,9 +402,7 @@ pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave_out, int only) {
     PGK_LAUNCHED(c);
     k_ewk_coef<<<ncb, EWK_SB, 0, c->st>>>(c->ewk_part, nchunk, c->ewk_nv, nwave, a, c->dyn, c->ewk_coef, c->ewk_red);
     PGK_LAUNCHED(c);
-    k_ewk_atom<<<(n + 127) / 128, 128, 0, c->st>>>(c->pos, c->chrg, n, c->ewk_nv, c->ewk_coef, nwave, a, c->dyn,
-                                                    c->ewk_out);
-    PGK_LAUNCHED(c);
+    atom_kernels();
     k_ewk_final<<<1, 32, 0, c->st>>>(c->ewk_red, ncb, c->ewk_out + 13 * (size_t)n);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());

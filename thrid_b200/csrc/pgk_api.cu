@@ -607,7 +607,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->blk_ip, c->blk_incp, c->blk_inc,
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec,
-                    c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out,
+                    c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out, c->ewk_seg,
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
                     c->hfk_tw[1], c->hfk_tw[2]};

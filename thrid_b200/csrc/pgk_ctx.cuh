@@ -203,7 +203,8 @@ struct pgk_ctx {
     double* ewk_coef = nullptr;   // [nwave][EWK_NCOEF] per-wave coefficients
     double* ewk_red = nullptr;    // [wave blocks][8] energy / tensor partials
     double* ewk_out = nullptr;    // force 3N | energy N | tensor 9N | scalars 11
-    size_t ewk_bytes[5] = {0, 0, 0, 0, 0};   // allocated sizes of tab, part, coef, red, out
+    double* ewk_seg = nullptr;    // [nseg][11][N] per-atom sums of the wave segments
+    size_t ewk_bytes[6] = {0, 0, 0, 0, 0, 0};   // allocated sizes of tab, part, coef, red, out, seg
 
     // ---- SPME per-atom reciprocal split of the heat flux (k_spme.cu) ----
     double* hfk_q = nullptr;      // [K^3] double charge grid
