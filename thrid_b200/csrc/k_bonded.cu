@@ -764,7 +764,7 @@ static void reorder(std::vector<V>& v, const std::vector<int>& order) {
 template <typename T>
 static pgk_status up(pgk_ctx* c, T** dst, const std::vector<T>& v) {
     if (v.empty()) { *dst = nullptr; return PGK_OK; }
-    PGK_CUDA(c, cudaMalloc(dst, v.size() * sizeof(T)));
+    PGK_CUDA(c, pgk_dmalloc(c, dst, v.size() * sizeof(T)));
     PGK_CUDA(c, cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
     return PGK_OK;
 }

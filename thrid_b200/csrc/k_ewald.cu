@@ -311,11 +311,10 @@ static int ewk_waves(int kmax, int ny0, int nz0, std::vector<int4>& nv) {
 
 static pgk_status ewk_buf(pgk_ctx* c, void** p, size_t& have, size_t want) {
     if (have >= want) return PGK_OK;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-    if (*p) cudaFree(*p);
+    if (*p) pgk_dfree(c, *p);
     *p = nullptr;
     have = 0;
-    PGK_CUDA(c, cudaMalloc(p, want));
+    PGK_CUDA(c, pgk_dmalloc(c, p, want));
     have = want;
     return PGK_OK;
 }
@@ -331,13 +330,13 @@ pgk_status launch_ewk_hf(pgk_ctx* c, int kmax, int* nwave_out, int only) {
         std::vector<int4> nv;
         const int nw = ewk_waves(kmax, ny0, nz0, nv);
         {
-            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-            if (c->ewk_nv) cudaFree(c->ewk_nv);
+            if (c->ewk_nv) pgk_dfree(c, c->ewk_nv);
             c->ewk_nv = nullptr;
             c->ewk_kmax = 0;
-            PGK_CUDA(c, cudaMalloc(&c->ewk_nv, sizeof(int4) * nw));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->ewk_nv, sizeof(int4) * nw));
         }
-        PGK_CUDA(c, cudaMemcpy(c->ewk_nv, nv.data(), sizeof(int4) * nw, cudaMemcpyHostToDevice));
+        PGK_CUDA(c, cudaMemcpyAsync(c->ewk_nv, nv.data(), sizeof(int4) * nw, cudaMemcpyHostToDevice, c->st));
+        PGK_CUDA(c, cudaStreamSynchronize(c->st));
         c->ewk_nwave = nw;
         c->ewk_nmax[0] = kmax; c->ewk_nmax[1] = kmax * ny0; c->ewk_nmax[2] = kmax * nz0;
         c->ewk_kmax = kmax;

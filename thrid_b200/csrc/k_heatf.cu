@@ -371,9 +371,9 @@ static LtDev lt_dev(const pgk_ctx* c) {
 
 template <typename T>
 static pgk_status upload_vec(pgk_ctx* c, T** dst, const std::vector<T>& v) {
-    if (*dst) { cudaFree(*dst); *dst = nullptr; }
+    if (*dst) { pgk_dfree(c, *dst); *dst = nullptr; }
     if (v.empty()) return PGK_OK;
-    PGK_CUDA(c, cudaMalloc(dst, sizeof(T) * v.size()));
+    PGK_CUDA(c, pgk_dmalloc(c, dst, sizeof(T) * v.size()));
     PGK_CUDA(c, cudaMemcpyAsync(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->st));
     return PGK_OK;
 }
@@ -412,9 +412,9 @@ pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p) {
         (s = upload_vec(c, &c->lt_mole, ltm)))
         return s;
     auto realloc = [&](double** b, size_t cnt) -> pgk_status {
-        if (*b) { cudaFree(*b); *b = nullptr; }
+        if (*b) { pgk_dfree(c, *b); *b = nullptr; }
         if (cnt == 0) return PGK_OK;
-        if (cudaMalloc(b, cnt * sizeof(double)) != cudaSuccess) return pgk_fail(c, PGK_E_NOMEM, "heat-flux arrays");
+        if (pgk_dmalloc(c, b, cnt * sizeof(double)) != cudaSuccess) return pgk_fail(c, PGK_E_NOMEM, "heat-flux arrays");
         PGK_CUDA(c, cudaMemsetAsync(*b, 0, cnt * sizeof(double), c->st));
         return PGK_OK;
     };
@@ -428,9 +428,9 @@ pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p) {
         (s = realloc(&c->lt_frand, (size_t)3 * n)) || (s = realloc(&c->lt_dekin, PGK_LT_MAX_REGIONS)))
         return s;
     c->hf_rec_cap = 1;
-    if (c->lt_reg) cudaFree(c->lt_reg);
+    if (c->lt_reg) pgk_dfree(c, c->lt_reg);
     c->lt_reg = nullptr;
-    PGK_CUDA(c, cudaMalloc(&c->lt_reg, sizeof(int) * n));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->lt_reg, sizeof(int) * n));
     PGK_CUDA(c, cudaMemsetAsync(c->lt_reg, 0xff, sizeof(int) * n, c->st));
     c->hf_set = true;
     if (c->hfp.nlangeregion > 0 && (s = launch_lt_regist(c))) return s;
@@ -440,11 +440,10 @@ pgk_status hf_setup(pgk_ctx* c, const pgk_hfparams* p) {
 
 static pgk_status ensure_hf_slots(pgk_ctx* c) {
     if (c->hf_slots_cap >= c->npad_cap) return PGK_OK;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-    cudaFree(c->hf_zs); cudaFree(c->hf_ms);
+    pgk_dfree(c, c->hf_zs); pgk_dfree(c, c->hf_ms);
     c->hf_zs = nullptr; c->hf_ms = nullptr;
-    PGK_CUDA(c, cudaMalloc(&c->hf_zs, sizeof(double) * c->npad_cap));
-    PGK_CUDA(c, cudaMalloc(&c->hf_ms, sizeof(int) * c->npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->hf_zs, sizeof(double) * c->npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->hf_ms, sizeof(int) * c->npad_cap));
     c->hf_slots_cap = c->npad_cap;
     return PGK_OK;
 }

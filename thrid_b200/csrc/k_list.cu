@@ -420,14 +420,14 @@ static int list_mode_for(const pgk_ctx* c, const double* box, int* nc) {
 // (re)allocate the sorted/padded arrays for up to npad_cap slots
 // cluster rows (book and pruned) for npad_cap/8 clusters of ccap entries
 static pgk_status alloc_rows(pgk_ctx* c) {
-    cudaFree(c->clist); cudaFree(c->plist);
+    pgk_dfree(c, c->clist); pgk_dfree(c, c->plist);
     c->clist = nullptr; c->plist = nullptr;
     const size_t bytes = sizeof(int) * (size_t)(c->npad_cap / 8) * c->ccap;
-    if (cudaMalloc(&c->clist, bytes) != cudaSuccess) {
+    if (pgk_dmalloc(c, &c->clist, bytes) != cudaSuccess) {
         c->clist = nullptr;
         return pgk_fail(c, PGK_E_NOMEM, "cluster pair list exceeds device memory");
     }
-    if (c->prune_buffer > 0.f && cudaMalloc(&c->plist, bytes) != cudaSuccess) {
+    if (c->prune_buffer > 0.f && pgk_dmalloc(c, &c->plist, bytes) != cudaSuccess) {
         c->plist = nullptr;
         return pgk_fail(c, PGK_E_NOMEM, "pruned pair list exceeds device memory");
     }
@@ -436,26 +436,26 @@ static pgk_status alloc_rows(pgk_ctx* c) {
 
 static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
     if (npad_cap <= c->npad_cap) return PGK_OK;
-    cudaFree(c->perm); cudaFree(c->pos_s); cudaFree(c->typ_s); cudaFree(c->xq); cudaFree(c->xq64);
-    cudaFree(c->ccnt); cudaFree(c->clist); cudaFree(c->fsort); cudaFree(c->plist); cudaFree(c->pcnt);
-    cudaFree(c->xq_prune);
+    pgk_dfree(c, c->perm); pgk_dfree(c, c->pos_s); pgk_dfree(c, c->typ_s); pgk_dfree(c, c->xq); pgk_dfree(c, c->xq64);
+    pgk_dfree(c, c->ccnt); pgk_dfree(c, c->clist); pgk_dfree(c, c->fsort); pgk_dfree(c, c->plist); pgk_dfree(c, c->pcnt);
+    pgk_dfree(c, c->xq_prune);
     c->perm = nullptr; c->pos_s = nullptr; c->typ_s = nullptr; c->xq = nullptr; c->xq64 = nullptr;
     c->ccnt = nullptr; c->clist = nullptr; c->fsort = nullptr; c->plist = nullptr; c->pcnt = nullptr;
     c->xq_prune = nullptr;
     int ncl = npad_cap / 8;
-    PGK_CUDA(c, cudaMalloc(&c->perm, sizeof(int) * npad_cap));
-    PGK_CUDA(c, cudaMalloc(&c->pos_s, sizeof(double) * 3 * npad_cap));
-    PGK_CUDA(c, cudaMalloc(&c->typ_s, sizeof(int) * npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->perm, sizeof(int) * npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->pos_s, sizeof(double) * 3 * npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->typ_s, sizeof(int) * npad_cap));
     if (c->mixed()) {
-        PGK_CUDA(c, cudaMalloc(&c->xq, sizeof(int4) * npad_cap));
-        PGK_CUDA(c, cudaMalloc(&c->fsort, sizeof(long long) * 3 * (size_t)npad_cap));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->xq, sizeof(int4) * npad_cap));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->fsort, sizeof(long long) * 3 * (size_t)npad_cap));
         PGK_CUDA(c, cudaMemsetAsync(c->fsort, 0, sizeof(long long) * 3 * (size_t)npad_cap, c->st));
     }
-    else PGK_CUDA(c, cudaMalloc(&c->xq64, sizeof(double4) * npad_cap));
-    PGK_CUDA(c, cudaMalloc(&c->ccnt, sizeof(int) * ncl));
+    else PGK_CUDA(c, pgk_dmalloc(c, &c->xq64, sizeof(double4) * npad_cap));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->ccnt, sizeof(int) * ncl));
     if (c->prune_buffer > 0.f) {
-        PGK_CUDA(c, cudaMalloc(&c->pcnt, sizeof(int) * ncl));
-        PGK_CUDA(c, cudaMalloc(&c->xq_prune, sizeof(int4) * npad_cap));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->pcnt, sizeof(int) * ncl));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->xq_prune, sizeof(int4) * npad_cap));
         PGK_CUDA(c, cudaMemsetAsync(c->xq_prune, 0, sizeof(int4) * npad_cap, c->st));
     }
     c->npad_cap = npad_cap;
@@ -463,9 +463,6 @@ static pgk_status ensure_sorted_capacity(pgk_ctx* c, int npad_cap) {
 }
 
 pgk_status launch_mklist(pgk_ctx* c) {
-    // g_alloc_mu is taken only around the (rare) growth of the list arrays, so
-    // the list builds of concurrent replicas (kernels and host round trips)
-    // do not wait for each other
     int n = c->natom;
     // the box may have changed on the device (MTK): read it back
     PGK_CUDA(c, cudaMemcpyAsync(&c->hdyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToHost, c->st));
@@ -477,18 +474,16 @@ pgk_status launch_mklist(pgk_ctx* c) {
     for (int d = 0; d < 3; ++d) nc[d] = std::max(1, nc[d]);
     long long ncells = (long long)nc[0] * nc[1] * nc[2];
     if (ncells > c->maxcells) {
-        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-        cudaFree(c->cell_cnt); cudaFree(c->cell_start); cudaFree(c->cell_fill);
+        pgk_dfree(c, c->cell_cnt); pgk_dfree(c, c->cell_start); pgk_dfree(c, c->cell_fill);
         c->maxcells = (int)ncells;
-        PGK_CUDA(c, cudaMalloc(&c->cell_cnt, sizeof(int) * (ncells + 1)));
-        PGK_CUDA(c, cudaMalloc(&c->cell_start, sizeof(int) * (ncells + 1)));
-        PGK_CUDA(c, cudaMalloc(&c->cell_fill, sizeof(int) * (ncells + 1)));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->cell_cnt, sizeof(int) * (ncells + 1)));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->cell_start, sizeof(int) * (ncells + 1)));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->cell_fill, sizeof(int) * (ncells + 1)));
     }
     long long npad_max = (long long)n + 7 * ncells;
     if (npad_max >= (1 << 24)) return pgk_fail(c, PGK_E_UNSUPPORTED, "more than 2^24 padded atom slots");
     pgk_status s;
     if ((npad_max + 7) / 8 * 8 > c->npad_cap) {
-        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
         if ((s = ensure_sorted_capacity(c, (int)((npad_max + 7) / 8 * 8)))) return s;
     }
     DynState& h = c->hdyn;
@@ -540,11 +535,10 @@ pgk_status launch_mklist(pgk_ctx* c) {
         if (st & ST_LIST_OVERFLOW) {
             // grow the cluster rows and rebuild (the reference STOPs here)
             unsigned zero = 0;
-            PGK_CUDA(c, cudaMemcpy(c->status, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+            PGK_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(zero), c->st));
             // a quarter of headroom above the longest row, so the rows of
             // later builds (density fluctuations) rarely force another regrowth
             c->ccap = (int)(((long long)cnt[1] * 5 / 4 + 32 + 31) / 32 * 32);
-            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
             if ((s = alloc_rows(c))) return s;
             continue;
         }

@@ -267,14 +267,14 @@ pgk_status morse_setup(pgk_ctx* c, const pgk_system* s) {
     if (atoms.empty()) return PGK_OK;
     if (c->prm.rcutmor <= 0.0) return pgk_fail(c, PGK_E_INVALID, "rcutmor must be positive with Morse pairs");
     c->nmor = (int)atoms.size();
-    PGK_CUDA(c, cudaMalloc(&c->mor_par, par.size() * sizeof(double4)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_par, par.size() * sizeof(double4)));
     PGK_CUDA(c, cudaMemcpy(c->mor_par, par.data(), par.size() * sizeof(double4), cudaMemcpyHostToDevice));
-    PGK_CUDA(c, cudaMalloc(&c->mor_atoms, atoms.size() * sizeof(int)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_atoms, atoms.size() * sizeof(int)));
     PGK_CUDA(c, cudaMemcpy(c->mor_atoms, atoms.data(), atoms.size() * sizeof(int), cudaMemcpyHostToDevice));
-    PGK_CUDA(c, cudaMalloc(&c->mor_cnt, atoms.size() * sizeof(int)));
-    PGK_CUDA(c, cudaMalloc(&c->mor_cell, atoms.size() * sizeof(int)));
-    PGK_CUDA(c, cudaMalloc(&c->mor_csort, atoms.size() * sizeof(int)));
-    PGK_CUDA(c, cudaMalloc(&c->mor_ctr, 2 * sizeof(unsigned long long)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_cnt, atoms.size() * sizeof(int)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_cell, atoms.size() * sizeof(int)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_csort, atoms.size() * sizeof(int)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->mor_ctr, 2 * sizeof(unsigned long long)));
     // rows: the partners of a Morse atom inside rcut_bookmor at the Morse
     // atoms' mean density, half of them stored (j > i), regrown on overflow
     const double vol = c->prm.xcel * c->prm.ycel * c->prm.zcel;
@@ -313,13 +313,12 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
     if (cell) {
         if (ncells > (1LL << 24)) return pgk_fail(c, PGK_E_UNSUPPORTED, "too many Morse list cells");
         if (ncells > c->mor_maxcells) {
-            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-            cudaFree(c->mor_ccnt); cudaFree(c->mor_cstart); cudaFree(c->mor_cfill);
+            pgk_dfree(c, c->mor_ccnt); pgk_dfree(c, c->mor_cstart); pgk_dfree(c, c->mor_cfill);
             c->mor_ccnt = c->mor_cstart = c->mor_cfill = nullptr;
             c->mor_maxcells = (int)ncells;
-            PGK_CUDA(c, cudaMalloc(&c->mor_ccnt, sizeof(int) * (ncells + 1)));
-            PGK_CUDA(c, cudaMalloc(&c->mor_cstart, sizeof(int) * (ncells + 1)));
-            PGK_CUDA(c, cudaMalloc(&c->mor_cfill, sizeof(int) * (ncells + 1)));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->mor_ccnt, sizeof(int) * (ncells + 1)));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->mor_cstart, sizeof(int) * (ncells + 1)));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->mor_cfill, sizeof(int) * (ncells + 1)));
         }
         double cs[3];
         for (int d = 0; d < 3; ++d) cs[d] = box[d] / (double)nc[d];
@@ -335,8 +334,7 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
     }
     for (int attempt = 0; attempt < 3; ++attempt) {
         if (!c->mor_rows) {
-            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-            if (cudaMalloc(&c->mor_rows, sizeof(int) * (size_t)nm * c->mor_cap) != cudaSuccess) {
+            if (pgk_dmalloc(c, &c->mor_rows, sizeof(int) * (size_t)nm * c->mor_cap) != cudaSuccess) {
                 c->mor_rows = nullptr;
                 return pgk_fail(c, PGK_E_NOMEM, "Morse pair list exceeds device memory");
             }
@@ -364,8 +362,7 @@ pgk_status launch_mklist_mor(pgk_ctx* c) {
             return pgk_fail(c, PGK_E_CELL_OVERFLOW, "number of atoms in a cell exceeds max (morse)");
         if ((long long)ctr[1] > c->mor_cap) {
             // grow the rows and rebuild (the reference STOPs: "nlistmorall exceed")
-            std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-            cudaFree(c->mor_rows);
+            pgk_dfree(c, c->mor_rows);
             c->mor_rows = nullptr;
             c->mor_cap = (int)(((long long)ctr[1] * 5 / 4 + 32 + 31) / 32 * 32);
             continue;

@@ -711,9 +711,9 @@ pgk_status spme_setup(pgk_ctx* c) {
         if (!factor(c->K[d], c->plan[d]))
             return pgk_fail(c, PGK_E_UNSUPPORTED, "SPME grid sizes must factor into 2, 3, 5");
     size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
-    PGK_CUDA(c, cudaMalloc(&c->qacc, KK * 8));
-    PGK_CUDA(c, cudaMalloc(&c->qc, KK * (c->mixed() ? sizeof(float2) : sizeof(double2))));
-    PGK_CUDA(c, cudaMalloc(&c->qr, KK * (c->mixed() ? sizeof(float) : sizeof(double))));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->qacc, KK * 8));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->qc, KK * (c->mixed() ? sizeof(float2) : sizeof(double2))));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->qr, KK * (c->mixed() ? sizeof(float) : sizeof(double))));
     PGK_CUDA(c, cudaMemset(c->qr, 0, KK * (c->mixed() ? sizeof(float) : sizeof(double))));
     // B-spline moduli (DFTMOD, fft_pme_init.F90:263-289)
     double arr[16], darr[16];
@@ -736,7 +736,7 @@ pgk_status spme_setup(pgk_ctx* c) {
         for (int k = 1; k < n - 1; ++k) if (mod[k] < 1.0e-7) mod[k] = 0.5 * (mod[k - 1] + mod[k + 1]);
         bsp.insert(bsp.end(), mod.begin(), mod.end());
     }
-    PGK_CUDA(c, cudaMalloc(&c->bsp, bsp.size() * sizeof(double)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->bsp, bsp.size() * sizeof(double)));
     PGK_CUDA(c, cudaMemcpy(c->bsp, bsp.data(), bsp.size() * sizeof(double), cudaMemcpyHostToDevice));
     for (int d = 0; d < 3; ++d) {
         if (!factor(c->K[d], c->plan[d]))
@@ -748,7 +748,7 @@ pgk_status spme_setup(pgk_ctx* c) {
                 double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
                 tw[m] = make_float2((float)std::cos(ang), (float)std::sin(ang));
             }
-            PGK_CUDA(c, cudaMalloc(&c->plan[d].tw, n * sizeof(float2)));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->plan[d].tw, n * sizeof(float2)));
             PGK_CUDA(c, cudaMemcpy(c->plan[d].tw, tw.data(), n * sizeof(float2), cudaMemcpyHostToDevice));
         } else {
             std::vector<double2> tw(n);
@@ -756,7 +756,7 @@ pgk_status spme_setup(pgk_ctx* c) {
                 double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
                 tw[m] = make_double2(std::cos(ang), std::sin(ang));
             }
-            PGK_CUDA(c, cudaMalloc(&c->plan[d].tw, n * sizeof(double2)));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->plan[d].tw, n * sizeof(double2)));
             PGK_CUDA(c, cudaMemcpy(c->plan[d].tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
         }
     }
@@ -1014,11 +1014,10 @@ static pgk_status hfk_fft_pass(pgk_ctx* c, double2* data, const void* src, int K
 // context's plans, which hold FP32 twiddles in mixed precision)
 static pgk_status hfk_setup(pgk_ctx* c) {
     if (c->hfk_g) return PGK_OK;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     const size_t KK = (size_t)c->K[0] * c->K[1] * c->K[2];
-    PGK_CUDA(c, cudaMalloc(&c->hfk_q, KK * sizeof(double)));
-    PGK_CUDA(c, cudaMalloc(&c->hfk_g, 7 * KK * sizeof(double2)));
-    PGK_CUDA(c, cudaMalloc(&c->hfk_out, (size_t)10 * c->natom * sizeof(double)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->hfk_q, KK * sizeof(double)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->hfk_g, 7 * KK * sizeof(double2)));
+    PGK_CUDA(c, pgk_dmalloc(c, &c->hfk_out, (size_t)10 * c->natom * sizeof(double)));
     for (int d = 0; d < 3; ++d) {
         const int n = c->K[d];
         std::vector<double2> tw(n);
@@ -1026,8 +1025,9 @@ static pgk_status hfk_setup(pgk_ctx* c) {
             const double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)n;
             tw[m] = make_double2(std::cos(ang), std::sin(ang));
         }
-        PGK_CUDA(c, cudaMalloc(&c->hfk_tw[d], n * sizeof(double2)));
-        PGK_CUDA(c, cudaMemcpy(c->hfk_tw[d], tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->hfk_tw[d], n * sizeof(double2)));
+        PGK_CUDA(c, cudaMemcpyAsync(c->hfk_tw[d], tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+        PGK_CUDA(c, cudaStreamSynchronize(c->st));
     }
     return PGK_OK;
 }

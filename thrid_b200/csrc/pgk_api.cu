@@ -12,7 +12,42 @@
 
 #include "pgk_ctx.cuh"
 
-std::shared_mutex g_alloc_mu;   // see pgk_ctx.cuh
+// the device's memory pool of the contexts (see pgk_ctx.cuh): created on
+// first use per device, release threshold at its maximum (memory stays cached)
+static cudaMemPool_t device_pool() {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    pools[dev] = pool;
+    return pool;
+}
+
+cudaError_t pgk_dmalloc(pgk_ctx* c, void** p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes > 0 ? bytes : 1, c->pool, c->st);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    return cudaStreamSynchronize(c->st);
+}
+
+cudaError_t pgk_dfree(pgk_ctx* c, void* p) {
+    if (!p) return cudaSuccess;
+    return cudaFreeAsync(p, c->st);
+}
 
 cudaError_t smem_limit(const void* kernel, size_t bytes) {
     static std::mutex mu;
@@ -66,7 +101,7 @@ double rkcut_host(const double* box, int n1, int n2, int n3) {   // erf_corr_cut
 template <typename T>
 pgk_status upload(pgk_ctx* c, T** dst, const std::vector<T>& v) {
     if (v.empty()) { *dst = nullptr; return PGK_OK; }
-    PGK_CUDA(c, cudaMalloc(dst, v.size() * sizeof(T)));
+    PGK_CUDA(c, pgk_dmalloc(c, dst, v.size() * sizeof(T)));
     PGK_CUDA(c, cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
     return PGK_OK;
 }
@@ -77,7 +112,7 @@ pgk_status read_status(pgk_ctx* c) {
     PGK_CUDA(c, cudaStreamSynchronize(c->st));
     if (!st) return PGK_OK;
     unsigned z = 0;
-    PGK_CUDA(c, cudaMemcpy(c->status, &z, sizeof(z), cudaMemcpyHostToDevice));
+    PGK_CUDA(c, cudaMemsetAsync(c->status, 0, sizeof(z), c->st));
     if (st & ST_RATTLE_NOCONV) return pgk_fail(c, PGK_E_RATTLE_NOCONV, "ERROR: RATTLE(C) failed to converge within MAXITER = 300");
     if (st & ST_RATTLEV_NOCONV) return pgk_fail(c, PGK_E_RATTLEV_NOCONV, "ERROR: RATTLE(V) failed to converge within MAXITER = 300");
     if (st & ST_BOX_TOO_SMALL) return pgk_fail(c, PGK_E_BOX_TOO_SMALL, "Error: rcut is over half cell length");
@@ -190,7 +225,7 @@ pgk_status read_acc(pgk_ctx* c, int gmask, pgk_energies* e, pgk_virials* v, bool
 
 pgk_status force_to_host(pgk_ctx* c, int g, double* force, bool add) {
     int n3 = 3 * c->natom;
-    if (!c->fout) PGK_CUDA(c, cudaMalloc(&c->fout, sizeof(double) * n3));
+    if (!c->fout) PGK_CUDA(c, pgk_dmalloc(c, &c->fout, sizeof(double) * n3));
     pgk_status s = launch_copy_force(c, g, c->fout);
     if (s) return s;
     c->hbuf.resize(n3);
@@ -242,7 +277,6 @@ extern "C" {
 
 pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     if (!s || !p || !out) return PGK_E_INVALID;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     *out = nullptr;
     int n = s->natom;
     if (n >= (1 << 25)) return PGK_E_INVALID;   // sort key packs the atom index in 25 bits
@@ -274,6 +308,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return PGK_E_CUDA; }
+    c->pool = device_pool();
+    if (!c->pool) { cudaStreamDestroy(c->st); delete c; return PGK_E_CUDA; }
     if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
@@ -303,17 +339,17 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     c->netchrgsq = q * q;
     c->pot_ewc = -1.0 / std::sqrt(std::acos(-1.0)) * p->alpha * q2;   // fft_pme_init.F90:147-156
     size_t n3 = (size_t)3 * n;
-    if (cudaMalloc(&c->pos, n3 * 8) || cudaMalloc(&c->vel, n3 * 8) || cudaMalloc(&c->pos_old, n3 * 8) ||
-        cudaMalloc(&c->facc[0], n3 * 8) || cudaMalloc(&c->facc[1], n3 * 8) ||
-        cudaMalloc(&c->acc, sizeof(long long) * 2 * NACC) || cudaMalloc(&c->dyn, sizeof(DynState)) ||
-        cudaMalloc(&c->chain, sizeof(ChainDev)) || cudaMalloc(&c->status, sizeof(unsigned))) {
+    if (pgk_dmalloc(c, &c->pos, n3 * 8) || pgk_dmalloc(c, &c->vel, n3 * 8) || pgk_dmalloc(c, &c->pos_old, n3 * 8) ||
+        pgk_dmalloc(c, &c->facc[0], n3 * 8) || pgk_dmalloc(c, &c->facc[1], n3 * 8) ||
+        pgk_dmalloc(c, &c->acc, sizeof(long long) * 2 * NACC) || pgk_dmalloc(c, &c->dyn, sizeof(DynState)) ||
+        pgk_dmalloc(c, &c->chain, sizeof(ChainDev)) || pgk_dmalloc(c, &c->status, sizeof(unsigned))) {
         pgk_free(c);
         return PGK_E_NOMEM;
     }
-    cudaMemset(c->vel, 0, n3 * 8);
-    cudaMemset(c->pos, 0, n3 * 8);
-    cudaMemset(c->status, 0, sizeof(unsigned));
-    cudaMemset(c->acc, 0, sizeof(long long) * 2 * NACC);
+    cudaMemsetAsync(c->vel, 0, n3 * 8, c->st);
+    cudaMemsetAsync(c->pos, 0, n3 * 8, c->st);
+    cudaMemsetAsync(c->status, 0, sizeof(unsigned), c->st);
+    cudaMemsetAsync(c->acc, 0, sizeof(long long) * 2 * NACC, c->st);
     // ---- LJ tables ----
     c->ntyp = s->ntyp;
     std::vector<double2> lj64(s->ntyp * s->ntyp);
@@ -555,14 +591,15 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
             const double buf = pb ? atof(pb) : 1.0;
             const double rmax = std::max(p->rcut, p->rrcut);
             c->prune_buffer = (buf > 0.0 && rmax + buf < p->rcut_book) ? (float)buf : 0.f;
-            if (cudaMalloc(&c->prune, sizeof(PruneDev)) || cudaMemset(c->prune, 0, sizeof(PruneDev))) {
+            if (pgk_dmalloc(c, &c->prune, sizeof(PruneDev)) ||
+                cudaMemsetAsync(c->prune, 0, sizeof(PruneDev), c->st)) {
                 pgk_free(c);
                 return PGK_E_NOMEM;
             }
         }
-        if (cudaMalloc(&c->iperm, n * sizeof(int)) || cudaMalloc(&c->cell_of, n * sizeof(int)) ||
-            cudaMalloc(&c->subkey, n * sizeof(int)) || cudaMalloc(&c->counters, 8 * sizeof(unsigned long long)) ||
-            cudaMalloc(&c->hasup, std::max(n, 1))) {
+        if (pgk_dmalloc(c, &c->iperm, n * sizeof(int)) || pgk_dmalloc(c, &c->cell_of, n * sizeof(int)) ||
+            pgk_dmalloc(c, &c->subkey, n * sizeof(int)) || pgk_dmalloc(c, &c->counters, 8 * sizeof(unsigned long long)) ||
+            pgk_dmalloc(c, &c->hasup, std::max(n, 1))) {
             pgk_free(c);
             return PGK_E_NOMEM;
         }
@@ -587,15 +624,21 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         if (cudaMemcpy(c->chain, &ch, sizeof(ch), cudaMemcpyHostToDevice)) { pgk_free(c); return PGK_E_CUDA; }
     }
 #undef TRY
-    if (cudaDeviceSynchronize() != cudaSuccess) { pgk_free(c); return PGK_E_CUDA; }
+    // the set-up copies ran on the legacy stream (synchronous host arrays),
+    // the memsets on the context's: both are complete after these waits
+    if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
+        pgk_free(c);
+        return PGK_E_CUDA;
+    }
     *out = c;
     return PGK_OK;
 }
 
 pgk_status pgk_free(pgk_ctx* c) {
     if (!c) return PGK_OK;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
+    // the context's own streams only: other contexts keep running
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st2) cudaStreamSynchronize(c->st2);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
                     c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list, c->exs_rng,
@@ -611,8 +654,9 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
                     c->hfk_tw[1], c->hfk_tw[2]};
-    for (void* b : bufs) if (b) cudaFree(b);
-    if (c->st2) { cudaStreamSynchronize(c->st2); cudaStreamDestroy(c->st2); }
+    for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st2) cudaStreamDestroy(c->st2);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->st) cudaStreamDestroy(c->st);
@@ -934,11 +978,9 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                 // place (same topology, new launch parameters), else instantiated
                 cudaGraph_t g = nullptr;
                 const long long l0 = c->launches;
-                std::shared_lock<std::shared_mutex> capture_lock(g_alloc_mu);
                 PGK_CUDA(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
                 pgk_status bs = step_body(step, ene, vir, tens, false, false);
                 cudaError_t ce = cudaStreamEndCapture(c->st, &g);
-                capture_lock.unlock();
                 if (bs != PGK_OK || ce != cudaSuccess) {
                     // nothing of the step ran during the failed capture: run it
                     // eagerly and stop capturing on this context
@@ -1071,13 +1113,12 @@ pgk_status pgk_moldyn_mtk(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdpara
 
 pgk_status pgk_set_output(pgk_ctx* c, int64_t cap) {
     if (!c || cap < 0) return PGK_E_INVALID;
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
     PGK_CUDA(c, cudaStreamSynchronize(c->st));
-    if (c->out_rec) { cudaFree(c->out_rec); c->out_rec = nullptr; }
+    if (c->out_rec) { pgk_dfree(c, c->out_rec); c->out_rec = nullptr; }
     c->out_cap = 0;
     c->out_n = 0;
     if (cap > 0) {
-        if (cudaMalloc(&c->out_rec, sizeof(double) * PGK_OUT_NCOL * (size_t)cap) != cudaSuccess) {
+        if (pgk_dmalloc(c, &c->out_rec, sizeof(double) * PGK_OUT_NCOL * (size_t)cap) != cudaSuccess) {
             c->out_rec = nullptr;
             return pgk_fail(c, PGK_E_NOMEM, "output record buffer");
         }
@@ -1102,8 +1143,10 @@ pgk_status pgk_set_hf(pgk_ctx* c, const pgk_hfparams* hf) {
     if (!c || !hf) return PGK_E_INVALID;
     if (c->nmor)   // the per-atom Morse shares of morsep_hf (morse_hf.F90) are not built on the device
         return pgk_fail(c, PGK_E_UNSUPPORTED, "heat flux with Morse pairs (morsep_hf) is not built");
-    std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-    return hf_setup(c, hf);
+    pgk_status s = hf_setup(c, hf);
+    if (s) return s;
+    PGK_CUDA(c, cudaStreamSynchronize(cudaStreamLegacy));   // its table copies (synchronous host arrays)
+    return PGK_OK;
 }
 
 pgk_status pgk_moldyn_hf(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparams* md, pgk_energies* e,
@@ -1117,10 +1160,9 @@ pgk_status pgk_moldyn_hf(pgk_ctx* c, int64_t ini, int64_t end, const pgk_mdparam
         for (int64_t st = std::max<int64_t>(ini, 1); st <= end; ++st) expect += (hfi == 1 || st % hfi == 1) ? 1 : 0;
     long long want = hf_out ? std::min<long long>(expect, cap_records) : 0;
     if (per > 0 && want > c->hf_rec_cap) {
-        std::unique_lock<std::shared_mutex> alloc_lock(g_alloc_mu);
-        cudaFree(c->hf_rec);
+        pgk_dfree(c, c->hf_rec);
         c->hf_rec = nullptr;
-        PGK_CUDA(c, cudaMalloc(&c->hf_rec, sizeof(double) * per * want));
+        PGK_CUDA(c, pgk_dmalloc(c, &c->hf_rec, sizeof(double) * per * want));
         c->hf_rec_cap = want;
     }
     long long cap_save = c->hf_rec_cap;
@@ -1190,7 +1232,7 @@ pgk_status pgk_langevin_dekin(pgk_ctx* c, double* out) {
     double h[PGK_LT_MAX_REGIONS];
     PGK_CUDA(c, cudaMemcpy(h, c->lt_dekin, sizeof(h), cudaMemcpyDeviceToHost));
     for (int r = 0; r < c->hfp.nlangeregion; ++r) out[r] = h[r];
-    PGK_CUDA(c, cudaMemset(c->lt_dekin, 0, sizeof(h)));
+    PGK_CUDA(c, cudaMemsetAsync(c->lt_dekin, 0, sizeof(h), c->st));
     return PGK_OK;
 }
 }

@@ -41,6 +41,7 @@ struct pgk_ctx {
     // integer or FP64 atomics on the shared force and energy accumulators)
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaMemPool_t pool = nullptr; // the device's memory pool (pgk_dmalloc)
     std::string err;
     long long launches = 0;
     int nsm = 148;
@@ -228,11 +229,18 @@ struct pgk_ctx {
     std::vector<double> hbuf;
 };
 
-// Device allocation and stream capture across host threads (replica server):
-// cudaMalloc/cudaFree may synchronise the device, which would invalidate a
-// capture running on another thread, so allocating code takes this mutex
-// exclusively and captures take it shared.
-extern std::shared_mutex g_alloc_mu;
+// Device memory of a context is stream-ordered: allocations come from one
+// memory pool per device (cached: nothing is returned to the driver between
+// contexts) on the context's stream, followed by a wait on that stream so
+// the memory is usable by any stream and by synchronous copies at once;
+// frees are ordered on the context's stream.  Neither synchronises the
+// device (cudaMalloc / cudaFree would), so the contexts of concurrent
+// replicas start, grow their lists and end without stalling each other's
+// streams or invalidating a graph capture in flight on another thread.
+cudaError_t pgk_dmalloc(pgk_ctx* c, void** p, size_t bytes);
+cudaError_t pgk_dfree(pgk_ctx* c, void* p);
+template <typename T>
+inline cudaError_t pgk_dmalloc(pgk_ctx* c, T** p, size_t bytes) { return pgk_dmalloc(c, (void**)p, bytes); }
 
 // Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The
 // limit is a process-wide property of the kernel, shared by every context
