@@ -738,6 +738,7 @@ def main():
         print(json.dumps(run_ewk(args)))
         return
     if args.serve:
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")   # before CUDA starts (see thrid_b200/serve.py)
         print(json.dumps(run_serve(args)))
         return
     rank, world, local = dist_init()

@@ -182,9 +182,8 @@ __device__ __forceinline__ void pair_term(const float dx, const float dy, const 
 // warps take every 8th cluster of it, so they read overlapping j ranges at
 // the same time (shared L1 lines).  Per-lane energy/virial sums stay in FP32
 // registers across the block's clusters and are reduced once per block.
-// PRUNE: the instance that runs on prune steps (reads the book rows, writes
-// the pruned ones); the other instance runs on all other steps.  Both are
-// launched; each returns at once when the step is not its kind.
+// PRUNE: the body of prune steps (reads the book rows, writes the pruned
+// ones); the other body runs on all other steps (one launch, see k_pair_mixed).
 // FRAME (boxes wide enough that the cluster atoms and every listed j, each
 // taken as its minimum image from cluster atom 0, never wrap against each
 // other): positions enter as FP32 offsets from cluster atom 0, so a pair's
@@ -192,11 +191,9 @@ __device__ __forceinline__ void pair_term(const float dx, const float dy, const 
 // as sum_a F_a (x) x_a over the cluster atoms and the entries' j (equal to
 // sum over pairs f (x) r, with the lever arms of the cluster frame).
 template <int MODE, bool PRUNE, bool FRAME>
-__global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
-                                                       const float2* __restrict__ lj_g,
-                                                       const float4* __restrict__ spl_g,
-                                                       const DynState* __restrict__ dyn) {
-    if (PRUNE ? (a.P == nullptr || !a.P->do_prune) : (a.P != nullptr && a.P->do_prune)) return;   // other step kind
+__device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, const PairArgs& a,
+                                                const float2* __restrict__ lj_g, const float4* __restrict__ spl_g,
+                                                const DynState* __restrict__ dyn) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     extern __shared__ float4 sm[];
     float4* sf = sm;                        // force table  (spline 0)
@@ -333,6 +330,17 @@ __global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ 
         const int idx[2] = {A_VDW, A_ELC};
         block_acc<2>(v, a.acc, idx, false);
     }
+}
+
+// One launch per evaluation: the step kind that k_prune_decide wrote on the
+// device (prune step or not) selects the body, block-uniformly.
+template <int MODE, bool FRAME>
+__global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
+                                                       const float2* __restrict__ lj_g,
+                                                       const float4* __restrict__ spl_g,
+                                                       const DynState* __restrict__ dyn) {
+    if (a.P != nullptr && a.P->do_prune) pair_mixed_body<MODE, true, FRAME>(xq, a, lj_g, spl_g, dyn);
+    else pair_mixed_body<MODE, false, FRAME>(xq, a, lj_g, spl_g, dyn);
 }
 
 // ---- pair kernel, FP64 (parity path) ---------------------------------------
@@ -525,14 +533,9 @@ template <int MODE, bool FRAME>
 static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a, int blocks) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-    smem_limit(k_pair_mixed<MODE, false, FRAME>, sm);
-    k_pair_mixed<MODE, false, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+    smem_limit(k_pair_mixed<MODE, FRAME>, sm);
+    k_pair_mixed<MODE, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
     PGK_LAUNCHED(c);
-    if (a.P) {
-        smem_limit(k_pair_mixed<MODE, true, FRAME>, sm);
-        k_pair_mixed<MODE, true, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
-        PGK_LAUNCHED(c);
-    }
 }
 
 // The cluster frame is exact when no cluster atom or listed j, taken as its

@@ -11,8 +11,16 @@ budget allow; each replica runs in its own context and CUDA stream.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
+
+# Every replica context drives two CUDA streams; with the default eight
+# hardware work queues per device, more than four concurrent replicas would
+# share queues and serialise each other's kernels.  The setting only takes
+# effect before the process initialises CUDA, so it is made on import unless
+# the caller chose a value.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 from thrid_b200 import abi
 from thrid_b200.pgk import PgkError, lib as _pgk_lib
