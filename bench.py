@@ -199,6 +199,8 @@ def run_ours(args, rank, world, local_rank):
         "energies_last": {k: ene[k] for k in ("pot_tot", "pot_vdw", "pot_elc", "pot_ewk")} if ene else None,
     }
     out["clocks"] = clk.summary()
+    from thrid_b200.pgk import tuning_table
+    out["autotune"] = tuning_table().splitlines()
     if rank == 0 and not args.no_configs:
         out["other_configs"] = other_configs(args)
     if rank == 0 and not args.no_cpu_baseline:
@@ -571,6 +573,7 @@ def run_serve(args):
     import torch
     from thrid_b200 import abi
     from thrid_b200 import systems as S
+    from thrid_b200.pgk import tuning_table
     from thrid_b200.serve import ReplicaServer
     torch.cuda.set_device(0)
     rng = np.random.default_rng(args.serve_seed)
@@ -617,6 +620,7 @@ def run_serve(args):
                           "latency_p99_s": float(np.percentile(seq_lat, 99))},
         "single_large_system": single,
         "fraction_of_single_large_system": (work / span) / single["value"],
+        "autotune": tuning_table().splitlines(),
         "data": "synthetic (seeded lattices)",
     }
 

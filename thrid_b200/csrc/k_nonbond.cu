@@ -466,11 +466,11 @@ __global__ void k_prune_decide(PruneDev* __restrict__ P, const DynState* __restr
 // in shared memory, as the book rows), so the pair kernel's loops over the
 // mask bits stay uniform across a warp.  One warp per row; no-op unless a
 // prune was decided.
-__global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, const int* __restrict__ pcnt, int ccap,
-                                                    int ncl, const PruneDev* __restrict__ P) {
+__device__ __forceinline__ void prune_sort_rows(int blk, int* __restrict__ plist, const int* __restrict__ pcnt,
+                                                int ccap, int ncl, const PruneDev* __restrict__ P) {
     if (!P->do_prune) return;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int cl = (blk * blockDim.x + threadIdx.x) >> 5;
     if (cl >= ncl) return;
     extern __shared__ int prow_raw[];
     int* buf = prow_raw + (size_t)wib * (ccap + 256);
@@ -515,9 +515,9 @@ __global__ void __launch_bounds__(128) k_prune_sort(int* __restrict__ plist, con
 
 // sorted-slot pair forces -> the group accumulator, leaving the slot buffer
 // zero for the next call
-__global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __restrict__ perm, int npad,
-                         long long* __restrict__ facc) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void unsort_slots(int blk, long long* __restrict__ fsort, int fst,
+                                             const int* __restrict__ perm, int npad, long long* __restrict__ facc) {
+    const int s = blk * blockDim.x + threadIdx.x;
     if (s >= npad) return;
     const int i = perm[s];
     const long long vx = fsort[s], vy = fsort[s + fst], vz = fsort[s + 2 * (size_t)fst];
@@ -527,6 +527,19 @@ __global__ void k_unsort(long long* __restrict__ fsort, int fst, const int* __re
         atomicAdd((unsigned long long*)facc + 3 * (size_t)i + 2, (unsigned long long)vz);
     }
     if (vx | vy | vz) { fsort[s] = 0; fsort[s + fst] = 0; fsort[s + 2 * (size_t)fst] = 0; }
+}
+
+// The two finishing steps of a mixed pair evaluation in one launch: blocks
+// [0, nbu) move the sorted-slot forces into the accumulator, the blocks after
+// them regroup the pruned rows by mask on a prune step (128 threads a block,
+// four rows per block; they return at once on the other steps).
+__global__ void __launch_bounds__(128) k_pair_finish(long long* __restrict__ fsort, int fst,
+                                                     const int* __restrict__ perm, int npad,
+                                                     long long* __restrict__ facc, int nbu, int* __restrict__ plist,
+                                                     const int* __restrict__ pcnt, int ccap, int ncl,
+                                                     const PruneDev* __restrict__ P) {
+    if ((int)blockIdx.x < nbu) unsort_slots(blockIdx.x, fsort, fst, perm, npad, facc);
+    else prune_sort_rows(blockIdx.x - nbu, plist, pcnt, ccap, ncl, P);
 }
 
 template <int MODE, bool FRAME>
@@ -562,18 +575,20 @@ static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
 // it beside the SPME chain: the accumulator adds are atomic).
 pgk_status launch_pair_finish(pgk_ctx* c, int group) {
     if (c->ncl <= 0 || !c->mixed()) return PGK_OK;
-    k_unsort<<<(c->npad + 255) / 256, 256, 0, c->st>>>(c->fsort, c->npad_cap, c->perm, c->npad,
-                                                       (long long*)c->facc[group]);
-    PGK_LAUNCHED(c);
+    const int nbu = (c->npad + 127) / 128;
+    int nbs = 0;
+    size_t sort_sm = 0;
     if (c->prune_buffer > 0.f) {
-        const size_t sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each
-        if (sort_sm <= 160 * 1024 && smem_limit(k_prune_sort, sort_sm) == cudaSuccess) {
-            const long long threads = (long long)c->ncl * 32;
-            k_prune_sort<<<(unsigned)((threads + 127) / 128), 128, sort_sm, c->st>>>(c->plist, c->pcnt, c->ccap,
-                                                                                     c->ncl, c->prune);
-            PGK_LAUNCHED(c);
-        }
+        sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each
+        if (sort_sm <= 160 * 1024 && smem_limit(k_pair_finish, sort_sm) == cudaSuccess)
+            nbs = (int)(((long long)c->ncl * 32 + 127) / 128);
+        else
+            sort_sm = 0;
     }
+    k_pair_finish<<<nbu + nbs, 128, sort_sm, c->st>>>(c->fsort, c->npad_cap, c->perm, c->npad,
+                                                      (long long*)c->facc[group], nbu, c->plist, c->pcnt, c->ccap,
+                                                      c->ncl, c->prune);
+    PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }

@@ -13,6 +13,13 @@
 //  k_gather   grad_sum: force from the convolved grid, p^3 loads per atom.
 // Complex grid: float2 (mixed) or double2 (FP64), x fastest, K1*K2*K3.
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
 #include <vector>
 
 #include "pgk_ctx.cuh"
@@ -782,6 +789,8 @@ static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) 
     int K1 = c->K[0], K2 = c->K[1], K3 = c->K[2];
     int P = sizeof(T) == 4 ? 16 : 8;
     if (AXIS == 0) P = std::max(1, (sizeof(T) == 4 ? 2048 : 1024) / K1);
+    const int tuned = CONV ? c->fft_p[3] : c->fft_p[AXIS];   // pencils per block chosen by spme_autotune
+    if (tuned > 0) P = tuned;
     int grid;
     if (AXIS == 0) grid = (K2 * K3 + P - 1) / P;
     else if (AXIS == 1) grid = ((K1 + P - 1) / P) * K3;
@@ -829,6 +838,113 @@ static pgk_status fft_convolve(pgk_ctx* c, long long* acc, int want) {
     if ((s = fft_pass<T, 2, 0, true>(c, -1, &ca))) return s;
     if ((s = fft_pass<T, 1, 0>(c, +1))) return s;
     return fft_pass<T, 0, 3>(c, +1);
+}
+
+// ---- autotuner of the FFT launch shapes ----------------------------------------
+// Pencils per block of each axis pass (and of the z pass with the influence
+// function) decide how many blocks a pass has: many pencils per block suit
+// large grids, few suit the small grids of small replicas, whose SPME chain
+// is latency-bound.  Every pencil is transformed on its own, so the results
+// do not depend on the choice.  Each candidate (powers of two that fit the
+// shared memory) is timed with CUDA events on the context's stream over a
+// few launches on the context's grid; the fastest is kept per (grid shape,
+// precision) for the whole process and listed by pgk_tuning_table.
+struct TuneKey {
+    int k1, k2, k3, fp32;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(k1, k2, k3, fp32) < std::tie(o.k1, o.k2, o.k3, o.fp32);
+    }
+};
+struct TuneVal { int p[4]; float us[4]; };
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal> g_tune;
+
+template <typename T, int AXIS, int SRC, bool CONV>
+static pgk_status tune_axis(pgk_ctx* c, int slot, int& best, float& best_us) {
+    typedef typename C2<T>::t T2;
+    const int n = c->K[AXIS];
+    const int npen = AXIS == 0 ? c->K[1] * c->K[2] : c->K[0];
+    cudaEvent_t e0, e1;
+    PGK_CUDA(c, cudaEventCreate(&e0));
+    PGK_CUDA(c, cudaEventCreate(&e1));
+    ConvArgs ca{};
+    ca.bsp = c->bsp; ca.alpha = c->prm.alpha; ca.netchrgsq = c->netchrgsq; ca.corr = c->prm.ifnetqcorrp;
+    ca.acc = c->acc; ca.want = 0;
+    best = 0; best_us = 1e30f;
+    for (int P = 1; P <= 64 && P <= npen; P *= 2) {
+        if (((size_t)2 * P * (n + 1) + n) * sizeof(T2) > 160 * 1024) break;
+        c->fft_p[slot] = P;
+        pgk_status s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr);    // warm-up (and smem limit)
+        if (s) return s;
+        PGK_CUDA(c, cudaEventRecord(e0, c->st));
+        for (int r = 0; r < 3; ++r)
+            if ((s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr))) return s;
+        PGK_CUDA(c, cudaEventRecord(e1, c->st));
+        PGK_CUDA(c, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PGK_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+        const float us = ms * 1e3f / 3.f;
+        if (us < best_us) { best_us = us; best = P; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->fft_p[slot] = best;
+    return PGK_OK;
+}
+
+template <typename T>
+static pgk_status autotune_fft(pgk_ctx* c, TuneVal& v) {
+    pgk_status s;
+    if ((s = tune_axis<T, 0, 0, false>(c, 0, v.p[0], v.us[0])) || (s = tune_axis<T, 1, 0, false>(c, 1, v.p[1], v.us[1])) ||
+        (s = tune_axis<T, 2, 0, false>(c, 2, v.p[2], v.us[2])) || (s = tune_axis<T, 2, 0, true>(c, 3, v.p[3], v.us[3])))
+        return s;
+    return PGK_OK;
+}
+
+// launch shapes of this context's SPME passes: the process-wide choice for
+// its grid shape, measured now if there is none yet (PGK_AUTOTUNE=0: the
+// fixed defaults).  Runs at context set-up, outside any stream capture.
+pgk_status spme_autotune(pgk_ctx* c) {
+    for (int q = 0; q < 4; ++q) c->fft_p[q] = 0;
+    const char* env = getenv("PGK_AUTOTUNE");
+    if ((env && atoi(env) == 0) || !c->prm.ifspme) return PGK_OK;
+    const TuneKey key{c->K[0], c->K[1], c->K[2], c->mixed() ? 1 : 0};
+    std::lock_guard<std::mutex> lk(g_tune_mu);     // contexts of one grid shape share one measurement
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) {
+        TuneVal v{};
+        PGK_CUDA(c, cudaMemsetAsync(c->qc, 0, (size_t)c->K[0] * c->K[1] * c->K[2] * (c->mixed() ? 8 : 16), c->st));
+        pgk_status s = c->mixed() ? autotune_fft<float>(c, v) : autotune_fft<double>(c, v);
+        if (s) return s;
+        PGK_CUDA(c, cudaMemsetAsync(c->acc, 0, sizeof(long long) * 2 * NACC, c->st));
+        PGK_CUDA(c, cudaStreamSynchronize(c->st));
+        it = g_tune.emplace(key, v).first;
+    }
+    for (int q = 0; q < 4; ++q) c->fft_p[q] = it->second.p[q];
+    return PGK_OK;
+}
+
+extern "C" int64_t pgk_tuning_table(char* buf, int64_t cap) {
+    std::string t;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (auto& kv : g_tune) {
+            char line[256];
+            snprintf(line, sizeof(line),
+                     "spme %dx%dx%d %s: pencils per block x %d (%.1f us) y %d (%.1f us) z %d (%.1f us) "
+                     "z+influence %d (%.1f us)\n",
+                     kv.first.k1, kv.first.k2, kv.first.k3, kv.first.fp32 ? "fp32" : "fp64", kv.second.p[0],
+                     kv.second.us[0], kv.second.p[1], kv.second.us[1], kv.second.p[2], kv.second.us[2],
+                     kv.second.p[3], kv.second.us[3]);
+            t += line;
+        }
+    }
+    if (buf && cap > 0) {
+        const size_t m = std::min((size_t)cap - 1, t.size());
+        memcpy(buf, t.data(), m);
+        buf[m] = 0;
+    }
+    return (int64_t)t.size() + 1;
 }
 
 template <bool MIXED, int P>

@@ -623,13 +623,14 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         ch.xboxh[0] = p->xcel; ch.xboxh[1] = p->ycel; ch.xboxh[2] = p->zcel;
         if (cudaMemcpy(c->chain, &ch, sizeof(ch), cudaMemcpyHostToDevice)) { pgk_free(c); return PGK_E_CUDA; }
     }
-#undef TRY
     // the set-up copies ran on the legacy stream (synchronous host arrays),
     // the memsets on the context's: both are complete after these waits
     if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess || cudaStreamSynchronize(c->st) != cudaSuccess) {
         pgk_free(c);
         return PGK_E_CUDA;
     }
+    TRY(spme_autotune(c));
+#undef TRY
     *out = c;
     return PGK_OK;
 }
@@ -947,6 +948,8 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
     };
     pgk_status s;
 #define RUN(x) do { if ((s = (x)) != PGK_OK) return s; } while (0)
+    // the kick / drift coefficients of NVE-type steps depend on md alone
+    if (kind == 0 || kind == 3) RUN(launch_coeffs(c, 0, *md, 0));
     for (int64_t step = ini; step <= end; ++step) {
         bool out = md->outinterval > 0 ? (step % md->outinterval == 0) : (step == end);
         const bool rec = out && c->out_cap > 0;         // device-side output record
@@ -1073,9 +1076,9 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
     if (kind == 1 || kind == 2) {
         if (!ke_ready) RUN(launch_kinetic(c, 0));
         RUN(launch_chain_coeffs(c, chain_kind, hfdrv ? 0 : kind, *md));
-    } else {
-        RUN(launch_coeffs(c, hfdrv ? 0 : kind, *md, 0));
     }
+    // NVE and heat-flux steps: constant kick / drift coefficients, written
+    // once per stage by run_md
     for (int is = 1; is <= md->nstep_short; ++is) {
         bool last = is == md->nstep_short;
         // the standard-Ewald heat-flux option evaluates the reciprocal term of

@@ -152,6 +152,7 @@ struct pgk_ctx {
     void* qr = nullptr;           // real part after the backward transform (float / double), read by the gather
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
+    int fft_p[4] = {0, 0, 0, 0};  // pencils per block of the x, y, z and z+influence passes (0: default)
 
     // ---- Morse pairs (k_morse.cu): own list (radius rcut_bookmor) and kernel ----
     int nmor = 0;                 // Morse atoms (0: no Morse pairs or Morse switched off)
@@ -280,6 +281,7 @@ pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long l
 
 // ---- launchers (k_spme.cu) ----
 pgk_status spme_setup(pgk_ctx* c);
+pgk_status spme_autotune(pgk_ctx* c);   // FFT launch shapes (after the dynamic state is set)
 pgk_status launch_spme(pgk_ctx* c, int group, bool ene, bool vir);
 
 // per-atom split of the SPME reciprocal energy / tensor into c->hfk_out

@@ -97,6 +97,18 @@ def _p(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def tuning_table():
+    """Launch shapes the engine's autotuner chose in this process (one line
+    per SPME grid shape and precision), as text."""
+    L = lib()
+    L.pgk_tuning_table.restype = C.c_int64
+    L.pgk_tuning_table.argtypes = [C.c_char_p, C.c_int64]
+    n = int(L.pgk_tuning_table(None, 0))
+    buf = C.create_string_buffer(max(n, 1))
+    L.pgk_tuning_table(buf, n)
+    return buf.value.decode()
+
+
 class PgkEngine:
     """One device context (the md_global state of one system)."""
 
