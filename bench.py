@@ -580,17 +580,23 @@ def run_serve(args):
     reps = [serve_replica(rng, k, abi.PREC_MIXED) for k in range(args.serve_replicas)]
     md = abi.md_struct(S.fs_to_reduced(1.0), ifrattle=1, outinterval=0)
     work = sum(s.natom for s in reps) * args.serve_steps
+    # --serve-hf: the heat flux of the whole box every step, streamed back as
+    # J_z(t) records for Green-Kubo (one region spanning the box, no thermostat)
+    kind = 3 if args.serve_hf else 0
+    hfs = [dict(regions=[(0.0, float(s.box[2]))], heatfinterval=1) if args.serve_hf else None for s in reps]
 
     def run(slots, arrivals):
         srv = ReplicaServer(max_slots=slots)
         t0 = time.perf_counter()
         ids = []
-        for s, ta in zip(reps, arrivals):
+        for s, h, ta in zip(reps, hfs, arrivals):
             dt = ta - (time.perf_counter() - t0)
             if dt > 0:
                 time.sleep(dt)
-            ids.append(srv.submit(s, md, kind=0, nsteps=args.serve_steps))
+            ids.append(srv.submit(s, md, kind=kind, nsteps=args.serve_steps, hf=h))
         res = [srv.result(i) for i in ids]
+        if args.serve_hf:
+            assert all(r[4].shape[0] == args.serve_steps and np.isfinite(r[4]).all() for r in res)
         srv.close()
         t = np.array([r[5] for r in res])
         lat = t[:, 2] - t[:, 0]
@@ -599,7 +605,7 @@ def run_serve(args):
 
     # warm-up (library load, first context)
     srv = ReplicaServer(max_slots=1)
-    srv.result(srv.submit(reps[0], md, kind=0, nsteps=5))
+    srv.result(srv.submit(reps[0], md, kind=kind, nsteps=5, hf=hfs[0]))
     srv.close()
     seq_lat, seq_span = run(1, [0.0] * len(reps))               # one at a time, all queued at t=0
     mean_service = seq_span / len(reps)
@@ -610,7 +616,8 @@ def run_serve(args):
     return {
         "metric": "replica serving: aggregate atom-steps/s and p50/p99 latency (mixed precision)",
         "value": work / span, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
-        "config": {"workload": "poisson_replicas_water_or_propanol_1.5k-30k_nve", "replicas": len(reps),
+        "config": {"workload": "poisson_replicas_water_or_propanol_1.5k-30k_nve" + ("_jz_every_step" if args.serve_hf
+                                                                                        else ""), "replicas": len(reps),
                    "steps_per_replica": args.serve_steps, "slots": args.serve_slots,
                    "offered_load": args.serve_load, "natom_total": int(sum(s.natom for s in reps))},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -734,6 +741,7 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-load", type=float, default=4.0, help="arrival rate / one-at-a-time service rate")
     ap.add_argument("--serve-seed", type=int, default=2025)
+    ap.add_argument("--serve-hf", action="store_true", help="replicas stream the box heat flux J_z(t) every step")
     ap.add_argument("--ewk-hf", type=int, default=0, metavar="KMAX",
                     help="ewaldkp_hf benchmark at this kmax instead of the main line")
     args = ap.parse_args()
