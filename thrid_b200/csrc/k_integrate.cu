@@ -516,6 +516,7 @@ struct RattleStage {
     double x[3 * RATTLE_WSPAN], v[3 * RATTLE_WSPAN], o[3 * RATTLE_WSPAN], im[RATTLE_WSPAN];
     int2 ij[32 * RATTLE_WCON];
     double d2[32 * RATTLE_WCON];
+    double rc[32 * RATTLE_WCON];   // per constraint: 1/d^2 (positions), 1/(d^2 (1/m_i + 1/m_j)) (velocities)
 };
 
 template <bool POS>
@@ -559,9 +560,20 @@ __global__ void __launch_bounds__(32 * RATTLE_WARPS) k_rattle_warp(double* __res
         S.d2[lane * RATTLE_WCON + q] = dij * dij;
     }
     __syncwarp();
+    // The sweeps' convergence tests and the velocity correction divide by
+    // per-constraint constants: their reciprocals are formed once here, so
+    // the serial sweep chain holds one FP64 division per correction instead
+    // of two per constraint (the tests differ from the reference's quotient
+    // by at most an ulp of eps)
+    for (int q = 0; q < ncon; ++q) {
+        const int2 p = S.ij[lane * RATTLE_WCON + q];
+        const double d2 = S.d2[lane * RATTLE_WCON + q];
+        S.rc[lane * RATTLE_WCON + q] = POS ? 1.0 / d2 : 1.0 / (d2 * (S.im[p.x] + S.im[p.y]));
+    }
     double* X = S.x; double* V = S.v; const double* O = S.o; const double* IM = S.im;
     const int2* C = S.ij + lane * RATTLE_WCON;
     const double* D2 = S.d2 + lane * RATTLE_WCON;
+    const double* RC = S.rc + lane * RATTLE_WCON;
     bool finished = false;
     if (POS) {
         double rvi[3] = {1.0, 1.0, 1.0};
@@ -573,7 +585,7 @@ __global__ void __launch_bounds__(32 * RATTLE_WARPS) k_rattle_warp(double* __res
                 const double d2 = D2[q];
                 double R0 = X[3 * ib] - X[3 * jb], R1 = X[3 * ib + 1] - X[3 * jb + 1], R2 = X[3 * ib + 2] - X[3 * jb + 2];
                 double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
-                double delta = fabs(Rsq - d2) / d2;
+                double delta = fabs(Rsq - d2) * RC[q];      // |r^2 - d^2| / d^2
                 if (delta < eps) continue;
                 finished = false;
                 double O0 = O[3 * ib] - O[3 * jb], O1 = O[3 * ib + 1] - O[3 * jb + 1], O2 = O[3 * ib + 2] - O[3 * jb + 2];
@@ -610,11 +622,11 @@ __global__ void __launch_bounds__(32 * RATTLE_WARPS) k_rattle_warp(double* __res
                 double RV = R[0] * W[0] + R[1] * W[1] + R[2] * W[2];
                 double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
                 double V2 = W[0] * W[0] + W[1] * W[1] + W[2] * W[2];
-                double phi = RV * RV / R2 * V2;   // precedence as in the reference
-                if (phi < eps2) continue;
+                if (RV * RV * V2 < eps2 * R2) continue;     // (RV^2 / R^2) V^2 < eps^2, R^2 > 0
                 finished = false;
                 double mi = IM[ib], mj = IM[jb];
-                double kij = RV / (dd * (mi + mj));
+                double kij = RV * RC[q];                    // RV / (d^2 (1/m_i + 1/m_j))
+                (void)dd;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     double KR = kij * R[d];
