@@ -29,6 +29,15 @@
 
 #include "pgk_ctx.cuh"
 
+// Mixed pair kernel launch shapes, one wave of nsm * blocks-per-SM blocks.
+// Packed cluster-frame body: 128-thread blocks, five resident per SM (its ~94
+// registers); smaller blocks stage the spline table more often than they
+// gain, larger ones finish their fixed cluster chunks less evenly.  Scalar
+// body: 256-thread blocks, three per SM (80 registers).
+constexpr int pair_threads(bool frame) { return frame ? 128 : 256; }
+constexpr int pair_minb(bool frame) { return frame ? 5 : 3; }
+constexpr int PAIR_WARPS = 8;                      // shared-memory rows per block (the larger shape)
+
 // ---- pack: sorted (padded) positions for the pair kernel ---------------------
 __global__ void k_pack_mixed(const double* __restrict__ pos, const double* __restrict__ chrg,
                              const int* __restrict__ perm, int npad, const DynState* __restrict__ dyn,
@@ -184,13 +193,9 @@ __device__ __forceinline__ void pair_term(const float dx, const float dy, const 
 // registers across the block's clusters and are reduced once per block.
 // PRUNE: the body of prune steps (reads the book rows, writes the pruned
 // ones); the other body runs on all other steps (one launch, see k_pair_mixed).
-// FRAME (boxes wide enough that the cluster atoms and every listed j, each
-// taken as its minimum image from cluster atom 0, never wrap against each
-// other): positions enter as FP32 offsets from cluster atom 0, so a pair's
-// displacement is three subtractions, and the tensor-only virial is summed
-// as sum_a F_a (x) x_a over the cluster atoms and the entries' j (equal to
-// sum over pairs f (x) r, with the lever arms of the cluster frame).
-template <int MODE, bool PRUNE, bool FRAME>
+// This body serves boxes in which a pair needs its own minimum image; wider
+// boxes run the packed cluster-frame body (pair_mixed_body_x2).
+template <int MODE, bool PRUNE>
 __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, const PairArgs& a,
                                                 const float2* __restrict__ lj_g, const float4* __restrict__ spl_g,
                                                 const DynState* __restrict__ dyn) {
@@ -199,9 +204,8 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
     float4* sf = sm;                        // force table  (spline 0)
     float4* sp = sm + a.nspl;               // pot table    (spline 1), ENE only
     float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
-    __shared__ int4 si[8][8];
-    __shared__ float4 sif[8][8];          // FRAME: offsets from cluster atom 0 (A) and charge
-    __shared__ int sti[8][8];
+    __shared__ int4 si[PAIR_WARPS][8];
+    __shared__ int sti[PAIR_WARPS][8];
     for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) {
         sf[k] = spl_g[k];
         if (ENE) sp[k] = spl_g[a.nspl + k];
@@ -228,13 +232,9 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
 
     for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
         __syncwarp();
-        const int4 p0 = __ldg(xq + 8 * cl);
         if (lane < 8) {
             const int4 v = __ldg(xq + 8 * cl + lane);
             si[warp][lane] = v;
-            if (FRAME)
-                sif[warp][lane] = make_float4((float)(v.x - p0.x) * sx, (float)(v.y - p0.y) * sy,
-                                              (float)(v.z - p0.z) * sz, __int_as_float(v.w));
             sti[warp][lane] = __ldg(typ_s + 8 * cl + lane) * a.ntyp;
             if (prune) a.xq_prune[8 * cl + lane] = v;
         }
@@ -246,44 +246,33 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
         float f[8][3];
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) { f[ii][0] = 0.f; f[ii][1] = 0.f; f[ii][2] = 0.f; }
+        // two-deep prefetch: entries two iterations ahead, their j records one
+        // ahead, so no gather waits on the entry load it depends on
         unsigned e = lane < cnt ? (unsigned)__ldg(row + lane) : 0u;
+        unsigned e1 = 32 + lane < cnt ? (unsigned)__ldg(row + 32 + lane) : 0u;
         int4 pj = __ldg(xq + (e & 0xFFFFFFu));
         int tj = __ldg(typ_s + (e & 0xFFFFFFu));
         for (int k0 = 0; k0 < cnt; k0 += 32) {          // warp-uniform trip count
-            const int kn = k0 + 32 + lane;
-            const unsigned en = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
-            const int4 pjn = __ldg(xq + (en & 0xFFFFFFu));
-            const int tjn = __ldg(typ_s + (en & 0xFFFFFFu));
+            const int kn = k0 + 64 + lane;
+            const unsigned e2 = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
+            const int4 pjn = __ldg(xq + (e1 & 0xFFFFFFu));
+            const int tjn = __ldg(typ_s + (e1 & 0xFFFFFFu));
             const unsigned m = e >> 24;
             const int sj = e & 0xFFFFFFu;
             float gx = 0.f, gy = 0.f, gz = 0.f;
             unsigned nm = 0;
-            const float jx = FRAME ? (float)(pj.x - p0.x) * sx : 0.f;
-            const float jy = FRAME ? (float)(pj.y - p0.y) * sy : 0.f;
-            const float jz = FRAME ? (float)(pj.z - p0.z) * sz : 0.f;
 #pragma unroll
             for (int ii = 0; ii < 8; ++ii)
                 if ((m >> ii) & 1u) {
-                    float r2, dx, dy, dz, qq;
-                    if (FRAME) {
-                        const float4 pi = sif[warp][ii];
-                        dx = pi.x - jx; dy = pi.y - jy; dz = pi.z - jz;
-                        qq = pi.w * __int_as_float(pj.w);
-                    } else {
-                        const int4 pi = si[warp][ii];
-                        dx = (float)(pi.x - pj.x) * sx; dy = (float)(pi.y - pj.y) * sy;
-                        dz = (float)(pi.z - pj.z) * sz;
-                        qq = __int_as_float(pi.w) * __int_as_float(pj.w);
-                    }
-                    pair_term<MODE, !FRAME>(dx, dy, dz, qq, sti[warp][ii] + tj, a.rr2f, a.rl2f, a.inv_hf, a.hf,
-                                            a.nsplm1, sf, sp,
-                                            slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
+                    const int4 pi = si[warp][ii];
+                    const float dx = (float)(pi.x - pj.x) * sx, dy = (float)(pi.y - pj.y) * sy;
+                    const float dz = (float)(pi.z - pj.z) * sz;
+                    const float qq = __int_as_float(pi.w) * __int_as_float(pj.w);
+                    float r2;
+                    pair_term<MODE, true>(dx, dy, dz, qq, sti[warp][ii] + tj, a.rr2f, a.rl2f, a.inv_hf, a.hf,
+                                          a.nsplm1, sf, sp, slj, f[ii], gx, gy, gz, ev, ee, wc, wl, r2);
                     if (PRUNE) nm |= r2 < rp2 ? 1u << ii : 0u;
                 }
-            if (FRAME && MODE == PM_TENS && m) {     // j's share of sum F (x) x (frame coordinates)
-                wc[0] = fmaf(gx, jx, wc[0]); wc[1] = fmaf(gx, jy, wc[1]); wc[2] = fmaf(gx, jz, wc[2]);
-                wc[3] = fmaf(gy, jy, wc[3]); wc[4] = fmaf(gy, jz, wc[4]); wc[5] = fmaf(gz, jz, wc[5]);
-            }
             if (m) {
                 unsigned long long* fj = (unsigned long long*)fs0 + sj;
                 atomicAdd(fj, (unsigned long long)__float2ll_rn(gx * (float)PGK_FORCE_SCALE));
@@ -295,17 +284,12 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
                 if (nm) prow[pcount + __popc(b & ((1u << lane) - 1u))] = (int)((nm << 24) | (unsigned)sj);
                 pcount += __popc(b);
             }
-            e = en; pj = pjn; tj = tjn;
+            e = e1; e1 = e2; pj = pjn; tj = tjn;
         }
         if (prune && lane == 0) a.pcnt[cl] = pcount;
 #pragma unroll
         for (int ii = 0; ii < 8; ++ii) {
             const float fx = warp_sum(f[ii][0]), fy = warp_sum(f[ii][1]), fz = warp_sum(f[ii][2]);
-            if (FRAME && MODE == PM_TENS && lane == ii) {      // cluster atom's share of sum F (x) x
-                const float4 pi = sif[warp][ii];
-                wc[0] = fmaf(fx, pi.x, wc[0]); wc[1] = fmaf(fx, pi.y, wc[1]); wc[2] = fmaf(fx, pi.z, wc[2]);
-                wc[3] = fmaf(fy, pi.y, wc[3]); wc[4] = fmaf(fy, pi.z, wc[4]); wc[5] = fmaf(fz, pi.z, wc[5]);
-            }
             if (lane == ii) {     // padding slots get zero sums (no mask bits)
                 unsigned long long* fi = (unsigned long long*)fs0 + 8 * cl + ii;
                 atomicAdd(fi, (unsigned long long)__double2ll_rn((double)fx * PGK_FORCE_SCALE));
@@ -332,15 +316,301 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
     }
 }
 
+// ---- packed (FP32x2) pair arithmetic for the cluster frame -------------------
+// The cluster's 8 atoms are taken as 4 pairs (2p, 2p+1); one packed operation
+// (fma/add/mul.f32x2, sm_100) evaluates both atoms of a pair against the
+// lane's j, so the arithmetic of two list pairs issues as one instruction.
+// Only the spline and LJ table fetches, the reciprocal square root and the
+// cutoff selects stay per element.  `mb` holds the entry's two mask bits for
+// the pair: an element whose bit is clear, or that lies beyond its cutoff,
+// contributes zero (same cutoffs and zero rules as pair_term).  SC: the LJ
+// and Coulomb cutoffs are equal (one select per element).  L holds the LJ
+// parameters of both atoms with j's type as (R_a^2, R_b^2, 12 eps_a,
+// 12 eps_b): fl = 12 eps (R^2/r^2)^3 ((R^2/r^2)^3 - 1) / r^2, and the LJ
+// energy 12 eps t6 (t6 - 2) is divided by 12 once per block.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+template <int MODE, bool SC>
+__device__ __forceinline__ void pair_term_x2(const float2 dx, const float2 dy, const float2 dz, const float2 qq,
+                                             const float4 L, const unsigned mb, const float rr2,
+                                             const float rl2, const float2 inv_h2, const float2 mh2,
+                                             const int nsplm1, const float4* __restrict__ sf,
+                                             const float4* __restrict__ sp,
+                                             float2 (&fi)[3], float2& gx, float2& gy, float2& gz, float2& ev,
+                                             float2& ee, float2* wc, float2* wl, float2& r2o) {
+    constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
+    const float2 two23 = make_float2(8388608.0f, 8388608.0f), mtwo23 = make_float2(-8388608.0f, -8388608.0f);
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+    r2o = r2;
+    const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+    const float2 rinv2 = __fmul2_rn(rinv, rinv);
+    const float2 r = __fmul2_rn(r2, rinv);
+    // floor(r/h) as in pair_term, both elements at once
+    const float2 fb = __fadd2_rd(__fmul2_rn(r, inv_h2), two23);
+    const float2 fm = __fadd2_rn(fb, mtwo23);
+    const int ia = (int)min((unsigned)(__float_as_int(fb.x) - 0x4B000000), (unsigned)nsplm1);
+    const int ib = (int)min((unsigned)(__float_as_int(fb.y) - 0x4B000000), (unsigned)nsplm1);
+    const float2 d = __ffma2_rn(fm, mh2, r);
+    const float4 ca = sf[ia], cb = sf[ib];
+    const float2 poly = make_float2(fmaf(d.x, fmaf(d.x, fmaf(d.x, ca.w, ca.z), ca.y), ca.x),
+                                    fmaf(d.y, fmaf(d.y, fmaf(d.y, cb.w, cb.z), cb.y), cb.x));
+    float2 fc = __fmul2_rn(qq, poly);
+    const float2 c12 = make_float2(L.z, L.w);
+    const float2 t2 = __fmul2_rn(rinv2, make_float2(L.x, L.y));
+    const float2 t6 = __fmul2_rn(__fmul2_rn(t2, t2), t2);
+    const float2 w = __fmul2_rn(__fmul2_rn(t6, __fadd2_rn(t6, make_float2(-1.f, -1.f))), rinv2);
+    float2 fl = __fmul2_rn(c12, w);
+    const bool ba = mb & 1u, bb = mb & 2u;
+    const bool ra = ba && r2.x <= rr2, rb = bb && r2.y <= rr2;
+    float2 fs;
+    if (SC) {
+        fs = __fadd2_rn(fc, fl);
+        fs.x = ra ? fs.x : 0.f;
+        fs.y = rb ? fs.y : 0.f;
+        if (MODE == PM_FULL) {
+            fc.x = ra ? fc.x : 0.f; fc.y = rb ? fc.y : 0.f;
+            fl.x = ra ? fl.x : 0.f; fl.y = rb ? fl.y : 0.f;
+        }
+    } else {
+        fc.x = ra ? fc.x : 0.f;
+        fc.y = rb ? fc.y : 0.f;
+        fl.x = (ba && r2.x <= rl2) ? fl.x : 0.f;
+        fl.y = (bb && r2.y <= rl2) ? fl.y : 0.f;
+        fs = __fadd2_rn(fc, fl);
+    }
+    if (ENE) {
+        const bool la_in = SC ? ra : (ba && r2.x <= rl2), lb_in = SC ? rb : (bb && r2.y <= rl2);
+        const float4 pa = sp[ia], pb = sp[ib];
+        float2 pe = __fmul2_rn(qq, make_float2(fmaf(d.x, fmaf(d.x, fmaf(d.x, pa.w, pa.z), pa.y), pa.x),
+                                               fmaf(d.y, fmaf(d.y, fmaf(d.y, pb.w, pb.z), pb.y), pb.x)));
+        pe.x = ra ? pe.x : 0.f;
+        pe.y = rb ? pe.y : 0.f;
+        ee = __fadd2_rn(ee, pe);
+        const float2 v = __fmul2_rn(t6, __fadd2_rn(t6, make_float2(-2.f, -2.f)));
+        float2 vl = __fmul2_rn(c12, v);
+        vl.x = la_in ? vl.x : 0.f;
+        vl.y = lb_in ? vl.y : 0.f;
+        ev = __fadd2_rn(ev, vl);
+    }
+    const float2 cx = __fmul2_rn(fs, dx), cy = __fmul2_rn(fs, dy), cz = __fmul2_rn(fs, dz);
+    fi[0] = __fadd2_rn(fi[0], cx); fi[1] = __fadd2_rn(fi[1], cy); fi[2] = __fadd2_rn(fi[2], cz);
+    gx = __fadd2_rn(gx, cx); gy = __fadd2_rn(gy, cy); gz = __fadd2_rn(gz, cz);
+    if (MODE == PM_FULL) {
+        const float2 ax = __fmul2_rn(fc, dx), ay = __fmul2_rn(fc, dy), az = __fmul2_rn(fc, dz);
+        wc[0] = __ffma2_rn(ax, dx, wc[0]); wc[1] = __ffma2_rn(ax, dy, wc[1]); wc[2] = __ffma2_rn(ax, dz, wc[2]);
+        wc[3] = __ffma2_rn(ay, dy, wc[3]); wc[4] = __ffma2_rn(ay, dz, wc[4]); wc[5] = __ffma2_rn(az, dz, wc[5]);
+        const float2 lx = __fmul2_rn(fl, dx), ly = __fmul2_rn(fl, dy), lz = __fmul2_rn(fl, dz);
+        wl[0] = __ffma2_rn(lx, dx, wl[0]); wl[1] = __ffma2_rn(lx, dy, wl[1]); wl[2] = __ffma2_rn(lx, dz, wl[2]);
+        wl[3] = __ffma2_rn(ly, dy, wl[3]); wl[4] = __ffma2_rn(ly, dz, wl[4]); wl[5] = __ffma2_rn(lz, dz, wl[5]);
+    }
+}
+
+// Cluster-frame body with packed arithmetic: the same rows, entries, prune
+// compaction, force sums and accumulator layout as pair_mixed_body.
+// The cluster atoms are staged as 4 atom pairs (x0,x1,y0,y1 | z0,z1,q0,q1);
+// each lane holds its j as (-x_j, -x_j) ... so a displacement pair is one
+// packed add.  The per-lane force sums of the cluster atoms are 4 packed
+// triples (the same 24 registers as 8 scalar ones); j's force is summed as a
+// packed pair and its two halves added once per entry.
+struct __align__(16) IPair { float4 xy; float4 zq; };
+
+template <int MODE, bool PRUNE, bool SC>
+__device__ __forceinline__ void pair_mixed_body_x2(const int4* __restrict__ xq, const PairArgs& a,
+                                                   const float2* __restrict__ lj_g,
+                                                   const float4* __restrict__ spl_g,
+                                                   const DynState* __restrict__ dyn) {
+    constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
+    extern __shared__ float4 sm[];
+    float4* sf = sm;
+    float4* sp = sm + a.nspl;
+    float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
+    // per warp: the cluster's LJ rows, [tj][p] = (R^2, R^2, 12 eps, 12 eps) of
+    // atoms 2p, 2p+1 with type tj (after the block's type table)
+    float4* sljc = (float4*)(slj + ((a.ntyp * a.ntyp + 1) & ~1)) + (size_t)(threadIdx.x >> 5) * 4 * a.ntyp;
+    __shared__ IPair sip[PAIR_WARPS][4];
+    __shared__ int2 stp[PAIR_WARPS][4];
+    for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) {
+        sf[k] = spl_g[k];
+        if (ENE) sp[k] = spl_g[a.nspl + k];
+    }
+    for (int k = threadIdx.x; k < a.ntyp * a.ntyp; k += blockDim.x) {
+        const float2 l = lj_g[k];
+        slj[k] = make_float2(l.x, 12.f * l.y);
+    }
+    __syncthreads();
+
+    const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
+    const float sy = (float)(dyn->box[1] * (1.0 / 4294967296.0));
+    const float sz = (float)(dyn->box[2] * (1.0 / 4294967296.0));
+    const float2 inv_h2 = make_float2(a.inv_hf, a.inv_hf), mh2 = make_float2(-a.hf, -a.hf);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int chunk = (a.ncl + gridDim.x - 1) / gridDim.x;
+    const int c_end = min(a.ncl, (blockIdx.x + 1) * chunk);
+    const int* __restrict__ typ_s = a.typ_s;
+    long long* __restrict__ fs0 = a.fsort;
+    const int fst = a.fstride;
+    float2 ev = make_float2(0.f, 0.f), ee = make_float2(0.f, 0.f);
+    float wt[6] = {0, 0, 0, 0, 0, 0};                     // TENS: sum F (x) x in the cluster frame
+    float2 wc[6], wl[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { wc[k] = make_float2(0.f, 0.f); wl[k] = make_float2(0.f, 0.f); }
+
+    const int* __restrict__ rows = PRUNE ? a.blist : a.clist;
+    const int* __restrict__ rcnt = PRUNE ? a.bcnt : a.ccnt;
+    const float rp2 = a.rp2;
+
+    for (int cl = blockIdx.x * chunk + warp; cl < c_end; cl += wpb) {
+        __syncwarp();
+        const int4 p0 = __ldg(xq + 8 * cl);
+        if (lane < 8) {
+            const int4 v = __ldg(xq + 8 * cl + lane);
+            float* ip = (float*)&sip[warp][lane >> 1];
+            const int h = lane & 1;
+            ip[h] = (float)(v.x - p0.x) * sx;
+            ip[2 + h] = (float)(v.y - p0.y) * sy;
+            ip[4 + h] = (float)(v.z - p0.z) * sz;
+            ip[6 + h] = __int_as_float(v.w);
+            ((int*)&stp[warp][lane >> 1])[h] = __ldg(typ_s + 8 * cl + lane) * a.ntyp;
+            if (PRUNE) a.xq_prune[8 * cl + lane] = v;
+        }
+        __syncwarp();
+        for (int k = lane; k < 4 * a.ntyp; k += 32) {
+            const int2 T = stp[warp][k & 3];
+            const float2 la = slj[T.x + (k >> 2)], lb = slj[T.y + (k >> 2)];
+            sljc[k] = make_float4(la.x, lb.x, la.y, lb.y);
+        }
+        __syncwarp();
+        const int cnt = __ldg(rcnt + cl);
+        const int* __restrict__ row = rows + (size_t)cl * a.ccap;
+        int* __restrict__ prow = a.plist + (size_t)cl * a.ccap;
+        int pcount = 0;
+        float2 f[4][3];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) { f[p][0] = make_float2(0.f, 0.f); f[p][1] = f[p][0]; f[p][2] = f[p][0]; }
+        // two-deep prefetch: entries two iterations ahead, their j records one
+        // ahead, so no gather waits on the entry load it depends on
+        unsigned e = lane < cnt ? (unsigned)__ldg(row + lane) : 0u;
+        unsigned e1 = 32 + lane < cnt ? (unsigned)__ldg(row + 32 + lane) : 0u;
+        int4 pj = __ldg(xq + (e & 0xFFFFFFu));
+        int tj = __ldg(typ_s + (e & 0xFFFFFFu));
+        for (int k0 = 0; k0 < cnt; k0 += 32) {          // warp-uniform trip count
+            const int kn = k0 + 64 + lane;
+            const unsigned e2 = kn < cnt ? (unsigned)__ldg(row + kn) : 0u;
+            const int4 pjn = __ldg(xq + (e1 & 0xFFFFFFu));
+            const int tjn = __ldg(typ_s + (e1 & 0xFFFFFFu));
+            const unsigned m = e >> 24;
+            const int sj = e & 0xFFFFFFu;
+            const float jx = (float)(pj.x - p0.x) * sx;
+            const float jy = (float)(pj.y - p0.y) * sy;
+            const float jz = (float)(pj.z - p0.z) * sz;
+            const float2 njx = make_float2(-jx, -jx), njy = make_float2(-jy, -jy), njz = make_float2(-jz, -jz);
+            const float2 qj = make_float2(__int_as_float(pj.w), __int_as_float(pj.w));
+            const float4* ljr = sljc + 4 * tj;
+            float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
+            unsigned nm = 0;
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const unsigned mb = (m >> (2 * p)) & 3u;
+                if (mb) {
+                    const IPair I = sip[warp][p];
+                    const float4 L = ljr[p];
+                    const float2 dx = __fadd2_rn(make_float2(I.xy.x, I.xy.y), njx);
+                    const float2 dy = __fadd2_rn(make_float2(I.xy.z, I.xy.w), njy);
+                    const float2 dz = __fadd2_rn(make_float2(I.zq.x, I.zq.y), njz);
+                    const float2 qq = __fmul2_rn(make_float2(I.zq.z, I.zq.w), qj);
+                    float2 r2;
+                    pair_term_x2<MODE, SC>(dx, dy, dz, qq, L, mb, a.rr2f, a.rl2f, inv_h2, mh2, a.nsplm1, sf, sp,
+                                           f[p], gx, gy, gz, ev, ee, wc, wl, r2);
+                    if (PRUNE)
+                        nm |= ((((mb & 1u) && r2.x < rp2) ? 1u : 0u) | (((mb & 2u) && r2.y < rp2) ? 2u : 0u))
+                              << (2 * p);
+                }
+            }
+            // force on j: minus the sum of its pairs' forces on the cluster atoms
+            const float fjx = -(gx.x + gx.y), fjy = -(gy.x + gy.y), fjz = -(gz.x + gz.y);
+            if (MODE == PM_TENS && m) {     // j's share of sum F (x) x (frame coordinates)
+                wt[0] = fmaf(fjx, jx, wt[0]); wt[1] = fmaf(fjx, jy, wt[1]); wt[2] = fmaf(fjx, jz, wt[2]);
+                wt[3] = fmaf(fjy, jy, wt[3]); wt[4] = fmaf(fjy, jz, wt[4]); wt[5] = fmaf(fjz, jz, wt[5]);
+            }
+            if (m) {
+                unsigned long long* fj = (unsigned long long*)fs0 + sj;
+                atomicAdd(fj, (unsigned long long)__float2ll_rn(fjx * (float)PGK_FORCE_SCALE));
+                atomicAdd(fj + fst, (unsigned long long)__float2ll_rn(fjy * (float)PGK_FORCE_SCALE));
+                atomicAdd(fj + 2 * fst, (unsigned long long)__float2ll_rn(fjz * (float)PGK_FORCE_SCALE));
+            }
+            if (PRUNE) {       // compact the entries that keep a pair inside rprune
+                const unsigned b = __ballot_sync(0xffffffffu, nm != 0);
+                if (nm) prow[pcount + __popc(b & ((1u << lane) - 1u))] = (int)((nm << 24) | (unsigned)sj);
+                pcount += __popc(b);
+            }
+            e = e1; e1 = e2; pj = pjn; tj = tjn;
+        }
+        if (PRUNE && lane == 0) a.pcnt[cl] = pcount;
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            const float2* fp = f[ii >> 1];
+            const float fx = warp_sum((ii & 1) ? fp[0].y : fp[0].x);
+            const float fy = warp_sum((ii & 1) ? fp[1].y : fp[1].x);
+            const float fz = warp_sum((ii & 1) ? fp[2].y : fp[2].x);
+            if (lane == ii) {     // padding slots get zero sums (no mask bits)
+                if (MODE == PM_TENS) {      // cluster atom's share of sum F (x) x
+                    const float* ip = (const float*)&sip[warp][ii >> 1];
+                    const float px = ip[ii & 1], py = ip[2 + (ii & 1)], pz = ip[4 + (ii & 1)];
+                    wt[0] = fmaf(fx, px, wt[0]); wt[1] = fmaf(fx, py, wt[1]); wt[2] = fmaf(fx, pz, wt[2]);
+                    wt[3] = fmaf(fy, py, wt[3]); wt[4] = fmaf(fy, pz, wt[4]); wt[5] = fmaf(fz, pz, wt[5]);
+                }
+                unsigned long long* fi = (unsigned long long*)fs0 + 8 * cl + ii;
+                atomicAdd(fi, (unsigned long long)__double2ll_rn((double)fx * PGK_FORCE_SCALE));
+                atomicAdd(fi + fst, (unsigned long long)__double2ll_rn((double)fy * PGK_FORCE_SCALE));
+                atomicAdd(fi + 2 * fst, (unsigned long long)__double2ll_rn((double)fz * PGK_FORCE_SCALE));
+            }
+        }
+    }
+    // every pair evaluated once.  Tensor (a,b) -> 3*b + a, stored as its lower triangle.
+    if (MODE == PM_FULL) {
+        const double evs = ((double)ev.x + (double)ev.y) * (1.0 / 12.0);
+        const double ees = (double)ee.x + (double)ee.y;
+        double v[16] = {evs, ees, ees};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            v[3 + k] = (double)wc[k].x + (double)wc[k].y;
+            v[9 + k] = (double)wl[k].x + (double)wl[k].y;
+        }
+        v[15] = v[9] + v[12] + v[14];
+        const int idx[16] = {A_VDW, A_ELC, A_VC, A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8,
+                             A_VTLJ + 0, A_VTLJ + 1, A_VTLJ + 2, A_VTLJ + 4, A_VTLJ + 5, A_VTLJ + 8, A_VLJ};
+        block_acc<16>(v, a.acc, idx, false);
+    } else if (MODE == PM_TENS) {
+        double v[6] = {wt[0], wt[1], wt[2], wt[3], wt[4], wt[5]};
+        const int idx[6] = {A_VTC + 0, A_VTC + 1, A_VTC + 2, A_VTC + 4, A_VTC + 5, A_VTC + 8};
+        block_acc<6>(v, a.acc, idx, false);
+    } else if (MODE == PM_ENE) {
+        double v[2] = {((double)ev.x + (double)ev.y) * (1.0 / 12.0), (double)ee.x + (double)ee.y};
+        const int idx[2] = {A_VDW, A_ELC};
+        block_acc<2>(v, a.acc, idx, false);
+    }
+}
+
 // One launch per evaluation: the step kind that k_prune_decide wrote on the
-// device (prune step or not) selects the body, block-uniformly.
-template <int MODE, bool FRAME>
-__global__ void __launch_bounds__(256, 3) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
-                                                       const float2* __restrict__ lj_g,
-                                                       const float4* __restrict__ spl_g,
-                                                       const DynState* __restrict__ dyn) {
-    if (a.P != nullptr && a.P->do_prune) pair_mixed_body<MODE, true, FRAME>(xq, a, lj_g, spl_g, dyn);
-    else pair_mixed_body<MODE, false, FRAME>(xq, a, lj_g, spl_g, dyn);
+// device (prune step or not) selects the body, block-uniformly.  FRAME boxes
+// run the packed body (SC: equal LJ and Coulomb cutoffs).
+template <int MODE, bool FRAME, bool SC>
+__global__ void __launch_bounds__(pair_threads(FRAME), pair_minb(FRAME)) k_pair_mixed(const int4* __restrict__ xq, PairArgs a,
+                                                                        const float2* __restrict__ lj_g,
+                                                                        const float4* __restrict__ spl_g,
+                                                                        const DynState* __restrict__ dyn) {
+    const bool prune = a.P != nullptr && a.P->do_prune;
+    if (FRAME) {
+        if (prune) pair_mixed_body_x2<MODE, true, SC>(xq, a, lj_g, spl_g, dyn);
+        else pair_mixed_body_x2<MODE, false, SC>(xq, a, lj_g, spl_g, dyn);
+    } else {
+        if (prune) pair_mixed_body<MODE, true>(xq, a, lj_g, spl_g, dyn);
+        else pair_mixed_body<MODE, false>(xq, a, lj_g, spl_g, dyn);
+    }
 }
 
 // ---- pair kernel, FP64 (parity path) ---------------------------------------
@@ -542,12 +812,19 @@ __global__ void __launch_bounds__(128) k_pair_finish(long long* __restrict__ fso
     else prune_sort_rows(blockIdx.x - nbu, plist, pcnt, ccap, ncl, P);
 }
 
-template <int MODE, bool FRAME>
-static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a, int blocks) {
+template <int MODE, bool FRAME, bool SC>
+static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
-    size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) + c->ntyp * c->ntyp * sizeof(float2);
-    smem_limit(k_pair_mixed<MODE, FRAME>, sm);
-    k_pair_mixed<MODE, FRAME><<<blocks, 256, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
+    constexpr int nt = pair_threads(FRAME);
+    size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) +
+                (size_t)((c->ntyp * c->ntyp + 1) & ~1) * sizeof(float2);
+    if (FRAME) sm += (size_t)(nt / 32) * 4 * c->ntyp * sizeof(float4);
+    long long blocks = (long long)c->nsm * pair_minb(FRAME);
+    const long long need = (c->ncl + nt / 32 - 1) / (nt / 32);
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    smem_limit(k_pair_mixed<MODE, FRAME, SC>, sm);
+    k_pair_mixed<MODE, FRAME, SC><<<(int)blocks, nt, sm, c->st>>>(c->xq, a, c->lj32, c->spl32, c->dyn);
     PGK_LAUNCHED(c);
 }
 
@@ -559,14 +836,18 @@ static bool frame_ok(const pgk_ctx* c) {
     const DynState& h = c->hdyn;
     double cs = 0.0, lmin = 1e300;
     for (int d = 0; d < 3; ++d) { cs = std::max(cs, h.cellsize[d]); lmin = std::min(lmin, h.box[d]); }
-    if (h.list_mode_used != PGK_LIST_CELL) return false;
+    if (h.list_mode_used != PGK_LIST_CELL || c->ntyp > 64) return false;   // 64: per-warp LJ rows in smem
     return 0.5 * lmin > std::sqrt(3.0) * cs + c->prm.rcut_book + 4.0;
 }
 
 template <int MODE>
-static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a, int blocks) {
-    if (frame_ok(c) && !c->no_frame) pair_mixed_launch2<MODE, true>(c, a, blocks);
-    else pair_mixed_launch2<MODE, false>(c, a, blocks);
+static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a) {
+    if (frame_ok(c) && !c->no_frame) {
+        if (a.rr2f == a.rl2f) pair_mixed_launch2<MODE, true, true>(c, a);
+        else pair_mixed_launch2<MODE, true, false>(c, a);
+    } else {
+        pair_mixed_launch2<MODE, false, false>(c, a);
+    }
 }
 
 // After the mixed pair kernel: the sorted-slot forces into the group
@@ -620,19 +901,18 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
         a.xq_prune = c->xq_prune; a.rp2 = rp * rp;
         a.clist = c->plist; a.ccnt = c->pcnt;
     }
-    const int warps_per_block = 8;
-    int blocks = c->nsm * (c->mixed() ? 3 : 2);
-    long long need = (c->ncl + warps_per_block - 1) / warps_per_block;
-    if (blocks > need) blocks = (int)need;
-    if (blocks < 1) blocks = 1;
     if (c->mixed()) {
         switch (vmode) {
-            case PM_FULL: pair_mixed_launch<PM_FULL>(c, a, blocks); break;
-            case PM_TENS: pair_mixed_launch<PM_TENS>(c, a, blocks); break;
-            case PM_ENE: pair_mixed_launch<PM_ENE>(c, a, blocks); break;
-            default: pair_mixed_launch<PM_FORCE>(c, a, blocks); break;
+            case PM_FULL: pair_mixed_launch<PM_FULL>(c, a); break;
+            case PM_TENS: pair_mixed_launch<PM_TENS>(c, a); break;
+            case PM_ENE: pair_mixed_launch<PM_ENE>(c, a); break;
+            default: pair_mixed_launch<PM_FORCE>(c, a); break;
         }
     } else {
+        int blocks = c->nsm * 2;                     // 256-thread blocks, two per SM
+        const long long need = (c->ncl + 7) / 8;
+        if (blocks > need) blocks = (int)need;
+        if (blocks < 1) blocks = 1;
         size_t sm = (size_t)2 * c->nspl * sizeof(double4) + c->ntyp * c->ntyp * sizeof(double2);
         if (vmode != PM_FORCE) {
             smem_limit(k_pair_fp64<true>, sm);

@@ -316,6 +316,9 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         pgk_free(c);
         return PGK_E_CUDA;
     }
+    if (const char* ns = getenv("PGK_STREAMS")) {       // 1: the whole force evaluation on one stream
+        if (atoi(ns) == 1) { cudaStreamDestroy(c->st2); c->st2 = nullptr; }
+    }
     c->degfree = s->degfree_all;
     pgk_status st;
 #define TRY(x) do { if ((st = (x)) != PGK_OK) { pgk_free(c); return st; } } while (0)
@@ -599,7 +602,8 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         }
         if (pgk_dmalloc(c, &c->iperm, n * sizeof(int)) || pgk_dmalloc(c, &c->cell_of, n * sizeof(int)) ||
             pgk_dmalloc(c, &c->subkey, n * sizeof(int)) || pgk_dmalloc(c, &c->counters, 8 * sizeof(unsigned long long)) ||
-            pgk_dmalloc(c, &c->hasup, std::max(n, 1))) {
+            pgk_dmalloc(c, &c->hasup, std::max(n, 1)) ||
+            cudaMemsetAsync(c->counters, 0, 8 * sizeof(unsigned long long), c->st)) {
             pgk_free(c);
             return PGK_E_NOMEM;
         }

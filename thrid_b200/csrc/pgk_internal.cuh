@@ -161,15 +161,31 @@ __device__ __forceinline__ double force_get(const void* facc, size_t k) {
     return ((const double*)facc)[k];
 }
 
-// Sort bin of a cluster-row entry's 8-bit mask: the inverse Gray code, so
-// that masks next to each other in the sorted row differ in few bits (the
-// pair kernel's loop over the mask bits then leaves fewer lanes idle than in
-// numeric mask order)
+// Sort bin of a cluster-row entry's 8-bit mask (a dense rank 0..255).  The
+// pair kernel evaluates the cluster atoms as four pairs (bits 2p, 2p+1), and a
+// warp runs a pair's evaluation when any of its 32 lanes has a bit in it; so
+// entries are grouped first by which of the four pairs are occupied (groups in
+// inverse-Gray-code order of that 4-bit occupancy: neighbouring groups differ
+// in one pair), and inside a group by the occupied pairs' states taken as a
+// mixed-radix-3 number (bits 01 -> 0, 11 -> 1, 10 -> 2).  Group g starts at
+// the sum of 3^popcount over the groups before it: offsets 0, 1, 4, 13, 16, 25,
+// 52, 61, 64, 73, 100, 181, 208, 217, 244, 253, packed eight to a word below.
 __device__ __forceinline__ unsigned mask_bin(unsigned m) {
-    m ^= m >> 1;
-    m ^= m >> 2;
-    m ^= m >> 4;
-    return m & 0xFFu;
+    unsigned occ = 0, w = 0, mul = 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const unsigned b = (m >> (2 * q)) & 3u;
+        if (b) {
+            occ |= 1u << q;
+            w += (b == 1u ? 0u : (b == 3u ? 1u : 2u)) * mul;
+            mul *= 3u;
+        }
+    }
+    occ ^= occ >> 1;
+    occ ^= occ >> 2;
+    occ &= 0xFu;
+    const unsigned long long off = occ < 8u ? 0x3d3419100d040100ull : 0xfdf4d9d0b5644940ull;
+    return (unsigned)((off >> (8u * (occ & 7u))) & 0xFFull) + w;
 }
 
 // Fortran dnint/anint (round half away from zero), exact FP64 min image
