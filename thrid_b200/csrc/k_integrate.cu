@@ -650,6 +650,124 @@ __global__ void __launch_bounds__(32 * RATTLE_WARPS) k_rattle_warp(double* __res
     }
 }
 
+// Rigid three-atom groups (rigid water): constraints q0 = (a0,a1), q1 =
+// (a0,a2), q2 = (a1,a2), swept in that order.  One thread per group with its
+// three atoms' positions, velocities, old positions and inverse masses in
+// registers: the sweeps are the same arithmetic in the same order as
+// k_rattle_warp (rattle_c / rattle_cmtk, rattle_mtk.F90:278-542 for the
+// velocities), without a shared-memory round trip in the serial chain.
+template <bool POS>
+__global__ void __launch_bounds__(128) k_rattle_rigid3(double* __restrict__ pos, double* __restrict__ vel,
+                                                       const double* __restrict__ old,
+                                                       const double* __restrict__ invm,
+                                                       const int4* __restrict__ atoms,
+                                                       const double4* __restrict__ dl, int ngroup, double eps,
+                                                       double dt, int use_rv, const DynState* __restrict__ dyn,
+                                                       unsigned* status) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroup) return;
+    const int4 A = atoms[g];
+    const int at[3] = {A.x, A.y, A.z};
+    const double4 D = dl[g];
+    double X[3][3], V[3][3], O[3][3], IM[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        IM[a] = invm[at[a]];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            X[a][d] = pos[3 * (size_t)at[a] + d];
+            V[a][d] = vel[3 * (size_t)at[a] + d];
+            O[a][d] = POS ? old[3 * (size_t)at[a] + d] : 0.0;
+        }
+    }
+    constexpr int CI[3] = {0, 0, 1}, CJ[3] = {1, 2, 2};
+    const double dd[3] = {D.x * D.x, D.y * D.y, D.z * D.z};
+    double RC[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) RC[q] = POS ? 1.0 / dd[q] : 1.0 / (dd[q] * (IM[CI[q]] + IM[CJ[q]]));
+    bool finished = false;
+    if (POS) {
+        double rvi[3] = {1.0, 1.0, 1.0};
+        if (use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int ib = CI[q], jb = CJ[q];
+                const double d2 = dd[q];
+                const double R0 = X[ib][0] - X[jb][0], R1 = X[ib][1] - X[jb][1], R2 = X[ib][2] - X[jb][2];
+                const double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
+                const double delta = fabs(Rsq - d2) * RC[q];      // |r^2 - d^2| / d^2
+                if (delta < eps) continue;
+                finished = false;
+                const double O0 = O[ib][0] - O[jb][0], O1 = O[ib][1] - O[jb][1], O2 = O[ib][2] - O[jb][2];
+                const double RR = R0 * O0 + R1 * O1 + R2 * O2;
+                const double mi = IM[ib], mj = IM[jb];
+                const double gij = (Rsq - d2) / (2.0 * RR * (mi + mj) * dt);
+                const double G[3] = {gij * O0, gij * O1, gij * O2};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    X[ib][d] = X[ib][d] - mi * G[d] * dt;
+                    X[jb][d] = X[jb][d] + mj * G[d] * dt;
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double Gv = G[d] * rvi[d];
+                    V[ib][d] = V[ib][d] - mi * Gv;
+                    V[jb][d] = V[jb][d] + mj * Gv;
+                }
+            }
+        }
+    } else {
+        const double eps2 = eps * eps;
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const int ib = CI[q], jb = CJ[q];
+                double R[3], W[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    R[d] = X[ib][d] - X[jb][d];
+                    W[d] = V[ib][d] - V[jb][d];
+                }
+                const double RV = R[0] * W[0] + R[1] * W[1] + R[2] * W[2];
+                const double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+                const double V2 = W[0] * W[0] + W[1] * W[1] + W[2] * W[2];
+                if (RV * RV * V2 < eps2 * R2) continue;     // (RV^2 / R^2) V^2 < eps^2, R^2 > 0
+                finished = false;
+                const double mi = IM[ib], mj = IM[jb];
+                const double kij = RV * RC[q];              // RV / (d^2 (1/m_i + 1/m_j))
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double KR = kij * R[d];
+                    V[ib][d] = V[ib][d] - mi * KR;
+                    V[jb][d] = V[jb][d] + mj * KR;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (POS) pos[3 * (size_t)at[a] + d] = X[a][d];
+            vel[3 * (size_t)at[a] + d] = V[a][d];
+        }
+    if (!finished) atomicOr(status, POS ? ST_RATTLE_NOCONV : ST_RATTLEV_NOCONV);
+}
+
+static void rattle_rigid3_launch(pgk_ctx* c, bool pos, double eps, double dt, bool use_rv) {
+    const int blocks = (c->nr3 + 127) / 128;
+    if (pos)
+        k_rattle_rigid3<true><<<blocks, 128, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->r3_atoms,
+                                                         c->r3_d, c->nr3, eps, dt, use_rv ? 1 : 0, c->dyn, c->status);
+    else
+        k_rattle_rigid3<false><<<blocks, 128, 0, c->st>>>(c->pos, c->vel, nullptr, c->invmass, c->r3_atoms,
+                                                          c->r3_d, c->nr3, eps, 0.0, 0, c->dyn, c->status);
+    PGK_LAUNCHED(c);
+}
+
 static void rattle_warp_launch(pgk_ctx* c, bool pos, double eps, double dt, bool use_rv) {
     const int nwarp = (c->ncgroup + 31) / 32;
     const int blocks = (nwarp + RATTLE_WARPS - 1) / RATTLE_WARPS;
@@ -671,7 +789,8 @@ static void rattle_warp_launch(pgk_ctx* c, bool pos, double eps, double dt, bool
 }
 
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
-    if (c->ncgroup == 0) return PGK_OK;
+    if (c->nr3 > 0) rattle_rigid3_launch(c, true, eps, dt, use_rv);
+    if (c->ncgroup == 0) { PGK_CUDA(c, cudaGetLastError()); return PGK_OK; }
     if (c->cg_nfit > 0) rattle_warp_launch(c, true, eps, dt, use_rv);
     if (c->cg_nfit < (c->ncgroup + 31) / 32) {
         k_rattle_pos<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->cg_idx,
@@ -685,7 +804,8 @@ pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
 }
 
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
-    if (c->ncgroup == 0) return PGK_OK;
+    if (c->nr3 > 0) rattle_rigid3_launch(c, false, eps, 0.0, false);
+    if (c->ncgroup == 0) { PGK_CUDA(c, cudaGetLastError()); return PGK_OK; }
     if (c->cg_nfit > 0) rattle_warp_launch(c, false, eps, 0.0, false);
     if (c->cg_nfit < (c->ncgroup + 31) / 32) {
         k_rattle_vel<<<(c->ncgroup + 63) / 64, 64, 0, c->st>>>(c->pos, c->vel, c->invmass, c->cg_idx, c->cg_list,

@@ -539,6 +539,33 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
                     gi.push_back((int)gl.size());
                 }
             }
+            // Rigid three-atom groups: the constraints (a0,a1), (a0,a2), (a1,a2)
+            // in this order, each stored with its lower-listed atom first as
+            // here (rigid water: O-H1, O-H2, H1-H2).  They leave the group
+            // arrays for k_rattle_rigid3; the order of groups does not matter
+            // (each moves only its own atoms).
+            {
+                std::vector<int4> r3a;
+                std::vector<double4> r3d;
+                std::vector<int> gi2(1, 0), gl2;
+                for (int g = 0; g + 1 < (int)gi.size(); ++g) {
+                    if (gi[g + 1] - gi[g] == 3) {
+                        const int2 q0 = cij[gl[gi[g]]], q1 = cij[gl[gi[g] + 1]], q2 = cij[gl[gi[g] + 2]];
+                        if (q1.x == q0.x && q2.x == q0.y && q2.y == q1.y && q0.x != q0.y && q1.y != q0.x &&
+                            q1.y != q0.y) {
+                            r3a.push_back(make_int4(q0.x, q0.y, q1.y, 0));
+                            r3d.push_back(make_double4(cd[gl[gi[g]]], cd[gl[gi[g] + 1]], cd[gl[gi[g] + 2]], 0.0));
+                            continue;
+                        }
+                    }
+                    gl2.insert(gl2.end(), gl.begin() + gi[g], gl.begin() + gi[g + 1]);
+                    gi2.push_back((int)gl2.size());
+                }
+                c->nr3 = (int)r3a.size();
+                if (c->nr3) { TRY(upload(c, &c->r3_atoms, r3a)); TRY(upload(c, &c->r3_d, r3d)); }
+                gi.swap(gi2);
+                gl.swap(gl2);
+            }
             c->ncgroup = (int)gi.size() - 1;
             std::vector<int2> span(c->ncgroup);
             for (int g = 0; g < c->ncgroup; ++g) {
@@ -658,7 +685,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out, c->ewk_seg,
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
-                    c->hfk_tw[1], c->hfk_tw[2]};
+                    c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d};
     for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamDestroy(c->st2);
@@ -1067,7 +1094,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
 static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
                                bool tens, bool hfs, bool lt, bool ke_ready) {
     const double dts = md->dt_long_cal / (double)md->nstep_short;
-    const bool rattle = md->ifrattle && c->ncgroup > 0;
+    const bool rattle = md->ifrattle && (c->ncgroup > 0 || c->nr3 > 0);
     const bool mtk = kind == 2;
     const bool hfdrv = kind == 3;
     const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);

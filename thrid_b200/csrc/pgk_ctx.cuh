@@ -111,6 +111,12 @@ struct pgk_ctx {
     int2* cg_span = nullptr;      // (first atom, atom count) of each group's contiguous span
     unsigned char* cg_fit = nullptr;   // per 32 groups: 1 = staged in shared memory (k_rattle_warp)
     int cg_nfit = 0;
+    // rigid three-atom groups (constraints (a0,a1), (a0,a2), (a1,a2) in that
+    // order: rigid water) kept out of the group arrays above, run by
+    // k_rattle_rigid3 with their state in registers
+    int nr3 = 0;
+    int4* r3_atoms = nullptr;     // (a0, a1, a2, -)
+    double4* r3_d = nullptr;      // constraint lengths (d01, d02, d12, -)
 
     // ---- pair list ----
     int maxcells = 0;
