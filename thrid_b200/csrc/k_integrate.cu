@@ -757,6 +757,136 @@ __global__ void __launch_bounds__(128) k_rattle_rigid3(double* __restrict__ pos,
     if (!finished) atomicOr(status, POS ? ST_RATTLE_NOCONV : ST_RATTLEV_NOCONV);
 }
 
+// Star groups: constraints q = (c, a_{q+1}), q = 0..K-1, swept in that order
+// (the X-H bonds of one heavy atom).  One thread per group, state in
+// registers; same arithmetic and order as k_rattle_warp.
+template <bool POS, int K>
+__device__ __forceinline__ void rattle_star_group(int g, double* __restrict__ pos, double* __restrict__ vel,
+                                                  const double* __restrict__ old, const double* __restrict__ invm,
+                                                  const int* __restrict__ sa, const double* __restrict__ sd,
+                                                  double eps, double dt, const double (&rvi)[3],
+                                                  unsigned* status) {
+    int at[K + 1];
+    double X[K + 1][3], V[K + 1][3], O[K + 1][3], IM[K + 1], dd[K], RC[K];
+#pragma unroll
+    for (int a = 0; a <= K; ++a) {
+        at[a] = sa[5 * (size_t)g + a];
+        IM[a] = invm[at[a]];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            X[a][d] = pos[3 * (size_t)at[a] + d];
+            V[a][d] = vel[3 * (size_t)at[a] + d];
+            O[a][d] = POS ? old[3 * (size_t)at[a] + d] : 0.0;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const double dij = sd[4 * (size_t)g + q];
+        dd[q] = dij * dij;
+        RC[q] = POS ? 1.0 / dd[q] : 1.0 / (dd[q] * (IM[0] + IM[q + 1]));
+    }
+    bool finished = false;
+    if (POS) {
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                constexpr int ib = 0;
+                const int jb = q + 1;
+                const double d2 = dd[q];
+                const double R0 = X[ib][0] - X[jb][0], R1 = X[ib][1] - X[jb][1], R2 = X[ib][2] - X[jb][2];
+                const double Rsq = R0 * R0 + R1 * R1 + R2 * R2;
+                const double delta = fabs(Rsq - d2) * RC[q];      // |r^2 - d^2| / d^2
+                if (delta < eps) continue;
+                finished = false;
+                const double O0 = O[ib][0] - O[jb][0], O1 = O[ib][1] - O[jb][1], O2 = O[ib][2] - O[jb][2];
+                const double RR = R0 * O0 + R1 * O1 + R2 * O2;
+                const double mi = IM[ib], mj = IM[jb];
+                const double gij = (Rsq - d2) / (2.0 * RR * (mi + mj) * dt);
+                const double G[3] = {gij * O0, gij * O1, gij * O2};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    X[ib][d] = X[ib][d] - mi * G[d] * dt;
+                    X[jb][d] = X[jb][d] + mj * G[d] * dt;
+                }
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double Gv = G[d] * rvi[d];
+                    V[ib][d] = V[ib][d] - mi * Gv;
+                    V[jb][d] = V[jb][d] + mj * Gv;
+                }
+            }
+        }
+    } else {
+        const double eps2 = eps * eps;
+        for (int it = 0; it < 300 && !finished; ++it) {
+            finished = true;
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                constexpr int ib = 0;
+                const int jb = q + 1;
+                double R[3], W[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    R[d] = X[ib][d] - X[jb][d];
+                    W[d] = V[ib][d] - V[jb][d];
+                }
+                const double RV = R[0] * W[0] + R[1] * W[1] + R[2] * W[2];
+                const double R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+                const double V2 = W[0] * W[0] + W[1] * W[1] + W[2] * W[2];
+                if (RV * RV * V2 < eps2 * R2) continue;     // (RV^2 / R^2) V^2 < eps^2, R^2 > 0
+                finished = false;
+                const double mi = IM[ib], mj = IM[jb];
+                const double kij = RV * RC[q];              // RV / (d^2 (1/m_i + 1/m_j))
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double KR = kij * R[d];
+                    V[ib][d] = V[ib][d] - mi * KR;
+                    V[jb][d] = V[jb][d] + mj * KR;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a <= K; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (POS) pos[3 * (size_t)at[a] + d] = X[a][d];
+            vel[3 * (size_t)at[a] + d] = V[a][d];
+        }
+    if (!finished) atomicOr(status, POS ? ST_RATTLE_NOCONV : ST_RATTLEV_NOCONV);
+}
+
+// seg: first group with K = 3, 2, 1 and the group count (groups sorted by K
+// from 4 down, so a warp's groups mostly share K)
+template <bool POS>
+__global__ void __launch_bounds__(128) k_rattle_star(double* __restrict__ pos, double* __restrict__ vel,
+                                                     const double* __restrict__ old, const double* __restrict__ invm,
+                                                     const int* __restrict__ sa, const double* __restrict__ sd,
+                                                     int4 seg, double eps, double dt, int use_rv,
+                                                     const DynState* __restrict__ dyn, unsigned* status) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= seg.w) return;
+    double rvi[3] = {1.0, 1.0, 1.0};
+    if (POS && use_rv) { rvi[0] = dyn->rvinv[0]; rvi[1] = dyn->rvinv[1]; rvi[2] = dyn->rvinv[2]; }
+    if (g < seg.x) rattle_star_group<POS, 4>(g, pos, vel, old, invm, sa, sd, eps, dt, rvi, status);
+    else if (g < seg.y) rattle_star_group<POS, 3>(g, pos, vel, old, invm, sa, sd, eps, dt, rvi, status);
+    else if (g < seg.z) rattle_star_group<POS, 2>(g, pos, vel, old, invm, sa, sd, eps, dt, rvi, status);
+    else rattle_star_group<POS, 1>(g, pos, vel, old, invm, sa, sd, eps, dt, rvi, status);
+}
+
+static void rattle_star_launch(pgk_ctx* c, bool pos, double eps, double dt, bool use_rv) {
+    const int blocks = (c->nstar + 127) / 128;
+    const int4 seg = make_int4(c->star_seg[0], c->star_seg[1], c->star_seg[2], c->star_seg[3]);
+    if (pos)
+        k_rattle_star<true><<<blocks, 128, 0, c->st>>>(c->pos, c->vel, c->pos_old, c->invmass, c->star_atoms,
+                                                       c->star_d, seg, eps, dt, use_rv ? 1 : 0, c->dyn, c->status);
+    else
+        k_rattle_star<false><<<blocks, 128, 0, c->st>>>(c->pos, c->vel, nullptr, c->invmass, c->star_atoms,
+                                                        c->star_d, seg, eps, 0.0, 0, c->dyn, c->status);
+    PGK_LAUNCHED(c);
+}
+
 static void rattle_rigid3_launch(pgk_ctx* c, bool pos, double eps, double dt, bool use_rv) {
     const int blocks = (c->nr3 + 127) / 128;
     if (pos)
@@ -790,6 +920,7 @@ static void rattle_warp_launch(pgk_ctx* c, bool pos, double eps, double dt, bool
 
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
     if (c->nr3 > 0) rattle_rigid3_launch(c, true, eps, dt, use_rv);
+    if (c->nstar > 0) rattle_star_launch(c, true, eps, dt, use_rv);
     if (c->ncgroup == 0) { PGK_CUDA(c, cudaGetLastError()); return PGK_OK; }
     if (c->cg_nfit > 0) rattle_warp_launch(c, true, eps, dt, use_rv);
     if (c->cg_nfit < (c->ncgroup + 31) / 32) {
@@ -805,6 +936,7 @@ pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rv) {
 
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
     if (c->nr3 > 0) rattle_rigid3_launch(c, false, eps, 0.0, false);
+    if (c->nstar > 0) rattle_star_launch(c, false, eps, 0.0, false);
     if (c->ncgroup == 0) { PGK_CUDA(c, cudaGetLastError()); return PGK_OK; }
     if (c->cg_nfit > 0) rattle_warp_launch(c, false, eps, 0.0, false);
     if (c->cg_nfit < (c->ncgroup + 31) / 32) {

@@ -566,6 +566,46 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
                 gi.swap(gi2);
                 gl.swap(gl2);
             }
+            // Star groups: K <= 4 constraints (c, a_1) ... (c, a_K) with one
+            // first atom c and K distinct second atoms (the X-H bonds of one
+            // heavy atom after the component split), sorted by K descending.
+            {
+                std::vector<int> sa[5];
+                std::vector<double> sd[5];
+                std::vector<int> gi2(1, 0), gl2;
+                for (int g = 0; g + 1 < (int)gi.size(); ++g) {
+                    const int K = gi[g + 1] - gi[g];
+                    bool star = K >= 1 && K <= 4;
+                    const int ctr = star ? cij[gl[gi[g]]].x : -1;
+                    for (int q = 0; star && q < K; ++q) {
+                        const int2 p2 = cij[gl[gi[g] + q]];
+                        star = p2.x == ctr && p2.y != ctr;
+                        for (int r = 0; star && r < q; ++r) star = cij[gl[gi[g] + r]].y != p2.y;
+                    }
+                    if (star) {
+                        sa[K].push_back(ctr);
+                        for (int q = 0; q < 4; ++q) {
+                            sa[K].push_back(q < K ? cij[gl[gi[g] + q]].y : -1);
+                            sd[K].push_back(q < K ? cd[gl[gi[g] + q]] : 0.0);
+                        }
+                        continue;
+                    }
+                    gl2.insert(gl2.end(), gl.begin() + gi[g], gl.begin() + gi[g + 1]);
+                    gi2.push_back((int)gl2.size());
+                }
+                std::vector<int> atoms;
+                std::vector<double> dls;
+                for (int K = 4; K >= 1; --K) {
+                    if (K < 4) c->star_seg[3 - K] = (int)(atoms.size() / 5);
+                    atoms.insert(atoms.end(), sa[K].begin(), sa[K].end());
+                    dls.insert(dls.end(), sd[K].begin(), sd[K].end());
+                }
+                c->nstar = (int)(atoms.size() / 5);
+                c->star_seg[3] = c->nstar;
+                if (c->nstar) { TRY(upload(c, &c->star_atoms, atoms)); TRY(upload(c, &c->star_d, dls)); }
+                gi.swap(gi2);
+                gl.swap(gl2);
+            }
             c->ncgroup = (int)gi.size() - 1;
             std::vector<int2> span(c->ncgroup);
             for (int g = 0; g < c->ncgroup; ++g) {
@@ -685,7 +725,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out, c->ewk_seg,
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
-                    c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d};
+                    c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d, c->star_atoms, c->star_d};
     for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamDestroy(c->st2);
@@ -1094,7 +1134,7 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
 static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdparams* md, bool ene, bool vir,
                                bool tens, bool hfs, bool lt, bool ke_ready) {
     const double dts = md->dt_long_cal / (double)md->nstep_short;
-    const bool rattle = md->ifrattle && (c->ncgroup > 0 || c->nr3 > 0);
+    const bool rattle = md->ifrattle && (c->ncgroup > 0 || c->nr3 > 0 || c->nstar > 0);
     const bool mtk = kind == 2;
     const bool hfdrv = kind == 3;
     const int chain_kind = kind == 1 ? 1 : (md->pcont_axis == PGK_PCONT_ISO ? 2 : 3);

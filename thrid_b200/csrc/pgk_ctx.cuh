@@ -117,6 +117,13 @@ struct pgk_ctx {
     int nr3 = 0;
     int4* r3_atoms = nullptr;     // (a0, a1, a2, -)
     double4* r3_d = nullptr;      // constraint lengths (d01, d02, d12, -)
+    // star groups: constraints (c, a1), (c, a2), ... (c, aK), K <= 4 (X-H
+    // bonds of one heavy atom), sorted by K from 4 down to 1, run by
+    // k_rattle_star with their state in registers
+    int nstar = 0;
+    int star_seg[4] = {0, 0, 0, 0};   // first group with K = 3, 2, 1; [3] = nstar
+    int* star_atoms = nullptr;    // [nstar][5]: c, a1..a4 (unused arms -1)
+    double* star_d = nullptr;     // [nstar][4] constraint lengths
 
     // ---- pair list ----
     int maxcells = 0;
