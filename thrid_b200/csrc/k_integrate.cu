@@ -210,19 +210,24 @@ struct ChainArgs {
     int kind;          // 1 nhcint, 2 nhcpisoint, 3 nhcpanisoint
 };
 
-__device__ void chain_tail(ChainDev& c, const pgk_mdparams& md, double* glogs, double w4, double w8, double gkt,
-                           bool down) {
-    int M = md.mchain;
+// The chain length M is a template parameter (mchain is checked to be 2..8
+// before any launch), so the loops over the chain unroll and the chain's
+// variables stay in registers through the serial update.
+template <int M>
+__device__ __forceinline__ void chain_tail(ChainDev& c, const pgk_mdparams& md, double* glogs, double w4,
+                                           double w8, double gkt, bool down) {
     const double* q = md.qmass;
     if (down) {
         glogs[M - 1] = (q[M - 2] * c.vlogs[M - 2] * c.vlogs[M - 2] - gkt) / q[M - 1];
         c.vlogs[M - 1] = c.vlogs[M - 1] + glogs[M - 1] * w4;
+#pragma unroll
         for (int i = M - 2; i >= 1; --i) {
             glogs[i] = (q[i - 1] * c.vlogs[i - 1] * c.vlogs[i - 1] - gkt) / q[i];
             double e8 = exp(-1.0 * w8 * c.vlogs[i + 1]);
             c.vlogs[i] = c.vlogs[i] * e8 * e8 + w4 * glogs[i] * e8;
         }
     } else {
+#pragma unroll
         for (int i = 1; i <= M - 2; ++i) {
             glogs[i] = (q[i - 1] * c.vlogs[i - 1] * c.vlogs[i - 1] - gkt) / q[i];
             double e8 = exp(-1.0 * w8 * c.vlogs[i + 1]);
@@ -233,10 +238,10 @@ __device__ void chain_tail(ChainDev& c, const pgk_mdparams& md, double* glogs, d
     }
 }
 
-__device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restrict__ acc, const ChainArgs& a) {
+template <int M>
+__device__ void chain_run_m(ChainDev* __restrict__ chain, const long long* __restrict__ acc, const ChainArgs& a) {
     ChainDev c = *chain;
     const pgk_mdparams& md = a.md;
-    int M = md.mchain;
     double dt = md.dt_long_cal;
     double kint = acc_get(acc, A_KE, a.dbl != 0);
     double glogs[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -247,12 +252,13 @@ __device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restr
         for (int inc = 0; inc < md.next; ++inc)
             for (int iy = 0; iy < md.nyosh; ++iy) {
                 double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
-                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, true);
                 double e8 = exp(-1.0 * w8 * c.vlogs[1]);
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
+#pragma unroll
                 for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
-                chain_tail(c, md, glogs, w4, w8, gkt, false);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, false);
             }
     } else if (a.kind == 2) {   // nhcpisoint.F90:6-162
         double gn1kt = md.text * (double)(a.degfree + 1);
@@ -263,17 +269,18 @@ __device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restr
         for (int inc = 0; inc < md.next; ++inc)
             for (int iy = 0; iy < md.nyosh; ++iy) {
                 double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
-                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, true);
                 double e8 = exp(-1.0 * w8 * c.vlogs[1]);
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
                 e8 = exp(-1.0 * w8 * c.vlogs[0]);
                 c.vlogv = c.vlogv * e8 * e8 + w4 * glogv * e8;
+#pragma unroll
                 for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
                 c.vlogv = c.vlogv * e8 * e8 + w4 * glogv * e8;
                 glogs[0] = (kint + md.vmass * c.vlogv * c.vlogv - gn1kt) / md.qmass[0];
                 e8 = exp(-1.0 * w8 * c.vlogs[1]);
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
-                chain_tail(c, md, glogs, w4, w8, gkt, false);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, false);
             }
     } else {   // nhcpanisoint.F90:8-189
         int dir = md.pcont_axis == PGK_PCONT_ANISO ? 0 : md.pcont_axis - 1;
@@ -288,12 +295,13 @@ __device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restr
         for (int inc = 0; inc < md.next; ++inc)
             for (int iy = 0; iy < md.nyosh; ++iy) {
                 double w2 = md.yscoeff[iy] * dt / (double)md.next / 2.0, w4 = w2 / 2.0, w8 = w4 / 2.0;
-                chain_tail(c, md, glogs, w4, w8, gkt, true);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, true);
                 double e8 = exp(-1.0 * w8 * c.vlogs[1]);
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
                 e8 = exp(-1.0 * w8 * c.vlogs[0]);
                 for (int d = 0; d < 3; ++d)
                     if (dir == 0 || d == dir - 1) c.vboxg[d] = c.vboxg[d] * e8 * e8 + w4 * gb[d] * e8;
+#pragma unroll
                 for (int i = 0; i < M; ++i) c.xlogs[i] = c.xlogs[i] + c.vlogs[i] * w2;
                 for (int d = 0; d < 3; ++d)
                     if (dir == 0 || d == dir - 1) c.vboxg[d] = c.vboxg[d] * e8 * e8 + w4 * gb[d] * e8;
@@ -301,10 +309,22 @@ __device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restr
                 glogs[0] = (kint + md.vmass * vb2 - gndfkt) / md.qmass[0];
                 e8 = exp(-1.0 * w8 * c.vlogs[1]);
                 c.vlogs[0] = c.vlogs[0] * e8 * e8 + w4 * glogs[0] * e8;
-                chain_tail(c, md, glogs, w4, w8, gkt, false);
+                chain_tail<M>(c, md, glogs, w4, w8, gkt, false);
             }
     }
     *chain = c;
+}
+
+__device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restrict__ acc, const ChainArgs& a) {
+    switch (a.md.mchain) {
+        case 2: chain_run_m<2>(chain, acc, a); break;
+        case 3: chain_run_m<3>(chain, acc, a); break;
+        case 4: chain_run_m<4>(chain, acc, a); break;
+        case 5: chain_run_m<5>(chain, acc, a); break;
+        case 6: chain_run_m<6>(chain, acc, a); break;
+        case 7: chain_run_m<7>(chain, acc, a); break;
+        default: chain_run_m<8>(chain, acc, a); break;
+    }
 }
 
 __global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs a) {

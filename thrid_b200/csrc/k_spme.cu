@@ -293,13 +293,17 @@ struct FftStages<T, T2, NC, 12> {
 };
 
 // influence function of one grid point (scalar_sum, fft_pme.F90:590-680)
+// K1f > 0: the grid holds the k1 = 0 .. K1f/2 half of the spectrum of a real
+// grid of K1f x-points (real-to-complex x transform); the energy and virial
+// sums then count every point with 0 < k1 < K1f/2 twice (it stands for k and
+// its mirror -k, with the same |S|^2 and the same products h_a h_b).
 struct ConvArgs {
-    const double* bsp; double alpha, netchrgsq; int corr; long long* acc; int want;
+    const double* bsp; double alpha, netchrgsq; int corr; long long* acc; int want; int K1f;
 };
 
 __device__ __forceinline__ double conv_point(int k1, int k2, int k3, int K1, int K2, int K3, double s2,
                                              const ConvArgs& ca, const DynState* __restrict__ dyn, double& en,
-                                             double& vs, double* vt) {
+                                             double& vs, double* vt, double w = 1.0) {
     const double pi = 3.14159265358979323846;
     int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
     int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
@@ -317,10 +321,10 @@ __device__ __forceinline__ double conv_point(int k1, int k2, int k3, int K1, int
     double eterm = ex / denom;
     if (ca.want) {
         double vterm = 2.0 * (fac * msq + 1.0) / msq;
-        double es = eterm * s2;
+        double es = eterm * s2 * w;
         en += es;
         if (ca.corr) {
-            double e2 = ex * ca.netchrgsq / (pi * vol * msq);
+            double e2 = ex * ca.netchrgsq / (pi * vol * msq) * w;
             vs += e2 * (-1.0 + 2.0 * fac * msq);
             es -= e2;
         }
@@ -341,7 +345,7 @@ struct ConvF { float bi[3], rk2, fac, pivol; };
 
 __device__ __forceinline__ float conv_point_f(int k1, int k2, int k3, int K1, int K2, int K3, float s2,
                                               const ConvArgs& ca, const ConvF& cf, double& en, double& vs,
-                                              double* vt) {
+                                              double* vt, float w = 1.f) {
     int nf1 = K1 / 2; if (2 * nf1 < K1) ++nf1;
     int nf2 = K2 / 2; if (2 * nf2 < K2) ++nf2;
     int nf3 = K3 / 2; if (2 * nf3 < K3) ++nf3;
@@ -356,10 +360,10 @@ __device__ __forceinline__ float conv_point_f(int k1, int k2, int k3, int K1, in
     const float eterm = ex / denom;
     if (ca.want) {
         const float vterm = 2.f * (cf.fac * msq + 1.f) / msq;
-        float es = eterm * s2;
+        float es = eterm * s2 * w;
         en += (double)es;
         if (ca.corr) {
-            const float e2 = ex * (float)ca.netchrgsq / (cf.pivol * msq);
+            const float e2 = ex * (float)ca.netchrgsq / (cf.pivol * msq) * w;
             vs += (double)(e2 * (-1.f + 2.f * cf.fac * msq));
             es -= e2;
         }
@@ -460,21 +464,23 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
             cf.fac = (float)(pi * pi / (ca.alpha * ca.alpha));
             cf.pivol = (float)(pi * dyn->box[0] * dyn->box[1] * dyn->box[2]);
         }
+        const int K1f = ca.K1f > 0 ? ca.K1f : K1;       // x points of the real grid
         for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
             int p = idx / n, m = idx - p * n;
             const int sidx = p * ld + m;
             int k1 = x0 + p;
             if (k1 >= K1) continue;
             if (k1 == 0 && yz == 0 && m == 0) continue;   // m = 0 is skipped by scalar_sum
+            const int w = (ca.K1f > 0 && k1 > 0 && 2 * k1 != ca.K1f) ? 2 : 1;
             T2 v = src[sidx];
             if (sizeof(T) == 4) {
-                const float et = conv_point_f(k1, yz, m, K1, K2, K3, (float)v.x * (float)v.x + (float)v.y * (float)v.y,
-                                              ca, cf, en, vs, vt);
+                const float et = conv_point_f(k1, yz, m, K1f, K2, K3, (float)v.x * (float)v.x + (float)v.y * (float)v.y,
+                                              ca, cf, en, vs, vt, (float)w);
                 v.x = (T)((float)v.x * et);
                 v.y = (T)((float)v.y * et);
             } else {
                 double s2 = (double)v.x * (double)v.x + (double)v.y * (double)v.y;
-                double et = conv_point(k1, yz, m, K1, K2, K3, s2, ca, dyn, en, vs, vt);
+                double et = conv_point(k1, yz, m, K1f, K2, K3, s2, ca, dyn, en, vs, vt, (double)w);
                 v.x = (T)((double)v.x * et);
                 v.y = (T)((double)v.y * et);
             }
@@ -498,6 +504,103 @@ __global__ void __launch_bounds__(256) k_fft(typename C2<T>::t* __restrict__ dat
             size_t off = AXIS == 0 ? base + (size_t)p * K1 + m : base + p + stride * m;
             if (SRC == 3) ((T*)acc)[off] = src[p * ld + m].x;     // real part only (what the gather reads)
             else data[off] = src[p * ld + m];
+        }
+    }
+}
+
+// Real-to-complex x pass (FWD) and its complex-to-real inverse, on x lines of
+// a real grid of K1 = 2N points.  Forward: the line's even and odd points are
+// taken as one complex sequence z_n = x_2n + i x_2n+1 (n < N), transformed by
+// the length-N pencil FFT (exp(-2 pi i nk/N)), and split:
+//   E_k = (Z_k + conj Z_{N-k}) / 2,  O_k = (Z_k - conj Z_{N-k}) / 2i,
+//   X_k = E_k + exp(-2 pi i k / K1) O_k,  k = 0..N,
+// the k1 = 0..K1/2 half of the line's spectrum (the other half is its complex
+// conjugate mirror), stored with pitch N + 1.  Inverse (unnormalised,
+// exp(+2 pi i)): from a Hermitian half spectrum Y_0..Y_N,
+//   A_k = Y_k + conj Y_{N-k},  B_k = (Y_k - conj Y_{N-k}) exp(+2 pi i k / K1),
+//   z = length-N inverse FFT of A + iB,  y_2n = Re z_n,  y_2n+1 = Im z_n,
+// written to the real grid that the gather reads.  SRC (forward): 1 = int64
+// fixed-point accumulation grid, 2 = double accumulation grid.
+template <typename T, int SRC, int NC, bool FWD>
+__global__ void __launch_bounds__(256) k_fft_rx(typename C2<T>::t* __restrict__ data, void* __restrict__ real,
+                                                int K1, int nline, FftDev plan, const void* __restrict__ tw2g,
+                                                int P) {
+    typedef typename C2<T>::t T2;
+    extern __shared__ unsigned char smraw[];
+    const int N = NC > 0 ? NC : plan.n;
+    const int ld = N + 1;
+    const int K1h = N + 1;
+    T2* bufA = (T2*)smraw;
+    T2* bufB = bufA + P * ld;
+    T2* tws = bufB + P * ld;              // length-N twiddles
+    T2* tw2 = tws + N;                    // exp(-2 pi i k / K1), k = 0..N
+    for (int k = threadIdx.x; k < N; k += blockDim.x) tws[k] = ((const T2*)plan.tw)[k];
+    for (int k = threadIdx.x; k <= N; k += blockDim.x) tw2[k] = ((const T2*)tw2g)[k];
+    const int line0 = blockIdx.x * P;
+    if (FWD) {
+        for (int idx = threadIdx.x; idx < P * N; idx += blockDim.x) {
+            const int p = idx / N, m = idx - p * N;
+            T2 v; v.x = 0; v.y = 0;
+            if (line0 + p < nline) {
+                const size_t off = (size_t)(line0 + p) * K1 + 2 * m;
+                if (SRC == 1) {
+                    const longlong2 q = *(const longlong2*)((const long long*)real + off);
+                    v.x = (T)((double)q.x * PGK_GRID_ISCALE);
+                    v.y = (T)((double)q.y * PGK_GRID_ISCALE);
+                } else {
+                    const double2 q = *(const double2*)((const double*)real + off);
+                    v.x = (T)q.x;
+                    v.y = (T)q.y;
+                }
+            }
+            bufA[p * ld + m] = v;
+        }
+        __syncthreads();
+        T2* src = bufA;
+        T2* dst = bufB;
+        FftStages<T, T2, NC>::run(src, dst, P, N, plan, T(-1), tws);
+        for (int idx = threadIdx.x; idx < P * K1h; idx += blockDim.x) {
+            const int p = idx / K1h, k = idx - p * K1h;
+            if (line0 + p >= nline) continue;
+            const T2 zk = src[p * ld + (k == N ? 0 : k)];
+            T2 zc = src[p * ld + (k == 0 ? 0 : N - k)];
+            zc.y = -zc.y;
+            const T2 e = cscale<T2, T>(cadd(zk, zc), T(0.5));
+            const T2 d = csub(zk, zc);
+            T2 o; o.x = T(0.5) * d.y; o.y = T(-0.5) * d.x;        // d / 2i
+            data[(size_t)(line0 + p) * K1h + k] = cadd(e, cmul(tw2[k], o));
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < P * K1h; idx += blockDim.x) {
+            const int p = idx / K1h, k = idx - p * K1h;
+            T2 v; v.x = 0; v.y = 0;
+            if (line0 + p < nline) v = data[(size_t)(line0 + p) * K1h + k];
+            bufB[p * ld + k] = v;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < P * N; idx += blockDim.x) {
+            const int p = idx / N, k = idx - p * N;
+            const T2 yk = bufB[p * ld + k];
+            T2 yc = bufB[p * ld + N - k];
+            yc.y = -yc.y;
+            const T2 a = cadd(yk, yc);
+            T2 t = tw2[k];
+            t.y = -t.y;                                           // exp(+2 pi i k / K1)
+            const T2 b = cmul(csub(yk, yc), t);
+            T2 z; z.x = a.x - b.y; z.y = a.y + b.x;               // A + iB
+            bufA[p * ld + k] = z;
+        }
+        __syncthreads();
+        T2* src = bufA;
+        T2* dst = bufB;
+        FftStages<T, T2, NC>::run(src, dst, P, N, plan, T(1), tws);
+        for (int idx = threadIdx.x; idx < P * N; idx += blockDim.x) {
+            const int p = idx / N, m = idx - p * N;
+            if (line0 + p >= nline) continue;
+            const T2 z = src[p * ld + m];
+            T* out = (T*)real + (size_t)(line0 + p) * K1 + 2 * m;
+            out[0] = z.x;
+            out[1] = z.y;
         }
     }
 }
@@ -767,26 +870,55 @@ pgk_status spme_setup(pgk_ctx* c) {
             PGK_CUDA(c, cudaMemcpy(c->plan[d].tw, tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice));
         }
     }
+    // real-to-complex x transform when K1 is even and K1/2 factors into 2, 3, 5
+    // (PGK_SPME_R2C=0: the complex x transform of the full grid)
+    c->r2c = false;
+    const char* rx = getenv("PGK_SPME_R2C");
+    if (c->K[0] % 2 == 0 && factor(c->K[0] / 2, c->plan_rx) && !(rx && atoi(rx) == 0)) {
+        const int nh = c->K[0] / 2;
+        const double pi2 = 2.0 * 3.14159265358979323846;
+        std::vector<double2> a((size_t)nh), b((size_t)nh + 1);
+        for (int m = 0; m < nh; ++m) a[m] = make_double2(std::cos(-pi2 * m / nh), std::sin(-pi2 * m / nh));
+        for (int k = 0; k <= nh; ++k) b[k] = make_double2(std::cos(-pi2 * k / c->K[0]), std::sin(-pi2 * k / c->K[0]));
+        if (c->mixed()) {
+            std::vector<float2> af(a.size()), bf(b.size());
+            for (size_t k = 0; k < a.size(); ++k) af[k] = make_float2((float)a[k].x, (float)a[k].y);
+            for (size_t k = 0; k < b.size(); ++k) bf[k] = make_float2((float)b[k].x, (float)b[k].y);
+            PGK_CUDA(c, pgk_dmalloc(c, &c->plan_rx.tw, af.size() * sizeof(float2)));
+            PGK_CUDA(c, cudaMemcpy(c->plan_rx.tw, af.data(), af.size() * sizeof(float2), cudaMemcpyHostToDevice));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->tw_rx, bf.size() * sizeof(float2)));
+            PGK_CUDA(c, cudaMemcpy(c->tw_rx, bf.data(), bf.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        } else {
+            PGK_CUDA(c, pgk_dmalloc(c, &c->plan_rx.tw, a.size() * sizeof(double2)));
+            PGK_CUDA(c, cudaMemcpy(c->plan_rx.tw, a.data(), a.size() * sizeof(double2), cudaMemcpyHostToDevice));
+            PGK_CUDA(c, pgk_dmalloc(c, &c->tw_rx, b.size() * sizeof(double2)));
+            PGK_CUDA(c, cudaMemcpy(c->tw_rx, b.data(), b.size() * sizeof(double2), cudaMemcpyHostToDevice));
+        }
+        c->r2c = true;
+    }
     return PGK_OK;
 }
 
 template <typename T, int AXIS, int SRC, int NC, bool CONV>
-static void fft_launch(pgk_ctx* c, const FftDev& fd, int grid, int P, size_t sm, int sign, const ConvArgs& ca) {
+static void fft_launch(pgk_ctx* c, const FftDev& fd, int grid, int P, size_t sm, int sign, const ConvArgs& ca,
+                       int K1) {
     typedef typename C2<T>::t T2;
     smem_limit(k_fft<T, AXIS, SRC, NC, CONV>, sm);
-    k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, SRC == 3 ? c->qr : c->qacc, c->K[0], c->K[1],
+    k_fft<T, AXIS, SRC, NC, CONV><<<grid, 256, sm, c->st>>>((T2*)c->qc, SRC == 3 ? c->qr : c->qacc, K1, c->K[1],
                                                             c->K[2], fd, P, (T)sign, ca, c->dyn);
 }
 
+// x_ext: x points of the complex grid (0: K1; K1/2 + 1 on the half spectrum of
+// the real-to-complex transform, for the y and z passes)
 template <typename T, int AXIS, int SRC, bool CONV = false>
-static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) {
+static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr, int x_ext = 0) {
     typedef typename C2<T>::t T2;
     const FftPlan& pl = c->plan[AXIS];
     FftDev fd;
     fd.n = pl.n; fd.nstage = pl.nstage;
     for (int s = 0; s < PGK_MAX_RADIX_STAGES; ++s) fd.radix[s] = pl.radix[s];
     fd.tw = pl.tw;
-    int K1 = c->K[0], K2 = c->K[1], K3 = c->K[2];
+    int K1 = x_ext > 0 ? x_ext : c->K[0], K2 = c->K[1], K3 = c->K[2];
     int P = sizeof(T) == 4 ? 16 : 8;
     if (AXIS == 0) P = std::max(1, (sizeof(T) == 4 ? 2048 : 1024) / K1);
     const int tuned = CONV ? c->fft_p[3] : c->fft_p[AXIS];   // pencils per block chosen by spme_autotune
@@ -799,12 +931,43 @@ static pgk_status fft_pass(pgk_ctx* c, int sign, const ConvArgs* cap = nullptr) 
     ConvArgs ca{};
     if (cap) ca = *cap;
     switch (pl.n) {   // compile-time lengths of the configured grids; others run the generic stage loop
-        case 32: fft_launch<T, AXIS, SRC, 32, CONV>(c, fd, grid, P, sm, sign, ca); break;
-        case 64: fft_launch<T, AXIS, SRC, 64, CONV>(c, fd, grid, P, sm, sign, ca); break;
-        case 128: fft_launch<T, AXIS, SRC, 128, CONV>(c, fd, grid, P, sm, sign, ca); break;
-        case 192: fft_launch<T, AXIS, SRC, 192, CONV>(c, fd, grid, P, sm, sign, ca); break;
-        default: fft_launch<T, AXIS, SRC, 0, CONV>(c, fd, grid, P, sm, sign, ca); break;
+        case 32: fft_launch<T, AXIS, SRC, 32, CONV>(c, fd, grid, P, sm, sign, ca, K1); break;
+        case 64: fft_launch<T, AXIS, SRC, 64, CONV>(c, fd, grid, P, sm, sign, ca, K1); break;
+        case 128: fft_launch<T, AXIS, SRC, 128, CONV>(c, fd, grid, P, sm, sign, ca, K1); break;
+        case 192: fft_launch<T, AXIS, SRC, 192, CONV>(c, fd, grid, P, sm, sign, ca, K1); break;
+        default: fft_launch<T, AXIS, SRC, 0, CONV>(c, fd, grid, P, sm, sign, ca, K1); break;
     }
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
+    return PGK_OK;
+}
+
+// the real-to-complex x pass (FWD) or its inverse on the context's grids
+template <typename T, int SRC, bool FWD>
+static pgk_status fft_rx_pass(pgk_ctx* c) {
+    typedef typename C2<T>::t T2;
+    const FftPlan& pl = c->plan_rx;
+    FftDev fd;
+    fd.n = pl.n; fd.nstage = pl.nstage;
+    for (int s = 0; s < PGK_MAX_RADIX_STAGES; ++s) fd.radix[s] = pl.radix[s];
+    fd.tw = pl.tw;
+    const int nline = c->K[1] * c->K[2];
+    int P = c->fft_p[4] > 0 ? c->fft_p[4] : std::max(1, (sizeof(T) == 4 ? 2048 : 1024) / pl.n);
+    const int grid = (nline + P - 1) / P;
+    const size_t sm = ((size_t)2 * P * (pl.n + 1) + 2 * pl.n + 1) * sizeof(T2);
+    void* real = FWD ? (void*)c->qacc : (void*)c->qr;
+#define PGK_RX(NCV)                                                                                            \
+    do {                                                                                                       \
+        smem_limit(k_fft_rx<T, SRC, NCV, FWD>, sm);                                                            \
+        k_fft_rx<T, SRC, NCV, FWD><<<grid, 256, sm, c->st>>>((T2*)c->qc, real, c->K[0], nline, fd, c->tw_rx, P); \
+    } while (0)
+    switch (pl.n) {
+        case 16: PGK_RX(16); break;
+        case 32: PGK_RX(32); break;
+        case 64: PGK_RX(64); break;
+        default: PGK_RX(0); break;
+    }
+#undef PGK_RX
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -825,12 +988,25 @@ static pgk_status fft3(pgk_ctx* c, int sign, bool first) {
 }
 
 // forward x, y; fused [forward z, influence function, backward z]; backward y, x
+// With the real-to-complex x transform: real x, y on the half spectrum,
+// [z, influence function, z backward], y backward, complex-to-real x.
 template <typename T>
 static pgk_status fft_convolve(pgk_ctx* c, long long* acc, int want) {
     pgk_status s;
     ConvArgs ca;
     ca.bsp = c->bsp; ca.alpha = c->prm.alpha; ca.netchrgsq = c->netchrgsq; ca.corr = c->prm.ifnetqcorrp;
-    ca.acc = acc; ca.want = want;
+    ca.acc = acc; ca.want = want; ca.K1f = 0;
+    if (c->r2c) {
+        const int xh = c->K[0] / 2 + 1;
+        ca.K1f = c->K[0];
+        if (sizeof(T) == 4) s = fft_rx_pass<T, 1, true>(c);
+        else s = fft_rx_pass<T, 2, true>(c);
+        if (s) return s;
+        if ((s = fft_pass<T, 1, 0>(c, -1, nullptr, xh))) return s;
+        if ((s = fft_pass<T, 2, 0, true>(c, -1, &ca, xh))) return s;
+        if ((s = fft_pass<T, 1, 0>(c, +1, nullptr, xh))) return s;
+        return fft_rx_pass<T, 0, false>(c);
+    }
     if (sizeof(T) == 4) s = fft_pass<T, 0, 1>(c, -1);
     else s = fft_pass<T, 0, 2>(c, -1);
     if (s) return s;
@@ -855,30 +1031,32 @@ struct TuneKey {
         return std::tie(k1, k2, k3, fp32) < std::tie(o.k1, o.k2, o.k3, o.fp32);
     }
 };
-struct TuneVal { int p[4]; float us[4]; };
+struct TuneVal { int p[5]; float us[5]; };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal> g_tune;
 
+// x_ext: as fft_pass (the half spectrum's width for the y and z passes of the
+// real-to-complex transform)
 template <typename T, int AXIS, int SRC, bool CONV>
-static pgk_status tune_axis(pgk_ctx* c, int slot, int& best, float& best_us) {
+static pgk_status tune_axis(pgk_ctx* c, int slot, int& best, float& best_us, int x_ext = 0) {
     typedef typename C2<T>::t T2;
     const int n = c->K[AXIS];
-    const int npen = AXIS == 0 ? c->K[1] * c->K[2] : c->K[0];
+    const int npen = AXIS == 0 ? c->K[1] * c->K[2] : (x_ext > 0 ? x_ext : c->K[0]);
     cudaEvent_t e0, e1;
     PGK_CUDA(c, cudaEventCreate(&e0));
     PGK_CUDA(c, cudaEventCreate(&e1));
     ConvArgs ca{};
     ca.bsp = c->bsp; ca.alpha = c->prm.alpha; ca.netchrgsq = c->netchrgsq; ca.corr = c->prm.ifnetqcorrp;
-    ca.acc = c->acc; ca.want = 0;
+    ca.acc = c->acc; ca.want = 0; ca.K1f = x_ext > 0 ? c->K[0] : 0;
     best = 0; best_us = 1e30f;
     for (int P = 1; P <= 64 && P <= npen; P *= 2) {
         if (((size_t)2 * P * (n + 1) + n) * sizeof(T2) > 160 * 1024) break;
         c->fft_p[slot] = P;
-        pgk_status s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr);    // warm-up (and smem limit)
+        pgk_status s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr, x_ext);   // warm-up (and smem limit)
         if (s) return s;
         PGK_CUDA(c, cudaEventRecord(e0, c->st));
         for (int r = 0; r < 3; ++r)
-            if ((s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr))) return s;
+            if ((s = fft_pass<T, AXIS, SRC, CONV>(c, -1, CONV ? &ca : nullptr, x_ext))) return s;
         PGK_CUDA(c, cudaEventRecord(e1, c->st));
         PGK_CUDA(c, cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -892,12 +1070,47 @@ static pgk_status tune_axis(pgk_ctx* c, int slot, int& best, float& best_us) {
     return PGK_OK;
 }
 
+// the real-to-complex x pass (forward; the inverse uses the same shape)
+template <typename T>
+static pgk_status tune_rx(pgk_ctx* c, int& best, float& best_us) {
+    typedef typename C2<T>::t T2;
+    const int n = c->plan_rx.n, npen = c->K[1] * c->K[2];
+    cudaEvent_t e0, e1;
+    PGK_CUDA(c, cudaEventCreate(&e0));
+    PGK_CUDA(c, cudaEventCreate(&e1));
+    best = 0; best_us = 1e30f;
+    for (int P = 1; P <= 64 && P <= npen; P *= 2) {
+        if (((size_t)2 * P * (n + 1) + 2 * n + 1) * sizeof(T2) > 160 * 1024) break;
+        c->fft_p[4] = P;
+        pgk_status s = sizeof(T) == 4 ? fft_rx_pass<T, 1, true>(c) : fft_rx_pass<T, 2, true>(c);
+        if (s) return s;
+        PGK_CUDA(c, cudaEventRecord(e0, c->st));
+        for (int r = 0; r < 3; ++r)
+            if ((s = sizeof(T) == 4 ? fft_rx_pass<T, 1, true>(c) : fft_rx_pass<T, 2, true>(c))) return s;
+        PGK_CUDA(c, cudaEventRecord(e1, c->st));
+        PGK_CUDA(c, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PGK_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+        const float us = ms * 1e3f / 3.f;
+        if (us < best_us) { best_us = us; best = P; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->fft_p[4] = best;
+    return PGK_OK;
+}
+
 template <typename T>
 static pgk_status autotune_fft(pgk_ctx* c, TuneVal& v) {
     pgk_status s;
-    if ((s = tune_axis<T, 0, 0, false>(c, 0, v.p[0], v.us[0])) || (s = tune_axis<T, 1, 0, false>(c, 1, v.p[1], v.us[1])) ||
-        (s = tune_axis<T, 2, 0, false>(c, 2, v.p[2], v.us[2])) || (s = tune_axis<T, 2, 0, true>(c, 3, v.p[3], v.us[3])))
+    const int xh = c->r2c ? c->K[0] / 2 + 1 : 0;     // the y and z passes run on the half spectrum
+    if ((s = tune_axis<T, 0, 0, false>(c, 0, v.p[0], v.us[0])) ||
+        (s = tune_axis<T, 1, 0, false>(c, 1, v.p[1], v.us[1], xh)) ||
+        (s = tune_axis<T, 2, 0, false>(c, 2, v.p[2], v.us[2], xh)) ||
+        (s = tune_axis<T, 2, 0, true>(c, 3, v.p[3], v.us[3], xh)))
         return s;
+    v.p[4] = 0; v.us[4] = 0.f;
+    if (c->r2c && (s = tune_rx<T>(c, v.p[4], v.us[4]))) return s;
     return PGK_OK;
 }
 
@@ -905,22 +1118,23 @@ static pgk_status autotune_fft(pgk_ctx* c, TuneVal& v) {
 // its grid shape, measured now if there is none yet (PGK_AUTOTUNE=0: the
 // fixed defaults).  Runs at context set-up, outside any stream capture.
 pgk_status spme_autotune(pgk_ctx* c) {
-    for (int q = 0; q < 4; ++q) c->fft_p[q] = 0;
+    for (int q = 0; q < 5; ++q) c->fft_p[q] = 0;
     const char* env = getenv("PGK_AUTOTUNE");
     if ((env && atoi(env) == 0) || !c->prm.ifspme) return PGK_OK;
-    const TuneKey key{c->K[0], c->K[1], c->K[2], c->mixed() ? 1 : 0};
+    const TuneKey key{c->K[0], c->K[1], c->K[2], (c->mixed() ? 1 : 0) | (c->r2c ? 2 : 0)};
     std::lock_guard<std::mutex> lk(g_tune_mu);     // contexts of one grid shape share one measurement
     auto it = g_tune.find(key);
     if (it == g_tune.end()) {
         TuneVal v{};
         PGK_CUDA(c, cudaMemsetAsync(c->qc, 0, (size_t)c->K[0] * c->K[1] * c->K[2] * (c->mixed() ? 8 : 16), c->st));
+        PGK_CUDA(c, cudaMemsetAsync(c->qacc, 0, (size_t)c->K[0] * c->K[1] * c->K[2] * 8, c->st));
         pgk_status s = c->mixed() ? autotune_fft<float>(c, v) : autotune_fft<double>(c, v);
         if (s) return s;
         PGK_CUDA(c, cudaMemsetAsync(c->acc, 0, sizeof(long long) * 2 * NACC, c->st));
         PGK_CUDA(c, cudaStreamSynchronize(c->st));
         it = g_tune.emplace(key, v).first;
     }
-    for (int q = 0; q < 4; ++q) c->fft_p[q] = it->second.p[q];
+    for (int q = 0; q < 5; ++q) c->fft_p[q] = it->second.p[q];
     return PGK_OK;
 }
 
@@ -930,12 +1144,14 @@ extern "C" int64_t pgk_tuning_table(char* buf, int64_t cap) {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         for (auto& kv : g_tune) {
             char line[256];
+            char rx[64] = "";
+            if (kv.first.fp32 & 2) snprintf(rx, sizeof(rx), " real-x %d (%.1f us)", kv.second.p[4], kv.second.us[4]);
             snprintf(line, sizeof(line),
                      "spme %dx%dx%d %s: pencils per block x %d (%.1f us) y %d (%.1f us) z %d (%.1f us) "
-                     "z+influence %d (%.1f us)\n",
-                     kv.first.k1, kv.first.k2, kv.first.k3, kv.first.fp32 ? "fp32" : "fp64", kv.second.p[0],
+                     "z+influence %d (%.1f us)%s\n",
+                     kv.first.k1, kv.first.k2, kv.first.k3, (kv.first.fp32 & 1) ? "fp32" : "fp64", kv.second.p[0],
                      kv.second.us[0], kv.second.p[1], kv.second.us[1], kv.second.p[2], kv.second.us[2],
-                     kv.second.p[3], kv.second.us[3]);
+                     kv.second.p[3], kv.second.us[3], rx);
             t += line;
         }
     }

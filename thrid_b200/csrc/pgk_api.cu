@@ -725,7 +725,8 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out, c->ewk_seg,
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
-                    c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d, c->star_atoms, c->star_d};
+                    c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d, c->star_atoms, c->star_d, c->plan_rx.tw,
+                    c->tw_rx};
     for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamDestroy(c->st2);

@@ -165,7 +165,13 @@ struct pgk_ctx {
     void* qr = nullptr;           // real part after the backward transform (float / double), read by the gather
     double* bsp = nullptr;        // bsp_mod1|2|3
     FftPlan plan[3];
-    int fft_p[4] = {0, 0, 0, 0};  // pencils per block of the x, y, z and z+influence passes (0: default)
+    // real-to-complex x transform (K1 even, K1/2 a product of 2, 3, 5): the
+    // complex grid holds K1/2 + 1 points per x line; plan_rx is the length-
+    // K1/2 complex transform, tw_rx the K1/2 + 1 factors exp(-2 pi i k / K1)
+    bool r2c = false;
+    FftPlan plan_rx;
+    void* tw_rx = nullptr;
+    int fft_p[5] = {0, 0, 0, 0, 0};  // pencils per block: x, y, z, z+influence, real x (0: default)
 
     // ---- Morse pairs (k_morse.cu): own list (radius rcut_bookmor) and kernel ----
     int nmor = 0;                 // Morse atoms (0: no Morse pairs or Morse switched off)
