@@ -186,6 +186,36 @@ def test_mixed_forces_within_1e5(oracle_mod, name):
     assert rel_rms(f1 + f2 + f3, rf + kf + bf) < MIXED_FORCE
 
 
+@pytest.mark.parametrize("nfft", [(20, 16, 24), (15, 16, 16)])
+def test_spme_real_transform_matches_complex(oracle_mod, monkeypatch, nfft):
+    """The SPME convolution with the real-to-complex x transform (half
+    spectrum, mirrored points counted twice in the energy and virial) equals
+    the complex transform of the full grid and the oracle's fft_pmep, in FP64
+    (<= 1e-12) and in mixed precision (<= 1e-5); an odd K1 (15) runs the
+    complex transform whatever the switch says."""
+    s = S.small_box("propanol", nside=4, spacing=5.6)
+    s.params.update(nfft1=nfft[0], nfft2=nfft[1], nfft3=nfft[2])
+    o = oracle_for(oracle_mod, s)
+    o.mklist()
+    kf, ke, kv = o.fft_pmep()
+    res = {}
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        for r2c in ("1", "0"):
+            monkeypatch.setenv("PGK_SPME_R2C", r2c)
+            e = engine(s, prec)
+            e.mklist_cell()
+            res[(prec, r2c)] = e.fft_pme()
+            e.close()
+    for prec, tol in ((abi.PREC_FP64, FP64_FORCE), (abi.PREC_MIXED, MIXED_FORCE)):
+        (f1, e1, v1), (f0, e0, v0) = res[(prec, "1")], res[(prec, "0")]
+        assert rel_rms(f1, kf) < tol and rel_rms(f0, kf) < tol
+        assert rel_rms(f1, f0) < tol
+        assert erel(e1["pot_ewk"], ke["pot_ewk"]) < (FP64_ENERGY if prec == abi.PREC_FP64 else MIXED_ENERGY)
+        vt = np.abs(kv["pot_virit_coul"]).max()
+        assert np.abs(v1["pot_virit_coul"] - kv["pot_virit_coul"]).max() < (1e-9 if prec == abi.PREC_FP64 else 1e-5) * vt
+        assert np.abs(v1["pot_virit_coul"] - v0["pot_virit_coul"]).max() < (1e-9 if prec == abi.PREC_FP64 else 1e-5) * vt
+
+
 def test_calforce_mts_groups(oracle_mod):
     s = case("propanol_small")
     over = dict(mts_bond=abi.MTS_SHORT, mts_angl=abi.MTS_SHORT, mts_tors=abi.MTS_SHORT,
