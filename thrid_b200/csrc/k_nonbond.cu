@@ -100,6 +100,7 @@ struct PairArgs {
     // FP32 copies for the mixed kernel, read straight from the parameter
     // bank inside the pair loop (no registers held for them)
     float rr2f, rl2f, inv_hf, hf; int nsplm1;
+    float ew_pa, ew_c2a, ew_mk;        // analytic real-space Ewald (EwaldF)
     void* facc; long long* acc;
     long long* fsort; int fstride;     // mixed: forces by sorted slot (SoA, stride fstride)
     // pruned rows (mixed; P null = none): on a prune step (P->do_prune) the
@@ -108,6 +109,58 @@ struct PairArgs {
     // xq_prune; otherwise it reads plist/pcnt
     const PruneDev* P; const int* blist; const int* bcnt; int* plist; int* pcnt; int4* xq_prune; float rp2;
 };
+
+// ---- real-space Ewald force without a table (mixed precision) -----------------
+// The screened Coulomb force per unit charge product, divided by r,
+//   erfc(a r)/r^3 + (2a/sqrt(pi)) exp(-a^2 r^2)/r^2   (a = alpha),
+// with erfc(x) = t (c1 + t (c2 + t (c3 + t (c4 + t c5)))) exp(-x^2) and
+// t = 1/(1 + p x): Hastings' rational approximation as given in Abramowitz &
+// Stegun, Handbook of Mathematical Functions, 7.1.26 (absolute error of erfc
+// <= 1.5e-7).  Evaluated in FP32 (rcp, ex2 on the MUFU unit), the force is
+// within 6e-7 of the FP64 value on the scale of the bare Coulomb force 1/r^2
+// for 0.8 <= r <= 14 A and 0.28 <= a <= 0.40; where erfc(a r) is small the
+// pair force is small too.  The packed cluster-frame body uses it instead of
+// the spline-table fetch of the force, whose random rows cost shared-memory
+// bank conflicts in every evaluation (0.358 -> 0.300 ms per evaluation on the
+// 200k butane rows); the reference's spline tables (spline_interp.F90) still
+// give the Coulomb energy on the steps that need energies, the force of the
+// scalar body (small boxes, where the table measured faster) and the FP64
+// path.
+struct EwaldF { float pa, c2a, mk; };      // p a, 2a/sqrt(pi), -a^2 log2(e)
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+#define AS_P 0.3275911f
+#define AS_C1 0.254829592f
+#define AS_C2 -0.284496736f
+#define AS_C3 1.421413741f
+#define AS_C4 -1.453152027f
+#define AS_C5 1.061405429f
+__device__ __forceinline__ float2 ewald_force2(float2 r, float2 r2, float2 rinv, float2 rinv2, const EwaldF& ew) {
+    const float2 den = __ffma2_rn(r, make_float2(ew.pa, ew.pa), make_float2(1.f, 1.f));
+    const float2 t = make_float2(rcp_ftz(den.x), rcp_ftz(den.y));
+    float2 poly = __ffma2_rn(t, make_float2(AS_C5, AS_C5), make_float2(AS_C4, AS_C4));
+    poly = __ffma2_rn(poly, t, make_float2(AS_C3, AS_C3));
+    poly = __ffma2_rn(poly, t, make_float2(AS_C2, AS_C2));
+    poly = __ffma2_rn(poly, t, make_float2(AS_C1, AS_C1));
+    poly = __fmul2_rn(poly, t);
+    const float2 xa = __fmul2_rn(r2, make_float2(ew.mk, ew.mk));
+    const float2 ex = make_float2(ex2_ftz(xa.x), ex2_ftz(xa.y));
+    const float2 ec = __fmul2_rn(poly, ex);
+    return __fmul2_rn(__ffma2_rn(ec, rinv, __fmul2_rn(make_float2(ew.c2a, ew.c2a), ex)), rinv2);
+}
 
 // ---- one pair, mixed precision -----------------------------------------------
 // Branch-free: every pair of an entry's mask is evaluated to the end and the
@@ -127,7 +180,7 @@ __device__ __forceinline__ void pair_term(const float dx, const float dy, const 
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     r2o = r2;
-    const float rinv = rsqrtf(r2);
+    const float rinv = rsqrt_ftz(r2);
     const float rinv2 = rinv * rinv;
     const float r = r2 * rinv;
     // floor(r/h) on the FP32/ALU pipes: adding 2^23 rounded toward -inf
@@ -202,7 +255,7 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     extern __shared__ float4 sm[];
     float4* sf = sm;                        // force table  (spline 0)
-    float4* sp = sm + a.nspl;               // pot table    (spline 1), ENE only
+    float4* sp = sm + a.nspl;               // energy table (spline 1), ENE only
     float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
     __shared__ int4 si[PAIR_WARPS][8];
     __shared__ int sti[PAIR_WARPS][8];
@@ -328,17 +381,11 @@ __device__ __forceinline__ void pair_mixed_body(const int4* __restrict__ xq, con
 // parameters of both atoms with j's type as (R_a^2, R_b^2, 12 eps_a,
 // 12 eps_b): fl = 12 eps (R^2/r^2)^3 ((R^2/r^2)^3 - 1) / r^2, and the LJ
 // energy 12 eps t6 (t6 - 2) is divided by 12 once per block.
-__device__ __forceinline__ float rsqrt_ftz(float x) {
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
 template <int MODE, bool SC>
 __device__ __forceinline__ void pair_term_x2(const float2 dx, const float2 dy, const float2 dz, const float2 qq,
                                              const float4 L, const unsigned mb, const float rr2,
                                              const float rl2, const float2 inv_h2, const float2 mh2,
-                                             const int nsplm1, const float4* __restrict__ sf,
+                                             const int nsplm1, const EwaldF& ew,
                                              const float4* __restrict__ sp,
                                              float2 (&fi)[3], float2& gx, float2& gy, float2& gz, float2& ev,
                                              float2& ee, float2* wc, float2* wl, float2& r2o) {
@@ -349,16 +396,7 @@ __device__ __forceinline__ void pair_term_x2(const float2 dx, const float2 dy, c
     const float2 rinv = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
     const float2 rinv2 = __fmul2_rn(rinv, rinv);
     const float2 r = __fmul2_rn(r2, rinv);
-    // floor(r/h) as in pair_term, both elements at once
-    const float2 fb = __fadd2_rd(__fmul2_rn(r, inv_h2), two23);
-    const float2 fm = __fadd2_rn(fb, mtwo23);
-    const int ia = (int)min((unsigned)(__float_as_int(fb.x) - 0x4B000000), (unsigned)nsplm1);
-    const int ib = (int)min((unsigned)(__float_as_int(fb.y) - 0x4B000000), (unsigned)nsplm1);
-    const float2 d = __ffma2_rn(fm, mh2, r);
-    const float4 ca = sf[ia], cb = sf[ib];
-    const float2 poly = make_float2(fmaf(d.x, fmaf(d.x, fmaf(d.x, ca.w, ca.z), ca.y), ca.x),
-                                    fmaf(d.y, fmaf(d.y, fmaf(d.y, cb.w, cb.z), cb.y), cb.x));
-    float2 fc = __fmul2_rn(qq, poly);
+    float2 fc = __fmul2_rn(qq, ewald_force2(r, r2, rinv, rinv2, ew));
     const float2 c12 = make_float2(L.z, L.w);
     const float2 t2 = __fmul2_rn(rinv2, make_float2(L.x, L.y));
     const float2 t6 = __fmul2_rn(__fmul2_rn(t2, t2), t2);
@@ -383,6 +421,12 @@ __device__ __forceinline__ void pair_term_x2(const float2 dx, const float2 dy, c
         fs = __fadd2_rn(fc, fl);
     }
     if (ENE) {
+        // Coulomb energy from the reference's spline (floor(r/h) as in pair_term)
+        const float2 fb = __fadd2_rd(__fmul2_rn(r, inv_h2), two23);
+        const float2 fm = __fadd2_rn(fb, mtwo23);
+        const int ia = (int)min((unsigned)(__float_as_int(fb.x) - 0x4B000000), (unsigned)nsplm1);
+        const int ib = (int)min((unsigned)(__float_as_int(fb.y) - 0x4B000000), (unsigned)nsplm1);
+        const float2 d = __ffma2_rn(fm, mh2, r);
         const bool la_in = SC ? ra : (ba && r2.x <= rl2), lb_in = SC ? rb : (bb && r2.y <= rl2);
         const float4 pa = sp[ia], pb = sp[ib];
         float2 pe = __fmul2_rn(qq, make_float2(fmaf(d.x, fmaf(d.x, fmaf(d.x, pa.w, pa.z), pa.y), pa.x),
@@ -425,22 +469,20 @@ __device__ __forceinline__ void pair_mixed_body_x2(const int4* __restrict__ xq, 
                                                    const DynState* __restrict__ dyn) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     extern __shared__ float4 sm[];
-    float4* sf = sm;
-    float4* sp = sm + a.nspl;
-    float2* slj = (float2*)(sm + (ENE ? 2 : 1) * a.nspl);
+    float4* sp = sm;                        // energy table (spline 1), ENE only
+    float2* slj = (float2*)(sm + (ENE ? 1 : 0) * a.nspl);
     // per warp: the cluster's LJ rows, [tj][p] = (R^2, R^2, 12 eps, 12 eps) of
     // atoms 2p, 2p+1 with type tj (after the block's type table)
     float4* sljc = (float4*)(slj + ((a.ntyp * a.ntyp + 1) & ~1)) + (size_t)(threadIdx.x >> 5) * 4 * a.ntyp;
     __shared__ IPair sip[PAIR_WARPS][4];
     __shared__ int2 stp[PAIR_WARPS][4];
-    for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) {
-        sf[k] = spl_g[k];
-        if (ENE) sp[k] = spl_g[a.nspl + k];
-    }
+    if (ENE)
+        for (int k = threadIdx.x; k < a.nspl; k += blockDim.x) sp[k] = spl_g[a.nspl + k];
     for (int k = threadIdx.x; k < a.ntyp * a.ntyp; k += blockDim.x) {
         const float2 l = lj_g[k];
         slj[k] = make_float2(l.x, 12.f * l.y);
     }
+    const EwaldF ew{a.ew_pa, a.ew_c2a, a.ew_mk};
     __syncthreads();
 
     const float sx = (float)(dyn->box[0] * (1.0 / 4294967296.0));
@@ -523,7 +565,7 @@ __device__ __forceinline__ void pair_mixed_body_x2(const int4* __restrict__ xq, 
                     const float2 dz = __fadd2_rn(make_float2(I.zq.x, I.zq.y), njz);
                     const float2 qq = __fmul2_rn(make_float2(I.zq.z, I.zq.w), qj);
                     float2 r2;
-                    pair_term_x2<MODE, SC>(dx, dy, dz, qq, L, mb, a.rr2f, a.rl2f, inv_h2, mh2, a.nsplm1, sf, sp,
+                    pair_term_x2<MODE, SC>(dx, dy, dz, qq, L, mb, a.rr2f, a.rl2f, inv_h2, mh2, a.nsplm1, ew, sp,
                                            f[p], gx, gy, gz, ev, ee, wc, wl, r2);
                     if (PRUNE)
                         nm |= ((((mb & 1u) && r2.x < rp2) ? 1u : 0u) | (((mb & 2u) && r2.y < rp2) ? 2u : 0u))
@@ -816,7 +858,10 @@ template <int MODE, bool FRAME, bool SC>
 static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a) {
     constexpr bool ENE = MODE == PM_ENE || MODE == PM_FULL;
     constexpr int nt = pair_threads(FRAME);
-    size_t sm = (size_t)(ENE ? 2 : 1) * c->nspl * sizeof(float4) +
+    // spline rows: the packed body stages the energy table only (ENE modes; its
+    // force is analytic), the scalar body the force table and, in ENE modes,
+    // the energy table
+    size_t sm = (size_t)((FRAME ? 0 : 1) + (ENE ? 1 : 0)) * c->nspl * sizeof(float4) +
                 (size_t)((c->ntyp * c->ntyp + 1) & ~1) * sizeof(float2);
     if (FRAME) sm += (size_t)(nt / 32) * 4 * c->ntyp * sizeof(float4);
     long long blocks = (long long)c->nsm * pair_minb(FRAME);
@@ -887,6 +932,12 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
     a.rmax2 = a.rr2 > a.rl2 ? a.rr2 : a.rl2;
     a.rr2f = (float)a.rr2; a.rl2f = (float)a.rl2; a.inv_hf = (float)a.inv_h; a.hf = (float)a.h;
     a.nsplm1 = c->nspl - 1;
+    {
+        const double al = c->prm.alpha;
+        a.ew_pa = (float)(0.3275911 * al);
+        a.ew_c2a = (float)(2.0 * al / std::sqrt(std::acos(-1.0)));
+        a.ew_mk = (float)(-al * al * 1.4426950408889634);     // -alpha^2 log2(e)
+    }
     a.facc = c->facc[group];
     a.acc = c->acc + (size_t)group * NACC;
     a.fsort = c->fsort; a.fstride = c->npad_cap;
