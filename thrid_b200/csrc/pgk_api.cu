@@ -145,13 +145,23 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
     if (fork) {
         PGK_CUDA(c, cudaEventRecord(c->ev_fork, c->st));
         PGK_CUDA(c, cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+        if (c->st3) PGK_CUDA(c, cudaStreamWaitEvent(c->st3, c->ev_fork, 0));
         cudaStream_t main_st = c->st;
         c->st = c->st2;
         s = launch_spme(c, g, ene, vir);
-        if (!s) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
-        c->st = main_st;
-        if (s) return s;
-        PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
+        if (!s && c->st3) {                 // bonded terms beside the SPME chain
+            PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
+            c->st = c->st3;
+            s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+            c->st = main_st;
+            if (s) return s;
+            PGK_CUDA(c, cudaEventRecord(c->ev_join3, c->st3));
+        } else {
+            if (!s) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+            c->st = main_st;
+            if (s) return s;
+            PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
+        }
     }
     if (pairs) {
         if ((s = launch_pack(c))) return s;
@@ -161,6 +171,7 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
     if (c->nmor && c->prm.mts_mor == flag && (s = launch_morse(c, g, ene || vir))) return s;   // calforce.F90:360-400
     if (fork) {
         PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join, 0));
+        if (c->st3) PGK_CUDA(c, cudaStreamWaitEvent(c->st, c->ev_join3, 0));
         return PGK_OK;
     }
     if (spme && (s = launch_spme(c, g, ene, vir))) return s;
@@ -311,13 +322,17 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     c->pool = device_pool();
     if (!c->pool) { cudaStreamDestroy(c->st); delete c; return PGK_E_CUDA; }
     if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join3, cudaEventDisableTiming) != cudaSuccess) {
         pgk_free(c);
         return PGK_E_CUDA;
     }
     if (const char* ns = getenv("PGK_STREAMS")) {       // 1: the whole force evaluation on one stream
-        if (atoi(ns) == 1) { cudaStreamDestroy(c->st2); c->st2 = nullptr; }
+        const int n = atoi(ns);       // 1: one stream; 2: the bonded terms after the SPME chain
+        if (n <= 2) { cudaStreamDestroy(c->st3); c->st3 = nullptr; }
+        if (n == 1) { cudaStreamDestroy(c->st2); c->st2 = nullptr; }
     }
     c->degfree = s->degfree_all;
     pgk_status st;
@@ -711,6 +726,7 @@ pgk_status pgk_free(pgk_ctx* c) {
     // the context's own streams only: other contexts keep running
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamSynchronize(c->st2);
+    if (c->st3) cudaStreamSynchronize(c->st3);
     for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
                     c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list, c->exs_rng,
@@ -730,8 +746,10 @@ pgk_status pgk_free(pgk_ctx* c) {
     for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamDestroy(c->st2);
+    if (c->st3) cudaStreamDestroy(c->st3);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->ev_join3) cudaEventDestroy(c->ev_join3);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return PGK_OK;

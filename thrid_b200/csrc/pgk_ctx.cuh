@@ -39,8 +39,9 @@ struct pgk_ctx {
     // second stream of the force evaluation: the SPME chain runs on it beside
     // the pair and bonded kernels (fork and join through the two events;
     // integer or FP64 atomics on the shared force and energy accumulators)
-    cudaStream_t st2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t st2 = nullptr;   // SPME chain of a force evaluation
+    cudaStream_t st3 = nullptr;   // bonded terms of a force evaluation
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
     cudaMemPool_t pool = nullptr; // the device's memory pool (pgk_dmalloc)
     std::string err;
     long long launches = 0;
