@@ -184,23 +184,6 @@ __global__ void k_rattle_vel(const double* __restrict__ pos, double* __restrict_
 }
 
 // sum m v^2 and sum m v_a v_b (nhcint kint, calpress kinetic terms)
-__global__ void k_kinetic(const double* __restrict__ vel, const double* __restrict__ mass, int n, long long* acc,
-                          int dbl) {
-    double v[10] = {0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double m = mass[i], x = vel[3 * i], y = vel[3 * i + 1], z = vel[3 * i + 2];
-        v[0] += m * (x * x + y * y + z * z);
-        const double w[3] = {x, y, z};
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) v[1 + a + 3 * b] += m * w[a] * w[b];
-    }
-    const int idx[10] = {A_KE, A_KET + 0, A_KET + 1, A_KET + 2, A_KET + 3, A_KET + 4, A_KET + 5, A_KET + 6,
-                         A_KET + 7, A_KET + 8};
-    block_acc<10>(v, acc, idx, dbl != 0);
-}
-
 
 // ---- chain updates (single thread) -------------------------------------------
 struct ChainArgs {
@@ -325,10 +308,6 @@ __device__ void chain_run(ChainDev* __restrict__ chain, const long long* __restr
         case 7: chain_run_m<7>(chain, acc, a); break;
         default: chain_run_m<8>(chain, acc, a); break;
     }
-}
-
-__global__ void k_chain(ChainDev* __restrict__ chain, const long long* __restrict__ acc, ChainArgs a) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) chain_run(chain, acc, a);
 }
 
 // kick / drift coefficients of the step (moldyn_*.F90 at istep_short == 1)
@@ -487,12 +466,76 @@ __global__ void k_press(const long long* __restrict__ acc, const DynState* __res
     if (threadIdx.x == 0 && blockIdx.x == 0) press_run(acc, dyn, chain, a);
 }
 
-// pressure of the step end followed by the chain update (end of an MTK step)
-__global__ void k_press_chain(const long long* __restrict__ acc, const DynState* __restrict__ dyn,
-                              ChainDev* chain, PressArgs pa, ChainArgs ca) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    press_run(acc, dyn, chain, pa);
-    chain_run(chain, acc, ca);
+// Kinetic sums (calkin: sum m v^2 and the tensor sum m v_a v_b) by a
+// two-level reduction: every block writes its partial sums, and the last
+// block to finish adds them in block order into the accumulator slots, which
+// it overwrites (so nothing has to clear them first).  In mixed precision the
+// partials are converted to 2^32 fixed point and added as integers (the exact
+// sum per-block atomic adds would give); in FP64 the fixed order makes the
+// sum deterministic.  MODE 1 then runs the chain update (nhcint, the end of an NHC
+// step), MODE 2 the pressure and the chain update (calpress + nhcp*int, the
+// end of an MTK step), in the last block's first thread: one launch instead of
+// a clear, the reduction and a single-thread kernel.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_kinetic_end(const double* __restrict__ vel, const double* __restrict__ mass,
+                                                     int n, long long* acc, int dbl, double* part,
+                                                     unsigned* done, const DynState* __restrict__ dyn,
+                                                     ChainDev* chain, PressArgs pa, ChainArgs ca) {
+    __shared__ double red[8][10];
+    __shared__ bool last;
+    double v[10] = {0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m = mass[i], x = vel[3 * i], y = vel[3 * i + 1], z = vel[3 * i + 2];
+        v[0] += m * (x * x + y * y + z * z);
+        const double w[3] = {x, y, z};
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) v[1 + a + 3 * b] += m * w[a] * w[b];
+    }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 10; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) red[wp][k] = v[k];
+    }
+    __syncthreads();
+    if (wp == 0) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            double x = lane < nw ? red[lane][k] : 0.0;
+            x = warp_sum(x);
+            if (lane == 0) part[10 * (size_t)blockIdx.x + k] = x;
+        }
+        if (lane == 0) {
+            __threadfence();
+            last = atomicAdd(done, 1u) == gridDim.x - 1u;
+        }
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int idx[10] = {A_KE, A_KET + 0, A_KET + 1, A_KET + 2, A_KET + 3, A_KET + 4, A_KET + 5, A_KET + 6,
+                         A_KET + 7, A_KET + 8};
+    if (threadIdx.x < 10) {
+        const int k = threadIdx.x;
+        if (dbl) {
+            double s = 0.0;
+            for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(part + 10 * (size_t)b + k);
+            acc[idx[k]] = __double_as_longlong(s);
+        } else {
+            long long s = 0;
+            for (int b = 0; b < (int)gridDim.x; ++b) s += to_fix(__ldcg(part + 10 * (size_t)b + k), PGK_FORCE_SCALE);
+            acc[idx[k]] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *done = 0u;
+        if (MODE == 2) press_run(acc, dyn, chain, pa);
+        if (MODE >= 1) chain_run(chain, acc, ca);
+    }
 }
 
 template <bool MIXED>
@@ -502,9 +545,24 @@ __global__ void k_copy_force(const void* __restrict__ f, double* __restrict__ ou
 }
 
 // ---- launchers ----------------------------------------------------------------
+// one MTS group's force accumulator (3N x 8 B) and energy/virial slots
+// cleared by one kernel (16-byte stores; the accumulator is 16-byte aligned)
+__global__ void k_zero_group(longlong2* __restrict__ f, size_t n2, long long* __restrict__ f_tail, int tail,
+                             long long* __restrict__ acc) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n2) f[k] = make_longlong2(0, 0);
+    if (k < (size_t)tail) f_tail[k] = 0;
+    if (k < NACC) acc[k] = 0;
+}
+
 pgk_status launch_zero_group(pgk_ctx* c, int g) {
-    PGK_CUDA(c, cudaMemsetAsync(c->facc[g], 0, (size_t)24 * c->natom, c->st));
-    PGK_CUDA(c, cudaMemsetAsync(c->acc + (size_t)g * NACC, 0, sizeof(long long) * NACC, c->st));
+    const size_t n3 = (size_t)3 * c->natom, n2 = n3 / 2;
+    const size_t nt = std::max(n2, (size_t)NACC);
+    k_zero_group<<<(unsigned)((nt + 255) / 256), 256, 0, c->st>>>((longlong2*)c->facc[g], n2,
+                                                                 (long long*)c->facc[g] + 2 * n2, (int)(n3 - 2 * n2),
+                                                                 c->acc + (size_t)g * NACC);
+    PGK_LAUNCHED(c);
+    PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
 
@@ -969,24 +1027,42 @@ pgk_status launch_rattle_vel(pgk_ctx* c, double eps) {
     return PGK_OK;
 }
 
+// kinetic sums into the group's accumulator (the kinetic slots of group 0
+// are the ones calpress and the chains read)
 pgk_status launch_kinetic(pgk_ctx* c, int group) {
     long long* acc = c->acc + (size_t)group * NACC;
-    PGK_CUDA(c, cudaMemsetAsync(acc + A_KE, 0, sizeof(long long) * 10, c->st));
     int blocks = std::min(c->nsm * 2, (c->natom + 255) / 256);
     if (blocks < 1) blocks = 1;
-    k_kinetic<<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, acc, c->mixed() ? 0 : 1);
+    k_kinetic_end<0><<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, acc, c->mixed() ? 0 : 1, c->ke_part,
+                                                 c->ke_done, c->dyn, c->chain, PressArgs{}, ChainArgs{});
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
 }
 
-pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md) {
-    ChainArgs a;
-    a.md = md;
-    a.degfree = c->degfree;
-    a.dbl = c->mixed() ? 0 : 1;
-    a.kind = kind;
-    k_chain<<<1, 32, 0, c->st>>>(c->chain, c->acc, a);
+// mode 1: kinetic sums + chain update (end of an NHC step); 2: kinetic sums +
+// pressure + chain update (end of an MTK step)
+pgk_status launch_kinetic_end(pgk_ctx* c, int mode, int chain_kind, const pgk_mdparams& md) {
+    PressArgs pa;
+    pa.pot_ewc = c->pot_ewc;
+    pa.netchrgsq = c->netchrgsq;
+    pa.alpha = c->prm.alpha;
+    pa.ifspme = c->prm.ifspme;
+    pa.ifnetqcorrp = c->prm.ifnetqcorrp;
+    pa.dbl = c->mixed() ? 0 : 1;
+    ChainArgs ca;
+    ca.md = md;
+    ca.degfree = c->degfree;
+    ca.dbl = c->mixed() ? 0 : 1;
+    ca.kind = chain_kind;
+    int blocks = std::min(c->nsm * 2, (c->natom + 255) / 256);
+    if (blocks < 1) blocks = 1;
+    if (mode == 2)
+        k_kinetic_end<2><<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, c->acc, pa.dbl, c->ke_part, c->ke_done,
+                                                     c->dyn, c->chain, pa, ca);
+    else
+        k_kinetic_end<1><<<blocks, 256, 0, c->st>>>(c->vel, c->mass, c->natom, c->acc, pa.dbl, c->ke_part, c->ke_done,
+                                                     c->dyn, c->chain, pa, ca);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
@@ -1042,25 +1118,6 @@ pgk_status launch_press(pgk_ctx* c) {
     a.ifnetqcorrp = c->prm.ifnetqcorrp;
     a.dbl = c->mixed() ? 0 : 1;
     k_press<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, a);
-    PGK_LAUNCHED(c);
-    PGK_CUDA(c, cudaGetLastError());
-    return PGK_OK;
-}
-
-pgk_status launch_press_chain(pgk_ctx* c, int chain_kind, const pgk_mdparams& md) {
-    PressArgs pa;
-    pa.pot_ewc = c->pot_ewc;
-    pa.netchrgsq = c->netchrgsq;
-    pa.alpha = c->prm.alpha;
-    pa.ifspme = c->prm.ifspme;
-    pa.ifnetqcorrp = c->prm.ifnetqcorrp;
-    pa.dbl = c->mixed() ? 0 : 1;
-    ChainArgs ca;
-    ca.md = md;
-    ca.degfree = c->degfree;
-    ca.dbl = c->mixed() ? 0 : 1;
-    ca.kind = chain_kind;
-    k_press_chain<<<1, 32, 0, c->st>>>(c->acc, c->dyn, c->chain, pa, ca);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;

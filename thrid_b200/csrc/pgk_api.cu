@@ -360,7 +360,9 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     if (pgk_dmalloc(c, &c->pos, n3 * 8) || pgk_dmalloc(c, &c->vel, n3 * 8) || pgk_dmalloc(c, &c->pos_old, n3 * 8) ||
         pgk_dmalloc(c, &c->facc[0], n3 * 8) || pgk_dmalloc(c, &c->facc[1], n3 * 8) ||
         pgk_dmalloc(c, &c->acc, sizeof(long long) * 2 * NACC) || pgk_dmalloc(c, &c->dyn, sizeof(DynState)) ||
-        pgk_dmalloc(c, &c->chain, sizeof(ChainDev)) || pgk_dmalloc(c, &c->status, sizeof(unsigned))) {
+        pgk_dmalloc(c, &c->chain, sizeof(ChainDev)) || pgk_dmalloc(c, &c->status, sizeof(unsigned)) ||
+        pgk_dmalloc(c, &c->ke_part, sizeof(double) * 20 * std::max(c->nsm, 1)) ||
+        pgk_dmalloc(c, &c->ke_done, sizeof(unsigned)) || cudaMemsetAsync(c->ke_done, 0, sizeof(unsigned), c->st)) {
         pgk_free(c);
         return PGK_E_NOMEM;
     }
@@ -742,7 +744,7 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->mor_atoms, c->mor_par, c->mor_rows, c->mor_cnt, c->mor_cell, c->mor_csort, c->mor_ccnt,
                     c->mor_cstart, c->mor_cfill, c->mor_ctr, c->hfk_q, c->hfk_g, c->hfk_out, c->hfk_tw[0],
                     c->hfk_tw[1], c->hfk_tw[2], c->r3_atoms, c->r3_d, c->star_atoms, c->star_d, c->plan_rx.tw,
-                    c->tw_rx};
+                    c->tw_rx, c->ke_part, c->ke_done};
     for (void* b : bufs) if (b) pgk_dfree(c, b);     // stream-ordered frees on c->st
     if (c->st) cudaStreamSynchronize(c->st);
     if (c->st2) cudaStreamDestroy(c->st2);
@@ -1187,8 +1189,8 @@ static pgk_status md_step_body(pgk_ctx* c, int kind, int64_t step, const pgk_mdp
         RUN(launch_kick_drift(c, kshort | KD_SHORT_FIRST | (last ? KD_LONG : 0)));
         if (rattle) RUN(launch_rattle_vel(c, md->eps_rattle));
     }
-    if (kind == 1) { RUN(launch_kinetic(c, 0)); RUN(launch_chain(c, chain_kind, *md)); }
-    if (mtk) { RUN(launch_kinetic(c, 0)); RUN(launch_press_chain(c, chain_kind, *md)); }
+    if (kind == 1) RUN(launch_kinetic_end(c, 1, chain_kind, *md));      // kinetic sums + nhcint
+    if (mtk) RUN(launch_kinetic_end(c, 2, chain_kind, *md));            // + calpress + nhcp*int
 #undef RUN
     return PGK_OK;
 }

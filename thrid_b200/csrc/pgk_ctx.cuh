@@ -39,6 +39,8 @@ struct pgk_ctx {
     // second stream of the force evaluation: the SPME chain runs on it beside
     // the pair and bonded kernels (fork and join through the two events;
     // integer or FP64 atomics on the shared force and energy accumulators)
+    double* ke_part = nullptr;    // [2 nsm][10] per-block kinetic sums (k_kinetic_end)
+    unsigned* ke_done = nullptr;  // blocks of k_kinetic_end finished (zero between launches)
     cudaStream_t st2 = nullptr;   // SPME chain of a force evaluation
     cudaStream_t st3 = nullptr;   // bonded terms of a force evaluation
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
@@ -350,11 +352,10 @@ pgk_status launch_zero_group(pgk_ctx* c, int group);
 #define KD_SHORT_FIRST 16
 pgk_status launch_kick_drift(pgk_ctx* c, int flags);
 pgk_status launch_chain_coeffs(pgk_ctx* c, int chain_kind, int coef_kind, const pgk_mdparams& md);
-pgk_status launch_press_chain(pgk_ctx* c, int chain_kind, const pgk_mdparams& md);
 pgk_status launch_rattle_pos(pgk_ctx* c, double eps, double dt, bool use_rvinv);
 pgk_status launch_rattle_vel(pgk_ctx* c, double eps);
 pgk_status launch_kinetic(pgk_ctx* c, int group);
-pgk_status launch_chain(pgk_ctx* c, int kind, const pgk_mdparams& md);
+pgk_status launch_kinetic_end(pgk_ctx* c, int mode, int chain_kind, const pgk_mdparams& md);
 pgk_status launch_press(pgk_ctx* c);
 pgk_status launch_coeffs(pgk_ctx* c, int kind, const pgk_mdparams& md, int phase);
 pgk_status launch_box_update(pgk_ctx* c, int kind, const pgk_mdparams& md, bool with_rkcut = false);
