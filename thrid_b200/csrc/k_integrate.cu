@@ -518,17 +518,38 @@ __global__ void __launch_bounds__(256) k_kinetic_end(const double* __restrict__ 
     __threadfence();
     const int idx[10] = {A_KE, A_KET + 0, A_KET + 1, A_KET + 2, A_KET + 3, A_KET + 4, A_KET + 5, A_KET + 6,
                          A_KET + 7, A_KET + 8};
+    // every thread adds the partials of blocks t, t + 256, ... (loads in
+    // flight together), then a fixed-shape block reduction: deterministic
+    __shared__ long long ired[8][10];
+    __shared__ double dred[8][10];
+    long long is[10];
+    double ds[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) { is[k] = 0; ds[k] = 0.0; }
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) {
+            const double x = __ldcg(part + 10 * (size_t)b + k);
+            if (dbl) ds[k] += x;
+            else is[k] += to_fix(x, PGK_FORCE_SCALE);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        if (dbl) ds[k] = warp_sum(ds[k]);
+        else is[k] = warp_sum(is[k]);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 10; ++k) { ired[wp][k] = is[k]; dred[wp][k] = ds[k]; }
+    }
+    __syncthreads();
     if (threadIdx.x < 10) {
         const int k = threadIdx.x;
-        if (dbl) {
-            double s = 0.0;
-            for (int b = 0; b < (int)gridDim.x; ++b) s += __ldcg(part + 10 * (size_t)b + k);
-            acc[idx[k]] = __double_as_longlong(s);
-        } else {
-            long long s = 0;
-            for (int b = 0; b < (int)gridDim.x; ++b) s += to_fix(__ldcg(part + 10 * (size_t)b + k), PGK_FORCE_SCALE);
-            acc[idx[k]] = s;
-        }
+        long long si = 0;
+        double sd = 0.0;
+        for (int w = 0; w < nw; ++w) { si += ired[w][k]; sd += dred[w][k]; }
+        acc[idx[k]] = dbl ? __double_as_longlong(sd) : si;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
