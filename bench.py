@@ -203,6 +203,15 @@ def run_ours(args, rank, world, local_rank):
     out["autotune"] = tuning_table().splitlines()
     if rank == 0 and not args.no_configs:
         out["other_configs"] = other_configs(args)
+    if rank == 0 and world == 1 and not args.no_serve:
+        # the serving workload in a bounded form: 32 seeded
+        # replicas x 2,000 NVE steps, against this line's single large system
+        sa = argparse.Namespace(**vars(args))
+        sa.serve_replicas, sa.serve_steps, sa.serve_hf = 32, 2000, False
+        sv = run_serve(sa, single={"value": value, "unit": UNIT, "steps": nsteps, "workload": WORKLOAD,
+                                   "note": "this line's own timed window"})
+        sv.pop("autotune", None)
+        out["serving"] = sv
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     return out
@@ -589,9 +598,11 @@ def _nfft(L):
     return 128
 
 
-def run_serve(args):
+def run_serve(args, single=None):
     """Continuous batching of independent replicas (the serving configuration):
-    Poisson arrivals, admission by slots and memory, per-replica latency."""
+    Poisson arrivals, admission by slots and memory, per-replica latency.
+    `single`: the single large system's rate measured in the same run (else
+    measured here)."""
     import torch
     from thrid_b200 import abi
     from thrid_b200 import systems as S
@@ -634,7 +645,8 @@ def run_serve(args):
     gaps = rng.exponential(mean_service / args.serve_load * 1.0, size=len(reps))
     arrivals = np.cumsum(gaps) - gaps[0]
     lat, span = run(args.serve_slots, arrivals)
-    single = single_system_rate()
+    if single is None:
+        single = single_system_rate()
     return {
         "metric": "replica serving: aggregate atom-steps/s and p50/p99 latency (mixed precision)",
         "value": work / span, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
@@ -757,6 +769,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-path comparison leg")
     ap.add_argument("--no-configs", action="store_true", help="skip the other named shapes (C1-C3, drift)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the bounded serving leg of the main line")
     ap.add_argument("--serve", action="store_true", help="replica-serving benchmark instead of the main line")
     ap.add_argument("--serve-replicas", type=int, default=32)
     ap.add_argument("--serve-steps", type=int, default=2000)
@@ -775,6 +788,10 @@ def main():
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")   # before CUDA starts (see thrid_b200/serve.py)
         print(json.dumps(run_serve(args)))
         return
+    if args.impl == "ours" and not args.no_serve:
+        # the serving leg runs after the main line in the same process: give
+        # its replicas' streams their own hardware queues before CUDA starts
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     rank, world, local = dist_init()
     if args.impl == "reference":
         out = run_reference(args, rank, world)
