@@ -226,6 +226,27 @@ __device__ __forceinline__ void eval_14(const double* P, int i, int j, double qq
     dv_out = (double)dv;
 }
 
+// the same with the pair's constants formed once at setup:
+// K = (q_i q_j elc fac, R^2, eps vdw fac, 0)
+template <typename T>
+__device__ __forceinline__ void eval_14k(const double* P, int i, int j, double4 K, const DynState* dyn,
+                                         double (&F)[3], double (&rd)[3], double& de_out, double& dv_out) {
+    T r[3];
+    disp<T>(P, i, j, dyn, r);
+    T r2 = dt3(r, r);
+    T ri2 = T(1) / r2, ri1 = sqrt(ri2);
+    T de = (T)K.x * ri1;
+    T t2 = ri2 * (T)K.y, t6 = t2 * t2 * t2, t12 = t6 * t6;
+    T E = (T)K.z;
+    T dv = E * (t12 - T(2) * t6);
+    T ft = T(12) * E * (t12 - t6) * ri2;
+    T fs = de * ri2 + ft;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { F[d] = (double)(fs * r[d]); rd[d] = (double)r[d]; }
+    de_out = (double)de;
+    dv_out = (double)dv;
+}
+
 // ---- mixed-precision force-and-tensor forms (tensor-only steps) ---------------
 // Same forces as eval_angl / eval_tors in FP32 without the energy: no inverse
 // trigonometry in the torsion (the force factor is a polynomial in cos phi,
@@ -489,8 +510,8 @@ struct TermsDev {
     const int4* angl_ijk; const double2* angl_p;
     const int4* tors_ijkl; const double4* tors_p;
     const int4* rb_ijkl; const double* rb_c;
-    const int2* p14_ij; const double2* p14_f;
-    const int2* expair;
+    const int2* p14_ij; const double2* p14_f; const double4* p14_k;
+    const int2* expair; const double* ex_q;
     const double* chrg; const int* typ; const double2* lj64; int ntyp;
     const double4* spl64; const float4* spl32; int nspl; double hspl;
 };
@@ -580,10 +601,16 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
             for (int aa = 0; aa < 3; ++aa) tv[aa + 3 * bb] += F[aa] * P[3 * l + bb];
     };
     const bool full = want && !TENS;
+    // the block's terms of all types as one sequence dealt round-robin to the
+    // threads: term v of the sequence goes to thread v mod nt, so every thread
+    // gets about the same number of terms and no warp waits at the block's
+    // barriers for another that drew the leftovers of every type
+    int base = 0;
+    auto first = [&](int t0) { return t0 + ((tid - base) % nt + nt) % nt; };
     if (mask & 1) {
         int t0, t1; range(0, t0, t1);
         double v[11] = {0};
-        for (int k = t0 + tid; k < t1; k += nt) {
+        for (int k = first(t0); k < t1; k += nt) {
             double F[3] = {0, 0, 0}, rd[3], e;
             const int2 ij = D.bond_ij[k];
             const bool on = eval_bond<T>(P, ij.x - a0, ij.y - a0, D.bond_p[k], dyn, F, rd, e);
@@ -592,6 +619,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
             if (TENS && on) tens_pair(F, rd);
             if (full && on) { v[0] += e; vir_pair(v + 1, F, rd); }
         }
+        base += t1 - t0;
         if (full) {
             const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
                                  A_VTB + 6, A_VTB + 7, A_VTB + 8};
@@ -602,7 +630,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     if (mask & 2) {
         int t0, t1; range(1, t0, t1);
         double v[11] = {0};
-        for (int k = t0 + tid; k < t1; k += nt) {
+        for (int k = first(t0); k < t1; k += nt) {
             const int4 q4 = D.angl_ijk[k];
             const int at[3] = {q4.x - a0, q4.y - a0, q4.z - a0};
             const int sl = so[1] + 3 * (k - t0);
@@ -632,6 +660,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], P, at[q]);
             }
         }
+        base += t1 - t0;
         if (full) {
             const int idx[11] = {A_ANGL, A_VA, A_VTA + 0, A_VTA + 1, A_VTA + 2, A_VTA + 3, A_VTA + 4, A_VTA + 5,
                                  A_VTA + 6, A_VTA + 7, A_VTA + 8};
@@ -644,7 +673,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         if (!(mask & (4 << rb))) continue;
         int t0, t1; range(2 + rb, t0, t1);
         double v[11] = {0};
-        for (int k = t0 + tid; k < t1; k += nt) {
+        for (int k = first(t0); k < t1; k += nt) {
             const int4 q4 = rb ? D.rb_ijkl[k] : D.tors_ijkl[k];
             const int at[4] = {q4.x - a0, q4.y - a0, q4.z - a0, q4.w - a0};
             if (FAST) {
@@ -677,6 +706,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 for (int q = 0; q < 4; ++q) vir_abs(v + 1, F[q], P, at[q]);
             }
         }
+        base += t1 - t0;
         if (full) {
             const int idx[11] = {rb ? A_TORSRB : A_TORS, A_VT, A_VTT + 0, A_VTT + 1, A_VTT + 2, A_VTT + 3,
                                  A_VTT + 4, A_VTT + 5, A_VTT + 6, A_VTT + 7, A_VTT + 8};
@@ -687,16 +717,16 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     if (mask & 16) {
         int t0, t1; range(4, t0, t1);
         double v[12] = {0};
-        for (int k = t0 + tid; k < t1; k += nt) {
+        for (int k = first(t0); k < t1; k += nt) {
             const int2 ij = D.p14_ij[k];
             double F[3], rd[3], de, dv;
-            eval_14<T>(P, ij.x - a0, ij.y - a0, D.chrg[ij.x] * D.chrg[ij.y], D.lj64[D.typ[ij.x] * D.ntyp + D.typ[ij.y]],
-                       D.p14_f[k], dyn, F, rd, de, dv);
+            eval_14k<T>(P, ij.x - a0, ij.y - a0, D.p14_k[k], dyn, F, rd, de, dv);
             const int sl = so[4] + 2 * (k - t0);
             put(sl, F, 1.0); put(sl + 1, F, -1.0);
             if (TENS) tens_pair(F, rd);
             if (full) { v[0] += de; v[1] += dv; vir_pair(v + 2, F, rd); }
         }
+        base += t1 - t0;
         if (full) {
             const int idx[12] = {A_ELC14, A_VDW14, A_V14, A_VT14 + 0, A_VT14 + 1, A_VT14 + 2, A_VT14 + 3,
                                  A_VT14 + 4, A_VT14 + 5, A_VT14 + 6, A_VT14 + 7, A_VT14 + 8};
@@ -707,16 +737,16 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     if (mask & 32) {
         int t0, t1; range(5, t0, t1);
         double v[11] = {0};
-        for (int k = t0 + tid; k < t1; k += nt) {
+        for (int k = first(t0); k < t1; k += nt) {
             const int2 ij = D.expair[k];
             double F[3], rd[3], e;
-            eval_excl<MIXED>(P, ij.x - a0, ij.y - a0, D.chrg[ij.x] * D.chrg[ij.y], D.spl64, D.spl32, D.nspl, D.hspl,
-                             dyn, F, rd, e);
+            eval_excl<MIXED>(P, ij.x - a0, ij.y - a0, D.ex_q[k], D.spl64, D.spl32, D.nspl, D.hspl, dyn, F, rd, e);
             const int sl = so[5] + 2 * (k - t0);
             put(sl, F, 1.0); put(sl + 1, F, -1.0);
             if (TENS) tens_pair(F, rd);
             if (full) { v[0] -= e; vir_pair(v + 1, F, rd); }
         }
+        base += t1 - t0;
         if (full) {
             // pot_elc -= potij; pot_viri_coul -= potij; tensor (lower triangle) += f r
             double w[8] = {v[0], v[0], v[2], v[3], v[4], v[6], v[7], v[10]};
@@ -834,6 +864,20 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
         (s = up(c, &c->rb_ijkl, t.rij)) || (s = up(c, &c->rb_c, t.rc)) || (s = up(c, &c->p14_ij, t.p14)) ||
         (s = up(c, &c->p14_f, t.f14)) || (s = up(c, &c->expair, t.ex)))
         return s;
+    // per-term constants of the 1-4 and excluded pairs (charges, types and
+    // LJ parameters are fixed at init): one load per term in the block kernel
+    // instead of a chain of dependent gathers
+    if (t.q && t.ty && t.lj) {
+        std::vector<double4> k14(t.p14.size());
+        for (size_t k = 0; k < t.p14.size(); ++k) {
+            const int i = t.p14[k].x, j = t.p14[k].y;
+            const double2 lp = t.lj[t.ty[i] * t.ntyp + t.ty[j]];
+            k14[k] = make_double4(t.q[i] * t.q[j] * t.f14[k].x, lp.x, lp.y * t.f14[k].y, 0.0);
+        }
+        std::vector<double> qex(t.ex.size());
+        for (size_t k = 0; k < t.ex.size(); ++k) qex[k] = t.q[t.ex[k].x] * t.q[t.ex[k].y];
+        if ((s = up(c, &c->p14_k, k14)) || (s = up(c, &c->ex_q, qex))) return s;
+    }
 
     // ---- block plan ----
     const int cap = blk_slot_cap(c->mixed());
@@ -1026,8 +1070,8 @@ static void terms_impl(pgk_ctx* c, int group, int mask, bool want, bool tens) {
     const int w = want ? 1 : 0;
     if (c->nblk > 0) {
         TermsDev D{c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl, c->tors_p, c->rb_ijkl, c->rb_c,
-                   c->p14_ij, c->p14_f, c->expair, c->chrg, c->typ, c->lj64, c->ntyp, c->spl64, c->spl32, c->nspl,
-                   c->hspl};
+                   c->p14_ij, c->p14_f, c->p14_k, c->expair, c->ex_q, c->chrg, c->typ, c->lj64, c->ntyp, c->spl64,
+                   c->spl32, c->nspl, c->hspl};
         const int cap = blk_slot_cap(MIXED);
         BlkDev K{c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff, c->blk_ip, c->blk_incp, c->blk_inc, c->nblk, cap};
         const size_t sm = 3 * BLK_LOC_MAX * sizeof(double) + 3 * (size_t)cap * (MIXED ? sizeof(float) : sizeof(double)) +

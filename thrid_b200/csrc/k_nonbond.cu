@@ -774,57 +774,6 @@ __global__ void k_prune_decide(PruneDev* __restrict__ P, const DynState* __restr
     }
 }
 
-// After a prune step: regroup each pruned row by mask (stable counting sort
-// in shared memory, as the book rows), so the pair kernel's loops over the
-// mask bits stay uniform across a warp.  One warp per row; no-op unless a
-// prune was decided.
-__device__ __forceinline__ void prune_sort_rows(int blk, int* __restrict__ plist, const int* __restrict__ pcnt,
-                                                int ccap, int ncl, const PruneDev* __restrict__ P) {
-    if (!P->do_prune) return;
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cl = (blk * blockDim.x + threadIdx.x) >> 5;
-    if (cl >= ncl) return;
-    extern __shared__ int prow_raw[];
-    int* buf = prow_raw + (size_t)wib * (ccap + 256);
-    int* bin = buf + ccap;
-    int* out = plist + (size_t)cl * ccap;
-    const int count = pcnt[cl];
-    for (int q = lane; q < 256; q += 32) bin[q] = 0;
-    // stage the row: eight loads in flight per lane
-    for (int k0 = 0; k0 < count; k0 += 256) {
-        int r[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) { const int k = k0 + 32 * q + lane; r[q] = k < count ? out[k] : 0; }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) { const int k = k0 + 32 * q + lane; if (k < count) buf[k] = r[q]; }
-    }
-    __syncwarp();
-    for (int k0 = 0; k0 < count; k0 += 32) {
-        const int k = k0 + lane;
-        const unsigned key = k < count ? mask_bin((unsigned)buf[k] >> 24) : 256u + lane;
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        if (k < count && (grp & ((1u << lane) - 1u)) == 0) atomicAdd(&bin[key], __popc(grp));
-    }
-    __syncwarp();
-    warp_scan256(bin, lane);                 // exclusive scan of the 256 bins
-    __syncwarp();
-    for (int k0 = 0; k0 < count; k0 += 32) {
-        const int k = k0 + lane;
-        const bool ok = k < count;
-        const int e = ok ? buf[k] : 0;
-        const unsigned key = ok ? mask_bin((unsigned)e >> 24) : 256u + lane;
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        const int rank = __popc(grp & ((1u << lane) - 1u));
-        const int base = ok ? bin[key] : 0;
-        __syncwarp();
-        if (ok) {
-            out[base + rank] = e;
-            if (rank == 0) bin[key] = base + __popc(grp);
-        }
-        __syncwarp();
-    }
-}
-
 // sorted-slot pair forces -> the group accumulator, leaving the slot buffer
 // zero for the next call
 __device__ __forceinline__ void unsort_slots(int blk, long long* __restrict__ fsort, int fst,
@@ -841,17 +790,12 @@ __device__ __forceinline__ void unsort_slots(int blk, long long* __restrict__ fs
     if (vx | vy | vz) { fsort[s] = 0; fsort[s + fst] = 0; fsort[s + 2 * (size_t)fst] = 0; }
 }
 
-// The two finishing steps of a mixed pair evaluation in one launch: blocks
-// [0, nbu) move the sorted-slot forces into the accumulator, the blocks after
-// them regroup the pruned rows by mask on a prune step (128 threads a block,
-// four rows per block; they return at once on the other steps).
+// After a mixed pair evaluation: the sorted-slot forces into the group
+// accumulator (128 threads a block).
 __global__ void __launch_bounds__(128) k_pair_finish(long long* __restrict__ fsort, int fst,
                                                      const int* __restrict__ perm, int npad,
-                                                     long long* __restrict__ facc, int nbu, int* __restrict__ plist,
-                                                     const int* __restrict__ pcnt, int ccap, int ncl,
-                                                     const PruneDev* __restrict__ P) {
-    if ((int)blockIdx.x < nbu) unsort_slots(blockIdx.x, fsort, fst, perm, npad, facc);
-    else prune_sort_rows(blockIdx.x - nbu, plist, pcnt, ccap, ncl, P);
+                                                     long long* __restrict__ facc) {
+    unsort_slots(blockIdx.x, fsort, fst, perm, npad, facc);
 }
 
 template <int MODE, bool FRAME, bool SC>
@@ -896,24 +840,16 @@ static void pair_mixed_launch(pgk_ctx* c, const PairArgs& a) {
 }
 
 // After the mixed pair kernel: the sorted-slot forces into the group
-// accumulator and, after a prune step, the mask regrouping of the pruned
-// rows.  Runs on the context's current stream (the force evaluation may put
-// it beside the SPME chain: the accumulator adds are atomic).
+// accumulator.  Runs on the context's current stream (the force evaluation
+// may put it beside the SPME chain: the accumulator adds are atomic).  The
+// pruned rows keep the order of the book rows (grouped by their book masks):
+// regrouping them by their pruned masks after every prune cost more (146 us a
+// prune on the 200k-atom butane rows) than it saved on the steps between
+// prunes.
 pgk_status launch_pair_finish(pgk_ctx* c, int group) {
     if (c->ncl <= 0 || !c->mixed()) return PGK_OK;
     const int nbu = (c->npad + 127) / 128;
-    int nbs = 0;
-    size_t sort_sm = 0;
-    if (c->prune_buffer > 0.f) {
-        sort_sm = (size_t)4 * (c->ccap + 256) * sizeof(int);      // 4 warps, one row each
-        if (sort_sm <= 160 * 1024 && smem_limit(k_pair_finish, sort_sm) == cudaSuccess)
-            nbs = (int)(((long long)c->ncl * 32 + 127) / 128);
-        else
-            sort_sm = 0;
-    }
-    k_pair_finish<<<nbu + nbs, 128, sort_sm, c->st>>>(c->fsort, c->npad_cap, c->perm, c->npad,
-                                                      (long long*)c->facc[group], nbu, c->plist, c->pcnt, c->ccap,
-                                                      c->ncl, c->prune);
+    k_pair_finish<<<nbu, 128, 0, c->st>>>(c->fsort, c->npad_cap, c->perm, c->npad, (long long*)c->facc[group]);
     PGK_LAUNCHED(c);
     PGK_CUDA(c, cudaGetLastError());
     return PGK_OK;
