@@ -23,6 +23,9 @@
 // Angle and torsion virials use absolute coordinates exactly like the
 // reference (sum f_a x_b over the term's atoms).
 #include <algorithm>
+#include <array>
+#include <cstring>
+#include <map>
 #include <vector>
 
 #include "pgk_ctx.cuh"
@@ -514,12 +517,23 @@ struct TermsDev {
     const int2* expair; const double* ex_q;
     const double* chrg; const int* typ; const double2* lj64; int ntyp;
     const double4* spl64; const float4* spl32; int nspl; double hspl;
+    const uint2* rec[6]; const double* tab[6];    // compact near-term records, parameter tables
 };
 struct BlkDev {
     const int* a0; const int* nloc; const int* t; const int* soff; const int* ip; const int* incp;
     const unsigned short* inc;
     int nblk, smax;
 };
+
+// compact near-term record (bonded_setup): four 9-bit block-local atom
+// indices and a 28-bit index into the type's parameter table
+__device__ __forceinline__ void rec_atoms(uint2 r, int (&at)[4]) {
+    at[0] = (int)(r.x & 511u);
+    at[1] = (int)((r.x >> 9) & 511u);
+    at[2] = (int)((r.x >> 18) & 511u);
+    at[3] = (int)((r.x >> 27) | ((r.y & 15u) << 5));
+}
+__device__ __forceinline__ unsigned rec_par(uint2 r) { return r.y >> 4; }
 
 // TENS: the steps that need only the total bonded virial tensor (anisotropic
 // MTK steps without output): one 9-entry tensor summed over all types into
@@ -541,6 +555,25 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     int* IP = (int*)(SZ + K.smax);                           // [BLK_LOC_MAX+1] incidence pointers
     unsigned short* INC = (unsigned short*)(IP + BLK_LOC_MAX + 4);   // [smax] incidence (16-byte aligned)
     const int* ipg = K.incp + K.ip[b];
+    // The block's terms of all enabled types as one sequence dealt round-robin
+    // to the threads (term v to thread v mod nt), so every thread gets about
+    // the same number of terms and no warp waits at the block's barriers for
+    // another that drew the leftovers of every type.  sT[ty] = (first term,
+    // end, position of the type's first term in the sequence), written by
+    // warp 0 beside the staging loads.
+    __shared__ int sT[6][3];
+    if (tid < 32) {
+        int t0 = 0, t1 = 0;
+        if (tid < 6) { t0 = K.t[tid * (K.nblk + 1) + b]; t1 = K.t[tid * (K.nblk + 1) + b + 1]; }
+        const int cnt = tid < 6 && ((mask >> tid) & 1) ? t1 - t0 : 0;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (tid >= o) incl += y;
+        }
+        if (tid < 6) { sT[tid][0] = t0; sT[tid][1] = t1; sT[tid][2] = incl - cnt; }
+    }
     const int inc0 = ipg[0], ninc = ipg[nloc] - inc0;
     {
         // staging: every load of a thread is issued before its stores (the
@@ -569,13 +602,26 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         for (int q = 0; q < NV; ++q) { const int l = tid + q * nt; if (l < nv) ((uint4*)INC)[l] = rv[q]; }
     }
     __syncthreads();
-    auto range = [&](int ty, int& t0, int& t1) {
-        t0 = K.t[ty * (K.nblk + 1) + b];
-        t1 = K.t[ty * (K.nblk + 1) + b + 1];
-    };
     auto put = [&](int sl, const double* F, double sg) {
         SX[sl] = (T)(sg * F[0]); SY[sl] = (T)(sg * F[1]); SZ[sl] = (T)(sg * F[2]);
     };
+    // this thread's first term of a type; the records: each type's loop loads
+    // the next record one term ahead, and at its start the first record of
+    // the next enabled type (carry), so no record load waits in the open
+    auto kfirst = [&](int ty) { return sT[ty][0] + ((tid - sT[ty][2]) % nt + nt) % nt; };
+    auto first_rec = [&](int ty) {
+        const int k = kfirst(ty);
+        return k < sT[ty][1] ? __ldg(D.rec[ty] + k) : make_uint2(0u, 0u);
+    };
+    auto next_rec = [&](int ty, int k) {
+        return k + nt < sT[ty][1] ? __ldg(D.rec[ty] + k + nt) : make_uint2(0u, 0u);
+    };
+    auto carry_after = [&](int ty) {
+        int u = ty + 1;
+        while (u < 6 && !((mask >> u) & 1)) ++u;
+        return u < 6 ? first_rec(u) : make_uint2(0u, 0u);
+    };
+    uint2 carry = carry_after(-1);
     double tv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};               // TENS: total tensor (a + 3b)
     float tvf[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};               // mixed TENS: FP32 sums of lever-arm terms
     constexpr bool FAST = MIXED && TENS;
@@ -601,25 +647,22 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
             for (int aa = 0; aa < 3; ++aa) tv[aa + 3 * bb] += F[aa] * P[3 * l + bb];
     };
     const bool full = want && !TENS;
-    // the block's terms of all types as one sequence dealt round-robin to the
-    // threads: term v of the sequence goes to thread v mod nt, so every thread
-    // gets about the same number of terms and no warp waits at the block's
-    // barriers for another that drew the leftovers of every type
-    int base = 0;
-    auto first = [&](int t0) { return t0 + ((tid - base) % nt + nt) % nt; };
     if (mask & 1) {
-        int t0, t1; range(0, t0, t1);
+        const int t0 = sT[0][0], t1 = sT[0][1];
         double v[11] = {0};
-        for (int k = first(t0); k < t1; k += nt) {
+        uint2 r = carry, rn;
+        carry = carry_after(0);
+        for (int k = kfirst(0); k < t1; k += nt, r = rn) {
+            rn = next_rec(0, k);
+            int at[4];
+            rec_atoms(r, at);
             double F[3] = {0, 0, 0}, rd[3], e;
-            const int2 ij = D.bond_ij[k];
-            const bool on = eval_bond<T>(P, ij.x - a0, ij.y - a0, D.bond_p[k], dyn, F, rd, e);
+            const bool on = eval_bond<T>(P, at[0], at[1], __ldg((const double2*)D.tab[0] + rec_par(r)), dyn, F, rd, e);
             const int sl = so[0] + 2 * (k - t0);
             put(sl, F, 1.0); put(sl + 1, F, -1.0);
             if (TENS && on) tens_pair(F, rd);
             if (full && on) { v[0] += e; vir_pair(v + 1, F, rd); }
         }
-        base += t1 - t0;
         if (full) {
             const int idx[11] = {A_BOND, A_VB, A_VTB + 0, A_VTB + 1, A_VTB + 2, A_VTB + 3, A_VTB + 4, A_VTB + 5,
                                  A_VTB + 6, A_VTB + 7, A_VTB + 8};
@@ -628,14 +671,17 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         }
     }
     if (mask & 2) {
-        int t0, t1; range(1, t0, t1);
+        const int t0 = sT[1][0], t1 = sT[1][1];
         double v[11] = {0};
-        for (int k = first(t0); k < t1; k += nt) {
-            const int4 q4 = D.angl_ijk[k];
-            const int at[3] = {q4.x - a0, q4.y - a0, q4.z - a0};
+        uint2 r = carry, rn;
+        carry = carry_after(1);
+        for (int k = kfirst(1); k < t1; k += nt, r = rn) {
+            rn = next_rec(1, k);
+            int at[4];
+            rec_atoms(r, at);
+            const double2 pp = __ldg((const double2*)D.tab[1] + rec_par(r));
             const int sl = so[1] + 3 * (k - t0);
             if (FAST) {
-                const double2 pp = D.angl_p[k];
                 float Ff[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, arm[3][3];
                 if (fabs(pp.x) >= 1.0e-32) {
                     angl_force_f(P, at[0], at[1], at[2], pp, dyn, Ff, arm);
@@ -647,7 +693,7 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 continue;
             }
             double F[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, e;
-            const bool on = eval_angl<T>(P, at[0], at[1], at[2], D.angl_p[k], dyn, F, e);
+            const bool on = eval_angl<T>(P, at[0], at[1], at[2], pp, dyn, F, e);
 #pragma unroll
             for (int q = 0; q < 3; ++q) put(sl + q, F[q], 1.0);
             if (TENS && on) {
@@ -660,7 +706,6 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 for (int q = 0; q < 3; ++q) vir_abs(v + 1, F[q], P, at[q]);
             }
         }
-        base += t1 - t0;
         if (full) {
             const int idx[11] = {A_ANGL, A_VA, A_VTA + 0, A_VTA + 1, A_VTA + 2, A_VTA + 3, A_VTA + 4, A_VTA + 5,
                                  A_VTA + 6, A_VTA + 7, A_VTA + 8};
@@ -671,16 +716,21 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
 #pragma unroll
     for (int rb = 0; rb < 2; ++rb) {
         if (!(mask & (4 << rb))) continue;
-        int t0, t1; range(2 + rb, t0, t1);
+        const int t0 = sT[2 + rb][0], t1 = sT[2 + rb][1];
         double v[11] = {0};
-        for (int k = first(t0); k < t1; k += nt) {
-            const int4 q4 = rb ? D.rb_ijkl[k] : D.tors_ijkl[k];
-            const int at[4] = {q4.x - a0, q4.y - a0, q4.z - a0, q4.w - a0};
+        uint2 r = carry, rn;
+        carry = carry_after(2 + rb);
+        for (int k = kfirst(2 + rb); k < t1; k += nt, r = rn) {
+            rn = next_rec(2 + rb, k);
+            int at[4];
+            rec_atoms(r, at);
+            const unsigned pi = rec_par(r);
+            const double4 tp = rb ? make_double4(0, 0, 0, 0) : ((const double4*)D.tab[2])[pi];
+            const double* C = rb ? D.tab[3] + 6 * (size_t)pi : nullptr;
             if (FAST) {
                 float Ff[4][3], arm[4][3];
-                if (rb) tors_force_f<true>(P, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0),
-                                           D.rb_c + 6 * (size_t)k, dyn, Ff, arm, status);
-                else tors_force_f<false>(P, at[0], at[1], at[2], at[3], D.tors_p[k], nullptr, dyn, Ff, arm, status);
+                if (rb) tors_force_f<true>(P, at[0], at[1], at[2], at[3], tp, C, dyn, Ff, arm, status);
+                else tors_force_f<false>(P, at[0], at[1], at[2], at[3], tp, nullptr, dyn, Ff, arm, status);
                 const int slf = so[2 + rb] + 4 * (k - t0);
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -690,9 +740,8 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 continue;
             }
             double F[4][3], e;
-            if (rb) eval_tors<T, true>(P, at[0], at[1], at[2], at[3], make_double4(0, 0, 0, 0), D.rb_c + 6 * (size_t)k,
-                                       dyn, F, e, status);
-            else eval_tors<T, false>(P, at[0], at[1], at[2], at[3], D.tors_p[k], nullptr, dyn, F, e, status);
+            if (rb) eval_tors<T, true>(P, at[0], at[1], at[2], at[3], tp, C, dyn, F, e, status);
+            else eval_tors<T, false>(P, at[0], at[1], at[2], at[3], tp, nullptr, dyn, F, e, status);
             const int sl = so[2 + rb] + 4 * (k - t0);
 #pragma unroll
             for (int q = 0; q < 4; ++q) put(sl + q, F[q], 1.0);
@@ -706,7 +755,6 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
                 for (int q = 0; q < 4; ++q) vir_abs(v + 1, F[q], P, at[q]);
             }
         }
-        base += t1 - t0;
         if (full) {
             const int idx[11] = {rb ? A_TORSRB : A_TORS, A_VT, A_VTT + 0, A_VTT + 1, A_VTT + 2, A_VTT + 3,
                                  A_VTT + 4, A_VTT + 5, A_VTT + 6, A_VTT + 7, A_VTT + 8};
@@ -715,18 +763,21 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         }
     }
     if (mask & 16) {
-        int t0, t1; range(4, t0, t1);
+        const int t0 = sT[4][0], t1 = sT[4][1];
         double v[12] = {0};
-        for (int k = first(t0); k < t1; k += nt) {
-            const int2 ij = D.p14_ij[k];
+        uint2 r = carry, rn;
+        carry = carry_after(4);
+        for (int k = kfirst(4); k < t1; k += nt, r = rn) {
+            rn = next_rec(4, k);
+            int at[4];
+            rec_atoms(r, at);
             double F[3], rd[3], de, dv;
-            eval_14k<T>(P, ij.x - a0, ij.y - a0, D.p14_k[k], dyn, F, rd, de, dv);
+            eval_14k<T>(P, at[0], at[1], ((const double4*)D.tab[4])[rec_par(r)], dyn, F, rd, de, dv);
             const int sl = so[4] + 2 * (k - t0);
             put(sl, F, 1.0); put(sl + 1, F, -1.0);
             if (TENS) tens_pair(F, rd);
             if (full) { v[0] += de; v[1] += dv; vir_pair(v + 2, F, rd); }
         }
-        base += t1 - t0;
         if (full) {
             const int idx[12] = {A_ELC14, A_VDW14, A_V14, A_VT14 + 0, A_VT14 + 1, A_VT14 + 2, A_VT14 + 3,
                                  A_VT14 + 4, A_VT14 + 5, A_VT14 + 6, A_VT14 + 7, A_VT14 + 8};
@@ -735,18 +786,22 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
         }
     }
     if (mask & 32) {
-        int t0, t1; range(5, t0, t1);
+        const int t0 = sT[5][0], t1 = sT[5][1];
         double v[11] = {0};
-        for (int k = first(t0); k < t1; k += nt) {
-            const int2 ij = D.expair[k];
+        uint2 r = carry, rn;
+        carry = carry_after(5);
+        for (int k = kfirst(5); k < t1; k += nt, r = rn) {
+            rn = next_rec(5, k);
+            int at[4];
+            rec_atoms(r, at);
             double F[3], rd[3], e;
-            eval_excl<MIXED>(P, ij.x - a0, ij.y - a0, D.ex_q[k], D.spl64, D.spl32, D.nspl, D.hspl, dyn, F, rd, e);
+            eval_excl<MIXED>(P, at[0], at[1], __ldg(D.tab[5] + rec_par(r)), D.spl64, D.spl32, D.nspl, D.hspl, dyn, F,
+                             rd, e);
             const int sl = so[5] + 2 * (k - t0);
             put(sl, F, 1.0); put(sl + 1, F, -1.0);
             if (TENS) tens_pair(F, rd);
             if (full) { v[0] -= e; vir_pair(v + 1, F, rd); }
         }
-        base += t1 - t0;
         if (full) {
             // pot_elc -= potij; pot_viri_coul -= potij; tensor (lower triangle) += f r
             double w[8] = {v[0], v[0], v[2], v[3], v[4], v[6], v[7], v[10]};
@@ -867,17 +922,16 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
     // per-term constants of the 1-4 and excluded pairs (charges, types and
     // LJ parameters are fixed at init): one load per term in the block kernel
     // instead of a chain of dependent gathers
-    if (t.q && t.ty && t.lj) {
-        std::vector<double4> k14(t.p14.size());
-        for (size_t k = 0; k < t.p14.size(); ++k) {
-            const int i = t.p14[k].x, j = t.p14[k].y;
-            const double2 lp = t.lj[t.ty[i] * t.ntyp + t.ty[j]];
-            k14[k] = make_double4(t.q[i] * t.q[j] * t.f14[k].x, lp.x, lp.y * t.f14[k].y, 0.0);
-        }
-        std::vector<double> qex(t.ex.size());
-        for (size_t k = 0; k < t.ex.size(); ++k) qex[k] = t.q[t.ex[k].x] * t.q[t.ex[k].y];
-        if ((s = up(c, &c->p14_k, k14)) || (s = up(c, &c->ex_q, qex))) return s;
+    if (!t.q || !t.ty || !t.lj) return pgk_fail(c, PGK_E_INVALID, "bonded setup without atom data");
+    std::vector<double4> k14(t.p14.size());
+    for (size_t k = 0; k < t.p14.size(); ++k) {
+        const int i = t.p14[k].x, j = t.p14[k].y;
+        const double2 lp = t.lj[t.ty[i] * t.ntyp + t.ty[j]];
+        k14[k] = make_double4(t.q[i] * t.q[j] * t.f14[k].x, lp.x, lp.y * t.f14[k].y, 0.0);
     }
+    std::vector<double> qex(t.ex.size());
+    for (size_t k = 0; k < t.ex.size(); ++k) qex[k] = t.q[t.ex[k].x] * t.q[t.ex[k].y];
+    if ((s = up(c, &c->p14_k, k14)) || (s = up(c, &c->ex_q, qex))) return s;
 
     // ---- block plan ----
     const int cap = blk_slot_cap(c->mixed());
@@ -957,6 +1011,57 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
         (s = up(c, &c->blk_soff, soffv)) || (s = up(c, &c->blk_ip, ipv)) || (s = up(c, &c->blk_incp, incp)) ||
         (s = up(c, &c->blk_inc, inc)))
         return s;
+    // Compact records of the near terms for the block kernel: one uint2 per
+    // term (brec_pack) holding its atoms as indices local to the owning block
+    // (atom - a0 < BLK_LOC_MAX = 512: 9 bits each) and the index of its
+    // parameters in the type's table of distinct parameter tuples (bit-exact
+    // copies of the per-term values, so results do not change).  8 bytes a
+    // term instead of 24-64, so a thread can hold the first record of every
+    // type in registers while the block stages its positions.
+    const int npar[6] = {2, 2, 4, 6, 4, 1};
+    for (int ty = 0; ty < 6; ++ty) {
+        const int nn = c->nnear[ty];
+        if (nn == 0) continue;
+        std::vector<uint2> rec(nn);
+        std::vector<double> tab;
+        std::map<std::array<unsigned long long, 6>, unsigned> seen;
+        for (int b = 0; b < c->nblk; ++b) {
+            const int k0 = tst[ty][b], k1 = b + 1 < c->nblk ? tst[ty][b + 1] : ptr[ty];
+            for (int k = k0; k < k1; ++k) {
+                int at[4] = {0, 0, 0, 0};
+                atoms_of(ty, k, at);
+                unsigned l[4] = {0, 0, 0, 0};
+                for (int q = 0; q < K[ty]; ++q) {
+                    const int d = at[q] - a0v[b];
+                    if (d < 0 || d >= BLK_LOC_MAX) return pgk_fail(c, PGK_E_INVALID, "bonded term outside its block");
+                    l[q] = (unsigned)d;
+                }
+                double pv[6] = {0, 0, 0, 0, 0, 0};
+                switch (ty) {
+                    case 0: pv[0] = t.bp[k].x; pv[1] = t.bp[k].y; break;
+                    case 1: pv[0] = t.ap[k].x; pv[1] = t.ap[k].y; break;
+                    case 2: pv[0] = t.tp[k].x; pv[1] = t.tp[k].y; pv[2] = t.tp[k].z; pv[3] = t.tp[k].w; break;
+                    case 3: for (int q = 0; q < 6; ++q) pv[q] = t.rc[6 * (size_t)k + q]; break;
+                    case 4: pv[0] = k14[k].x; pv[1] = k14[k].y; pv[2] = k14[k].z; pv[3] = k14[k].w; break;
+                    default: pv[0] = qex[k]; break;
+                }
+                std::array<unsigned long long, 6> key{};
+                std::memcpy(key.data(), pv, sizeof(pv));
+                auto it = seen.find(key);
+                unsigned idx;
+                if (it == seen.end()) {
+                    idx = (unsigned)seen.size();
+                    if (idx >= (1u << 28)) return pgk_fail(c, PGK_E_UNSUPPORTED, "too many distinct bonded parameters");
+                    seen.emplace(key, idx);
+                    tab.insert(tab.end(), pv, pv + npar[ty]);
+                } else {
+                    idx = it->second;
+                }
+                rec[k] = make_uint2(l[0] | (l[1] << 9) | (l[2] << 18) | ((l[3] & 31u) << 27), (l[3] >> 5) | (idx << 4));
+            }
+        }
+        if ((s = up(c, &c->brec[ty], rec)) || (s = up(c, &c->btab[ty], tab))) return s;
+    }
     return PGK_OK;
 }
 
@@ -1071,7 +1176,8 @@ static void terms_impl(pgk_ctx* c, int group, int mask, bool want, bool tens) {
     if (c->nblk > 0) {
         TermsDev D{c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl, c->tors_p, c->rb_ijkl, c->rb_c,
                    c->p14_ij, c->p14_f, c->p14_k, c->expair, c->ex_q, c->chrg, c->typ, c->lj64, c->ntyp, c->spl64,
-                   c->spl32, c->nspl, c->hspl};
+                   c->spl32, c->nspl, c->hspl, {}, {}};
+        for (int ty = 0; ty < 6; ++ty) { D.rec[ty] = c->brec[ty]; D.tab[ty] = c->btab[ty]; }
         const int cap = blk_slot_cap(MIXED);
         BlkDev K{c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff, c->blk_ip, c->blk_incp, c->blk_inc, c->nblk, cap};
         const size_t sm = 3 * BLK_LOC_MAX * sizeof(double) + 3 * (size_t)cap * (MIXED ? sizeof(float) : sizeof(double)) +

@@ -740,7 +740,8 @@ pgk_status pgk_free(pgk_ctx* c) {
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
                     c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->qr, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->cg_fit, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,
-                    c->blk_ip, c->blk_incp, c->blk_inc,
+                    c->blk_ip, c->blk_incp, c->blk_inc, c->brec[0], c->brec[1], c->brec[2], c->brec[3], c->brec[4],
+                    c->brec[5], c->btab[0], c->btab[1], c->btab[2], c->btab[3], c->btab[4], c->btab[5],
                     c->mol_of, c->hftyp, c->molecom, c->molevel, c->hf_pot, c->hf_W, c->hf_part, c->hf_rec, c->hf_zs,
                     c->hf_ms, c->lt_mole, c->lt_reg, c->lt_frand, c->lt_dekin, c->hasup, c->out_rec,
                     c->ewk_nv, c->ewk_tab, c->ewk_part, c->ewk_coef, c->ewk_red, c->ewk_out, c->ewk_seg,

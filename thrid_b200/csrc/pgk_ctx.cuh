@@ -109,6 +109,8 @@ struct pgk_ctx {
     int* blk_ip = nullptr;        // [nblk] offset of the block's nloc+1 pointers in blk_incp
     int* blk_incp = nullptr;      // per block and local atom: range in blk_inc
     unsigned short* blk_inc = nullptr;   // local slot ids, per atom by type, term, position
+    uint2* brec[6] = {};          // per type: compact records of the near terms
+    double* btab[6] = {};         // per type: distinct parameter tuples
 
     // ---- constraints ----
     bool short_empty = false;     // no term in the short MTS group
