@@ -888,6 +888,10 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
         a.xq_prune = c->xq_prune; a.rp2 = rp * rp;
         a.clist = c->plist; a.ccnt = c->pcnt;
     }
+    if (c->rec_pre_pair) {
+        PGK_CUDA(c, cudaEventRecord(c->ev_pre_pair, c->st));
+        c->rec_pre_pair_done = true;
+    }
     if (c->mixed()) {
         switch (vmode) {
             case PM_FULL: pair_mixed_launch<PM_FULL>(c, a); break;

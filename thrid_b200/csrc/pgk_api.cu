@@ -142,6 +142,11 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
     const bool ewk_hf = c->hf_ewk_now && c->prm.mts_ewk == flag;
     const bool spme = c->prm.ifspme && c->prm.mts_ewk == flag && !ewk_hf;
     const bool fork = spme && c->st2 && (pairs || mask);
+    // third stream: the bonded terms, released together with the pair kernel
+    // (after the pack and the prune decision) so that the pair kernel's
+    // blocks, on the higher-priority stream, take the SMs first and the
+    // bonded blocks fill in beside them
+    const bool third = fork && c->st3;
     if (fork) {
         PGK_CUDA(c, cudaEventRecord(c->ev_fork, c->st));
         PGK_CUDA(c, cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
@@ -149,24 +154,30 @@ pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_onl
         cudaStream_t main_st = c->st;
         c->st = c->st2;
         s = launch_spme(c, g, ene, vir);
-        if (!s && c->st3) {                 // bonded terms beside the SPME chain
-            PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
-            c->st = c->st3;
-            s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
-            c->st = main_st;
-            if (s) return s;
-            PGK_CUDA(c, cudaEventRecord(c->ev_join3, c->st3));
-        } else {
-            if (!s) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
-            c->st = main_st;
-            if (s) return s;
-            PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
-        }
+        if (!s && !third) s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+        c->st = main_st;
+        if (s) return s;
+        PGK_CUDA(c, cudaEventRecord(c->ev_join, c->st2));
     }
+    bool bonded_after_pair = false;
     if (pairs) {
         if ((s = launch_pack(c))) return s;
         const int vmode = vir ? (tensor_only ? PM_TENS : PM_FULL) : (ene ? PM_ENE : PM_FORCE);
-        if ((s = launch_pair(c, g, vmode))) return s;
+        c->rec_pre_pair = third;
+        c->rec_pre_pair_done = false;
+        s = launch_pair(c, g, vmode);
+        bonded_after_pair = third && c->rec_pre_pair_done;
+        c->rec_pre_pair = false;
+        if (s) return s;
+    }
+    if (third) {
+        if (bonded_after_pair) PGK_CUDA(c, cudaStreamWaitEvent(c->st3, c->ev_pre_pair, 0));
+        cudaStream_t main_st = c->st;
+        c->st = c->st3;
+        s = launch_intra(c, g, mask, ene || vir, vir && tensor_only);
+        c->st = main_st;
+        if (s) return s;
+        PGK_CUDA(c, cudaEventRecord(c->ev_join3, c->st3));
     }
     if (c->nmor && c->prm.mts_mor == flag && (s = launch_morse(c, g, ene || vir))) return s;   // calforce.F90:360-400
     if (fork) {
@@ -318,14 +329,20 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return PGK_E_CUDA; }
+    // the context's stream (pack, pair kernel, integrator) at the highest
+    // priority, the SPME and bonded streams at the lowest: blocks of the pair
+    // kernel are dispatched before theirs when SMs free up
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess) { delete c; return PGK_E_CUDA; }
     c->pool = device_pool();
     if (!c->pool) { cudaStreamDestroy(c->st); delete c; return PGK_E_CUDA; }
-    if (cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithPriority(&c->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->st3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_join3, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_join3, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_pre_pair, cudaEventDisableTiming) != cudaSuccess) {
         pgk_free(c);
         return PGK_E_CUDA;
     }
@@ -756,6 +773,7 @@ pgk_status pgk_free(pgk_ctx* c) {
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->ev_join3) cudaEventDestroy(c->ev_join3);
+    if (c->ev_pre_pair) cudaEventDestroy(c->ev_pre_pair);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return PGK_OK;
@@ -1111,7 +1129,8 @@ static pgk_status run_md(pgk_ctx* c, int kind, int64_t ini, int64_t end, const p
                     cudaGraphDestroy(g);
                 } else {
                     cudaGraphExec_t ex = nullptr;
-                    cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                    // node priorities: the pair kernel's stream outranks the others
+                    cudaError_t ie = cudaGraphInstantiateWithFlags(&ex, g, cudaGraphInstantiateFlagUseNodePriority);
                     cudaGraphDestroy(g);
                     PGK_CUDA(c, ie);
                     it = c->graphs.emplace(key, pgk_ctx::GraphEntry{ex, nl, c->list_epoch}).first;

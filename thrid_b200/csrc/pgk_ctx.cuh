@@ -46,6 +46,10 @@ struct pgk_ctx {
     cudaStream_t st2 = nullptr;   // SPME chain of a force evaluation
     cudaStream_t st3 = nullptr;   // bonded terms of a force evaluation
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
+    // recorded by launch_pair just before the pair kernel when rec_pre_pair
+    // is set: the bonded terms of a forked evaluation wait for it
+    cudaEvent_t ev_pre_pair = nullptr;
+    bool rec_pre_pair = false, rec_pre_pair_done = false;
     cudaMemPool_t pool = nullptr; // the device's memory pool (pgk_dmalloc)
     std::string err;
     long long launches = 0;
