@@ -549,7 +549,7 @@ pgk_status launch_mklist(pgk_ctx* c) {
         c->list_valid = true;
         ++c->list_epoch;
         if (c->prune_buffer > 0.f) PGK_CUDA(c, cudaMemsetAsync(&c->prune->force, 1, 1, c->st));   // re-prune
-        return PGK_OK;
+        return pair_autotune(c);      // once per context
     }
     return pgk_fail(c, PGK_E_LIST_OVERFLOW, "pair list overflow after regrowth");
 }

@@ -25,6 +25,9 @@
 // 4-byte entry, one 16-byte (32-byte FP64) position and one 4-byte type
 // gather per (cluster, j) entry.
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "pgk_ctx.cuh"
@@ -808,7 +811,7 @@ static void pair_mixed_launch2(pgk_ctx* c, const PairArgs& a) {
     size_t sm = (size_t)((FRAME ? 0 : 1) + (ENE ? 1 : 0)) * c->nspl * sizeof(float4) +
                 (size_t)((c->ntyp * c->ntyp + 1) & ~1) * sizeof(float2);
     if (FRAME) sm += (size_t)(nt / 32) * 4 * c->ntyp * sizeof(float4);
-    long long blocks = (long long)c->nsm * pair_minb(FRAME);
+    long long blocks = (long long)c->nsm * pair_minb(FRAME) * (FRAME ? std::max(c->pair_waves, 1) : 1);
     const long long need = (c->ncl + nt / 32 - 1) / (nt / 32);
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
@@ -856,8 +859,8 @@ pgk_status launch_pair_finish(pgk_ctx* c, int group) {
 }
 
 // vmode: PM_FORCE / PM_ENE / PM_TENS / PM_FULL (see above)
-pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
-    if (c->ncl <= 0) return PGK_OK;
+// the pair kernel's arguments for one MTS group, reading the book rows
+static PairArgs pair_args(pgk_ctx* c, int group) {
     PairArgs a;
     a.clist = c->clist; a.ccnt = c->ccnt; a.ccap = c->ccap; a.ncl = c->ncl;
     a.typ_s = c->typ_s; a.perm = c->perm; a.ntyp = c->ntyp; a.nspl = c->nspl;
@@ -879,6 +882,77 @@ pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
     a.fsort = c->fsort; a.fstride = c->npad_cap;
     a.P = nullptr; a.blist = nullptr; a.bcnt = nullptr; a.plist = nullptr; a.pcnt = nullptr; a.xq_prune = nullptr;
     a.rp2 = 0.f;
+    return a;
+}
+
+// ---- autotuned grid of the cluster-frame pair kernel ---------------------------
+// The packed body's blocks take fixed chunks of cluster rows, five blocks a
+// SM.  In one wave the chunks finish unevenly; several waves of smaller
+// chunks balance better, at the cost of more block starts.  At its first
+// list build a context times the regular body (force only, on the book rows)
+// with 1 to 4 waves and keeps the fastest (on the 200k-atom butane rows: 0.31,
+// 0.28, 0.26, 0.28 ms per evaluation, and the step time follows); the
+// choice changes no result (each cluster row is summed by one warp in the
+// same order whatever block runs it).  PGK_AUTOTUNE=0 keeps 3 waves.
+static std::mutex g_pair_tune_mu;
+static std::map<int, std::string> g_pair_tune;       // cluster count -> table line
+
+pgk_status pair_autotune(pgk_ctx* c) {
+    if (c->pair_tuned) return PGK_OK;
+    c->pair_tuned = true;
+    c->pair_waves = 3;
+    const char* env = getenv("PGK_AUTOTUNE");
+    if ((env && atoi(env) == 0) || !c->mixed() || c->ncl <= 0 || !frame_ok(c) || c->no_frame) return PGK_OK;
+    pgk_status s;
+    if ((s = launch_pack(c))) return s;               // current positions into the sorted slots
+    const PairArgs a = pair_args(c, 0);
+    const bool sc = a.rr2f == a.rl2f;
+    cudaEvent_t e0, e1;
+    PGK_CUDA(c, cudaEventCreate(&e0));
+    PGK_CUDA(c, cudaEventCreate(&e1));
+    float us[5] = {0, 0, 0, 0, 0}, best_us = 1e30f;
+    int best = 3;
+    const long long l0 = c->launches;
+    for (int w = 1; w <= 4; ++w) {
+        c->pair_waves = w;
+        for (int r = 0; r < 4; ++r) {                 // one warm-up, three timed
+            if (r == 1) PGK_CUDA(c, cudaEventRecord(e0, c->st));
+            if (sc) pair_mixed_launch2<PM_FORCE, true, true>(c, a);
+            else pair_mixed_launch2<PM_FORCE, true, false>(c, a);
+        }
+        PGK_CUDA(c, cudaEventRecord(e1, c->st));
+        PGK_CUDA(c, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PGK_CUDA(c, cudaEventElapsedTime(&ms, e0, e1));
+        us[w] = ms * 1e3f / 3.f;
+        if (us[w] < best_us) { best_us = us[w]; best = w; }
+    }
+    c->launches = l0;                                 // not part of any step
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->pair_waves = best;
+    // the timing launches' forces out of the slot buffer
+    PGK_CUDA(c, cudaMemsetAsync(c->fsort, 0, sizeof(long long) * 3 * (size_t)c->npad_cap, c->st));
+    PGK_CUDA(c, cudaStreamSynchronize(c->st));
+    char line[256];
+    snprintf(line, sizeof(line),
+             "pair %d clusters (%d atoms) fp32: waves of blocks %d (1: %.1f us, 2: %.1f us, 3: %.1f us, 4: %.1f us)\n",
+             c->ncl, c->natom, best, us[1], us[2], us[3], us[4]);
+    std::lock_guard<std::mutex> lk(g_pair_tune_mu);
+    g_pair_tune[c->ncl] = line;
+    return PGK_OK;
+}
+
+std::string pair_tuning_text() {
+    std::lock_guard<std::mutex> lk(g_pair_tune_mu);
+    std::string t;
+    for (auto& kv : g_pair_tune) t += kv.second;
+    return t;
+}
+
+pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish) {
+    if (c->ncl <= 0) return PGK_OK;
+    PairArgs a = pair_args(c, group);
     const bool pruned = c->mixed() && c->prune_buffer > 0.f;
     if (pruned) {
         const float rp = (float)std::sqrt(a.rmax2) + c->prune_buffer;

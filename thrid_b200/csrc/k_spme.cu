@@ -1155,6 +1155,7 @@ extern "C" int64_t pgk_tuning_table(char* buf, int64_t cap) {
             t += line;
         }
     }
+    t += pair_tuning_text();
     if (buf && cap > 0) {
         const size_t m = std::min((size_t)cap - 1, t.size());
         memcpy(buf, t.data(), m);

@@ -159,6 +159,8 @@ struct pgk_ctx {
     PruneDev* prune = nullptr;
     float prune_buffer = 0.f;     // A; 0 = no pruning (pair kernel reads the book rows)
     bool no_frame = false;        // PGK_PAIR_FRAME=0: always the per-pair minimum image
+    int pair_waves = 3;           // waves of blocks of the cluster-frame pair kernel (pair_autotune)
+    bool pair_tuned = false;
     int ccap = 0;
     int4* xq = nullptr;           // mixed: fixed-point fractional coords + q bits
     long long* fsort = nullptr;   // mixed: pair forces by sorted slot, [3][npad_cap] int64 fixed point (kept zero between uses)
@@ -307,6 +309,8 @@ pgk_status launch_pack(pgk_ctx* c);
 // finish = false: the caller launches launch_pair_finish itself (mixed: the
 // sorted-slot forces into the accumulator, the pruned-row regrouping)
 pgk_status launch_pair(pgk_ctx* c, int group, int vmode, bool finish = true);
+pgk_status pair_autotune(pgk_ctx* c);   // at the first list build (outside any capture)
+std::string pair_tuning_text();
 pgk_status launch_pair_finish(pgk_ctx* c, int group);
 pgk_status launch_excl(pgk_ctx* c, int group, bool ene, bool vir);
 pgk_status count_pairs(pgk_ctx* c, long long* npair, long long* nentries, long long* nbits = nullptr);
