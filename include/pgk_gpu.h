@@ -525,12 +525,14 @@ pgk_status pgk_server_release(pgk_server* sv, int64_t id);
 /* Finishes every queued request, then stops the workers. */
 pgk_status pgk_server_free(pgk_server* sv);
 
-/* Launch shapes chosen by the engine's autotuner, as text (one line per SPME
- * grid shape and precision: pencils per block of each FFT pass and its
- * measured time).  Every context measures the candidates for its grid shape
- * at pgk_init unless the process already holds a choice for that shape
- * (PGK_AUTOTUNE=0 in the environment keeps the fixed defaults); the choice
- * does not change any result.  Copies at most cap bytes (NUL-terminated)
+/* Launch shapes chosen by the engine's autotuner, as text: one line per SPME
+ * grid shape and precision (pencils per block of each FFT pass and its
+ * measured time; every context measures the candidates for its grid shape
+ * at pgk_init unless the process already holds a choice for that shape) and
+ * one line per mixed-precision pair list in the cluster frame (waves of
+ * blocks of the pair kernel, 1 to 4, timed at the context's first list
+ * build).  PGK_AUTOTUNE=0 in the environment keeps the fixed defaults; no
+ * choice changes any result.  Copies at most cap bytes (NUL-terminated)
  * and returns the length needed.  No counterpart in the reference. */
 int64_t pgk_tuning_table(char* buf, int64_t cap);
 
