@@ -688,9 +688,9 @@ pgk_status pgk_init(const pgk_system* s, const pgk_params* p, pgk_ctx** out) {
         cap = ((cap + 31) / 32) * 32;
         c->ccap = std::max(cap, 32);
         // pruned list buffer (mixed): PGK_PRUNE_BUFFER overrides the 0.7 A default
-        // (200k-atom butane NPT: 0.607 ms per step against 0.609 at 1 A and 0.607
-        // at 0.8 A, the pair kernel 0.307 against 0.320 ms); 0 disables pruning,
-        // as does a book skin too thin for the buffer
+        // (200k-atom butane NPT: 0.607 ms per step against 0.609 at 1 A with one
+        // wave of pair blocks; 0.587 ms at 0.6, 0.7 and 0.8 A with the autotuned
+        // waves); 0 disables pruning, as does a book skin too thin for the buffer
         if (c->mixed()) {
             const char* pf = getenv("PGK_PAIR_FRAME");
             c->no_frame = pf && atoi(pf) == 0;
