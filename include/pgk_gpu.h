@@ -528,11 +528,13 @@ pgk_status pgk_server_free(pgk_server* sv);
 /* Launch shapes chosen by the engine's autotuner, as text: one line per SPME
  * grid shape and precision (pencils per block of each FFT pass and its
  * measured time; every context measures the candidates for its grid shape
- * at pgk_init unless the process already holds a choice for that shape) and
- * one line per mixed-precision pair list in the cluster frame (waves of
- * blocks of the pair kernel, 1 to 4, timed at the context's first list
- * build).  PGK_AUTOTUNE=0 in the environment keeps the fixed defaults; no
- * choice changes any result.  Copies at most cap bytes (NUL-terminated)
+ * at pgk_init unless the process already holds a choice for that shape;
+ * PGK_AUTOTUNE=0 in the environment keeps the fixed defaults; the choice
+ * changes no result).  With PGK_PAIR_AUTOTUNE=1 also one line per
+ * mixed-precision pair list in the cluster frame: the waves of blocks of the
+ * pair kernel (1 to 4) timed at the context's first list build, which change
+ * no force but the last bits of the kernel's FP32 energy and virial partials
+ * (by default the kernel runs a fixed 3 waves).   Copies at most cap bytes (NUL-terminated)
  * and returns the length needed.  No counterpart in the reference. */
 int64_t pgk_tuning_table(char* buf, int64_t cap);
 

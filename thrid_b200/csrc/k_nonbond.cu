@@ -885,15 +885,19 @@ static PairArgs pair_args(pgk_ctx* c, int group) {
     return a;
 }
 
-// ---- autotuned grid of the cluster-frame pair kernel ---------------------------
+// ---- grid of the cluster-frame pair kernel ---------------------------------------
 // The packed body's blocks take fixed chunks of cluster rows, five blocks a
 // SM.  In one wave the chunks finish unevenly; several waves of smaller
-// chunks balance better, at the cost of more block starts.  At its first
-// list build a context times the regular body (force only, on the book rows)
-// with 1 to 4 waves and keeps the fastest (on the 200k-atom butane rows: 0.31,
-// 0.28, 0.26, 0.28 ms per evaluation, and the step time follows); the
-// choice changes no result (each cluster row is summed by one warp in the
-// same order whatever block runs it).  PGK_AUTOTUNE=0 keeps 3 waves.
+// chunks balance better, at the cost of more block starts.  Timing the
+// regular body (force only, on the book rows) with 1 to 4 waves on the
+// 200k-atom butane rows gives 0.33, 0.30, 0.27, 0.29 ms per evaluation, and
+// the step time follows: the kernel runs 3 waves.  Forces do not depend on
+// the grid (each row's pair forces are summed by one warp and added as
+// int64), but the energy and virial partials are FP32 sums per warp over the
+// rows a warp takes, which follow the grid; so the wave count is fixed (the
+// same grid, the same bits, run after run) and the per-context measurement
+// runs only when PGK_PAIR_AUTOTUNE=1 (at the context's first list build; the
+// choice is listed in the tuning table).
 static std::mutex g_pair_tune_mu;
 static std::map<int, std::string> g_pair_tune;       // cluster count -> table line
 
@@ -901,8 +905,8 @@ pgk_status pair_autotune(pgk_ctx* c) {
     if (c->pair_tuned) return PGK_OK;
     c->pair_tuned = true;
     c->pair_waves = 3;
-    const char* env = getenv("PGK_AUTOTUNE");
-    if ((env && atoi(env) == 0) || !c->mixed() || c->ncl <= 0 || !frame_ok(c) || c->no_frame) return PGK_OK;
+    const char* env = getenv("PGK_PAIR_AUTOTUNE");
+    if (!env || atoi(env) == 0 || !c->mixed() || c->ncl <= 0 || !frame_ok(c) || c->no_frame) return PGK_OK;
     pgk_status s;
     if ((s = launch_pack(c))) return s;               // current positions into the sorted slots
     const PairArgs a = pair_args(c, 0);
