@@ -508,16 +508,12 @@ __global__ void k_excl(const double* __restrict__ pos, const double* __restrict_
 }
 
 // ---- block kernel (near terms) ---------------------------------------------------
+// what the block kernel reads besides positions and the block plan: the
+// compact near-term records and parameter tables of each type (bonded_setup)
+// and the spline tables of the excluded-pair correction
 struct TermsDev {
-    const int2* bond_ij; const double2* bond_p;
-    const int4* angl_ijk; const double2* angl_p;
-    const int4* tors_ijkl; const double4* tors_p;
-    const int4* rb_ijkl; const double* rb_c;
-    const int2* p14_ij; const double2* p14_f; const double4* p14_k;
-    const int2* expair; const double* ex_q;
-    const double* chrg; const int* typ; const double2* lj64; int ntyp;
     const double4* spl64; const float4* spl32; int nspl; double hspl;
-    const uint2* rec[6]; const double* tab[6];    // compact near-term records, parameter tables
+    const uint2* rec[6]; const double* tab[6];
 };
 struct BlkDev {
     const int* a0; const int* nloc; const int* t; const int* soff; const int* ip; const int* incp;
@@ -609,9 +605,19 @@ __global__ void __launch_bounds__(BLK_THREADS, 2) k_intra_blk(const double* __re
     // the next record one term ahead, and at its start the first record of
     // the next enabled type (carry), so no record load waits in the open
     auto kfirst = [&](int ty) { return sT[ty][0] + ((tid - sT[ty][2]) % nt + nt) % nt; };
+    auto rec_at = [&](int ty, int k) {       // constant indices into D.rec (no local copy of D)
+        switch (ty) {
+            case 0: return __ldg(D.rec[0] + k);
+            case 1: return __ldg(D.rec[1] + k);
+            case 2: return __ldg(D.rec[2] + k);
+            case 3: return __ldg(D.rec[3] + k);
+            case 4: return __ldg(D.rec[4] + k);
+            default: return __ldg(D.rec[5] + k);
+        }
+    };
     auto first_rec = [&](int ty) {
         const int k = kfirst(ty);
-        return k < sT[ty][1] ? __ldg(D.rec[ty] + k) : make_uint2(0u, 0u);
+        return k < sT[ty][1] ? rec_at(ty, k) : make_uint2(0u, 0u);
     };
     auto next_rec = [&](int ty, int k) {
         return k + nt < sT[ty][1] ? __ldg(D.rec[ty] + k + nt) : make_uint2(0u, 0u);
@@ -920,8 +926,9 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
         (s = up(c, &c->p14_f, t.f14)) || (s = up(c, &c->expair, t.ex)))
         return s;
     // per-term constants of the 1-4 and excluded pairs (charges, types and
-    // LJ parameters are fixed at init): one load per term in the block kernel
-    // instead of a chain of dependent gathers
+    // LJ parameters are fixed at init), entries of the block kernel's
+    // parameter tables below: one table read per term instead of the chain
+    // charges -> types -> LJ row
     if (!t.q || !t.ty || !t.lj) return pgk_fail(c, PGK_E_INVALID, "bonded setup without atom data");
     std::vector<double4> k14(t.p14.size());
     for (size_t k = 0; k < t.p14.size(); ++k) {
@@ -931,7 +938,6 @@ pgk_status bonded_setup(pgk_ctx* c, HostTerms& t, const std::vector<int>&, const
     }
     std::vector<double> qex(t.ex.size());
     for (size_t k = 0; k < t.ex.size(); ++k) qex[k] = t.q[t.ex[k].x] * t.q[t.ex[k].y];
-    if ((s = up(c, &c->p14_k, k14)) || (s = up(c, &c->ex_q, qex))) return s;
 
     // ---- block plan ----
     const int cap = blk_slot_cap(c->mixed());
@@ -1174,9 +1180,7 @@ static void terms_impl(pgk_ctx* c, int group, int mask, bool want, bool tens) {
     void* facc = c->facc[group];
     const int w = want ? 1 : 0;
     if (c->nblk > 0) {
-        TermsDev D{c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl, c->tors_p, c->rb_ijkl, c->rb_c,
-                   c->p14_ij, c->p14_f, c->p14_k, c->expair, c->ex_q, c->chrg, c->typ, c->lj64, c->ntyp, c->spl64,
-                   c->spl32, c->nspl, c->hspl, {}, {}};
+        TermsDev D{c->spl64, c->spl32, c->nspl, c->hspl, {}, {}};
         for (int ty = 0; ty < 6; ++ty) { D.rec[ty] = c->brec[ty]; D.tab[ty] = c->btab[ty]; }
         const int cap = blk_slot_cap(MIXED);
         BlkDev K{c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff, c->blk_ip, c->blk_incp, c->blk_inc, c->nblk, cap};

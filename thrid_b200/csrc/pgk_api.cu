@@ -753,7 +753,7 @@ pgk_status pgk_free(pgk_ctx* c) {
     void* bufs[] = {c->pos, c->vel, c->pos_old, c->mass, c->invmass, c->chrg, c->typ, c->facc[0], c->facc[1], c->acc,
                     c->dyn, c->chain, c->status, c->lj64, c->lj32, c->spl64, c->spl32, c->exs_idx, c->exs_list, c->exs_rng,
                     c->expair, c->mol_idx, c->mol_list, c->bond_ij, c->bond_p, c->angl_ijk, c->angl_p, c->tors_ijkl,
-                    c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->p14_k, c->ex_q, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
+                    c->tors_p, c->rb_ijkl, c->rb_c, c->p14_ij, c->p14_f, c->cg_idx, c->cg_list, c->c_ij, c->c_d,
                     c->cell_of, c->subkey, c->cell_cnt, c->cell_start, c->cell_fill, c->perm, c->iperm, c->pos_s, c->clist,
                     c->ccnt, c->xq, c->xq64, c->fsort, c->plist, c->pcnt, c->xq_prune, c->prune, c->typ_s, c->counters, c->qacc, c->qc, c->qr, c->bsp,
                     c->plan[0].tw, c->plan[1].tw, c->plan[2].tw, c->fout, c->cg_span, c->cg_fit, c->blk_a0, c->blk_nloc, c->blk_t, c->blk_soff,

@@ -95,8 +95,6 @@ struct pgk_ctx {
     int ntors = 0; int4* tors_ijkl = nullptr; double4* tors_p = nullptr;   // (barhig/divfac, phsang, period, cos(phs))
     int ntorsrb = 0; int4* rb_ijkl = nullptr; double* rb_c = nullptr;       // [6*n]
     int n14 = 0; int2* p14_ij = nullptr; double2* p14_f = nullptr;          // (elc fac, vdw fac)
-    double4* p14_k = nullptr;   // per 1-4 pair: (q_i q_j elc fac, R^2, eps vdw fac, 0)
-    double* ex_q = nullptr;     // per excluded pair: q_i q_j
 
     // ---- bonded block plan ----
     // Per type (bond, angle, tors, RB, 1-4, excl) the terms [0, nnear) are the
