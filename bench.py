@@ -525,6 +525,10 @@ _pg = None
 
 
 def dist_init():
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): NCCL
+    on GPUs, gloo on a host without CUDA (the multi-process tests).  The
+    ranks run independent replicas; the process group only carries the
+    barriers around the timed window and the max over ranks of its time."""
     global _pg
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -533,8 +537,10 @@ def dist_init():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        cuda = torch.cuda.is_available()
+        if cuda:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if cuda else "gloo", timeout=datetime.timedelta(seconds=600))
         _pg = dist
     return rank, world, local
 
@@ -545,12 +551,20 @@ def dist_barrier(world):
 
 
 def dist_max(x, world):
+    """Max of x over the ranks (the job's time is its slowest rank's)."""
     if world > 1 and _pg is not None:
         import torch
-        t = torch.tensor([float(x)], device="cuda")
+        dev = "cuda" if _pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(x)], device=dev)
         _pg.all_reduce(t, op=_pg.ReduceOp.MAX)
         return float(t.item())
     return float(x)
+
+
+def dist_close(world):
+    if world > 1 and _pg is not None:
+        _pg.barrier()
+        _pg.destroy_process_group()
 
 
 def min_intermolecular_distance(s, atoms_per_molecule):
@@ -799,9 +813,7 @@ def main():
         out = run_ours(args, rank, world, local)
     if rank == 0 and out is not None:
         print(json.dumps(out))
-    if world > 1 and _pg is not None:
-        _pg.barrier()
-        _pg.destroy_process_group()
+    dist_close(world)
 
 
 if __name__ == "__main__":
