@@ -175,7 +175,7 @@ def run_ours(args, rank, world, local_rank):
     nxt = step0 + nsteps
     # ---- end to end through the public API with host buffers ----
     e2e = None if args.no_e2e else e2e_leg(eng, s, md, nxt, nsteps, world)
-    # ---- the all-FP64 device path on the same state (north-star comparison) ----
+    # ---- the all-FP64 device path on the same state (the mixed-vs-FP64 comparison) ----
     fp64 = None if args.no_fp64 else fp64_leg(eng, s, md, stream)
     # ---- rooflines of the dominant kernel and the HBM-bound kernels, measured
     #      live (last: the kick/drift launches move the atoms) ----
@@ -204,7 +204,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_configs:
         out["other_configs"] = other_configs(args)
     if rank == 0 and world == 1 and not args.no_serve:
-        # the serving workload in a bounded form: 32 seeded
+        # the replica-serving workload in a bounded form: 32 seeded
         # replicas x 2,000 NVE steps, against this line's single large system
         sa = argparse.Namespace(**vars(args))
         sa.serve_replicas, sa.serve_steps, sa.serve_hf = 32, 2000, False
@@ -285,7 +285,7 @@ def e2e_leg(eng, s, md, start, nsteps, world):
             "path": "pgk_upload_state (pinned x, v) -> pgk_moldyn_mtk (1 step) -> pgk_download_state (pinned x, v)"}
 
 
-# algorithmic bytes per unit of the HBM-bound kernels (SURVEY 8(d) formulas)
+# algorithmic bytes per unit of the HBM-bound kernels (formula beside each entry)
 HBM_KERNELS = (
     # (bench id, name, profile summary, unit, bytes(natom, K3, entries))
     (1, "k_spread_rows<5> (fill_charge_grid)", "k_spread_rows_butane200k.md",

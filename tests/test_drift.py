@@ -1,5 +1,5 @@
 """NVE energy drift of the mixed-precision path against the FP64 device path
-(mixed drift within 2x the FP64 drift).
+(the mixed path's bound: its drift within 2x the FP64 drift).
 
 Total energy E = pot_tot + sum(m v^2)/2 is sampled every 100 steps of a
 rigid-water NVE run (RATTLE, 1 fs, 2 ps); the drift is the slope of a

@@ -3,7 +3,7 @@
 Bars (written here, per result):
   pair list          bit-exact: identical nb_indexall / nb_listall / nlistnball
   FP64 device path   force RMS relative error <= 1e-12, energies <= 1e-10 relative
-  mixed precision    force RMS relative error <= 1e-5
+  mixed precision    force RMS relative error <= 1e-5 (the mixed path's accuracy bound)
   MD trajectories    FP64 positions within 1e-9 A of the oracle after the steps run
 """
 import numpy as np
