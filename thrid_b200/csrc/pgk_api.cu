@@ -124,11 +124,14 @@ pgk_status read_status(pgk_ctx* c) {
 
 // one MTS group of calforce (calforce.F90:8-1073); tensor_only selects the
 // pair kernel's combined-tensor mode (anisotropic MTK steps without output)
-// Two streams: the SPME chain and then the bonded terms run on the second
-// stream beside the pair kernel and its finishing kernels (the pair kernel is
-// issue-bound, the SPME and bonded kernels latency-bound, so they fill each
-// other's idle issue slots).  Every add into the shared force and energy accumulators is
-// atomic (int64 in mixed precision: exact and independent of the interleaving).
+// Three streams: the SPME chain on the second and the bonded terms on the
+// third run beside the pack, the pair kernel and its finishing kernel on the
+// context's stream (the pair kernel is issue-bound, the SPME and bonded
+// kernels latency-bound, so they fill each other's idle issue slots).  The
+// context's stream has the highest priority and the bonded terms wait for
+// the prune decision, so the pair kernel's blocks are dispatched first.
+// Every add into the shared force and energy accumulators is atomic (int64 in
+// mixed precision: exact and independent of the interleaving).
 pgk_status force_group(pgk_ctx* c, int flag, bool ene, bool vir, bool tensor_only = false) {
     int g = flag == PGK_MTS_LONG ? 0 : 1;
     pgk_status s;
